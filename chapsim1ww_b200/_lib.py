@@ -1,0 +1,86 @@
+"""ctypes binding of libchapsim.so (the sm_100a CUDA library) and of its C ABI.
+
+The shared library is built in-tree (chapsim1ww_b200/libchapsim.so) by
+``chapsim1ww_b200.build.build()``.  There is no CPU fallback: importing a
+symbol from a missing library raises immediately.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libchapsim.so")
+
+CHAPSIM_OK = 0
+ERRORS = {
+    1: "CHAPSIM_ERR_ARG", 2: "CHAPSIM_ERR_CUDA", 3: "CHAPSIM_ERR_NOMEM", 4: "CHAPSIM_ERR_STATE",
+    5: "CHAPSIM_ERR_NUMERIC", 6: "CHAPSIM_ERR_UNSUPPORTED", 7: "CHAPSIM_ERR_NODEVICE",
+}
+ITG, IIO = 1, 2
+FP64, MIXED = 0, 1
+F_U, F_V, F_W, F_P, F_PHI, F_RHSPHI, F_H0U, F_H0V, F_H0W = range(9)
+R_DIVMAX, R_BULK, R_NANCOUNT = 0, 1, 2
+PHASES = ["rhs", "adix", "adiz", "adiy", "fftx", "fftz", "ysolve", "ifftz", "ifftx", "corr"]
+
+
+class ChapsimConfig(ctypes.Structure):
+    """Mirror of ``chapsim_config`` in include/chapsim.h."""
+    _fields_ = [
+        ("struct_size", ctypes.c_int32), ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+        ("lx", ctypes.c_double), ("lz", ctypes.c_double), ("str2", ctypes.c_double),
+        ("istr2", ctypes.c_int32), ("flowdrvtp", ctypes.c_int32),
+        ("ren", ctypes.c_double), ("dt", ctypes.c_double), ("cfgv", ctypes.c_double),
+        ("precision", ctypes.c_int32), ("device", ctypes.c_int32),
+    ]
+
+
+# (name, restype, argtypes) for every symbol declared in include/chapsim.h
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+_DP = ctypes.POINTER(ctypes.c_double)
+SIGNATURES = [
+    ("chapsim_config_default", _I, [ctypes.POINTER(ChapsimConfig)]),
+    ("chapsim_create", _I, [ctypes.POINTER(ChapsimConfig), ctypes.POINTER(_P)]),
+    ("chapsim_destroy", _I, [_P]),
+    ("chapsim_last_error", ctypes.c_char_p, [_P]),
+    ("chapsim_sync", _I, [_P]),
+    ("chapsim_field_len", _I64, [_P]),
+    ("chapsim_set_field", _I, [_P, _I, _I, _P, _I64]),
+    ("chapsim_get_field", _I, [_P, _I, _I, _P, _I64]),
+    ("chapsim_set_field_device", _I, [_P, _I, _I, _P, _I64]),
+    ("chapsim_get_field_device", _I, [_P, _I, _I, _P, _I64]),
+    ("chapsim_get_mesh", _I, [_P, _I, _P, _I64]),
+    ("chapsim_init_random", _I, [_P, ctypes.c_uint64, _D, _I]),
+    ("chapsim_rk3_mom_tg", _I, [_P, _I]),
+    ("chapsim_step_tg", _I, [_P, _I]),
+    ("chapsim_divg", _I, [_P, _I, _I]),
+    ("chapsim_pois3d", _I, [_P, _I]),
+    ("chapsim_velo_correction", _I, [_P, _I, _I]),
+    ("chapsim_reduce", _I, [_P, _I, _I, _DP]),
+    ("chapsim_get_stream", _I, [_P, ctypes.POINTER(_P)]),
+    ("chapsim_phase_timing", _I, [_P, _I]),
+    ("chapsim_phase_times", _I, [_P, _DP, _I, ctypes.POINTER(_I64)]),
+    ("chapsim_phase_reset", _I, [_P]),
+    ("chapsim_launch_count", _I, [_P, ctypes.POINTER(_I64)]),
+    ("chapsim_launch_count_reset", _I, [_P]),
+]
+
+_lib = None
+
+
+def load():
+    """Load libchapsim.so once; raise if it is missing (no fallback path)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"libchapsim.so not found at {LIB_PATH}; build it with "
+                "`python -c 'import __graft_entry__ as g; g.build()'` or `make -C chapsim1ww_b200/csrc`")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, res, args in SIGNATURES:
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib

@@ -1,0 +1,657 @@
+// C ABI of libchapsim: context life cycle, host-side set-up (mesh, RK and
+// line-solve coefficient tables, FFT plans), field transfer and the substep
+// entry points.  Set-up restates, in host C++, the reference's initialisation
+// routines: CONSPARA (src/CONSPARA.f90:41-73), COORDJR
+// (src/COORDJR.f90:27-143,427-450,495-520), TDMA_COEF
+// (src/TDMA_COEF.f90:53-119), CONS_RKCOEF (src/CONS_RKCOEF.f90:24-54) and
+// FFT99_POIS3D_INIT (src/possion3d_FFT99.f90:54-220).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "chapsim_internal.cuh"
+
+using namespace chapsim;
+
+#define CKC(call)                                                          \
+  do {                                                                     \
+    cudaError_t e_ = (call);                                               \
+    if (e_ != cudaSuccess) {                                               \
+      ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);       \
+      return CHAPSIM_ERR_CUDA;                                             \
+    }                                                                      \
+  } while (0)
+
+#define REQUIRE(cond, code, msg)   \
+  do {                             \
+    if (!(cond)) {                 \
+      if (ctx) ctx->err = (msg);   \
+      return (code);               \
+    }                              \
+  } while (0)
+
+namespace {
+
+uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+// Uniform draw in [-1, 1) keyed by (seed, component, i, j, k), all 1-based.
+double rnd_pm1(uint64_t seed, int comp, int i, int j, int k) {
+  uint64_t ctr = ((uint64_t)comp << 60) ^ ((uint64_t)k << 40) ^ ((uint64_t)j << 20) ^ (uint64_t)i;
+  uint64_t x = splitmix64(splitmix64(seed) ^ ctr);
+  return -1.0 + 2.0 * ((double)(x >> 11) * (1.0 / 9007199254740992.0));
+}
+
+bool factor_plan(int n, FFTPlan &pl) {
+  pl.n = n;
+  pl.nrad = 0;
+  int m = n;
+  const int radices[] = {4, 2, 3, 5, 7, 11};
+  for (int r : radices)
+    while (m % r == 0) {
+      if (pl.nrad >= 16) return false;
+      pl.rad[pl.nrad++] = r;
+      m /= r;
+    }
+  for (int s = pl.nrad; s < 16; ++s) pl.rad[s] = 1;
+  return m == 1;
+}
+
+// Cyclic factor tables for (1 - beta delta) with constant a = c, b = 1 - 2a
+// (TDMAIJI_CYC coefficient-only recurrences, src/TDMAIJI_CYC.f90:100-146).
+void cyc_tables(int n, double a, double *pp, double *h0, double *g2, double &b, double &qq) {
+  const double c = a;
+  b = 1.0 - 2.0 * a;
+  h0[0] = c / b;
+  g2[0] = -a / b;
+  pp[0] = 1.0 / b;
+  for (int i = 1; i <= n - 3; ++i) {
+    pp[i] = 1.0 / (b - h0[i - 1] * a);
+    h0[i] = c * pp[i];
+    g2[i] = -(g2[i - 1] * a) * pp[i];
+  }
+  {
+    const int i = n - 2;
+    pp[i] = 1.0 / (b - h0[i - 1] * a);
+    h0[i] = 0.0;
+    g2[i] = (-c - g2[i - 1] * a) * pp[i];
+  }
+  pp[n - 1] = 0.0;
+  h0[n - 1] = 0.0;
+  g2[n - 1] = 0.0;
+  for (int i = n - 3; i >= 0; --i) g2[i] = -h0[i] * g2[i + 1] + g2[i];
+  qq = b + c * g2[0] + a * g2[n - 2];
+}
+
+}  // namespace
+
+extern "C" {
+
+int chapsim_config_default(chapsim_config *cfg) {
+  if (!cfg) return CHAPSIM_ERR_ARG;
+  memset(cfg, 0, sizeof(*cfg));
+  cfg->struct_size = (int32_t)sizeof(chapsim_config);
+  cfg->nx = 64;
+  cfg->ny = 64;
+  cfg->nz = 64;
+  cfg->lx = 4.0 * M_PI;
+  cfg->lz = 4.0 * M_PI / 3.0;
+  cfg->str2 = 2.0;
+  cfg->istr2 = 1;
+  cfg->flowdrvtp = 1;
+  cfg->ren = 2800.0;
+  cfg->dt = 1e-3;
+  cfg->cfgv = 0.0;
+  cfg->precision = CHAPSIM_FP64;
+  cfg->device = 0;
+  return CHAPSIM_OK;
+}
+
+static void free_all(chapsim_ctx *ctx) {
+  if (ctx->step_graph) cudaGraphExecDestroy(ctx->step_graph);
+  ctx->step_graph = nullptr;
+  for (void *p : ctx->allocs) cudaFree(p);
+  ctx->allocs.clear();
+  for (auto &e : ctx->ev)
+    if (e) { cudaEventDestroy(e); e = nullptr; }
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  ctx->stream = nullptr;
+}
+
+static int dalloc(chapsim_ctx *ctx, void **p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    ctx->err = std::string("cudaMalloc(") + std::to_string(bytes) + "): " + cudaGetErrorString(e);
+    cudaGetLastError();
+    return CHAPSIM_ERR_NOMEM;
+  }
+  ctx->allocs.push_back(*p);
+  return CHAPSIM_OK;
+}
+
+static void setup_mesh(chapsim_ctx *ctx) {
+  const chapsim_config &cf = ctx->cfg;
+  const int ny = cf.ny, nnd2 = ny + 1;
+  auto &ynd = ctx->ynd, &ycc = ctx->ycc, &dyfi = ctx->dyfi, &dyci = ctx->dyci, &wff = ctx->wff,
+       &wfb = ctx->wfb;
+  ynd.assign(ny + 2, 0.0); ycc.assign(ny + 2, 0.0); dyfi.assign(ny + 2, 0.0);
+  dyci.assign(ny + 2, 0.0); wff.assign(ny + 2, 0.0); wfb.assign(ny + 2, 0.0);
+  for (int j = 1; j <= nnd2; ++j) {
+    if (cf.istr2 == 1)
+      ynd[j] = tanh(cf.str2 * ((double)(j - 1) / (double)(nnd2 - 1) - 0.5)) / tanh(cf.str2 * 0.5);
+    else
+      ynd[j] = -1.0 + (double)(j - 1) * (2.0 / (double)ny);
+  }
+  for (int j = 1; j <= ny; ++j) {
+    if (cf.istr2 == 1)
+      ycc[j] = tanh(cf.str2 * (((double)(j - 1) + 0.5) / (double)(nnd2 - 1) - 0.5)) / tanh(cf.str2 * 0.5);
+    else
+      ycc[j] = 0.5 * (ynd[j] + ynd[j + 1]);
+  }
+  for (int j = 1; j <= ny; ++j) dyfi[j] = 1.0 / (ynd[j + 1] - ynd[j]);
+  for (int j = 2; j <= nnd2 - 1; ++j) dyci[j] = 1.0 / ((ynd[j + 1] - ynd[j - 1]) * 0.5);
+  dyci[1] = 2.0 / (ynd[2] - ynd[1]);
+  dyci[nnd2] = 2.0 / (ynd[nnd2] - ynd[ny]);
+  for (int jc = 2; jc <= ny; ++jc) {
+    wff[jc] = (ynd[jc] - ycc[jc - 1]) / (ycc[jc] - ycc[jc - 1]);
+    wfb[jc] = (ycc[jc] - ynd[jc]) / (ycc[jc] - ycc[jc - 1]);
+  }
+  wfb[1] = 1.0; wff[1] = 0.0; wfb[nnd2] = 0.0; wff[nnd2] = 1.0;
+}
+
+// Build every coefficient table into ctx->hcoef and return offsets through
+// the lambda-set pointers after upload.
+static int build_tables(chapsim_ctx *ctx) {
+  const chapsim_config &cf = ctx->cfg;
+  const int nx = cf.nx, ny = cf.ny, nz = cf.nz, lh = nx / 2 + 1, nnd2 = ny + 1;
+  const double dxi = nx / cf.lx, dzi = nz / cf.lz, dxqi = dxi * dxi, dzqi = dzi * dzi;
+  const double cvisc = 1.0 / cf.ren;
+  const std::vector<double> &dyfi = ctx->dyfi, &dyci = ctx->dyci;
+  std::vector<double> &H = ctx->hcoef;
+  H.clear();
+  auto alloc = [&](size_t n) { size_t o = H.size(); H.resize(o + ((n + 1) & ~(size_t)1), 0.0); return o; };
+  const int Y = ny + 2;
+  size_t o_dyfi = alloc(Y), o_dyci = alloc(Y), o_wff = alloc(Y), o_wfb = alloc(Y);
+  for (int j = 0; j < Y; ++j) {
+    H[o_dyfi + j] = dyfi[j]; H[o_dyci + j] = dyci[j]; H[o_wff + j] = ctx->wff[j]; H[o_wfb + j] = ctx->wfb[j];
+  }
+  size_t o_am[3], o_ac[3], o_ap[3];
+  for (int c = 0; c < 3; ++c) { o_am[c] = alloc(Y); o_ac[c] = alloc(Y); o_ap[c] = alloc(Y); }
+  // TDMA_COEF viscous y-operators (src/TDMA_COEF.f90:76-116)
+  for (int c = 0; c < 3; ++c) {
+    double *am = &H[o_am[c]], *ac = &H[o_ac[c]], *ap = &H[o_ap[c]];
+    if (c != 1) {
+      for (int jc = 2; jc <= ny - 1; ++jc) {
+        am[jc] = dyfi[jc] * dyci[jc];
+        ap[jc] = dyfi[jc] * dyci[jc + 1];
+        ac[jc] = -(am[jc] + ap[jc]);
+      }
+      double ucaj = 4.0 / (2.0 / dyci[2] + 1.0 / dyfi[1]);
+      am[1] = 0.0; ap[1] = ucaj * dyci[2]; ac[1] = -ucaj * (dyci[2] + 2.0 * dyfi[1]);
+      ucaj = 4.0 / (2.0 / dyci[ny] + 1.0 / dyfi[ny]);
+      am[ny] = ucaj * dyci[ny]; ap[ny] = 0.0; ac[ny] = -ucaj * (2.0 * dyfi[ny] + dyci[ny]);
+    } else {
+      for (int jc = 2; jc <= ny; ++jc) {
+        am[jc] = dyfi[jc - 1] * dyci[jc];
+        ap[jc] = dyfi[jc] * dyci[jc];
+        ac[jc] = -(am[jc] + ap[jc]);
+      }
+      am[1] = 0.0; ap[1] = 0.0; ac[1] = 1.0;
+      am[nnd2] = 0.0; ap[nnd2] = 0.0; ac[nnd2] = 1.0;
+    }
+  }
+  // Poisson y-operator with Neumann folding (src/TDMA_COEF.f90:53-74)
+  size_t o_amph = alloc(Y), o_acph = alloc(Y), o_apph = alloc(Y);
+  {
+    double *am = &H[o_amph], *ac = &H[o_acph], *ap = &H[o_apph];
+    for (int jc = 1; jc <= ny; ++jc) {
+      am[jc] = dyfi[jc] * dyci[jc];
+      ap[jc] = dyfi[jc] * dyci[jc + 1];
+      if (jc == 1) am[jc] = dyfi[jc] * dyci[jc] * 0.5;
+      if (jc + 1 == nnd2) ap[jc] = dyfi[jc] * dyci[jc + 1] * 0.5;
+    }
+    for (int jc = 1; jc <= ny; ++jc) ac[jc] = -(am[jc] + ap[jc]);
+    ac[1] = am[1] + ac[1]; am[1] = 0.0;
+    ac[ny] = ap[ny] + ac[ny]; ap[ny] = 0.0;
+  }
+  // modified wavenumbers (src/possion3d_FFT99.f90:155-179)
+  size_t o_ak1 = alloc(lh), o_ak3 = alloc(nz);
+  for (int i = 0; i < lh; ++i) H[o_ak1 + i] = 2.0 * (1.0 - cos(2.0 * M_PI * (double)i / (double)nx)) * dxqi;
+  for (int k = 0; k < nz; ++k) {
+    // AN(K) = (K-1) 2 pi for K <= nz/2, -(nz-K+1) 2 pi beyond; cos is even.
+    const int kk = k < nz / 2 ? k : -(nz - k);
+    H[o_ak3 + k] = 2.0 * (1.0 - cos(2.0 * M_PI * (double)kk / (double)nz)) * dzqi;
+  }
+  // RK coefficients (src/CONS_RKCOEF.f90:28-54)
+  const double tgam[4] = {1.0, 8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
+  const double troh[4] = {0.0, 0.0, -17.0 / 60.0, -5.0 / 12.0};
+  size_t o_ya[4][3], o_ypp[4][3], o_yh[4][3], o_x[4][3], o_z[4][3];
+  double xb[4], xa[4], xqq[4], zb[4], za[4], zqq[4];
+  for (int ns = 0; ns < 4; ++ns) {
+    const double alp = tgam[ns] + troh[ns];
+    const double facoe = 0.5 * alp * cf.dt * cvisc;  // MOMFA_tg.f90:30
+    for (int c = 0; c < 3; ++c) {
+      o_ya[ns][c] = alloc(Y); o_ypp[ns][c] = alloc(Y); o_yh[ns][c] = alloc(Y);
+      double *ya = &H[o_ya[ns][c]], *ypp = &H[o_ypp[ns][c]], *yh = &H[o_yh[ns][c]];
+      const double *am = &H[o_am[c]], *ac = &H[o_ac[c]], *ap = &H[o_ap[c]];
+      double hprev = 0.0;
+      for (int j = 1; j <= ny; ++j) {
+        const double a = -facoe * am[j], b = 1.0 - facoe * ac[j], cc = -facoe * ap[j];
+        ya[j] = a;
+        ypp[j] = j == 1 ? 1.0 / b : 1.0 / (b - hprev * a);
+        yh[j] = cc * ypp[j];
+        hprev = yh[j];
+      }
+    }
+    for (int t = 0; t < 3; ++t) { o_x[ns][t] = alloc(nx); o_z[ns][t] = alloc(nz); }
+    xa[ns] = -facoe * dxqi;
+    za[ns] = -facoe * dzqi;
+    cyc_tables(nx, xa[ns], &H[o_x[ns][0]], &H[o_x[ns][1]], &H[o_x[ns][2]], xb[ns], xqq[ns]);
+    cyc_tables(nz, za[ns], &H[o_z[ns][0]], &H[o_z[ns][1]], &H[o_z[ns][2]], zb[ns], zqq[ns]);
+  }
+  // FFT twiddles exp(-2 pi i m / n)
+  size_t o_twx = alloc(2 * (size_t)nx), o_twz = alloc(2 * (size_t)nz);
+  for (int m = 0; m < nx; ++m) {
+    H[o_twx + 2 * m] = cos(2.0 * M_PI * (double)m / nx);
+    H[o_twx + 2 * m + 1] = -sin(2.0 * M_PI * (double)m / nx);
+  }
+  for (int m = 0; m < nz; ++m) {
+    H[o_twz + 2 * m] = cos(2.0 * M_PI * (double)m / nz);
+    H[o_twz + 2 * m + 1] = -sin(2.0 * M_PI * (double)m / nz);
+  }
+  // float twiddles packed after the doubles (2 floats per double slot)
+  size_t o_twx32 = alloc(nx), o_twz32 = alloc(nz);
+  {
+    float *fx = reinterpret_cast<float *>(&H[o_twx32]);
+    for (int m = 0; m < 2 * nx; ++m) fx[m] = (float)H[o_twx + m];
+    float *fz = reinterpret_cast<float *>(&H[o_twz32]);
+    for (int m = 0; m < 2 * nz; ++m) fz[m] = (float)H[o_twz + m];
+  }
+
+  // upload
+  void *p = nullptr;
+  int rc = dalloc(ctx, &p, H.size() * sizeof(double));
+  if (rc) return rc;
+  ctx->dcoef = (double *)p;
+  CKC(cudaMemcpy(ctx->dcoef, H.data(), H.size() * sizeof(double), cudaMemcpyHostToDevice));
+  const double *D = ctx->dcoef;
+  TGDev &d = ctx->d;
+  d.dyfi = D + o_dyfi; d.dyci = D + o_dyci; d.wff = D + o_wff; d.wfb = D + o_wfb;
+  for (int c = 0; c < 3; ++c) { d.amvr[c] = D + o_am[c]; d.acvr[c] = D + o_ac[c]; d.apvr[c] = D + o_ap[c]; }
+  d.amph = D + o_amph; d.acph = D + o_acph; d.apph = D + o_apph;
+  d.ak1 = D + o_ak1; d.ak3 = D + o_ak3;
+  d.dxi = dxi; d.dzi = dzi; d.dxqi = dxqi; d.dzqi = dzqi; d.cvisc = cvisc; d.dt = cf.dt;
+  double volm = 0.0, area = 0.0;
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j) {
+      area += 1.0 / dyfi[j] / dzi;
+      for (int i = 1; i <= nx; ++i) volm += 1.0 / dyfi[j];
+    }
+  d.volm = volm;
+  ctx->area_inlet = area;
+  for (int ns = 0; ns < 4; ++ns) {
+    SubParams &sp = ctx->sp[ns];
+    sp.ns = ns;
+    sp.gam = tgam[ns]; sp.roh = troh[ns]; sp.alp = tgam[ns] + troh[ns];
+    for (int c = 0; c < 3; ++c) { sp.ya[c] = D + o_ya[ns][c]; sp.ypp[c] = D + o_ypp[ns][c]; sp.yh[c] = D + o_yh[ns][c]; }
+    sp.xpp = D + o_x[ns][0]; sp.xh0 = D + o_x[ns][1]; sp.xg2 = D + o_x[ns][2];
+    sp.xa = xa[ns]; sp.xb = xb[ns]; sp.xqq = xqq[ns];
+    sp.zpp = D + o_z[ns][0]; sp.zh0 = D + o_z[ns][1]; sp.zg2 = D + o_z[ns][2];
+    sp.za = za[ns]; sp.zb = zb[ns]; sp.zqq = zqq[ns];
+    sp.flowdrvtp = cf.flowdrvtp;
+    sp.dp_const = -0.5 * cf.cfgv * sp.alp * cf.dt;
+  }
+  ctx->fx.tw64 = reinterpret_cast<const double2 *>(D + o_twx);
+  ctx->fz.tw64 = reinterpret_cast<const double2 *>(D + o_twz);
+  ctx->fx.tw32 = reinterpret_cast<const float2 *>(D + o_twx32);
+  ctx->fz.tw32 = reinterpret_cast<const float2 *>(D + o_twz32);
+  return CHAPSIM_OK;
+}
+
+int chapsim_create(const chapsim_config *cfg, chapsim_ctx **out) {
+  chapsim_ctx *ctx = nullptr;
+  if (!cfg || !out) return CHAPSIM_ERR_ARG;
+  *out = nullptr;
+  if (cfg->struct_size != (int32_t)sizeof(chapsim_config)) return CHAPSIM_ERR_ARG;
+  if (cfg->nx < 8 || cfg->nz < 8 || cfg->ny < 4 || (cfg->nx & 1) || (cfg->nz & 1)) return CHAPSIM_ERR_ARG;
+  if (!(cfg->lx > 0) || !(cfg->lz > 0) || !(cfg->ren > 0) || !(cfg->dt > 0)) return CHAPSIM_ERR_ARG;
+  if (cfg->istr2 != 0 && cfg->istr2 != 1) return CHAPSIM_ERR_ARG;
+  if (cfg->flowdrvtp != 1 && cfg->flowdrvtp != 2) return CHAPSIM_ERR_ARG;
+  if (cfg->precision != CHAPSIM_FP64 && cfg->precision != CHAPSIM_MIXED) return CHAPSIM_ERR_ARG;
+  if (cfg->nx > 4096 || cfg->nz > 4096 || cfg->ny > 4096) return CHAPSIM_ERR_UNSUPPORTED;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return CHAPSIM_ERR_NODEVICE;
+  }
+  if (cfg->device < 0 || cfg->device >= ndev) return CHAPSIM_ERR_ARG;
+  ctx = new chapsim_ctx();
+  ctx->cfg = *cfg;
+  ctx->device = cfg->device;
+  int rc = CHAPSIM_OK;
+  FFTPlan px{}, pz{};
+  if (!factor_plan(cfg->nx, px) || !factor_plan(cfg->nz, pz)) {
+    delete ctx;
+    return CHAPSIM_ERR_UNSUPPORTED;  // lengths with prime factors > 11
+  }
+  if (cfg->precision == CHAPSIM_MIXED) {
+    delete ctx;
+    return CHAPSIM_ERR_UNSUPPORTED;
+  }
+  if (cudaSetDevice(ctx->device) != cudaSuccess) { delete ctx; return CHAPSIM_ERR_CUDA; }
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return CHAPSIM_ERR_CUDA;
+  }
+  for (auto &e : ctx->ev)
+    if (cudaEventCreate(&e) != cudaSuccess) { free_all(ctx); delete ctx; return CHAPSIM_ERR_CUDA; }
+  setup_mesh(ctx);
+  TGDev &d = ctx->d;
+  d.nx = cfg->nx; d.ny = cfg->ny; d.nz = cfg->nz; d.lh = cfg->nx / 2 + 1;
+  d.sy = cfg->nx;
+  d.sz = (int64_t)cfg->nx * (cfg->ny + 2);
+  const size_t n = (size_t)d.sz * cfg->nz;
+  void *p = nullptr;
+  double **f64[] = {&d.u, &d.v, &d.w, &d.p, &d.phi, &d.rhsphi, &d.h0[0], &d.h0[1], &d.h0[2]};
+  for (double **f : f64) {
+    if ((rc = dalloc(ctx, &p, n * sizeof(double)))) goto fail;
+    *f = (double *)p;
+    cudaMemsetAsync(p, 0, n * sizeof(double), ctx->stream);
+  }
+  for (int c = 0; c < 3; ++c) {
+    if ((rc = dalloc(ctx, &p, n * sizeof(double)))) goto fail;
+    d.rhs[c] = p;
+    cudaMemsetAsync(p, 0, n * sizeof(double), ctx->stream);
+  }
+  {
+    const size_t ns = (size_t)d.lh * cfg->ny * cfg->nz;
+    if ((rc = dalloc(ctx, &p, ns * sizeof(double2)))) goto fail;
+    d.spec = p;
+    if ((rc = dalloc(ctx, &p, ns * sizeof(double)))) goto fail;
+    d.ysc = (double *)p;
+    d.spec64 = nullptr;
+  }
+  {
+    // block partials: one per 32x8 tile of the (x, y) plane per z plane
+    ctx->npart = ((cfg->nx + 31) / 32) * ((cfg->ny + 7) / 8) * cfg->nz;
+    if ((rc = dalloc(ctx, &p, (size_t)ctx->npart * sizeof(double)))) goto fail;
+    d.partials = (double *)p;
+    if ((rc = dalloc(ctx, &p, 16 * sizeof(double)))) goto fail;
+    d.scal = (double *)p;
+    cudaMemsetAsync(p, 0, 16 * sizeof(double), ctx->stream);
+  }
+  if ((rc = build_tables(ctx))) goto fail;
+  px.tw64 = ctx->fx.tw64; px.tw32 = ctx->fx.tw32;
+  pz.tw64 = ctx->fz.tw64; pz.tw32 = ctx->fz.tw32;
+  ctx->fx = px;
+  ctx->fz = pz;
+  if ((rc = init_kernels(ctx))) goto fail;
+  if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { rc = CHAPSIM_ERR_CUDA; goto fail; }
+  *out = ctx;
+  return CHAPSIM_OK;
+fail:
+  free_all(ctx);
+  delete ctx;
+  return rc;
+}
+
+int chapsim_destroy(chapsim_ctx *ctx) {
+  if (!ctx) return CHAPSIM_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  free_all(ctx);
+  delete ctx;
+  return CHAPSIM_OK;
+}
+
+const char *chapsim_last_error(const chapsim_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int chapsim_sync(chapsim_ctx *ctx) {
+  if (!ctx) return CHAPSIM_ERR_ARG;
+  CKC(cudaStreamSynchronize(ctx->stream));
+  return CHAPSIM_OK;
+}
+
+int64_t chapsim_field_len(const chapsim_ctx *ctx) {
+  return ctx ? ctx->d.sz * (int64_t)ctx->d.nz : -1;
+}
+
+static double *field_ptr(chapsim_ctx *ctx, int domain, int field) {
+  if (domain != CHAPSIM_ITG) return nullptr;
+  TGDev &d = ctx->d;
+  switch (field) {
+    case CHAPSIM_F_U: return d.u;
+    case CHAPSIM_F_V: return d.v;
+    case CHAPSIM_F_W: return d.w;
+    case CHAPSIM_F_P: return d.p;
+    case CHAPSIM_F_PHI: return d.phi;
+    case CHAPSIM_F_RHSPHI: return d.rhsphi;
+    case CHAPSIM_F_H0U: return d.h0[0];
+    case CHAPSIM_F_H0V: return d.h0[1];
+    case CHAPSIM_F_H0W: return d.h0[2];
+  }
+  return nullptr;
+}
+
+static int xfer(chapsim_ctx *ctx, int domain, int field, void *dst_or_src, int64_t n, cudaMemcpyKind kind,
+                bool to_dev) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  double *f = field_ptr(ctx, domain, field);
+  REQUIRE(f, CHAPSIM_ERR_ARG, "unknown domain/field id");
+  REQUIRE(dst_or_src, CHAPSIM_ERR_ARG, "null buffer");
+  REQUIRE(n == chapsim_field_len(ctx), CHAPSIM_ERR_ARG, "field length mismatch");
+  CKC(cudaSetDevice(ctx->device));
+  const size_t bytes = (size_t)n * sizeof(double);
+  if (to_dev)
+    CKC(cudaMemcpyAsync(f, dst_or_src, bytes, kind, ctx->stream));
+  else
+    CKC(cudaMemcpyAsync(dst_or_src, f, bytes, kind, ctx->stream));
+  if (kind != cudaMemcpyDeviceToDevice) CKC(cudaStreamSynchronize(ctx->stream));
+  return CHAPSIM_OK;
+}
+
+int chapsim_set_field(chapsim_ctx *ctx, int domain, int field, const double *host, int64_t n) {
+  return xfer(ctx, domain, field, (void *)host, n, cudaMemcpyHostToDevice, true);
+}
+int chapsim_get_field(chapsim_ctx *ctx, int domain, int field, double *host, int64_t n) {
+  return xfer(ctx, domain, field, host, n, cudaMemcpyDeviceToHost, false);
+}
+int chapsim_set_field_device(chapsim_ctx *ctx, int domain, int field, const double *dev, int64_t n) {
+  return xfer(ctx, domain, field, (void *)dev, n, cudaMemcpyDeviceToDevice, true);
+}
+int chapsim_get_field_device(chapsim_ctx *ctx, int domain, int field, double *dev, int64_t n) {
+  return xfer(ctx, domain, field, dev, n, cudaMemcpyDeviceToDevice, false);
+}
+
+int chapsim_get_mesh(const chapsim_ctx *ctx, int what, double *out, int64_t n) {
+  if (!ctx || !out) return CHAPSIM_ERR_ARG;
+  const int ny = ctx->cfg.ny;
+  const std::vector<double> *v = nullptr;
+  int hi = ny;
+  switch (what) {
+    case 0: v = &ctx->ynd; hi = ny + 1; break;
+    case 1: v = &ctx->ycc; break;
+    case 2: v = &ctx->dyfi; break;
+    case 3: v = &ctx->dyci; hi = ny + 1; break;
+    default: return CHAPSIM_ERR_ARG;
+  }
+  if (n != hi) return CHAPSIM_ERR_ARG;
+  for (int j = 1; j <= hi; ++j) out[j - 1] = (*v)[j];
+  return CHAPSIM_OK;
+}
+
+int chapsim_init_random(chapsim_ctx *ctx, uint64_t seed, double amp, int project) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  const int nx = ctx->cfg.nx, ny = ctx->cfg.ny, nz = ctx->cfg.nz;
+  const int64_t sy = nx, sz = (int64_t)nx * (ny + 2), n = sz * nz;
+  std::vector<double> q[3];
+  for (auto &f : q) f.assign((size_t)n, 0.0);
+  auto id = [&](int i, int j, int k) { return (size_t)((i - 1) + sy * j + sz * (k - 1)); };
+  // RANDOM_FL_FLD_TG (src/INITIAL_FL_FLD_TG.f90:2-72) with a counter-based
+  // generator in place of gfortran's random_number.
+  for (int j = 1; j <= ny; ++j)
+    for (int k = 1; k <= nz; ++k)
+      for (int i = 1; i <= nx; ++i)
+        for (int c = 0; c < 3; ++c) q[c][id(i, j, k)] = amp * rnd_pm1(seed, c + 1, i, j, k);
+  for (int k = 1; k <= nz; ++k)
+    for (int i = 1; i <= nx; ++i) q[1][id(i, 1, k)] = 0.0;
+  for (int c = 0; c < 3; ++c)
+    for (int j = 1; j <= ny; ++j) {
+      double s = 0.0;
+      for (int i = 1; i <= nx; ++i)
+        for (int k = 1; k <= nz; ++k) s += q[c][id(i, j, k)];
+      s /= (double)nx * (double)nz;
+      for (int i = 1; i <= nx; ++i)
+        for (int k = 1; k <= nz; ++k) q[c][id(i, j, k)] -= s;
+    }
+  for (int j = 1; j <= ny; ++j) {
+    const double vini = 1.5 * (1.0 - ctx->ycc[j] * ctx->ycc[j]);  // LAMPOISLPROF.f90:49-56
+    for (int k = 1; k <= nz; ++k)
+      for (int i = 1; i <= nx; ++i) q[0][id(i, j, k)] += vini;
+  }
+  for (int k = 1; k <= nz; ++k)
+    for (int i = 1; i <= nx; ++i) q[1][id(i, 1, k)] = 0.0;
+  // bulk velocity rescale (BULK_VELOCITY_TG, src/INITIAL_FL_FLD_TG.f90:122-149)
+  double s = 0.0;
+  for (int j = 1; j <= ny; ++j)
+    for (int i = 1; i <= nx; ++i)
+      for (int k = 1; k <= nz; ++k) s += q[0][id(i, j, k)] / ctx->dyfi[j];
+  s = s / (nz / ctx->cfg.lz);
+  const double ub = s / (ctx->area_inlet * (double)nx);
+  for (auto &x : q[0]) x /= ub;
+  // wall ghosts
+  for (int k = 1; k <= nz; ++k)
+    for (int i = 1; i <= nx; ++i)
+      for (int c = 0; c < 3; ++c) { q[c][id(i, 0, k)] = 0.0; q[c][id(i, ny + 1, k)] = 0.0; }
+  int rc;
+  for (int c = 0; c < 3; ++c)
+    if ((rc = chapsim_set_field(ctx, CHAPSIM_ITG, CHAPSIM_F_U + c, q[c].data(), n))) return rc;
+  TGDev &d = ctx->d;
+  const size_t bytes = (size_t)n * sizeof(double);
+  CKC(cudaMemsetAsync(d.p, 0, bytes, ctx->stream));
+  for (int c = 0; c < 3; ++c) CKC(cudaMemsetAsync(d.h0[c], 0, bytes, ctx->stream));
+  if (project) {
+    rc = launch_substep(ctx, 0);  // CALC_INITIALIZATION_tg: SOLVERRK3_MOM_tg(0)
+    if (rc) return rc;
+  }
+  CKC(cudaStreamSynchronize(ctx->stream));
+  return CHAPSIM_OK;
+}
+
+int chapsim_rk3_mom_tg(chapsim_ctx *ctx, int ns) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
+  CKC(cudaSetDevice(ctx->device));
+  return launch_substep(ctx, ns);
+}
+
+int chapsim_step_tg(chapsim_ctx *ctx, int nsteps) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(nsteps >= 0, CHAPSIM_ERR_ARG, "nsteps must be >= 0");
+  CKC(cudaSetDevice(ctx->device));
+  if (ctx->timing) {
+    for (int s = 0; s < nsteps; ++s)
+      for (int ns = 1; ns <= 3; ++ns) {
+        int rc = launch_substep(ctx, ns);
+        if (rc) return rc;
+      }
+    return CHAPSIM_OK;
+  }
+  if (!ctx->step_graph) {
+    cudaGraph_t g = nullptr;
+    const int64_t before = ctx->launches;
+    CKC(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = CHAPSIM_OK;
+    for (int ns = 1; ns <= 3 && rc == CHAPSIM_OK; ++ns) rc = launch_substep(ctx, ns);
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+    if (e != cudaSuccess) { ctx->err = cudaGetErrorString(e); return CHAPSIM_ERR_CUDA; }
+    e = cudaGraphInstantiate(&ctx->step_graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { ctx->step_graph = nullptr; ctx->err = cudaGetErrorString(e); return CHAPSIM_ERR_CUDA; }
+    ctx->kernels_per_step = ctx->launches - before;  // kernels inside one replay
+    ctx->launches = before;
+  }
+  for (int s = 0; s < nsteps; ++s) {
+    CKC(cudaGraphLaunch(ctx->step_graph, ctx->stream));
+    ctx->launches += ctx->kernels_per_step;
+  }
+  return CHAPSIM_OK;
+}
+
+int chapsim_divg(chapsim_ctx *ctx, int domain, int ns) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(domain == CHAPSIM_ITG, CHAPSIM_ERR_ARG, "only the TG domain is built");
+  REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
+  return launch_divg(ctx, ns);
+}
+
+int chapsim_pois3d(chapsim_ctx *ctx, int domain) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(domain == CHAPSIM_ITG, CHAPSIM_ERR_ARG, "only the TG domain is built");
+  return launch_pois3d(ctx);
+}
+
+int chapsim_velo_correction(chapsim_ctx *ctx, int domain, int ns) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(domain == CHAPSIM_ITG, CHAPSIM_ERR_ARG, "only the TG domain is built");
+  REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
+  return launch_correction(ctx, ns);
+}
+
+int chapsim_reduce(chapsim_ctx *ctx, int domain, int what, double *out) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(out, CHAPSIM_ERR_ARG, "null output");
+  REQUIRE(domain == CHAPSIM_ITG, CHAPSIM_ERR_ARG, "only the TG domain is built");
+  REQUIRE(what >= 0 && what <= 2, CHAPSIM_ERR_ARG, "unknown reduction");
+  CKC(cudaSetDevice(ctx->device));
+  double v = 0.0;
+  int rc = launch_reduce(ctx, what, &v);
+  if (rc) return rc;
+  if (what == CHAPSIM_R_BULK) v = v / (ctx->cfg.nz / ctx->cfg.lz) / (ctx->area_inlet * (double)ctx->cfg.nx);
+  *out = v;
+  return CHAPSIM_OK;
+}
+
+int chapsim_get_stream(const chapsim_ctx *ctx, void **stream) {
+  if (!ctx || !stream) return CHAPSIM_ERR_ARG;
+  *stream = (void *)ctx->stream;
+  return CHAPSIM_OK;
+}
+
+int chapsim_phase_timing(chapsim_ctx *ctx, int enable) {
+  if (!ctx) return CHAPSIM_ERR_ARG;
+  ctx->timing = enable != 0;
+  return CHAPSIM_OK;
+}
+int chapsim_phase_times(chapsim_ctx *ctx, double *ms, int n, int64_t *substeps) {
+  if (!ctx || !ms || n < CHAPSIM_PH_COUNT) return CHAPSIM_ERR_ARG;
+  for (int i = 0; i < CHAPSIM_PH_COUNT; ++i) ms[i] = ctx->phase_ms[i];
+  if (substeps) *substeps = ctx->timed_substeps;
+  return CHAPSIM_OK;
+}
+int chapsim_phase_reset(chapsim_ctx *ctx) {
+  if (!ctx) return CHAPSIM_ERR_ARG;
+  for (double &m : ctx->phase_ms) m = 0.0;
+  ctx->timed_substeps = 0;
+  return CHAPSIM_OK;
+}
+
+int chapsim_launch_count(const chapsim_ctx *ctx, int64_t *count) {
+  if (!ctx || !count) return CHAPSIM_ERR_ARG;
+  *count = ctx->launches;
+  return CHAPSIM_OK;
+}
+int chapsim_launch_count_reset(chapsim_ctx *ctx) {
+  if (!ctx) return CHAPSIM_ERR_ARG;
+  ctx->launches = 0;
+  return CHAPSIM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,104 @@
+// Internal definitions shared by the libchapsim translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/chapsim.h"
+
+namespace chapsim {
+
+// Device-side parameters of one TG domain, passed by value to every kernel.
+// Index convention: field(i, j, k) at i + nx*(j + (ny+2)*k), i in [0,nx),
+// j in [0,ny+1] (j = 0 and ny+1 are the wall ghost layers), k in [0,nz).
+// Spectral data: S(kx, j, kz) at kx + lh*((j-1) + ny*kz), kx in [0,lh).
+struct TGDev {
+  int nx, ny, nz, lh;
+  int64_t sy, sz;  // strides of j and k in a field
+  // FP64 state
+  double *u, *v, *w, *p, *phi, *rhsphi;
+  double *h0[3];
+  // temporaries (double in the FP64 form, float in the mixed form)
+  void *rhs[3];
+  void *spec;       // complex spectral array
+  double *ysc;      // Poisson y-solve scratch (h_j), lh*ny*nz
+  double2 *spec64;  // FP64 spectral scratch for the refinement sweep (mixed)
+  double *partials; // per-block mass-flux partial sums
+  double *scal;     // device scalars: [0] dpgrns, [1..] reduction outputs
+  // mesh coefficients (1-based in j, arrays of length ny+2)
+  const double *dyfi, *dyci, *wff, *wfb;
+  const double *amvr[3], *acvr[3], *apvr[3];
+  const double *amph, *acph, *apph;
+  const double *ak1, *ak3;
+  double dxi, dzi, dxqi, dzqi, cvisc, dt, volm;
+};
+
+// Per-substep scalars.
+struct SubParams {
+  int ns;
+  double gam, roh, alp;
+  // y Crank-Nicolson factor rows (length ny+2, j = 1..ny), per component
+  const double *ya[3], *ypp[3], *yh[3];
+  // cyclic x / z factors: pp, h0, G2 (length n), and scalars
+  const double *xpp, *xh0, *xg2;
+  double xa, xb, xqq;
+  const double *zpp, *zh0, *zg2;
+  double za, zb, zqq;
+  int flowdrvtp;
+  double dp_const;  // flowdrvtp == 2: -0.5*cfgv*alp*dt
+};
+
+struct FFTPlan {
+  int n;
+  int nrad;
+  int rad[16];
+  const double2 *tw64;  // exp(-2 pi i m / n), m in [0,n)
+  const float2 *tw32;
+};
+
+}  // namespace chapsim
+
+struct chapsim_ctx {
+  chapsim_config cfg;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int64_t launches = 0;
+
+  chapsim::TGDev d{};
+  chapsim::FFTPlan fx{}, fz{};
+  // host mesh copies
+  std::vector<double> ynd, ycc, dyfi, dyci, wff, wfb;
+  double area_inlet = 0.0;
+  // host-precomputed substep factor tables and their device copies
+  std::vector<double> hcoef;
+  double *dcoef = nullptr;
+  chapsim::SubParams sp[4]{};
+  // allocations owned by the context
+  std::vector<void *> allocs;
+  int npart = 0;
+
+  // phase timing
+  bool timing = false;
+  cudaEvent_t ev[CHAPSIM_PH_COUNT + 1]{};
+  double phase_ms[CHAPSIM_PH_COUNT]{};
+  int64_t timed_substeps = 0;
+
+  // CUDA graph of one full step (NS = 1, 2, 3)
+  cudaGraphExec_t step_graph = nullptr;
+  int64_t kernels_per_step = 0;
+};
+
+// Kernel launch wrappers (defined in tg_kernels.cu).
+namespace chapsim {
+int init_kernels(chapsim_ctx *c);
+int launch_substep(chapsim_ctx *c, int ns);
+int launch_divg(chapsim_ctx *c, int ns);
+int launch_pois3d(chapsim_ctx *c);
+int launch_correction(chapsim_ctx *c, int ns);
+int launch_reduce(chapsim_ctx *c, int what, double *host_out);
+int launch_bc_q(chapsim_ctx *c);
+}  // namespace chapsim

@@ -1,0 +1,133 @@
+// Block-cooperative mixed-radix Stockham FFT on shared memory.
+//
+// Replaces the vendored Temperton FFT99 (real, x) and CFFT99 (complex, z)
+// transforms the reference's Poisson solver calls
+// (src/possion3d_FFT99.f90:299,310,460,474).  Transform definitions follow the
+// FFT99/CFFT99 documentation (libs/fft99/FFT99.f90:87-94,
+// libs/fft99/CFFT99.f90:171-196): forward = sum x e^{-2 pi i jk/N}, inverse =
+// sum C e^{+2 pi i jk/N}; normalisation is applied by the callers.  Unlike
+// FFT99 (radices 2, 3, 5 only) every length whose prime factors are in
+// {2, 3, 5, 7, 11} is supported.
+//
+// Algorithm: self-sorting Stockham decimation in time.  Stage s with radix R
+// and Ns = product of earlier radices maps, for j in [0, N/R):
+//   v_r = in[j + r N/R] * w^{r (j mod Ns) N/(Ns R)},  V = DFT_R(v),
+//   out[(j / Ns) Ns R + (j mod Ns) + s' Ns] = V_s'.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace chapsim {
+
+template <typename C> struct CTraits;
+template <> struct CTraits<double2> { typedef double R; };
+template <> struct CTraits<float2> { typedef float R; };
+
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  C r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { C r; r.x = a.x + b.x; r.y = a.y + b.y; return r; }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { C r; r.x = a.x - b.x; r.y = a.y - b.y; return r; }
+template <typename C> __device__ __forceinline__ C cconj(C a) { a.y = -a.y; return a; }
+// multiply by -i (sign < 0) or +i (sign > 0)
+template <typename C> __device__ __forceinline__ C cmuli(C a, int sign) {
+  C r;
+  if (sign < 0) { r.x = a.y; r.y = -a.x; } else { r.x = -a.y; r.y = a.x; }
+  return r;
+}
+
+// twiddle w^m = exp(sign 2 pi i m / N) from the forward table exp(-2 pi i m/N)
+template <typename C> __device__ __forceinline__ C twiddle(const C *tw, int m, int sign) {
+  C t = tw[m];
+  if (sign > 0) t.y = -t.y;
+  return t;
+}
+
+template <typename C, int R>
+__device__ __forceinline__ void dft_small(C *v, const C *tw, int n, int sign) {
+  if (R == 2) {
+    C a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  } else if (R == 4) {
+    C x0 = v[0], x1 = v[1], x2 = v[2], x3 = v[3];
+    C s02 = cadd(x0, x2), d02 = csub(x0, x2);
+    C s13 = cadd(x1, x3), d13 = cmuli(csub(x1, x3), sign);
+    v[0] = cadd(s02, s13);
+    v[2] = csub(s02, s13);
+    v[1] = cadd(d02, d13);
+    v[3] = csub(d02, d13);
+  } else {
+    // generic odd radix: V_s = sum_r v_r w_R^{rs}, w_R = table[(n/R) * m]
+    C out[R];
+    const int step = n / R;
+#pragma unroll
+    for (int s = 0; s < R; ++s) {
+      C acc = v[0];
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        int m = (r * s) % R;
+        acc = cadd(acc, cmul(v[r], twiddle(tw, m * step, sign)));
+      }
+      out[s] = acc;
+    }
+#pragma unroll
+    for (int s = 0; s < R; ++s) v[s] = out[s];
+  }
+}
+
+template <typename C, int R>
+__device__ __forceinline__ void stockham_stage(const C *__restrict__ in, C *__restrict__ out, int nlines,
+                                               int n, int lstride, int Ns, const C *__restrict__ tw,
+                                               int sign) {
+  const int nb = n / R;
+  const int total = nlines * nb;
+  const int tstep = n / (Ns * R);
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int line = t / nb;
+    const int j = t - line * nb;
+    const int k = j % Ns;
+    const C *src = in + line * lstride;
+    C *dst = out + line * lstride;
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[j + r * nb];
+    if (k != 0) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twiddle(tw, r * k * tstep, sign));  // r k tstep < n
+    }
+    dft_small<C, R>(v, tw, n, sign);
+    const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[base + r * Ns] = v[r];
+  }
+}
+
+// Transform nlines lines (each n complex values, stride lstride) held in
+// shared memory buffer a; b is scratch of the same size.  Returns the buffer
+// holding the result.  Must be called by every thread of the block.
+template <typename C>
+__device__ C *fft_lines(C *a, C *b, int nlines, int n, int lstride, const int *rad, int nrad,
+                        const C *__restrict__ tw, int sign) {
+  int Ns = 1;
+  for (int s = 0; s < nrad; ++s) {
+    const int R = rad[s];
+    switch (R) {
+      case 2: stockham_stage<C, 2>(a, b, nlines, n, lstride, Ns, tw, sign); break;
+      case 3: stockham_stage<C, 3>(a, b, nlines, n, lstride, Ns, tw, sign); break;
+      case 4: stockham_stage<C, 4>(a, b, nlines, n, lstride, Ns, tw, sign); break;
+      case 5: stockham_stage<C, 5>(a, b, nlines, n, lstride, Ns, tw, sign); break;
+      case 7: stockham_stage<C, 7>(a, b, nlines, n, lstride, Ns, tw, sign); break;
+      case 11: stockham_stage<C, 11>(a, b, nlines, n, lstride, Ns, tw, sign); break;
+      default: break;  // plans only contain the radices above
+    }
+    __syncthreads();
+    C *t = a; a = b; b = t;
+    Ns *= R;
+  }
+  return a;
+}
+
+}  // namespace chapsim

@@ -1,0 +1,784 @@
+// sm_100a kernels of the TG channel RK3 substep, SOLVERRK3_MOM_tg
+// (src/SOLVERRK3_MOM_tg.f90:18-61 of the CHAPSim1WW reference).
+//
+// Phase structure (one launch each, all on the context stream):
+//   rhs      CONVECTION_X/Y/Z_tg + RHS_CvLpGpS_tg for all three components at
+//            once (the three RHS only read the pre-substep velocity), with the
+//            constant-mass-flux volume integral reduced per block.
+//   dpgrns   fixed-order reduction of the block partials -> uniform dp/dx.
+//   adix     MOMFA1_X_tg: cyclic (1 - beta d_xx) lines, staged in shared memory.
+//   adiz     MOMFA2_Z_tg: cyclic (1 - beta d_zz) lines, staged in shared memory.
+//   adiy     MOMFA3_Y_tg + q += dq + BC_WALL_Q_tg: one thread per (i,k) line.
+//   fftx     DIVG_tg + forward real FFT along x (pairs of rows packed as one
+//            complex line), scaled 1/nx.
+//   fftz     forward complex FFT along z, scaled 1/nz, mean mode zeroed.
+//   ysolve   Poisson y-tridiagonal per (kx, kz).
+//   ifftz    inverse complex FFT along z.
+//   ifftx    inverse real FFT along x -> phi, BC_WALL_DPH ghost copy.
+//   corr     VELOUPDT_tg + PRCALC_tg + BC_WALL_Q_tg/BC_WALL_PR_tg.
+#include <cuda_runtime.h>
+#include <stdio.h>
+
+#include "chapsim_internal.cuh"
+#include "fft_smem.cuh"
+
+namespace chapsim {
+
+#define CK(call)                                                          \
+  do {                                                                    \
+    cudaError_t e_ = (call);                                              \
+    if (e_ != cudaSuccess) {                                              \
+      c->err = std::string(#call) + ": " + cudaGetErrorString(e_);        \
+      return CHAPSIM_ERR_CUDA;                                            \
+    }                                                                     \
+  } while (0)
+
+#define LAUNCHED()                                   \
+  do {                                               \
+    ++c->launches;                                   \
+    cudaError_t e_ = cudaGetLastError();             \
+    if (e_ != cudaSuccess) {                         \
+      c->err = std::string("kernel launch: ") + cudaGetErrorString(e_); \
+      return CHAPSIM_ERR_CUDA;                       \
+    }                                                \
+  } while (0)
+
+template <typename T> struct Cplx;
+template <> struct Cplx<double> { typedef double2 type; };
+template <> struct Cplx<float> { typedef float2 type; };
+
+// ----------------------------------------------------------------- helpers
+__device__ __forceinline__ int wrapp(int i, int n) { return i + 1 == n ? 0 : i + 1; }
+__device__ __forceinline__ int wrapm(int i, int n) { return i == 0 ? n - 1 : i - 1; }
+
+// Deterministic block sum (fixed shuffle tree, then warps in index order).
+__device__ double block_sum(double v, double *sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nt = blockDim.x * blockDim.y * blockDim.z;
+  const int lane = tid & 31, wid = tid >> 5, nw = (nt + 31) >> 5;
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (tid == 0)
+    for (int i = 0; i < nw; ++i) s += sh[i];
+  __syncthreads();
+  return s;  // valid in thread 0
+}
+__device__ double block_max(double v, double *sh) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nt = blockDim.x * blockDim.y * blockDim.z;
+  const int lane = tid & 31, wid = tid >> 5, nw = (nt + 31) >> 5;
+  if (lane == 0) sh[wid] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (tid == 0)
+    for (int i = 0; i < nw; ++i) s = fmax(s, sh[i]);
+  __syncthreads();
+  return s;
+}
+
+// ============================================================ rhs kernel
+// CONVECTION_X_tg (src/CONVECTION_X.f90:23-74), CONVECTION_Y_tg
+// (src/CONVECTION_Y.f90:22-91, channel branch; the bottom wall face j = 1 is
+// skipped), CONVECTION_Z_tg (src/CONVECTION_Z.f90:22-75) and RHS_CvLpGpS_tg
+// (src/RHS_CvLpGpS_tg.f90:61-176): rhs = dt[gam H + roh H0 + alp/Re L(q)]
+// - alp dt grad(p); H0 <- H.  Partial volume integrals of rhs_u/DYFI feed the
+// constant-mass-flux correction (:183-198).
+constexpr int RHS_BX = 32, RHS_BY = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(RHS_BX *RHS_BY)
+k_rhs(TGDev d, SubParams sp) {
+  __shared__ double sh[32];
+  const int nx = d.nx, ny = d.ny;
+  const int i = blockIdx.x * RHS_BX + threadIdx.x;
+  const int j = blockIdx.y * RHS_BY + threadIdx.y + 1;
+  const int k = blockIdx.z;
+  double part = 0.0;
+  if (i < nx && j <= ny) {
+    const int nz = d.nz;
+    const int ip = wrapp(i, nx), im = wrapm(i, nx);
+    const int kp = wrapp(k, nz), km = wrapm(k, nz);
+    const int64_t sy = d.sy, sz = d.sz;
+    const int64_t c0 = i + sy * j + sz * k;
+    const int64_t cip = c0 + (ip - i), cim = c0 + (im - i);
+    const int64_t ckp = c0 + sz * (kp - k), ckm = c0 + sz * (km - k);
+    const double *__restrict__ U = d.u;
+    const double *__restrict__ V = d.v;
+    const double *__restrict__ W = d.w;
+    const double *__restrict__ P = d.p;
+    const double u0 = U[c0], uip = U[cip], uim = U[cim], ujp = U[c0 + sy], ujm = U[c0 - sy];
+    const double ukp = U[ckp], ukm = U[ckm], uipjm = U[cip - sy], uipkm = U[cip + (ckm - c0)];
+    const double v0 = V[c0], vim = V[cim], vip = V[cip], vjp = V[c0 + sy], vimjp = V[cim + sy];
+    const double vjm = V[c0 - sy], vkp = V[ckp], vkm = V[ckm], vjpkm = V[ckm + sy];
+    const double w0 = W[c0], wim = W[cim], wip = W[cip], wkp = W[ckp], wimkp = W[cim + (ckp - c0)];
+    const double wkm = W[ckm], wjm = W[c0 - sy], wjp = W[c0 + sy], wjmkp = W[ckp - sy];
+    const double wffj = d.wff[j], wfbj = d.wfb[j], wffp = d.wff[j + 1], wfbp = d.wfb[j + 1];
+    const double dyfi = d.dyfi[j];
+    const double dxi = d.dxi, dzi = d.dzi;
+    const double coe1 = sp.alp * d.cvisc;
+    const double coe2 = sp.alp * d.dt;
+    // ---- x momentum
+    {
+      const double h11 = ((uip + u0) * (uip + u0) - (uim + u0) * (uim + u0)) * (0.25 * dxi);
+      const double h12 = ((vjp + vimjp) * (wffp * ujp + wfbp * u0) - (v0 + vim) * (wffj * u0 + wfbj * ujm)) *
+                         (dyfi * 0.5);
+      const double h13 = ((wkp + wimkp) * (ukp + u0) - (w0 + wim) * (u0 + ukm)) * (0.25 * dzi);
+      const double H = -(h11 + h12 + h13);
+      double *h0 = d.h0[0];
+      const double rhsc = sp.gam * H + sp.roh * h0[c0];
+      const double lap = (uip - 2.0 * u0 + uim) * d.dxqi + (ukp - 2.0 * u0 + ukm) * d.dzqi +
+                         (ujp * d.apvr[0][j] + u0 * d.acvr[0][j] + ujm * d.amvr[0][j]);
+      h0[c0] = H;
+      const double pgm = (P[c0] - P[cim]) * dxi * coe2;
+      const double r = (rhsc + coe1 * lap) * d.dt - pgm;
+      reinterpret_cast<T *>(d.rhs[0])[c0] = (T)r;
+      part = r / dyfi;
+    }
+    // ---- y momentum (faces j >= 2)
+    if (j >= 2) {
+      const double h21 = ((wffj * uip + wfbj * uipjm) * (vip + v0) - (wffj * u0 + wfbj * ujm) * (v0 + vim)) *
+                         (dxi * 0.5);
+      const double h22 = ((vjp + v0) * (vjp + v0) - (v0 + vjm) * (v0 + vjm)) * (d.dyci[j] * 0.25);
+      const double h23 = ((wffj * wkp + wfbj * wjmkp) * (vkp + v0) - (wffj * w0 + wfbj * wjm) * (v0 + vkm)) *
+                         (dzi * 0.5);
+      const double H = -(h21 + h22 + h23);
+      double *h0 = d.h0[1];
+      const double rhsc = sp.gam * H + sp.roh * h0[c0];
+      const double lap = (vip - 2.0 * v0 + vim) * d.dxqi + (vkp - 2.0 * v0 + vkm) * d.dzqi +
+                         (vjp * d.apvr[1][j] + v0 * d.acvr[1][j] + vjm * d.amvr[1][j]);
+      h0[c0] = H;
+      const double pgm = (P[c0] - P[c0 - sy]) * d.dyci[j] * coe2;
+      reinterpret_cast<T *>(d.rhs[1])[c0] = (T)((rhsc + coe1 * lap) * d.dt - pgm);
+    }
+    // ---- z momentum
+    {
+      const double h31 = ((uip + uipkm) * (wip + w0) - (u0 + ukm) * (w0 + wim)) * (0.25 * dxi);
+      const double h32 = ((vjp + vjpkm) * (wffp * wjp + wfbp * w0) - (v0 + vkm) * (wffj * w0 + wfbj * wjm)) *
+                         (dyfi * 0.5);
+      const double h33 = ((wkp + w0) * (wkp + w0) - (w0 + wkm) * (w0 + wkm)) * (0.25 * dzi);
+      const double H = -(h31 + h32 + h33);
+      double *h0 = d.h0[2];
+      const double rhsc = sp.gam * H + sp.roh * h0[c0];
+      const double lap = (wip - 2.0 * w0 + wim) * d.dxqi + (wkp - 2.0 * w0 + wkm) * d.dzqi +
+                         (wjp * d.apvr[2][j] + w0 * d.acvr[2][j] + wjm * d.amvr[2][j]);
+      h0[c0] = H;
+      const double pgm = (P[c0] - P[ckm]) * dzi * coe2;
+      reinterpret_cast<T *>(d.rhs[2])[c0] = (T)((rhsc + coe1 * lap) * d.dt - pgm);
+    }
+  }
+  const double s = block_sum(part, sh);
+  if (threadIdx.x == 0 && threadIdx.y == 0)
+    d.partials[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = s;
+}
+
+// Fixed-order reduction of the mass-flux partials; scal[0] = DPGRNS.
+__global__ void __launch_bounds__(1024) k_dpgrns(TGDev d, SubParams sp, int npart) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int t = threadIdx.x; t < npart; t += blockDim.x) s += d.partials[t];
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) d.scal[0] = sp.flowdrvtp == 1 ? s / d.volm : (sp.flowdrvtp == 2 ? sp.dp_const : 0.0);
+}
+
+// ============================================================ cyclic lines
+// TDMAIJI_CYC (src/TDMAIJI_CYC.f90:67-154) with the coefficient-only parts
+// (pivots pp, h0 and the second right-hand side G2 after back substitution,
+// plus the corner denominator qq) precomputed on the host, because every line
+// of the x and z factors has the same constant coefficients.  s points to the
+// line in shared memory, element m at s[m*st].
+template <typename T>
+__device__ __forceinline__ void cyc_line(T *s, int st, int n, const double *__restrict__ pp,
+                                         const double *__restrict__ h0, const double *__restrict__ g2,
+                                         double a, double c, double b, double qq) {
+  double g = (double)s[0] / b;
+  s[0] = (T)g;
+  for (int m = 1; m <= n - 2; ++m) {
+    g = ((double)s[m * st] - g * a) * pp[m];
+    s[m * st] = (T)g;
+  }
+  // back substitution of g1 (g2 is precomputed)
+  double gn = g;  // g1[n-2]
+  for (int m = n - 3; m >= 0; --m) {
+    gn = (double)s[m * st] - h0[m] * gn;
+    s[m * st] = (T)gn;
+  }
+  const double g10 = gn;
+  const double g1n2 = (double)s[(n - 2) * st];
+  const double xn = ((double)s[(n - 1) * st] - c * g10 - a * g1n2) / qq;
+  s[(n - 1) * st] = (T)xn;
+  for (int m = n - 2; m >= 0; --m) s[m * st] = (T)((double)s[m * st] + g2[m] * xn);
+}
+
+// MOMFA1_X_tg (src/MOMFA_tg.f90:52-107): rows j0.. of plane k, all three
+// components (grid.z), rows contiguous in memory.  The u rows first take off
+// the mass-flux correction DPGRNS (src/RHS_CvLpGpS_tg.f90:205-211).
+template <typename T>
+__global__ void __launch_bounds__(128) k_adix(TGDev d, SubParams sp, int lb) {
+  extern __shared__ unsigned char smem_raw[];
+  T *s = reinterpret_cast<T *>(smem_raw);
+  const int nx = d.nx, ny = d.ny;
+  const int comp = blockIdx.z;
+  const int k = blockIdx.y;
+  const int jbeg = (comp == 1 ? 2 : 1) + blockIdx.x * lb;
+  if (jbeg > ny) return;
+  const int nrow = min(lb, ny - jbeg + 1);
+  T *g = reinterpret_cast<T *>(d.rhs[comp]) + d.sy * jbeg + d.sz * k;
+  const int ld = nx + 1;
+  const double sub = comp == 0 ? d.scal[0] : 0.0;
+  const int tot = nrow * nx;
+  for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+    const int r = t / nx, i = t - r * nx;
+    s[r * ld + i] = (T)((double)g[t] - sub);
+  }
+  // double-precision coefficient tables into shared memory
+  double *cf = reinterpret_cast<double *>(smem_raw + (((size_t)lb * ld * sizeof(T) + 15) & ~(size_t)15));
+  for (int t = threadIdx.x; t < nx; t += blockDim.x) {
+    cf[t] = sp.xpp[t];
+    cf[nx + t] = sp.xh0[t];
+    cf[2 * nx + t] = sp.xg2[t];
+  }
+  __syncthreads();
+  if (threadIdx.x < nrow)
+    cyc_line<T>(s + threadIdx.x * ld, 1, nx, cf, cf + nx, cf + 2 * nx, sp.xa, sp.xa, sp.xb, sp.xqq);
+  __syncthreads();
+  for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+    const int r = t / nx, i = t - r * nx;
+    g[t] = s[r * ld + i];
+  }
+}
+
+// MOMFA2_Z_tg (src/MOMFA_tg.f90:111-170): lines along z for consecutive i at
+// row j; tile [nz][LZ] in shared memory.
+constexpr int LZ = 32;
+template <typename T>
+__global__ void __launch_bounds__(128) k_adiz(TGDev d, SubParams sp) {
+  extern __shared__ unsigned char smem_raw[];
+  T *s = reinterpret_cast<T *>(smem_raw);
+  const int nx = d.nx, nz = d.nz;
+  const int comp = blockIdx.z;
+  const int j = blockIdx.y + 1;
+  if (comp == 1 && j == 1) return;
+  const int i0 = blockIdx.x * LZ;
+  const int nl = min(LZ, nx - i0);
+  T *g = reinterpret_cast<T *>(d.rhs[comp]) + i0 + d.sy * j;
+  const int tot = nz * LZ;
+  for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+    const int kk = t / LZ, l = t - kk * LZ;
+    if (l < nl) s[kk * LZ + l] = g[d.sz * kk + l];
+  }
+  double *cf = reinterpret_cast<double *>(smem_raw + (((size_t)nz * LZ * sizeof(T) + 15) & ~(size_t)15));
+  for (int t = threadIdx.x; t < nz; t += blockDim.x) {
+    cf[t] = sp.zpp[t];
+    cf[nz + t] = sp.zh0[t];
+    cf[2 * nz + t] = sp.zg2[t];
+  }
+  __syncthreads();
+  if (threadIdx.x < nl) cyc_line<T>(s + threadIdx.x, LZ, nz, cf, cf + nz, cf + 2 * nz, sp.za, sp.za, sp.zb, sp.zqq);
+  __syncthreads();
+  for (int t = threadIdx.x; t < tot; t += blockDim.x) {
+    const int kk = t / LZ, l = t - kk * LZ;
+    if (l < nl) g[d.sz * kk + l] = s[kk * LZ + l];
+  }
+}
+
+// ============================================================ y lines
+// MOMFA3_Y_tg (src/MOMFA_tg.f90:173-240) with TDMAIJJ_nonCYC
+// (src/TDMAIJJ_nonCYC.f90:67-120), q += dq (src/MOMFA_tg.f90:38-44) and
+// BC_WALL_Q_tg.  One thread per (i, k) line handles u, v, w in turn; the v
+// line's row 1 right-hand side is the u increment at j = 1, as in the
+// reference, whose RHS_tg row 1 is not rebuilt for IDR = 2.  Pivots depend
+// only on (NS, IDR, j) and are precomputed; the forward-swept g is kept in the
+// rhs array in place.
+template <typename T>
+__global__ void __launch_bounds__(128) k_adiy(TGDev d, SubParams sp) {
+  const int nx = d.nx, ny = d.ny;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  if (i >= nx) return;
+  const int64_t sy = d.sy;
+  const int64_t base = i + d.sz * k;
+  double du1 = 0.0;
+#pragma unroll 1
+  for (int comp = 0; comp < 3; ++comp) {
+    T *r = reinterpret_cast<T *>(d.rhs[comp]) + base;
+    double *q = comp == 0 ? d.u : (comp == 1 ? d.v : d.w);
+    q += base;
+    const double *__restrict__ a = sp.ya[comp];
+    const double *__restrict__ pp = sp.ypp[comp];
+    const double *__restrict__ h = sp.yh[comp];
+    // forward sweep, rows j = 1..ny
+    double g = (comp == 1 ? du1 : (double)r[sy]) * pp[1];
+    r[sy] = (T)g;
+    for (int j = 2; j <= ny; ++j) {
+      g = ((double)r[sy * j] - a[j] * g) * pp[j];
+      r[sy * j] = (T)g;
+    }
+    // back substitution and update; row 1 of v is solved but not added
+    double x = g;
+    const int jlo = comp == 1 ? 2 : 1;
+    q[sy * ny] += x;
+    for (int j = ny - 1; j >= 1; --j) {
+      x = (double)r[sy * j] - h[j] * x;
+      if (j >= jlo) q[sy * j] += x;
+    }
+    if (comp == 0) du1 = x;  // final u increment at j = 1
+    // no-slip ghosts (src/BC_WALL.f90:204-230)
+    q[0] = 0.0;
+    q[sy * (ny + 1)] = 0.0;
+    if (comp == 1) q[sy] = 0.0;
+  }
+}
+
+// ============================================================ Poisson
+// DIVG_tg (src/DIVG.f90:21-57) fused with the forward real transform along x
+// of FFT99_POIS3D_periodicxz (src/possion3d_FFT99.f90:265-318): rows j of
+// plane k are packed in pairs as one complex line, transformed, separated and
+// scaled by 1/nx.  mode 0 computes the divergence (and stores RHSLLPHI);
+// mode 1 transforms the stored RHSLLPHI.
+template <typename T>
+__global__ void __launch_bounds__(256) k_fftx(TGDev d, SubParams sp, FFTPlan pl, int lb, int mode) {
+  typedef typename Cplx<T>::type C;
+  extern __shared__ unsigned char smem_raw[];
+  const int nx = d.nx, ny = d.ny, lh = d.lh;
+  const int k = blockIdx.y;
+  const int jbeg = 1 + blockIdx.x * lb;
+  const int nrow = min(lb, ny - jbeg + 1);
+  const int nl = lb / 2;
+  C *A = reinterpret_cast<C *>(smem_raw);
+  C *B = A + nl * nx;
+  __shared__ int rad[16];
+  if (threadIdx.x < 16) rad[threadIdx.x] = pl.rad[threadIdx.x];
+  const double coe0 = 1.0 / (d.dt * sp.alp);
+  const int kp = wrapp(k, d.nz);
+  for (int t = threadIdx.x; t < lb * nx; t += blockDim.x) {
+    const int r = t / nx, i = t - r * nx;
+    const int j = jbeg + r;
+    double val = 0.0;
+    if (r < nrow) {
+      const int64_t c0 = i + d.sy * j + d.sz * k;
+      if (mode == 0) {
+        const int ip = wrapp(i, nx);
+        const double dv = (d.u[c0 + (ip - i)] - d.u[c0]) * d.dxi + (d.v[c0 + d.sy] - d.v[c0]) * d.dyfi[j] +
+                          (d.w[c0 + d.sz * (kp - k)] - d.w[c0]) * d.dzi;
+        val = dv * coe0;
+        d.rhsphi[c0] = val;
+      } else {
+        val = d.rhsphi[c0];
+      }
+    }
+    C *z = A + (r >> 1) * nx + i;
+    if (r & 1) z->y = (T)val; else z->x = (T)val;
+  }
+  __syncthreads();
+  C *res = fft_lines<C>(A, B, nl, nx, nx, rad, pl.nrad, (const C *)(sizeof(T) == 8 ? (const void *)pl.tw64 : (const void *)pl.tw32), -1);
+  const T scale = (T)(1.0 / nx);
+  C *S = reinterpret_cast<C *>(d.spec);
+  for (int t = threadIdx.x; t < nl * lh; t += blockDim.x) {
+    const int p = t / lh, kx = t - p * lh;
+    const C z = res[p * nx + kx];
+    const C zc = cconj(res[p * nx + (kx == 0 ? 0 : nx - kx)]);
+    C x0, x1;
+    x0.x = (T)0.5 * (z.x + zc.x) * scale;
+    x0.y = (T)0.5 * (z.y + zc.y) * scale;
+    // x1 = -i (z - zc) / 2
+    x1.x = (T)0.5 * (z.y - zc.y) * scale;
+    x1.y = (T)-0.5 * (z.x - zc.x) * scale;
+    const int r0 = 2 * p;
+    if (r0 < nrow) S[kx + (int64_t)lh * ((jbeg + r0 - 1) + (int64_t)ny * k)] = x0;
+    if (r0 + 1 < nrow) S[kx + (int64_t)lh * ((jbeg + r0) + (int64_t)ny * k)] = x1;
+  }
+}
+
+// Complex transform along z for lz consecutive kx at row j
+// (src/possion3d_FFT99.f90:301-317 forward with 1/nz and the (1,1,1) mode
+// zeroed (:324-327); :448-458 inverse).
+template <typename T>
+__global__ void __launch_bounds__(256) k_fftz(TGDev d, FFTPlan pl, int lz, int sign) {
+  typedef typename Cplx<T>::type C;
+  extern __shared__ unsigned char smem_raw[];
+  const int nz = d.nz, ny = d.ny, lh = d.lh;
+  const int j = blockIdx.y + 1;
+  const int kx0 = blockIdx.x * lz;
+  const int nl = min(lz, lh - kx0);
+  const int ld = nz + 1;
+  C *A = reinterpret_cast<C *>(smem_raw);
+  C *B = A + lz * ld;
+  __shared__ int rad[16];
+  if (threadIdx.x < 16) rad[threadIdx.x] = pl.rad[threadIdx.x];
+  C *S = reinterpret_cast<C *>(d.spec) + kx0 + (int64_t)lh * (j - 1);
+  const int64_t skz = (int64_t)lh * ny;
+  for (int t = threadIdx.x; t < nz * lz; t += blockDim.x) {
+    const int kz = t / lz, l = t - kz * lz;
+    C v;
+    if (l < nl) v = S[skz * kz + l]; else { v.x = 0; v.y = 0; }
+    A[l * ld + kz] = v;
+  }
+  __syncthreads();
+  C *res = fft_lines<C>(A, B, lz, nz, ld, rad, pl.nrad, (const C *)(sizeof(T) == 8 ? (const void *)pl.tw64 : (const void *)pl.tw32), sign);
+  const T scale = sign < 0 ? (T)(1.0 / nz) : (T)1;
+  for (int t = threadIdx.x; t < nz * lz; t += blockDim.x) {
+    const int kz = t / lz, l = t - kz * lz;
+    if (l < nl) {
+      C v = res[l * ld + kz];
+      v.x *= scale;
+      v.y *= scale;
+      if (sign < 0 && j == 1 && kz == 0 && kx0 + l == 0) { v.x = 0; v.y = 0; }
+      S[skz * kz + l] = v;
+    }
+  }
+}
+
+// Poisson y-tridiagonal per (kx, kz) (src/possion3d_FFT99.f90:334-443 with the
+// coefficients of TDMA_PHI_COEF :185-220): A = AMPH, B = ACPH - AK1 - AK3,
+// C = APPH; for the mean mode row 1 is decoupled and its rhs set to zero.
+// Real and imaginary parts share the pivots.
+template <typename T>
+__global__ void __launch_bounds__(128) k_ysolve(TGDev d) {
+  typedef typename Cplx<T>::type C;
+  const int lh = d.lh, ny = d.ny;
+  const int kx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int kz = blockIdx.y;
+  if (kx >= lh) return;
+  C *S = reinterpret_cast<C *>(d.spec) + kx + (int64_t)lh * ny * kz;
+  double *H = d.ysc + kx + (int64_t)lh * ny * kz;
+  const double shift = d.ak1[kx] + d.ak3[kz];
+  const bool mean = (kx == 0 && kz == 0);
+  // j = 1
+  double b = d.acph[1] - shift;
+  double cc = mean ? 0.0 : d.apph[1];
+  double h = cc / b;
+  C r = S[0];
+  double gr = mean ? 0.0 : (double)r.x / b;
+  double gi = mean ? 0.0 : (double)r.y / b;
+  H[0] = h;
+  {
+    C o; o.x = (T)gr; o.y = (T)gi; S[0] = o;
+  }
+  for (int j = 2; j <= ny; ++j) {
+    const int64_t o = (int64_t)lh * (j - 1);
+    const double a = d.amph[j];
+    b = d.acph[j] - shift;
+    const double pp = 1.0 / (b - h * a);
+    r = S[o];
+    gr = ((double)r.x - a * gr) * pp;
+    gi = ((double)r.y - a * gi) * pp;
+    if (j < ny) {
+      h = d.apph[j] * pp;
+      H[o] = h;
+    }
+    C w; w.x = (T)gr; w.y = (T)gi; S[o] = w;
+  }
+  double xr = gr, xi = gi;
+  for (int j = ny - 1; j >= 1; --j) {
+    const int64_t o = (int64_t)lh * (j - 1);
+    const double hh = H[o];
+    r = S[o];
+    xr = (double)r.x - hh * xr;
+    xi = (double)r.y - hh * xi;
+    C w; w.x = (T)xr; w.y = (T)xi; S[o] = w;
+  }
+}
+
+// Inverse real transform along x (src/possion3d_FFT99.f90:461-485): pairs of
+// rows rebuilt as one complex Hermitian-extended line; phi ghosts copied
+// (BC_WALL_DPH, src/BC_WALL.f90:342-364).
+template <typename T>
+__global__ void __launch_bounds__(256) k_ifftx(TGDev d, FFTPlan pl, int lb) {
+  typedef typename Cplx<T>::type C;
+  extern __shared__ unsigned char smem_raw[];
+  const int nx = d.nx, ny = d.ny, lh = d.lh;
+  const int k = blockIdx.y;
+  const int jbeg = 1 + blockIdx.x * lb;
+  const int nrow = min(lb, ny - jbeg + 1);
+  const int nl = lb / 2;
+  C *A = reinterpret_cast<C *>(smem_raw);
+  C *B = A + nl * nx;
+  __shared__ int rad[16];
+  if (threadIdx.x < 16) rad[threadIdx.x] = pl.rad[threadIdx.x];
+  const C *S = reinterpret_cast<const C *>(d.spec);
+  for (int t = threadIdx.x; t < nl * lh; t += blockDim.x) {
+    const int p = t / lh, kx = t - p * lh;
+    const int r0 = 2 * p;
+    C x0, x1;
+    x0.x = 0; x0.y = 0; x1.x = 0; x1.y = 0;
+    if (r0 < nrow) x0 = S[kx + (int64_t)lh * ((jbeg + r0 - 1) + (int64_t)ny * k)];
+    if (r0 + 1 < nrow) x1 = S[kx + (int64_t)lh * ((jbeg + r0) + (int64_t)ny * k)];
+    if (kx == 0 || 2 * kx == nx) { x0.y = 0; x1.y = 0; }
+    // Z(k) = X0 + i X1 ; Z(n-k) = conj(X0) + i conj(X1)
+    C z; z.x = x0.x - x1.y; z.y = x0.y + x1.x;
+    A[p * nx + kx] = z;
+    if (kx != 0 && 2 * kx != nx) {
+      C zc; zc.x = x0.x + x1.y; zc.y = -x0.y + x1.x;
+      A[p * nx + (nx - kx)] = zc;
+    }
+  }
+  __syncthreads();
+  C *res = fft_lines<C>(A, B, nl, nx, nx, rad, pl.nrad, (const C *)(sizeof(T) == 8 ? (const void *)pl.tw64 : (const void *)pl.tw32), +1);
+  for (int t = threadIdx.x; t < nrow * nx; t += blockDim.x) {
+    const int r = t / nx, i = t - r * nx;
+    const int j = jbeg + r;
+    const C z = res[(r >> 1) * nx + i];
+    const double val = (r & 1) ? (double)z.y : (double)z.x;
+    const int64_t c0 = i + d.sy * j + d.sz * k;
+    d.phi[c0] = val;
+    if (j == 1) d.phi[c0 - d.sy] = val;
+    if (j == ny) d.phi[c0 + d.sy] = val;
+  }
+}
+
+// VELOUPDT_tg (src/VELO_CORRECTION.f90:19-105), PRCALC_tg
+// (src/PRESSURE_CORRECTION.f90:1-24) and the wall BCs of u, v, w, p.
+__global__ void __launch_bounds__(RHS_BX *RHS_BY) k_corr(TGDev d, SubParams sp) {
+  const int nx = d.nx, ny = d.ny;
+  const int i = blockIdx.x * RHS_BX + threadIdx.x;
+  const int j = blockIdx.y * RHS_BY + threadIdx.y + 1;
+  const int k = blockIdx.z;
+  if (i >= nx || j > ny) return;
+  const int64_t sy = d.sy;
+  const int64_t c0 = i + sy * j + d.sz * k;
+  const int im = wrapm(i, nx), km = wrapm(k, d.nz);
+  const double phi = d.phi[c0];
+  const double cx = d.dt * sp.alp * d.dxi, cz = d.dt * sp.alp * d.dzi;
+  d.u[c0] -= (phi - d.phi[c0 + (im - i)]) * cx;
+  d.w[c0] -= (phi - d.phi[c0 + d.sz * (km - k)]) * cz;
+  if (j >= 2) d.v[c0] -= (phi - d.phi[c0 - sy]) * (d.dt * sp.alp * d.dyci[j]);
+  const double be = 0.5 * sp.alp * d.dt * d.cvisc;
+  const double pn = d.p[c0] + phi - be * d.rhsphi[c0];
+  d.p[c0] = pn;
+  if (j == 1) {
+    d.u[c0 - sy] = 0.0; d.w[c0 - sy] = 0.0; d.v[c0 - sy] = 0.0; d.v[c0] = 0.0;
+    d.p[c0 - sy] = pn;
+  }
+  if (j == ny) {
+    d.u[c0 + sy] = 0.0; d.w[c0 + sy] = 0.0; d.v[c0 + sy] = 0.0;
+    d.p[c0 + sy] = pn;
+  }
+}
+
+// Stand-alone BC_WALL_Q_tg on all ghost cells.
+__global__ void k_bc_q(TGDev d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  if (i >= d.nx) return;
+  const int64_t c1 = i + d.sy + d.sz * k;
+  d.u[c1 - d.sy] = 0.0; d.w[c1 - d.sy] = 0.0; d.v[c1 - d.sy] = 0.0; d.v[c1] = 0.0;
+  const int64_t cn = i + d.sy * (d.ny + 1) + d.sz * k;
+  d.u[cn] = 0.0; d.w[cn] = 0.0; d.v[cn] = 0.0;
+}
+
+// ============================================================ reductions
+// what 0: max |div u| (DIVGCK_tg, src/DIVGCK.f90:16-58) -> block maxima
+// what 1: sum u/DYFI (BULK_VELOCITY_TG) -> block sums
+// what 2: count of non-finite u, v, w, p -> block sums
+__global__ void __launch_bounds__(RHS_BX *RHS_BY) k_reduce_part(TGDev d, int what) {
+  __shared__ double sh[32];
+  const int nx = d.nx, ny = d.ny;
+  const int i = blockIdx.x * RHS_BX + threadIdx.x;
+  const int j = blockIdx.y * RHS_BY + threadIdx.y + 1;
+  const int k = blockIdx.z;
+  double v = 0.0;
+  if (i < nx && j <= ny) {
+    const int64_t c0 = i + d.sy * j + d.sz * k;
+    if (what == 0) {
+      const int ip = wrapp(i, nx), kp = wrapp(k, d.nz);
+      const double dv = (d.u[c0 + (ip - i)] - d.u[c0]) * d.dxi + (d.v[c0 + d.sy] - d.v[c0]) * d.dyfi[j] +
+                        (d.w[c0 + d.sz * (kp - k)] - d.w[c0]) * d.dzi;
+      v = fabs(dv);
+      if (dv != dv) v = __longlong_as_double(0x7ff0000000000000ll);  // NaN -> +inf
+    } else if (what == 1) {
+      v = d.u[c0] / d.dyfi[j];
+    } else {
+      v = (double)(!isfinite(d.u[c0])) + (double)(!isfinite(d.v[c0])) + (double)(!isfinite(d.w[c0])) +
+          (double)(!isfinite(d.p[c0]));
+    }
+  }
+  const double s = what == 0 ? block_max(v, sh) : block_sum(v, sh);
+  if (threadIdx.x == 0 && threadIdx.y == 0)
+    d.partials[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = s;
+}
+
+__global__ void __launch_bounds__(1024) k_reduce_final(TGDev d, int what, int npart) {
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int t = threadIdx.x; t < npart; t += blockDim.x) s = what == 0 ? fmax(s, d.partials[t]) : s + d.partials[t];
+  s = what == 0 ? block_max(s, sh) : block_sum(s, sh);
+  if (threadIdx.x == 0) d.scal[1] = s;
+}
+
+// ============================================================ launchers
+static int fftx_lb(int nx) {
+  // rows per block of the x transforms: two complex buffers of lb/2 lines
+  int lb = (int)(96 * 1024 / ((size_t)nx * sizeof(double2)));
+  lb = lb & ~1;
+  if (lb > 16) lb = 16;
+  if (lb < 2) lb = 2;
+  return lb;
+}
+static size_t fftx_smem(int nx, int lb) { return (size_t)lb * nx * sizeof(double2); }
+static int fftz_lz(int nz) {
+  int lz = (int)(96 * 1024 / ((size_t)2 * (nz + 1) * sizeof(double2)));
+  if (lz > 16) lz = 16;
+  if (lz < 1) lz = 1;
+  return lz;
+}
+static size_t fftz_smem(int nz, int lz) { return (size_t)2 * lz * (nz + 1) * sizeof(double2); }
+static int adix_lb(int nx) {
+  int lb = (int)(96 * 1024 / ((size_t)(nx + 1) * sizeof(double)));
+  if (lb > 64) lb = 64;
+  if (lb < 1) lb = 1;
+  return lb;
+}
+static size_t adix_smem(int nx, int lb) {
+  return (((size_t)lb * (nx + 1) * sizeof(double) + 15) & ~(size_t)15) + 3 * (size_t)nx * sizeof(double);
+}
+static size_t adiz_smem(int nz) {
+  return (((size_t)nz * LZ * sizeof(double) + 15) & ~(size_t)15) + 3 * (size_t)nz * sizeof(double);
+}
+
+int init_kernels(chapsim_ctx *c) {
+  const int nx = c->d.nx, nz = c->d.nz;
+  CK(cudaFuncSetAttribute(k_adix<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adix_smem(nx, adix_lb(nx))));
+  CK(cudaFuncSetAttribute(k_adiz<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adiz_smem(nz)));
+  CK(cudaFuncSetAttribute(k_fftx<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftx_smem(nx, fftx_lb(nx))));
+  CK(cudaFuncSetAttribute(k_ifftx<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftx_smem(nx, fftx_lb(nx))));
+  CK(cudaFuncSetAttribute(k_fftz<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftz_smem(nz, fftz_lz(nz))));
+  return CHAPSIM_OK;
+}
+
+static inline void phase_mark(chapsim_ctx *c, int ph) {
+  if (c->timing) cudaEventRecord(c->ev[ph], c->stream);
+}
+
+int launch_divg(chapsim_ctx *c, int ns) {
+  // DIVG_tg alone: the fused divergence + x-transform kernel in mode 0 stores
+  // RHSLLPHI (its spectral output is scratch).
+  TGDev &d = c->d;
+  const int lb = fftx_lb(d.nx);
+  dim3 grid((d.ny + lb - 1) / lb, d.nz);
+  k_fftx<double><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->sp[ns], c->fx, lb, 0);
+  LAUNCHED();
+  return CHAPSIM_OK;
+}
+
+static int poisson_from_rhs(chapsim_ctx *c, int ns, int mode) {
+  TGDev &d = c->d;
+  const int lb = fftx_lb(d.nx);
+  phase_mark(c, CHAPSIM_PH_FFTX);
+  {
+    dim3 grid((d.ny + lb - 1) / lb, d.nz);
+    k_fftx<double><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->sp[ns], c->fx, lb, mode);
+    LAUNCHED();
+  }
+  phase_mark(c, CHAPSIM_PH_FFTZ);
+  const int lz = fftz_lz(d.nz);
+  {
+    dim3 grid((d.lh + lz - 1) / lz, d.ny);
+    k_fftz<double><<<grid, 256, fftz_smem(d.nz, lz), c->stream>>>(d, c->fz, lz, -1);
+    LAUNCHED();
+  }
+  phase_mark(c, CHAPSIM_PH_YSOLVE);
+  {
+    dim3 grid((d.lh + 127) / 128, d.nz);
+    k_ysolve<double><<<grid, 128, 0, c->stream>>>(d);
+    LAUNCHED();
+  }
+  phase_mark(c, CHAPSIM_PH_IFFTZ);
+  {
+    dim3 grid((d.lh + lz - 1) / lz, d.ny);
+    k_fftz<double><<<grid, 256, fftz_smem(d.nz, lz), c->stream>>>(d, c->fz, lz, +1);
+    LAUNCHED();
+  }
+  phase_mark(c, CHAPSIM_PH_IFFTX);
+  {
+    dim3 grid((d.ny + lb - 1) / lb, d.nz);
+    k_ifftx<double><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->fx, lb);
+    LAUNCHED();
+  }
+  return CHAPSIM_OK;
+}
+
+int launch_pois3d(chapsim_ctx *c) { return poisson_from_rhs(c, 1, 1); }
+
+int launch_correction(chapsim_ctx *c, int ns) {
+  TGDev &d = c->d;
+  dim3 grid((d.nx + RHS_BX - 1) / RHS_BX, (d.ny + RHS_BY - 1) / RHS_BY, d.nz);
+  k_corr<<<grid, dim3(RHS_BX, RHS_BY), 0, c->stream>>>(d, c->sp[ns]);
+  LAUNCHED();
+  return CHAPSIM_OK;
+}
+
+int launch_bc_q(chapsim_ctx *c) {
+  TGDev &d = c->d;
+  dim3 grid((d.nx + 127) / 128, d.nz);
+  k_bc_q<<<grid, 128, 0, c->stream>>>(d);
+  LAUNCHED();
+  return CHAPSIM_OK;
+}
+
+int launch_substep(chapsim_ctx *c, int ns) {
+  TGDev &d = c->d;
+  const SubParams &sp = c->sp[ns];
+  phase_mark(c, CHAPSIM_PH_RHS);
+  {
+    dim3 grid((d.nx + RHS_BX - 1) / RHS_BX, (d.ny + RHS_BY - 1) / RHS_BY, d.nz);
+    k_rhs<double><<<grid, dim3(RHS_BX, RHS_BY), 0, c->stream>>>(d, sp);
+    LAUNCHED();
+    const int npart = grid.x * grid.y * grid.z;
+    k_dpgrns<<<1, 1024, 0, c->stream>>>(d, sp, npart);
+    LAUNCHED();
+  }
+  phase_mark(c, CHAPSIM_PH_ADIX);
+  {
+    const int lb = adix_lb(d.nx);
+    dim3 grid((d.ny + lb - 1) / lb, d.nz, 3);
+    k_adix<double><<<grid, 128, adix_smem(d.nx, lb), c->stream>>>(d, sp, lb);
+    LAUNCHED();
+  }
+  phase_mark(c, CHAPSIM_PH_ADIZ);
+  {
+    dim3 grid((d.nx + LZ - 1) / LZ, d.ny, 3);
+    k_adiz<double><<<grid, 128, adiz_smem(d.nz), c->stream>>>(d, sp);
+    LAUNCHED();
+  }
+  phase_mark(c, CHAPSIM_PH_ADIY);
+  {
+    dim3 grid((d.nx + 127) / 128, d.nz);
+    k_adiy<double><<<grid, 128, 0, c->stream>>>(d, sp);
+    LAUNCHED();
+  }
+  int rc = poisson_from_rhs(c, ns, 0);
+  if (rc) return rc;
+  phase_mark(c, CHAPSIM_PH_CORR);
+  rc = launch_correction(c, ns);
+  if (rc) return rc;
+  if (c->timing) {
+    cudaEventRecord(c->ev[CHAPSIM_PH_COUNT], c->stream);
+    CK(cudaEventSynchronize(c->ev[CHAPSIM_PH_COUNT]));
+    for (int ph = 0; ph < CHAPSIM_PH_COUNT; ++ph) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, c->ev[ph], c->ev[ph + 1]));
+      c->phase_ms[ph] += ms;
+    }
+    c->timed_substeps++;
+  }
+  return CHAPSIM_OK;
+}
+
+int launch_reduce(chapsim_ctx *c, int what, double *host_out) {
+  TGDev &d = c->d;
+  dim3 grid((d.nx + RHS_BX - 1) / RHS_BX, (d.ny + RHS_BY - 1) / RHS_BY, d.nz);
+  k_reduce_part<<<grid, dim3(RHS_BX, RHS_BY), 0, c->stream>>>(d, what);
+  LAUNCHED();
+  k_reduce_final<<<1, 1024, 0, c->stream>>>(d, what, (int)(grid.x * grid.y * grid.z));
+  LAUNCHED();
+  double v = 0.0;
+  CK(cudaMemcpyAsync(&v, d.scal + 1, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *host_out = v;
+  return CHAPSIM_OK;
+}
+
+}  // namespace chapsim

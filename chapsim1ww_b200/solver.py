@@ -1,0 +1,172 @@
+"""Host-side mirror of the reference's TG-channel entry points over libchapsim.
+
+Method names follow the Fortran subroutines they replace (CHAPSim1WW,
+paths relative to the project root):
+
+=========================  ==================================================
+``solverrk3_mom_tg(ns)``   SOLVERRK3_MOM_tg(NS), src/SOLVERRK3_MOM_tg.f90:18-61
+``divg_tg(ns)``            DIVG_tg(NS), src/DIVG.f90:21-57
+``fft99_pois3d()``         FFT99_POIS3D_periodicxz(ITG), src/possion3d_FFT99.f90:254-488
+``veloupdt_tg(ns)``        VELOUPDT_tg + PRCALC_tg with wall BCs,
+                           src/VELO_CORRECTION.f90:19-105, src/PRESSURE_CORRECTION.f90:1-24
+``divgck_tg()``            DIVGCK_tg, src/DIVGCK.f90:16-58
+``bulk_velocity_tg()``     BULK_VELOCITY_TG, src/INITIAL_FL_FLD_TG.f90:122-149
+``random_fl_fld_tg()``     RANDOM_FL_FLD_TG + CALC_INITIALIZATION_tg,
+                           src/INITIAL_FL_FLD_TG.f90:2-119
+=========================  ==================================================
+
+Fields are numpy views of the Fortran layout F(1:nx, 0:ny+1, 1:nz): arrays of
+shape (nz, ny+2, nx) in C order, so ``a[k-1, j, i-1]`` is F(i, j, k).
+Errors raise ``ChapsimError`` (the reference prints and STOPs in ERRHDL).
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+
+FIELD_IDS = {"u": _lib.F_U, "v": _lib.F_V, "w": _lib.F_W, "p": _lib.F_P, "phi": _lib.F_PHI,
+             "rhsphi": _lib.F_RHSPHI, "h0u": _lib.F_H0U, "h0v": _lib.F_H0V, "h0w": _lib.F_H0W}
+
+
+class ChapsimError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{_lib.ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def default_config(**kw):
+    cfg = _lib.ChapsimConfig()
+    _lib.load().chapsim_config_default(ctypes.byref(cfg))
+    for k, v in kw.items():
+        if not hasattr(cfg, k):
+            raise KeyError(k)
+        setattr(cfg, k, v)
+    return cfg
+
+
+class TGChannel:
+    """One TG (periodic) channel domain resident on a GPU."""
+
+    def __init__(self, nx=64, ny=64, nz=64, lx=4 * math.pi, lz=4 * math.pi / 3, str2=2.0, istr2=1,
+                 ren=2800.0, dt=1e-3, flowdrvtp=1, cfgv=0.0, precision=_lib.FP64, device=0):
+        self.lib = _lib.load()
+        self.cfg = default_config(nx=nx, ny=ny, nz=nz, lx=lx, lz=lz, str2=str2, istr2=istr2, ren=ren, dt=dt,
+                                  flowdrvtp=flowdrvtp, cfgv=cfgv, precision=precision, device=device)
+        h = ctypes.c_void_p()
+        rc = self.lib.chapsim_create(ctypes.byref(self.cfg), ctypes.byref(h))
+        if rc != _lib.CHAPSIM_OK:
+            raise ChapsimError(rc, "chapsim_create failed")
+        self.h = h
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.n = self.lib.chapsim_field_len(self.h)
+
+    # ---------------------------------------------------------------- basics
+    def _chk(self, rc):
+        if rc != _lib.CHAPSIM_OK:
+            raise ChapsimError(rc, self.lib.chapsim_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.chapsim_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def shape(self):
+        return (self.nz, self.ny + 2, self.nx)
+
+    def set_field(self, name, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if a.size != self.n:
+            raise ValueError(f"field {name}: expected {self.n} values, got {a.size}")
+        self._chk(self.lib.chapsim_set_field(self.h, _lib.ITG, FIELD_IDS[name], a.ctypes.data, self.n))
+
+    def get_field(self, name, out=None):
+        a = np.empty(self.shape, dtype=np.float64) if out is None else out
+        self._chk(self.lib.chapsim_get_field(self.h, _lib.ITG, FIELD_IDS[name], a.ctypes.data, self.n))
+        return a
+
+    def set_field_device(self, name, ptr):
+        self._chk(self.lib.chapsim_set_field_device(self.h, _lib.ITG, FIELD_IDS[name], ptr, self.n))
+
+    def get_field_device(self, name, ptr):
+        self._chk(self.lib.chapsim_get_field_device(self.h, _lib.ITG, FIELD_IDS[name], ptr, self.n))
+
+    def mesh(self, what):
+        n = self.ny + 1 if what in (0, 3) else self.ny
+        out = np.empty(n)
+        self._chk(self.lib.chapsim_get_mesh(self.h, what, out.ctypes.data, n))
+        return out
+
+    def sync(self):
+        self._chk(self.lib.chapsim_sync(self.h))
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        self._chk(self.lib.chapsim_get_stream(self.h, ctypes.byref(s)))
+        return s.value
+
+    # ------------------------------------------------------ reference entries
+    def random_fl_fld_tg(self, seed=0, amp=0.1, project=True):
+        self._chk(self.lib.chapsim_init_random(self.h, seed, amp, 1 if project else 0))
+
+    def solverrk3_mom_tg(self, ns):
+        self._chk(self.lib.chapsim_rk3_mom_tg(self.h, ns))
+
+    def step(self, nsteps=1):
+        """NS = 1, 2, 3 for each of nsteps time steps (graph-replayed)."""
+        self._chk(self.lib.chapsim_step_tg(self.h, nsteps))
+
+    def divg_tg(self, ns):
+        self._chk(self.lib.chapsim_divg(self.h, _lib.ITG, ns))
+
+    def fft99_pois3d(self):
+        self._chk(self.lib.chapsim_pois3d(self.h, _lib.ITG))
+
+    def veloupdt_tg(self, ns):
+        self._chk(self.lib.chapsim_velo_correction(self.h, _lib.ITG, ns))
+
+    def _reduce(self, what):
+        v = ctypes.c_double()
+        self._chk(self.lib.chapsim_reduce(self.h, _lib.ITG, what, ctypes.byref(v)))
+        return v.value
+
+    def divgck_tg(self):
+        return self._reduce(_lib.R_DIVMAX)
+
+    def bulk_velocity_tg(self):
+        return self._reduce(_lib.R_BULK)
+
+    def nan_count(self):
+        return int(self._reduce(_lib.R_NANCOUNT))
+
+    # ------------------------------------------------------------- timing
+    def phase_timing(self, enable):
+        self._chk(self.lib.chapsim_phase_timing(self.h, 1 if enable else 0))
+
+    def phase_times(self):
+        ms = (ctypes.c_double * len(_lib.PHASES))()
+        n = ctypes.c_int64()
+        self._chk(self.lib.chapsim_phase_times(self.h, ms, len(_lib.PHASES), ctypes.byref(n)))
+        return dict(zip(_lib.PHASES, list(ms))), n.value
+
+    def phase_reset(self):
+        self._chk(self.lib.chapsim_phase_reset(self.h))
+
+    def launch_count(self):
+        n = ctypes.c_int64()
+        self._chk(self.lib.chapsim_launch_count(self.h, ctypes.byref(n)))
+        return n.value

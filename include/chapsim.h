@@ -1,0 +1,186 @@
+/*
+ * chapsim.h -- C ABI of libchapsim, the B200 (sm_100a) implementation of
+ * CHAPSim's RK3 fractional-step substep.
+ *
+ * The reference (weiwangstfc/CHAPSim1WW, Fortran 90 + MPI) has no plugin or
+ * FFI layer: its hot path is a set of Fortran subroutines that take a substep
+ * index and work on module-global arrays.  Each entry point below replaces one
+ * of those subroutines; the comment names the reference routine (file:line,
+ * relative to the CHAPSim1WW project root) it stands in for.  A Fortran host
+ * binds them with ISO_C_BINDING interfaces.
+ *
+ * Conventions
+ *  - Every function returns an int status: CHAPSIM_OK (0) or a CHAPSIM_ERR_*
+ *    code.  chapsim_last_error() gives a one-line message for the last error on
+ *    a context.  The reference's equivalent is ERRHDL, which prints and STOPs
+ *    (src/WRTHDL.f90:18-30); a Fortran shim calls ERRHDL on a nonzero status.
+ *  - The device owns the solution between calls.  Host arrays are uploaded with
+ *    chapsim_set_field and read back with chapsim_get_field, in the reference's
+ *    own Fortran layout F(1:nx, 0:ny+1, 1:nz) (x fastest, one y ghost layer on
+ *    each side, z slowest), the layout of Q_tg/PR_tg/DPH_tg
+ *    (src/MEMALLOCT.f90:99-106).  A velocity component of Q_tg(:,:,:,n) is the
+ *    contiguous slab starting at Q_tg(1,0,1,n).
+ *  - Work is queued on the context's CUDA stream; calls return before the GPU
+ *    finishes.  chapsim_sync waits and reports any device-side error.  Calls
+ *    that return host data synchronise by themselves.
+ *  - One host thread per context; a context is not re-entrant.
+ *  - Everything is FP64 at the boundary.
+ */
+#ifndef CHAPSIM_H
+#define CHAPSIM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CHAPSIM_ABI_VERSION 1
+
+/* status codes */
+#define CHAPSIM_OK 0
+#define CHAPSIM_ERR_ARG 1         /* invalid argument or size mismatch        */
+#define CHAPSIM_ERR_CUDA 2        /* a CUDA runtime call failed               */
+#define CHAPSIM_ERR_NOMEM 3       /* device allocation failed                 */
+#define CHAPSIM_ERR_STATE 4       /* call not valid in the context's state    */
+#define CHAPSIM_ERR_NUMERIC 5     /* NaN/Inf detected by a checked reduction  */
+#define CHAPSIM_ERR_UNSUPPORTED 6 /* configuration not supported              */
+#define CHAPSIM_ERR_NODEVICE 7    /* no CUDA device visible                   */
+
+/* domain ids: the reference's ITG / IIO parameters (src/modules.f90:46-47) */
+#define CHAPSIM_ITG 1
+#define CHAPSIM_IIO 2
+
+/* precision forms */
+#define CHAPSIM_FP64 0  /* every array and operation in FP64                    */
+#define CHAPSIM_MIXED 1 /* FP64 state; FP32 temporaries, FFT and line solves,
+                           FP64 low-mode Poisson lines, reductions and one
+                           FP64-residual refinement sweep of the Poisson solve */
+
+/* field ids for chapsim_set_field / chapsim_get_field (TG domain) */
+#define CHAPSIM_F_U 0      /* Q_tg(:,:,:,1)   */
+#define CHAPSIM_F_V 1      /* Q_tg(:,:,:,2)   */
+#define CHAPSIM_F_W 2      /* Q_tg(:,:,:,3)   */
+#define CHAPSIM_F_P 3      /* PR_tg           */
+#define CHAPSIM_F_PHI 4    /* DPH_tg          */
+#define CHAPSIM_F_RHSPHI 5 /* RHSLLPHI_tg     */
+#define CHAPSIM_F_H0U 6    /* CONVH0_tg(:,:,:,1) (y ghosts ignored) */
+#define CHAPSIM_F_H0V 7    /* CONVH0_tg(:,:,:,2) */
+#define CHAPSIM_F_H0W 8    /* CONVH0_tg(:,:,:,3) */
+
+/* reductions for chapsim_reduce */
+#define CHAPSIM_R_DIVMAX 0 /* max |div u|, DIVGCK_tg (src/DIVGCK.f90:16-58)          */
+#define CHAPSIM_R_BULK 1   /* bulk velocity, BULK_VELOCITY_TG
+                              (src/INITIAL_FL_FLD_TG.f90:122-149)                  */
+#define CHAPSIM_R_NANCOUNT 2 /* number of non-finite values in u, v, w, p          */
+
+/* Per-phase timer slots for chapsim_phase_times (milliseconds, accumulated). */
+#define CHAPSIM_PH_RHS 0     /* convection + RHS assembly (+ mass-flux sum)   */
+#define CHAPSIM_PH_ADIX 1    /* x Crank-Nicolson factor                       */
+#define CHAPSIM_PH_ADIZ 2    /* z Crank-Nicolson factor                       */
+#define CHAPSIM_PH_ADIY 3    /* y Crank-Nicolson factor + q += dq + wall BC   */
+#define CHAPSIM_PH_FFTX 4    /* divergence + forward real FFT along x         */
+#define CHAPSIM_PH_FFTZ 5    /* forward complex FFT along z                   */
+#define CHAPSIM_PH_YSOLVE 6  /* Poisson y-tridiagonals (incl. refinement)     */
+#define CHAPSIM_PH_IFFTZ 7   /* inverse FFT along z                           */
+#define CHAPSIM_PH_IFFTX 8   /* inverse real FFT along x + phi ghosts         */
+#define CHAPSIM_PH_CORR 9    /* velocity + pressure correction + wall BC      */
+#define CHAPSIM_PH_COUNT 10
+
+/*
+ * Run configuration.  Replaces the module globals the reference reads from
+ * readdata.ini (src/READINI.f90:43-435) for the TG channel section.
+ * Geometry is the plane channel (icase = ICHANL, y in [-1, 1]).
+ */
+typedef struct chapsim_config {
+  int32_t struct_size; /* sizeof(chapsim_config), for ABI checks             */
+  int32_t nx;          /* NCL1_tg, even, >= 8                                */
+  int32_t ny;          /* NCL2, >= 4                                         */
+  int32_t nz;          /* NCL3, even, >= 8                                   */
+  double lx;           /* HX_tg, streamwise length                          */
+  double lz;           /* HZ, spanwise length                               */
+  double str2;         /* STR2, tanh stretching factor                      */
+  int32_t istr2;       /* ISTR2: 1 tanh stretching, 0 uniform               */
+  int32_t flowdrvtp;   /* FLOWDRVTP: 1 constant mass flux, 2 constant dp/dx */
+  double ren;          /* REN, bulk Reynolds number                         */
+  double dt;           /* DT, fixed time step                               */
+  double cfgv;         /* CFGV, skin-friction coefficient for flowdrvtp=2   */
+  int32_t precision;   /* CHAPSIM_FP64 or CHAPSIM_MIXED                     */
+  int32_t device;      /* CUDA device ordinal                               */
+} chapsim_config;
+
+typedef struct chapsim_ctx chapsim_ctx;
+
+/* Fill *cfg with defaults (64^3, Lx=4pi, Lz=4pi/3, beta=2, Re=2800, dt=1e-3,
+ * constant mass flux, FP64, device 0). */
+int chapsim_config_default(chapsim_config *cfg);
+
+/* Set-up: MEM_ALLOCAT + COORDJR + TDMA_COEF + CONS_RKCOEF + CONSPARA +
+ * FFT99_POIS3D_INIT(ITG) (src/DNS_THERMAL.f90:117-176,
+ * src/possion3d_FFT99.f90:54-220).  Allocates all device state. */
+int chapsim_create(const chapsim_config *cfg, chapsim_ctx **out);
+int chapsim_destroy(chapsim_ctx *ctx);
+const char *chapsim_last_error(const chapsim_ctx *ctx);
+int chapsim_sync(chapsim_ctx *ctx);
+
+/* Length in doubles of one Fortran-layout field: nx*(ny+2)*nz. */
+int64_t chapsim_field_len(const chapsim_ctx *ctx);
+
+/* Upload / download one field in Fortran layout.  n must equal
+ * chapsim_field_len.  host may be pageable or pinned. */
+int chapsim_set_field(chapsim_ctx *ctx, int domain, int field, const double *host, int64_t n);
+int chapsim_get_field(chapsim_ctx *ctx, int domain, int field, double *host, int64_t n);
+/* Device-resident variants: dev is a device pointer on the context's device. */
+int chapsim_set_field_device(chapsim_ctx *ctx, int domain, int field, const double *dev, int64_t n);
+int chapsim_get_field_device(chapsim_ctx *ctx, int domain, int field, double *dev, int64_t n);
+
+/* Mesh and coefficient arrays (host copies), for checks:
+ * what = 0 YND(1:ny+1), 1 YCC(1:ny), 2 DYFI(1:ny), 3 DYCI(1:ny+1). */
+int chapsim_get_mesh(const chapsim_ctx *ctx, int what, double *out, int64_t n);
+
+/* Seeded initial field: RANDOM_FL_FLD_TG + CALC_INITIALIZATION_tg
+ * (src/INITIAL_FL_FLD_TG.f90:2-119).  Uniform perturbations of amplitude amp
+ * on u, v, w from a counter-based splitmix64 keyed by (seed, component, i, j,
+ * k), xz-mean removal, the laminar profile 1.5(1-y^2) on u, v = 0 at the wall,
+ * bulk velocity rescaled to 1.  When project != 0 an NS=0 substep follows
+ * (the reference's initial projection). */
+int chapsim_init_random(chapsim_ctx *ctx, uint64_t seed, double amp, int project);
+
+/* SOLVERRK3_MOM_tg(NS) (src/SOLVERRK3_MOM_tg.f90:18-61), NS in 0..3. */
+int chapsim_rk3_mom_tg(chapsim_ctx *ctx, int ns);
+/* One full time step: NS = 1, 2, 3. */
+int chapsim_step_tg(chapsim_ctx *ctx, int nsteps);
+
+/* Stand-alone pieces of the substep (each updates device state only):
+ * DIVG_tg(NS) (src/DIVG.f90:21-57): RHSPHI = div(u)/(alpha dt). */
+int chapsim_divg(chapsim_ctx *ctx, int domain, int ns);
+/* FFT99_POIS3D_periodicxz(IDOMAIN) (src/possion3d_FFT99.f90:254-488):
+ * PHI = L^{-1} RHSPHI (plus the ghost copy of BC_WALL_DPH). */
+int chapsim_pois3d(chapsim_ctx *ctx, int domain);
+/* VELOUPDT_tg(NS) + PRCALC_tg(NS) with their wall BCs
+ * (src/VELO_CORRECTION.f90:19-105, src/PRESSURE_CORRECTION.f90:1-24). */
+int chapsim_velo_correction(chapsim_ctx *ctx, int domain, int ns);
+
+/* Device reductions (DIVGCK_tg, BULK_VELOCITY_TG); synchronises. */
+int chapsim_reduce(chapsim_ctx *ctx, int domain, int what, double *out);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that time or order
+ * work against it. */
+int chapsim_get_stream(const chapsim_ctx *ctx, void **stream);
+
+/* Phase timers: enable (1) / disable (0) CUDA-event timing between phases of
+ * every substep; read accumulated milliseconds per phase and the number of
+ * substeps timed; reset clears them. */
+int chapsim_phase_timing(chapsim_ctx *ctx, int enable);
+int chapsim_phase_times(chapsim_ctx *ctx, double *ms, int n, int64_t *substeps);
+int chapsim_phase_reset(chapsim_ctx *ctx);
+
+/* Number of kernel launches the library issued on this context since creation
+ * (or the last reset). */
+int chapsim_launch_count(const chapsim_ctx *ctx, int64_t *count);
+int chapsim_launch_count_reset(chapsim_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CHAPSIM_H */
