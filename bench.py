@@ -1,0 +1,341 @@
+"""Benchmark of the CHAPSim TG RK3 step on B200 (libchapsim, sm_100a).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload NAME] [--precision fp64|mixed]
+
+A "step" is one full RK3 time step (substeps NS = 1, 2, 3) of the workload's
+channel.  Metric: cell-steps/s = cells x steps / seconds.
+
+Default workload: the 256x192x256 TG channel of the coupled TG+IO
+configuration (Lx = 4 pi, Lz = 4 pi / 3, tanh stretching beta = 2,
+Re_b = 2800, dt = 1e-3, seed 1), synthetic seeded initial field.  With N > 1
+GPUs every rank advances its own independent channel (replicas, weak scaling,
+no data-path collective); timing is the max over ranks.
+
+Arms:
+  ours       libchapsim through the C ABI; `value` with the state resident in
+             HBM (CUDA-graph replay of the step), `e2e` through the public API
+             with host buffers (upload u, v, w, p from pinned memory, one step,
+             download u, v, w, p and max|div u| every step).
+  reference  the reference algorithm's CPU path: the FP64 oracle port
+             (OpenMP, all host threads) on the same workload, rank 0 only.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # TG section of the coupled TG+IO configuration
+    "tg_256x192x256": dict(nx=256, ny=192, nz=256, lx=4 * math.pi, lz=4 * math.pi / 3, ren=2800.0, dt=1e-3, seed=1),
+    # the CPU-runnable plain-method configuration
+    "tg_64x64x64": dict(nx=64, ny=64, nz=64, lx=4 * math.pi, lz=4 * math.pi / 3, ren=2800.0, dt=1e-3, seed=0),
+}
+METRIC = "cell-steps/s"
+
+# Algorithmic HBM bytes per launch of each phase kernel, FP64 form, in units
+# of 8-byte values per cell (spectral phases: per complex spectral value).
+PHASE_VALUES_PER_CELL = {"rhs": 13, "adix": 6, "adiz": 6, "adiy": 9, "fftx": 4, "corr": 10}
+PHASE_SPECTRAL_PASSES = {"fftx": 1, "fftz": 2, "ysolve": 2, "ifftz": 2, "ifftx": 1}
+PHASE_KERNEL = {"rhs": "k_rhs", "adix": "k_adix", "adiz": "k_adiz", "adiy": "k_adiy", "fftx": "k_fftx",
+                "fftz": "k_fftz", "ysolve": "k_ysolve", "ifftz": "k_fftz", "ifftx": "k_ifftx", "corr": "k_corr"}
+
+
+def phase_bytes(ph, nx, ny, nz, real_bytes=8):
+    cells = nx * ny * nz
+    spec = (nx // 2 + 1) * ny * nz
+    b = PHASE_VALUES_PER_CELL.get(ph, 0) * real_bytes * cells
+    if ph == "ifftx":
+        b += real_bytes * cells  # phi written
+    b += PHASE_SPECTRAL_PASSES.get(ph, 0) * 2 * real_bytes * spec
+    return b
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[3:7]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def load_traffic(workload, kernel):
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return d.get(workload, {}).get(kernel)
+    except Exception:
+        return None
+
+
+def cpu_baseline_oracle(wl, steps):
+    """FP64 oracle port on the host cores: init + NS=0, then `steps` timed steps."""
+    from oracle.pyoracle import OracleTG, get_threads
+    o = OracleTG(wl["nx"], wl["ny"], wl["nz"], lx=wl["lx"], lz=wl["lz"], ren=wl["ren"], dt=wl["dt"])
+    o.init_random(wl["seed"], 0.1)
+    o.substep(0)
+    t0 = time.perf_counter()
+    o.step(steps)
+    t = time.perf_counter() - t0
+    cells = wl["nx"] * wl["ny"] * wl["nz"]
+    return cells * steps / t, t, get_threads()
+
+
+def run_reference(args, wl, ws, rank):
+    if rank != 0:
+        return 0
+    from oracle.pyoracle import OracleTG, get_threads
+    o = OracleTG(wl["nx"], wl["ny"], wl["nz"], lx=wl["lx"], lz=wl["lz"], ren=wl["ren"], dt=wl["dt"])
+    o.init_random(wl["seed"], 0.1)
+    o.substep(0)
+    for _ in range(args.warmup):
+        o.step(1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.step(1)
+    t = time.perf_counter() - t0
+    cells = wl["nx"] * wl["ny"] * wl["nz"]
+    v = cells * args.steps / t
+    cores = get_threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * t / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded splitmix64 field)",
+        "config": {"workload": args.workload, **{k: wl[k] for k in ("nx", "ny", "nz", "ren", "dt")},
+                   "parallelism": "host threads"},
+        "cpu_baseline": {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} full RK3 steps of the {args.workload} channel, FP64 oracle "
+                                   f"(restatement of the Fortran path), OpenMP {cores} threads"},
+        "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, wl, ws, rank, local):
+    import numpy as np
+    import torch
+
+    import chapsim1ww_b200 as cs
+    from chapsim1ww_b200 import TGChannel
+
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    prec = cs.MIXED if args.precision == "mixed" else cs.FP64
+    s = TGChannel(wl["nx"], wl["ny"], wl["nz"], lx=wl["lx"], lz=wl["lz"], ren=wl["ren"], dt=wl["dt"],
+                  precision=prec, device=local)
+    s.random_fl_fld_tg(wl["seed"] + rank, 0.1, project=True)
+    cells = wl["nx"] * wl["ny"] * wl["nz"]
+    stream = torch.cuda.ExternalStream(s.stream(), device=local)
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    def max_over_ranks(x):
+        if pg is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- resident timing (graph replay)
+    s.step(args.warmup)
+    s.sync()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n0 = s.launch_count()
+    e0.record(stream)
+    s.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    launches = s.launch_count() - n0
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = cells * ws * args.steps / (ms / 1000.0)
+    divmax = s.divgck_tg()
+
+    # ---- per-phase kernel times (eager launches, CUDA events between phases)
+    s.phase_timing(True)
+    s.phase_reset()
+    s.step(args.steps)
+    ph, nsub = s.phase_times()
+    s.phase_timing(False)
+    per_launch = {k: v / max(nsub, 1) for k, v in ph.items()}
+    dom = max(per_launch, key=per_launch.get)
+    peak, peak_kind = measured_peak()
+    bytes_dom = phase_bytes(dom, wl["nx"], wl["ny"], wl["nz"])
+    achieved = bytes_dom / (per_launch[dom] / 1000.0) / 1e9
+    total_bytes = sum(phase_bytes(p, wl["nx"], wl["ny"], wl["nz"]) for p in ph)
+    step_ms_phases = 3 * sum(per_launch.values())
+    traffic = load_traffic(args.workload, PHASE_KERNEL[dom])
+
+    # ---- end to end through the public API with host buffers
+    names = ("u", "v", "w", "p")
+    host = {}
+    for n in names:
+        t = torch.empty(s.shape, dtype=torch.float64, pin_memory=True)
+        host[n] = t.numpy()
+        s.get_field(n, out=host[n])
+    barrier()
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(1, min(args.steps, 20))
+    e2.record(stream)
+    for _ in range(e2e_steps):
+        for n in names:
+            s.set_field(n, host[n])
+        s.step(1)
+        for n in names:
+            s.get_field(n, out=host[n])
+        _ = s.divgck_tg()
+    e3.record(stream)
+    e3.synchronize()
+    barrier()
+    ms_e2e = max_over_ranks(e2.elapsed_time(e3))
+    e2e_value = cells * ws * e2e_steps / (ms_e2e / 1000.0)
+    nbytes = 4 * s.n * 8
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            v, t, cores = cpu_baseline_oracle(wl, args.cpu_steps)
+            cpu = {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
+                   "sample": f"{args.cpu_steps} full RK3 steps of the {args.workload} channel after init, "
+                             f"FP64 oracle port, OpenMP {cores} threads, {t:.1f} s"}
+        except Exception as ex:  # the checker is optional for the GPU arm
+            cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if prec == cs.FP64 else "f64 state / f32 temporaries",
+            "data": "synthetic (seeded splitmix64 initial field, NS=0 projection)",
+            "config": {"workload": args.workload, **{k: wl[k] for k in ("nx", "ny", "nz", "ren", "dt")},
+                       "precision": args.precision, "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                       "l2": "working set (>1 GB) larger than the 126 MB L2"},
+            "max_div_u": divmax,
+            "gpu_launches": launches,
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes + 8, "steps": e2e_steps},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "kernel": PHASE_KERNEL[dom],
+                         "phase": dom, "algorithmic_bytes_per_launch": bytes_dom,
+                         "avg_launch_ms": per_launch[dom], "peak_source": peak_kind},
+            "phases_ms_per_launch": per_launch,
+            "step_roofline": {"algorithmic_bytes_per_step": 3 * total_bytes,
+                              "achieved_gbs": 3 * total_bytes / (ms / args.steps / 1000.0) / 1e9,
+                              "frac": 3 * total_bytes / (ms / args.steps / 1000.0) / 1e9 / peak,
+                              "phase_sum_ms": step_ms_phases},
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="tg_256x192x256")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    wl = WORKLOADS[args.workload]
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        return run_reference(args, wl, ws, rank)
+    return run_ours(args, wl, ws, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

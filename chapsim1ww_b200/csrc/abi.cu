@@ -89,6 +89,39 @@ void cyc_tables(int n, double a, double *pp, double *h0, double *g2, double &b, 
   qq = b + c * g2[0] + a * g2[n - 2];
 }
 
+// x = A^{-1} r for the cyclic tridiagonal (a, b, a) with the tables above
+// (the same sweeps as the device routine cyc_line).
+void cyc_apply(int n, double a, double b, double qq, const double *pp, const double *h0, const double *g2,
+               double *r) {
+  std::vector<double> g(n);
+  g[0] = r[0] / b;
+  for (int m = 1; m <= n - 2; ++m) g[m] = (r[m] - g[m - 1] * a) * pp[m];
+  double gn = g[n - 2];
+  for (int m = n - 3; m >= 0; --m) {
+    gn = g[m] - h0[m] * gn;
+    g[m] = gn;
+  }
+  const double xn = (r[n - 1] - a * g[0] - a * g[n - 2]) / qq;
+  r[n - 1] = xn;
+  for (int m = 0; m <= n - 2; ++m) r[m] = g[m] + g2[m] * xn;
+}
+
+// First row of the circulant inverse and the width past which its entries sum
+// to less than 2^-60 of the central one (-1 when wider than wmax).
+int circulant_band(int n, double a, double b, double qq, const double *pp, const double *h0, const double *g2,
+                   int wmax, std::vector<double> &g) {
+  g.assign(n, 0.0);
+  g[0] = 1.0;
+  cyc_apply(n, a, b, qq, pp, h0, g2, g.data());
+  const double tol = ldexp(fabs(g[0]), -60);
+  for (int w = 0; w <= wmax && 2 * w + 1 <= n; ++w) {
+    double tail = 0.0;
+    for (int m = w + 1; m <= n / 2; ++m) tail += fabs(g[m]) + (m != n - m ? fabs(g[n - m]) : 0.0);
+    if (tail <= tol) return w;
+  }
+  return -1;
+}
+
 }  // namespace
 
 extern "C" {
@@ -120,6 +153,9 @@ static void free_all(chapsim_ctx *ctx) {
   ctx->allocs.clear();
   for (auto &e : ctx->ev)
     if (e) { cudaEventDestroy(e); e = nullptr; }
+  for (auto &e : ctx->evpool)
+    if (e) cudaEventDestroy(e);
+  ctx->evpool.clear();
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   ctx->stream = nullptr;
 }
@@ -255,6 +291,19 @@ static int build_tables(chapsim_ctx *ctx) {
     cyc_tables(nx, xa[ns], &H[o_x[ns][0]], &H[o_x[ns][1]], &H[o_x[ns][2]], xb[ns], xqq[ns]);
     cyc_tables(nz, za[ns], &H[o_z[ns][0]], &H[o_z[ns][1]], &H[o_z[ns][2]], zb[ns], zqq[ns]);
   }
+  // truncated circulant inverses of the x and z factors
+  size_t o_gx[4], o_gz[4];
+  int wx[4], wz[4];
+  for (int ns = 0; ns < 4; ++ns) {
+    std::vector<double> g;
+    const int band_max = 12;  // BAND_WMAX in tg_kernels.cu
+    wx[ns] = circulant_band(nx, xa[ns], xb[ns], xqq[ns], &H[o_x[ns][0]], &H[o_x[ns][1]], &H[o_x[ns][2]], band_max, g);
+    o_gx[ns] = alloc(band_max + 1);
+    if (wx[ns] >= 0) for (int m = 0; m <= wx[ns]; ++m) H[o_gx[ns] + m] = g[m];
+    wz[ns] = circulant_band(nz, za[ns], zb[ns], zqq[ns], &H[o_z[ns][0]], &H[o_z[ns][1]], &H[o_z[ns][2]], band_max, g);
+    o_gz[ns] = alloc(band_max + 1);
+    if (wz[ns] >= 0) for (int m = 0; m <= wz[ns]; ++m) H[o_gz[ns] + m] = g[m];
+  }
   // FFT twiddles exp(-2 pi i m / n)
   size_t o_twx = alloc(2 * (size_t)nx), o_twz = alloc(2 * (size_t)nz);
   for (int m = 0; m < nx; ++m) {
@@ -306,6 +355,11 @@ static int build_tables(chapsim_ctx *ctx) {
     sp.za = za[ns]; sp.zb = zb[ns]; sp.zqq = zqq[ns];
     sp.flowdrvtp = cf.flowdrvtp;
     sp.dp_const = -0.5 * cf.cfgv * sp.alp * cf.dt;
+    sp.gx = D + o_gx[ns];
+    sp.gz = D + o_gz[ns];
+    sp.wx = wx[ns];
+    sp.wz = wz[ns];
+    sp.band = (wx[ns] >= 0 && wz[ns] >= 0 && ctx->allow_band) ? 1 : 0;
   }
   ctx->fx.tw64 = reinterpret_cast<const double2 *>(D + o_twx);
   ctx->fz.tw64 = reinterpret_cast<const double2 *>(D + o_twz);
@@ -351,6 +405,9 @@ int chapsim_create(const chapsim_config *cfg, chapsim_ctx **out) {
   }
   for (auto &e : ctx->ev)
     if (cudaEventCreate(&e) != cudaSuccess) { free_all(ctx); delete ctx; return CHAPSIM_ERR_CUDA; }
+  ctx->evpool.assign((size_t)chapsim_ctx::kEvSub * (CHAPSIM_PH_COUNT + 1), nullptr);
+  for (auto &e : ctx->evpool)
+    if (cudaEventCreate(&e) != cudaSuccess) { free_all(ctx); delete ctx; return CHAPSIM_ERR_CUDA; }
   setup_mesh(ctx);
   TGDev &d = ctx->d;
   d.nx = cfg->nx; d.ny = cfg->ny; d.nz = cfg->nz; d.lh = cfg->nx / 2 + 1;
@@ -367,6 +424,9 @@ int chapsim_create(const chapsim_config *cfg, chapsim_ctx **out) {
   for (int c = 0; c < 3; ++c) {
     if ((rc = dalloc(ctx, &p, n * sizeof(double)))) goto fail;
     d.rhs[c] = p;
+    cudaMemsetAsync(p, 0, n * sizeof(double), ctx->stream);
+    if ((rc = dalloc(ctx, &p, n * sizeof(double)))) goto fail;
+    d.dq[c] = p;
     cudaMemsetAsync(p, 0, n * sizeof(double), ctx->stream);
   }
   {
@@ -385,6 +445,9 @@ int chapsim_create(const chapsim_config *cfg, chapsim_ctx **out) {
     if ((rc = dalloc(ctx, &p, 16 * sizeof(double)))) goto fail;
     d.scal = (double *)p;
     cudaMemsetAsync(p, 0, 16 * sizeof(double), ctx->stream);
+    if ((rc = dalloc(ctx, &p, 16 * sizeof(int)))) goto fail;
+    d.err = (int *)p;
+    cudaMemsetAsync(p, 0, 16 * sizeof(int), ctx->stream);
   }
   if ((rc = build_tables(ctx))) goto fail;
   px.tw64 = ctx->fx.tw64; px.tw32 = ctx->fx.tw32;
@@ -412,10 +475,23 @@ int chapsim_destroy(chapsim_ctx *ctx) {
 
 const char *chapsim_last_error(const chapsim_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
+// Read and clear the device error word (bounded waits that gave up).
+static int check_device_error(chapsim_ctx *ctx) {
+  int e = 0;
+  CKC(cudaMemcpyAsync(&e, ctx->d.err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CKC(cudaStreamSynchronize(ctx->stream));
+  if (e != 0) {
+    CKC(cudaMemsetAsync(ctx->d.err, 0, sizeof(int), ctx->stream));
+    ctx->err = "device-side wait gave up (error word " + std::to_string(e) + ")";
+    return CHAPSIM_ERR_CUDA;
+  }
+  return CHAPSIM_OK;
+}
+
 int chapsim_sync(chapsim_ctx *ctx) {
   if (!ctx) return CHAPSIM_ERR_ARG;
   CKC(cudaStreamSynchronize(ctx->stream));
-  return CHAPSIM_OK;
+  return check_device_error(ctx);
 }
 
 int64_t chapsim_field_len(const chapsim_ctx *ctx) {
@@ -627,17 +703,25 @@ int chapsim_get_stream(const chapsim_ctx *ctx, void **stream) {
 
 int chapsim_phase_timing(chapsim_ctx *ctx, int enable) {
   if (!ctx) return CHAPSIM_ERR_ARG;
+  if (!enable && ctx->timing) {
+    int rc = flush_phase_events(ctx);
+    if (rc) return rc;
+  }
   ctx->timing = enable != 0;
   return CHAPSIM_OK;
 }
 int chapsim_phase_times(chapsim_ctx *ctx, double *ms, int n, int64_t *substeps) {
   if (!ctx || !ms || n < CHAPSIM_PH_COUNT) return CHAPSIM_ERR_ARG;
+  int rc = flush_phase_events(ctx);
+  if (rc) return rc;
   for (int i = 0; i < CHAPSIM_PH_COUNT; ++i) ms[i] = ctx->phase_ms[i];
   if (substeps) *substeps = ctx->timed_substeps;
   return CHAPSIM_OK;
 }
 int chapsim_phase_reset(chapsim_ctx *ctx) {
   if (!ctx) return CHAPSIM_ERR_ARG;
+  int rc = flush_phase_events(ctx);
+  if (rc) return rc;
   for (double &m : ctx->phase_ms) m = 0.0;
   ctx->timed_substeps = 0;
   return CHAPSIM_OK;

@@ -1,6 +1,7 @@
 // Internal definitions shared by the libchapsim translation units.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -23,11 +24,13 @@ struct TGDev {
   double *h0[3];
   // temporaries (double in the FP64 form, float in the mixed form)
   void *rhs[3];
+  void *dq[3];      // x/z-solved increments (banded-inverse path)
   void *spec;       // complex spectral array
   double *ysc;      // Poisson y-solve scratch (h_j), lh*ny*nz
   double2 *spec64;  // FP64 spectral scratch for the refinement sweep (mixed)
   double *partials; // per-block mass-flux partial sums
   double *scal;     // device scalars: [0] dpgrns, [1..] reduction outputs
+  int *err;         // device error word (bounded waits that gave up)
   // mesh coefficients (1-based in j, arrays of length ny+2)
   const double *dyfi, *dyci, *wff, *wfb;
   const double *amvr[3], *acvr[3], *apvr[3];
@@ -49,6 +52,10 @@ struct SubParams {
   double za, zb, zqq;
   int flowdrvtp;
   double dp_const;  // flowdrvtp == 2: -0.5*cfgv*alp*dt
+  // truncated circulant inverses of the x and z factors (first rows g_0..g_W)
+  const double *gx, *gz;
+  int wx, wz;
+  int band;  // 1: x/z factors applied by k_adixz_band
 };
 
 struct FFTPlan {
@@ -83,10 +90,19 @@ struct chapsim_ctx {
 
   // phase timing
   bool timing = false;
-  cudaEvent_t ev[CHAPSIM_PH_COUNT + 1]{};
+  cudaEvent_t ev[CHAPSIM_PH_COUNT + 1]{};  // scratch events for stand-alone use
+  static constexpr int kEvSub = 48;       // substeps buffered before a readback
+  std::vector<cudaEvent_t> evpool;        // (PH_COUNT + 1) events per buffered substep
+  int ev_pending = 0;
   double phase_ms[CHAPSIM_PH_COUNT]{};
   int64_t timed_substeps = 0;
 
+  // TMA descriptors of u, v, w, p for the z-marching RHS kernel
+  CUtensorMap rhs_maps[7];
+  bool use_tma_rhs = false;
+  bool allow_band = true;   // banded x/z inverses when narrow enough
+  bool fft_big = false;     // FFT plans with radix 7 or 11
+  int rhs_nzc = 16;
   // CUDA graph of one full step (NS = 1, 2, 3)
   cudaGraphExec_t step_graph = nullptr;
   int64_t kernels_per_step = 0;
@@ -95,6 +111,7 @@ struct chapsim_ctx {
 // Kernel launch wrappers (defined in tg_kernels.cu).
 namespace chapsim {
 int init_kernels(chapsim_ctx *c);
+int flush_phase_events(chapsim_ctx *c);
 int launch_substep(chapsim_ctx *c, int ns);
 int launch_divg(chapsim_ctx *c, int ns);
 int launch_pois3d(chapsim_ctx *c);

@@ -108,7 +108,9 @@ __device__ __forceinline__ void stockham_stage(const C *__restrict__ in, C *__re
 // Transform nlines lines (each n complex values, stride lstride) held in
 // shared memory buffer a; b is scratch of the same size.  Returns the buffer
 // holding the result.  Must be called by every thread of the block.
-template <typename C>
+// BIG selects whether radices 7 and 11 are compiled in (they raise register
+// use of every stage, so plans with only 2, 3, 4, 5 use the small variant).
+template <typename C, bool BIG>
 __device__ C *fft_lines(C *a, C *b, int nlines, int n, int lstride, const int *rad, int nrad,
                         const C *__restrict__ tw, int sign) {
   int Ns = 1;
@@ -119,8 +121,8 @@ __device__ C *fft_lines(C *a, C *b, int nlines, int n, int lstride, const int *r
       case 3: stockham_stage<C, 3>(a, b, nlines, n, lstride, Ns, tw, sign); break;
       case 4: stockham_stage<C, 4>(a, b, nlines, n, lstride, Ns, tw, sign); break;
       case 5: stockham_stage<C, 5>(a, b, nlines, n, lstride, Ns, tw, sign); break;
-      case 7: stockham_stage<C, 7>(a, b, nlines, n, lstride, Ns, tw, sign); break;
-      case 11: stockham_stage<C, 11>(a, b, nlines, n, lstride, Ns, tw, sign); break;
+      case 7: if (BIG) stockham_stage<C, 7>(a, b, nlines, n, lstride, Ns, tw, sign); break;
+      case 11: if (BIG) stockham_stage<C, 11>(a, b, nlines, n, lstride, Ns, tw, sign); break;
       default: break;  // plans only contain the radices above
     }
     __syncthreads();

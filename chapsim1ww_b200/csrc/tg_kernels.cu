@@ -17,10 +17,13 @@
 //   ifftx    inverse real FFT along x -> phi, BC_WALL_DPH ghost copy.
 //   corr     VELOUPDT_tg + PRCALC_tg + BC_WALL_Q_tg/BC_WALL_PR_tg.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <stdio.h>
+#include <string.h>
 
 #include "chapsim_internal.cuh"
 #include "fft_smem.cuh"
+#include "tma.cuh"
 
 namespace chapsim {
 
@@ -174,11 +177,213 @@ k_rhs(TGDev d, SubParams sp) {
     d.partials[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = s;
 }
 
+// Same arithmetic as k_rhs, organised as a 2.5-D stencil: a block owns a
+// 32 x 8 (x, y) tile and marches along z over nzc planes.  Each plane of u,
+// v, w, p arrives in shared memory as one TMA box of 36 x 10 doubles
+// (x0-2 .. x0+33, j0-1 .. j0+8; the x start is 16-byte aligned), in a ring of
+// four plane slots, so plane k+2 is in flight while plane k is computed.
+// Periodic x neighbours outside the box are patched in from global memory on
+// the first and last x tiles; z wraps by plane index.
+constexpr int RT_BXW = 36, RT_BYW = 10, RT_PLANE = RT_BXW * RT_BYW;
+// field planes are padded to 368 doubles (2944 B) so every TMA destination is
+// 128-byte aligned; a slot holds u, v, w, p of one plane (36 x 10 boxes) and
+// the three H0 components of that plane (32 x 8 boxes of T).
+constexpr int RT_PST = 368;
+constexpr int RT_HBOX = RHS_BX * RHS_BY;  // 256 values
+static_assert((RT_PST * 8) % 128 == 0 && RT_PST >= RT_PLANE, "TMA destinations must stay 128-byte aligned");
+template <typename T> struct RtLayout {
+  static constexpr size_t field_bytes = (size_t)4 * RT_PST * sizeof(double);
+  static constexpr size_t h0_bytes = (size_t)RT_HBOX * sizeof(T);  // 2048 or 1024: multiples of 128
+  static constexpr size_t slot_bytes = field_bytes + 3 * h0_bytes;
+  static constexpr size_t smem_bytes = 4 * slot_bytes + 4 * sizeof(uint64_t);
+  static constexpr uint32_t tx_bytes = (uint32_t)(4 * RT_PLANE * sizeof(double) + 3 * RT_HBOX * sizeof(T));
+};
+struct RhsMaps {
+  CUtensorMap m[7];  // u, v, w, p, H0u, H0v, H0w
+};
+
+template <typename T>
+__global__ void __launch_bounds__(RHS_BX *RHS_BY, 3)
+k_rhs_tma(const __grid_constant__ RhsMaps maps, TGDev d, SubParams sp, int nzc) {
+  typedef RtLayout<T> L;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  auto slot_f = [&](int sl) { return reinterpret_cast<double *>(smem_raw + (size_t)sl * L::slot_bytes); };
+  auto slot_h = [&](int sl, int c) {
+    return reinterpret_cast<T *>(smem_raw + (size_t)sl * L::slot_bytes + L::field_bytes + (size_t)c * L::h0_bytes);
+  };
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + 4 * L::slot_bytes);
+  __shared__ double red[32];
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + RHS_BX * ty;
+  const int x0 = blockIdx.x * RHS_BX, j0 = 1 + blockIdx.y * RHS_BY;
+  const int kbeg = blockIdx.z * nzc;
+  const int kend = min(kbeg + nzc, nz);
+  const int i = x0 + tx, j = j0 + ty;
+  const bool active = (i < nx) && (j <= ny);
+  const bool left_edge = (x0 == 0), right_edge = (x0 + RHS_BX >= nx);
+  const int right_col = nx - x0 + 2;  // smem column of x = nx (wraps to 0)
+  if (tid == 0) {
+    for (int s = 0; s < 4; ++s) mbar_init(&bar[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  auto slot_of = [&](int k) { return (k - kbeg + 1) & 3; };
+  auto issue = [&](int k) {
+    const int sl = slot_of(k);
+    const int kz = k < 0 ? k + nz : (k >= nz ? k - nz : k);
+    mbar_expect_tx(&bar[sl], L::tx_bytes);
+    for (int f = 0; f < 4; ++f) tma_load_3d(slot_f(sl) + f * RT_PST, &maps.m[f], x0 - 2, j0 - 1, kz, &bar[sl]);
+    for (int c3 = 0; c3 < 3; ++c3) tma_load_3d(slot_h(sl, c3), &maps.m[4 + c3], x0, j0, kz, &bar[sl]);
+  };
+  uint32_t par = 0;  // parity bit per slot, packed
+  auto wait_plane = [&](int k) -> bool {
+    const int sl = slot_of(k);
+    const bool ok = mbar_wait(&bar[sl], (par >> sl) & 1u, d.err);
+    par ^= 1u << sl;
+    // periodic x patches (generic-proxy writes, fenced before the slot is reused)
+    const int kz = k < 0 ? k + nz : (k >= nz ? k - nz : k);
+    if (left_edge && tid < 40) {
+      const int f = tid / 10, r = tid - f * 10, jr = j0 - 1 + r;
+      if (jr <= ny + 1) {
+        const double *src = f == 0 ? d.u : (f == 1 ? d.v : (f == 2 ? d.w : d.p));
+        slot_f(sl)[f * RT_PST + r * RT_BXW + 1] = src[(nx - 1) + d.sy * jr + d.sz * kz];
+      }
+    }
+    if (right_edge && tid >= 64 && tid < 104) {
+      const int q = tid - 64, f = q / 10, r = q - f * 10, jr = j0 - 1 + r;
+      if (jr <= ny + 1) {
+        const double *src = f == 0 ? d.u : (f == 1 ? d.v : (f == 2 ? d.w : d.p));
+        slot_f(sl)[f * RT_PST + r * RT_BXW + right_col] = src[d.sy * jr + d.sz * kz];
+      }
+    }
+    return ok;
+  };
+  if (tid == 0) {
+    issue(kbeg - 1);
+    issue(kbeg);
+    issue(kbeg + 1);
+  }
+  bool ok = wait_plane(kbeg - 1);
+  ok = wait_plane(kbeg) && ok;
+  double part = 0.0;
+  const double dxi = d.dxi, dzi = d.dzi, dt = d.dt;
+  const double coe1 = sp.alp * d.cvisc, coe2 = sp.alp * dt;
+  const int xx = tx + 2, yy = ty + 1;
+  // per-row metric and viscous y-operator coefficients, staged once per block
+  __shared__ double ycoef[RHS_BY][16];
+  if (tid < RHS_BY * 16) {
+    const int r = tid >> 4, q = tid & 15, jr = j0 + r;
+    double v = 0.0;
+    if (jr <= ny) {
+      switch (q) {
+        case 0: v = d.wff[jr]; break;
+        case 1: v = d.wfb[jr]; break;
+        case 2: v = d.wff[jr + 1]; break;
+        case 3: v = d.wfb[jr + 1]; break;
+        case 4: v = d.dyfi[jr]; break;
+        case 5: v = d.dyci[jr]; break;
+        default:
+          if (q < 15) {
+            const int cc = (q - 6) / 3, t3 = (q - 6) % 3;
+            v = t3 == 0 ? d.apvr[cc][jr] : (t3 == 1 ? d.acvr[cc][jr] : d.amvr[cc][jr]);
+          }
+      }
+    }
+    ycoef[r][q] = v;
+  }
+  const double *yc = ycoef[ty];
+  for (int k = kbeg; k < kend; ++k) {
+    if (tid == 0 && k + 2 <= kend) {
+      fence_proxy_async();
+      issue(k + 2);
+    }
+    ok = wait_plane(k + 1) && ok;
+    __syncthreads();
+    if (active && ok) {
+      const double *Sm = slot_f(slot_of(k - 1));
+      const double *Sc = slot_f(slot_of(k));
+      const double *Sp = slot_f(slot_of(k + 1));
+      const int hc = tid;  // this cell in the 32 x 8 H0 boxes
+#define AT(base, f, dx, dy) base[(f) * RT_PST + (yy + (dy)) * RT_BXW + xx + (dx)]
+      const double u0 = AT(Sc, 0, 0, 0), uip = AT(Sc, 0, 1, 0), uim = AT(Sc, 0, -1, 0);
+      const double ujp = AT(Sc, 0, 0, 1), ujm = AT(Sc, 0, 0, -1), ukp = AT(Sp, 0, 0, 0), ukm = AT(Sm, 0, 0, 0);
+      const double uipjm = AT(Sc, 0, 1, -1), uipkm = AT(Sm, 0, 1, 0);
+      const double v0 = AT(Sc, 1, 0, 0), vim = AT(Sc, 1, -1, 0), vip = AT(Sc, 1, 1, 0), vjp = AT(Sc, 1, 0, 1);
+      const double vimjp = AT(Sc, 1, -1, 1), vjm = AT(Sc, 1, 0, -1), vkp = AT(Sp, 1, 0, 0), vkm = AT(Sm, 1, 0, 0);
+      const double vjpkm = AT(Sm, 1, 0, 1);
+      const double w0 = AT(Sc, 2, 0, 0), wim = AT(Sc, 2, -1, 0), wip = AT(Sc, 2, 1, 0), wkp = AT(Sp, 2, 0, 0);
+      const double wimkp = AT(Sp, 2, -1, 0), wkm = AT(Sm, 2, 0, 0), wjm = AT(Sc, 2, 0, -1), wjp = AT(Sc, 2, 0, 1);
+      const double wjmkp = AT(Sp, 2, 0, -1);
+      const double p0 = AT(Sc, 3, 0, 0), pim = AT(Sc, 3, -1, 0), pjm = AT(Sc, 3, 0, -1), pkm = AT(Sm, 3, 0, 0);
+#undef AT
+      const int64_t c0 = i + d.sy * j + d.sz * k;
+      {
+        const double h11 = ((uip + u0) * (uip + u0) - (uim + u0) * (uim + u0)) * (0.25 * dxi);
+        const double h12 = ((vjp + vimjp) * (yc[2] * ujp + yc[3] * u0) - (v0 + vim) * (yc[0] * u0 + yc[1] * ujm)) *
+                           (yc[4] * 0.5);
+        const double h13 = ((wkp + wimkp) * (ukp + u0) - (w0 + wim) * (u0 + ukm)) * (0.25 * dzi);
+        const double H = -(h11 + h12 + h13);
+        T *h0 = reinterpret_cast<T *>(d.h0[0]);
+        const double rhsc = sp.gam * H + sp.roh * (double)slot_h(slot_of(k), 0)[hc];
+        const double lap = (uip - 2.0 * u0 + uim) * d.dxqi + (ukp - 2.0 * u0 + ukm) * d.dzqi +
+                           (ujp * yc[6] + u0 * yc[7] + ujm * yc[8]);
+        h0[c0] = (T)H;
+        const double pgm = (p0 - pim) * dxi * coe2;
+        const double r = (rhsc + coe1 * lap) * dt - pgm;
+        reinterpret_cast<T *>(d.rhs[0])[c0] = (T)r;
+        part += r / yc[4];
+      }
+      if (j >= 2) {
+        const double h21 = ((yc[0] * uip + yc[1] * uipjm) * (vip + v0) - (yc[0] * u0 + yc[1] * ujm) * (v0 + vim)) *
+                           (dxi * 0.5);
+        const double h22 = ((vjp + v0) * (vjp + v0) - (v0 + vjm) * (v0 + vjm)) * (yc[5] * 0.25);
+        const double h23 = ((yc[0] * wkp + yc[1] * wjmkp) * (vkp + v0) - (yc[0] * w0 + yc[1] * wjm) * (v0 + vkm)) *
+                           (dzi * 0.5);
+        const double H = -(h21 + h22 + h23);
+        T *h0 = reinterpret_cast<T *>(d.h0[1]);
+        const double rhsc = sp.gam * H + sp.roh * (double)slot_h(slot_of(k), 1)[hc];
+        const double lap = (vip - 2.0 * v0 + vim) * d.dxqi + (vkp - 2.0 * v0 + vkm) * d.dzqi +
+                           (vjp * yc[9] + v0 * yc[10] + vjm * yc[11]);
+        h0[c0] = (T)H;
+        const double pgm = (p0 - pjm) * yc[5] * coe2;
+        reinterpret_cast<T *>(d.rhs[1])[c0] = (T)((rhsc + coe1 * lap) * dt - pgm);
+      }
+      {
+        const double h31 = ((uip + uipkm) * (wip + w0) - (u0 + ukm) * (w0 + wim)) * (0.25 * dxi);
+        const double h32 = ((vjp + vjpkm) * (yc[2] * wjp + yc[3] * w0) - (v0 + vkm) * (yc[0] * w0 + yc[1] * wjm)) *
+                           (yc[4] * 0.5);
+        const double h33 = ((wkp + w0) * (wkp + w0) - (w0 + wkm) * (w0 + wkm)) * (0.25 * dzi);
+        const double H = -(h31 + h32 + h33);
+        T *h0 = reinterpret_cast<T *>(d.h0[2]);
+        const double rhsc = sp.gam * H + sp.roh * (double)slot_h(slot_of(k), 2)[hc];
+        const double lap = (wip - 2.0 * w0 + wim) * d.dxqi + (wkp - 2.0 * w0 + wkm) * d.dzqi +
+                           (wjp * yc[12] + w0 * yc[13] + wjm * yc[14]);
+        h0[c0] = (T)H;
+        const double pgm = (p0 - pkm) * dzi * coe2;
+        reinterpret_cast<T *>(d.rhs[2])[c0] = (T)((rhsc + coe1 * lap) * dt - pgm);
+      }
+    }
+    __syncthreads();
+  }
+  // every issued plane has been waited for (kbeg-1 .. kend), so no bulk copy
+  // is in flight when the block exits
+  const double s = block_sum(part, red);
+  if (tid == 0) d.partials[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = s;
+}
+
 // Fixed-order reduction of the mass-flux partials; scal[0] = DPGRNS.
 __global__ void __launch_bounds__(1024) k_dpgrns(TGDev d, SubParams sp, int npart) {
   __shared__ double sh[32];
-  double s = 0.0;
-  for (int t = threadIdx.x; t < npart; t += blockDim.x) s += d.partials[t];
+  double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const int stride = blockDim.x * 8;
+  for (int t0 = threadIdx.x; t0 < npart; t0 += stride) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int t = t0 + q * blockDim.x;
+      if (t < npart) a[q] += d.partials[t];
+    }
+  }
+  double s = ((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7]));
   s = block_sum(s, sh);
   if (threadIdx.x == 0) d.scal[0] = sp.flowdrvtp == 1 ? s / d.volm : (sp.flowdrvtp == 2 ? sp.dp_const : 0.0);
 }
@@ -217,7 +422,7 @@ __device__ __forceinline__ void cyc_line(T *s, int st, int n, const double *__re
 // the mass-flux correction DPGRNS (src/RHS_CvLpGpS_tg.f90:205-211).
 template <typename T>
 __global__ void __launch_bounds__(128) k_adix(TGDev d, SubParams sp, int lb) {
-  extern __shared__ unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   T *s = reinterpret_cast<T *>(smem_raw);
   const int nx = d.nx, ny = d.ny;
   const int comp = blockIdx.z;
@@ -255,7 +460,7 @@ __global__ void __launch_bounds__(128) k_adix(TGDev d, SubParams sp, int lb) {
 constexpr int LZ = 32;
 template <typename T>
 __global__ void __launch_bounds__(128) k_adiz(TGDev d, SubParams sp) {
-  extern __shared__ unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   T *s = reinterpret_cast<T *>(smem_raw);
   const int nx = d.nx, nz = d.nz;
   const int comp = blockIdx.z;
@@ -282,6 +487,54 @@ __global__ void __launch_bounds__(128) k_adiz(TGDev d, SubParams sp) {
     const int kk = t / LZ, l = t - kk * LZ;
     if (l < nl) g[d.sz * kk + l] = s[kk * LZ + l];
   }
+}
+
+// ============================================================ x/z factors
+// MOMFA1_X_tg + MOMFA2_Z_tg (src/MOMFA_tg.f90:52-170) applied as the exact
+// inverses of their constant-coefficient cyclic tridiagonal matrices.  The
+// inverse of (1 - beta delta) on a periodic line is a symmetric circulant whose
+// first row g_m (computed on the host by solving A g = e_0 with the same
+// two-sweep algorithm) decays geometrically; it is kept up to the width W past
+// which the neglected entries sum to < 2^-60 g_0, i.e. below FP64 round-off of
+// the solution.  (Wider inverses fall back to k_adix/k_adiz.)  One pass reads
+// rhs with an (x, z) halo, applies the x then the z inverse, writes dq.
+constexpr int BZ_TX = 32, BZ_TZ = 8, BAND_WMAX = 12;
+template <typename T>
+__global__ void __launch_bounds__(BZ_TX *BZ_TZ) k_adixz_band(TGDev d, SubParams sp) {
+  __shared__ double tin[(BZ_TZ + 2 * BAND_WMAX) * (BZ_TX + 2 * BAND_WMAX)];
+  __shared__ double tmx[(BZ_TZ + 2 * BAND_WMAX) * BZ_TX];
+  const int nx = d.nx, nz = d.nz;
+  const int comp = blockIdx.z % 3, kt = blockIdx.z / 3;
+  const int j = blockIdx.y + 1;
+  if (comp == 1 && j == 1) return;
+  const int x0 = blockIdx.x * BZ_TX, k0 = kt * BZ_TZ;
+  const int wx = sp.wx, wz = sp.wz, XW = BZ_TX + 2 * wx, ZW = BZ_TZ + 2 * wz;
+  const int tid = threadIdx.x + BZ_TX * threadIdx.y;
+  const double sub = comp == 0 ? d.scal[0] : 0.0;
+  const T *src = reinterpret_cast<const T *>(d.rhs[comp]) + d.sy * j;
+  for (int t = tid; t < XW * ZW; t += BZ_TX * BZ_TZ) {
+    const int zz = t / XW, xx = t - zz * XW;
+    int x = (x0 - wx + xx) % nx, k = (k0 - wz + zz) % nz;  // tiles may exceed short lines
+    x = x < 0 ? x + nx : x;
+    k = k < 0 ? k + nz : k;
+    tin[t] = (double)src[x + d.sz * k] - sub;
+  }
+  __syncthreads();
+  const double *gx = sp.gx, *gz = sp.gz;
+  for (int t = tid; t < BZ_TX * ZW; t += BZ_TX * BZ_TZ) {
+    const int zz = t / BZ_TX, xo = t - zz * BZ_TX;
+    const double *row = tin + zz * XW + xo + wx;
+    double acc = gx[0] * row[0];
+    for (int m = 1; m <= wx; ++m) acc += gx[m] * (row[-m] + row[m]);
+    tmx[t] = acc;
+  }
+  __syncthreads();
+  const int xo = threadIdx.x, zo = threadIdx.y;
+  const double *col = tmx + (zo + wz) * BZ_TX + xo;
+  double acc = gz[0] * col[0];
+  for (int m = 1; m <= wz; ++m) acc += gz[m] * (col[-m * BZ_TX] + col[m * BZ_TX]);
+  if (x0 + xo < nx && k0 + zo < nz)
+    reinterpret_cast<T *>(d.dq[comp])[(x0 + xo) + d.sy * j + d.sz * (k0 + zo)] = (T)acc;
 }
 
 // ============================================================ y lines
@@ -332,16 +585,74 @@ __global__ void __launch_bounds__(128) k_adiy(TGDev d, SubParams sp) {
   }
 }
 
+// MOMFA3_Y_tg with the lines staged in shared memory: a block owns 32
+// consecutive i at one k; all 128 threads load the [ny][32] tile (coalesced,
+// many loads in flight), warp 0 runs the Thomas sweeps from shared memory with
+// the precomputed pivots, all threads add the increment to q.  The v line's
+// row 1 takes the u increment at j = 1 (same quirk as k_adiy).
+constexpr int AY_TL = 32;
+template <typename T>
+__global__ void __launch_bounds__(128) k_adiy_smem(TGDev d, SubParams sp, int from_dq) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  T *tile = reinterpret_cast<T *>(smem_raw);
+  const int nx = d.nx, ny = d.ny;
+  const int i0 = blockIdx.x * AY_TL, k = blockIdx.y;
+  const int tid = threadIdx.x;
+  const int nl = min(AY_TL, nx - i0);
+  const int64_t sy = d.sy;
+  const int64_t base = i0 + d.sz * k;
+  double du1 = 0.0;
+  for (int comp = 0; comp < 3; ++comp) {
+    const T *src = reinterpret_cast<const T *>(from_dq ? d.dq[comp] : d.rhs[comp]) + base;
+    for (int t = tid; t < ny * AY_TL; t += blockDim.x) {
+      const int r = t / AY_TL, l = t - r * AY_TL;
+      if (l < nl) tile[t] = src[l + sy * (r + 1)];
+    }
+    __syncthreads();
+    if (tid < nl) {
+      const double *__restrict__ a = sp.ya[comp];
+      const double *__restrict__ pp = sp.ypp[comp];
+      const double *__restrict__ h = sp.yh[comp];
+      T *col = tile + tid;
+      double g = (comp == 1 ? du1 : (double)col[0]) * pp[1];
+      col[0] = (T)g;
+      for (int jj = 2; jj <= ny; ++jj) {
+        g = ((double)col[(jj - 1) * AY_TL] - a[jj] * g) * pp[jj];
+        col[(jj - 1) * AY_TL] = (T)g;
+      }
+      double x = g;
+      for (int jj = ny - 1; jj >= 1; --jj) {
+        x = (double)col[(jj - 1) * AY_TL] - h[jj] * x;
+        col[(jj - 1) * AY_TL] = (T)x;
+      }
+      if (comp == 0) du1 = x;
+    }
+    __syncthreads();
+    double *q = (comp == 0 ? d.u : (comp == 1 ? d.v : d.w)) + base;
+    const int jlo = comp == 1 ? 2 : 1;
+    for (int t = tid; t < ny * AY_TL; t += blockDim.x) {
+      const int r = t / AY_TL, l = t - r * AY_TL;
+      if (l < nl && r + 1 >= jlo) q[l + sy * (r + 1)] += (double)tile[t];
+    }
+    if (tid < nl) {
+      q[tid] = 0.0;
+      q[tid + sy * (ny + 1)] = 0.0;
+      if (comp == 1) q[tid + sy] = 0.0;
+    }
+    __syncthreads();
+  }
+}
+
 // ============================================================ Poisson
 // DIVG_tg (src/DIVG.f90:21-57) fused with the forward real transform along x
 // of FFT99_POIS3D_periodicxz (src/possion3d_FFT99.f90:265-318): rows j of
 // plane k are packed in pairs as one complex line, transformed, separated and
 // scaled by 1/nx.  mode 0 computes the divergence (and stores RHSLLPHI);
 // mode 1 transforms the stored RHSLLPHI.
-template <typename T>
-__global__ void __launch_bounds__(256) k_fftx(TGDev d, SubParams sp, FFTPlan pl, int lb, int mode) {
+template <typename T, bool BIG>
+__global__ void __launch_bounds__(256, 2) k_fftx(TGDev d, SubParams sp, FFTPlan pl, int lb, int mode) {
   typedef typename Cplx<T>::type C;
-  extern __shared__ unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int nx = d.nx, ny = d.ny, lh = d.lh;
   const int k = blockIdx.y;
   const int jbeg = 1 + blockIdx.x * lb;
@@ -373,7 +684,7 @@ __global__ void __launch_bounds__(256) k_fftx(TGDev d, SubParams sp, FFTPlan pl,
     if (r & 1) z->y = (T)val; else z->x = (T)val;
   }
   __syncthreads();
-  C *res = fft_lines<C>(A, B, nl, nx, nx, rad, pl.nrad, (const C *)(sizeof(T) == 8 ? (const void *)pl.tw64 : (const void *)pl.tw32), -1);
+  C *res = fft_lines<C, BIG>(A, B, nl, nx, nx, rad, pl.nrad, (const C *)(sizeof(T) == 8 ? (const void *)pl.tw64 : (const void *)pl.tw32), -1);
   const T scale = (T)(1.0 / nx);
   C *S = reinterpret_cast<C *>(d.spec);
   for (int t = threadIdx.x; t < nl * lh; t += blockDim.x) {
@@ -395,10 +706,10 @@ __global__ void __launch_bounds__(256) k_fftx(TGDev d, SubParams sp, FFTPlan pl,
 // Complex transform along z for lz consecutive kx at row j
 // (src/possion3d_FFT99.f90:301-317 forward with 1/nz and the (1,1,1) mode
 // zeroed (:324-327); :448-458 inverse).
-template <typename T>
-__global__ void __launch_bounds__(256) k_fftz(TGDev d, FFTPlan pl, int lz, int sign) {
+template <typename T, bool BIG>
+__global__ void __launch_bounds__(256, 2) k_fftz(TGDev d, FFTPlan pl, int lz, int sign) {
   typedef typename Cplx<T>::type C;
-  extern __shared__ unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int nz = d.nz, ny = d.ny, lh = d.lh;
   const int j = blockIdx.y + 1;
   const int kx0 = blockIdx.x * lz;
@@ -417,7 +728,7 @@ __global__ void __launch_bounds__(256) k_fftz(TGDev d, FFTPlan pl, int lz, int s
     A[l * ld + kz] = v;
   }
   __syncthreads();
-  C *res = fft_lines<C>(A, B, lz, nz, ld, rad, pl.nrad, (const C *)(sizeof(T) == 8 ? (const void *)pl.tw64 : (const void *)pl.tw32), sign);
+  C *res = fft_lines<C, BIG>(A, B, lz, nz, ld, rad, pl.nrad, (const C *)(sizeof(T) == 8 ? (const void *)pl.tw64 : (const void *)pl.tw32), sign);
   const T scale = sign < 0 ? (T)(1.0 / nz) : (T)1;
   for (int t = threadIdx.x; t < nz * lz; t += blockDim.x) {
     const int kz = t / lz, l = t - kz * lz;
@@ -482,13 +793,75 @@ __global__ void __launch_bounds__(128) k_ysolve(TGDev d) {
   }
 }
 
+// Poisson y-tridiagonals with the lines staged in shared memory: 16
+// consecutive kx at one kz per block; the pivots h_j are kept in shared memory
+// for the back substitution.  Arithmetic as k_ysolve.
+constexpr int YS_TL = 16;
+template <typename T>
+__global__ void __launch_bounds__(128) k_ysolve_smem(TGDev d) {
+  typedef typename Cplx<T>::type C;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int lh = d.lh, ny = d.ny;
+  C *tile = reinterpret_cast<C *>(smem_raw);
+  double *hh = reinterpret_cast<double *>(smem_raw + (size_t)ny * YS_TL * sizeof(C));
+  const int kx0 = blockIdx.x * YS_TL, kz = blockIdx.y;
+  const int nl = min(YS_TL, lh - kx0);
+  const int tid = threadIdx.x;
+  C *S = reinterpret_cast<C *>(d.spec) + kx0 + (int64_t)lh * ny * kz;
+  for (int t = tid; t < ny * YS_TL; t += blockDim.x) {
+    const int r = t / YS_TL, l = t - r * YS_TL;
+    if (l < nl) tile[t] = S[l + (int64_t)lh * r];
+  }
+  __syncthreads();
+  if (tid < nl) {
+    const int kx = kx0 + tid;
+    C *col = tile + tid;
+    double *hc = hh + tid;
+    const double shift = d.ak1[kx] + d.ak3[kz];
+    const bool mean = (kx == 0 && kz == 0);
+    double b = d.acph[1] - shift;
+    double h = (mean ? 0.0 : d.apph[1]) / b;
+    C r = col[0];
+    double gr = mean ? 0.0 : (double)r.x / b;
+    double gi = mean ? 0.0 : (double)r.y / b;
+    hc[0] = h;
+    { C o; o.x = (T)gr; o.y = (T)gi; col[0] = o; }
+    for (int j = 2; j <= ny; ++j) {
+      const double a = d.amph[j];
+      b = d.acph[j] - shift;
+      const double pp = 1.0 / (b - h * a);
+      r = col[(j - 1) * YS_TL];
+      gr = ((double)r.x - a * gr) * pp;
+      gi = ((double)r.y - a * gi) * pp;
+      if (j < ny) {
+        h = d.apph[j] * pp;
+        hc[(j - 1) * YS_TL] = h;
+      }
+      C o; o.x = (T)gr; o.y = (T)gi; col[(j - 1) * YS_TL] = o;
+    }
+    double xr = gr, xi = gi;
+    for (int j = ny - 1; j >= 1; --j) {
+      const double hj = hc[(j - 1) * YS_TL];
+      r = col[(j - 1) * YS_TL];
+      xr = (double)r.x - hj * xr;
+      xi = (double)r.y - hj * xi;
+      C o; o.x = (T)xr; o.y = (T)xi; col[(j - 1) * YS_TL] = o;
+    }
+  }
+  __syncthreads();
+  for (int t = tid; t < ny * YS_TL; t += blockDim.x) {
+    const int r = t / YS_TL, l = t - r * YS_TL;
+    if (l < nl) S[l + (int64_t)lh * r] = tile[t];
+  }
+}
+
 // Inverse real transform along x (src/possion3d_FFT99.f90:461-485): pairs of
 // rows rebuilt as one complex Hermitian-extended line; phi ghosts copied
 // (BC_WALL_DPH, src/BC_WALL.f90:342-364).
-template <typename T>
-__global__ void __launch_bounds__(256) k_ifftx(TGDev d, FFTPlan pl, int lb) {
+template <typename T, bool BIG>
+__global__ void __launch_bounds__(256, 2) k_ifftx(TGDev d, FFTPlan pl, int lb) {
   typedef typename Cplx<T>::type C;
-  extern __shared__ unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int nx = d.nx, ny = d.ny, lh = d.lh;
   const int k = blockIdx.y;
   const int jbeg = 1 + blockIdx.x * lb;
@@ -516,7 +889,7 @@ __global__ void __launch_bounds__(256) k_ifftx(TGDev d, FFTPlan pl, int lb) {
     }
   }
   __syncthreads();
-  C *res = fft_lines<C>(A, B, nl, nx, nx, rad, pl.nrad, (const C *)(sizeof(T) == 8 ? (const void *)pl.tw64 : (const void *)pl.tw32), +1);
+  C *res = fft_lines<C, BIG>(A, B, nl, nx, nx, rad, pl.nrad, (const C *)(sizeof(T) == 8 ? (const void *)pl.tw64 : (const void *)pl.tw32), +1);
   for (int t = threadIdx.x; t < nrow * nx; t += blockDim.x) {
     const int r = t / nx, i = t - r * nx;
     const int j = jbeg + r;
@@ -625,6 +998,8 @@ static int fftz_lz(int nz) {
   return lz;
 }
 static size_t fftz_smem(int nz, int lz) { return (size_t)2 * lz * (nz + 1) * sizeof(double2); }
+static size_t adiy_smem(int ny) { return (size_t)ny * AY_TL * sizeof(double); }
+static size_t ysolve_smem(int ny) { return (size_t)ny * YS_TL * (sizeof(double2) + sizeof(double)); }
 static int adix_lb(int nx) {
   int lb = (int)(96 * 1024 / ((size_t)(nx + 1) * sizeof(double)));
   if (lb > 64) lb = 64;
@@ -638,18 +1013,91 @@ static size_t adiz_smem(int nz) {
   return (((size_t)nz * LZ * sizeof(double) + 15) & ~(size_t)15) + 3 * (size_t)nz * sizeof(double);
 }
 
+static size_t rhs_tma_smem() { return RtLayout<double>::smem_bytes; }
+
+// TMA descriptors of the four state fields: dims (nx, ny+2, nz) doubles,
+// box (36, 10, 1), no swizzle, out-of-bounds boxes zero filled.
+static int make_rhs_maps(chapsim_ctx *c) {
+  TGDev &d = c->d;
+  c->use_tma_rhs = false;
+  if (d.nx < RT_BXW || d.ny < 8) return CHAPSIM_OK;  // small grids use k_rhs
+  PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void **)&encode, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !encode) {
+    cudaGetLastError();
+    return CHAPSIM_OK;
+  }
+  void *f[7] = {d.u, d.v, d.w, d.p, d.h0[0], d.h0[1], d.h0[2]};
+  cuuint64_t dims[3] = {(cuuint64_t)d.nx, (cuuint64_t)(d.ny + 2), (cuuint64_t)d.nz};
+  cuuint64_t strides[2] = {(cuuint64_t)d.sy * sizeof(double), (cuuint64_t)d.sz * sizeof(double)};
+  cuuint32_t box[3] = {RT_BXW, RT_BYW, 1};
+  cuuint32_t hbox[3] = {RHS_BX, RHS_BY, 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  for (int m = 0; m < 7; ++m) {
+    CUresult r = encode(&c->rhs_maps[m], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, f[m], dims, strides, m < 4 ? box : hbox, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+      c->err = "cuTensorMapEncodeTiled failed";
+      return CHAPSIM_ERR_CUDA;
+    }
+  }
+  CK(cudaFuncSetAttribute(k_rhs_tma<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tma_smem()));
+  CK(cudaFuncSetAttribute(k_rhs_tma<double>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  c->use_tma_rhs = true;
+  return CHAPSIM_OK;
+}
+
 int init_kernels(chapsim_ctx *c) {
   const int nx = c->d.nx, nz = c->d.nz;
+  {
+    int rc = make_rhs_maps(c);
+    if (rc) return rc;
+  }
   CK(cudaFuncSetAttribute(k_adix<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adix_smem(nx, adix_lb(nx))));
   CK(cudaFuncSetAttribute(k_adiz<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adiz_smem(nz)));
-  CK(cudaFuncSetAttribute(k_fftx<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftx_smem(nx, fftx_lb(nx))));
-  CK(cudaFuncSetAttribute(k_ifftx<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftx_smem(nx, fftx_lb(nx))));
-  CK(cudaFuncSetAttribute(k_fftz<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftz_smem(nz, fftz_lz(nz))));
+  const int ny = c->d.ny;
+  c->fft_big = false;
+  for (int s2 = 0; s2 < 16; ++s2) if (c->fx.rad[s2] > 5 || c->fz.rad[s2] > 5) c->fft_big = true;
+#define FFT_ATTR(BIG)                                                                                           \
+  CK(cudaFuncSetAttribute(k_fftx<double, BIG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftx_smem(nx, fftx_lb(nx)))); \
+  CK(cudaFuncSetAttribute(k_ifftx<double, BIG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftx_smem(nx, fftx_lb(nx)))); \
+  CK(cudaFuncSetAttribute(k_fftz<double, BIG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftz_smem(nz, fftz_lz(nz))));
+  FFT_ATTR(false)
+  FFT_ATTR(true)
+#undef FFT_ATTR
+  if (adiy_smem(ny) > 200 * 1024 || ysolve_smem(ny) > 200 * 1024) {
+    c->err = "ny too large for the shared-memory y-line kernels";
+    return CHAPSIM_ERR_UNSUPPORTED;
+  }
+  CK(cudaFuncSetAttribute(k_adiy_smem<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adiy_smem(ny)));
+  CK(cudaFuncSetAttribute(k_ysolve_smem<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ysolve_smem(ny)));
+  CK(cudaFuncSetAttribute(k_adiy_smem<double>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  CK(cudaFuncSetAttribute(k_ysolve_smem<double>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   return CHAPSIM_OK;
 }
 
 static inline void phase_mark(chapsim_ctx *c, int ph) {
-  if (c->timing) cudaEventRecord(c->ev[ph], c->stream);
+  if (c->timing) cudaEventRecord(c->evpool[(size_t)c->ev_pending * (CHAPSIM_PH_COUNT + 1) + ph], c->stream);
+}
+
+// Read back every buffered substep's phase events and accumulate them.
+int flush_phase_events(chapsim_ctx *c) {
+  if (c->ev_pending == 0) return CHAPSIM_OK;
+  const size_t last = (size_t)(c->ev_pending - 1) * (CHAPSIM_PH_COUNT + 1) + CHAPSIM_PH_COUNT;
+  CK(cudaEventSynchronize(c->evpool[last]));
+  for (int s = 0; s < c->ev_pending; ++s) {
+    cudaEvent_t *e = &c->evpool[(size_t)s * (CHAPSIM_PH_COUNT + 1)];
+    for (int ph = 0; ph < CHAPSIM_PH_COUNT; ++ph) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e[ph], e[ph + 1]));
+      c->phase_ms[ph] += ms;
+    }
+  }
+  c->timed_substeps += c->ev_pending;
+  c->ev_pending = 0;
+  return CHAPSIM_OK;
 }
 
 int launch_divg(chapsim_ctx *c, int ns) {
@@ -658,7 +1106,10 @@ int launch_divg(chapsim_ctx *c, int ns) {
   TGDev &d = c->d;
   const int lb = fftx_lb(d.nx);
   dim3 grid((d.ny + lb - 1) / lb, d.nz);
-  k_fftx<double><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->sp[ns], c->fx, lb, 0);
+  if (c->fft_big)
+    k_fftx<double, true><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->sp[ns], c->fx, lb, 0);
+  else
+    k_fftx<double, false><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->sp[ns], c->fx, lb, 0);
   LAUNCHED();
   return CHAPSIM_OK;
 }
@@ -669,32 +1120,44 @@ static int poisson_from_rhs(chapsim_ctx *c, int ns, int mode) {
   phase_mark(c, CHAPSIM_PH_FFTX);
   {
     dim3 grid((d.ny + lb - 1) / lb, d.nz);
-    k_fftx<double><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->sp[ns], c->fx, lb, mode);
+    if (c->fft_big)
+      k_fftx<double, true><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->sp[ns], c->fx, lb, mode);
+    else
+      k_fftx<double, false><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->sp[ns], c->fx, lb, mode);
     LAUNCHED();
   }
   phase_mark(c, CHAPSIM_PH_FFTZ);
   const int lz = fftz_lz(d.nz);
   {
     dim3 grid((d.lh + lz - 1) / lz, d.ny);
-    k_fftz<double><<<grid, 256, fftz_smem(d.nz, lz), c->stream>>>(d, c->fz, lz, -1);
+    if (c->fft_big)
+      k_fftz<double, true><<<grid, 256, fftz_smem(d.nz, lz), c->stream>>>(d, c->fz, lz, -1);
+    else
+      k_fftz<double, false><<<grid, 256, fftz_smem(d.nz, lz), c->stream>>>(d, c->fz, lz, -1);
     LAUNCHED();
   }
   phase_mark(c, CHAPSIM_PH_YSOLVE);
   {
-    dim3 grid((d.lh + 127) / 128, d.nz);
-    k_ysolve<double><<<grid, 128, 0, c->stream>>>(d);
+    dim3 grid((d.lh + YS_TL - 1) / YS_TL, d.nz);
+    k_ysolve_smem<double><<<grid, 128, ysolve_smem(d.ny), c->stream>>>(d);
     LAUNCHED();
   }
   phase_mark(c, CHAPSIM_PH_IFFTZ);
   {
     dim3 grid((d.lh + lz - 1) / lz, d.ny);
-    k_fftz<double><<<grid, 256, fftz_smem(d.nz, lz), c->stream>>>(d, c->fz, lz, +1);
+    if (c->fft_big)
+      k_fftz<double, true><<<grid, 256, fftz_smem(d.nz, lz), c->stream>>>(d, c->fz, lz, +1);
+    else
+      k_fftz<double, false><<<grid, 256, fftz_smem(d.nz, lz), c->stream>>>(d, c->fz, lz, +1);
     LAUNCHED();
   }
   phase_mark(c, CHAPSIM_PH_IFFTX);
   {
     dim3 grid((d.ny + lb - 1) / lb, d.nz);
-    k_ifftx<double><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->fx, lb);
+    if (c->fft_big)
+      k_ifftx<double, true><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->fx, lb);
+    else
+      k_ifftx<double, false><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->fx, lb);
     LAUNCHED();
   }
   return CHAPSIM_OK;
@@ -724,29 +1187,40 @@ int launch_substep(chapsim_ctx *c, int ns) {
   phase_mark(c, CHAPSIM_PH_RHS);
   {
     dim3 grid((d.nx + RHS_BX - 1) / RHS_BX, (d.ny + RHS_BY - 1) / RHS_BY, d.nz);
-    k_rhs<double><<<grid, dim3(RHS_BX, RHS_BY), 0, c->stream>>>(d, sp);
+    if (c->use_tma_rhs) {
+      const int nzc = c->rhs_nzc;
+      grid.z = (d.nz + nzc - 1) / nzc;
+      RhsMaps maps;
+      memcpy(maps.m, c->rhs_maps, sizeof(maps.m));
+      k_rhs_tma<double><<<grid, dim3(RHS_BX, RHS_BY), rhs_tma_smem(), c->stream>>>(maps, d, sp, nzc);
+    } else {
+      k_rhs<double><<<grid, dim3(RHS_BX, RHS_BY), 0, c->stream>>>(d, sp);
+    }
     LAUNCHED();
     const int npart = grid.x * grid.y * grid.z;
     k_dpgrns<<<1, 1024, 0, c->stream>>>(d, sp, npart);
     LAUNCHED();
   }
   phase_mark(c, CHAPSIM_PH_ADIX);
-  {
+  if (sp.band) {
+    dim3 grid((d.nx + BZ_TX - 1) / BZ_TX, d.ny, 3 * ((d.nz + BZ_TZ - 1) / BZ_TZ));
+    k_adixz_band<double><<<grid, dim3(BZ_TX, BZ_TZ), 0, c->stream>>>(d, sp);
+    LAUNCHED();
+    phase_mark(c, CHAPSIM_PH_ADIZ);
+  } else {
     const int lb = adix_lb(d.nx);
     dim3 grid((d.ny + lb - 1) / lb, d.nz, 3);
     k_adix<double><<<grid, 128, adix_smem(d.nx, lb), c->stream>>>(d, sp, lb);
     LAUNCHED();
-  }
-  phase_mark(c, CHAPSIM_PH_ADIZ);
-  {
-    dim3 grid((d.nx + LZ - 1) / LZ, d.ny, 3);
-    k_adiz<double><<<grid, 128, adiz_smem(d.nz), c->stream>>>(d, sp);
+    phase_mark(c, CHAPSIM_PH_ADIZ);
+    dim3 grid2((d.nx + LZ - 1) / LZ, d.ny, 3);
+    k_adiz<double><<<grid2, 128, adiz_smem(d.nz), c->stream>>>(d, sp);
     LAUNCHED();
   }
   phase_mark(c, CHAPSIM_PH_ADIY);
   {
-    dim3 grid((d.nx + 127) / 128, d.nz);
-    k_adiy<double><<<grid, 128, 0, c->stream>>>(d, sp);
+    dim3 grid((d.nx + AY_TL - 1) / AY_TL, d.nz);
+    k_adiy_smem<double><<<grid, 128, adiy_smem(d.ny), c->stream>>>(d, sp, sp.band);
     LAUNCHED();
   }
   int rc = poisson_from_rhs(c, ns, 0);
@@ -755,14 +1229,8 @@ int launch_substep(chapsim_ctx *c, int ns) {
   rc = launch_correction(c, ns);
   if (rc) return rc;
   if (c->timing) {
-    cudaEventRecord(c->ev[CHAPSIM_PH_COUNT], c->stream);
-    CK(cudaEventSynchronize(c->ev[CHAPSIM_PH_COUNT]));
-    for (int ph = 0; ph < CHAPSIM_PH_COUNT; ++ph) {
-      float ms = 0.f;
-      CK(cudaEventElapsedTime(&ms, c->ev[ph], c->ev[ph + 1]));
-      c->phase_ms[ph] += ms;
-    }
-    c->timed_substeps++;
+    phase_mark(c, CHAPSIM_PH_COUNT);
+    if (++c->ev_pending == chapsim_ctx::kEvSub) return flush_phase_events(c);
   }
   return CHAPSIM_OK;
 }

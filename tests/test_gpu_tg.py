@@ -188,3 +188,22 @@ def test_nan_scan_and_divmax():
     s.set_field("u", u)
     assert s.nan_count() == 1
     assert math.isinf(s.divgck_tg())
+
+
+def test_adi_fallback_wide_inverse():
+    # Re = 1, dt = 0.05: the x/z inverses are too wide for the banded kernel,
+    # so the shared-memory cyclic Thomas kernels run instead
+    g, o = pair(32, 24, 16, ren=1.0, dt=0.05)
+    for ns in (0, 1):
+        g.solverrk3_mom_tg(ns)
+        o.substep(ns)
+    compare(g, o, tag="fallback")
+
+
+def test_short_lines_wrap():
+    # nx, nz shorter than a 32 x 8 tile plus its halo
+    g, o = pair(8, 8, 8, lx=1.0, lz=0.5)
+    for ns in (0, 1, 2, 3):
+        g.solverrk3_mom_tg(ns)
+        o.substep(ns)
+    compare(g, o, tag="short")
