@@ -291,6 +291,62 @@ static int build_tables(chapsim_ctx *ctx) {
     cyc_tables(nx, xa[ns], &H[o_x[ns][0]], &H[o_x[ns][1]], &H[o_x[ns][2]], xb[ns], xqq[ns]);
     cyc_tables(nz, za[ns], &H[o_z[ns][0]], &H[o_z[ns][1]], &H[o_z[ns][2]], zb[ns], zqq[ns]);
   }
+  // banded inverses of the y factors: (A^{-1})_{j, j+m}, |m| <= wy
+  const int YW = 16;  // AYB_WMAX in tg_kernels.cu
+  size_t o_yg[4][3];
+  int wy[4];
+  for (int ns = 0; ns < 4; ++ns) {
+    wy[ns] = 0;
+    std::vector<std::vector<double>> inv(3);
+    for (int c = 0; c < 3; ++c) {
+      const double *ya = &H[o_ya[ns][c]], *ypp = &H[o_ypp[ns][c]], *yh = &H[o_yh[ns][c]];
+      std::vector<double> &A = inv[c];
+      A.assign((size_t)(ny + 1) * (ny + 1), 0.0);  // A[j*(ny+1)+col], 1-based
+      std::vector<double> x(ny + 2);
+      for (int col = 1; col <= ny; ++col) {
+        // Thomas on e_col with the precomputed pivots (same sweeps as the device)
+        double g = (col == 1 ? 1.0 : 0.0) * ypp[1];
+        x[1] = g;
+        for (int j = 2; j <= ny; ++j) { g = ((j == col ? 1.0 : 0.0) - ya[j] * g) * ypp[j]; x[j] = g; }
+        double xv = g;
+        for (int j = ny - 1; j >= 1; --j) { xv = x[j] - yh[j] * xv; x[j] = xv; }
+        for (int j = 1; j <= ny; ++j) A[(size_t)j * (ny + 1) + col] = x[j];
+      }
+      std::vector<double> dm(ny + 1);
+      for (int j = 1; j <= ny; ++j) {
+        double rmax = 0.0;
+        for (int col = 1; col <= ny; ++col) rmax = fmax(rmax, fabs(A[(size_t)j * (ny + 1) + col]));
+        const double tol = ldexp(rmax, -60);
+        // dm[m] = |A(j, j+m)| + |A(j, j-m)|; smallest w whose tail sum is below tol
+        for (int m = 0; m <= ny; ++m) {
+          double v = 0.0;
+          if (j + m <= ny) v += fabs(A[(size_t)j * (ny + 1) + j + m]);
+          if (m > 0 && j - m >= 1) v += fabs(A[(size_t)j * (ny + 1) + j - m]);
+          dm[m] = v;
+        }
+        double tail = 0.0;
+        int w = ny;
+        for (int m = ny; m >= 1; --m) {
+          tail += dm[m];
+          if (tail > tol) break;
+          w = m - 1;
+        }
+        wy[ns] = w > wy[ns] ? w : wy[ns];
+      }
+    }
+    if (wy[ns] > YW) wy[ns] = -1;
+    for (int c = 0; c < 3; ++c) {
+      o_yg[ns][c] = alloc((size_t)(ny + 1) * (2 * YW + 1));
+      if (wy[ns] < 0) continue;
+      const std::vector<double> &A = inv[c];
+      for (int j = 1; j <= ny; ++j)
+        for (int m = -wy[ns]; m <= wy[ns]; ++m) {
+          const int col = j + m;
+          if (col >= 1 && col <= ny)
+            H[o_yg[ns][c] + (size_t)j * (2 * YW + 1) + YW + m] = A[(size_t)j * (ny + 1) + col];
+        }
+    }
+  }
   // truncated circulant inverses of the x and z factors
   size_t o_gx[4], o_gz[4];
   int wx[4], wz[4];
@@ -360,6 +416,8 @@ static int build_tables(chapsim_ctx *ctx) {
     sp.wx = wx[ns];
     sp.wz = wz[ns];
     sp.band = (wx[ns] >= 0 && wz[ns] >= 0 && ctx->allow_band) ? 1 : 0;
+    for (int c = 0; c < 3; ++c) sp.yg[c] = D + o_yg[ns][c];
+    sp.wy = ctx->allow_band ? wy[ns] : -1;
   }
   ctx->fx.tw64 = reinterpret_cast<const double2 *>(D + o_twx);
   ctx->fz.tw64 = reinterpret_cast<const double2 *>(D + o_twz);

@@ -56,6 +56,9 @@ struct SubParams {
   const double *gx, *gz;
   int wx, wz;
   int band;  // 1: x/z factors applied by k_adixz_band
+  // banded inverses of the y factors: yg[c][j*(2*16+1) + 16 + m], m in [-wy, wy]
+  const double *yg[3];
+  int wy;     // -1: too wide, the Thomas kernel runs
 };
 
 struct FFTPlan {

@@ -498,43 +498,144 @@ __global__ void __launch_bounds__(128) k_adiz(TGDev d, SubParams sp) {
 // which the neglected entries sum to < 2^-60 g_0, i.e. below FP64 round-off of
 // the solution.  (Wider inverses fall back to k_adix/k_adiz.)  One pass reads
 // rhs with an (x, z) halo, applies the x then the z inverse, writes dq.
-constexpr int BZ_TX = 32, BZ_TZ = 8, BAND_WMAX = 12;
+constexpr int BAND_WMAX = 12;
+// z-marching form: a block owns a 32 (x) by 8 (j) tile and a segment of z
+// planes.  Each rhs plane of the tile (with its periodic x halo) is loaded
+// once (the next plane is prefetched into registers while the current one is
+// processed), the x inverse is applied into a ring of 2*wz+1 x-solved planes
+// in shared memory, and the z inverse over the ring gives the output plane
+// k - wz.
+constexpr int BM_TX = 32, BM_TY = 8, BM_SEG = 32;
 template <typename T>
-__global__ void __launch_bounds__(BZ_TX *BZ_TZ) k_adixz_band(TGDev d, SubParams sp) {
-  __shared__ double tin[(BZ_TZ + 2 * BAND_WMAX) * (BZ_TX + 2 * BAND_WMAX)];
-  __shared__ double tmx[(BZ_TZ + 2 * BAND_WMAX) * BZ_TX];
-  const int nx = d.nx, nz = d.nz;
-  const int comp = blockIdx.z % 3, kt = blockIdx.z / 3;
-  const int j = blockIdx.y + 1;
-  if (comp == 1 && j == 1) return;
-  const int x0 = blockIdx.x * BZ_TX, k0 = kt * BZ_TZ;
-  const int wx = sp.wx, wz = sp.wz, XW = BZ_TX + 2 * wx, ZW = BZ_TZ + 2 * wz;
-  const int tid = threadIdx.x + BZ_TX * threadIdx.y;
+__global__ void __launch_bounds__(BM_TX *BM_TY) k_adixz_band(TGDev d, SubParams sp) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int wx = sp.wx, wz = sp.wz, RS = 2 * wz + 1, XW = BM_TX + 2 * wx;
+  double *ring = reinterpret_cast<double *>(smem_raw);          // [RS][8][32]
+  double *tin = ring + RS * BM_TY * BM_TX;                      // [8][XW]
+  __shared__ double gxs[BAND_WMAX + 1], gzs[BAND_WMAX + 1];
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  const int nseg = (nz + BM_SEG - 1) / BM_SEG;
+  const int comp = blockIdx.z % 3, seg = blockIdx.z / 3;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int x0 = blockIdx.x * BM_TX, j = 1 + blockIdx.y * BM_TY + ty;
+  const int kb = seg * BM_SEG, ke = min(kb + BM_SEG, nz);
+  (void)nseg;
+  if (ty == 0 && tx <= BAND_WMAX) {
+    gxs[tx] = tx <= wx ? sp.gx[tx] : 0.0;
+    gzs[tx] = tx <= wz ? sp.gz[tx] : 0.0;
+  }
+  const bool row_ok = (j <= ny) && !(comp == 1 && j == 1);
   const double sub = comp == 0 ? d.scal[0] : 0.0;
-  const T *src = reinterpret_cast<const T *>(d.rhs[comp]) + d.sy * j;
-  for (int t = tid; t < XW * ZW; t += BZ_TX * BZ_TZ) {
-    const int zz = t / XW, xx = t - zz * XW;
-    int x = (x0 - wx + xx) % nx, k = (k0 - wz + zz) % nz;  // tiles may exceed short lines
-    x = x < 0 ? x + nx : x;
-    k = k < 0 ? k + nz : k;
-    tin[t] = (double)src[x + d.sz * k] - sub;
+  const T *src = reinterpret_cast<const T *>(d.rhs[comp]) + d.sy * (row_ok ? j : 1);
+  // this thread's input columns: x0 - wx + tx and x0 - wx + tx + 32 (if < XW)
+  int xa = (x0 - wx + tx) % nx;
+  xa = xa < 0 ? xa + nx : xa;
+  const bool has_b = tx + BM_TX < XW;
+  int xb = (x0 - wx + tx + BM_TX) % nx;
+  xb = xb < 0 ? xb + nx : xb;
+  auto zwrap = [&](int k) { k %= nz; return k < 0 ? k + nz : k; };
+  const int pbeg = kb - wz, pend = ke + wz;  // planes [pbeg, pend)
+  double na = 0.0, nb = 0.0;
+  if (row_ok) {
+    const T *r = src + d.sz * (int64_t)zwrap(pbeg);
+    na = (double)r[xa] - sub;
+    if (has_b) nb = (double)r[xb] - sub;
   }
-  __syncthreads();
-  const double *gx = sp.gx, *gz = sp.gz;
-  for (int t = tid; t < BZ_TX * ZW; t += BZ_TX * BZ_TZ) {
-    const int zz = t / BZ_TX, xo = t - zz * BZ_TX;
-    const double *row = tin + zz * XW + xo + wx;
-    double acc = gx[0] * row[0];
-    for (int m = 1; m <= wx; ++m) acc += gx[m] * (row[-m] + row[m]);
-    tmx[t] = acc;
+  const int i = x0 + tx;
+  T *dst = reinterpret_cast<T *>(d.dq[comp]) + d.sy * j + i;
+  const int tid = tx + BM_TX * ty;
+  int slot = 0;  // ring slot of plane p (planes are stored in order, modulo RS)
+  for (int p = pbeg; p < pend; ++p) {
+    // publish the prefetched plane p, prefetch plane p + 1
+    tin[ty * XW + tx] = na;
+    if (has_b) tin[ty * XW + tx + BM_TX] = nb;
+    if (row_ok && p + 1 < pend) {
+      const T *r = src + d.sz * (int64_t)zwrap(p + 1);
+      na = (double)r[xa] - sub;
+      if (has_b) nb = (double)r[xb] - sub;
+    }
+    __syncthreads();
+    {
+      const double *rr = tin + ty * XW + tx + wx;
+      double acc = gxs[0] * rr[0];
+      for (int m = 1; m <= wx; ++m) acc += gxs[m] * (rr[-m] + rr[m]);
+      ring[slot * (BM_TY * BM_TX) + tid] = acc;
+    }
+    __syncthreads();
+    const int k = p - wz;  // output plane once its whole z window is in the ring
+    if (k >= kb) {
+      // planes k - wz .. k + wz = p - 2wz .. p sit in slots slot+1 .. slot (mod RS)
+      int sl = slot + 1 == RS ? 0 : slot + 1;
+      double acc = 0.0;
+      for (int q = -wz; q <= wz; ++q) {
+        acc += gzs[q < 0 ? -q : q] * ring[sl * (BM_TY * BM_TX) + tid];
+        sl = sl + 1 == RS ? 0 : sl + 1;
+      }
+      if (row_ok && i < nx) dst[d.sz * (int64_t)k] = (T)acc;
+    }
+    slot = slot + 1 == RS ? 0 : slot + 1;
   }
-  __syncthreads();
-  const int xo = threadIdx.x, zo = threadIdx.y;
-  const double *col = tmx + (zo + wz) * BZ_TX + xo;
-  double acc = gz[0] * col[0];
-  for (int m = 1; m <= wz; ++m) acc += gz[m] * (col[-m * BZ_TX] + col[m * BZ_TX]);
-  if (x0 + xo < nx && k0 + zo < nz)
-    reinterpret_cast<T *>(d.dq[comp])[(x0 + xo) + d.sy * j + d.sz * (k0 + zo)] = (T)acc;
+}
+static size_t band_smem(int wx, int wz) {
+  return ((size_t)(2 * wz + 1) * BM_TY * BM_TX + (size_t)BM_TY * (BM_TX + 2 * wx)) * sizeof(double);
+}
+
+// MOMFA3_Y_tg (src/MOMFA_tg.f90:173-240) applied as the banded part of the
+// exact inverse of each component's y tridiagonal matrix (rows j = 1..ny),
+// G[j][m] = (A^{-1})_{j, j+m} for |m| <= WY, precomputed on the host from
+// the Thomas sweeps and truncated where the dropped entries of every row sum
+// to < 2^-60 of its largest entry.  Then q += dq and BC_WALL_Q_tg.  A block
+// owns 32 x-columns, AY_JT rows and one z plane; rows outside [1, ny] carry
+// zero weight.  The v line's row-1 right-hand side is the final u increment
+// at j = 1 (reference quirk, see k_adiy), computed here from the u data.
+constexpr int AY_JT = 32, AY_TX = 32, AY_TY = 8, AYB_WMAX = 16;
+template <typename T>
+__global__ void __launch_bounds__(AY_TX *AY_TY) k_adiy_band(TGDev d, SubParams sp) {
+  __shared__ double tile[(AY_JT + 2 * AYB_WMAX) * AY_TX];
+  __shared__ double du1[AY_TX];
+  const int nx = d.nx, ny = d.ny;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int x0 = blockIdx.x * AY_TX, j0 = 1 + blockIdx.y * AY_JT, k = blockIdx.z;
+  const int i = x0 + tx;
+  const bool col_ok = i < nx;
+  const int64_t base = (int64_t)i + d.sz * k;
+  const int W = sp.wy;
+  const int nrow = AY_JT + 2 * W;  // tile rows j0-W .. j0+AY_JT-1+W
+  for (int comp = 0; comp < 3; ++comp) {
+    const T *src = reinterpret_cast<const T *>(d.dq[comp]);
+    for (int r = ty; r < nrow; r += AY_TY) {
+      const int j = j0 - W + r;
+      double v = 0.0;
+      if (col_ok && j >= 1 && j <= ny) v = (double)src[base + d.sy * j];
+      tile[r * AY_TX + tx] = v;
+    }
+    if (comp == 1 && j0 == 1) {
+      __syncthreads();
+      if (ty == 0) tile[(1 - j0 + W) * AY_TX + tx] = du1[tx];  // row j = 1 of v <- u increment
+    }
+    __syncthreads();
+    const double *G = sp.yg[comp];
+    double *q = comp == 0 ? d.u : (comp == 1 ? d.v : d.w);
+    const int jlo = comp == 1 ? 2 : 1;
+    for (int jr = ty; jr < AY_JT; jr += AY_TY) {
+      const int j = j0 + jr;
+      if (j > ny) break;
+      const double *g = G + (size_t)j * (2 * AYB_WMAX + 1) + AYB_WMAX;  // g[m], m in [-W, W]
+      const double *t = tile + (jr + W) * AY_TX + tx;
+      double acc = g[0] * t[0];
+      for (int m = 1; m <= W; ++m) acc += g[-m] * t[-m * AY_TX] + g[m] * t[m * AY_TX];
+      if (comp == 0 && j == 1) du1[tx] = acc;
+      if (col_ok && j >= jlo) q[base + d.sy * j] += acc;
+    }
+    if (col_ok && ty == 0) {
+      if (j0 == 1) {
+        q[base] = 0.0;
+        if (comp == 1) q[base + d.sy] = 0.0;
+      }
+      if (j0 + AY_JT > ny) q[base + d.sy * (ny + 1)] = 0.0;
+    }
+    __syncthreads();
+  }
 }
 
 // ============================================================ y lines
@@ -1072,6 +1173,8 @@ int init_kernels(chapsim_ctx *c) {
     return CHAPSIM_ERR_UNSUPPORTED;
   }
   CK(cudaFuncSetAttribute(k_adiy_smem<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adiy_smem(ny)));
+  CK(cudaFuncSetAttribute(k_adixz_band<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)band_smem(BAND_WMAX, BAND_WMAX)));
   CK(cudaFuncSetAttribute(k_ysolve_smem<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ysolve_smem(ny)));
   CK(cudaFuncSetAttribute(k_adiy_smem<double>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   CK(cudaFuncSetAttribute(k_ysolve_smem<double>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
@@ -1203,8 +1306,8 @@ int launch_substep(chapsim_ctx *c, int ns) {
   }
   phase_mark(c, CHAPSIM_PH_ADIX);
   if (sp.band) {
-    dim3 grid((d.nx + BZ_TX - 1) / BZ_TX, d.ny, 3 * ((d.nz + BZ_TZ - 1) / BZ_TZ));
-    k_adixz_band<double><<<grid, dim3(BZ_TX, BZ_TZ), 0, c->stream>>>(d, sp);
+    dim3 grid((d.nx + BM_TX - 1) / BM_TX, (d.ny + BM_TY - 1) / BM_TY, 3 * ((d.nz + BM_SEG - 1) / BM_SEG));
+    k_adixz_band<double><<<grid, dim3(BM_TX, BM_TY), band_smem(sp.wx, sp.wz), c->stream>>>(d, sp);
     LAUNCHED();
     phase_mark(c, CHAPSIM_PH_ADIZ);
   } else {
@@ -1218,7 +1321,11 @@ int launch_substep(chapsim_ctx *c, int ns) {
     LAUNCHED();
   }
   phase_mark(c, CHAPSIM_PH_ADIY);
-  {
+  if (sp.band && sp.wy >= 0) {
+    dim3 grid((d.nx + AY_TX - 1) / AY_TX, (d.ny + AY_JT - 1) / AY_JT, d.nz);
+    k_adiy_band<double><<<grid, dim3(AY_TX, AY_TY), 0, c->stream>>>(d, sp);
+    LAUNCHED();
+  } else {
     dim3 grid((d.nx + AY_TL - 1) / AY_TL, d.nz);
     k_adiy_smem<double><<<grid, 128, adiy_smem(d.ny), c->stream>>>(d, sp, sp.band);
     LAUNCHED();
