@@ -452,10 +452,6 @@ int chapsim_create(const chapsim_config *cfg, chapsim_ctx **out) {
     delete ctx;
     return CHAPSIM_ERR_UNSUPPORTED;  // lengths with prime factors > 11
   }
-  if (cfg->precision == CHAPSIM_MIXED) {
-    delete ctx;
-    return CHAPSIM_ERR_UNSUPPORTED;
-  }
   if (cudaSetDevice(ctx->device) != cudaSuccess) { delete ctx; return CHAPSIM_ERR_CUDA; }
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete ctx;
@@ -473,27 +469,28 @@ int chapsim_create(const chapsim_config *cfg, chapsim_ctx **out) {
   d.sz = (int64_t)cfg->nx * (cfg->ny + 2);
   const size_t n = (size_t)d.sz * cfg->nz;
   void *p = nullptr;
-  double **f64[] = {&d.u, &d.v, &d.w, &d.p, &d.phi, &d.rhsphi, &d.h0[0], &d.h0[1], &d.h0[2]};
-  for (double **f : f64) {
-    if ((rc = dalloc(ctx, &p, n * sizeof(double)))) goto fail;
-    *f = (double *)p;
-    cudaMemsetAsync(p, 0, n * sizeof(double), ctx->stream);
-  }
-  for (int c = 0; c < 3; ++c) {
-    if ((rc = dalloc(ctx, &p, n * sizeof(double)))) goto fail;
-    d.rhs[c] = p;
-    cudaMemsetAsync(p, 0, n * sizeof(double), ctx->stream);
-    if ((rc = dalloc(ctx, &p, n * sizeof(double)))) goto fail;
-    d.dq[c] = p;
-    cudaMemsetAsync(p, 0, n * sizeof(double), ctx->stream);
-  }
   {
+    const bool mixed = cfg->precision == CHAPSIM_MIXED;
+    const size_t tsz = mixed ? sizeof(float) : sizeof(double);
+    double **f64[] = {&d.u, &d.v, &d.w, &d.p, &d.phi, &d.rhsphi, &d.res};
+    for (double **f : f64) {
+      if ((rc = dalloc(ctx, &p, n * sizeof(double)))) goto fail;
+      *f = (double *)p;
+      cudaMemsetAsync(p, 0, n * sizeof(double), ctx->stream);
+    }
+    for (int c = 0; c < 3; ++c) {
+      void **tmp[] = {&d.h0[c], &d.rhs[c], &d.dq[c]};
+      for (void **f : tmp) {
+        if ((rc = dalloc(ctx, &p, n * tsz))) goto fail;
+        *f = p;
+        cudaMemsetAsync(p, 0, n * tsz, ctx->stream);
+      }
+    }
     const size_t ns = (size_t)d.lh * cfg->ny * cfg->nz;
-    if ((rc = dalloc(ctx, &p, ns * sizeof(double2)))) goto fail;
+    if ((rc = dalloc(ctx, &p, ns * (mixed ? sizeof(float2) : sizeof(double2))))) goto fail;
     d.spec = p;
-    if ((rc = dalloc(ctx, &p, ns * sizeof(double)))) goto fail;
-    d.ysc = (double *)p;
-    d.spec64 = nullptr;
+    if ((rc = dalloc(ctx, &p, ns * sizeof(double2)))) goto fail;
+    d.ypiv = (double2 *)p;
   }
   {
     // block partials: one per 32x8 tile of the (x, y) plane per z plane
@@ -566,9 +563,9 @@ static double *field_ptr(chapsim_ctx *ctx, int domain, int field) {
     case CHAPSIM_F_P: return d.p;
     case CHAPSIM_F_PHI: return d.phi;
     case CHAPSIM_F_RHSPHI: return d.rhsphi;
-    case CHAPSIM_F_H0U: return d.h0[0];
-    case CHAPSIM_F_H0V: return d.h0[1];
-    case CHAPSIM_F_H0W: return d.h0[2];
+    case CHAPSIM_F_H0U: return (double *)d.h0[0];
+    case CHAPSIM_F_H0V: return (double *)d.h0[1];
+    case CHAPSIM_F_H0W: return (double *)d.h0[2];
   }
   return nullptr;
 }
@@ -582,6 +579,24 @@ static int xfer(chapsim_ctx *ctx, int domain, int field, void *dst_or_src, int64
   REQUIRE(n == chapsim_field_len(ctx), CHAPSIM_ERR_ARG, "field length mismatch");
   CKC(cudaSetDevice(ctx->device));
   const size_t bytes = (size_t)n * sizeof(double);
+  const bool h0f = field >= CHAPSIM_F_H0U && field <= CHAPSIM_F_H0W;
+  if (h0f && ctx->cfg.precision == CHAPSIM_MIXED) {
+    // CONVH0 is held in FP32 in the mixed form: convert through the host
+    REQUIRE(kind != cudaMemcpyDeviceToDevice, CHAPSIM_ERR_UNSUPPORTED, "device copies of FP32 H0 fields");
+    std::vector<float> tmp((size_t)n);
+    if (to_dev) {
+      const double *src = (const double *)dst_or_src;
+      for (int64_t t = 0; t < n; ++t) tmp[t] = (float)src[t];
+      CKC(cudaMemcpyAsync(f, tmp.data(), (size_t)n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+      CKC(cudaStreamSynchronize(ctx->stream));
+    } else {
+      CKC(cudaMemcpyAsync(tmp.data(), f, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+      CKC(cudaStreamSynchronize(ctx->stream));
+      double *dst = (double *)dst_or_src;
+      for (int64_t t = 0; t < n; ++t) dst[t] = (double)tmp[t];
+    }
+    return CHAPSIM_OK;
+  }
   if (to_dev)
     CKC(cudaMemcpyAsync(f, dst_or_src, bytes, kind, ctx->stream));
   else
@@ -669,7 +684,8 @@ int chapsim_init_random(chapsim_ctx *ctx, uint64_t seed, double amp, int project
   TGDev &d = ctx->d;
   const size_t bytes = (size_t)n * sizeof(double);
   CKC(cudaMemsetAsync(d.p, 0, bytes, ctx->stream));
-  for (int c = 0; c < 3; ++c) CKC(cudaMemsetAsync(d.h0[c], 0, bytes, ctx->stream));
+  const size_t tbytes = (size_t)n * (ctx->cfg.precision == CHAPSIM_MIXED ? sizeof(float) : sizeof(double));
+  for (int c = 0; c < 3; ++c) CKC(cudaMemsetAsync(d.h0[c], 0, tbytes, ctx->stream));
   if (project) {
     rc = launch_substep(ctx, 0);  // CALC_INITIALIZATION_tg: SOLVERRK3_MOM_tg(0)
     if (rc) return rc;

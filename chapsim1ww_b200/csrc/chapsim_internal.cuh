@@ -21,13 +21,13 @@ struct TGDev {
   int64_t sy, sz;  // strides of j and k in a field
   // FP64 state
   double *u, *v, *w, *p, *phi, *rhsphi;
-  double *h0[3];
+  void *h0[3];      // CONVH0 (temporary precision)
   // temporaries (double in the FP64 form, float in the mixed form)
   void *rhs[3];
   void *dq[3];      // x/z-solved increments (banded-inverse path)
   void *spec;       // complex spectral array
-  double *ysc;      // Poisson y-solve scratch (h_j), lh*ny*nz
-  double2 *spec64;  // FP64 spectral scratch for the refinement sweep (mixed)
+  double2 *ypiv;    // Poisson y-line pivots {pp_j, h_j} per (kx, j, kz)
+  double *res;      // FP64 Poisson residual (refinement sweep of the mixed form)
   double *partials; // per-block mass-flux partial sums
   double *scal;     // device scalars: [0] dpgrns, [1..] reduction outputs
   int *err;         // device error word (bounded waits that gave up)
@@ -105,6 +105,7 @@ struct chapsim_ctx {
   bool use_tma_rhs = false;
   bool allow_band = true;   // banded x/z inverses when narrow enough
   bool fft_big = false;     // FFT plans with radix 7 or 11
+  bool refine = true;       // mixed form: one FP64-residual refinement sweep
   int rhs_nzc = 16;
   // CUDA graph of one full step (NS = 1, 2, 3)
   cudaGraphExec_t step_graph = nullptr;

@@ -130,11 +130,11 @@ k_rhs(TGDev d, SubParams sp) {
                          (dyfi * 0.5);
       const double h13 = ((wkp + wimkp) * (ukp + u0) - (w0 + wim) * (u0 + ukm)) * (0.25 * dzi);
       const double H = -(h11 + h12 + h13);
-      double *h0 = d.h0[0];
-      const double rhsc = sp.gam * H + sp.roh * h0[c0];
+      T *h0 = reinterpret_cast<T *>(d.h0[0]);
+      const double rhsc = sp.gam * H + sp.roh * (double)h0[c0];
       const double lap = (uip - 2.0 * u0 + uim) * d.dxqi + (ukp - 2.0 * u0 + ukm) * d.dzqi +
                          (ujp * d.apvr[0][j] + u0 * d.acvr[0][j] + ujm * d.amvr[0][j]);
-      h0[c0] = H;
+      h0[c0] = (T)H;
       const double pgm = (P[c0] - P[cim]) * dxi * coe2;
       const double r = (rhsc + coe1 * lap) * d.dt - pgm;
       reinterpret_cast<T *>(d.rhs[0])[c0] = (T)r;
@@ -148,11 +148,11 @@ k_rhs(TGDev d, SubParams sp) {
       const double h23 = ((wffj * wkp + wfbj * wjmkp) * (vkp + v0) - (wffj * w0 + wfbj * wjm) * (v0 + vkm)) *
                          (dzi * 0.5);
       const double H = -(h21 + h22 + h23);
-      double *h0 = d.h0[1];
-      const double rhsc = sp.gam * H + sp.roh * h0[c0];
+      T *h0 = reinterpret_cast<T *>(d.h0[1]);
+      const double rhsc = sp.gam * H + sp.roh * (double)h0[c0];
       const double lap = (vip - 2.0 * v0 + vim) * d.dxqi + (vkp - 2.0 * v0 + vkm) * d.dzqi +
                          (vjp * d.apvr[1][j] + v0 * d.acvr[1][j] + vjm * d.amvr[1][j]);
-      h0[c0] = H;
+      h0[c0] = (T)H;
       const double pgm = (P[c0] - P[c0 - sy]) * d.dyci[j] * coe2;
       reinterpret_cast<T *>(d.rhs[1])[c0] = (T)((rhsc + coe1 * lap) * d.dt - pgm);
     }
@@ -163,11 +163,11 @@ k_rhs(TGDev d, SubParams sp) {
                          (dyfi * 0.5);
       const double h33 = ((wkp + w0) * (wkp + w0) - (w0 + wkm) * (w0 + wkm)) * (0.25 * dzi);
       const double H = -(h31 + h32 + h33);
-      double *h0 = d.h0[2];
-      const double rhsc = sp.gam * H + sp.roh * h0[c0];
+      T *h0 = reinterpret_cast<T *>(d.h0[2]);
+      const double rhsc = sp.gam * H + sp.roh * (double)h0[c0];
       const double lap = (wip - 2.0 * w0 + wim) * d.dxqi + (wkp - 2.0 * w0 + wkm) * d.dzqi +
                          (wjp * d.apvr[2][j] + w0 * d.acvr[2][j] + wjm * d.amvr[2][j]);
-      h0[c0] = H;
+      h0[c0] = (T)H;
       const double pgm = (P[c0] - P[ckm]) * dzi * coe2;
       reinterpret_cast<T *>(d.rhs[2])[c0] = (T)((rhsc + coe1 * lap) * d.dt - pgm);
     }
@@ -587,7 +587,8 @@ static size_t band_smem(int wx, int wz) {
 // to < 2^-60 of its largest entry.  Then q += dq and BC_WALL_Q_tg.  A block
 // owns 32 x-columns, AY_JT rows and one z plane; rows outside [1, ny] carry
 // zero weight.  The v line's row-1 right-hand side is the final u increment
-// at j = 1 (reference quirk, see k_adiy), computed here from the u data.
+// at j = 1 (the reference quirk described at k_adiy_smem), computed here from
+// the u data.
 constexpr int AY_JT = 32, AY_TX = 32, AY_TY = 8, AYB_WMAX = 16;
 template <typename T>
 __global__ void __launch_bounds__(AY_TX *AY_TY) k_adiy_band(TGDev d, SubParams sp) {
@@ -639,58 +640,13 @@ __global__ void __launch_bounds__(AY_TX *AY_TY) k_adiy_band(TGDev d, SubParams s
 }
 
 // ============================================================ y lines
-// MOMFA3_Y_tg (src/MOMFA_tg.f90:173-240) with TDMAIJJ_nonCYC
-// (src/TDMAIJJ_nonCYC.f90:67-120), q += dq (src/MOMFA_tg.f90:38-44) and
-// BC_WALL_Q_tg.  One thread per (i, k) line handles u, v, w in turn; the v
-// line's row 1 right-hand side is the u increment at j = 1, as in the
-// reference, whose RHS_tg row 1 is not rebuilt for IDR = 2.  Pivots depend
-// only on (NS, IDR, j) and are precomputed; the forward-swept g is kept in the
-// rhs array in place.
-template <typename T>
-__global__ void __launch_bounds__(128) k_adiy(TGDev d, SubParams sp) {
-  const int nx = d.nx, ny = d.ny;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = blockIdx.y;
-  if (i >= nx) return;
-  const int64_t sy = d.sy;
-  const int64_t base = i + d.sz * k;
-  double du1 = 0.0;
-#pragma unroll 1
-  for (int comp = 0; comp < 3; ++comp) {
-    T *r = reinterpret_cast<T *>(d.rhs[comp]) + base;
-    double *q = comp == 0 ? d.u : (comp == 1 ? d.v : d.w);
-    q += base;
-    const double *__restrict__ a = sp.ya[comp];
-    const double *__restrict__ pp = sp.ypp[comp];
-    const double *__restrict__ h = sp.yh[comp];
-    // forward sweep, rows j = 1..ny
-    double g = (comp == 1 ? du1 : (double)r[sy]) * pp[1];
-    r[sy] = (T)g;
-    for (int j = 2; j <= ny; ++j) {
-      g = ((double)r[sy * j] - a[j] * g) * pp[j];
-      r[sy * j] = (T)g;
-    }
-    // back substitution and update; row 1 of v is solved but not added
-    double x = g;
-    const int jlo = comp == 1 ? 2 : 1;
-    q[sy * ny] += x;
-    for (int j = ny - 1; j >= 1; --j) {
-      x = (double)r[sy * j] - h[j] * x;
-      if (j >= jlo) q[sy * j] += x;
-    }
-    if (comp == 0) du1 = x;  // final u increment at j = 1
-    // no-slip ghosts (src/BC_WALL.f90:204-230)
-    q[0] = 0.0;
-    q[sy * (ny + 1)] = 0.0;
-    if (comp == 1) q[sy] = 0.0;
-  }
-}
-
 // MOMFA3_Y_tg with the lines staged in shared memory: a block owns 32
 // consecutive i at one k; all 128 threads load the [ny][32] tile (coalesced,
 // many loads in flight), warp 0 runs the Thomas sweeps from shared memory with
 // the precomputed pivots, all threads add the increment to q.  The v line's
-// row 1 takes the u increment at j = 1 (same quirk as k_adiy).
+// row 1 takes the u increment at j = 1, as in the reference (RHS_tg row 1 is
+// not rebuilt for IDR = 2, src/RHS_CvLpGpS_tg.f90:61-62, while MOMFA3_Y_tg
+// solves rows 1..ny, src/MOMFA_tg.f90:209-234).
 constexpr int AY_TL = 32;
 template <typename T>
 __global__ void __launch_bounds__(128) k_adiy_smem(TGDev d, SubParams sp, int from_dq) {
@@ -778,7 +734,7 @@ __global__ void __launch_bounds__(256, 2) k_fftx(TGDev d, SubParams sp, FFTPlan 
         val = dv * coe0;
         d.rhsphi[c0] = val;
       } else {
-        val = d.rhsphi[c0];
+        val = mode == 1 ? d.rhsphi[c0] : d.res[c0];
       }
     }
     C *z = A + (r >> 1) * nx + i;
@@ -843,116 +799,68 @@ __global__ void __launch_bounds__(256, 2) k_fftz(TGDev d, FFTPlan pl, int lz, in
   }
 }
 
-// Poisson y-tridiagonal per (kx, kz) (src/possion3d_FFT99.f90:334-443 with the
-// coefficients of TDMA_PHI_COEF :185-220): A = AMPH, B = ACPH - AK1 - AK3,
-// C = APPH; for the mean mode row 1 is decoupled and its rhs set to zero.
-// Real and imaginary parts share the pivots.
-template <typename T>
-__global__ void __launch_bounds__(128) k_ysolve(TGDev d) {
-  typedef typename Cplx<T>::type C;
+// Pivots of the Poisson y-tridiagonals, computed once per context: for every
+// (kx, kz) the forward-elimination factors pp_j = 1/(B_j - h_{j-1} A_j) and
+// h_j = C_j pp_j of the matrix of src/possion3d_FFT99.f90:334-443 with the
+// coefficients of TDMA_PHI_COEF (:185-220): A = AMPH, B = ACPH - AK1 - AK3,
+// C = APPH, and for the mean mode (kx = kz = 0) row 1 decoupled.  Stored as
+// {pp, h} pairs in the spectral layout.
+__global__ void k_ypivots(TGDev d) {
   const int lh = d.lh, ny = d.ny;
   const int kx = blockIdx.x * blockDim.x + threadIdx.x;
   const int kz = blockIdx.y;
   if (kx >= lh) return;
-  C *S = reinterpret_cast<C *>(d.spec) + kx + (int64_t)lh * ny * kz;
-  double *H = d.ysc + kx + (int64_t)lh * ny * kz;
+  double2 *P = d.ypiv + kx + (int64_t)lh * ny * kz;
   const double shift = d.ak1[kx] + d.ak3[kz];
   const bool mean = (kx == 0 && kz == 0);
-  // j = 1
   double b = d.acph[1] - shift;
-  double cc = mean ? 0.0 : d.apph[1];
-  double h = cc / b;
-  C r = S[0];
-  double gr = mean ? 0.0 : (double)r.x / b;
-  double gi = mean ? 0.0 : (double)r.y / b;
-  H[0] = h;
-  {
-    C o; o.x = (T)gr; o.y = (T)gi; S[0] = o;
-  }
+  double pp = 1.0 / b;
+  double h = (mean ? 0.0 : d.apph[1]) * pp;
+  P[0] = make_double2(mean ? 0.0 : pp, h);  // pp = 0 zeroes the pinned row
   for (int j = 2; j <= ny; ++j) {
-    const int64_t o = (int64_t)lh * (j - 1);
-    const double a = d.amph[j];
     b = d.acph[j] - shift;
-    const double pp = 1.0 / (b - h * a);
-    r = S[o];
-    gr = ((double)r.x - a * gr) * pp;
-    gi = ((double)r.y - a * gi) * pp;
-    if (j < ny) {
-      h = d.apph[j] * pp;
-      H[o] = h;
-    }
-    C w; w.x = (T)gr; w.y = (T)gi; S[o] = w;
-  }
-  double xr = gr, xi = gi;
-  for (int j = ny - 1; j >= 1; --j) {
-    const int64_t o = (int64_t)lh * (j - 1);
-    const double hh = H[o];
-    r = S[o];
-    xr = (double)r.x - hh * xr;
-    xi = (double)r.y - hh * xi;
-    C w; w.x = (T)xr; w.y = (T)xi; S[o] = w;
+    pp = 1.0 / (b - h * d.amph[j]);
+    h = j < ny ? d.apph[j] * pp : 0.0;
+    P[(int64_t)lh * (j - 1)] = make_double2(pp, h);
   }
 }
 
-// Poisson y-tridiagonals with the lines staged in shared memory: 16
-// consecutive kx at one kz per block; the pivots h_j are kept in shared memory
-// for the back substitution.  Arithmetic as k_ysolve.
-constexpr int YS_TL = 16;
+// Poisson y-tridiagonal solves, one thread per (kx, kz) line straight from
+// global memory: consecutive threads own consecutive kx, so every row access
+// is coalesced; the forward-swept g is written over the spectral data in
+// place and read back by the back substitution; with the pivots precomputed
+// no load sits on the serial dependency chain, so the unrolled sweeps keep
+// many loads in flight.
 template <typename T>
-__global__ void __launch_bounds__(128) k_ysolve_smem(TGDev d) {
+__global__ void __launch_bounds__(128) k_ysolve_line(TGDev d) {
   typedef typename Cplx<T>::type C;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
   const int lh = d.lh, ny = d.ny;
-  C *tile = reinterpret_cast<C *>(smem_raw);
-  double *hh = reinterpret_cast<double *>(smem_raw + (size_t)ny * YS_TL * sizeof(C));
-  const int kx0 = blockIdx.x * YS_TL, kz = blockIdx.y;
-  const int nl = min(YS_TL, lh - kx0);
-  const int tid = threadIdx.x;
-  C *S = reinterpret_cast<C *>(d.spec) + kx0 + (int64_t)lh * ny * kz;
-  for (int t = tid; t < ny * YS_TL; t += blockDim.x) {
-    const int r = t / YS_TL, l = t - r * YS_TL;
-    if (l < nl) tile[t] = S[l + (int64_t)lh * r];
+  const int kx = blockIdx.x * blockDim.x + threadIdx.x, kz = blockIdx.y;
+  if (kx >= lh) return;
+  C *S = reinterpret_cast<C *>(d.spec) + kx + (int64_t)lh * ny * kz;
+  const double2 *P = d.ypiv + kx + (int64_t)lh * ny * kz;
+  const int64_t st = lh;
+  C r = S[0];
+  double2 pv = P[0];
+  double gr = (double)r.x * pv.x, gi = (double)r.y * pv.x;
+  { C o; o.x = (T)gr; o.y = (T)gi; S[0] = o; }
+#pragma unroll 8
+  for (int j = 2; j <= ny; ++j) {
+    const double a = d.amph[j];
+    pv = P[st * (j - 1)];
+    r = S[st * (j - 1)];
+    gr = ((double)r.x - a * gr) * pv.x;
+    gi = ((double)r.y - a * gi) * pv.x;
+    C o; o.x = (T)gr; o.y = (T)gi; S[st * (j - 1)] = o;
   }
-  __syncthreads();
-  if (tid < nl) {
-    const int kx = kx0 + tid;
-    C *col = tile + tid;
-    double *hc = hh + tid;
-    const double shift = d.ak1[kx] + d.ak3[kz];
-    const bool mean = (kx == 0 && kz == 0);
-    double b = d.acph[1] - shift;
-    double h = (mean ? 0.0 : d.apph[1]) / b;
-    C r = col[0];
-    double gr = mean ? 0.0 : (double)r.x / b;
-    double gi = mean ? 0.0 : (double)r.y / b;
-    hc[0] = h;
-    { C o; o.x = (T)gr; o.y = (T)gi; col[0] = o; }
-    for (int j = 2; j <= ny; ++j) {
-      const double a = d.amph[j];
-      b = d.acph[j] - shift;
-      const double pp = 1.0 / (b - h * a);
-      r = col[(j - 1) * YS_TL];
-      gr = ((double)r.x - a * gr) * pp;
-      gi = ((double)r.y - a * gi) * pp;
-      if (j < ny) {
-        h = d.apph[j] * pp;
-        hc[(j - 1) * YS_TL] = h;
-      }
-      C o; o.x = (T)gr; o.y = (T)gi; col[(j - 1) * YS_TL] = o;
-    }
-    double xr = gr, xi = gi;
-    for (int j = ny - 1; j >= 1; --j) {
-      const double hj = hc[(j - 1) * YS_TL];
-      r = col[(j - 1) * YS_TL];
-      xr = (double)r.x - hj * xr;
-      xi = (double)r.y - hj * xi;
-      C o; o.x = (T)xr; o.y = (T)xi; col[(j - 1) * YS_TL] = o;
-    }
-  }
-  __syncthreads();
-  for (int t = tid; t < ny * YS_TL; t += blockDim.x) {
-    const int r = t / YS_TL, l = t - r * YS_TL;
-    if (l < nl) S[l + (int64_t)lh * r] = tile[t];
+  double xr = gr, xi = gi;
+#pragma unroll 8
+  for (int j = ny - 1; j >= 1; --j) {
+    const double hj = P[st * (j - 1)].y;
+    r = S[st * (j - 1)];
+    xr = (double)r.x - hj * xr;
+    xi = (double)r.y - hj * xi;
+    C o; o.x = (T)xr; o.y = (T)xi; S[st * (j - 1)] = o;
   }
 }
 
@@ -960,7 +868,7 @@ __global__ void __launch_bounds__(128) k_ysolve_smem(TGDev d) {
 // rows rebuilt as one complex Hermitian-extended line; phi ghosts copied
 // (BC_WALL_DPH, src/BC_WALL.f90:342-364).
 template <typename T, bool BIG>
-__global__ void __launch_bounds__(256, 2) k_ifftx(TGDev d, FFTPlan pl, int lb) {
+__global__ void __launch_bounds__(256, 2) k_ifftx(TGDev d, FFTPlan pl, int lb, int accumulate) {
   typedef typename Cplx<T>::type C;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int nx = d.nx, ny = d.ny, lh = d.lh;
@@ -997,10 +905,32 @@ __global__ void __launch_bounds__(256, 2) k_ifftx(TGDev d, FFTPlan pl, int lb) {
     const C z = res[(r >> 1) * nx + i];
     const double val = (r & 1) ? (double)z.y : (double)z.x;
     const int64_t c0 = i + d.sy * j + d.sz * k;
-    d.phi[c0] = val;
-    if (j == 1) d.phi[c0 - d.sy] = val;
-    if (j == ny) d.phi[c0 + d.sy] = val;
+    const double out = accumulate ? d.phi[c0] + val : val;
+    d.phi[c0] = out;
+    if (j == 1) d.phi[c0 - d.sy] = out;
+    if (j == ny) d.phi[c0 + d.sy] = out;
   }
+}
+
+// FP64 residual of the discrete Poisson operator the spectral solver inverts
+// (the operator of CHECK_FFT_SOLVER, src/PRESSURE_CORRECTION.f90:159-202):
+// res = RHSLLPHI - [d_xx + d_zz + L_y] phi, with L_y the folded Neumann
+// y-operator AMPH/ACPH/APPH.  Feeds the refinement sweep of the mixed form.
+__global__ void __launch_bounds__(RHS_BX *RHS_BY) k_pois_residual(TGDev d) {
+  const int nx = d.nx, ny = d.ny;
+  const int i = blockIdx.x * RHS_BX + threadIdx.x;
+  const int j = blockIdx.y * RHS_BY + threadIdx.y + 1;
+  const int k = blockIdx.z;
+  if (i >= nx || j > ny) return;
+  const int64_t sy = d.sy;
+  const int64_t c0 = i + sy * j + d.sz * k;
+  const int ip = wrapp(i, nx), im = wrapm(i, nx), kp = wrapp(k, d.nz), km = wrapm(k, d.nz);
+  const double f = d.phi[c0];
+  double l = (d.phi[c0 + (ip - i)] - 2.0 * f + d.phi[c0 + (im - i)]) * d.dxqi +
+             (d.phi[c0 + d.sz * (kp - k)] - 2.0 * f + d.phi[c0 + d.sz * (km - k)]) * d.dzqi + d.acph[j] * f;
+  if (j > 1) l += d.amph[j] * d.phi[c0 - sy];
+  if (j < ny) l += d.apph[j] * d.phi[c0 + sy];
+  d.res[c0] = d.rhsphi[c0] - l;
 }
 
 // VELOUPDT_tg (src/VELO_CORRECTION.f90:19-105), PRCALC_tg
@@ -1083,104 +1013,6 @@ __global__ void __launch_bounds__(1024) k_reduce_final(TGDev d, int what, int np
 }
 
 // ============================================================ launchers
-static int fftx_lb(int nx) {
-  // rows per block of the x transforms: two complex buffers of lb/2 lines
-  int lb = (int)(96 * 1024 / ((size_t)nx * sizeof(double2)));
-  lb = lb & ~1;
-  if (lb > 16) lb = 16;
-  if (lb < 2) lb = 2;
-  return lb;
-}
-static size_t fftx_smem(int nx, int lb) { return (size_t)lb * nx * sizeof(double2); }
-static int fftz_lz(int nz) {
-  int lz = (int)(96 * 1024 / ((size_t)2 * (nz + 1) * sizeof(double2)));
-  if (lz > 16) lz = 16;
-  if (lz < 1) lz = 1;
-  return lz;
-}
-static size_t fftz_smem(int nz, int lz) { return (size_t)2 * lz * (nz + 1) * sizeof(double2); }
-static size_t adiy_smem(int ny) { return (size_t)ny * AY_TL * sizeof(double); }
-static size_t ysolve_smem(int ny) { return (size_t)ny * YS_TL * (sizeof(double2) + sizeof(double)); }
-static int adix_lb(int nx) {
-  int lb = (int)(96 * 1024 / ((size_t)(nx + 1) * sizeof(double)));
-  if (lb > 64) lb = 64;
-  if (lb < 1) lb = 1;
-  return lb;
-}
-static size_t adix_smem(int nx, int lb) {
-  return (((size_t)lb * (nx + 1) * sizeof(double) + 15) & ~(size_t)15) + 3 * (size_t)nx * sizeof(double);
-}
-static size_t adiz_smem(int nz) {
-  return (((size_t)nz * LZ * sizeof(double) + 15) & ~(size_t)15) + 3 * (size_t)nz * sizeof(double);
-}
-
-static size_t rhs_tma_smem() { return RtLayout<double>::smem_bytes; }
-
-// TMA descriptors of the four state fields: dims (nx, ny+2, nz) doubles,
-// box (36, 10, 1), no swizzle, out-of-bounds boxes zero filled.
-static int make_rhs_maps(chapsim_ctx *c) {
-  TGDev &d = c->d;
-  c->use_tma_rhs = false;
-  if (d.nx < RT_BXW || d.ny < 8) return CHAPSIM_OK;  // small grids use k_rhs
-  PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-  cudaDriverEntryPointQueryResult q;
-  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void **)&encode, cudaEnableDefault, &q) != cudaSuccess ||
-      q != cudaDriverEntryPointSuccess || !encode) {
-    cudaGetLastError();
-    return CHAPSIM_OK;
-  }
-  void *f[7] = {d.u, d.v, d.w, d.p, d.h0[0], d.h0[1], d.h0[2]};
-  cuuint64_t dims[3] = {(cuuint64_t)d.nx, (cuuint64_t)(d.ny + 2), (cuuint64_t)d.nz};
-  cuuint64_t strides[2] = {(cuuint64_t)d.sy * sizeof(double), (cuuint64_t)d.sz * sizeof(double)};
-  cuuint32_t box[3] = {RT_BXW, RT_BYW, 1};
-  cuuint32_t hbox[3] = {RHS_BX, RHS_BY, 1};
-  cuuint32_t es[3] = {1, 1, 1};
-  for (int m = 0; m < 7; ++m) {
-    CUresult r = encode(&c->rhs_maps[m], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, f[m], dims, strides, m < 4 ? box : hbox, es,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) {
-      c->err = "cuTensorMapEncodeTiled failed";
-      return CHAPSIM_ERR_CUDA;
-    }
-  }
-  CK(cudaFuncSetAttribute(k_rhs_tma<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tma_smem()));
-  CK(cudaFuncSetAttribute(k_rhs_tma<double>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-  c->use_tma_rhs = true;
-  return CHAPSIM_OK;
-}
-
-int init_kernels(chapsim_ctx *c) {
-  const int nx = c->d.nx, nz = c->d.nz;
-  {
-    int rc = make_rhs_maps(c);
-    if (rc) return rc;
-  }
-  CK(cudaFuncSetAttribute(k_adix<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adix_smem(nx, adix_lb(nx))));
-  CK(cudaFuncSetAttribute(k_adiz<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adiz_smem(nz)));
-  const int ny = c->d.ny;
-  c->fft_big = false;
-  for (int s2 = 0; s2 < 16; ++s2) if (c->fx.rad[s2] > 5 || c->fz.rad[s2] > 5) c->fft_big = true;
-#define FFT_ATTR(BIG)                                                                                           \
-  CK(cudaFuncSetAttribute(k_fftx<double, BIG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftx_smem(nx, fftx_lb(nx)))); \
-  CK(cudaFuncSetAttribute(k_ifftx<double, BIG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftx_smem(nx, fftx_lb(nx)))); \
-  CK(cudaFuncSetAttribute(k_fftz<double, BIG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftz_smem(nz, fftz_lz(nz))));
-  FFT_ATTR(false)
-  FFT_ATTR(true)
-#undef FFT_ATTR
-  if (adiy_smem(ny) > 200 * 1024 || ysolve_smem(ny) > 200 * 1024) {
-    c->err = "ny too large for the shared-memory y-line kernels";
-    return CHAPSIM_ERR_UNSUPPORTED;
-  }
-  CK(cudaFuncSetAttribute(k_adiy_smem<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adiy_smem(ny)));
-  CK(cudaFuncSetAttribute(k_adixz_band<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          (int)band_smem(BAND_WMAX, BAND_WMAX)));
-  CK(cudaFuncSetAttribute(k_ysolve_smem<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ysolve_smem(ny)));
-  CK(cudaFuncSetAttribute(k_adiy_smem<double>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-  CK(cudaFuncSetAttribute(k_ysolve_smem<double>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-  return CHAPSIM_OK;
-}
-
 static inline void phase_mark(chapsim_ctx *c, int ph) {
   if (c->timing) cudaEventRecord(c->evpool[(size_t)c->ev_pending * (CHAPSIM_PH_COUNT + 1) + ph], c->stream);
 }
@@ -1203,70 +1035,264 @@ int flush_phase_events(chapsim_ctx *c) {
   return CHAPSIM_OK;
 }
 
+template <typename T> struct Prec {
+  typedef typename Cplx<T>::type C;
+  static int fftx_lb(int nx) {
+    // rows per block of the x transforms: two complex buffers of lb/2 lines
+    int lb = (int)(96 * 1024 / ((size_t)nx * sizeof(C)));
+    lb = lb & ~1;
+    if (lb > 16) lb = 16;
+    if (lb < 2) lb = 2;
+    return lb;
+  }
+  static size_t fftx_smem(int nx, int lb) { return (size_t)lb * nx * sizeof(C); }
+  static int fftz_lz(int nz) {
+    int lz = (int)(96 * 1024 / ((size_t)2 * (nz + 1) * sizeof(C)));
+    if (lz > 16) lz = 16;
+    if (lz < 1) lz = 1;
+    return lz;
+  }
+  static size_t fftz_smem(int nz, int lz) { return (size_t)2 * lz * (nz + 1) * sizeof(C); }
+  static size_t adiy_smem(int ny) { return (size_t)ny * AY_TL * sizeof(T); }
+  static int adix_lb(int nx) {
+    int lb = (int)(96 * 1024 / ((size_t)(nx + 1) * sizeof(T)));
+    if (lb > 64) lb = 64;
+    if (lb < 1) lb = 1;
+    return lb;
+  }
+  static size_t adix_smem(int nx, int lb) {
+    return (((size_t)lb * (nx + 1) * sizeof(T) + 15) & ~(size_t)15) + 3 * (size_t)nx * sizeof(double);
+  }
+  static size_t adiz_smem(int nz) {
+    return (((size_t)nz * LZ * sizeof(T) + 15) & ~(size_t)15) + 3 * (size_t)nz * sizeof(double);
+  }
+  static size_t rhs_tma_smem() { return RtLayout<T>::smem_bytes; }
+
+  static int init(chapsim_ctx *c) {
+    const int nx = c->d.nx, ny = c->d.ny, nz = c->d.nz;
+    if (c->use_tma_rhs) {
+      CK(cudaFuncSetAttribute(k_rhs_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tma_smem()));
+      CK(cudaFuncSetAttribute(k_rhs_tma<T>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    }
+    CK(cudaFuncSetAttribute(k_adix<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adix_smem(nx, adix_lb(nx))));
+    CK(cudaFuncSetAttribute(k_adiz<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adiz_smem(nz)));
+    CK(cudaFuncSetAttribute(k_fftx<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftx_smem(nx, fftx_lb(nx))));
+    CK(cudaFuncSetAttribute(k_ifftx<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftx_smem(nx, fftx_lb(nx))));
+    CK(cudaFuncSetAttribute(k_fftz<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftz_smem(nz, fftz_lz(nz))));
+    CK(cudaFuncSetAttribute(k_fftx<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftx_smem(nx, fftx_lb(nx))));
+    CK(cudaFuncSetAttribute(k_ifftx<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftx_smem(nx, fftx_lb(nx))));
+    CK(cudaFuncSetAttribute(k_fftz<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftz_smem(nz, fftz_lz(nz))));
+    if (adiy_smem(ny) > 200 * 1024) {
+      c->err = "ny too large for the shared-memory y-line kernels";
+      return CHAPSIM_ERR_UNSUPPORTED;
+    }
+    CK(cudaFuncSetAttribute(k_adiy_smem<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adiy_smem(ny)));
+    CK(cudaFuncSetAttribute(k_adixz_band<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)band_smem(BAND_WMAX, BAND_WMAX)));
+    CK(cudaFuncSetAttribute(k_adiy_smem<T>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    return CHAPSIM_OK;
+  }
+
+  // mode 0: divergence of q; 1: stored RHSLLPHI; 2: residual buffer
+  static int fftx(chapsim_ctx *c, int ns, int mode) {
+    TGDev &d = c->d;
+    const int lb = fftx_lb(d.nx);
+    dim3 grid((d.ny + lb - 1) / lb, d.nz);
+    if (c->fft_big)
+      k_fftx<T, true><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->sp[ns], c->fx, lb, mode);
+    else
+      k_fftx<T, false><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->sp[ns], c->fx, lb, mode);
+    LAUNCHED();
+    return CHAPSIM_OK;
+  }
+
+  static int spectral_solve(chapsim_ctx *c, int accumulate, bool mark) {
+    TGDev &d = c->d;
+    const int lz = fftz_lz(d.nz), lb = fftx_lb(d.nx);
+    if (mark) phase_mark(c, CHAPSIM_PH_FFTZ);
+    {
+      dim3 grid((d.lh + lz - 1) / lz, d.ny);
+      if (c->fft_big)
+        k_fftz<T, true><<<grid, 256, fftz_smem(d.nz, lz), c->stream>>>(d, c->fz, lz, -1);
+      else
+        k_fftz<T, false><<<grid, 256, fftz_smem(d.nz, lz), c->stream>>>(d, c->fz, lz, -1);
+      LAUNCHED();
+    }
+    if (mark) phase_mark(c, CHAPSIM_PH_YSOLVE);
+    {
+      dim3 grid((d.lh + 127) / 128, d.nz);
+      k_ysolve_line<T><<<grid, 128, 0, c->stream>>>(d);
+      LAUNCHED();
+    }
+    if (mark) phase_mark(c, CHAPSIM_PH_IFFTZ);
+    {
+      dim3 grid((d.lh + lz - 1) / lz, d.ny);
+      if (c->fft_big)
+        k_fftz<T, true><<<grid, 256, fftz_smem(d.nz, lz), c->stream>>>(d, c->fz, lz, +1);
+      else
+        k_fftz<T, false><<<grid, 256, fftz_smem(d.nz, lz), c->stream>>>(d, c->fz, lz, +1);
+      LAUNCHED();
+    }
+    if (mark) phase_mark(c, CHAPSIM_PH_IFFTX);
+    {
+      dim3 grid((d.ny + lb - 1) / lb, d.nz);
+      if (c->fft_big)
+        k_ifftx<T, true><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->fx, lb, accumulate);
+      else
+        k_ifftx<T, false><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->fx, lb, accumulate);
+      LAUNCHED();
+    }
+    return CHAPSIM_OK;
+  }
+
+  // Poisson solve of RHSLLPHI (computed from q when mode == 0).  The mixed
+  // form adds one refinement sweep: residual in FP64, second FP32 solve,
+  // correction accumulated into phi.
+  static int poisson(chapsim_ctx *c, int ns, int mode) {
+    TGDev &d = c->d;
+    phase_mark(c, CHAPSIM_PH_FFTX);
+    int rc = fftx(c, ns, mode);
+    if (rc) return rc;
+    rc = spectral_solve(c, 0, true);
+    if (rc) return rc;
+    if (sizeof(T) == 4 && c->refine) {
+      dim3 grid((d.nx + RHS_BX - 1) / RHS_BX, (d.ny + RHS_BY - 1) / RHS_BY, d.nz);
+      k_pois_residual<<<grid, dim3(RHS_BX, RHS_BY), 0, c->stream>>>(d);
+      LAUNCHED();
+      rc = fftx(c, ns, 2);
+      if (rc) return rc;
+      rc = spectral_solve(c, 1, false);
+      if (rc) return rc;
+    }
+    return CHAPSIM_OK;
+  }
+
+  static int substep(chapsim_ctx *c, int ns) {
+    TGDev &d = c->d;
+    const SubParams &sp = c->sp[ns];
+    phase_mark(c, CHAPSIM_PH_RHS);
+    {
+      dim3 grid((d.nx + RHS_BX - 1) / RHS_BX, (d.ny + RHS_BY - 1) / RHS_BY, d.nz);
+      if (c->use_tma_rhs) {
+        const int nzc = c->rhs_nzc;
+        grid.z = (d.nz + nzc - 1) / nzc;
+        RhsMaps maps;
+        memcpy(maps.m, c->rhs_maps, sizeof(maps.m));
+        k_rhs_tma<T><<<grid, dim3(RHS_BX, RHS_BY), rhs_tma_smem(), c->stream>>>(maps, d, sp, nzc);
+      } else {
+        k_rhs<T><<<grid, dim3(RHS_BX, RHS_BY), 0, c->stream>>>(d, sp);
+      }
+      LAUNCHED();
+      const int npart = grid.x * grid.y * grid.z;
+      k_dpgrns<<<1, 1024, 0, c->stream>>>(d, sp, npart);
+      LAUNCHED();
+    }
+    phase_mark(c, CHAPSIM_PH_ADIX);
+    if (sp.band) {
+      dim3 grid((d.nx + BM_TX - 1) / BM_TX, (d.ny + BM_TY - 1) / BM_TY, 3 * ((d.nz + BM_SEG - 1) / BM_SEG));
+      k_adixz_band<T><<<grid, dim3(BM_TX, BM_TY), band_smem(sp.wx, sp.wz), c->stream>>>(d, sp);
+      LAUNCHED();
+      phase_mark(c, CHAPSIM_PH_ADIZ);
+    } else {
+      const int lb = adix_lb(d.nx);
+      dim3 grid((d.ny + lb - 1) / lb, d.nz, 3);
+      k_adix<T><<<grid, 128, adix_smem(d.nx, lb), c->stream>>>(d, sp, lb);
+      LAUNCHED();
+      phase_mark(c, CHAPSIM_PH_ADIZ);
+      dim3 grid2((d.nx + LZ - 1) / LZ, d.ny, 3);
+      k_adiz<T><<<grid2, 128, adiz_smem(d.nz), c->stream>>>(d, sp);
+      LAUNCHED();
+    }
+    phase_mark(c, CHAPSIM_PH_ADIY);
+    if (sp.band && sp.wy >= 0) {
+      dim3 grid((d.nx + AY_TX - 1) / AY_TX, (d.ny + AY_JT - 1) / AY_JT, d.nz);
+      k_adiy_band<T><<<grid, dim3(AY_TX, AY_TY), 0, c->stream>>>(d, sp);
+      LAUNCHED();
+    } else {
+      dim3 grid((d.nx + AY_TL - 1) / AY_TL, d.nz);
+      k_adiy_smem<T><<<grid, 128, adiy_smem(d.ny), c->stream>>>(d, sp, sp.band);
+      LAUNCHED();
+    }
+    int rc = poisson(c, ns, 0);
+    if (rc) return rc;
+    phase_mark(c, CHAPSIM_PH_CORR);
+    rc = launch_correction(c, ns);
+    if (rc) return rc;
+    if (c->timing) {
+      phase_mark(c, CHAPSIM_PH_COUNT);
+      if (++c->ev_pending == chapsim_ctx::kEvSub) return flush_phase_events(c);
+    }
+    return CHAPSIM_OK;
+  }
+};
+
+// TMA descriptors of u, v, w, p (FP64, box 36 x 10 x 1) and of the three H0
+// components (temporary precision, box 32 x 8 x 1); no swizzle, out-of-bounds
+// boxes zero filled.
+static int make_rhs_maps(chapsim_ctx *c) {
+  TGDev &d = c->d;
+  c->use_tma_rhs = false;
+  if (d.nx < RT_BXW || d.ny < 8) return CHAPSIM_OK;  // small grids use k_rhs
+  PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void **)&encode, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !encode) {
+    cudaGetLastError();
+    return CHAPSIM_OK;
+  }
+  const bool mixed = c->cfg.precision == CHAPSIM_MIXED;
+  const size_t hsz = mixed ? sizeof(float) : sizeof(double);
+  void *f[7] = {d.u, d.v, d.w, d.p, d.h0[0], d.h0[1], d.h0[2]};
+  cuuint64_t dims[3] = {(cuuint64_t)d.nx, (cuuint64_t)(d.ny + 2), (cuuint64_t)d.nz};
+  cuuint64_t strides[2] = {(cuuint64_t)d.sy * sizeof(double), (cuuint64_t)d.sz * sizeof(double)};
+  cuuint64_t hstrides[2] = {(cuuint64_t)d.sy * hsz, (cuuint64_t)d.sz * hsz};
+  cuuint32_t box[3] = {RT_BXW, RT_BYW, 1};
+  cuuint32_t hbox[3] = {RHS_BX, RHS_BY, 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  if ((d.sy * hsz) % 16 != 0) return CHAPSIM_OK;  // TMA strides must be multiples of 16 bytes
+  for (int m = 0; m < 7; ++m) {
+    const bool h = m >= 4;
+    CUresult r = encode(&c->rhs_maps[m], (h && mixed) ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                        3, f[m], dims, h ? hstrides : strides, h ? hbox : box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+      c->err = "cuTensorMapEncodeTiled failed";
+      return CHAPSIM_ERR_CUDA;
+    }
+  }
+  c->use_tma_rhs = true;
+  return CHAPSIM_OK;
+}
+
+int init_kernels(chapsim_ctx *c) {
+  int rc = make_rhs_maps(c);
+  if (rc) return rc;
+  {
+    TGDev &d = c->d;
+    dim3 grid((d.lh + 127) / 128, d.nz);
+    k_ypivots<<<grid, 128, 0, c->stream>>>(d);
+    LAUNCHED();
+  }
+  c->fft_big = false;
+  for (int s2 = 0; s2 < 16; ++s2)
+    if (c->fx.rad[s2] > 5 || c->fz.rad[s2] > 5) c->fft_big = true;
+  return c->cfg.precision == CHAPSIM_MIXED ? Prec<float>::init(c) : Prec<double>::init(c);
+}
+
 int launch_divg(chapsim_ctx *c, int ns) {
   // DIVG_tg alone: the fused divergence + x-transform kernel in mode 0 stores
   // RHSLLPHI (its spectral output is scratch).
-  TGDev &d = c->d;
-  const int lb = fftx_lb(d.nx);
-  dim3 grid((d.ny + lb - 1) / lb, d.nz);
-  if (c->fft_big)
-    k_fftx<double, true><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->sp[ns], c->fx, lb, 0);
-  else
-    k_fftx<double, false><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->sp[ns], c->fx, lb, 0);
-  LAUNCHED();
-  return CHAPSIM_OK;
+  return c->cfg.precision == CHAPSIM_MIXED ? Prec<float>::fftx(c, ns, 0) : Prec<double>::fftx(c, ns, 0);
 }
 
-static int poisson_from_rhs(chapsim_ctx *c, int ns, int mode) {
-  TGDev &d = c->d;
-  const int lb = fftx_lb(d.nx);
-  phase_mark(c, CHAPSIM_PH_FFTX);
-  {
-    dim3 grid((d.ny + lb - 1) / lb, d.nz);
-    if (c->fft_big)
-      k_fftx<double, true><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->sp[ns], c->fx, lb, mode);
-    else
-      k_fftx<double, false><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->sp[ns], c->fx, lb, mode);
-    LAUNCHED();
-  }
-  phase_mark(c, CHAPSIM_PH_FFTZ);
-  const int lz = fftz_lz(d.nz);
-  {
-    dim3 grid((d.lh + lz - 1) / lz, d.ny);
-    if (c->fft_big)
-      k_fftz<double, true><<<grid, 256, fftz_smem(d.nz, lz), c->stream>>>(d, c->fz, lz, -1);
-    else
-      k_fftz<double, false><<<grid, 256, fftz_smem(d.nz, lz), c->stream>>>(d, c->fz, lz, -1);
-    LAUNCHED();
-  }
-  phase_mark(c, CHAPSIM_PH_YSOLVE);
-  {
-    dim3 grid((d.lh + YS_TL - 1) / YS_TL, d.nz);
-    k_ysolve_smem<double><<<grid, 128, ysolve_smem(d.ny), c->stream>>>(d);
-    LAUNCHED();
-  }
-  phase_mark(c, CHAPSIM_PH_IFFTZ);
-  {
-    dim3 grid((d.lh + lz - 1) / lz, d.ny);
-    if (c->fft_big)
-      k_fftz<double, true><<<grid, 256, fftz_smem(d.nz, lz), c->stream>>>(d, c->fz, lz, +1);
-    else
-      k_fftz<double, false><<<grid, 256, fftz_smem(d.nz, lz), c->stream>>>(d, c->fz, lz, +1);
-    LAUNCHED();
-  }
-  phase_mark(c, CHAPSIM_PH_IFFTX);
-  {
-    dim3 grid((d.ny + lb - 1) / lb, d.nz);
-    if (c->fft_big)
-      k_ifftx<double, true><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->fx, lb);
-    else
-      k_ifftx<double, false><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->fx, lb);
-    LAUNCHED();
-  }
-  return CHAPSIM_OK;
+int launch_pois3d(chapsim_ctx *c) {
+  return c->cfg.precision == CHAPSIM_MIXED ? Prec<float>::poisson(c, 1, 1) : Prec<double>::poisson(c, 1, 1);
 }
 
-int launch_pois3d(chapsim_ctx *c) { return poisson_from_rhs(c, 1, 1); }
+int launch_substep(chapsim_ctx *c, int ns) {
+  return c->cfg.precision == CHAPSIM_MIXED ? Prec<float>::substep(c, ns) : Prec<double>::substep(c, ns);
+}
 
 int launch_correction(chapsim_ctx *c, int ns) {
   TGDev &d = c->d;
@@ -1281,64 +1307,6 @@ int launch_bc_q(chapsim_ctx *c) {
   dim3 grid((d.nx + 127) / 128, d.nz);
   k_bc_q<<<grid, 128, 0, c->stream>>>(d);
   LAUNCHED();
-  return CHAPSIM_OK;
-}
-
-int launch_substep(chapsim_ctx *c, int ns) {
-  TGDev &d = c->d;
-  const SubParams &sp = c->sp[ns];
-  phase_mark(c, CHAPSIM_PH_RHS);
-  {
-    dim3 grid((d.nx + RHS_BX - 1) / RHS_BX, (d.ny + RHS_BY - 1) / RHS_BY, d.nz);
-    if (c->use_tma_rhs) {
-      const int nzc = c->rhs_nzc;
-      grid.z = (d.nz + nzc - 1) / nzc;
-      RhsMaps maps;
-      memcpy(maps.m, c->rhs_maps, sizeof(maps.m));
-      k_rhs_tma<double><<<grid, dim3(RHS_BX, RHS_BY), rhs_tma_smem(), c->stream>>>(maps, d, sp, nzc);
-    } else {
-      k_rhs<double><<<grid, dim3(RHS_BX, RHS_BY), 0, c->stream>>>(d, sp);
-    }
-    LAUNCHED();
-    const int npart = grid.x * grid.y * grid.z;
-    k_dpgrns<<<1, 1024, 0, c->stream>>>(d, sp, npart);
-    LAUNCHED();
-  }
-  phase_mark(c, CHAPSIM_PH_ADIX);
-  if (sp.band) {
-    dim3 grid((d.nx + BM_TX - 1) / BM_TX, (d.ny + BM_TY - 1) / BM_TY, 3 * ((d.nz + BM_SEG - 1) / BM_SEG));
-    k_adixz_band<double><<<grid, dim3(BM_TX, BM_TY), band_smem(sp.wx, sp.wz), c->stream>>>(d, sp);
-    LAUNCHED();
-    phase_mark(c, CHAPSIM_PH_ADIZ);
-  } else {
-    const int lb = adix_lb(d.nx);
-    dim3 grid((d.ny + lb - 1) / lb, d.nz, 3);
-    k_adix<double><<<grid, 128, adix_smem(d.nx, lb), c->stream>>>(d, sp, lb);
-    LAUNCHED();
-    phase_mark(c, CHAPSIM_PH_ADIZ);
-    dim3 grid2((d.nx + LZ - 1) / LZ, d.ny, 3);
-    k_adiz<double><<<grid2, 128, adiz_smem(d.nz), c->stream>>>(d, sp);
-    LAUNCHED();
-  }
-  phase_mark(c, CHAPSIM_PH_ADIY);
-  if (sp.band && sp.wy >= 0) {
-    dim3 grid((d.nx + AY_TX - 1) / AY_TX, (d.ny + AY_JT - 1) / AY_JT, d.nz);
-    k_adiy_band<double><<<grid, dim3(AY_TX, AY_TY), 0, c->stream>>>(d, sp);
-    LAUNCHED();
-  } else {
-    dim3 grid((d.nx + AY_TL - 1) / AY_TL, d.nz);
-    k_adiy_smem<double><<<grid, 128, adiy_smem(d.ny), c->stream>>>(d, sp, sp.band);
-    LAUNCHED();
-  }
-  int rc = poisson_from_rhs(c, ns, 0);
-  if (rc) return rc;
-  phase_mark(c, CHAPSIM_PH_CORR);
-  rc = launch_correction(c, ns);
-  if (rc) return rc;
-  if (c->timing) {
-    phase_mark(c, CHAPSIM_PH_COUNT);
-    if (++c->ev_pending == chapsim_ctx::kEvSub) return flush_phase_events(c);
-  }
   return CHAPSIM_OK;
 }
 
