@@ -319,6 +319,20 @@ def run_ours(args, wl, ws, rank, local):
     return 0
 
 
+def profile_case(spec, precision):
+    import chapsim1ww_b200 as cs
+    from chapsim1ww_b200 import TGChannel
+    nx, ny, nz = (int(x) for x in spec.lower().split("x"))
+    s = TGChannel(nx, ny, nz, precision=cs.MIXED if precision == "mixed" else cs.FP64)
+    s.random_fl_fld_tg(1, 0.1, project=True)
+    for _ in range(2):
+        for ns in (1, 2, 3):
+            s.solverrk3_mom_tg(ns)
+    s.sync()
+    print("profile case ok", spec, precision, "max|div u| =", s.divgck_tg())
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -329,7 +343,12 @@ def main():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", default=None, metavar="NXxNYxNZ",
+                    help="run init + NS=0 + 2 eager RK3 steps of a channel of this size and exit "
+                         "(the small case for ncu captures; no timing)")
     args = ap.parse_args()
+    if args.profile_case:
+        return profile_case(args.profile_case, args.precision)
     args.warmup = max(args.warmup, 3)
     wl = WORKLOADS[args.workload]
     ws, rank, local = dist_setup()
