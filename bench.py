@@ -139,6 +139,45 @@ def load_traffic(workload, kernel):
         return None
 
 
+def bench_learned(cells, device):
+    """THERM_PROP_UPDATE on one field of the workload's size: the table
+    splines against the learned model (MLP 1->64->64->5, trained on the GPU on
+    65,536 samples of the synthetic 4096-point table, seed 2; BF16 tensor-core
+    inference), with the error gate at 1e-4 relative."""
+    import torch
+
+    from chapsim1ww_b200 import PropertyEngine, synthetic_table
+    eng = PropertyEngine(*synthetic_table(4096), device=device)
+    t0 = time.perf_counter()
+    loss = eng.train(65536, 2, 8000, 3e-3)
+    t_train = time.perf_counter() - t0
+    g = torch.Generator(device=f"cuda:{device}").manual_seed(5)
+    h = torch.rand(cells, dtype=torch.float64, device=f"cuda:{device}", generator=g) * 1.998 - 0.999
+    outs = [torch.zeros(cells, dtype=torch.float64, device=f"cuda:{device}") for _ in range(5)]
+
+    def timed(mode, reps=10):
+        eng.update(h, *outs[:4], cp=outs[4], mode=mode)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            eng.update(h, *outs[:4], cp=outs[4], mode=mode)
+        b.record()
+        b.synchronize()
+        return a.elapsed_time(b) / reps
+
+    table_ms = timed(0)
+    eng.gate(1e9, 256)
+    mlp_ms = timed(1)
+    nbins, worst = eng.gate(1e-4, 256)
+    gated_ms = timed(1)
+    eng.close()
+    return {"train_loss": loss, "train_s": t_train, "train_steps": 8000, "gate_tol": 1e-4,
+            "mlp_bins": nbins, "bins": 256, "mlp_max_rel_err": worst,
+            "table_update_ms": table_ms, "mlp_update_ms": mlp_ms, "gated_update_ms": gated_ms,
+            "cells": cells}
+
+
 def cpu_baseline_oracle(wl, steps):
     """FP64 oracle port on the host cores: init + NS=0, then `steps` timed steps."""
     from oracle.pyoracle import OracleTG, get_threads
@@ -277,6 +316,10 @@ def run_ours(args, wl, ws, rank, local):
     e2e_value = cells * ws * e2e_steps / (ms_e2e / 1000.0)
     nbytes = 4 * s.n * 8
 
+    learned = None
+    if rank == 0 and not args.no_props:
+        learned = bench_learned(cells, local)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
@@ -310,6 +353,7 @@ def run_ours(args, wl, ws, rank, local):
                               "frac": 3 * total_bytes / (ms / args.steps / 1000.0) / 1e9 / peak,
                               "phase_sum_ms": step_ms_phases},
             "clocks": clk,
+            "learned": learned,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -343,6 +387,7 @@ def main():
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-props", action="store_true", help="skip the learned-property measurement")
     ap.add_argument("--profile-case", default=None, metavar="NXxNYxNZ",
                     help="run init + NS=0 + 2 eager RK3 steps of a channel of this size and exit "
                          "(the small case for ncu captures; no timing)")

@@ -64,7 +64,19 @@ SIGNATURES = [
     ("chapsim_phase_reset", _I, [_P]),
     ("chapsim_launch_count", _I, [_P, ctypes.POINTER(_I64)]),
     ("chapsim_launch_count_reset", _I, [_P]),
+    ("chapsim_props_create", _I, [_P, _P, _P, _P, _P, _P, _I, _I, ctypes.POINTER(_P)]),
+    ("chapsim_props_destroy", _I, [_P]),
+    ("chapsim_props_last_error", ctypes.c_char_p, [_P]),
+    ("chapsim_props_update", _I, [_P, _I, _P, _P, _P, _P, _P, _P, _I64, ctypes.POINTER(_I64)]),
+    ("chapsim_props_train", _I, [_P, _I, ctypes.c_uint64, _I, _D, _DP]),
+    ("chapsim_props_gate", _I, [_P, _D, _I, ctypes.POINTER(_I), _DP]),
+    ("chapsim_props_get_params", _I, [_P, _P, _I, _P, _I]),
+    ("chapsim_props_set_params", _I, [_P, _P, _I, _P, _I]),
+    ("chapsim_props_loss_grad", _I, [_P, _P, _P, _I, _DP, _P, _I]),
 ]
+PROPS_TABLE, PROPS_MLP = 0, 1
+ERR_RANGE = 8
+ERRORS[8] = "CHAPSIM_ERR_RANGE"
 
 _lib = None
 

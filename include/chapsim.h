@@ -180,6 +180,71 @@ int chapsim_phase_reset(chapsim_ctx *ctx);
 int chapsim_launch_count(const chapsim_ctx *ctx, int64_t *count);
 int chapsim_launch_count_reset(chapsim_ctx *ctx);
 
+
+/* ======================================================================
+ * Thermal properties: table splines (THERM_PROP_UPDATE) and the learned
+ * property model.
+ *
+ * A property engine holds a non-dimensional property table (the columns
+ * NIST_H, NIST_T, NIST_D, NIST_M, NIST_K, NIST_CP of the reference's
+ * thermal_info module after NIST_TABLE_SCALING, src/Flow_State.f90:394-433),
+ * its cubic splines (NIST_SPLINE_H / NIST_SPLINE_T, src/Flow_State.f90:916,
+ * 1296, coefficients by CUBIC_SPLINE :1693-1787) and, optionally, a trained
+ * MLP h -> (T, rho, mu, k, cp) of shape 1 -> 64 -> 64 -> 5 (tanh), which has
+ * no counterpart in the reference.
+ * ====================================================================== */
+typedef struct chapsim_props chapsim_props;
+
+/* property evaluation modes */
+#define CHAPSIM_PROPS_TABLE 0 /* cubic splines, as THERM_PROP_UPDATE          */
+#define CHAPSIM_PROPS_MLP 1   /* MLP (BF16 weights, FP32 accumulation) where the
+                                 error gate allows it, table splines elsewhere */
+
+/* Build the engine from n >= 4 strictly increasing H (with T increasing too).
+ * Columns are host arrays of length n. */
+int chapsim_props_create(const double *H, const double *T, const double *D, const double *M, const double *K,
+                         const double *CP, int n, int device, chapsim_props **out);
+int chapsim_props_destroy(chapsim_props *pe);
+const char *chapsim_props_last_error(const chapsim_props *pe);
+
+/* THERM_PROP_UPDATE(IREGION) (src/THERM_PROP_UPDATE.f90:129-205) on n cells
+ * of device arrays: h -> T (spline in h), then mu, k, rho (splines in T).
+ * Cells with |h| < 1e-10 are left unchanged, as in the reference; cells whose
+ * h or T lies outside the table are left unchanged and counted (the
+ * reference STOPs there): the call then returns CHAPSIM_ERR_RANGE and
+ * *n_out_of_range holds the count.  cp may be NULL; when given it receives
+ * cp(h) (spline in h, NIST_HCP).  Work runs on the engine's stream and the
+ * call synchronises. */
+#define CHAPSIM_ERR_RANGE 8
+int chapsim_props_update(chapsim_props *pe, int mode, const double *h, double *T, double *rho, double *mu,
+                         double *k, double *cp, int64_t n, int64_t *n_out_of_range);
+
+/* Train the MLP on the GPU (project-written forward, backward and Adam
+ * kernels, FP32) on nsamples table samples drawn uniformly in h from seed:
+ * full-batch Adam for `steps` steps, learning rate lr decayed by cosine to
+ * lr/100.  *final_loss receives the last mean-squared error of the
+ * standardised outputs. */
+int chapsim_props_train(chapsim_props *pe, int nsamples, uint64_t seed, int steps, double lr, double *final_loss);
+
+/* Error gate: evaluate MLP (inference precision) and table on a dense h grid,
+ * split [H_1, H_n] into nbins bins, and allow the MLP in a bin only where its
+ * largest error over T, rho, mu, k, cp, relative to each output's largest
+ * magnitude over the table, is <= tol.  Returns the number of MLP bins and
+ * the worst relative error seen. */
+int chapsim_props_gate(chapsim_props *pe, double tol, int nbins, int *n_mlp_bins, double *max_rel_err);
+
+/* MLP parameters (float32, 4613 values: W1[64] b1[64] W2[64][64] b2[64]
+ * W3[5][64] b3[5]) and the input/output normalisation (h_mid, h_half, then
+ * mean[5], std[5]). */
+int chapsim_props_get_params(const chapsim_props *pe, float *params, int nparams, double *norm, int nnorm);
+int chapsim_props_set_params(chapsim_props *pe, const float *params, int nparams, const double *norm, int nnorm);
+
+/* Gradient check: loss and gradient of the MSE over a given batch (host
+ * arrays: x = normalised inputs, t = standardised targets [n][5]), computed by
+ * the training kernels. */
+int chapsim_props_loss_grad(chapsim_props *pe, const float *x, const float *t, int n, double *loss, float *grad,
+                            int nparams);
+
 #ifdef __cplusplus
 }
 #endif

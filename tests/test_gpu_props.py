@@ -1,0 +1,115 @@
+"""GPU tests of the property engine: table splines (THERM_PROP_UPDATE)
+against the FP64 oracle, the MLP training kernels' loss and gradient against
+the FP64 numpy reference, training convergence, the BF16 tensor-core
+inference, the error gate and the out-of-table error path."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _need_gpu():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+@pytest.fixture(scope="module")
+def table():
+    from chapsim1ww_b200.props import synthetic_table
+    return synthetic_table(4096)
+
+
+@pytest.fixture(scope="module")
+def engine(table):
+    _need_gpu()
+    from chapsim1ww_b200 import PropertyEngine
+    return PropertyEngine(*table)
+
+
+def _oracle_update(table, h):
+    from oracle import pyoracle
+    L = pyoracle.load()
+    P = ctypes.c_void_p
+    L.oracle_therm_prop_update.argtypes = [ctypes.c_int] + [P] * 5 + [ctypes.c_int64] + [P] * 5
+    L.oracle_therm_prop_update.restype = ctypes.c_int64
+    H, T, D, M, K, _ = [np.ascontiguousarray(c) for c in table]
+    out = [np.full(len(h), -7.0) for _ in range(4)]
+    bad = L.oracle_therm_prop_update(len(H), H.ctypes.data, T.ctypes.data, D.ctypes.data, M.ctypes.data,
+                                     K.ctypes.data, len(h), h.ctypes.data, *[o.ctypes.data for o in out])
+    return bad, out
+
+
+def test_table_update_matches_oracle(engine, table):
+    import torch
+    rng = np.random.default_rng(3)
+    h = rng.uniform(-0.9999, 0.9999, 200_000)
+    h[:7] = [0.0, 3e-11, -5e-11, 0.1, -0.1, 0.5, H1 := table[0][1] * 0.5 + table[0][2] * 0.5]
+    bad_o, (To, Do, Mo, Ko) = _oracle_update(table, h)
+    assert bad_o == 0
+    dev = lambda a: torch.tensor(a, dtype=torch.float64, device="cuda")
+    hd = dev(h)
+    T, rho, mu, k = (dev(np.full(len(h), -7.0)) for _ in range(4))
+    engine.update(hd, T, rho, mu, k)
+    for g, o in ((T, To), (rho, Do), (mu, Mo), (k, Ko)):
+        g = g.cpu().numpy()
+        assert np.abs(g - o).max() <= 1e-13 * np.abs(o).max()
+    assert T[0].item() == -7.0 and T[1].item() == -7.0  # |h| < 1e-10 left unchanged
+
+
+def test_out_of_table_is_an_error(engine):
+    import torch
+    from chapsim1ww_b200 import ChapsimError
+    h = torch.tensor([0.2, 1.2, -3.0, 1.0], dtype=torch.float64, device="cuda")
+    outs = [torch.full((4,), -7.0, dtype=torch.float64, device="cuda") for _ in range(4)]
+    with pytest.raises(ChapsimError) as e:
+        engine.update(h, *outs)
+    assert "RANGE" in str(e.value)
+    assert engine.update(h, *outs, raise_on_range=False) == 3
+    assert outs[0][1].item() == -7.0 and outs[0][0].item() != -7.0
+
+
+def test_loss_and_gradient_match_fp64_reference(engine):
+    from oracle import mlp_ref
+    rng = np.random.default_rng(7)
+    p = rng.normal(0, 0.3, mlp_ref.NPARAM).astype(np.float32)
+    norm = np.array([0.0, 1.0] + [0.0] * 5 + [1.0] * 5)
+    engine.set_params(p, norm)
+    x = rng.uniform(-1, 1, 300).astype(np.float32)
+    t = rng.normal(0, 1, (300, 5)).astype(np.float32)
+    loss, g = engine.loss_grad(x, t)
+    lr, gr = mlp_ref.loss_and_grad(p.astype(np.float64), x.astype(np.float64), t.astype(np.float64))
+    assert abs(loss - lr) <= 1e-5 * lr
+    assert np.linalg.norm(g - gr) <= 2e-4 * np.linalg.norm(gr)
+    assert np.abs(g - gr).max() <= 1e-3 * np.abs(gr).max()
+
+
+def test_training_and_tensor_core_inference(engine, table):
+    import torch
+    from oracle import mlp_ref
+    loss = engine.train(nsamples=65536, seed=2, steps=1500, lr=3e-3)
+    assert loss < 2e-3, loss
+    p, norm = engine.get_params()
+    rng = np.random.default_rng(11)
+    h = rng.uniform(-0.999, 0.999, 4096)
+    # MLP everywhere (gate with an infinite bound), compare with the FP64 forward
+    nb, worst = engine.gate(tol=1e9, nbins=64)
+    assert nb == 64
+    hd = torch.tensor(h, dtype=torch.float64, device="cuda")
+    outs = [torch.zeros(4096, dtype=torch.float64, device="cuda") for _ in range(5)]
+    engine.update(hd, *outs[:4], cp=outs[4], mode=1)
+    y, _ = mlp_ref.forward(p.astype(np.float64), (h - norm[0]) / norm[1])
+    ref = y * norm[7:12] + norm[2:7]
+    for o in range(5):
+        got = outs[o].cpu().numpy()
+        assert np.abs(got - ref[:, o]).max() <= 3e-2 * np.abs(ref[:, o]).max(), o  # BF16 weights/activations
+    # gate with a zero bound: every bin falls back to the table splines
+    nb, _ = engine.gate(tol=0.0, nbins=64)
+    assert nb == 0
+    tab = [torch.zeros(4096, dtype=torch.float64, device="cuda") for _ in range(4)]
+    engine.update(hd, *tab)
+    engine.update(hd, *outs[:4], mode=1)
+    for a, b in zip(outs[:4], tab):
+        assert torch.equal(a, b)
