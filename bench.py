@@ -36,6 +36,8 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     # TG section of the coupled TG+IO configuration
     "tg_256x192x256": dict(nx=256, ny=192, nz=256, lx=4 * math.pi, lz=4 * math.pi / 3, ren=2800.0, dt=1e-3, seed=1),
+    # 64 independent TG channels of uneven sizes (seed 3), mixed precision
+    "batch64": dict(batch=True, seed=3),
     # the CPU-runnable plain-method configuration
     "tg_64x64x64": dict(nx=64, ny=64, nz=64, lx=4 * math.pi, lz=4 * math.pi / 3, ren=2800.0, dt=1e-3, seed=0),
 }
@@ -222,6 +224,52 @@ def run_reference(args, wl, ws, rank):
     return 0
 
 
+def run_batch(args, wl, ws, rank, local):
+    """64 uneven channels advanced by one graph launch per step."""
+    import torch
+
+    import chapsim1ww_b200 as cs
+    from chapsim1ww_b200 import ChannelBatch, batch64_configs
+
+    torch.cuda.set_device(local)
+    prec = cs.FP64 if args.precision == "fp64" else cs.MIXED
+    cfgs = batch64_configs(seed=wl["seed"] + rank)
+    b = ChannelBatch(cfgs, precision=prec, device=local)
+    t0 = time.perf_counter()
+    b.autotune(reps=3)
+    t_tune = time.perf_counter() - t0
+    b.init_random(seed=wl["seed"], amp=0.1, project=True)
+    b.step(args.warmup)
+    b.sync()
+    stream = torch.cuda.ExternalStream(b.stream(), device=local)
+    clocks = ClockSampler(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    b.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    divmax = max(ch.divgck_tg() for ch in b.channels)
+    value = b.cells * args.steps / (ms / 1000.0)
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if prec == cs.FP64 else "f64 state / f32 temporaries",
+        "data": "synthetic (64 channels, sizes and Re drawn from seed 3)",
+        "config": {"workload": "batch64", "channels": len(cfgs), "cells": b.cells, "precision": args.precision,
+                   "graph": "one CUDA graph launch per step, channels as parallel branches",
+                   "autotune_s": t_tune},
+        "max_div_u": divmax, "gpu_launches": b.kernels_per_step() * args.steps, "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    b.close()
+    return 0
+
+
 def run_ours(args, wl, ws, rank, local):
     import numpy as np
     import torch
@@ -399,6 +447,8 @@ def main():
     ws, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference(args, wl, ws, rank)
+    if wl.get("batch"):
+        return run_batch(args, wl, ws, rank, local)
     return run_ours(args, wl, ws, rank, local)
 
 

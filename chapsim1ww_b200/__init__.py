@@ -7,3 +7,4 @@ call goes to libchapsim.so (hand-written CUDA).  There is no CPU fallback.
 from ._lib import FP64, MIXED, ITG, IIO, load  # noqa: F401
 from .solver import TGChannel, ChapsimError, default_config  # noqa: F401
 from .props import PropertyEngine, synthetic_table  # noqa: F401
+from .batch import ChannelBatch, batch64_configs  # noqa: F401

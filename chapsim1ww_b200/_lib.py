@@ -74,6 +74,18 @@ SIGNATURES = [
     ("chapsim_props_set_params", _I, [_P, _P, _I, _P, _I]),
     ("chapsim_props_loss_grad", _I, [_P, _P, _P, _I, _DP, _P, _I]),
 ]
+SIGNATURES += [
+    ("chapsim_batch_create", _I, [ctypes.POINTER(ChapsimConfig), _I, ctypes.POINTER(_P)]),
+    ("chapsim_batch_destroy", _I, [_P]),
+    ("chapsim_batch_last_error", ctypes.c_char_p, [_P]),
+    ("chapsim_batch_channel", _I, [_P, _I, ctypes.POINTER(_P)]),
+    ("chapsim_batch_init_random", _I, [_P, ctypes.c_uint64, _D, _I]),
+    ("chapsim_batch_autotune", _I, [_P, _I]),
+    ("chapsim_batch_step", _I, [_P, _I]),
+    ("chapsim_batch_sync", _I, [_P]),
+    ("chapsim_batch_get_stream", _I, [_P, ctypes.POINTER(_P)]),
+    ("chapsim_batch_kernels_per_step", _I, [_P, ctypes.POINTER(_I64)]),
+]
 PROPS_TABLE, PROPS_MLP = 0, 1
 ERR_RANGE = 8
 ERRORS[8] = "CHAPSIM_ERR_RANGE"

@@ -106,7 +106,8 @@ struct chapsim_ctx {
   bool allow_band = true;   // banded x/z inverses when narrow enough
   bool fft_big = false;     // FFT plans with radix 7 or 11
   bool refine = true;       // mixed form: one FP64-residual refinement sweep
-  int rhs_nzc = 16;
+  int rhs_nzc = 16;   // z planes per block of k_rhs_tma (autotunable)
+  int fft_lb = 0;     // rows per block of the x transforms (0: default)
   // CUDA graph of one full step (NS = 1, 2, 3)
   cudaGraphExec_t step_graph = nullptr;
   int64_t kernels_per_step = 0;

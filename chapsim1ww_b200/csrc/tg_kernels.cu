@@ -1037,6 +1037,17 @@ int flush_phase_events(chapsim_ctx *c) {
 
 template <typename T> struct Prec {
   typedef typename Cplx<T>::type C;
+  static int max_fftx_lb(int nx) {
+    int lb = (int)(96 * 1024 / ((size_t)nx * sizeof(C)));
+    lb = lb & ~1;
+    if (lb > 32) lb = 32;
+    if (lb < 2) lb = 2;
+    return lb;
+  }
+  static int fftx_lb(const chapsim_ctx *c) {
+    if (c->fft_lb >= 2 && c->fft_lb <= max_fftx_lb(c->d.nx)) return c->fft_lb & ~1;
+    return fftx_lb(c->d.nx);
+  }
   static int fftx_lb(int nx) {
     // rows per block of the x transforms: two complex buffers of lb/2 lines
     int lb = (int)(96 * 1024 / ((size_t)nx * sizeof(C)));
@@ -1068,35 +1079,34 @@ template <typename T> struct Prec {
   }
   static size_t rhs_tma_smem() { return RtLayout<T>::smem_bytes; }
 
+  // Dynamic shared-memory limits are per kernel and process wide, so they are
+  // raised once to the device's opt-in maximum rather than to one context's
+  // sizes (a later, smaller context must not lower them for earlier ones).
   static int init(chapsim_ctx *c) {
-    const int nx = c->d.nx, ny = c->d.ny, nz = c->d.nz;
-    if (c->use_tma_rhs) {
-      CK(cudaFuncSetAttribute(k_rhs_tma<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rhs_tma_smem()));
-      CK(cudaFuncSetAttribute(k_rhs_tma<T>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-    }
-    CK(cudaFuncSetAttribute(k_adix<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adix_smem(nx, adix_lb(nx))));
-    CK(cudaFuncSetAttribute(k_adiz<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adiz_smem(nz)));
-    CK(cudaFuncSetAttribute(k_fftx<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftx_smem(nx, fftx_lb(nx))));
-    CK(cudaFuncSetAttribute(k_ifftx<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftx_smem(nx, fftx_lb(nx))));
-    CK(cudaFuncSetAttribute(k_fftz<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftz_smem(nz, fftz_lz(nz))));
-    CK(cudaFuncSetAttribute(k_fftx<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftx_smem(nx, fftx_lb(nx))));
-    CK(cudaFuncSetAttribute(k_ifftx<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftx_smem(nx, fftx_lb(nx))));
-    CK(cudaFuncSetAttribute(k_fftz<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fftz_smem(nz, fftz_lz(nz))));
+    const int ny = c->d.ny;
     if (adiy_smem(ny) > 200 * 1024) {
       c->err = "ny too large for the shared-memory y-line kernels";
       return CHAPSIM_ERR_UNSUPPORTED;
     }
-    CK(cudaFuncSetAttribute(k_adiy_smem<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)adiy_smem(ny)));
-    CK(cudaFuncSetAttribute(k_adixz_band<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            (int)band_smem(BAND_WMAX, BAND_WMAX)));
-    CK(cudaFuncSetAttribute(k_adiy_smem<T>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    int maxs = 0;
+    CK(cudaDeviceGetAttribute(&maxs, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+    const void *dyn[] = {(const void *)k_rhs_tma<T>,      (const void *)k_adix<T>,           (const void *)k_adiz<T>,
+                         (const void *)k_fftx<T, false>,  (const void *)k_ifftx<T, false>,   (const void *)k_fftz<T, false>,
+                         (const void *)k_fftx<T, true>,   (const void *)k_ifftx<T, true>,    (const void *)k_fftz<T, true>,
+                         (const void *)k_adiy_smem<T>,    (const void *)k_adixz_band<T>};
+    for (const void *f : dyn) {
+      cudaFuncAttributes fa;
+      CK(cudaFuncGetAttributes(&fa, f));
+      CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs - (int)fa.sharedSizeBytes));
+      CK(cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    }
     return CHAPSIM_OK;
   }
 
   // mode 0: divergence of q; 1: stored RHSLLPHI; 2: residual buffer
   static int fftx(chapsim_ctx *c, int ns, int mode) {
     TGDev &d = c->d;
-    const int lb = fftx_lb(d.nx);
+    const int lb = fftx_lb(c);
     dim3 grid((d.ny + lb - 1) / lb, d.nz);
     if (c->fft_big)
       k_fftx<T, true><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->sp[ns], c->fx, lb, mode);
@@ -1108,7 +1118,7 @@ template <typename T> struct Prec {
 
   static int spectral_solve(chapsim_ctx *c, int accumulate, bool mark) {
     TGDev &d = c->d;
-    const int lz = fftz_lz(d.nz), lb = fftx_lb(d.nx);
+    const int lz = fftz_lz(d.nz), lb = fftx_lb(c);
     if (mark) phase_mark(c, CHAPSIM_PH_FFTZ);
     {
       dim3 grid((d.lh + lz - 1) / lz, d.ny);

@@ -245,6 +245,34 @@ int chapsim_props_set_params(chapsim_props *pe, const float *params, int nparams
 int chapsim_props_loss_grad(chapsim_props *pe, const float *x, const float *t, int n, double *loss, float *grad,
                             int nparams);
 
+/* ======================================================================
+ * Batched channels: many independent TG channels of uneven sizes advanced
+ * together.  No reference counterpart (the reference runs one domain per
+ * job); each channel is a full chapsim_ctx.  chapsim_batch_step replays ONE
+ * captured CUDA graph per time step that holds every channel's three
+ * substeps as parallel branches, so small channels fill the GPU together.
+ * ====================================================================== */
+typedef struct chapsim_batch chapsim_batch;
+int chapsim_batch_create(const chapsim_config *cfgs, int n, chapsim_batch **out);
+int chapsim_batch_destroy(chapsim_batch *b);
+const char *chapsim_batch_last_error(const chapsim_batch *b);
+/* The i-th channel's context (for fields and reductions); owned by the batch. */
+int chapsim_batch_channel(chapsim_batch *b, int i, chapsim_ctx **ctx);
+/* chapsim_init_random on every channel, channel i with seed + i. */
+int chapsim_batch_init_random(chapsim_batch *b, uint64_t seed, double amp, int project);
+/* Autotuner: for every channel, time each candidate launch shape (z-segment
+ * length of the RHS kernel, rows per block of the x transforms) over `reps`
+ * substeps and keep the fastest.  The channel state is saved before and
+ * restored after the trials. */
+int chapsim_batch_autotune(chapsim_batch *b, int reps);
+/* nsteps time steps of every channel (one graph launch per step). */
+int chapsim_batch_step(chapsim_batch *b, int nsteps);
+int chapsim_batch_sync(chapsim_batch *b);
+/* The stream the batch graph is launched on (a cudaStream_t). */
+int chapsim_batch_get_stream(const chapsim_batch *b, void **stream);
+/* Total kernel launches inside one step's graph. */
+int chapsim_batch_kernels_per_step(const chapsim_batch *b, int64_t *count);
+
 #ifdef __cplusplus
 }
 #endif
