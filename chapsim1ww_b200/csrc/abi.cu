@@ -465,6 +465,7 @@ int chapsim_create(const chapsim_config *cfg, chapsim_ctx **out) {
   setup_mesh(ctx);
   TGDev &d = ctx->d;
   d.nx = cfg->nx; d.ny = cfg->ny; d.nz = cfg->nz; d.lh = cfg->nx / 2 + 1;
+  d.lp = (d.lh + 1) & ~1;
   d.sy = cfg->nx;
   d.sz = (int64_t)cfg->nx * (cfg->ny + 2);
   const size_t n = (size_t)d.sz * cfg->nz;
@@ -486,7 +487,7 @@ int chapsim_create(const chapsim_config *cfg, chapsim_ctx **out) {
         cudaMemsetAsync(p, 0, n * tsz, ctx->stream);
       }
     }
-    const size_t ns = (size_t)d.lh * cfg->ny * cfg->nz;
+    const size_t ns = (size_t)d.lp * cfg->ny * cfg->nz;
     if ((rc = dalloc(ctx, &p, ns * (mixed ? sizeof(float2) : sizeof(double2))))) goto fail;
     d.spec = p;
     if ((rc = dalloc(ctx, &p, ns * sizeof(double2)))) goto fail;
@@ -798,6 +799,24 @@ int chapsim_phase_reset(chapsim_ctx *ctx) {
   if (rc) return rc;
   for (double &m : ctx->phase_ms) m = 0.0;
   ctx->timed_substeps = 0;
+  return CHAPSIM_OK;
+}
+
+int chapsim_set_tuning(chapsim_ctx *ctx, int rhs_nzc, int fft_lb) {
+  if (!ctx || rhs_nzc < 1 || fft_lb < 0 || fft_lb > 64 || (fft_lb & 1)) return CHAPSIM_ERR_ARG;
+  ctx->rhs_nzc = rhs_nzc;
+  ctx->fft_lb = fft_lb;
+  if (ctx->step_graph) {
+    cudaGraphExecDestroy(ctx->step_graph);
+    ctx->step_graph = nullptr;
+  }
+  return CHAPSIM_OK;
+}
+
+int chapsim_get_tuning(const chapsim_ctx *ctx, int *rhs_nzc, int *fft_lb) {
+  if (!ctx || !rhs_nzc || !fft_lb) return CHAPSIM_ERR_ARG;
+  *rhs_nzc = ctx->rhs_nzc;
+  *fft_lb = ctx->fft_lb;
   return CHAPSIM_OK;
 }
 

@@ -15,9 +15,10 @@ namespace chapsim {
 // Device-side parameters of one TG domain, passed by value to every kernel.
 // Index convention: field(i, j, k) at i + nx*(j + (ny+2)*k), i in [0,nx),
 // j in [0,ny+1] (j = 0 and ny+1 are the wall ghost layers), k in [0,nz).
-// Spectral data: S(kx, j, kz) at kx + lh*((j-1) + ny*kz), kx in [0,lh).
+// Spectral data: S(kx, j, kz) at kx + lp*((j-1) + ny*kz), kx in [0,lh).
 struct TGDev {
   int nx, ny, nz, lh;
+  int lp;          // pitch of a spectral row: lh rounded up to even (16-byte rows)
   int64_t sy, sz;  // strides of j and k in a field
   // FP64 state
   double *u, *v, *w, *p, *phi, *rhsphi;

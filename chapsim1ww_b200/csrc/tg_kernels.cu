@@ -702,39 +702,82 @@ __global__ void __launch_bounds__(128) k_adiy_smem(TGDev d, SubParams sp, int fr
 
 // ============================================================ Poisson
 // DIVG_tg (src/DIVG.f90:21-57) fused with the forward real transform along x
-// of FFT99_POIS3D_periodicxz (src/possion3d_FFT99.f90:265-318): rows j of
-// plane k are packed in pairs as one complex line, transformed, separated and
-// scaled by 1/nx.  mode 0 computes the divergence (and stores RHSLLPHI);
-// mode 1 transforms the stored RHSLLPHI.
+// of FFT99_POIS3D_periodicxz (src/possion3d_FFT99.f90:265-318).  A block owns
+// lb consecutive rows j of plane k.  Its inputs arrive by bulk copies
+// (cp.async.bulk, one per array: u rows, v rows plus one, w rows of planes k
+// and k+1, all contiguous in memory) completed on one mbarrier; the
+// divergence is formed in shared memory, rows are packed in pairs as complex
+// lines, transformed, separated and scaled by 1/nx.  mode 0 computes the
+// divergence (and stores RHSLLPHI); mode 1 transforms the stored RHSLLPHI;
+// mode 2 the Poisson residual.
+__host__ __device__ constexpr size_t align128(size_t b) { return (b + 127) & ~(size_t)127; }
+template <typename C> __host__ __device__ constexpr size_t fftx_smem_bytes(int nx, int lb) {
+  return align128((size_t)(lb / 2) * nx * sizeof(C)) + (size_t)(4 * lb + 1) * nx * sizeof(double);
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"((uint64_t)src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
 template <typename T, bool BIG>
 __global__ void __launch_bounds__(256, 2) k_fftx(TGDev d, SubParams sp, FFTPlan pl, int lb, int mode) {
   typedef typename Cplx<T>::type C;
   extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t bar;
+  __shared__ int rad[16];
   const int nx = d.nx, ny = d.ny, lh = d.lh;
   const int k = blockIdx.y;
   const int jbeg = 1 + blockIdx.x * lb;
   const int nrow = min(lb, ny - jbeg + 1);
   const int nl = lb / 2;
+  const int tid = threadIdx.x;
   C *A = reinterpret_cast<C *>(smem_raw);
-  C *B = A + nl * nx;
-  __shared__ int rad[16];
-  if (threadIdx.x < 16) rad[threadIdx.x] = pl.rad[threadIdx.x];
-  const double coe0 = 1.0 / (d.dt * sp.alp);
+  double *in = reinterpret_cast<double *>(smem_raw + align128((size_t)nl * nx * sizeof(C)));
+  C *B = reinterpret_cast<C *>(in);  // FFT scratch, reuses the input area once A is filled
+  double *U = in, *V = in + (size_t)lb * nx, *W0 = V + (size_t)(lb + 1) * nx, *W1 = W0 + (size_t)lb * nx;
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  if (tid < 16) rad[tid] = pl.rad[tid];
+  __syncthreads();
   const int kp = wrapp(k, d.nz);
-  for (int t = threadIdx.x; t < lb * nx; t += blockDim.x) {
+  const uint32_t rowb = (uint32_t)nx * sizeof(double);
+  const int64_t row0 = d.sy * jbeg;
+  if (tid == 0) {
+    if (mode == 0) {
+      mbar_expect_tx(&bar, (4 * nrow + 1) * rowb);
+      bulk_g2s(U, d.u + row0 + d.sz * k, nrow * rowb, &bar);
+      bulk_g2s(V, d.v + row0 + d.sz * k, (nrow + 1) * rowb, &bar);
+      bulk_g2s(W0, d.w + row0 + d.sz * k, nrow * rowb, &bar);
+      bulk_g2s(W1, d.w + row0 + d.sz * kp, nrow * rowb, &bar);
+    } else {
+      mbar_expect_tx(&bar, nrow * rowb);
+      bulk_g2s(U, (mode == 1 ? d.rhsphi : d.res) + row0 + d.sz * k, nrow * rowb, &bar);
+    }
+  }
+  if (!mbar_wait(&bar, 0, d.err)) {
+    mbar_wait(&bar, 0, d.err);  // let copies in flight land before the block exits
+    return;
+  }
+  const double coe0 = 1.0 / (d.dt * sp.alp);
+  for (int t = tid; t < lb * nx; t += blockDim.x) {
     const int r = t / nx, i = t - r * nx;
-    const int j = jbeg + r;
     double val = 0.0;
     if (r < nrow) {
-      const int64_t c0 = i + d.sy * j + d.sz * k;
       if (mode == 0) {
         const int ip = wrapp(i, nx);
-        const double dv = (d.u[c0 + (ip - i)] - d.u[c0]) * d.dxi + (d.v[c0 + d.sy] - d.v[c0]) * d.dyfi[j] +
-                          (d.w[c0 + d.sz * (kp - k)] - d.w[c0]) * d.dzi;
+        const int j = jbeg + r;
+        const double dv = (U[r * nx + ip] - U[r * nx + i]) * d.dxi + (V[(r + 1) * nx + i] - V[r * nx + i]) * d.dyfi[j] +
+                          (W1[r * nx + i] - W0[r * nx + i]) * d.dzi;
         val = dv * coe0;
-        d.rhsphi[c0] = val;
+        d.rhsphi[row0 + d.sz * k + (int64_t)r * nx + i] = val;
       } else {
-        val = mode == 1 ? d.rhsphi[c0] : d.res[c0];
+        val = U[r * nx + i];
       }
     }
     C *z = A + (r >> 1) * nx + i;
@@ -744,7 +787,7 @@ __global__ void __launch_bounds__(256, 2) k_fftx(TGDev d, SubParams sp, FFTPlan 
   C *res = fft_lines<C, BIG>(A, B, nl, nx, nx, rad, pl.nrad, (const C *)(sizeof(T) == 8 ? (const void *)pl.tw64 : (const void *)pl.tw32), -1);
   const T scale = (T)(1.0 / nx);
   C *S = reinterpret_cast<C *>(d.spec);
-  for (int t = threadIdx.x; t < nl * lh; t += blockDim.x) {
+  for (int t = tid; t < nl * lh; t += blockDim.x) {
     const int p = t / lh, kx = t - p * lh;
     const C z = res[p * nx + kx];
     const C zc = cconj(res[p * nx + (kx == 0 ? 0 : nx - kx)]);
@@ -755,8 +798,8 @@ __global__ void __launch_bounds__(256, 2) k_fftx(TGDev d, SubParams sp, FFTPlan 
     x1.x = (T)0.5 * (z.y - zc.y) * scale;
     x1.y = (T)-0.5 * (z.x - zc.x) * scale;
     const int r0 = 2 * p;
-    if (r0 < nrow) S[kx + (int64_t)lh * ((jbeg + r0 - 1) + (int64_t)ny * k)] = x0;
-    if (r0 + 1 < nrow) S[kx + (int64_t)lh * ((jbeg + r0) + (int64_t)ny * k)] = x1;
+    if (r0 < nrow) S[kx + (int64_t)d.lp * ((jbeg + r0 - 1) + (int64_t)ny * k)] = x0;
+    if (r0 + 1 < nrow) S[kx + (int64_t)d.lp * ((jbeg + r0) + (int64_t)ny * k)] = x1;
   }
 }
 
@@ -776,8 +819,8 @@ __global__ void __launch_bounds__(256, 2) k_fftz(TGDev d, FFTPlan pl, int lz, in
   C *B = A + lz * ld;
   __shared__ int rad[16];
   if (threadIdx.x < 16) rad[threadIdx.x] = pl.rad[threadIdx.x];
-  C *S = reinterpret_cast<C *>(d.spec) + kx0 + (int64_t)lh * (j - 1);
-  const int64_t skz = (int64_t)lh * ny;
+  C *S = reinterpret_cast<C *>(d.spec) + kx0 + (int64_t)d.lp * (j - 1);
+  const int64_t skz = (int64_t)d.lp * ny;
   for (int t = threadIdx.x; t < nz * lz; t += blockDim.x) {
     const int kz = t / lz, l = t - kz * lz;
     C v;
@@ -810,7 +853,7 @@ __global__ void k_ypivots(TGDev d) {
   const int kx = blockIdx.x * blockDim.x + threadIdx.x;
   const int kz = blockIdx.y;
   if (kx >= lh) return;
-  double2 *P = d.ypiv + kx + (int64_t)lh * ny * kz;
+  double2 *P = d.ypiv + kx + (int64_t)d.lp * ny * kz;
   const double shift = d.ak1[kx] + d.ak3[kz];
   const bool mean = (kx == 0 && kz == 0);
   double b = d.acph[1] - shift;
@@ -821,7 +864,7 @@ __global__ void k_ypivots(TGDev d) {
     b = d.acph[j] - shift;
     pp = 1.0 / (b - h * d.amph[j]);
     h = j < ny ? d.apph[j] * pp : 0.0;
-    P[(int64_t)lh * (j - 1)] = make_double2(pp, h);
+    P[(int64_t)d.lp * (j - 1)] = make_double2(pp, h);
   }
 }
 
@@ -837,9 +880,9 @@ __global__ void __launch_bounds__(128) k_ysolve_line(TGDev d) {
   const int lh = d.lh, ny = d.ny;
   const int kx = blockIdx.x * blockDim.x + threadIdx.x, kz = blockIdx.y;
   if (kx >= lh) return;
-  C *S = reinterpret_cast<C *>(d.spec) + kx + (int64_t)lh * ny * kz;
-  const double2 *P = d.ypiv + kx + (int64_t)lh * ny * kz;
-  const int64_t st = lh;
+  C *S = reinterpret_cast<C *>(d.spec) + kx + (int64_t)d.lp * ny * kz;
+  const double2 *P = d.ypiv + kx + (int64_t)d.lp * ny * kz;
+  const int64_t st = d.lp;
   C r = S[0];
   double2 pv = P[0];
   double gr = (double)r.x * pv.x, gi = (double)r.y * pv.x;
@@ -864,30 +907,52 @@ __global__ void __launch_bounds__(128) k_ysolve_line(TGDev d) {
   }
 }
 
-// Inverse real transform along x (src/possion3d_FFT99.f90:461-485): pairs of
-// rows rebuilt as one complex Hermitian-extended line; phi ghosts copied
-// (BC_WALL_DPH, src/BC_WALL.f90:342-364).
+// Inverse real transform along x (src/possion3d_FFT99.f90:461-485): the
+// block's lb spectral rows (contiguous, pitch lp) arrive by one bulk copy;
+// pairs of rows are rebuilt as one complex Hermitian-extended line and
+// transformed; phi ghosts copied (BC_WALL_DPH, src/BC_WALL.f90:342-364).
+// accumulate != 0 adds the result to phi (refinement sweep).
+template <typename C> __host__ __device__ constexpr size_t ifftx_smem_bytes(int nx, int lp, int lb) {
+  return align128((size_t)lb * lp * sizeof(C)) + 2 * align128((size_t)(lb / 2) * nx * sizeof(C));
+}
+
 template <typename T, bool BIG>
 __global__ void __launch_bounds__(256, 2) k_ifftx(TGDev d, FFTPlan pl, int lb, int accumulate) {
   typedef typename Cplx<T>::type C;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  const int nx = d.nx, ny = d.ny, lh = d.lh;
+  __shared__ uint64_t bar;
+  __shared__ int rad[16];
+  const int nx = d.nx, ny = d.ny, lh = d.lh, lp = d.lp;
   const int k = blockIdx.y;
   const int jbeg = 1 + blockIdx.x * lb;
   const int nrow = min(lb, ny - jbeg + 1);
   const int nl = lb / 2;
-  C *A = reinterpret_cast<C *>(smem_raw);
-  C *B = A + nl * nx;
-  __shared__ int rad[16];
-  if (threadIdx.x < 16) rad[threadIdx.x] = pl.rad[threadIdx.x];
-  const C *S = reinterpret_cast<const C *>(d.spec);
-  for (int t = threadIdx.x; t < nl * lh; t += blockDim.x) {
+  const int tid = threadIdx.x;
+  C *SP = reinterpret_cast<C *>(smem_raw);
+  C *A = reinterpret_cast<C *>(smem_raw + align128((size_t)lb * lp * sizeof(C)));
+  C *B = reinterpret_cast<C *>(reinterpret_cast<unsigned char *>(A) + align128((size_t)nl * nx * sizeof(C)));
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  if (tid < 16) rad[tid] = pl.rad[tid];
+  __syncthreads();
+  if (tid == 0) {
+    const uint32_t bytes = (uint32_t)(nrow * lp * sizeof(C));
+    mbar_expect_tx(&bar, bytes);
+    bulk_g2s(SP, reinterpret_cast<const C *>(d.spec) + (int64_t)lp * ((jbeg - 1) + (int64_t)ny * k), bytes, &bar);
+  }
+  if (!mbar_wait(&bar, 0, d.err)) {
+    mbar_wait(&bar, 0, d.err);
+    return;
+  }
+  for (int t = tid; t < nl * lh; t += blockDim.x) {
     const int p = t / lh, kx = t - p * lh;
     const int r0 = 2 * p;
     C x0, x1;
     x0.x = 0; x0.y = 0; x1.x = 0; x1.y = 0;
-    if (r0 < nrow) x0 = S[kx + (int64_t)lh * ((jbeg + r0 - 1) + (int64_t)ny * k)];
-    if (r0 + 1 < nrow) x1 = S[kx + (int64_t)lh * ((jbeg + r0) + (int64_t)ny * k)];
+    if (r0 < nrow) x0 = SP[r0 * lp + kx];
+    if (r0 + 1 < nrow) x1 = SP[(r0 + 1) * lp + kx];
     if (kx == 0 || 2 * kx == nx) { x0.y = 0; x1.y = 0; }
     // Z(k) = X0 + i X1 ; Z(n-k) = conj(X0) + i conj(X1)
     C z; z.x = x0.x - x1.y; z.y = x0.y + x1.x;
@@ -899,7 +964,7 @@ __global__ void __launch_bounds__(256, 2) k_ifftx(TGDev d, FFTPlan pl, int lb, i
   }
   __syncthreads();
   C *res = fft_lines<C, BIG>(A, B, nl, nx, nx, rad, pl.nrad, (const C *)(sizeof(T) == 8 ? (const void *)pl.tw64 : (const void *)pl.tw32), +1);
-  for (int t = threadIdx.x; t < nrow * nx; t += blockDim.x) {
+  for (int t = tid; t < nrow * nx; t += blockDim.x) {
     const int r = t / nx, i = t - r * nx;
     const int j = jbeg + r;
     const C z = res[(r >> 1) * nx + i];
@@ -1038,10 +1103,8 @@ int flush_phase_events(chapsim_ctx *c) {
 template <typename T> struct Prec {
   typedef typename Cplx<T>::type C;
   static int max_fftx_lb(int nx) {
-    int lb = (int)(96 * 1024 / ((size_t)nx * sizeof(C)));
-    lb = lb & ~1;
-    if (lb > 32) lb = 32;
-    if (lb < 2) lb = 2;
+    int lb = 2;
+    while (lb < 32 && fftx_smem_bytes<C>(nx, lb + 2) <= 110 * 1024) lb += 2;
     return lb;
   }
   static int fftx_lb(const chapsim_ctx *c) {
@@ -1049,14 +1112,12 @@ template <typename T> struct Prec {
     return fftx_lb(c->d.nx);
   }
   static int fftx_lb(int nx) {
-    // rows per block of the x transforms: two complex buffers of lb/2 lines
-    int lb = (int)(96 * 1024 / ((size_t)nx * sizeof(C)));
-    lb = lb & ~1;
-    if (lb > 16) lb = 16;
-    if (lb < 2) lb = 2;
-    return lb;
+    // rows per block of the x transforms: the most rows whose bulk-loaded
+    // inputs fit (measured fastest on the 256x192x256 channel)
+    return max_fftx_lb(nx);
   }
-  static size_t fftx_smem(int nx, int lb) { return (size_t)lb * nx * sizeof(C); }
+  static size_t fftx_smem(int nx, int lb) { return fftx_smem_bytes<C>(nx, lb); }
+  static size_t ifftx_smem(int nx, int lp, int lb) { return ifftx_smem_bytes<C>(nx, lp, lb); }
   static int fftz_lz(int nz) {
     int lz = (int)(96 * 1024 / ((size_t)2 * (nz + 1) * sizeof(C)));
     if (lz > 16) lz = 16;
@@ -1147,9 +1208,9 @@ template <typename T> struct Prec {
     {
       dim3 grid((d.ny + lb - 1) / lb, d.nz);
       if (c->fft_big)
-        k_ifftx<T, true><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->fx, lb, accumulate);
+        k_ifftx<T, true><<<grid, 256, ifftx_smem(d.nx, d.lp, lb), c->stream>>>(d, c->fx, lb, accumulate);
       else
-        k_ifftx<T, false><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->fx, lb, accumulate);
+        k_ifftx<T, false><<<grid, 256, ifftx_smem(d.nx, d.lp, lb), c->stream>>>(d, c->fx, lb, accumulate);
       LAUNCHED();
     }
     return CHAPSIM_OK;

@@ -166,6 +166,14 @@ class TGChannel:
     def phase_reset(self):
         self._chk(self.lib.chapsim_phase_reset(self.h))
 
+    def set_tuning(self, rhs_nzc=16, fft_lb=0):
+        self._chk(self.lib.chapsim_set_tuning(self.h, rhs_nzc, fft_lb))
+
+    def get_tuning(self):
+        a, b = ctypes.c_int(), ctypes.c_int()
+        self._chk(self.lib.chapsim_get_tuning(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
     def launch_count(self):
         n = ctypes.c_int64()
         self._chk(self.lib.chapsim_launch_count(self.h, ctypes.byref(n)))

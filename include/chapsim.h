@@ -175,6 +175,13 @@ int chapsim_phase_timing(chapsim_ctx *ctx, int enable);
 int chapsim_phase_times(chapsim_ctx *ctx, double *ms, int n, int64_t *substeps);
 int chapsim_phase_reset(chapsim_ctx *ctx);
 
+/* Launch-shape tuning of one context: z planes per block of the RHS kernel
+ * (rhs_nzc) and rows per block of the x transforms (fft_lb, 0 = default).
+ * Results do not depend on fft_lb; rhs_nzc changes only the block order of
+ * the mass-flux sum (round-off level). */
+int chapsim_set_tuning(chapsim_ctx *ctx, int rhs_nzc, int fft_lb);
+int chapsim_get_tuning(const chapsim_ctx *ctx, int *rhs_nzc, int *fft_lb);
+
 /* Number of kernel launches the library issued on this context since creation
  * (or the last reset). */
 int chapsim_launch_count(const chapsim_ctx *ctx, int64_t *count);
