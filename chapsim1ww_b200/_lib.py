@@ -88,9 +88,14 @@ SIGNATURES += [
     ("chapsim_batch_get_stream", _I, [_P, ctypes.POINTER(_P)]),
     ("chapsim_batch_kernels_per_step", _I, [_P, ctypes.POINTER(_I64)]),
 ]
+SIGNATURES += [
+    ("chapsim_divmax_noalloc", _I, [_P, _P, _P, _P, _I, _I, _I, _D, _D, _P, _P]),
+]
 PROPS_TABLE, PROPS_MLP = 0, 1
 ERR_RANGE = 8
 ERRORS[8] = "CHAPSIM_ERR_RANGE"
+ERRORS[9] = "CHAPSIM_ERR_TOO_LARGE"
+ERR_TOO_LARGE = 9
 
 _lib = None
 

@@ -280,6 +280,31 @@ int chapsim_batch_get_stream(const chapsim_batch *b, void **stream);
 /* Total kernel launches inside one step's graph. */
 int chapsim_batch_kernels_per_step(const chapsim_batch *b, int64_t *count);
 
+/* ======================================================================
+ * Allocation-free check.  No counterpart in the reference: it is the
+ * DIVGCK_tg maximum (src/DIVGCK.f90:16-58) offered without a context for
+ * callers that may not allocate device memory when they need the check --
+ * e.g. a host recording its time step into its own CUDA graph (no cudaMalloc
+ * while a stream is captured) or a host whose device memory is a fixed pool
+ * managed by its own allocator.
+ *
+ * max |div u| of caller-owned device arrays u, v, w (Fortran layout
+ * F(1:nx, 0:ny+1, 1:nz)) with dyfi[j] = DYFI(j) at index j (length >= ny+1),
+ * written to *out (a device pointer), on `stream` (a cudaStream_t, NULL for
+ * the default stream); the call does not synchronise.  Scratch: one
+ * file-scope device array of 65,536 tile maxima (512 KiB, held by every GPU
+ * that loads the library until exit), enough for channels of up to 65,536
+ * tiles of 32 x 8 (x, y) cells summed over the z planes (for example
+ * 256 x 256 x 256); larger channels return CHAPSIM_ERR_TOO_LARGE.  No
+ * cudaMalloc, cudaFree or other allocation.  The first call on a device looks
+ * up the scratch address with that device current, so make it before any
+ * stream capture.  All calls share the scratch (it keeps the last call's
+ * tile maxima; every slot a call reads it writes first), so calls that
+ * overlap on the GPU race. */
+#define CHAPSIM_ERR_TOO_LARGE 9
+int chapsim_divmax_noalloc(const double *u, const double *v, const double *w, const double *dyfi, int nx, int ny,
+                           int nz, double dxi, double dzi, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
