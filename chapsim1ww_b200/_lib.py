@@ -33,6 +33,20 @@ class ChapsimConfig(ctypes.Structure):
     ]
 
 
+class ChapsimIOConfig(ctypes.Structure):
+    """Mirror of ``chapsim_io_config`` in include/chapsim.h."""
+    _fields_ = [
+        ("struct_size", ctypes.c_int32), ("thermal", ctypes.c_int32), ("prt", ctypes.c_double),
+        ("qw_bot", ctypes.c_double), ("qw_top", ctypes.c_double), ("gravdir", ctypes.c_int32),
+        ("pad", ctypes.c_int32), ("f_a", ctypes.c_double),
+    ]
+
+
+# IO domain field and reduction ids
+F_GX, F_GY, F_GZ, F_G0X, F_G0Y, F_G0Z = 10, 11, 12, 13, 14, 15
+F_H, F_T, F_RHO, F_MU, F_K, F_RHOH, F_RHO0, F_MU0, F_DRHO, F_RHSE0 = range(16, 26)
+R_DIVMAX_Q, R_BULK_G, R_BULK_H, R_BADCELLS = 3, 4, 5, 6
+
 # (name, restype, argtypes) for every symbol declared in include/chapsim.h
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -90,6 +104,14 @@ SIGNATURES += [
 ]
 SIGNATURES += [
     ("chapsim_divmax_noalloc", _I, [_P, _P, _P, _P, _I, _I, _I, _D, _D, _P, _P]),
+]
+SIGNATURES += [
+    ("chapsim_io_config_default", _I, [ctypes.POINTER(ChapsimIOConfig)]),
+    ("chapsim_create_io", _I, [ctypes.POINTER(ChapsimConfig), ctypes.POINTER(ChapsimIOConfig), ctypes.POINTER(_P)]),
+    ("chapsim_set_table", _I, [_P, _P, _P, _P, _P, _P, _I, _I]),
+    ("chapsim_rk3_eng_io", _I, [_P, _I]),
+    ("chapsim_rk3_mom_io", _I, [_P, _I]),
+    ("chapsim_step_io", _I, [_P, _I]),
 ]
 PROPS_TABLE, PROPS_MLP = 0, 1
 ERR_RANGE = 8

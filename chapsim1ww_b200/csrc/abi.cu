@@ -149,6 +149,10 @@ int chapsim_config_default(chapsim_config *cfg) {
 static void free_all(chapsim_ctx *ctx) {
   if (ctx->step_graph) cudaGraphExecDestroy(ctx->step_graph);
   ctx->step_graph = nullptr;
+  for (auto &g : ctx->io_graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  for (void *p : ctx->table_allocs) cudaFree(p);
+  ctx->table_allocs.clear();
   for (void *p : ctx->allocs) cudaFree(p);
   ctx->allocs.clear();
   for (auto &e : ctx->ev)
@@ -426,7 +430,7 @@ static int build_tables(chapsim_ctx *ctx) {
   return CHAPSIM_OK;
 }
 
-int chapsim_create(const chapsim_config *cfg, chapsim_ctx **out) {
+static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg, chapsim_ctx **out) {
   chapsim_ctx *ctx = nullptr;
   if (!cfg || !out) return CHAPSIM_ERR_ARG;
   *out = nullptr;
@@ -446,6 +450,10 @@ int chapsim_create(const chapsim_config *cfg, chapsim_ctx **out) {
   ctx = new chapsim_ctx();
   ctx->cfg = *cfg;
   ctx->device = cfg->device;
+  if (iocfg) {
+    ctx->domain = CHAPSIM_IIO;
+    ctx->iocfg = *iocfg;
+  }
   int rc = CHAPSIM_OK;
   FFTPlan px{}, pz{};
   if (!factor_plan(cfg->nx, px) || !factor_plan(cfg->nz, pz)) {
@@ -482,10 +490,33 @@ int chapsim_create(const chapsim_config *cfg, chapsim_ctx **out) {
     for (int c = 0; c < 3; ++c) {
       void **tmp[] = {&d.h0[c], &d.rhs[c], &d.dq[c]};
       for (void **f : tmp) {
+        if (iocfg && f != &d.h0[c]) continue;  // the IO substep needs EXPLT0 only
         if ((rc = dalloc(ctx, &p, n * tsz))) goto fail;
         *f = p;
         cudaMemsetAsync(p, 0, n * tsz, ctx->stream);
       }
+    }
+    if (iocfg) {
+      IODev &io = ctx->io;
+      double **f64io[] = {&io.g[0][0], &io.g[0][1], &io.g[0][2], &io.g[1][0], &io.g[1][1], &io.g[1][2],
+                          &io.drho, &io.rhoh, &io.h, &io.T, &io.D, &io.D0, &io.mu, &io.mu0, &io.kap, &io.rhse0};
+      for (double **f : f64io) {
+        if ((rc = dalloc(ctx, &p, n * sizeof(double)))) goto fail;
+        *f = (double *)p;
+        cudaMemsetAsync(p, 0, n * sizeof(double), ctx->stream);
+      }
+      if ((rc = dalloc(ctx, &p, sizeof(unsigned long long)))) goto fail;
+      io.bad = (unsigned long long *)p;
+      cudaMemsetAsync(p, 0, sizeof(unsigned long long), ctx->stream);
+      io.thermal = iocfg->thermal ? 1 : 0;
+      io.cthecd = 1.0 / cfg->ren / iocfg->prt;  // CTHECD, src/Flow_State.f90:87
+      io.qw_bot = iocfg->qw_bot;
+      io.qw_top = iocfg->qw_top;
+      io.gravdir = iocfg->gravdir;
+      io.f_a = iocfg->f_a;
+      io.cfgv = cfg->cfgv;
+      io.flowdrvtp = cfg->flowdrvtp;
+      d.pin_last = 1;  // FISHPACK's TRID0 pins the mean mode at the last row
     }
     const size_t ns = (size_t)d.lp * cfg->ny * cfg->nz;
     if ((rc = dalloc(ctx, &p, ns * (mixed ? sizeof(float2) : sizeof(double2))))) goto fail;
@@ -504,6 +535,8 @@ int chapsim_create(const chapsim_config *cfg, chapsim_ctx **out) {
     if ((rc = dalloc(ctx, &p, 16 * sizeof(int)))) goto fail;
     d.err = (int *)p;
     cudaMemsetAsync(p, 0, 16 * sizeof(int), ctx->stream);
+    ctx->io.dpg = d.scal;
+    ctx->io.part = d.partials;
   }
   if ((rc = build_tables(ctx))) goto fail;
   px.tw64 = ctx->fx.tw64; px.tw32 = ctx->fx.tw32;
@@ -511,6 +544,13 @@ int chapsim_create(const chapsim_config *cfg, chapsim_ctx **out) {
   ctx->fx = px;
   ctx->fz = pz;
   if ((rc = init_kernels(ctx))) goto fail;
+  if (iocfg) {
+    // reference property values (thermal off, or before the table is set)
+    IODev &io = ctx->io;
+    double *ones[] = {io.T, io.D, io.D0, io.mu, io.mu0, io.kap};
+    for (double *f : ones)
+      if ((rc = fill_value(ctx, f, n, 1.0))) goto fail;
+  }
   if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { rc = CHAPSIM_ERR_CUDA; goto fail; }
   *out = ctx;
   return CHAPSIM_OK;
@@ -518,6 +558,29 @@ fail:
   free_all(ctx);
   delete ctx;
   return rc;
+}
+
+int chapsim_create(const chapsim_config *cfg, chapsim_ctx **out) { return create_ctx(cfg, nullptr, out); }
+
+int chapsim_io_config_default(chapsim_io_config *io) {
+  if (!io) return CHAPSIM_ERR_ARG;
+  memset(io, 0, sizeof(*io));
+  io->struct_size = (int32_t)sizeof(chapsim_io_config);
+  io->thermal = 1;
+  io->prt = 0.71;
+  io->qw_bot = 1.0;
+  io->qw_top = 1.0;
+  io->gravdir = 0;
+  io->f_a = 0.0;
+  return CHAPSIM_OK;
+}
+
+int chapsim_create_io(const chapsim_config *cfg, const chapsim_io_config *io, chapsim_ctx **out) {
+  if (!cfg || !io || !out) return CHAPSIM_ERR_ARG;
+  if (io->struct_size != (int32_t)sizeof(chapsim_io_config)) return CHAPSIM_ERR_ARG;
+  if (cfg->precision != CHAPSIM_FP64) return CHAPSIM_ERR_UNSUPPORTED;
+  if (!(io->prt > 0) || io->gravdir < 0 || io->gravdir > 3) return CHAPSIM_ERR_ARG;
+  return create_ctx(cfg, io, out);
 }
 
 int chapsim_destroy(chapsim_ctx *ctx) {
@@ -555,8 +618,30 @@ int64_t chapsim_field_len(const chapsim_ctx *ctx) {
 }
 
 static double *field_ptr(chapsim_ctx *ctx, int domain, int field) {
-  if (domain != CHAPSIM_ITG) return nullptr;
+  if (domain != ctx->domain) return nullptr;
   TGDev &d = ctx->d;
+  if (domain == CHAPSIM_IIO) {
+    IODev &io = ctx->io;
+    const int cur = ctx->io_cur;
+    switch (field) {
+      case CHAPSIM_F_GX: return io.g[cur][0];
+      case CHAPSIM_F_GY: return io.g[cur][1];
+      case CHAPSIM_F_GZ: return io.g[cur][2];
+      case CHAPSIM_F_G0X: return io.g[1 - cur][0];
+      case CHAPSIM_F_G0Y: return io.g[1 - cur][1];
+      case CHAPSIM_F_G0Z: return io.g[1 - cur][2];
+      case CHAPSIM_F_H: return io.h;
+      case CHAPSIM_F_T: return io.T;
+      case CHAPSIM_F_RHO: return io.D;
+      case CHAPSIM_F_MU: return io.mu;
+      case CHAPSIM_F_K: return io.kap;
+      case CHAPSIM_F_RHOH: return io.rhoh;
+      case CHAPSIM_F_RHO0: return io.D0;
+      case CHAPSIM_F_MU0: return io.mu0;
+      case CHAPSIM_F_DRHO: return io.drho;
+      case CHAPSIM_F_RHSE0: return io.rhse0;
+    }
+  }
   switch (field) {
     case CHAPSIM_F_U: return d.u;
     case CHAPSIM_F_V: return d.v;
@@ -636,12 +721,13 @@ int chapsim_get_mesh(const chapsim_ctx *ctx, int what, double *out, int64_t n) {
   return CHAPSIM_OK;
 }
 
-int chapsim_init_random(chapsim_ctx *ctx, uint64_t seed, double amp, int project) {
-  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+// The seeded initial velocity of RANDOM_FL_FLD_TG (also used for the IO
+// domain): perturbation, xz-mean removal, laminar profile, v = 0 on the
+// wall, unit bulk velocity, zero wall ghosts.
+static void seeded_velocity(chapsim_ctx *ctx, uint64_t seed, double amp, std::vector<double> *q) {
   const int nx = ctx->cfg.nx, ny = ctx->cfg.ny, nz = ctx->cfg.nz;
   const int64_t sy = nx, sz = (int64_t)nx * (ny + 2), n = sz * nz;
-  std::vector<double> q[3];
-  for (auto &f : q) f.assign((size_t)n, 0.0);
+  for (int c = 0; c < 3; ++c) q[c].assign((size_t)n, 0.0);
   auto id = [&](int i, int j, int k) { return (size_t)((i - 1) + sy * j + sz * (k - 1)); };
   // RANDOM_FL_FLD_TG (src/INITIAL_FL_FLD_TG.f90:2-72) with a counter-based
   // generator in place of gfortran's random_number.
@@ -679,6 +765,118 @@ int chapsim_init_random(chapsim_ctx *ctx, uint64_t seed, double amp, int project
   for (int k = 1; k <= nz; ++k)
     for (int i = 1; i <= nx; ++i)
       for (int c = 0; c < 3; ++c) { q[c][id(i, 0, k)] = 0.0; q[c][id(i, ny + 1, k)] = 0.0; }
+}
+
+// Host spline look-up with the reference's search (table set-up only).
+static bool host_spline_eval(const std::vector<double> &x, const std::vector<double> &y, const std::vector<double> &b,
+                             const std::vector<double> &c, const std::vector<double> &dd, double u, double &out) {
+  const int n = (int)x.size();
+  if (u <= x[0] || u >= x[n - 1]) return false;
+  int i = 0, j = n;
+  while (j > i + 1) {
+    const int k = (i + j) / 2;
+    if (u < x[k]) j = k; else i = k;
+  }
+  const double dx = u - x[i];
+  out = y[i] + dx * (b[i] + dx * (c[i] + dx * dd[i]));
+  return true;
+}
+
+struct HostSpline {
+  std::vector<double> x, y, b, c, d;
+  HostSpline(const std::vector<double> &xs, const std::vector<double> &ys) : x(xs), y(ys) {
+    const int n = (int)x.size();
+    b.assign(n, 0.0); c.assign(n, 0.0); d.assign(n, 0.0);
+    chapsim_spl::fmm_spline(n, x.data(), y.data(), b.data(), c.data(), d.data());
+  }
+  bool eval(double u, double &out) const { return host_spline_eval(x, y, b, c, d, u, out); }
+};
+
+// IO initial field (RANDOM_FL_THEML_FLD_io + CALC_INITIALIZATION_io with the
+// seeded velocity of the TG recipe).
+static int io_init_random(chapsim_ctx *ctx, uint64_t seed, double amp, int project) {
+  IODev &io = ctx->io;
+  REQUIRE(!io.thermal || ctx->has_table, CHAPSIM_ERR_STATE, "thermal IO domain without a property table");
+  const int nx = ctx->cfg.nx, ny = ctx->cfg.ny, nz = ctx->cfg.nz;
+  const int64_t sy = nx, sz = (int64_t)nx * (ny + 2), n = sz * nz;
+  auto id = [&](int i, int j, int k) { return (size_t)((i - 1) + sy * j + sz * (k - 1)); };
+  std::vector<double> q[3], g[3];
+  for (auto &f : q) f.assign((size_t)n, 0.0);
+  for (auto &f : g) f.assign((size_t)n, 0.0);
+  seeded_velocity(ctx, seed, amp, q);
+  // properties at h = 0: the table's values, or the reference state 1 when the
+  // table keeps the reference shortcuts (INIFIELD_THERMAL_io)
+  double T0 = 1.0, D0 = 1.0, M0 = 1.0, K0 = 1.0;
+  if (io.thermal && !io.shortcuts) {
+    const HostSpline ht(ctx->tab[0], ctx->tab[1]), td(ctx->tab[1], ctx->tab[2]), tm(ctx->tab[1], ctx->tab[3]),
+        tk(ctx->tab[1], ctx->tab[4]);
+    REQUIRE(ht.eval(0.0, T0) && td.eval(T0, D0) && tm.eval(T0, M0) && tk.eval(T0, K0), CHAPSIM_ERR_RANGE,
+            "h = 0 lies outside the property table");
+  }
+  // RHO_STG of the uniform initial density (DENSITY_Staggered)
+  const double rx = io.thermal ? (D0 + D0 + D0 + D0) * 0.5 * 0.5 : 1.0;
+  std::vector<double> ry(ny + 2, 1.0);
+  if (io.thermal)
+    for (int j = 2; j <= ny; ++j) ry[j] = (ctx->wff[j] * (D0 + D0) + ctx->wfb[j] * (D0 + D0)) * 0.5;
+  auto velo2massflux = [&]() {  // VELO2MASSFLUX (src/INITIAL_FL_THEML_FLD_io.f90:481-560)
+    for (int k = 1; k <= nz; ++k)
+      for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) {
+          const size_t c = id(i, j, k);
+          g[0][c] = q[0][c] * rx;
+          g[2][c] = q[2][c] * rx;
+          if (j >= 2) g[1][c] = q[1][c] * ry[j];
+        }
+  };
+  velo2massflux();
+  // Unified_massflux (:653-682): unit bulk mass flux
+  double s = 0.0;
+  for (int j = 1; j <= ny; ++j)
+    for (int i = 1; i <= nx; ++i)
+      for (int k = 1; k <= nz; ++k) s += g[0][id(i, j, k)] / ctx->dyfi[j];
+  s = s / (nz / ctx->cfg.lz);
+  const double gm = s / (ctx->area_inlet * (double)nx);
+  for (int c = 0; c < 3; ++c)
+    for (auto &x : q[c]) x /= gm;
+  velo2massflux();
+  int rc;
+  for (int c = 0; c < 3; ++c) {
+    if ((rc = chapsim_set_field(ctx, CHAPSIM_IIO, CHAPSIM_F_U + c, q[c].data(), n))) return rc;
+    CKC(cudaMemcpyAsync(io.g[0][c], g[c].data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CKC(cudaMemsetAsync(io.g[1][c], 0, (size_t)n * sizeof(double), ctx->stream));  // G0_io = 0 until MOM_IO
+    CKC(cudaMemsetAsync(ctx->d.h0[c], 0, (size_t)n * sizeof(double), ctx->stream));
+  }
+  CKC(cudaStreamSynchronize(ctx->stream));
+  ctx->io_cur = 0;
+  TGDev &d = ctx->d;
+  const size_t bytes = (size_t)n * sizeof(double);
+  double *zero[] = {d.p, d.phi, d.rhsphi, io.drho, io.rhoh, io.h, io.rhse0};
+  for (double *f : zero) CKC(cudaMemsetAsync(f, 0, bytes, ctx->stream));
+  CKC(cudaMemsetAsync(io.bad, 0, sizeof(unsigned long long), ctx->stream));
+  const double *vals[] = {&T0, &D0, &D0, &M0, &M0, &K0};
+  double *arrs[] = {io.T, io.D, io.D0, io.mu, io.mu0, io.kap};
+  for (int a = 0; a < 6; ++a)
+    if ((rc = fill_value(ctx, arrs[a], (size_t)n, *vals[a]))) return rc;
+  if (project) {  // CALC_INITIALIZATION_io
+    if (io.thermal) {
+      if ((rc = io_thermal_bc(ctx))) return rc;
+      if ((rc = io_eng(ctx, 0))) return rc;
+    }
+    if ((rc = io_mom(ctx, 0, false))) return rc;
+  }
+  CKC(cudaStreamSynchronize(ctx->stream));
+  return CHAPSIM_OK;
+}
+
+int chapsim_init_random(chapsim_ctx *ctx, uint64_t seed, double amp, int project) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  CKC(cudaSetDevice(ctx->device));
+  if (ctx->domain == CHAPSIM_IIO) return io_init_random(ctx, seed, amp, project);
+  const int nx = ctx->cfg.nx, ny = ctx->cfg.ny, nz = ctx->cfg.nz;
+  const int64_t n = (int64_t)nx * (ny + 2) * nz;
+  std::vector<double> q[3];
+  for (auto &f : q) f.assign((size_t)n, 0.0);
+  seeded_velocity(ctx, seed, amp, q);
   int rc;
   for (int c = 0; c < 3; ++c)
     if ((rc = chapsim_set_field(ctx, CHAPSIM_ITG, CHAPSIM_F_U + c, q[c].data(), n))) return rc;
@@ -697,6 +895,7 @@ int chapsim_init_random(chapsim_ctx *ctx, uint64_t seed, double amp, int project
 
 int chapsim_rk3_mom_tg(chapsim_ctx *ctx, int ns) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(ctx->domain == CHAPSIM_ITG, CHAPSIM_ERR_STATE, "not a TG context");
   REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
   CKC(cudaSetDevice(ctx->device));
   return launch_substep(ctx, ns);
@@ -704,6 +903,7 @@ int chapsim_rk3_mom_tg(chapsim_ctx *ctx, int ns) {
 
 int chapsim_step_tg(chapsim_ctx *ctx, int nsteps) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(ctx->domain == CHAPSIM_ITG, CHAPSIM_ERR_STATE, "not a TG context");
   REQUIRE(nsteps >= 0, CHAPSIM_ERR_ARG, "nsteps must be >= 0");
   CKC(cudaSetDevice(ctx->device));
   if (ctx->timing) {
@@ -738,30 +938,167 @@ int chapsim_step_tg(chapsim_ctx *ctx, int nsteps) {
 
 int chapsim_divg(chapsim_ctx *ctx, int domain, int ns) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
-  REQUIRE(domain == CHAPSIM_ITG, CHAPSIM_ERR_ARG, "only the TG domain is built");
+  REQUIRE(domain == ctx->domain, CHAPSIM_ERR_ARG, "domain does not match the context");
   REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
+  CKC(cudaSetDevice(ctx->device));
+  if (domain == CHAPSIM_IIO) {
+    // DIVG_io (src/DIVG.f90:60-150) of the current G and DrhoDtP
+    const TGDev saved = ctx->d;
+    const int cur = ctx->io_cur;
+    ctx->d.u = ctx->io.g[cur][0]; ctx->d.v = ctx->io.g[cur][1]; ctx->d.w = ctx->io.g[cur][2];
+    ctx->d.drho = ctx->io.thermal ? ctx->io.drho : nullptr;
+    const int rc = launch_divg(ctx, ns);
+    ctx->d = saved;
+    return rc;
+  }
   return launch_divg(ctx, ns);
 }
 
 int chapsim_pois3d(chapsim_ctx *ctx, int domain) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
-  REQUIRE(domain == CHAPSIM_ITG, CHAPSIM_ERR_ARG, "only the TG domain is built");
-  return launch_pois3d(ctx);
+  REQUIRE(domain == ctx->domain, CHAPSIM_ERR_ARG, "domain does not match the context");
+  CKC(cudaSetDevice(ctx->device));
+  return launch_pois3d(ctx);  // FISHPACK_POIS3D_SIMPLE on an IO context (mean mode pinned last)
 }
 
 int chapsim_velo_correction(chapsim_ctx *ctx, int domain, int ns) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
-  REQUIRE(domain == CHAPSIM_ITG, CHAPSIM_ERR_ARG, "only the TG domain is built");
+  REQUIRE(domain == ctx->domain, CHAPSIM_ERR_ARG, "domain does not match the context");
   REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
+  CKC(cudaSetDevice(ctx->device));
+  if (domain == CHAPSIM_IIO) return io_correction(ctx, ns);
   return launch_correction(ctx, ns);
+}
+
+int chapsim_set_table(chapsim_ctx *ctx, const double *H, const double *T, const double *D, const double *M,
+                      const double *K, int n, int shortcuts) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(ctx->domain == CHAPSIM_IIO, CHAPSIM_ERR_STATE, "property tables belong to IO contexts");
+  REQUIRE(H && T && D && M && K && n >= 4, CHAPSIM_ERR_ARG, "table needs 5 columns of n >= 4 points");
+  for (int i = 1; i < n; ++i)
+    REQUIRE(H[i] > H[i - 1] && T[i] > T[i - 1], CHAPSIM_ERR_ARG, "H and T must increase strictly");
+  CKC(cudaSetDevice(ctx->device));
+  CKC(cudaStreamSynchronize(ctx->stream));
+  for (auto &g : ctx->io_graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  for (void *p : ctx->table_allocs) cudaFree(p);
+  ctx->table_allocs.clear();
+  const double *cols[5] = {H, T, D, M, K};
+  for (int q = 0; q < 5; ++q) ctx->tab[q].assign(cols[q], cols[q] + n);
+  IODev &io = ctx->io;
+  const std::pair<int, int> xy[4] = {{0, 1}, {1, 2}, {1, 3}, {1, 4}};
+  chapsim_spl::Spline *dst[4] = {&io.ht, &io.td, &io.tm, &io.tk};
+  for (int q = 0; q < 4; ++q) {
+    const cudaError_t e = chapsim_spl::upload_spline(ctx->table_allocs, ctx->tab[xy[q].first], ctx->tab[xy[q].second],
+                                                     *dst[q]);
+    if (e != cudaSuccess) {
+      ctx->err = std::string("property table upload: ") + cudaGetErrorString(e);
+      cudaGetLastError();
+      return CHAPSIM_ERR_NOMEM;
+    }
+  }
+  io.shortcuts = shortcuts ? 1 : 0;
+  // RHOHmax (src/Flow_State.f90:963-990): max of rho(h) h over 3n - 1 samples
+  const HostSpline hd(ctx->tab[0], ctx->tab[2]);
+  double rm = -1e-14;
+  for (int i = 2; i <= 3 * n; ++i) {
+    const double h = H[0] + (double)(i - 1) * (H[n - 1] - H[0]) / (double)(3 * n);
+    double dv = 0.0;
+    hd.eval(h, dv);
+    if (io.shortcuts && fabs(h) < 1.0e-10) dv = 1.0;
+    if (dv * h > rm) rm = dv * h;
+  }
+  io.rhohmax = rm;
+  ctx->has_table = true;
+  return CHAPSIM_OK;
+}
+
+int chapsim_rk3_eng_io(chapsim_ctx *ctx, int ns) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(ctx->domain == CHAPSIM_IIO, CHAPSIM_ERR_STATE, "not an IO context");
+  REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
+  REQUIRE(ctx->io.thermal, CHAPSIM_ERR_STATE, "thermal is off on this IO context");
+  REQUIRE(ctx->has_table, CHAPSIM_ERR_STATE, "no property table");
+  CKC(cudaSetDevice(ctx->device));
+  return io_eng(ctx, ns);
+}
+
+int chapsim_rk3_mom_io(chapsim_ctx *ctx, int ns) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(ctx->domain == CHAPSIM_IIO, CHAPSIM_ERR_STATE, "not an IO context");
+  REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
+  CKC(cudaSetDevice(ctx->device));
+  return io_mom(ctx, ns, ns >= 1);
+}
+
+static int io_substeps(chapsim_ctx *ctx) {
+  for (int ns = 1; ns <= 3; ++ns) {
+    int rc;
+    if (ctx->io.thermal && (rc = io_eng(ctx, ns))) return rc;
+    if ((rc = io_mom(ctx, ns, true))) return rc;
+  }
+  return CHAPSIM_OK;
+}
+
+int chapsim_step_io(chapsim_ctx *ctx, int nsteps) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(ctx->domain == CHAPSIM_IIO, CHAPSIM_ERR_STATE, "not an IO context");
+  REQUIRE(nsteps >= 0, CHAPSIM_ERR_ARG, "nsteps must be >= 0");
+  REQUIRE(!ctx->io.thermal || ctx->has_table, CHAPSIM_ERR_STATE, "no property table");
+  CKC(cudaSetDevice(ctx->device));
+  if (ctx->timing) {
+    for (int s = 0; s < nsteps; ++s) {
+      int rc = io_substeps(ctx);
+      if (rc) return rc;
+    }
+    return CHAPSIM_OK;
+  }
+  for (int s = 0; s < nsteps; ++s) {
+    // three substeps flip the G buffers three times: one graph per starting parity
+    const int par = ctx->io_cur;
+    if (!ctx->io_graph[par]) {
+      cudaGraph_t g = nullptr;
+      const int64_t before = ctx->launches;
+      CKC(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+      int rc = io_substeps(ctx);
+      cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+      ctx->io_cur = par;  // captured, not run
+      if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+      if (e != cudaSuccess) { ctx->err = cudaGetErrorString(e); return CHAPSIM_ERR_CUDA; }
+      e = cudaGraphInstantiate(&ctx->io_graph[par], g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) { ctx->io_graph[par] = nullptr; ctx->err = cudaGetErrorString(e); return CHAPSIM_ERR_CUDA; }
+      ctx->kernels_per_step = ctx->launches - before;
+      ctx->launches = before;
+    }
+    CKC(cudaGraphLaunch(ctx->io_graph[par], ctx->stream));
+    ctx->launches += ctx->kernels_per_step;
+    ctx->io_cur = 1 - par;
+  }
+  return CHAPSIM_OK;
 }
 
 int chapsim_reduce(chapsim_ctx *ctx, int domain, int what, double *out) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
   REQUIRE(out, CHAPSIM_ERR_ARG, "null output");
-  REQUIRE(domain == CHAPSIM_ITG, CHAPSIM_ERR_ARG, "only the TG domain is built");
-  REQUIRE(what >= 0 && what <= 2, CHAPSIM_ERR_ARG, "unknown reduction");
+  REQUIRE(domain == ctx->domain, CHAPSIM_ERR_ARG, "domain does not match the context");
   CKC(cudaSetDevice(ctx->device));
+  if (domain == CHAPSIM_IIO) {
+    if (what == CHAPSIM_R_BADCELLS) {
+      unsigned long long b = 0;
+      CKC(cudaMemcpyAsync(&b, ctx->io.bad, sizeof(b), cudaMemcpyDeviceToHost, ctx->stream));
+      CKC(cudaStreamSynchronize(ctx->stream));
+      *out = (double)b;
+      return CHAPSIM_OK;
+    }
+    if (what == CHAPSIM_R_DIVMAX_Q || what == CHAPSIM_R_NANCOUNT)
+      return launch_reduce(ctx, what == CHAPSIM_R_DIVMAX_Q ? 0 : 2, out);  // on u, v, w (, p)
+    REQUIRE(what == CHAPSIM_R_DIVMAX || what == CHAPSIM_R_BULK || what == CHAPSIM_R_BULK_G ||
+                what == CHAPSIM_R_BULK_H,
+            CHAPSIM_ERR_ARG, "unknown reduction");
+    return io_reduce(ctx, what, out);
+  }
+  REQUIRE(what >= 0 && what <= 2, CHAPSIM_ERR_ARG, "unknown reduction");
   double v = 0.0;
   int rc = launch_reduce(ctx, what, &v);
   if (rc) return rc;

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/chapsim.h"
+#include "spline.cuh"
 
 namespace chapsim {
 
@@ -38,6 +39,28 @@ struct TGDev {
   const double *amph, *acph, *apph;
   const double *ak1, *ak3;
   double dxi, dzi, dxqi, dzqi, cvisc, dt, volm;
+  // IO domain Poisson (FISHPACK_POIS3D_SIMPLE): drho is added to the
+  // divergence of the forward x-transform, and pin_last = 1 pins the mean
+  // mode at the last y-row instead of decoupling row 1.
+  const double *drho;
+  int pin_last;
+};
+
+// Device-side state of an IO domain (x-periodic channel section), on top of
+// the TGDev fields it shares: u, v, w = Q_io, p = PR_io, phi = DPH_io,
+// rhsphi = RHSLLPHI_io, h0[0..2] = EXPLT0_io (FP64).  The mass flux G_io and
+// its value at the start of the last momentum substep (G0_io) live in the
+// two buffers g[0..1]; which one holds G alternates every substep.
+struct IODev {
+  double *g[2][3];
+  double *drho;                               // DrhoDtP
+  double *rhoh, *h, *T, *D, *D0, *mu, *mu0, *kap, *rhse0;  // RHOH, ENTHALPY, ..., RHS_ENERGY0
+  chapsim_spl::Spline ht, td, tm, tk;          // h -> T; T -> rho, mu, k
+  double cthecd, qw_bot, qw_top, rhohmax, f_a, cfgv;
+  int thermal, shortcuts, gravdir, flowdrvtp;
+  double *dpg;       // device scalar: DPGRNS of the current substep
+  double *part;      // per-block partial sums of the x mass-flux forcing
+  unsigned long long *bad;  // table look-ups outside the table
 };
 
 // Per-substep scalars.
@@ -112,6 +135,17 @@ struct chapsim_ctx {
   // CUDA graph of one full step (NS = 1, 2, 3)
   cudaGraphExec_t step_graph = nullptr;
   int64_t kernels_per_step = 0;
+
+  // IO domain (domain == CHAPSIM_IIO)
+  int domain = CHAPSIM_ITG;
+  chapsim_io_config iocfg{};
+  chapsim::IODev io{};
+  int io_cur = 0;          // g[io_cur] holds G_io, g[1 - io_cur] holds G0_io
+  bool has_table = false;
+  int io_npart = 0;
+  std::vector<void *> table_allocs;
+  std::vector<double> tab[5];  // host copy of the table columns H, T, D, M, K
+  cudaGraphExec_t io_graph[2] = {nullptr, nullptr};  // one step starting from io_cur = 0 / 1
 };
 
 // Kernel launch wrappers (defined in tg_kernels.cu).
@@ -124,4 +158,15 @@ int launch_pois3d(chapsim_ctx *c);
 int launch_correction(chapsim_ctx *c, int ns);
 int launch_reduce(chapsim_ctx *c, int what, double *host_out);
 int launch_bc_q(chapsim_ctx *c);
+// Poisson solve of an IO domain: DIVG_io of (gx, gy, gz) + drho fused into the
+// forward x-transform, then the spectral y-solve with the mean mode pinned at
+// the last row, into phi.
+int launch_pois_io(chapsim_ctx *c, int ns, double *gx, double *gy, double *gz, const double *drho);
+// IO domain kernels (io_kernels.cu).
+int io_eng(chapsim_ctx *c, int ns);
+int io_thermal_bc(chapsim_ctx *c);
+int io_mom(chapsim_ctx *c, int ns, bool prep);
+int io_reduce(chapsim_ctx *c, int what, double *host_out);
+int io_correction(chapsim_ctx *c, int ns);
+int fill_value(chapsim_ctx *c, double *p, size_t n, double v);
 }  // namespace chapsim

@@ -18,22 +18,15 @@
 #include <vector>
 
 #include "../../include/chapsim.h"
+#include "spline.cuh"
 
 namespace {
+
+using namespace chapsim_spl;
 
 constexpr int NH = 64, NO = 5;
 constexpr int NP = NH + NH + NH * NH + NH + NO * NH + NO;  // 4613
 constexpr int O_W1 = 0, O_B1 = NH, O_W2 = 2 * NH, O_B2 = 2 * NH + NH * NH, O_W3 = O_B2 + NH, O_B3 = O_W3 + NO * NH;
-
-// Spline of y over x: coefficients b, c, d (Forsythe, Malcolm & Moler),
-// also packed per interval as one 32-byte record {y, b, c, d}.
-struct Spline {
-  const double *x, *y, *b, *c, *d;
-  const double4 *ybcd;
-  const int *blo;  // bucket -> first candidate interval
-  double x0, binv;
-  int n, nb;
-};
 
 struct PropsDev {
   Spline ht, hcp, td, tm, tk;
@@ -47,29 +40,6 @@ struct PropsDev {
   double g0, ginv;
   int nbins;
 };
-
-// Interval i with x[i] <= u < x[i+1] (u strictly inside the table); the
-// bucket gives a short range for the same binary search as the reference.
-__device__ __forceinline__ int spline_find(const Spline &s, double u) {
-  int b = (int)((u - s.x0) * s.binv);
-  b = b < 0 ? 0 : (b >= s.nb ? s.nb - 1 : b);
-  int i = __ldg(s.blo + b), j = min(s.n - 1, __ldg(s.blo + b + 1) + 3);
-  while (j > i + 1) {
-    const int k = (i + j) >> 1;
-    if (u < __ldg(s.x + k)) j = k; else i = k;
-  }
-  return i;
-}
-__device__ __forceinline__ double spline_at(const Spline &s, int i, double u) {
-  const double2 r0 = __ldg(reinterpret_cast<const double2 *>(s.ybcd + i));
-  const double2 r1 = __ldg(reinterpret_cast<const double2 *>(s.ybcd + i) + 1);
-  const double4 r = make_double4(r0.x, r0.y, r1.x, r1.y);
-  const double dx = u - __ldg(s.x + i);
-  return r.x + dx * (r.y + dx * (r.z + dx * r.w));
-}
-__device__ __forceinline__ double spline_eval(const Spline &s, double u) { return spline_at(s, spline_find(s, u), u); }
-
-__device__ __forceinline__ bool inside(const Spline &s, double u) { return u > s.x[0] && u < s.x[s.n - 1]; }
 
 // THERM_PROP_UPDATE for one cell; returns false when h or T is outside the
 // table (cell left unchanged).
@@ -391,65 +361,6 @@ uint64_t splitmix64(uint64_t x) {
   x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
   x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
   return x ^ (x >> 31);
-}
-
-// Host restatement of CUBIC_SPLINE (Forsythe-Malcolm-Moler, 1977).
-void fmm_spline(int n, const double *x, const double *y, double *b, double *c, double *d) {
-  const int nm1 = n - 1;
-  d[0] = x[1] - x[0];
-  c[1] = (y[1] - y[0]) / d[0];
-  for (int i = 1; i < nm1; ++i) {
-    d[i] = x[i + 1] - x[i];
-    b[i] = 2.0 * (d[i - 1] + d[i]);
-    c[i + 1] = (y[i + 1] - y[i]) / d[i];
-    c[i] = c[i + 1] - c[i];
-  }
-  b[0] = -d[0];
-  b[n - 1] = -d[n - 2];
-  c[0] = 0.0;
-  c[n - 1] = 0.0;
-  if (n > 3) {
-    c[0] = c[2] / (x[3] - x[1]) - c[1] / (x[2] - x[0]);
-    c[n - 1] = c[n - 2] / (x[n - 1] - x[n - 3]) - c[n - 3] / (x[n - 2] - x[n - 4]);
-    c[0] = c[0] * d[0] * d[0] / (x[3] - x[0]);
-    c[n - 1] = -c[n - 1] * d[n - 2] * d[n - 2] / (x[n - 1] - x[n - 4]);
-  }
-  for (int i = 1; i < n; ++i) {
-    const double t = d[i - 1] / b[i - 1];
-    b[i] = b[i] - t * d[i - 1];
-    c[i] = c[i] - t * c[i - 1];
-  }
-  c[n - 1] = c[n - 1] / b[n - 1];
-  for (int l = 1; l <= nm1; ++l) {
-    const int i = n - 1 - l;
-    c[i] = (c[i] - d[i] * c[i + 1]) / b[i];
-  }
-  b[n - 1] = (y[n - 1] - y[nm1 - 1]) / d[nm1 - 1] + d[nm1 - 1] * (c[nm1 - 1] + 2.0 * c[n - 1]);
-  for (int i = 0; i < nm1; ++i) {
-    b[i] = (y[i + 1] - y[i]) / d[i] - d[i] * (c[i + 1] + 2.0 * c[i]);
-    d[i] = (c[i + 1] - c[i]) / d[i];
-    c[i] = 3.0 * c[i];
-  }
-  c[n - 1] = 3.0 * c[n - 1];
-  d[n - 1] = d[n - 2];
-}
-
-// Bucket table over nb uniform buckets of [x_1, x_n]: blo[b] = I(start_b) - 1
-// with I(v) = max{i : x_i <= v}, so every u in bucket b satisfies
-// x[blo[b]] <= u < x[min(n-1, blo[b+1] + 3)] (one interval of slack each way
-// for rounding); the binary search between them finds the reference's i.
-void bucket_table(int n, const double *x, int nb, double &x0, double &binv, std::vector<int> &blo) {
-  x0 = x[0];
-  binv = nb / (x[n - 1] - x[0]);
-  blo.assign(nb + 1, 0);
-  int i = 0;
-  for (int b = 0; b <= nb; ++b) {
-    const double start = x0 + b / binv;
-    while (i + 1 < n && x[i + 1] <= start) ++i;
-    int l = i - 1;
-    l = l < 0 ? 0 : l;
-    blo[b] = l < n - 2 ? l : n - 2;
-  }
 }
 
 }  // namespace

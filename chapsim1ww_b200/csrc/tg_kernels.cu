@@ -772,8 +772,9 @@ __global__ void __launch_bounds__(256, 2) k_fftx(TGDev d, SubParams sp, FFTPlan 
       if (mode == 0) {
         const int ip = wrapp(i, nx);
         const int j = jbeg + r;
-        const double dv = (U[r * nx + ip] - U[r * nx + i]) * d.dxi + (V[(r + 1) * nx + i] - V[r * nx + i]) * d.dyfi[j] +
-                          (W1[r * nx + i] - W0[r * nx + i]) * d.dzi;
+        double dv = (U[r * nx + ip] - U[r * nx + i]) * d.dxi + (V[(r + 1) * nx + i] - V[r * nx + i]) * d.dyfi[j] +
+                    (W1[r * nx + i] - W0[r * nx + i]) * d.dzi;
+        if (d.drho) dv += d.drho[row0 + d.sz * k + (int64_t)r * nx + i];  // DIVG_io: + DrhoDtP
         val = dv * coe0;
         d.rhsphi[row0 + d.sz * k + (int64_t)r * nx + i] = val;
       } else {
@@ -836,7 +837,7 @@ __global__ void __launch_bounds__(256, 2) k_fftz(TGDev d, FFTPlan pl, int lz, in
       C v = res[l * ld + kz];
       v.x *= scale;
       v.y *= scale;
-      if (sign < 0 && j == 1 && kz == 0 && kx0 + l == 0) { v.x = 0; v.y = 0; }
+      if (sign < 0 && j == 1 && kz == 0 && kx0 + l == 0 && !d.pin_last) { v.x = 0; v.y = 0; }
       S[skz * kz + l] = v;
     }
   }
@@ -856,13 +857,16 @@ __global__ void k_ypivots(TGDev d) {
   double2 *P = d.ypiv + kx + (int64_t)d.lp * ny * kz;
   const double shift = d.ak1[kx] + d.ak3[kz];
   const bool mean = (kx == 0 && kz == 0);
+  const bool pin1 = mean && !d.pin_last, pinn = mean && d.pin_last;
   double b = d.acph[1] - shift;
   double pp = 1.0 / b;
-  double h = (mean ? 0.0 : d.apph[1]) * pp;
-  P[0] = make_double2(mean ? 0.0 : pp, h);  // pp = 0 zeroes the pinned row
+  double h = (pin1 ? 0.0 : d.apph[1]) * pp;
+  P[0] = make_double2(pin1 ? 0.0 : pp, h);  // pp = 0 zeroes the pinned row
   for (int j = 2; j <= ny; ++j) {
     b = d.acph[j] - shift;
-    pp = 1.0 / (b - h * d.amph[j]);
+    // TRID0's zero branch for the singular last pivot of the mean mode
+    // (src/possion3d_fishpack_reform.f90:53-58): phi(ny) = 0
+    pp = (pinn && j == ny) ? 0.0 : 1.0 / (b - h * d.amph[j]);
     h = j < ny ? d.apph[j] * pp : 0.0;
     P[(int64_t)d.lp * (j - 1)] = make_double2(pp, h);
   }
@@ -1355,6 +1359,16 @@ int launch_divg(chapsim_ctx *c, int ns) {
   // DIVG_tg alone: the fused divergence + x-transform kernel in mode 0 stores
   // RHSLLPHI (its spectral output is scratch).
   return c->cfg.precision == CHAPSIM_MIXED ? Prec<float>::fftx(c, ns, 0) : Prec<double>::fftx(c, ns, 0);
+}
+
+int launch_pois_io(chapsim_ctx *c, int ns, double *gx, double *gy, double *gz, const double *drho) {
+  // the fused divergence of the forward x-transform reads u, v, w: point them
+  // at the provisional mass flux for these launches only
+  const TGDev saved = c->d;
+  c->d.u = gx; c->d.v = gy; c->d.w = gz; c->d.drho = drho;
+  const int rc = Prec<double>::poisson(c, ns, 0);
+  c->d = saved;
+  return rc;
 }
 
 int launch_pois3d(chapsim_ctx *c) {

@@ -1,0 +1,127 @@
+"""Host-side mirror of the reference's IO-section entry points over libchapsim.
+
+An ``IOChannel`` is the inflow/outflow channel section run x-periodic
+(BCX_io = 3), with the explicit viscous scheme and, when thermal is on, the
+energy equation with table properties and iso-flux walls.  Method names follow
+the Fortran subroutines they replace (CHAPSim1WW, paths relative to the
+project root):
+
+=========================  ==================================================
+``solverrk3_eng_io(ns)``   SOLVERRK3_ENG_IO(NS), src/SOLVERRK3_ENG_IO.f90:1-77
+``solverrk3_mom_io(ns)``   DENSITY_TIME_DERIVATION, DENSITY_/MU_Staggered,
+                           VELOCITY_CALC_io (ns >= 1), then SOLVERRK3_MOM_IO(NS),
+                           src/SOLVE.f90:121-132, src/SOLVERRK3_MOM_IO.f90:1-168
+``divg_io(ns)``            DIVG_io(NS), src/DIVG.f90:60-150
+``fishpack_pois3d()``      FISHPACK_POIS3D_SIMPLE, src/possion3d_fishpack_reform.f90:431-547
+``massflux_update_io(ns)`` MASSFLUX_UPDATE_IO + PRCALC_io,
+                           src/VELO_CORRECTION.f90:107-185, src/PRESSURE_CORRECTION.f90:86-122
+``divgck_io()``            DIVGCK_io, src/DIVGCK.f90:60-190
+``random_fl_theml_fld_io`` RANDOM_FL_THEML_FLD_io + CALC_INITIALIZATION_io,
+                           src/INITIAL_FL_THEML_FLD_io.f90:2-172
+=========================  ==================================================
+
+Every compute call goes to libchapsim.so; there is no CPU fallback.
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+from .solver import FIELD_IDS, ChapsimError, TGChannel, default_config
+
+IO_FIELD_IDS = dict(FIELD_IDS)
+IO_FIELD_IDS.update({
+    "ex0x": _lib.F_H0U, "ex0y": _lib.F_H0V, "ex0z": _lib.F_H0W,
+    "gx": _lib.F_GX, "gy": _lib.F_GY, "gz": _lib.F_GZ, "g0x": _lib.F_G0X, "g0y": _lib.F_G0Y, "g0z": _lib.F_G0Z,
+    "h": _lib.F_H, "t": _lib.F_T, "rho": _lib.F_RHO, "mu": _lib.F_MU, "k": _lib.F_K, "rhoh": _lib.F_RHOH,
+    "rho0": _lib.F_RHO0, "mu0": _lib.F_MU0, "drho": _lib.F_DRHO, "rhse0": _lib.F_RHSE0,
+})
+
+
+def io_config(**kw):
+    io = _lib.ChapsimIOConfig()
+    _lib.load().chapsim_io_config_default(ctypes.byref(io))
+    for k, v in kw.items():
+        if not hasattr(io, k):
+            raise KeyError(k)
+        setattr(io, k, v)
+    return io
+
+
+class IOChannel(TGChannel):
+    """One x-periodic IO channel section resident on a GPU (FP64)."""
+
+    DOMAIN = _lib.IIO
+    FIELDS = IO_FIELD_IDS
+
+    def __init__(self, nx=64, ny=64, nz=64, lx=8 * math.pi, lz=4 * math.pi / 3, str2=2.0, istr2=1, ren=2800.0,
+                 dt=1e-3, flowdrvtp=1, cfgv=0.0, thermal=1, prt=0.71, qw=(1.0, 1.0), gravdir=0, f_a=0.0,
+                 table=None, shortcuts=0, device=0):
+        self.lib = _lib.load()
+        self.cfg = default_config(nx=nx, ny=ny, nz=nz, lx=lx, lz=lz, str2=str2, istr2=istr2, ren=ren, dt=dt,
+                                  flowdrvtp=flowdrvtp, cfgv=cfgv, precision=_lib.FP64, device=device)
+        self.iocfg = io_config(thermal=thermal, prt=prt, qw_bot=qw[0], qw_top=qw[1], gravdir=gravdir, f_a=f_a)
+        h = ctypes.c_void_p()
+        rc = self.lib.chapsim_create_io(ctypes.byref(self.cfg), ctypes.byref(self.iocfg), ctypes.byref(h))
+        if rc != _lib.CHAPSIM_OK:
+            raise ChapsimError(rc, "chapsim_create_io failed")
+        self.h = h
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.n = self.lib.chapsim_field_len(self.h)
+        if thermal:
+            if table is None:
+                from .props import synthetic_table
+                table = synthetic_table()
+            self.set_table(table, shortcuts)
+
+    def set_table(self, table, shortcuts=0):
+        """Columns H, T, D, M, K (extra columns ignored)."""
+        cols = [np.ascontiguousarray(c, dtype=np.float64) for c in list(table)[:5]]
+        self._chk(self.lib.chapsim_set_table(self.h, *[c.ctypes.data for c in cols], len(cols[0]),
+                                             1 if shortcuts else 0))
+
+    # ------------------------------------------------------ reference entries
+    def random_fl_theml_fld_io(self, seed=0, amp=0.1, project=True):
+        self._chk(self.lib.chapsim_init_random(self.h, seed, amp, 1 if project else 0))
+
+    def solverrk3_eng_io(self, ns):
+        self._chk(self.lib.chapsim_rk3_eng_io(self.h, ns))
+
+    def solverrk3_mom_io(self, ns):
+        self._chk(self.lib.chapsim_rk3_mom_io(self.h, ns))
+
+    def step(self, nsteps=1):
+        """NS = 1, 2, 3 (energy then momentum) for each of nsteps steps (graph-replayed)."""
+        self._chk(self.lib.chapsim_step_io(self.h, nsteps))
+
+    def divg_io(self, ns):
+        self._chk(self.lib.chapsim_divg(self.h, _lib.IIO, ns))
+
+    def fishpack_pois3d(self):
+        self._chk(self.lib.chapsim_pois3d(self.h, _lib.IIO))
+
+    def massflux_update_io(self, ns):
+        self._chk(self.lib.chapsim_velo_correction(self.h, _lib.IIO, ns))
+
+    def divgck_io(self):
+        return self._reduce(_lib.R_DIVMAX)
+
+    def divgck_q_io(self):
+        return self._reduce(_lib.R_DIVMAX_Q)
+
+    def bulk_velocity_io(self):
+        return self._reduce(_lib.R_BULK)
+
+    def bulk_massflux_io(self):
+        return self._reduce(_lib.R_BULK_G)
+
+    def bulk_h_io(self):
+        return self._reduce(_lib.R_BULK_H)
+
+    def bad_cells(self):
+        return int(self._reduce(_lib.R_BADCELLS))
+
+    # TG-only entries do not apply
+    def solverrk3_mom_tg(self, ns):
+        raise ChapsimError(4, "not a TG context")

@@ -49,6 +49,9 @@ def default_config(**kw):
 class TGChannel:
     """One TG (periodic) channel domain resident on a GPU."""
 
+    DOMAIN = _lib.ITG
+    FIELDS = FIELD_IDS
+
     def __init__(self, nx=64, ny=64, nz=64, lx=4 * math.pi, lz=4 * math.pi / 3, str2=2.0, istr2=1,
                  ren=2800.0, dt=1e-3, flowdrvtp=1, cfgv=0.0, precision=_lib.FP64, device=0):
         self.lib = _lib.load()
@@ -92,18 +95,18 @@ class TGChannel:
         a = np.ascontiguousarray(arr, dtype=np.float64)
         if a.size != self.n:
             raise ValueError(f"field {name}: expected {self.n} values, got {a.size}")
-        self._chk(self.lib.chapsim_set_field(self.h, _lib.ITG, FIELD_IDS[name], a.ctypes.data, self.n))
+        self._chk(self.lib.chapsim_set_field(self.h, self.DOMAIN, self.FIELDS[name], a.ctypes.data, self.n))
 
     def get_field(self, name, out=None):
         a = np.empty(self.shape, dtype=np.float64) if out is None else out
-        self._chk(self.lib.chapsim_get_field(self.h, _lib.ITG, FIELD_IDS[name], a.ctypes.data, self.n))
+        self._chk(self.lib.chapsim_get_field(self.h, self.DOMAIN, self.FIELDS[name], a.ctypes.data, self.n))
         return a
 
     def set_field_device(self, name, ptr):
-        self._chk(self.lib.chapsim_set_field_device(self.h, _lib.ITG, FIELD_IDS[name], ptr, self.n))
+        self._chk(self.lib.chapsim_set_field_device(self.h, self.DOMAIN, self.FIELDS[name], ptr, self.n))
 
     def get_field_device(self, name, ptr):
-        self._chk(self.lib.chapsim_get_field_device(self.h, _lib.ITG, FIELD_IDS[name], ptr, self.n))
+        self._chk(self.lib.chapsim_get_field_device(self.h, self.DOMAIN, self.FIELDS[name], ptr, self.n))
 
     def mesh(self, what):
         n = self.ny + 1 if what in (0, 3) else self.ny
@@ -141,7 +144,7 @@ class TGChannel:
 
     def _reduce(self, what):
         v = ctypes.c_double()
-        self._chk(self.lib.chapsim_reduce(self.h, _lib.ITG, what, ctypes.byref(v)))
+        self._chk(self.lib.chapsim_reduce(self.h, self.DOMAIN, what, ctypes.byref(v)))
         return v.value
 
     def divgck_tg(self):

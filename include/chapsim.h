@@ -143,7 +143,13 @@ int chapsim_get_mesh(const chapsim_ctx *ctx, int what, double *out, int64_t n);
  * on u, v, w from a counter-based splitmix64 keyed by (seed, component, i, j,
  * k), xz-mean removal, the laminar profile 1.5(1-y^2) on u, v = 0 at the wall,
  * bulk velocity rescaled to 1.  When project != 0 an NS=0 substep follows
- * (the reference's initial projection). */
+ * (the reference's initial projection).
+ * On an IO context: the same velocity recipe, then h = 0 with the table's
+ * properties at h = 0 (T = rho = mu = k = 1 when the table keeps the
+ * reference shortcuts), G = rho_stag u scaled to unit bulk mass flux
+ * (VELO2MASSFLUX, Unified_massflux, src/INITIAL_FL_THEML_FLD_io.f90:481-682),
+ * and with project != 0 CALC_INITIALIZATION_io (:133-172): wall ghosts,
+ * SOLVERRK3_ENG_IO(0), SOLVERRK3_MOM_IO(0). */
 int chapsim_init_random(chapsim_ctx *ctx, uint64_t seed, double amp, int project);
 
 /* SOLVERRK3_MOM_tg(NS) (src/SOLVERRK3_MOM_tg.f90:18-61), NS in 0..3. */
@@ -186,6 +192,84 @@ int chapsim_get_tuning(const chapsim_ctx *ctx, int *rhs_nzc, int *fft_lb);
  * (or the last reset). */
 int chapsim_launch_count(const chapsim_ctx *ctx, int64_t *count);
 int chapsim_launch_count_reset(chapsim_ctx *ctx);
+
+/* ======================================================================
+ * IO domain: the inflow/outflow section run x-periodic (BCX_io = 3, no TG
+ * section, src/READINI.f90:121-131), with the explicit viscous scheme
+ * (visthemflg = 0, src/readdata.ini:23), the FISHPACK Poisson solver and,
+ * when thermal is on, the energy equation with table properties and
+ * iso-flux walls.  A context is either a TG or an IO domain; the functions
+ * above that take a domain argument accept CHAPSIM_IIO on an IO context.
+ *
+ * On an IO context: u, v, w = Q_io, p = PR_io, phi = DPH_io, rhsphi =
+ * RHSLLPHI_io, H0U/H0V/H0W = EXPLT0_io(:,:,:,1..3), plus the fields below.
+ * The time-step form is FP64 only.
+ * ====================================================================== */
+#define CHAPSIM_F_GX 10     /* G_io(:,:,:,1), mass flux rho u       */
+#define CHAPSIM_F_GY 11     /* G_io(:,:,:,2)                        */
+#define CHAPSIM_F_GZ 12     /* G_io(:,:,:,3)                        */
+#define CHAPSIM_F_G0X 13    /* G0_io: G at the start of the last momentum substep */
+#define CHAPSIM_F_G0Y 14
+#define CHAPSIM_F_G0Z 15
+#define CHAPSIM_F_H 16      /* ENTHALPY    */
+#define CHAPSIM_F_T 17      /* TEMPERATURE */
+#define CHAPSIM_F_RHO 18    /* DENSITY     */
+#define CHAPSIM_F_MU 19     /* VISCOUSITY  */
+#define CHAPSIM_F_K 20      /* THERMCONDT  */
+#define CHAPSIM_F_RHOH 21   /* RHOH        */
+#define CHAPSIM_F_RHO0 22   /* DENSITY0    */
+#define CHAPSIM_F_MU0 23    /* VISCOUSITY0 */
+#define CHAPSIM_F_DRHO 24   /* DrhoDtP     */
+#define CHAPSIM_F_RHSE0 25  /* RHS_ENERGY0 */
+
+/* IO reductions (chapsim_reduce with domain CHAPSIM_IIO): CHAPSIM_R_DIVMAX is
+ * DIVGCK_io's max|div G + DrhoDtP| (src/DIVGCK.f90:60-190), CHAPSIM_R_BULK is
+ * BULK_VELOCITY_IO (src/INITIAL_FL_THEML_FLD_io.f90:385-413), and: */
+#define CHAPSIM_R_DIVMAX_Q 3 /* max|div u| (DIVGCK_Q_comm_io)              */
+#define CHAPSIM_R_BULK_G 4   /* BULK_MASSFLUX_IO                           */
+#define CHAPSIM_R_BULK_H 5   /* BULK_H_IO                                  */
+#define CHAPSIM_R_BADCELLS 6 /* table look-ups outside the table so far    */
+
+typedef struct chapsim_io_config {
+  int32_t struct_size; /* sizeof(chapsim_io_config)                               */
+  int32_t thermal;     /* thermlflg: 1 energy equation + table properties, 0 off   */
+  double prt;          /* PRT0, Prandtl number                                     */
+  double qw_bot;       /* iso-flux bottom wall: heat flux, > 0 heats the fluid      */
+  double qw_top;       /* iso-flux top wall (WALLFLUX = -qw_top, Flow_State.f90:124-148) */
+  int32_t gravdir;     /* GRAVDIR: 0 none, 1/2/3 buoyancy along x/y/z             */
+  int32_t pad;
+  double f_a;          /* F_A, buoyancy coefficient (Flow_State.f90:98-110)         */
+} chapsim_io_config;
+
+/* Defaults: thermal on, Pr = 0.71, qw = 1 on both walls, no buoyancy. */
+int chapsim_io_config_default(chapsim_io_config *io);
+
+/* IO domain set-up (MEM_ALLOCAT + COORDJR + FISHPACK_POIS3D_INIT,
+ * src/DNS_THERMAL.f90:117-176, src/possion3d_fishpack_reform.f90:337-430):
+ * cfg gives the IO grid (nx = NCL1_io, lx = HX_io); precision must be FP64. */
+int chapsim_create_io(const chapsim_config *cfg, const chapsim_io_config *io, chapsim_ctx **out);
+
+/* Property table of an IO context: columns H, T, D, M, K (host, length n >= 4,
+ * H and T increasing), splined as NIST_SPLINE_H / NIST_SPLINE_T.  shortcuts
+ * != 0 keeps the reference-state shortcuts of the look-ups (h = 0 -> T = 1;
+ * T = 1 -> rho = mu = k = 1; cells with |h| < 1e-10 keep their properties,
+ * src/Flow_State.f90:1068,1470 and src/THERM_PROP_UPDATE.f90:168-173), which
+ * assume a table normalised so that h = 0 is the reference state; 0 evaluates
+ * the table everywhere.  Also sets RHOHmax (src/Flow_State.f90:963-990). */
+int chapsim_set_table(chapsim_ctx *ctx, const double *H, const double *T, const double *D, const double *M,
+                      const double *K, int n, int shortcuts);
+
+/* SOLVERRK3_ENG_IO(NS) (src/SOLVERRK3_ENG_IO.f90:1-77): energy RHS, rho h
+ * update with the RHOHmax limiter, ENTHALPY/DENSITY_UPDATE,
+ * THERM_PROP_UPDATE and the iso-flux wall ghosts. */
+int chapsim_rk3_eng_io(chapsim_ctx *ctx, int ns);
+/* SOLVERRK3_MOM_IO(NS) (src/SOLVERRK3_MOM_IO.f90:1-168).  For ns >= 1 it is
+ * preceded by what SOLVE runs between the energy and momentum substeps
+ * (src/SOLVE.f90:121-132): DENSITY_TIME_DERIVATION, DENSITY_Staggered,
+ * MU_Staggered (formed on the fly) and VELOCITY_CALC_io. */
+int chapsim_rk3_mom_io(chapsim_ctx *ctx, int ns);
+/* nsteps full steps: for NS = 1, 2, 3, eng (thermal) then mom. */
+int chapsim_step_io(chapsim_ctx *ctx, int nsteps);
 
 
 /* ======================================================================

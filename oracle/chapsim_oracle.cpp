@@ -337,6 +337,21 @@ oracle_tg *oracle_tg_create(int nx, int ny, int nz, double lx, double lz, double
 }
 
 void oracle_tg_destroy(oracle_tg *o) { delete o; }
+
+// The complex DFT above, shared with the IO-section oracle.
+struct oracle_dft {
+  Dft d;
+};
+oracle_dft *oracle_dft_create(int n) {
+  if (n < 1) return nullptr;
+  oracle_dft *f = new oracle_dft();
+  f->d.init(n);
+  return f;
+}
+void oracle_dft_destroy(oracle_dft *f) { delete f; }
+void oracle_dft_run(const oracle_dft *f, const double *in, double *out, int sign, double *tmp) {
+  f->d.run(reinterpret_cast<const cplx *>(in), reinterpret_cast<cplx *>(out), sign, reinterpret_cast<cplx *>(tmp));
+}
 int64_t oracle_tg_field_len(const oracle_tg *o) { return o->len(); }
 
 static std::vector<double> *field_ptr(oracle_tg *o, int id) {

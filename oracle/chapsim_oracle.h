@@ -75,6 +75,57 @@ double oracle_tg_bulk(const oracle_tg *o);     /* BULK_VELOCITY_TG */
 double oracle_tg_pois_residual(const oracle_tg *o);
 
 /* Number of OpenMP threads used (0 = library default). */
+/* Complex DFT (interleaved re/im, unnormalised; sign -1 forward, +1
+ * inverse); tmp holds n complex values. */
+typedef struct oracle_dft oracle_dft;
+oracle_dft *oracle_dft_create(int n);
+void oracle_dft_destroy(oracle_dft *f);
+void oracle_dft_run(const oracle_dft *f, const double *in, double *out, int sign, double *tmp);
+
+/* ------------------------------------------------------------------------
+ * IO section: SOLVERRK3_ENG_IO + SOLVERRK3_MOM_IO of an x-periodic channel
+ * (BCX_io = 3, no TG section) with the explicit viscous scheme
+ * (visthemflg = 0), FISHPACK_POIS3D_SIMPLE Poisson solve, and, when thermal
+ * is on, the energy equation with table properties and iso-flux walls.
+ * Fields keep the layout F(1:nx, 0:ny+1, 1:nz) (no x ghosts: x is periodic).
+ */
+typedef struct oracle_io oracle_io;
+enum {
+  ORC_IO_GX = 20, ORC_IO_GY = 21, ORC_IO_GZ = 22,      /* G_io(:,:,:,1..3) */
+  ORC_IO_G0X = 23, ORC_IO_G0Y = 24, ORC_IO_G0Z = 25,   /* G0_io */
+  ORC_IO_H = 26, ORC_IO_T = 27, ORC_IO_D = 28,         /* ENTHALPY, TEMPERATURE, DENSITY */
+  ORC_IO_MU = 29, ORC_IO_K = 30, ORC_IO_RHOH = 31,     /* VISCOUSITY, THERMCONDT, RHOH */
+  ORC_IO_D0 = 32, ORC_IO_MU0 = 33, ORC_IO_DRHO = 34,   /* DENSITY0, VISCOUSITY0, DrhoDtP */
+  ORC_IO_EX0X = 35, ORC_IO_EX0Y = 36, ORC_IO_EX0Z = 37,/* EXPLT0_io(:,:,:,1..3) */
+  ORC_IO_RHSE0 = 38                                     /* RHS_ENERGY0 */
+};
+/* qw_bot / qw_top: non-dimensional wall heat flux, positive heats the fluid
+ * (WALLFLUX = +qw on the bottom wall, -qw on the top, Flow_State.f90:124-148).
+ * gravdir 0 = none, else the buoyancy direction with coefficient f_a. */
+oracle_io *oracle_io_create(int nx, int ny, int nz, double lx, double lz, double str2, int istr2, double ren,
+                            double dt, int flowdrvtp, double cfgv, int thermal, double prt, double qw_bot,
+                            double qw_top, int gravdir, double f_a);
+void oracle_io_destroy(oracle_io *o);
+/* Table columns H, T, D, M, K (length n, H and T increasing).  shortcuts != 0
+ * keeps the reference-state shortcuts (h = 0 -> T = 1, T = 1 -> rho = mu =
+ * k = 1, cells with |h| < 1e-10 keep their properties), which assume the
+ * reference table normalisation. */
+int oracle_io_set_table(oracle_io *o, const double *H, const double *T, const double *D, const double *M,
+                        const double *K, int n, int shortcuts);
+double oracle_io_rhohmax(const oracle_io *o);
+void oracle_io_init_random(oracle_io *o, uint64_t seed, double amp);
+int oracle_io_eng(oracle_io *o, int ns);      /* SOLVERRK3_ENG_IO(ns) */
+int oracle_io_mom(oracle_io *o, int ns);      /* ns >= 1: DENSITY_TIME_DERIVATION, DENSITY_/MU_Staggered,
+                                                 VELOCITY_CALC_io, then SOLVERRK3_MOM_IO(ns); ns = 0: MOM only */
+int oracle_io_substep(oracle_io *o, int ns);  /* eng (thermal) + mom */
+int oracle_io_step(oracle_io *o);
+int oracle_io_get_field(const oracle_io *o, int id, double *out);
+int oracle_io_set_field(oracle_io *o, int id, const double *in);
+double oracle_io_divmax(const oracle_io *o);   /* DIVGCK_io: max|div G + DrhoDtP| */
+double oracle_io_divmax_q(const oracle_io *o); /* max|div u| */
+double oracle_io_bulk(const oracle_io *o, int what); /* 0 BULK_VELOCITY_IO, 1 BULK_MASSFLUX_IO, 2 BULK_H_IO */
+int64_t oracle_io_bad_cells(const oracle_io *o);     /* table look-ups outside the table so far */
+
 void oracle_set_threads(int n);
 int oracle_get_threads(void);
 

@@ -1,0 +1,1083 @@
+// CPU FP64 oracle for the CHAPSim IO-section substep (x-periodic channel).
+//
+// TEST INFRASTRUCTURE ONLY: the checker for the CUDA IO path.  The product
+// never links or calls it.  Parity against reference outputs is unpinned (the
+// Fortran reference cannot be built here and ships no golden data).
+//
+// Restates (paths relative to the CHAPSim1WW project root), channel branches
+// only, so RCCI1 = RCCI2 = RNDI1 = RNDI2 = 1 (src/COORDJR.f90:20-23), the
+// explicit viscous scheme (visthemflg = 0, src/readdata.ini:23), no weighted
+// pressure, x periodic (BCX_io = 3: IPV_io/IMV_io wrap, src/INDEXSET.f90:24-32):
+//   SOLVERRK3_ENG_IO        src/SOLVERRK3_ENG_IO.f90:1-77
+//   RHS_ENERGY_EXPLICIT     src/RHS_ENERGY_EXPLICIT.f90:1-150
+//   ENTHALPY/DENSITY_UPDATE, THERM_PROP_UPDATE, DENSITY_TIME_DERIVATION
+//                           src/THERM_PROP_UPDATE.f90:2-291
+//   NIST_SLEVAL_*           src/Flow_State.f90:1015-1690 (binary search,
+//                           cubic, out of range = error, reference shortcuts)
+//   RHOHmax                 src/Flow_State.f90:963-990
+//   BC_WALL_ISOFLUX         src/BC_WALL.f90:522-627
+//   DENSITY/MU_Staggered, VELOCITY_CALC_io, MASSFLUX_CALC_IO
+//                           src/MASSFLUX_CALC_IO.f90:1-311
+//   SOLVERRK3_MOM_IO        src/SOLVERRK3_MOM_IO.f90:1-168
+//   CONVECTION_X/Y/Z_io     src/CONVECTION_X.f90:77-176, CONVECTION_Y.f90:125-230,
+//                           CONVECTION_Z.f90:113-200
+//   DIVG_U_io, DIVG_io      src/DIVG.f90:58-259
+//   VISCOUS_ALL_EXPLT_X/Y/Z_io  src/VISCOUS_X_EXPLICIT_io.f90:1-112,
+//                           VISCOUS_Y_EXPLICIT_io.f90 (ICHANL branch),
+//                           VISCOUS_Z_EXPLICIT_io.f90 (ICHANL branch)
+//   RHS_MOM_EXPLICIT_io     src/RHS_MOM_EXPLICIT_io.f90:1-297
+//   FISHPACK_POIS3D_SIMPLE  src/possion3d_fishpack_reform.f90:29-547 (RFFTF/
+//                           RFFTB in x and z from FFTPACK's documented
+//                           definitions, eigenvalues -4c sin^2, TRID0)
+//   PRCALC_io, MASSFLUX_UPDATE_IO, BC_WALL_G/Q/PR/DPH
+//                           src/PRESSURE_CORRECTION.f90:86-122,
+//                           src/VELO_CORRECTION.f90:107-185, src/BC_WALL.f90
+//   DIVGCK_io               src/DIVGCK.f90:60-190
+//   BULK_*_IO               src/INITIAL_FL_THEML_FLD_io.f90:385-476
+//
+// Decisions (each also stated where it applies):
+//  * The mean mode (x-slot 1, z-slot 1) of the Poisson y-solve is singular;
+//    TRID0 takes its zero branch only when the last pivot falls under 1e-14,
+//    which for that mode depends on round-off.  Here that mode always takes
+//    the zero branch (phi(ny) = 0 for the mean), the other modes use the
+//    threshold as written.
+//  * The reference-state shortcuts of the table look-ups are kept only when
+//    the table follows the reference normalisation (h = 0 <-> T = 1); the
+//    flag is set per table.
+//  * Initial field: the TG recipe (counter-based generator) for velocity,
+//    h = 0 for enthalpy with the table's properties at h = 0 (the reference
+//    writes T = rho = mu = k = 1, its normalised reference state), then the
+//    reference's CALC_INITIALIZATION_io projection.
+//  * Y ghosts of MU_STG, RHO_STG and DivU_io, filled by the periodic MPI halo
+//    exchange in the reference, are never read in the channel branch and are
+//    not formed.
+#include <cmath>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "chapsim_oracle.h"
+
+extern "C" void oracle_cubic_spline(int n, const double *x, const double *y, double *b, double *c, double *d);
+
+namespace {
+
+inline uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+// Same counter-based draw as the TG oracle and the library's initial field.
+inline double rnd_pm1(uint64_t seed, int comp, int i, int j, int k) {
+  uint64_t ctr = ((uint64_t)comp << 60) ^ ((uint64_t)k << 40) ^ ((uint64_t)j << 20) ^ (uint64_t)i;
+  uint64_t x = splitmix64(splitmix64(seed) ^ ctr);
+  double u = (double)(x >> 11) * (1.0 / 9007199254740992.0);
+  return -1.0 + 2.0 * u;
+}
+
+struct Spl {
+  std::vector<double> x, y, b, c, d;
+  int n = 0;
+  void build(const double *xs, const double *ys, int n_) {
+    n = n_;
+    x.assign(xs, xs + n);
+    y.assign(ys, ys + n);
+    b.assign(n, 0.0); c.assign(n, 0.0); d.assign(n, 0.0);
+    oracle_cubic_spline(n, x.data(), y.data(), b.data(), c.data(), d.data());
+  }
+  // NIST_SLEVAL_* (src/Flow_State.f90:1015-1070): false when u is outside
+  // (x(1), x(n)) -- the reference STOPs there.
+  bool eval(double u, double &out) const {
+    if (u <= x[0] || u >= x[n - 1]) return false;
+    int i = 0, j = n;
+    while (j > i + 1) {
+      int k = (i + j) / 2;
+      if (u < x[k]) j = k; else i = k;
+    }
+    double dx = u - x[i];
+    out = y[i] + dx * (b[i] + dx * (c[i] + dx * d[i]));
+    return true;
+  }
+};
+
+}  // namespace
+
+struct oracle_io {
+  int nx, ny, nz, istr2, flowdrvtp, thermal, gravdir;
+  double lx, lz, str2, ren, dt, cfgv, prt, qw[2], f_a;
+  double dxi, dzi, dxqi, dzqi, cvisc, cthecd, volm, area_inlet;
+  std::vector<double> ynd, ycc, dyfi, dyci, wff, wfb, amph, acph, apph;  // 1-based, size ny+2
+  double tgam[4], troh[4], talp[4];
+  // table
+  bool has_table = false;
+  int shortcuts = 0;
+  Spl ht, td, tm, tk, hd;
+  double rhohmax = 0.0;
+  int64_t bad = 0;
+  // flow fields (1..3 used)
+  std::vector<double> q[4], g[4], g0[4], explt0[4], mustg[4], rhostg[4];
+  std::vector<double> pr, dph, rhsllphi, qtmp, dphtmp, rhsz, divu, drho;
+  // thermal fields
+  std::vector<double> rhoh, hh, tt, dd, dd0, mu, mu0, kk, rhse, rhse0;
+  oracle_dft *dftx = nullptr, *dftz = nullptr;
+
+  int64_t len() const { return (int64_t)nx * (ny + 2) * nz; }
+  inline int64_t id(int i, int j, int k) const {
+    return (int64_t)(i - 1) + (int64_t)nx * ((int64_t)j + (int64_t)(ny + 2) * (k - 1));
+  }
+  inline int ip(int i) const { return i == nx ? 1 : i + 1; }
+  inline int im(int i) const { return i == 1 ? nx : i - 1; }
+  inline int kp(int k) const { return k == nz ? 1 : k + 1; }
+  inline int km(int k) const { return k == 1 ? nz : k - 1; }
+};
+
+namespace {
+
+constexpr double XND2CL = 0.5, YND2CL = 0.5, ZND2CL = 0.5;
+
+#define F(arr, i, j, k) (o->arr[o->id(i, j, k)])
+#define FC(arr, c, i, j, k) (o->arr[c][o->id(i, j, k)])
+
+int nthreads() { return oracle_get_threads(); }
+
+// ------------------------------------------------------------- table look-ups
+// h -> T, then T -> rho (DENSITY_UPDATE path, src/THERM_PROP_UPDATE.f90:74-127).
+bool lookup_ht(const oracle_io *o, double h, double &T) {
+  if (!o->ht.eval(h, T)) return false;
+  if (o->shortcuts && std::fabs(h) < 1.0e-10) T = 1.0;  // Flow_State.f90:1068
+  return true;
+}
+bool lookup_t(const oracle_io *o, const Spl &s, double T, double &v) {
+  if (!s.eval(T, v)) return false;
+  if (o->shortcuts && std::fabs(T - 1.0) < 1.0e-10) v = 1.0;  // Flow_State.f90:1470,1524,1578
+  return true;
+}
+
+// BC_WALL_ISOFLUX (src/BC_WALL.f90:522-627): ghost enthalpy extrapolated from
+// the first two cells, ghost properties from the table.
+void bc_wall_thermal(oracle_io *o) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  for (int side = 0; side < 2; ++side) {
+    const int j = side == 0 ? 0 : ny + 1;
+    for (int k = 1; k <= nz; ++k)
+      for (int i = 1; i <= nx; ++i) {
+        double h;
+        if (side == 0)
+          h = 2.0 * F(hh, i, 1, k) - o->wff[2] * F(hh, i, 2, k) - o->wfb[2] * F(hh, i, 1, k);
+        else
+          h = 2.0 * F(hh, i, ny, k) - o->wff[ny] * F(hh, i, ny, k) - o->wfb[ny] * F(hh, i, ny - 1, k);
+        F(hh, i, j, k) = h;
+        double T, M, K, D;
+        if (!lookup_ht(o, h, T) || !lookup_t(o, o->tm, T, M) || !lookup_t(o, o->tk, T, K) ||
+            !lookup_t(o, o->td, T, D)) {
+          ++o->bad;
+          continue;
+        }
+        F(dd, i, j, k) = D;
+        F(tt, i, j, k) = T;
+        F(mu, i, j, k) = M;
+        F(kk, i, j, k) = K;
+        F(rhoh, i, j, k) = h * D;
+      }
+  }
+}
+
+// RHS_ENERGY_EXPLICIT (src/RHS_ENERGY_EXPLICIT.f90:1-150), iso-flux walls.
+void rhs_energy(oracle_io *o) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  const double coe1 = o->dxi * XND2CL * 0.5, coe11 = o->dxqi * XND2CL * o->cthecd;
+  const double wallflux_bot = o->qw[0], wallflux_top = -o->qw[1];
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j) {
+      const int jp = j + 1, jm = j - 1;
+      const double coe2 = o->dyfi[j] * 0.5, coe3 = o->dzi * ZND2CL * 0.5;
+      const double coe33 = o->dzqi * ZND2CL * o->cthecd, coe22 = o->dyfi[j] * o->cthecd;
+      double coe221, coe222;
+      if (j == 1) {
+        coe221 = o->dyci[jp];
+        coe222 = 1.0;
+      } else if (j == ny) {
+        coe222 = o->dyci[j];
+        coe221 = 1.0;
+      } else {
+        coe221 = o->dyci[jp];
+        coe222 = o->dyci[j];
+      }
+      const int kpp = o->kp(k), kmm = o->km(k);
+      for (int i = 1; i <= nx; ++i) {
+        const int ipp = o->ip(i), imm = o->im(i);
+        const double hc = F(hh, i, j, k);
+        double dx_rhohu = (F(hh, ipp, j, k) + hc) * (FC(g0, 1, ipp, j, k) + FC(g, 1, ipp, j, k)) -
+                          (hc + F(hh, imm, j, k)) * (FC(g0, 1, i, j, k) + FC(g, 1, i, j, k));
+        dx_rhohu *= coe1;
+        double dy_rhohv = (o->wff[jp] * F(hh, i, jp, k) + o->wfb[jp] * hc) * (FC(g0, 2, i, jp, k) + FC(g, 2, i, jp, k)) -
+                          (o->wff[j] * hc + o->wfb[j] * F(hh, i, jm, k)) * (FC(g0, 2, i, j, k) + FC(g, 2, i, j, k));
+        dy_rhohv *= coe2;
+        double dz_rhohw = (F(hh, i, j, kpp) + hc) * (FC(g0, 3, i, j, kpp) + FC(g, 3, i, j, kpp)) -
+                          (hc + F(hh, i, j, kmm)) * (FC(g0, 3, i, j, k) + FC(g, 3, i, j, k));
+        dz_rhohw *= coe3;
+        const double tc = F(tt, i, j, k), kc = F(kk, i, j, k);
+        double dx_kdt = (F(kk, ipp, j, k) + kc) * (F(tt, ipp, j, k) - tc) - (kc + F(kk, imm, j, k)) * (tc - F(tt, imm, j, k));
+        dx_kdt *= coe11;
+        double kdty1 = (o->wff[jp] * F(kk, i, jp, k) + o->wfb[jp] * kc) * (F(tt, i, jp, k) - tc) * coe221;
+        double kdty2 = (o->wff[j] * kc + o->wfb[j] * F(kk, i, jm, k)) * (tc - F(tt, i, jm, k)) * coe222;
+        if (j == 1)
+          kdty2 = -wallflux_bot * coe222;
+        else if (j == ny)
+          kdty1 = -wallflux_top * coe221;
+        const double dy_kdt = (kdty1 - kdty2) * coe22;
+        double dz_kdt = (F(kk, i, j, kpp) + kc) * (F(tt, i, j, kpp) - tc) - (F(kk, i, j, kmm) + kc) * (tc - F(tt, i, j, kmm));
+        dz_kdt *= coe33;
+        F(rhse, i, j, k) = -dx_rhohu - dy_rhohv - dz_rhohw + dx_kdt + dy_kdt + dz_kdt;
+      }
+    }
+}
+
+// ------------------------------------------------------------- staggering
+// DENSITY_Staggered (src/MASSFLUX_CALC_IO.f90:242-311).
+void density_staggered(oracle_io *o) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  if (!o->thermal) {
+    for (int c = 1; c <= 3; ++c) std::fill(o->rhostg[c].begin(), o->rhostg[c].end(), 1.0);
+    return;
+  }
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j) {
+      const int kmm = o->km(k);
+      for (int i = 1; i <= nx; ++i) {
+        const int imm = o->im(i);
+        FC(rhostg, 1, i, j, k) = (F(dd, i, j, k) + F(dd, imm, j, k) + F(dd0, i, j, k) + F(dd0, imm, j, k)) * XND2CL * 0.5;
+        FC(rhostg, 3, i, j, k) = (F(dd, i, j, k) + F(dd, i, j, kmm) + F(dd0, i, j, k) + F(dd0, i, j, kmm)) * ZND2CL * 0.5;
+        if (j >= 2)
+          FC(rhostg, 2, i, j, k) = (o->wff[j] * (F(dd, i, j, k) + F(dd0, i, j, k)) +
+                                    o->wfb[j] * (F(dd, i, j - 1, k) + F(dd0, i, j - 1, k))) * 0.5;
+      }
+    }
+  for (int k = 1; k <= nz; ++k)
+    for (int i = 1; i <= nx; ++i) {
+      FC(rhostg, 2, i, 1, k) = 0.5 * (F(dd0, i, 0, k) + F(dd, i, 0, k));
+      FC(rhostg, 2, i, ny + 1, k) = 0.5 * (F(dd0, i, ny + 1, k) + F(dd, i, ny + 1, k));
+    }
+}
+
+// MU_Staggered (src/MASSFLUX_CALC_IO.f90:147-237).
+void mu_staggered(oracle_io *o) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  if (!o->thermal) {
+    for (int c = 1; c <= 3; ++c) std::fill(o->mustg[c].begin(), o->mustg[c].end(), 1.0);
+    return;
+  }
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j) {
+      const int kmm = o->km(k);
+      for (int i = 1; i <= nx; ++i) {
+        const int imm = o->im(i);
+        if (j >= 2) {
+          FC(mustg, 1, i, j, k) =
+              ((F(mu, i, j, k) + F(mu, imm, j, k) + F(mu0, i, j, k) + F(mu0, imm, j, k)) * o->wff[j] +
+               (F(mu, i, j - 1, k) + F(mu, imm, j - 1, k) + F(mu0, i, j - 1, k) + F(mu0, imm, j - 1, k)) * o->wfb[j]) *
+              XND2CL * 0.5;
+          FC(mustg, 3, i, j, k) =
+              ((F(mu, i, j, kmm) + F(mu, i, j, k) + F(mu0, i, j, kmm) + F(mu0, i, j, k)) * o->wff[j] +
+               (F(mu, i, j - 1, kmm) + F(mu, i, j - 1, k) + F(mu0, i, j - 1, kmm) + F(mu0, i, j - 1, k)) * o->wfb[j]) *
+              ZND2CL * 0.5;
+        }
+        FC(mustg, 2, i, j, k) = (F(mu, i, j, k) + F(mu, imm, j, k) + F(mu0, i, j, k) + F(mu0, imm, j, k) +
+                                 F(mu, i, j, kmm) + F(mu, imm, j, kmm) + F(mu0, i, j, kmm) + F(mu0, imm, j, kmm)) *
+                                XND2CL * ZND2CL * 0.5;
+      }
+    }
+  for (int k = 1; k <= nz; ++k)
+    for (int i = 1; i <= nx; ++i) {
+      const double b = 0.5 * (F(mu0, i, 0, k) + F(mu, i, 0, k));
+      const double t = 0.5 * (F(mu0, i, ny + 1, k) + F(mu, i, ny + 1, k));
+      FC(mustg, 1, i, 1, k) = b;
+      FC(mustg, 3, i, 1, k) = b;
+      FC(mustg, 1, i, ny + 1, k) = t;
+      FC(mustg, 3, i, ny + 1, k) = t;
+    }
+}
+
+// BC_WALL_Q / BC_WALL_G (src/BC_WALL.f90:185-263, 412-458).
+void bc_wall_vec(oracle_io *o, std::vector<double> *f) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  for (int k = 1; k <= nz; ++k)
+    for (int i = 1; i <= nx; ++i) {
+      f[1][o->id(i, 0, k)] = 0.0;
+      f[3][o->id(i, 0, k)] = 0.0;
+      f[2][o->id(i, 1, k)] = 0.0;
+      f[2][o->id(i, 0, k)] = 0.0;
+      f[1][o->id(i, ny + 1, k)] = 0.0;
+      f[3][o->id(i, ny + 1, k)] = 0.0;
+      f[2][o->id(i, ny + 1, k)] = 0.0;
+    }
+}
+// BC_WALL_PR / BC_WALL_DPH: zero normal gradient by copy.
+void bc_wall_copy(oracle_io *o, std::vector<double> &f) {
+  for (int k = 1; k <= o->nz; ++k)
+    for (int i = 1; i <= o->nx; ++i) {
+      f[o->id(i, 0, k)] = f[o->id(i, 1, k)];
+      f[o->id(i, o->ny + 1, k)] = f[o->id(i, o->ny, k)];
+    }
+}
+
+// VELOCITY_CALC_io (src/MASSFLUX_CALC_IO.f90:82-142).
+void velocity_calc(oracle_io *o) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        FC(q, 1, i, j, k) = FC(g, 1, i, j, k) / FC(rhostg, 1, i, j, k);
+        FC(q, 3, i, j, k) = FC(g, 3, i, j, k) / FC(rhostg, 3, i, j, k);
+        if (j >= 2) FC(q, 2, i, j, k) = FC(g, 2, i, j, k) / FC(rhostg, 2, i, j, k);
+      }
+  bc_wall_vec(o, o->q);
+}
+
+// DENSITY_TIME_DERIVATION (src/THERM_PROP_UPDATE.f90:225-291), the division by
+// (gamma - 2) as written.
+void density_time_derivation(oracle_io *o, int ns) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  const double gp = o->tgam[ns] + o->troh[ns], zr = o->troh[ns], den = o->tgam[ns] - 2.0;
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        const int ipp = o->ip(i), kpp = o->kp(k);
+        const double divx = (FC(g, 1, ipp, j, k) - FC(g, 1, i, j, k)) * o->dxi;
+        const double divx0 = (FC(g0, 1, ipp, j, k) - FC(g0, 1, i, j, k)) * o->dxi;
+        const double divy = (FC(g, 2, i, j + 1, k) - FC(g, 2, i, j, k)) * o->dyfi[j];
+        const double divy0 = (FC(g0, 2, i, j + 1, k) - FC(g0, 2, i, j, k)) * o->dyfi[j];
+        const double divz = (FC(g, 3, i, j, kpp) - FC(g, 3, i, j, k)) * o->dzi;
+        const double divz0 = (FC(g0, 3, i, j, kpp) - FC(g0, 3, i, j, k)) * o->dzi;
+        F(drho, i, j, k) = (gp * (divx + divy + divz) + zr * (divx0 + divy0 + divz0)) / den;
+      }
+}
+
+// ------------------------------------------------------------- momentum
+void convection(oracle_io *o) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  std::fill(o->qtmp.begin(), o->qtmp.end(), 0.0);
+  std::fill(o->dphtmp.begin(), o->dphtmp.end(), 0.0);
+  std::fill(o->rhsz.begin(), o->rhsz.end(), 0.0);
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j) {
+      const int jp = j + 1, jm = j - 1, kpp = o->kp(k), kmm = o->km(k);
+      for (int i = 1; i <= nx; ++i) {
+        const int ipp = o->ip(i), imm = o->im(i);
+        // CONVECTION_X_io (src/CONVECTION_X.f90:98-140)
+        {
+          const double coe1 = o->dxi * XND2CL * XND2CL, coe3 = o->dzi * XND2CL * ZND2CL;
+          const double coe2 = o->dyfi[j] * XND2CL, coe32 = coe3;
+          double h11f = (FC(g, 1, ipp, j, k) + FC(g, 1, i, j, k)) * (FC(q, 1, ipp, j, k) + FC(q, 1, i, j, k));
+          double h11b = (FC(g, 1, i, j, k) + FC(g, 1, imm, j, k)) * (FC(q, 1, i, j, k) + FC(q, 1, imm, j, k));
+          double h11 = (h11f - h11b) * coe1;
+          double h12f = (FC(g, 2, i, jp, k) + FC(g, 2, imm, jp, k)) *
+                        (o->wff[jp] * FC(q, 1, i, jp, k) + o->wfb[jp] * FC(q, 1, i, j, k));
+          double h12b = (FC(g, 2, i, j, k) + FC(g, 2, imm, j, k)) *
+                        (o->wff[j] * FC(q, 1, i, j, k) + o->wfb[j] * FC(q, 1, i, jm, k));
+          double h12 = (h12f - h12b) * coe2;
+          double h13f = (FC(g, 3, i, j, kpp) + FC(g, 3, imm, j, kpp)) * (FC(q, 1, i, j, kpp) + FC(q, 1, i, j, k));
+          double h13b = (FC(g, 3, i, j, k) + FC(g, 3, imm, j, k)) * (FC(q, 1, i, j, k) + FC(q, 1, i, j, kmm));
+          double h13 = (h13f - h13b) * coe32;
+          F(qtmp, i, j, k) = -(h11 + h12 + h13);
+        }
+        // CONVECTION_Y_io (src/CONVECTION_Y.f90:150-200), j >= 2
+        if (j >= 2) {
+          const double coe1 = o->dxi * XND2CL, coe2 = o->dyci[j] * YND2CL * YND2CL, coe31 = o->dzi * ZND2CL;
+          double h21f = (o->wff[j] * FC(g, 1, ipp, j, k) + o->wfb[j] * FC(g, 1, ipp, jm, k)) *
+                        (FC(q, 2, ipp, j, k) + FC(q, 2, i, j, k));
+          double h21b = (o->wff[j] * FC(g, 1, i, j, k) + o->wfb[j] * FC(g, 1, i, jm, k)) *
+                        (FC(q, 2, i, j, k) + FC(q, 2, imm, j, k));
+          double h21 = (h21f - h21b) * coe1;
+          double h22f = (FC(g, 2, i, jp, k) + FC(g, 2, i, j, k)) * (FC(q, 2, i, jp, k) + FC(q, 2, i, j, k));
+          double h22b = (FC(g, 2, i, j, k) + FC(g, 2, i, jm, k)) * (FC(q, 2, i, j, k) + FC(q, 2, i, jm, k));
+          double h22 = (h22f - h22b) * coe2;
+          double h23f = (o->wff[j] * FC(g, 3, i, j, kpp) + o->wfb[j] * FC(g, 3, i, jm, kpp)) *
+                        (FC(q, 2, i, j, kpp) + FC(q, 2, i, j, k));
+          double h23b = (o->wff[j] * FC(g, 3, i, j, k) + o->wfb[j] * FC(g, 3, i, jm, k)) *
+                        (FC(q, 2, i, j, k) + FC(q, 2, i, j, kmm));
+          double h23 = (h23f - h23b) * coe31;
+          F(dphtmp, i, j, k) = -(h21 + h22 + h23);
+        }
+        // CONVECTION_Z_io (src/CONVECTION_Z.f90:133-170)
+        {
+          const double coe1 = o->dxi * XND2CL * ZND2CL, coe2 = o->dyfi[j] * ZND2CL, coe31 = o->dzi * ZND2CL * ZND2CL;
+          double h31f = (FC(g, 1, ipp, j, k) + FC(g, 1, ipp, j, kmm)) * (FC(q, 3, ipp, j, k) + FC(q, 3, i, j, k));
+          double h31b = (FC(g, 1, i, j, k) + FC(g, 1, i, j, kmm)) * (FC(q, 3, i, j, k) + FC(q, 3, imm, j, k));
+          double h31 = (h31f - h31b) * coe1;
+          double h32f = (FC(g, 2, i, jp, k) + FC(g, 2, i, jp, kmm)) *
+                        (o->wff[jp] * FC(q, 3, i, jp, k) + o->wfb[jp] * FC(q, 3, i, j, k));
+          double h32b = (FC(g, 2, i, j, k) + FC(g, 2, i, j, kmm)) *
+                        (o->wff[j] * FC(q, 3, i, j, k) + o->wfb[j] * FC(q, 3, i, jm, k));
+          double h32 = (h32f - h32b) * coe2;
+          double h33f = (FC(g, 3, i, j, kpp) + FC(g, 3, i, j, k)) * (FC(q, 3, i, j, kpp) + FC(q, 3, i, j, k));
+          double h33b = (FC(g, 3, i, j, k) + FC(g, 3, i, j, kmm)) * (FC(q, 3, i, j, k) + FC(q, 3, i, j, kmm));
+          double h33 = (h33f - h33b) * coe31;
+          F(rhsz, i, j, k) = -(h31 + h32 + h33);
+        }
+      }
+    }
+}
+
+// DIVG_U_io (src/DIVG.f90:153-259): div u / 3 at cell centres.
+void divg_u(oracle_io *o) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        const double divx = (FC(q, 1, o->ip(i), j, k) - FC(q, 1, i, j, k)) * o->dxi;
+        const double divy = (FC(q, 2, i, j + 1, k) - FC(q, 2, i, j, k)) * o->dyfi[j];
+        const double divz = (FC(q, 3, i, j, o->kp(k)) - FC(q, 3, i, j, k)) * o->dzi;
+        F(divu, i, j, k) = (divx + divy + divz) / 3.0;
+      }
+}
+
+// 0.5 (mu0 + mu) at a cell centre.
+inline double muc(const oracle_io *o, int i, int j, int k) { return 0.5 * (F(mu0, i, j, k) + F(mu, i, j, k)); }
+
+// VISCOUS_ALL_EXPLT_X/Y/Z_io, channel branch.
+void viscous(oracle_io *o) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  const double cv = o->cvisc;
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j) {
+      const int jp = j + 1, jm = j - 1, kpp = o->kp(k), kmm = o->km(k);
+      for (int i = 1; i <= nx; ++i) {
+        const int ipp = o->ip(i), imm = o->im(i);
+        // X (src/VISCOUS_X_EXPLICIT_io.f90:38-104)
+        {
+          const double coe1 = 2.0 * o->dxi * cv, coe3 = o->dzi * cv, coe2 = o->dyfi[j] * cv, coe32 = coe3;
+          double dudx = (FC(q, 1, ipp, j, k) - FC(q, 1, i, j, k)) * o->dxi;
+          double tau11f = muc(o, i, j, k) * (dudx - F(divu, i, j, k));
+          dudx = (FC(q, 1, i, j, k) - FC(q, 1, imm, j, k)) * o->dxi;
+          double tau11b = muc(o, imm, j, k) * (dudx - F(divu, imm, j, k));
+          double d11 = (tau11f - tau11b) * coe1;
+          double vis12p = FC(mustg, 1, i, jp, k);
+          double dudy = (FC(q, 1, i, jp, k) - FC(q, 1, i, j, k)) * o->dyci[jp];
+          double dvdx = (FC(q, 2, i, jp, k) - FC(q, 2, imm, jp, k)) * o->dxi;
+          double tau12f = vis12p * (dudy + dvdx);
+          double vis12c = FC(mustg, 1, i, j, k);
+          dudy = (FC(q, 1, i, j, k) - FC(q, 1, i, jm, k)) * o->dyci[j];
+          dvdx = (FC(q, 2, i, j, k) - FC(q, 2, imm, j, k)) * o->dxi;
+          double tau12b = vis12c * (dudy + dvdx);
+          double d12 = (tau12f - tau12b) * coe2;
+          double vis13p = FC(mustg, 2, i, j, kpp);
+          double dudz = (FC(q, 1, i, j, kpp) - FC(q, 1, i, j, k)) * o->dzi;
+          double dwdx = (FC(q, 3, i, j, kpp) - FC(q, 3, imm, j, kpp)) * o->dxi;
+          double tau13f = vis13p * (dudz + dwdx);
+          double vis13c = FC(mustg, 2, i, j, k);
+          dudz = (FC(q, 1, i, j, k) - FC(q, 1, i, j, kmm)) * o->dzi;
+          dwdx = (FC(q, 3, i, j, k) - FC(q, 3, imm, j, k)) * o->dxi;
+          double tau13b = vis13c * (dudz + dwdx);
+          double d13 = (tau13f - tau13b) * coe32;
+          F(qtmp, i, j, k) = F(qtmp, i, j, k) + d11 + d12 + d13;
+        }
+        // Y, j >= 2 (src/VISCOUS_Y_EXPLICIT_io.f90, ICHANL branch)
+        if (j >= 2) {
+          const double coe1 = o->dxi * cv, coe3 = o->dzi * cv, coe2 = 2.0 * o->dyci[j] * cv;
+          double dvdy = (FC(q, 2, i, jp, k) - FC(q, 2, i, j, k)) * o->dyfi[j];
+          double tau22f = muc(o, i, j, k) * (dvdy - F(divu, i, j, k));
+          dvdy = (FC(q, 2, i, j, k) - FC(q, 2, i, jm, k)) * o->dyfi[jm];
+          double tau22b = muc(o, i, jm, k) * (dvdy - F(divu, i, jm, k));
+          double d22 = (tau22f - tau22b) * coe2;
+          double vis21p = FC(mustg, 1, ipp, j, k);
+          double dvdx = (FC(q, 2, ipp, j, k) - FC(q, 2, i, j, k)) * o->dxi;
+          double dudy = (FC(q, 1, ipp, j, k) - FC(q, 1, ipp, jm, k)) * o->dyci[j];
+          double tau21f = vis21p * (dvdx + dudy);
+          double vis21c = FC(mustg, 1, i, j, k);
+          dvdx = (FC(q, 2, i, j, k) - FC(q, 2, imm, j, k)) * o->dxi;
+          dudy = (FC(q, 1, i, j, k) - FC(q, 1, i, jm, k)) * o->dyci[j];
+          double tau21b = vis21c * (dvdx + dudy);
+          double d21 = (tau21f - tau21b) * coe1;
+          double vis23p = FC(mustg, 3, i, j, kpp);
+          double dvdz = (FC(q, 2, i, j, kpp) - FC(q, 2, i, j, k)) * o->dzi;
+          double dwdy = (FC(q, 3, i, j, kpp) - FC(q, 3, i, jm, kpp)) * o->dyci[j];
+          double tau23f = vis23p * (dvdz + dwdy);
+          double vis23c = FC(mustg, 3, i, j, k);
+          dvdz = (FC(q, 2, i, j, k) - FC(q, 2, i, j, kmm)) * o->dzi;
+          dwdy = (FC(q, 3, i, j, k) - FC(q, 3, i, jm, k)) * o->dyci[j];
+          double tau23b = vis23c * (dvdz + dwdy);
+          double d23 = (tau23f - tau23b) * coe3;
+          F(dphtmp, i, j, k) = F(dphtmp, i, j, k) + d21 + d22 + d23;
+        }
+        // Z (src/VISCOUS_Z_EXPLICIT_io.f90, ICHANL branch)
+        {
+          const double coe1 = o->dxi * cv, coe3 = 2.0 * o->dzi * cv, coe2 = o->dyfi[j] * cv;
+          double dwdz = (FC(q, 3, i, j, kpp) - FC(q, 3, i, j, k)) * o->dzi;
+          double tau33f = muc(o, i, j, k) * (dwdz - F(divu, i, j, k));
+          dwdz = (FC(q, 3, i, j, k) - FC(q, 3, i, j, kmm)) * o->dzi;
+          double tau33b = muc(o, i, j, kmm) * (dwdz - F(divu, i, j, kmm));
+          double d33 = (tau33f - tau33b) * coe3;
+          double vis31p = FC(mustg, 2, ipp, j, k);
+          double dwdx = (FC(q, 3, ipp, j, k) - FC(q, 3, i, j, k)) * o->dxi;
+          double dudz = (FC(q, 1, ipp, j, k) - FC(q, 1, ipp, j, kmm)) * o->dzi;
+          double tau31f = vis31p * (dwdx + dudz);
+          double vis31c = FC(mustg, 2, i, j, k);
+          dwdx = (FC(q, 3, i, j, k) - FC(q, 3, imm, j, k)) * o->dxi;
+          dudz = (FC(q, 1, i, j, k) - FC(q, 1, i, j, kmm)) * o->dzi;
+          double tau31b = vis31c * (dwdx + dudz);
+          double d31 = (tau31f - tau31b) * coe1;
+          double vis32p = FC(mustg, 3, i, jp, k);
+          double dwdy = (FC(q, 3, i, jp, k) - FC(q, 3, i, j, k)) * o->dyci[jp];
+          double dvdz = (FC(q, 2, i, jp, k) - FC(q, 2, i, jp, kmm)) * o->dzi;
+          double tau32f = vis32p * (dwdy + dvdz);
+          double vis32c = FC(mustg, 3, i, j, k);
+          dwdy = (FC(q, 3, i, j, k) - FC(q, 3, i, jm, k)) * o->dyci[j];
+          dvdz = (FC(q, 2, i, j, k) - FC(q, 2, i, j, kmm)) * o->dzi;
+          double tau32b = vis32c * (dwdy + dvdz);
+          double d32 = (tau32f - tau32b) * coe2;
+          F(rhsz, i, j, k) = F(rhsz, i, j, k) + d31 + d32 + d33;
+        }
+      }
+    }
+}
+
+// RHS_MOM_EXPLICIT_io(NS, IDR) (src/RHS_MOM_EXPLICIT_io.f90:1-297) for one
+// component; tmp holds EXPLT on entry and RHS_io on exit.
+void rhs_mom(oracle_io *o, int ns, int idr, std::vector<double> &tmp) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  const int nyi = idr == 2 ? 2 : 1;
+  const double gam = o->tgam[ns], roh = o->troh[ns], alp = o->talp[ns], dt = o->dt;
+  for (int k = 1; k <= nz; ++k)
+    for (int j = nyi; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        const int64_t c = o->id(i, j, k);
+        const double rhsc = tmp[c], rhsl = o->explt0[idr][c];
+        double r = (gam * rhsc + roh * rhsl) * dt;
+        o->explt0[idr][c] = rhsc;
+        double pgm;
+        if (idr == 1)
+          pgm = (F(pr, i, j, k) - F(pr, o->im(i), j, k)) * (alp * dt * o->dxi);
+        else if (idr == 2)
+          pgm = (F(pr, i, j, k) - F(pr, i, j - 1, k)) * (alp * dt * o->dyci[j]);
+        else
+          pgm = (F(pr, i, j, k) - F(pr, i, j, o->km(k))) * (alp * dt * o->dzi);
+        r -= pgm;
+        if (o->gravdir == idr) r += o->rhostg[idr][c] * (alp * dt * o->f_a);
+        tmp[c] = r;
+      }
+  if (idr == 1) {  // NFLOW = 1, no TG section
+    double dpgrns = 0.0;
+    if (o->flowdrvtp == 1) {
+      double s = 0.0;
+      for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i)
+          for (int k = 1; k <= nz; ++k) s += tmp[o->id(i, j, k)] / o->dyfi[j];
+      dpgrns = s / o->volm;
+    } else if (o->flowdrvtp == 2) {
+      dpgrns = -0.5 * o->cfgv * alp * dt;
+    }
+    for (int k = 1; k <= nz; ++k)
+      for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) tmp[o->id(i, j, k)] -= dpgrns;
+  }
+}
+
+// FFTPACK RFFTF / RFFTB by their documented definitions, through the complex
+// DFT: forward r(1) = sum x, r(2m) = sum x cos, r(2m+1) = -sum x sin,
+// r(n) = sum (-1)^i x for even n; backward the unnormalised synthesis.
+void rfftf(const oracle_dft *f, int n, double *x, double *w) {
+  double *in = w, *out = w + 2 * n, *tmp = w + 4 * n;
+  for (int i = 0; i < n; ++i) { in[2 * i] = x[i]; in[2 * i + 1] = 0.0; }
+  oracle_dft_run(f, in, out, -1, tmp);
+  x[0] = out[0];
+  for (int m = 1; 2 * m < n; ++m) { x[2 * m - 1] = out[2 * m]; x[2 * m] = out[2 * m + 1]; }
+  if (n % 2 == 0) x[n - 1] = out[n];
+}
+void rfftb(const oracle_dft *f, int n, double *x, double *w) {
+  double *in = w, *out = w + 2 * n, *tmp = w + 4 * n;
+  in[0] = x[0]; in[1] = 0.0;
+  for (int m = 1; 2 * m < n; ++m) {
+    in[2 * m] = x[2 * m - 1]; in[2 * m + 1] = x[2 * m];
+    in[2 * (n - m)] = x[2 * m - 1]; in[2 * (n - m) + 1] = -x[2 * m];
+  }
+  if (n % 2 == 0) { in[n] = x[n - 1]; in[n + 1] = 0.0; }
+  oracle_dft_run(f, in, out, +1, tmp);
+  for (int i = 0; i < n; ++i) x[i] = out[2 * i];
+}
+// FFTPACK_ROOT_1D, LP = 1 (src/possion3d_fishpack_reform.f90:98-110).
+std::vector<double> roots_periodic(int l, double c) {
+  std::vector<double> rt(l + 1, 0.0);  // 1-based
+  const double dx = M_PI / (2.0 * (double)l);
+  rt[1] = 0.0;
+  rt[l] = -4.0 * c;
+  for (int i = 3; i <= l; i += 2) {
+    const double s = std::sin((double)(i - 1) * dx);
+    rt[i - 1] = -4.0 * c * s * s;
+    rt[i] = rt[i - 1];
+  }
+  return rt;
+}
+
+// FISHPACK_POIS3D_SIMPLE (src/possion3d_fishpack_reform.f90:431-547) for
+// BCX_io = BCZ = periodic: RHSLLPHI -> DPH (interior), ghosts by copy.
+void fishpack_pois3d(oracle_io *o) {
+  const int l = o->nx, m = o->nz, ng = o->ny;
+  std::vector<double> fr((size_t)l * m * ng);  // FR(I, K, J): x fastest, then z, then y
+  auto FR = [&](int i, int k, int j) -> double & { return fr[(size_t)(i - 1) + (size_t)l * ((k - 1) + (size_t)m * (j - 1))]; };
+  for (int j = 1; j <= ng; ++j)
+    for (int k = 1; k <= m; ++k)
+      for (int i = 1; i <= l; ++i) FR(i, k, j) = F(rhsllphi, i, j, k);
+  const std::vector<double> xrt = roots_periodic(l, o->dxqi), yrt = roots_periodic(m, o->dzqi);
+  const int nmax = std::max(l, m);
+#pragma omp parallel num_threads(nthreads())
+  {
+    std::vector<double> w(6 * nmax), t(nmax);
+#pragma omp for schedule(static)
+    for (int j = 1; j <= ng; ++j) {
+      for (int k = 1; k <= m; ++k) {
+        for (int i = 1; i <= l; ++i) t[i - 1] = FR(i, k, j);
+        rfftf(o->dftx, l, t.data(), w.data());
+        for (int i = 1; i <= l; ++i) FR(i, k, j) = t[i - 1];
+      }
+      for (int i = 1; i <= l; ++i) {
+        for (int k = 1; k <= m; ++k) t[k - 1] = FR(i, k, j);
+        rfftf(o->dftz, m, t.data(), w.data());
+        for (int k = 1; k <= m; ++k) FR(i, k, j) = t[k - 1];
+      }
+    }
+  }
+  // TRID0 per (x-slot, z-slot) along y (:490-505, :33-63).
+#pragma omp parallel num_threads(nthreads())
+  {
+    std::vector<double> bb(ng + 1), tt(ng + 1), dd(ng + 1);
+#pragma omp for collapse(2) schedule(static)
+    for (int k = 1; k <= m; ++k)
+      for (int i = 1; i <= l; ++i) {
+        for (int jy = 1; jy <= ng; ++jy) {
+          bb[jy] = o->acph[jy] + xrt[i] + yrt[k];
+          tt[jy] = FR(i, k, jy);
+        }
+        const int nr = ng, mm1 = nr - 1;
+        double z = 1.0 / bb[1];
+        dd[1] = o->apph[1] * z;
+        tt[1] = tt[1] * z;
+        for (int jy = 2; jy <= mm1; ++jy) {
+          z = 1.0 / (bb[jy] - o->amph[jy] * dd[jy - 1]);
+          dd[jy] = o->apph[jy] * z;
+          tt[jy] = (tt[jy] - o->amph[jy] * tt[jy - 1]) * z;
+        }
+        z = bb[nr] - o->amph[nr] * dd[mm1];
+        const bool singular = (i == 1 && k == 1);  // the mean mode: zero branch
+        if (!singular && std::fabs(z) > 1.0e-14)
+          tt[nr] = (tt[nr] - o->amph[nr] * tt[mm1]) / z;
+        else
+          tt[nr] = 0.0;
+        for (int jy = mm1; jy >= 1; --jy) tt[jy] = tt[jy] - dd[jy] * tt[jy + 1];
+        for (int jy = 1; jy <= ng; ++jy) FR(i, k, jy) = tt[jy];
+      }
+  }
+#pragma omp parallel num_threads(nthreads())
+  {
+    std::vector<double> w(6 * nmax), t(nmax);
+#pragma omp for schedule(static)
+    for (int j = 1; j <= ng; ++j) {
+      for (int i = 1; i <= l; ++i) {
+        for (int k = 1; k <= m; ++k) t[k - 1] = FR(i, k, j);
+        rfftb(o->dftz, m, t.data(), w.data());
+        for (int k = 1; k <= m; ++k) FR(i, k, j) = t[k - 1];
+      }
+      for (int k = 1; k <= m; ++k) {
+        for (int i = 1; i <= l; ++i) t[i - 1] = FR(i, k, j);
+        rfftb(o->dftx, l, t.data(), w.data());
+        for (int i = 1; i <= l; ++i) FR(i, k, j) = t[i - 1];
+      }
+    }
+  }
+  const double scal = (double)l * (double)m;  // SCALX * SCALY
+  std::fill(o->dph.begin(), o->dph.end(), 0.0);
+  for (int j = 1; j <= ng; ++j)
+    for (int k = 1; k <= m; ++k)
+      for (int i = 1; i <= l; ++i) F(dph, i, j, k) = FR(i, k, j) / scal;
+  bc_wall_copy(o, o->dph);
+}
+
+void mom_io(oracle_io *o, int ns) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  for (int c = 1; c <= 3; ++c) o->g0[c] = o->g[c];  // :15
+  convection(o);
+  divg_u(o);
+  viscous(o);
+  rhs_mom(o, ns, 1, o->qtmp);
+  rhs_mom(o, ns, 2, o->dphtmp);
+  rhs_mom(o, ns, 3, o->rhsz);
+  // MASSFLUX_CALC_IO (src/MASSFLUX_CALC_IO.f90:1-79)
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        FC(g, 1, i, j, k) += F(qtmp, i, j, k);
+        FC(g, 3, i, j, k) += F(rhsz, i, j, k);
+        if (j >= 2) FC(g, 2, i, j, k) += F(dphtmp, i, j, k);
+      }
+  bc_wall_vec(o, o->g);
+  // DIVG_io (src/DIVG.f90:60-150)
+  const double coe0 = 1.0 / o->dt / o->talp[ns];
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        const double divx = (FC(g, 1, o->ip(i), j, k) - FC(g, 1, i, j, k)) * o->dxi;
+        const double divy = (FC(g, 2, i, j + 1, k) - FC(g, 2, i, j, k)) * o->dyfi[j];
+        const double divz = (FC(g, 3, i, j, o->kp(k)) - FC(g, 3, i, j, k)) * o->dzi;
+        F(rhsllphi, i, j, k) = (divx + divy + divz + F(drho, i, j, k)) * coe0;
+      }
+  fishpack_pois3d(o);
+  // PRCALC_io (src/PRESSURE_CORRECTION.f90:86-122), explicit branch
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) F(pr, i, j, k) += F(dph, i, j, k);
+  bc_wall_copy(o, o->pr);
+  // MASSFLUX_UPDATE_IO (src/VELO_CORRECTION.f90:107-185)
+  const double cx = o->dt * o->talp[ns] * o->dxi, cz = o->dt * o->talp[ns] * o->dzi;
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        FC(g, 1, i, j, k) -= (F(dph, i, j, k) - F(dph, o->im(i), j, k)) * cx;
+        FC(g, 3, i, j, k) -= (F(dph, i, j, k) - F(dph, i, j, o->km(k))) * cz;
+        if (j >= 2) FC(g, 2, i, j, k) -= (F(dph, i, j, k) - F(dph, i, j - 1, k)) * (o->dt * o->talp[ns] * o->dyci[j]);
+      }
+  bc_wall_vec(o, o->g);
+}
+
+void eng_io(oracle_io *o, int ns) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  o->mu0 = o->mu;  // :13-16 (DENSITY1 is never read)
+  o->dd0 = o->dd;
+  rhs_energy(o);
+  const double coe1 = o->tgam[ns] * o->dt, coe0 = o->troh[ns] * o->dt;
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        const int64_t c = o->id(i, j, k);
+        double r = o->rhoh[c] + coe1 * o->rhse[c] + coe0 * o->rhse0[c];
+        r = std::fmin(o->rhohmax + 1.0e-14, r);  // limiter, thermoStat = table
+        o->rhoh[c] = r;
+        o->rhse0[c] = o->rhse[c];
+      }
+  int64_t bad = 0;
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads()) reduction(+ : bad)
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        const int64_t c = o->id(i, j, k);
+        // ENTHALPY_UPDATE, DENSITY_UPDATE, ENTHALPY_UPDATE
+        double h = o->rhoh[c] / o->dd[c];
+        double T, D;
+        if (lookup_ht(o, h, T) && lookup_t(o, o->td, T, D))
+          o->dd[c] = D;
+        else
+          ++bad;
+        h = o->rhoh[c] / o->dd[c];
+        o->hh[c] = h;
+        // THERM_PROP_UPDATE (src/THERM_PROP_UPDATE.f90:129-205)
+        if (o->shortcuts && std::fabs(h) < 1.0e-10) continue;  // properties kept
+        double M, K;
+        if (!lookup_ht(o, h, T) || !lookup_t(o, o->tm, T, M) || !lookup_t(o, o->tk, T, K) ||
+            !lookup_t(o, o->td, T, D)) {
+          ++bad;
+          continue;
+        }
+        o->tt[c] = T;
+        o->mu[c] = M;
+        o->kk[c] = K;
+        o->dd[c] = D;
+      }
+  o->bad += bad;
+  bc_wall_thermal(o);
+}
+
+std::vector<double> *field_ptr(oracle_io *o, int id) {
+  switch (id) {
+    case ORC_U: return &o->q[1];
+    case ORC_V: return &o->q[2];
+    case ORC_W: return &o->q[3];
+    case ORC_P: return &o->pr;
+    case ORC_PHI: return &o->dph;
+    case ORC_RHSPHI: return &o->rhsllphi;
+    case ORC_IO_GX: return &o->g[1];
+    case ORC_IO_GY: return &o->g[2];
+    case ORC_IO_GZ: return &o->g[3];
+    case ORC_IO_G0X: return &o->g0[1];
+    case ORC_IO_G0Y: return &o->g0[2];
+    case ORC_IO_G0Z: return &o->g0[3];
+    case ORC_IO_H: return &o->hh;
+    case ORC_IO_T: return &o->tt;
+    case ORC_IO_D: return &o->dd;
+    case ORC_IO_MU: return &o->mu;
+    case ORC_IO_K: return &o->kk;
+    case ORC_IO_RHOH: return &o->rhoh;
+    case ORC_IO_D0: return &o->dd0;
+    case ORC_IO_MU0: return &o->mu0;
+    case ORC_IO_DRHO: return &o->drho;
+    case ORC_IO_EX0X: return &o->explt0[1];
+    case ORC_IO_EX0Y: return &o->explt0[2];
+    case ORC_IO_EX0Z: return &o->explt0[3];
+    case ORC_IO_RHSE0: return &o->rhse0;
+  }
+  return nullptr;
+}
+
+double bulk(const oracle_io *o, const std::vector<double> &f) {
+  double s = 0.0;
+  for (int j = 1; j <= o->ny; ++j)
+    for (int i = 1; i <= o->nx; ++i)
+      for (int k = 1; k <= o->nz; ++k) s += f[o->id(i, j, k)] / o->dyfi[j];
+  s /= o->dzi;
+  return s / (o->area_inlet * (double)o->nx);
+}
+
+// VELO2MASSFLUX (src/INITIAL_FL_THEML_FLD_io.f90:481-560).
+void velo2massflux(oracle_io *o) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        FC(g, 1, i, j, k) = FC(q, 1, i, j, k) * FC(rhostg, 1, i, j, k);
+        FC(g, 3, i, j, k) = FC(q, 3, i, j, k) * FC(rhostg, 3, i, j, k);
+        if (j >= 2) FC(g, 2, i, j, k) = FC(q, 2, i, j, k) * FC(rhostg, 2, i, j, k);
+      }
+  bc_wall_vec(o, o->g);
+}
+
+}  // namespace
+
+extern "C" {
+
+oracle_io *oracle_io_create(int nx, int ny, int nz, double lx, double lz, double str2, int istr2, double ren,
+                            double dt, int flowdrvtp, double cfgv, int thermal, double prt, double qw_bot,
+                            double qw_top, int gravdir, double f_a) {
+  if (nx < 4 || ny < 4 || nz < 4 || (nx % 2) || (nz % 2) || gravdir < 0 || gravdir > 3) return nullptr;
+  // the y mesh and Poisson y-coefficients are shared with the TG oracle
+  oracle_tg *t = oracle_tg_create(nx, ny, nz, lx, lz, str2, istr2, ren, dt, flowdrvtp, cfgv);
+  if (!t) return nullptr;
+  oracle_io *o = new oracle_io();
+  o->nx = nx; o->ny = ny; o->nz = nz; o->lx = lx; o->lz = lz; o->str2 = str2; o->istr2 = istr2;
+  o->ren = ren; o->dt = dt; o->flowdrvtp = flowdrvtp; o->cfgv = cfgv; o->thermal = thermal ? 1 : 0;
+  o->prt = prt; o->qw[0] = qw_bot; o->qw[1] = qw_top; o->gravdir = gravdir; o->f_a = f_a;
+  std::vector<double> tmp(ny + 2);
+  auto coef = [&](int what, std::vector<double> &dst) {
+    dst.assign(ny + 2, 0.0);
+    int n = oracle_tg_get_coef(t, what, tmp.data());
+    for (int j = 1; j <= n; ++j) dst[j] = tmp[j - 1];
+  };
+  coef(0, o->ynd); coef(1, o->ycc); coef(2, o->dyfi); coef(3, o->dyci); coef(4, o->wff); coef(5, o->wfb);
+  coef(6, o->amph); coef(7, o->acph); coef(8, o->apph);
+  o->volm = oracle_tg_volm(t);
+  oracle_tg_destroy(t);
+  o->dxi = nx / lx; o->dzi = nz / lz; o->dxqi = o->dxi * o->dxi; o->dzqi = o->dzi * o->dzi;
+  o->cvisc = 1.0 / ren;
+  o->cthecd = 1.0 / ren / prt;  // Flow_State.f90:87
+  o->area_inlet = 0.0;
+  for (int j = 1; j <= ny; ++j)
+    for (int k = 1; k <= nz; ++k) o->area_inlet += 1.0 / o->dyfi[j] / o->dzi;
+  o->tgam[0] = 1.0; o->tgam[1] = 8.0 / 15.0; o->tgam[2] = 5.0 / 12.0; o->tgam[3] = 3.0 / 4.0;
+  o->troh[0] = 0.0; o->troh[1] = 0.0; o->troh[2] = -17.0 / 60.0; o->troh[3] = -5.0 / 12.0;
+  for (int n = 0; n < 4; ++n) o->talp[n] = o->tgam[n] + o->troh[n];
+  const int64_t n = o->len();
+  for (int c = 1; c <= 3; ++c) {
+    o->q[c].assign(n, 0.0); o->g[c].assign(n, 0.0); o->g0[c].assign(n, 0.0); o->explt0[c].assign(n, 0.0);
+    o->mustg[c].assign(n, 1.0); o->rhostg[c].assign(n, 1.0);
+  }
+  for (auto *v : {&o->pr, &o->dph, &o->rhsllphi, &o->qtmp, &o->dphtmp, &o->rhsz, &o->divu, &o->drho, &o->rhoh,
+                  &o->hh, &o->rhse, &o->rhse0})
+    v->assign(n, 0.0);
+  for (auto *v : {&o->tt, &o->dd, &o->dd0, &o->mu, &o->mu0, &o->kk}) v->assign(n, 1.0);
+  o->dftx = oracle_dft_create(nx);
+  o->dftz = oracle_dft_create(nz);
+  return o;
+}
+
+void oracle_io_destroy(oracle_io *o) {
+  if (!o) return;
+  oracle_dft_destroy(o->dftx);
+  oracle_dft_destroy(o->dftz);
+  delete o;
+}
+
+int oracle_io_set_table(oracle_io *o, const double *H, const double *T, const double *D, const double *M,
+                        const double *K, int n, int shortcuts) {
+  if (n < 4) return -1;
+  o->ht.build(H, T, n);
+  o->td.build(T, D, n);
+  o->tm.build(T, M, n);
+  o->tk.build(T, K, n);
+  o->hd.build(H, D, n);
+  o->shortcuts = shortcuts ? 1 : 0;
+  o->has_table = true;
+  // RHOHmax (src/Flow_State.f90:963-990): max of D(h) h over 3n - 1 samples
+  double rm = -1e-14;
+  for (int i = 2; i <= 3 * n; ++i) {
+    const double h = H[0] + (double)(i - 1) * (H[n - 1] - H[0]) / (double)(3 * n);
+    double d = 0.0;
+    o->hd.eval(h, d);
+    if (o->shortcuts && std::fabs(h) < 1.0e-10) d = 1.0;  // Flow_State.f90:1112
+    if (d * h > rm) rm = d * h;
+  }
+  o->rhohmax = rm;
+  return 0;
+}
+
+double oracle_io_rhohmax(const oracle_io *o) { return o->rhohmax; }
+
+void oracle_io_init_random(oracle_io *o, uint64_t seed, double amp) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  o->bad = 0;
+  // thermal field (INIFIELD_THERMAL_io, src/INITIAL_FL_THEML_FLD_io.f90:352-381)
+  std::fill(o->rhoh.begin(), o->rhoh.end(), 0.0);
+  std::fill(o->hh.begin(), o->hh.end(), 0.0);
+  std::fill(o->rhse0.begin(), o->rhse0.end(), 0.0);
+  double T0 = 1.0, D0 = 1.0, M0 = 1.0, K0 = 1.0;
+  if (o->thermal && o->has_table && !o->shortcuts) {
+    lookup_ht(o, 0.0, T0);
+    lookup_t(o, o->td, T0, D0);
+    lookup_t(o, o->tm, T0, M0);
+    lookup_t(o, o->tk, T0, K0);
+  }
+  std::fill(o->tt.begin(), o->tt.end(), T0);
+  std::fill(o->dd.begin(), o->dd.end(), D0);
+  std::fill(o->dd0.begin(), o->dd0.end(), D0);
+  std::fill(o->mu.begin(), o->mu.end(), M0);
+  std::fill(o->mu0.begin(), o->mu0.end(), M0);
+  std::fill(o->kk.begin(), o->kk.end(), K0);
+  // velocity: the TG recipe
+  for (int c = 1; c <= 3; ++c) {
+    std::fill(o->q[c].begin(), o->q[c].end(), 0.0);
+    std::fill(o->g[c].begin(), o->g[c].end(), 0.0);
+    std::fill(o->g0[c].begin(), o->g0[c].end(), 0.0);
+    std::fill(o->explt0[c].begin(), o->explt0[c].end(), 0.0);
+  }
+  for (int j = 1; j <= ny; ++j)
+    for (int k = 1; k <= nz; ++k)
+      for (int i = 1; i <= nx; ++i)
+        for (int c = 1; c <= 3; ++c) FC(q, c, i, j, k) = amp * rnd_pm1(seed, c, i, j, k);
+  for (int k = 1; k <= nz; ++k)
+    for (int i = 1; i <= nx; ++i) FC(q, 2, i, 1, k) = 0.0;
+  for (int c = 1; c <= 3; ++c)
+    for (int j = 1; j <= ny; ++j) {
+      double s = 0.0;
+      for (int i = 1; i <= nx; ++i)
+        for (int k = 1; k <= nz; ++k) s += FC(q, c, i, j, k);
+      s /= (double)(nx * nz);
+      for (int i = 1; i <= nx; ++i)
+        for (int k = 1; k <= nz; ++k) FC(q, c, i, j, k) -= s;
+    }
+  for (int j = 1; j <= ny; ++j) {
+    const double vini = 1.5 * (1.0 - o->ycc[j] * o->ycc[j]);
+    for (int k = 1; k <= nz; ++k)
+      for (int i = 1; i <= nx; ++i) FC(q, 1, i, j, k) += vini;
+  }
+  for (int k = 1; k <= nz; ++k)
+    for (int i = 1; i <= nx; ++i) FC(q, 2, i, 1, k) = 0.0;
+  bc_wall_vec(o, o->q);
+  const double ub = bulk(o, o->q[1]);
+  for (auto &x : o->q[1]) x /= ub;
+  // mass flux from the velocity, then unit bulk mass flux (Unified_massflux,
+  // src/INITIAL_FL_THEML_FLD_io.f90:653-682)
+  density_staggered(o);
+  velo2massflux(o);
+  const double gm = bulk(o, o->g[1]);
+  for (int c = 1; c <= 3; ++c)
+    for (auto &x : o->q[c]) x /= gm;
+  velo2massflux(o);
+  bc_wall_vec(o, o->q);
+  std::fill(o->pr.begin(), o->pr.end(), 0.0);
+  std::fill(o->dph.begin(), o->dph.end(), 0.0);
+  std::fill(o->drho.begin(), o->drho.end(), 0.0);
+  mu_staggered(o);
+  // CALC_INITIALIZATION_io (src/INITIAL_FL_THEML_FLD_io.f90:133-172)
+  if (o->thermal) {
+    bc_wall_thermal(o);
+    eng_io(o, 0);
+    density_staggered(o);
+    mu_staggered(o);
+  }
+  mom_io(o, 0);
+}
+
+int oracle_io_eng(oracle_io *o, int ns) {
+  if (ns < 0 || ns > 3 || !o->thermal || !o->has_table) return -1;
+  eng_io(o, ns);
+  return 0;
+}
+
+int oracle_io_mom(oracle_io *o, int ns) {
+  if (ns < 0 || ns > 3) return -1;
+  if (ns >= 1) {
+    if (o->thermal) {
+      density_time_derivation(o, ns);
+      density_staggered(o);
+      mu_staggered(o);
+    }
+    velocity_calc(o);
+  }
+  mom_io(o, ns);
+  return 0;
+}
+
+int oracle_io_substep(oracle_io *o, int ns) {
+  if (ns < 1 || ns > 3) return -1;
+  if (o->thermal) eng_io(o, ns);
+  return oracle_io_mom(o, ns);
+}
+
+int oracle_io_step(oracle_io *o) {
+  for (int ns = 1; ns <= 3; ++ns)
+    if (oracle_io_substep(o, ns)) return -1;
+  return 0;
+}
+
+int oracle_io_get_field(const oracle_io *o, int id, double *out) {
+  auto *f = field_ptr(const_cast<oracle_io *>(o), id);
+  if (!f) return -1;
+  std::memcpy(out, f->data(), sizeof(double) * f->size());
+  return 0;
+}
+int oracle_io_set_field(oracle_io *o, int id, const double *in) {
+  auto *f = field_ptr(o, id);
+  if (!f) return -1;
+  std::memcpy(f->data(), in, sizeof(double) * f->size());
+  return 0;
+}
+
+double oracle_io_divmax(const oracle_io *o) {
+  double m = 0.0;
+  for (int k = 1; k <= o->nz; ++k)
+    for (int j = 1; j <= o->ny; ++j)
+      for (int i = 1; i <= o->nx; ++i) {
+        const double divx = (FC(g, 1, o->ip(i), j, k) - FC(g, 1, i, j, k)) * o->dxi;
+        const double divy = (FC(g, 2, i, j + 1, k) - FC(g, 2, i, j, k)) * o->dyfi[j];
+        const double divz = (FC(g, 3, i, j, o->kp(k)) - FC(g, 3, i, j, k)) * o->dzi;
+        m = std::fmax(m, std::fabs(divx + divy + divz + F(drho, i, j, k)));
+      }
+  return m;
+}
+
+double oracle_io_divmax_q(const oracle_io *o) {
+  double m = 0.0;
+  for (int k = 1; k <= o->nz; ++k)
+    for (int j = 1; j <= o->ny; ++j)
+      for (int i = 1; i <= o->nx; ++i) {
+        const double divx = (FC(q, 1, o->ip(i), j, k) - FC(q, 1, i, j, k)) * o->dxi;
+        const double divy = (FC(q, 2, i, j + 1, k) - FC(q, 2, i, j, k)) * o->dyfi[j];
+        const double divz = (FC(q, 3, i, j, o->kp(k)) - FC(q, 3, i, j, k)) * o->dzi;
+        m = std::fmax(m, std::fabs(divx + divy + divz));
+      }
+  return m;
+}
+
+double oracle_io_bulk(const oracle_io *o, int what) {
+  if (what == 0) return bulk(o, o->q[1]);
+  if (what == 1) return bulk(o, o->g[1]);
+  return bulk(o, o->hh);
+}
+
+int64_t oracle_io_bad_cells(const oracle_io *o) { return o->bad; }
+
+}  // extern "C"

@@ -46,6 +46,24 @@ def load(build=True):
     for f in ("oracle_tg_divmax", "oracle_tg_bulk", "oracle_tg_pois_residual"):
         getattr(L, f).restype = D
         getattr(L, f).argtypes = [P]
+    L.oracle_io_create.restype = P
+    L.oracle_io_create.argtypes = [I, I, I, D, D, D, I, D, D, I, D, I, D, D, D, I, D]
+    L.oracle_io_destroy.argtypes = [P]
+    L.oracle_io_set_table.argtypes = [P, P, P, P, P, P, I, I]
+    L.oracle_io_init_random.argtypes = [P, ctypes.c_uint64, D]
+    for f in ("oracle_io_eng", "oracle_io_mom", "oracle_io_substep"):
+        getattr(L, f).argtypes = [P, I]
+    L.oracle_io_step.argtypes = [P]
+    L.oracle_io_get_field.argtypes = [P, I, P]
+    L.oracle_io_set_field.argtypes = [P, I, P]
+    for f in ("oracle_io_divmax", "oracle_io_divmax_q", "oracle_io_rhohmax"):
+        getattr(L, f).restype = D
+        getattr(L, f).argtypes = [P]
+    L.oracle_io_bulk.restype = D
+    L.oracle_io_bulk.argtypes = [P, I]
+    L.oracle_io_bad_cells.restype = ctypes.c_int64
+    L.oracle_io_bad_cells.argtypes = [P]
+    L.oracle_synth_table.argtypes = [I, P, P, P, P, P, P, P]
     L.oracle_set_threads.argtypes = [I]
     L.oracle_get_threads.restype = I
     _lib = L
@@ -124,3 +142,88 @@ def set_threads(n):
 
 def get_threads():
     return load().oracle_get_threads()
+
+
+IO_FIELDS = {"u": 0, "v": 1, "w": 2, "p": 3, "phi": 4, "rhsphi": 5, "gx": 20, "gy": 21, "gz": 22, "g0x": 23,
+             "g0y": 24, "g0z": 25, "h": 26, "t": 27, "rho": 28, "mu": 29, "k": 30, "rhoh": 31, "rho0": 32,
+             "mu0": 33, "drho": 34, "ex0x": 35, "ex0y": 36, "ex0z": 37, "rhse0": 38}
+
+
+def synth_table(n=4096):
+    """The synthetic property table (columns H, T, D, M, K, CP, B) of the
+    heated IO configuration, from the oracle's restatement."""
+    L = load()
+    cols = [np.empty(n) for _ in range(7)]
+    L.oracle_synth_table(n, *[c.ctypes.data for c in cols])
+    return cols
+
+
+class OracleIO:
+    """x-periodic IO channel: SOLVERRK3_ENG_IO + SOLVERRK3_MOM_IO (explicit
+    viscous terms, FISHPACK Poisson), optionally with the energy equation."""
+
+    def __init__(self, nx, ny, nz, lx=8 * math.pi, lz=4 * math.pi / 3, str2=2.0, istr2=1, ren=2800.0, dt=1e-3,
+                 flowdrvtp=1, cfgv=0.0, thermal=1, prt=0.71, qw=(1.0, 1.0), gravdir=0, f_a=0.0, table=None,
+                 shortcuts=0):
+        self.L = load()
+        self.h = self.L.oracle_io_create(nx, ny, nz, lx, lz, str2, istr2, ren, dt, flowdrvtp, cfgv, thermal, prt,
+                                         qw[0], qw[1], gravdir, f_a)
+        if not self.h:
+            raise ValueError("oracle_io_create rejected the configuration")
+        self.nx, self.ny, self.nz = nx, ny, nz
+        if thermal:
+            if table is None:
+                table = synth_table()
+            self._table = [np.ascontiguousarray(c, dtype=np.float64) for c in table[:5]]
+            assert self.L.oracle_io_set_table(self.h, *[c.ctypes.data for c in self._table], len(self._table[0]),
+                                              shortcuts) == 0
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.oracle_io_destroy(self.h)
+            self.h = None
+
+    @property
+    def shape(self):
+        return (self.nz, self.ny + 2, self.nx)
+
+    def get(self, name):
+        a = np.empty(self.shape)
+        assert self.L.oracle_io_get_field(self.h, IO_FIELDS[name], a.ctypes.data) == 0
+        return a
+
+    def set(self, name, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        assert a.size == self.nx * (self.ny + 2) * self.nz
+        assert self.L.oracle_io_set_field(self.h, IO_FIELDS[name], a.ctypes.data) == 0
+
+    def init_random(self, seed, amp=0.1):
+        self.L.oracle_io_init_random(self.h, seed, amp)
+
+    def eng(self, ns):
+        assert self.L.oracle_io_eng(self.h, ns) == 0
+
+    def mom(self, ns):
+        assert self.L.oracle_io_mom(self.h, ns) == 0
+
+    def substep(self, ns):
+        assert self.L.oracle_io_substep(self.h, ns) == 0
+
+    def step(self, n=1):
+        for _ in range(n):
+            assert self.L.oracle_io_step(self.h) == 0
+
+    def divmax(self):
+        return self.L.oracle_io_divmax(self.h)
+
+    def divmax_q(self):
+        return self.L.oracle_io_divmax_q(self.h)
+
+    def bulk(self, what=0):
+        return self.L.oracle_io_bulk(self.h, what)
+
+    def rhohmax(self):
+        return self.L.oracle_io_rhohmax(self.h)
+
+    def bad_cells(self):
+        return self.L.oracle_io_bad_cells(self.h)
