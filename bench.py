@@ -40,6 +40,13 @@ WORKLOADS = {
     "batch64": dict(batch=True, seed=3),
     # the CPU-runnable plain-method configuration
     "tg_64x64x64": dict(nx=64, ny=64, nz=64, lx=4 * math.pi, lz=4 * math.pi / 3, ren=2800.0, dt=1e-3, seed=0),
+    # variable-property heated IO channel, x-periodic, synthetic 4096-point table
+    "io_384x192x192": dict(io=True, nx=384, ny=192, nz=192, lx=8 * math.pi, lz=4 * math.pi / 3, ren=2800.0,
+                           dt=1e-3, seed=2, thermal=1, prt=0.71, qw=1.0, table="synthetic"),
+    # IO section of the coupled configuration run x-periodic: constant-property
+    # passive heat (rho = mu = k = cp = 1, T = h), wall heat flux 1, Pr 0.71
+    "io_512x192x256": dict(io=True, nx=512, ny=192, nz=256, lx=8 * math.pi, lz=4 * math.pi / 3, ren=2800.0,
+                           dt=1e-3, seed=1, thermal=1, prt=0.71, qw=1.0, table="constant"),
 }
 METRIC = "cell-steps/s"
 
@@ -50,6 +57,40 @@ PHASE_SPECTRAL_PASSES = {"fftx": 1, "fftz": 2, "ysolve": 2, "ifftz": 2, "ifftx":
 PHASE_KERNEL = {"rhs": "k_rhs_tma", "adix": "k_adixz_band", "adiz": "k_adixz_band", "adiy": "k_adiy_band",
                 "fftx": "k_fftx", "fftz": "k_fftz", "ysolve": "k_ysolve_line", "ifftz": "k_fftz", "ifftx": "k_ifftx",
                 "corr": "k_corr"}
+
+
+# IO substep phases (the library's IO timer slots, in execution order) and
+# their algorithmic 8-byte values per cell (thermal form): energy RHS reads
+# h, T, k, G, G0, rho h, R0 and writes rho h, R0; the property update reads
+# rho h, rho, mu and writes mu0, rho0, rho, h, T, mu, k; prep reads G, G0,
+# rho, rho0 and writes u, v, w, DrhoDtP; the momentum RHS reads u, v, w, G,
+# mu, mu0, p, EXPLT0 and writes EXPLT0 and G*; the x-transform reads G* and
+# DrhoDtP and writes RHSLLPHI; the correction reads G*, phi, p and writes G, p.
+IO_PHASES = ["eng_rhs", "eng_props", "prep", "mom_rhs", "fftx", "fftz", "ysolve", "ifftz", "ifftx", "corr"]
+IO_VALUES_PER_CELL = {"eng_rhs": 13, "eng_props": 10, "prep": 12, "mom_rhs": 17, "fftx": 5, "corr": 9}
+IO_KERNEL = {"eng_rhs": "k_io_eng_rhs", "eng_props": "k_io_eng_props", "prep": "k_io_prep",
+             "mom_rhs": "k_io_rhs", "fftx": "k_fftx", "fftz": "k_fftz", "ysolve": "k_ysolve_line",
+             "ifftz": "k_fftz", "ifftx": "k_ifftx", "corr": "k_io_corr"}
+
+
+def io_phase_bytes(ph, nx, ny, nz, real_bytes=8):
+    cells = nx * ny * nz
+    spec = (nx // 2 + 1) * ny * nz
+    b = IO_VALUES_PER_CELL.get(ph, 0) * real_bytes * cells
+    if ph == "ifftx":
+        b += real_bytes * cells
+    b += PHASE_SPECTRAL_PASSES.get(ph, 0) * 2 * real_bytes * spec
+    return b
+
+
+def io_table(kind):
+    import numpy as np
+    if kind == "constant":
+        H = np.linspace(-1.0, 1.0, 4096)
+        one = np.ones_like(H)
+        return H, H.copy(), one, one.copy(), one.copy()
+    from chapsim1ww_b200 import synthetic_table
+    return synthetic_table(4096)[:5]
 
 
 def phase_bytes(ph, nx, ny, nz, real_bytes=8):
@@ -180,6 +221,152 @@ def bench_learned(cells, device):
             "cells": cells}
 
 
+def cpu_baseline_io(wl, steps):
+    """FP64 IO oracle port on the host cores: init + projection, then `steps` timed steps."""
+    from oracle.pyoracle import OracleIO, get_threads
+    o = OracleIO(wl["nx"], wl["ny"], wl["nz"], lx=wl["lx"], lz=wl["lz"], ren=wl["ren"], dt=wl["dt"],
+                 thermal=wl["thermal"], prt=wl["prt"], qw=(wl["qw"], wl["qw"]), table=io_table(wl["table"]))
+    o.init_random(wl["seed"], 0.1)
+    t0 = time.perf_counter()
+    o.step(steps)
+    t = time.perf_counter() - t0
+    cells = wl["nx"] * wl["ny"] * wl["nz"]
+    return cells * steps / t, t, get_threads()
+
+
+def run_io(args, wl, ws, rank, local):
+    """IO channel section: one step = NS 1, 2, 3 of SOLVERRK3_ENG_IO + SOLVERRK3_MOM_IO."""
+    import torch
+
+    from chapsim1ww_b200 import IOChannel
+
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    s = IOChannel(wl["nx"], wl["ny"], wl["nz"], lx=wl["lx"], lz=wl["lz"], ren=wl["ren"], dt=wl["dt"],
+                  thermal=wl["thermal"], prt=wl["prt"], qw=(wl["qw"], wl["qw"]), table=io_table(wl["table"]),
+                  device=local)
+    s.random_fl_theml_fld_io(wl["seed"] + rank, 0.1)
+    cells = wl["nx"] * wl["ny"] * wl["nz"]
+    stream = torch.cuda.ExternalStream(s.stream(), device=local)
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    def max_over_ranks(x):
+        if pg is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    s.step(args.warmup)
+    s.sync()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n0 = s.launch_count()
+    e0.record(stream)
+    s.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    launches = s.launch_count() - n0
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = cells * ws * args.steps / (ms / 1000.0)
+    divmax = s.divgck_io()
+    bad = s.bad_cells()
+
+    s.phase_timing(True)
+    s.phase_reset()
+    s.step(max(1, min(args.steps, 10)))
+    ph, nsub = s.phase_times()
+    s.phase_timing(False)
+    per_launch = {IO_PHASES[i]: v / max(nsub, 1) for i, v in enumerate(ph.values())}
+    dom = max(per_launch, key=per_launch.get)
+    peak, peak_kind = measured_peak()
+    nx, ny, nz = wl["nx"], wl["ny"], wl["nz"]
+    bytes_dom = io_phase_bytes(dom, nx, ny, nz)
+    achieved = bytes_dom / (per_launch[dom] / 1000.0) / 1e9
+    total_bytes = sum(io_phase_bytes(p, nx, ny, nz) for p in IO_PHASES)
+    traffic = load_traffic(args.workload, IO_KERNEL[dom])
+
+    names = ("u", "v", "w", "p", "gx", "gy", "gz", "rhoh")
+    host = {}
+    for n in names:
+        t = torch.empty(s.shape, dtype=torch.float64, pin_memory=True)
+        host[n] = t.numpy()
+        s.get_field(n, out=host[n])
+    barrier()
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(1, min(args.steps, 10))
+    e2.record(stream)
+    for _ in range(e2e_steps):
+        for n in names:
+            s.set_field(n, host[n])
+        s.step(1)
+        for n in names:
+            s.get_field(n, out=host[n])
+        _ = s.divgck_io()
+    e3.record(stream)
+    e3.synchronize()
+    barrier()
+    ms_e2e = max_over_ranks(e2.elapsed_time(e3))
+    e2e_value = cells * ws * e2e_steps / (ms_e2e / 1000.0)
+    nbytes = len(names) * s.n * 8
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            v, t, cores = cpu_baseline_io(wl, args.cpu_steps)
+            cpu = {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
+                   "sample": f"{args.cpu_steps} full RK3 steps of the {args.workload} channel after init, "
+                             f"FP64 oracle port, OpenMP {cores} threads, {t:.1f} s"}
+        except Exception as ex:
+            cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded splitmix64 velocity, h = 0, table properties, NS=0 projection)",
+            "config": {"workload": args.workload, **{k: wl[k] for k in ("nx", "ny", "nz", "ren", "dt", "prt")},
+                       "wall_heat_flux": wl["qw"], "table": wl["table"], "precision": "fp64",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                       "l2": "working set (>2 GB) larger than the 126 MB L2"},
+            "max_div_g_plus_drho": divmax, "out_of_table_cells": bad,
+            "gpu_launches": launches,
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes + 8, "steps": e2e_steps},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "kernel": IO_KERNEL[dom], "phase": dom,
+                         "algorithmic_bytes_per_launch": bytes_dom, "avg_launch_ms": per_launch[dom],
+                         "peak_source": peak_kind},
+            "phases_ms_per_launch": per_launch,
+            "step_roofline": {"algorithmic_bytes_per_step": 3 * total_bytes,
+                              "achieved_gbs": 3 * total_bytes / (ms / args.steps / 1000.0) / 1e9,
+                              "frac": 3 * total_bytes / (ms / args.steps / 1000.0) / 1e9 / peak,
+                              "phase_sum_ms": 3 * sum(per_launch.values())},
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    s.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
 def cpu_baseline_oracle(wl, steps):
     """FP64 oracle port on the host cores: init + NS=0, then `steps` timed steps."""
     from oracle.pyoracle import OracleTG, get_threads
@@ -196,10 +383,15 @@ def cpu_baseline_oracle(wl, steps):
 def run_reference(args, wl, ws, rank):
     if rank != 0:
         return 0
-    from oracle.pyoracle import OracleTG, get_threads
-    o = OracleTG(wl["nx"], wl["ny"], wl["nz"], lx=wl["lx"], lz=wl["lz"], ren=wl["ren"], dt=wl["dt"])
-    o.init_random(wl["seed"], 0.1)
-    o.substep(0)
+    from oracle.pyoracle import OracleIO, OracleTG, get_threads
+    if wl.get("io"):
+        o = OracleIO(wl["nx"], wl["ny"], wl["nz"], lx=wl["lx"], lz=wl["lz"], ren=wl["ren"], dt=wl["dt"],
+                     thermal=wl["thermal"], prt=wl["prt"], qw=(wl["qw"], wl["qw"]), table=io_table(wl["table"]))
+        o.init_random(wl["seed"], 0.1)
+    else:
+        o = OracleTG(wl["nx"], wl["ny"], wl["nz"], lx=wl["lx"], lz=wl["lz"], ren=wl["ren"], dt=wl["dt"])
+        o.init_random(wl["seed"], 0.1)
+        o.substep(0)
     for _ in range(args.warmup):
         o.step(1)
     t0 = time.perf_counter()
@@ -414,6 +606,18 @@ def run_ours(args, wl, ws, rank, local):
 def profile_case(spec, precision):
     import chapsim1ww_b200 as cs
     from chapsim1ww_b200 import TGChannel
+    if spec.lower().startswith("io"):
+        from chapsim1ww_b200 import IOChannel
+        nx, ny, nz = (int(x) for x in spec.lower()[2:].split("x"))
+        c = IOChannel(nx, ny, nz, table=io_table("synthetic"))
+        c.random_fl_theml_fld_io(2, 0.1)
+        for _ in range(2):
+            for ns in (1, 2, 3):
+                c.solverrk3_eng_io(ns)
+                c.solverrk3_mom_io(ns)
+        c.sync()
+        print("profile case ok", spec, "max|div G + drho| =", c.divgck_io())
+        return 0
     nx, ny, nz = (int(x) for x in spec.lower().split("x"))
     s = TGChannel(nx, ny, nz, precision=cs.MIXED if precision == "mixed" else cs.FP64)
     s.random_fl_fld_tg(1, 0.1, project=True)
@@ -438,7 +642,7 @@ def main():
     ap.add_argument("--no-props", action="store_true", help="skip the learned-property measurement")
     ap.add_argument("--profile-case", default=None, metavar="NXxNYxNZ",
                     help="run init + NS=0 + 2 eager RK3 steps of a channel of this size and exit "
-                         "(the small case for ncu captures; no timing)")
+                         "(the small case for ncu captures; no timing); prefix io for an IO channel")
     args = ap.parse_args()
     if args.profile_case:
         return profile_case(args.profile_case, args.precision)
@@ -449,6 +653,8 @@ def main():
         return run_reference(args, wl, ws, rank)
     if wl.get("batch"):
         return run_batch(args, wl, ws, rank, local)
+    if wl.get("io"):
+        return run_io(args, wl, ws, rank, local)
     return run_ours(args, wl, ws, rank, local)
 
 

@@ -499,7 +499,8 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
     if (iocfg) {
       IODev &io = ctx->io;
       double **f64io[] = {&io.g[0][0], &io.g[0][1], &io.g[0][2], &io.g[1][0], &io.g[1][1], &io.g[1][2],
-                          &io.drho, &io.rhoh, &io.h, &io.T, &io.D, &io.D0, &io.mu, &io.mu0, &io.kap, &io.rhse0};
+                          &io.drho, &io.rhoh, &io.h, &io.T, &io.D, &io.D0, &io.mu, &io.mu0, &io.kap, &io.rhse0,
+                          &io.msum};
       for (double **f : f64io) {
         if ((rc = dalloc(ctx, &p, n * sizeof(double)))) goto fail;
         *f = (double *)p;
@@ -544,12 +545,14 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
   ctx->fx = px;
   ctx->fz = pz;
   if ((rc = init_kernels(ctx))) goto fail;
+  if (iocfg && (rc = io_init_maps(ctx))) goto fail;
   if (iocfg) {
     // reference property values (thermal off, or before the table is set)
     IODev &io = ctx->io;
     double *ones[] = {io.T, io.D, io.D0, io.mu, io.mu0, io.kap};
     for (double *f : ones)
       if ((rc = fill_value(ctx, f, n, 1.0))) goto fail;
+    if ((rc = fill_value(ctx, io.msum, n, 2.0))) goto fail;
   }
   if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { rc = CHAPSIM_ERR_CUDA; goto fail; }
   *out = ctx;
@@ -687,6 +690,10 @@ static int xfer(chapsim_ctx *ctx, int domain, int field, void *dst_or_src, int64
     CKC(cudaMemcpyAsync(f, dst_or_src, bytes, kind, ctx->stream));
   else
     CKC(cudaMemcpyAsync(dst_or_src, f, bytes, kind, ctx->stream));
+  if (to_dev && domain == CHAPSIM_IIO && (field == CHAPSIM_F_MU || field == CHAPSIM_F_MU0)) {
+    const int rc = io_refresh_msum(ctx);  // keep mu0 + mu in step
+    if (rc) return rc;
+  }
   if (kind != cudaMemcpyDeviceToDevice) CKC(cudaStreamSynchronize(ctx->stream));
   return CHAPSIM_OK;
 }
@@ -853,9 +860,10 @@ static int io_init_random(chapsim_ctx *ctx, uint64_t seed, double amp, int proje
   double *zero[] = {d.p, d.phi, d.rhsphi, io.drho, io.rhoh, io.h, io.rhse0};
   for (double *f : zero) CKC(cudaMemsetAsync(f, 0, bytes, ctx->stream));
   CKC(cudaMemsetAsync(io.bad, 0, sizeof(unsigned long long), ctx->stream));
-  const double *vals[] = {&T0, &D0, &D0, &M0, &M0, &K0};
-  double *arrs[] = {io.T, io.D, io.D0, io.mu, io.mu0, io.kap};
-  for (int a = 0; a < 6; ++a)
+  const double M2 = M0 + M0;
+  const double *vals[] = {&T0, &D0, &D0, &M0, &M0, &K0, &M2};
+  double *arrs[] = {io.T, io.D, io.D0, io.mu, io.mu0, io.kap, io.msum};
+  for (int a = 0; a < 7; ++a)
     if ((rc = fill_value(ctx, arrs[a], (size_t)n, *vals[a]))) return rc;
   if (project) {  // CALC_INITIALIZATION_io
     if (io.thermal) {

@@ -55,6 +55,7 @@ struct IODev {
   double *g[2][3];
   double *drho;                               // DrhoDtP
   double *rhoh, *h, *T, *D, *D0, *mu, *mu0, *kap, *rhse0;  // RHOH, ENTHALPY, ..., RHS_ENERGY0
+  double *msum;                               // mu0 + mu (derived, kept in step)
   chapsim_spl::Spline ht, td, tm, tk;          // h -> T; T -> rho, mu, k
   double cthecd, qw_bot, qw_top, rhohmax, f_a, cfgv;
   int thermal, shortcuts, gravdir, flowdrvtp;
@@ -146,10 +147,18 @@ struct chapsim_ctx {
   std::vector<void *> table_allocs;
   std::vector<double> tab[5];  // host copy of the table columns H, T, D, M, K
   cudaGraphExec_t io_graph[2] = {nullptr, nullptr};  // one step starting from io_cur = 0 / 1
+  // TMA descriptors of the IO momentum RHS: u, v, w, p, mu0 + mu, g[0][0..2], g[1][0..2], EXPLT0
+  CUtensorMap io_maps[14];
+  bool use_tma_io = false;
+  int io_nzc = 16;  // z planes per block of the TMA momentum RHS
 };
 
 // Kernel launch wrappers (defined in tg_kernels.cu).
 namespace chapsim {
+// Phase timer mark: event slot ph of the substep being recorded (timing on).
+inline void phase_mark(chapsim_ctx *c, int ph) {
+  if (c->timing) cudaEventRecord(c->evpool[(size_t)c->ev_pending * (CHAPSIM_PH_COUNT + 1) + ph], c->stream);
+}
 int init_kernels(chapsim_ctx *c);
 int flush_phase_events(chapsim_ctx *c);
 int launch_substep(chapsim_ctx *c, int ns);
@@ -168,5 +177,7 @@ int io_thermal_bc(chapsim_ctx *c);
 int io_mom(chapsim_ctx *c, int ns, bool prep);
 int io_reduce(chapsim_ctx *c, int what, double *host_out);
 int io_correction(chapsim_ctx *c, int ns);
+int io_init_maps(chapsim_ctx *c);
+int io_refresh_msum(chapsim_ctx *c);
 int fill_value(chapsim_ctx *c, double *p, size_t n, double v);
 }  // namespace chapsim

@@ -36,11 +36,15 @@
 //    k_fftx with DrhoDtP added), and the spectral y-solve pins the mean mode
 //    at the last row as FISHPACK's TRID0 does.
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 #include <math.h>
+
+#include <string.h>
 
 #include <string>
 
 #include "chapsim_internal.cuh"
+#include "tma.cuh"
 
 namespace chapsim {
 namespace {
@@ -167,10 +171,13 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_eng_props(TGDev d, IODev io
   const int k = blockIdx.z;
   if (i >= nx || j > ny + 1) return;
   const int64_t c = i + d.sy * j + d.sz * k;
-  const double dold = io.D[c];
-  io.mu0[c] = io.mu[c];
+  const double dold = io.D[c], muold = io.mu[c];
+  io.mu0[c] = muold;
   io.D0[c] = dold;
-  if (j < 1 || j > ny) return;
+  if (j < 1 || j > ny) {
+    io.msum[c] = muold + muold;  // ghost rows: the ghost kernel sets the new value
+    return;
+  }
   const double rh = io.rhoh[c];
   int bad = 0;
   double h = rh / dold, T, D = dold;
@@ -182,6 +189,7 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_eng_props(TGDev d, IODev io
   h = rh / D;
   io.h[c] = h;
   bool keep = io.shortcuts && fabs(h) < 1.0e-10;
+  double munew = muold;
   if (!keep) {
     double M, K, D2;
     if (look_ht(io, h, T) && look_tprops(io, T, D2, M, K)) {
@@ -189,11 +197,13 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_eng_props(TGDev d, IODev io
       io.mu[c] = M;
       io.kap[c] = K;
       D = D2;
+      munew = M;
     } else {
       ++bad;
     }
   }
   io.D[c] = D;
+  io.msum[c] = muold + munew;  // VISCOUSITY0 + VISCOUSITY
   if (bad) atomicAdd(io.bad, (unsigned long long)bad);
 }
 
@@ -224,6 +234,13 @@ __global__ void k_io_eng_ghost(TGDev d, IODev io) {
   io.mu[c] = M;
   io.kap[c] = K;
   io.rhoh[c] = h * D;
+  io.msum[c] = io.mu0[c] + M;
+}
+
+// msum = mu0 + mu over the whole array (after the host replaces mu or mu0).
+__global__ void k_io_msum(IODev io, size_t n) {
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+    io.msum[t] = io.mu0[t] + io.mu[t];
 }
 
 // ---------------------------------------------------------------- momentum
@@ -470,6 +487,318 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_rhs(TGDev d, IODev io, doub
   }
 }
 
+// The same per-cell arithmetic as k_io_rhs, as a 2.5-D stencil: a block owns
+// a 32 x 8 (x, y) tile and marches along z over nzc planes.  Each plane of u,
+// v, w, G (three components), p and, with thermal on, M = mu0 + mu arrives in
+// shared memory as one TMA box of 36 x 10 doubles (x0-2 .. x0+33,
+// j0-1 .. j0+8; the x start is 16-byte aligned) in a ring of four plane
+// slots, so plane k+2 is in flight while plane k is computed.  Periodic x
+// neighbours outside the box are patched in from global memory on the first
+// and last x tiles; z wraps by plane index.  p travels with the plane, and
+// mu, mu0 as their sum M (the only combination MU_STG and the cell viscosity
+// use); EXPLT0 of the tile's own cells comes by 32 x 8 boxes in a two-slot
+// ring one plane ahead.
+constexpr int IT_BXW = 36, IT_BYW = 10, IT_PLANE = IT_BXW * IT_BYW, IT_PST = 368, IT_NF = 8;
+// halo fields of a plane slot; M = mu0 + mu (thermal only, last)
+constexpr int F_U = 0, F_V = 1, F_W = 2, F_GX = 3, F_GY = 4, F_GZ = 5, F_P = 6, F_M = 7;
+constexpr int IT_EBOX = IO_BX * IO_BY;  // EXPLT0 boxes: the tile's own 32 x 8 cells
+constexpr size_t IT_SLOT = (size_t)IT_NF * IT_PST * sizeof(double);
+constexpr size_t IT_ESLOT = (size_t)3 * IT_EBOX * sizeof(double);
+constexpr size_t IT_SMEM = 4 * IT_SLOT + 2 * IT_ESLOT + 6 * sizeof(uint64_t);
+static_assert((IT_PST * 8) % 128 == 0 && IT_PST >= IT_PLANE, "TMA destinations must stay 128-byte aligned");
+static_assert(IT_SLOT % 128 == 0 && IT_ESLOT % 128 == 0 && (IT_EBOX * 8) % 128 == 0, "128-byte aligned slots");
+struct IoMaps {
+  CUtensorMap m[14];  // u, v, w, p, msum, g[0][0..2], g[1][0..2], EXPLT0[0..2]
+};
+
+__global__ void __launch_bounds__(IO_BX *IO_BY, 2)
+k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam, double roh, double alp, int cur,
+             int nzc) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  auto slot = [&](int sl) { return reinterpret_cast<double *>(smem_raw + (size_t)sl * IT_SLOT); };
+  auto eslot = [&](int sl) { return reinterpret_cast<double *>(smem_raw + 4 * IT_SLOT + (size_t)sl * IT_ESLOT); };
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + 4 * IT_SLOT + 2 * IT_ESLOT);
+  uint64_t *ebar = bar + 4;
+  __shared__ double red[IO_BX * IO_BY / 32];
+  __shared__ double ycoef[IO_BY][8];
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + IO_BX * ty;
+  const int x0 = blockIdx.x * IO_BX, j0 = 1 + blockIdx.y * IO_BY;
+  const int kbeg = blockIdx.z * nzc;
+  const int kend = min(kbeg + nzc, nz);
+  const int i = x0 + tx, j = j0 + ty;
+  const bool active = (i < nx) && (j <= ny);
+  const bool left_edge = (x0 == 0), right_edge = (x0 + IO_BX >= nx);
+  const int right_col = nx - x0 + 2;  // smem column of x = nx (wraps to 0)
+  const int nf = io.thermal ? 8 : 7;
+  const uint32_t tx_bytes = (uint32_t)(nf * IT_PLANE * sizeof(double));
+  const CUtensorMap *mp[IT_NF] = {&maps.m[0], &maps.m[1], &maps.m[2], &maps.m[5 + 3 * cur], &maps.m[6 + 3 * cur],
+                                  &maps.m[7 + 3 * cur], &maps.m[3], &maps.m[4]};
+  const double *gsrc[IT_NF] = {d.u, d.v, d.w, io.g[cur][0], io.g[cur][1], io.g[cur][2], d.p, io.msum};
+  if (tid == 0) {
+    for (int q = 0; q < 6; ++q) mbar_init(&bar[q], 1);
+    fence_mbar_init();
+  }
+  if (tid < IO_BY * 8) {
+    const int r = tid >> 3, q = tid & 7, jr = j0 + r;
+    double v = 0.0;
+    if (jr <= ny) {
+      switch (q) {
+        case 0: v = d.wff[jr]; break;
+        case 1: v = d.wfb[jr]; break;
+        case 2: v = d.wff[jr + 1]; break;
+        case 3: v = d.wfb[jr + 1]; break;
+        case 4: v = d.dyfi[jr]; break;
+        case 5: v = d.dyci[jr]; break;
+        case 6: v = d.dyci[jr + 1]; break;
+        case 7: v = d.dyfi[jr - 1]; break;
+      }
+    }
+    ycoef[r][q] = v;
+  }
+  __syncthreads();
+  auto slot_of = [&](int k) { return (k - kbeg + 1) & 3; };
+  auto issue = [&](int k) {
+    const int sl = slot_of(k);
+    const int kz = k < 0 ? k + nz : (k >= nz ? k - nz : k);
+    mbar_expect_tx(&bar[sl], tx_bytes);
+#pragma unroll
+    for (int f = 0; f < IT_NF; ++f)
+      if (f < nf) tma_load_3d(slot(sl) + f * IT_PST, mp[f], x0 - 2, j0 - 1, kz, &bar[sl]);
+  };
+  uint32_t par = 0;
+  auto wait_plane = [&](int k) -> bool {
+    const int sl = slot_of(k);
+    const bool ok = mbar_wait(&bar[sl], (par >> sl) & 1u, d.err);
+    par ^= 1u << sl;
+    const int kz = k < 0 ? k + nz : (k >= nz ? k - nz : k);
+    if (left_edge && tid < 10 * IT_NF) {
+      const int f = tid / 10, r = tid - f * 10, jr = j0 - 1 + r;
+      if (f < nf && jr <= ny + 1) slot(sl)[f * IT_PST + r * IT_BXW + 1] = gsrc[f][(nx - 1) + d.sy * jr + d.sz * kz];
+    }
+    if (right_edge && tid >= 128 && tid < 128 + 10 * IT_NF) {
+      const int q = tid - 128, f = q / 10, r = q - f * 10, jr = j0 - 1 + r;
+      if (f < nf && jr <= ny + 1) slot(sl)[f * IT_PST + r * IT_BXW + right_col] = gsrc[f][d.sy * jr + d.sz * kz];
+    }
+    return ok;
+  };
+  // EXPLT0 of the tile's own cells, two-slot ring one plane ahead
+  auto issue_e = [&](int k) {
+    const int sl = (k - kbeg) & 1;
+    mbar_expect_tx(&ebar[sl], (uint32_t)(3 * IT_EBOX * sizeof(double)));
+#pragma unroll
+    for (int q = 0; q < 3; ++q) tma_load_3d(eslot(sl) + q * IT_EBOX, &maps.m[11 + q], x0, j0, k, &ebar[sl]);
+  };
+  uint32_t epar = 0;
+  if (tid == 0) {
+    issue(kbeg - 1);
+    issue(kbeg);
+    issue(kbeg + 1);
+    issue_e(kbeg);
+  }
+  bool ok = wait_plane(kbeg - 1);
+  ok = wait_plane(kbeg) && ok;
+  double part = 0.0;
+  const double dxi = d.dxi, dzi = d.dzi, cv = d.cvisc, dt = d.dt;
+  const double *yc = ycoef[ty];
+  const int xx = tx + 2, yy = ty + 1;
+  const bool th = io.thermal != 0;
+  for (int k = kbeg; k < kend; ++k) {
+    if (tid == 0) {
+      fence_proxy_async();
+      if (k + 2 <= kend) issue(k + 2);
+      if (k + 1 < kend) issue_e(k + 1);
+    }
+    ok = wait_plane(k + 1) && ok;
+    {
+      const int esl = (k - kbeg) & 1;
+      ok = mbar_wait(&ebar[esl], (epar >> esl) & 1u, d.err) && ok;
+      epar ^= 1u << esl;
+    }
+    __syncthreads();
+    const double *Es = eslot((k - kbeg) & 1);
+    if (active && ok) {
+      const double *Sm = slot(slot_of(k - 1));
+      const double *Sc = slot(slot_of(k));
+      const double *Sp = slot(slot_of(k + 1));
+#define A(S, f, dx, dy) S[(f) * IT_PST + (yy + (dy)) * IT_BXW + xx + (dx)]
+      const double wff = yc[0], wfb = yc[1], wffp = yc[2], wfbp = yc[3], dyfj = yc[4], dycj = yc[5], dycp = yc[6];
+      // cell-centred 0.5 (mu0 + mu), M = mu0 + mu
+      auto muc = [&](const double *S, int dx, int dy) { return th ? 0.5 * A(S, F_M, dx, dy) : 1.0; };
+      // MU_STG(.,.,.,1) at the cell (dx, dy) of plane S, row jj = j + dy
+      auto s1 = [&](const double *S, int dx, int dy, double wf, double wb) {
+        if (!th) return 1.0;
+        const int jj = j + dy;
+        if (jj == 1) return 0.5 * A(S, F_M, dx, dy - 1);
+        if (jj == ny + 1) return 0.5 * A(S, F_M, dx, dy);
+        return ((A(S, F_M, dx, dy) + A(S, F_M, dx - 1, dy)) * wf + (A(S, F_M, dx, dy - 1) + A(S, F_M, dx - 1, dy - 1)) * wb) *
+               0.5 * 0.5;
+      };
+      // MU_STG(.,.,.,2) at the cell (dx) of plane S (its z-minus plane Sb)
+      auto s2 = [&](const double *S, const double *Sb, int dx) {
+        if (!th) return 1.0;
+        return (A(S, F_M, dx, 0) + A(S, F_M, dx - 1, 0) + A(Sb, F_M, dx, 0) + A(Sb, F_M, dx - 1, 0)) * 0.5 * 0.5 * 0.5;
+      };
+      // MU_STG(.,.,.,3) at row jj = j + dy of plane S (z-minus plane Sb)
+      auto s3 = [&](const double *S, const double *Sb, int dy, double wf, double wb) {
+        if (!th) return 1.0;
+        const int jj = j + dy;
+        if (jj == 1) return 0.5 * A(S, F_M, 0, dy - 1);
+        if (jj == ny + 1) return 0.5 * A(S, F_M, 0, dy);
+        return ((A(Sb, F_M, 0, dy) + A(S, F_M, 0, dy)) * wf + (A(Sb, F_M, 0, dy - 1) + A(S, F_M, 0, dy - 1)) * wb) * 0.5 *
+               0.5;
+      };
+      // DIVG_U_io at (dx, dy) of plane S (its z-plus plane Sn), row jj
+      auto divu = [&](const double *S, const double *Sn, int dx, int dy, double dyf) {
+        return ((A(S, F_U, dx + 1, dy) - A(S, F_U, dx, dy)) * dxi + (A(S, F_V, dx, dy + 1) - A(S, F_V, dx, dy)) * dyf +
+                (A(Sn, F_W, dx, dy) - A(S, F_W, dx, dy)) * dzi) / 3.0;
+      };
+      const int64_t sy = d.sy, c = i + sy * j + d.sz * k;
+      const int64_t oxm = (i == 0 ? nx - 1 : i - 1) - i, ozm = d.sz * ((k == 0 ? nz - 1 : k - 1) - k);
+      const double p0 = A(Sc, F_P, 0, 0);
+      const double divc = divu(Sc, Sp, 0, 0, dyfj);
+      // ---------------- x
+      {
+        const double u0 = A(Sc, F_U, 0, 0);
+        double h11f = (A(Sc, F_GX, 1, 0) + A(Sc, F_GX, 0, 0)) * (A(Sc, F_U, 1, 0) + u0);
+        double h11b = (A(Sc, F_GX, 0, 0) + A(Sc, F_GX, -1, 0)) * (u0 + A(Sc, F_U, -1, 0));
+        double h11 = (h11f - h11b) * (dxi * 0.5 * 0.5);
+        double h12f = (A(Sc, F_GY, 0, 1) + A(Sc, F_GY, -1, 1)) * (wffp * A(Sc, F_U, 0, 1) + wfbp * u0);
+        double h12b = (A(Sc, F_GY, 0, 0) + A(Sc, F_GY, -1, 0)) * (wff * u0 + wfb * A(Sc, F_U, 0, -1));
+        double h12 = (h12f - h12b) * (dyfj * 0.5);
+        double h13f = (A(Sp, F_GZ, 0, 0) + A(Sp, F_GZ, -1, 0)) * (A(Sp, F_U, 0, 0) + u0);
+        double h13b = (A(Sc, F_GZ, 0, 0) + A(Sc, F_GZ, -1, 0)) * (u0 + A(Sm, F_U, 0, 0));
+        double h13 = (h13f - h13b) * (dzi * 0.5 * 0.5);
+        double ex = -(h11 + h12 + h13);
+        double dudx = (A(Sc, F_U, 1, 0) - u0) * dxi;
+        const double tau11f = muc(Sc, 0, 0) * (dudx - divc);
+        dudx = (u0 - A(Sc, F_U, -1, 0)) * dxi;
+        const double tau11b = muc(Sc, -1, 0) * (dudx - divu(Sc, Sp, -1, 0, dyfj));
+        const double d11 = (tau11f - tau11b) * (2.0 * dxi * cv);
+        double dudy = (A(Sc, F_U, 0, 1) - u0) * dycp;
+        double dvdx = (A(Sc, F_V, 0, 1) - A(Sc, F_V, -1, 1)) * dxi;
+        const double tau12f = s1(Sc, 0, 1, wffp, wfbp) * (dudy + dvdx);
+        dudy = (u0 - A(Sc, F_U, 0, -1)) * dycj;
+        dvdx = (A(Sc, F_V, 0, 0) - A(Sc, F_V, -1, 0)) * dxi;
+        const double tau12b = s1(Sc, 0, 0, wff, wfb) * (dudy + dvdx);
+        const double d12 = (tau12f - tau12b) * (dyfj * cv);
+        double dudz = (A(Sp, F_U, 0, 0) - u0) * dzi;
+        double dwdx = (A(Sp, F_W, 0, 0) - A(Sp, F_W, -1, 0)) * dxi;
+        const double tau13f = s2(Sp, Sc, 0) * (dudz + dwdx);
+        dudz = (u0 - A(Sm, F_U, 0, 0)) * dzi;
+        dwdx = (A(Sc, F_W, 0, 0) - A(Sc, F_W, -1, 0)) * dxi;
+        const double tau13b = s2(Sc, Sm, 0) * (dudz + dwdx);
+        const double d13 = (tau13f - tau13b) * (dzi * cv);
+        ex = ex + d11 + d12 + d13;
+        double r = (gam * ex + roh * Es[tid]) * dt;
+        ((double *)d.h0[0])[c] = ex;
+        r -= (p0 - A(Sc, F_P, -1, 0)) * (alp * dt * dxi);
+        if (io.gravdir == 1) {
+          const double rs = th ? (io.D[c] + io.D[c + oxm] + io.D0[c] + io.D0[c + oxm]) * 0.5 * 0.5 : 1.0;
+          r += rs * (alp * dt * io.f_a);
+        }
+        part += r / dyfj;
+        io.g[1 - cur][0][c] = A(Sc, F_GX, 0, 0) + r;
+      }
+      // ---------------- y (rows 2..ny)
+      if (j >= 2) {
+        const double v0 = A(Sc, F_V, 0, 0);
+        double h21f = (wff * A(Sc, F_GX, 1, 0) + wfb * A(Sc, F_GX, 1, -1)) * (A(Sc, F_V, 1, 0) + v0);
+        double h21b = (wff * A(Sc, F_GX, 0, 0) + wfb * A(Sc, F_GX, 0, -1)) * (v0 + A(Sc, F_V, -1, 0));
+        double h21 = (h21f - h21b) * (dxi * 0.5);
+        double h22f = (A(Sc, F_GY, 0, 1) + A(Sc, F_GY, 0, 0)) * (A(Sc, F_V, 0, 1) + v0);
+        double h22b = (A(Sc, F_GY, 0, 0) + A(Sc, F_GY, 0, -1)) * (v0 + A(Sc, F_V, 0, -1));
+        double h22 = (h22f - h22b) * (dycj * 0.5 * 0.5);
+        double h23f = (wff * A(Sp, F_GZ, 0, 0) + wfb * A(Sp, F_GZ, 0, -1)) * (A(Sp, F_V, 0, 0) + v0);
+        double h23b = (wff * A(Sc, F_GZ, 0, 0) + wfb * A(Sc, F_GZ, 0, -1)) * (v0 + A(Sm, F_V, 0, 0));
+        double h23 = (h23f - h23b) * (dzi * 0.5);
+        double ey = -(h21 + h22 + h23);
+        double dvdy = (A(Sc, F_V, 0, 1) - v0) * dyfj;
+        const double tau22f = muc(Sc, 0, 0) * (dvdy - divc);
+        dvdy = (v0 - A(Sc, F_V, 0, -1)) * yc[7];
+        const double tau22b = muc(Sc, 0, -1) * (dvdy - divu(Sc, Sp, 0, -1, yc[7]));
+        const double d22 = (tau22f - tau22b) * (2.0 * dycj * cv);
+        double dvdx = (A(Sc, F_V, 1, 0) - v0) * dxi;
+        double dudy = (A(Sc, F_U, 1, 0) - A(Sc, F_U, 1, -1)) * dycj;
+        const double tau21f = s1(Sc, 1, 0, wff, wfb) * (dvdx + dudy);
+        dvdx = (v0 - A(Sc, F_V, -1, 0)) * dxi;
+        dudy = (A(Sc, F_U, 0, 0) - A(Sc, F_U, 0, -1)) * dycj;
+        const double tau21b = s1(Sc, 0, 0, wff, wfb) * (dvdx + dudy);
+        const double d21 = (tau21f - tau21b) * (dxi * cv);
+        double dvdz = (A(Sp, F_V, 0, 0) - v0) * dzi;
+        double dwdy = (A(Sp, F_W, 0, 0) - A(Sp, F_W, 0, -1)) * dycj;
+        const double tau23f = s3(Sp, Sc, 0, wff, wfb) * (dvdz + dwdy);
+        dvdz = (v0 - A(Sm, F_V, 0, 0)) * dzi;
+        dwdy = (A(Sc, F_W, 0, 0) - A(Sc, F_W, 0, -1)) * dycj;
+        const double tau23b = s3(Sc, Sm, 0, wff, wfb) * (dvdz + dwdy);
+        const double d23 = (tau23f - tau23b) * (dzi * cv);
+        ey = ey + d21 + d22 + d23;
+        double r = (gam * ey + roh * Es[IT_EBOX + tid]) * dt;
+        ((double *)d.h0[1])[c] = ey;
+        r -= (p0 - A(Sc, F_P, 0, -1)) * (alp * dt * dycj);
+        if (io.gravdir == 2) {
+          const double rs = th ? (wff * (io.D[c] + io.D0[c]) + wfb * (io.D[c - sy] + io.D0[c - sy])) * 0.5 : 1.0;
+          r += rs * (alp * dt * io.f_a);
+        }
+        io.g[1 - cur][1][c] = A(Sc, F_GY, 0, 0) + r;
+      }
+      // ---------------- z
+      {
+        const double w0 = A(Sc, F_W, 0, 0);
+        double h31f = (A(Sc, F_GX, 1, 0) + A(Sm, F_GX, 1, 0)) * (A(Sc, F_W, 1, 0) + w0);
+        double h31b = (A(Sc, F_GX, 0, 0) + A(Sm, F_GX, 0, 0)) * (w0 + A(Sc, F_W, -1, 0));
+        double h31 = (h31f - h31b) * (dxi * 0.5 * 0.5);
+        double h32f = (A(Sc, F_GY, 0, 1) + A(Sm, F_GY, 0, 1)) * (wffp * A(Sc, F_W, 0, 1) + wfbp * w0);
+        double h32b = (A(Sc, F_GY, 0, 0) + A(Sm, F_GY, 0, 0)) * (wff * w0 + wfb * A(Sc, F_W, 0, -1));
+        double h32 = (h32f - h32b) * (dyfj * 0.5);
+        double h33f = (A(Sp, F_GZ, 0, 0) + A(Sc, F_GZ, 0, 0)) * (A(Sp, F_W, 0, 0) + w0);
+        double h33b = (A(Sc, F_GZ, 0, 0) + A(Sm, F_GZ, 0, 0)) * (w0 + A(Sm, F_W, 0, 0));
+        double h33 = (h33f - h33b) * (dzi * 0.5 * 0.5);
+        double ez = -(h31 + h32 + h33);
+        double dwdz = (A(Sp, F_W, 0, 0) - w0) * dzi;
+        const double tau33f = muc(Sc, 0, 0) * (dwdz - divc);
+        dwdz = (w0 - A(Sm, F_W, 0, 0)) * dzi;
+        const double tau33b = muc(Sm, 0, 0) * (dwdz - divu(Sm, Sc, 0, 0, dyfj));
+        const double d33 = (tau33f - tau33b) * (2.0 * dzi * cv);
+        double dwdx = (A(Sc, F_W, 1, 0) - w0) * dxi;
+        double dudz = (A(Sc, F_U, 1, 0) - A(Sm, F_U, 1, 0)) * dzi;
+        const double tau31f = s2(Sc, Sm, 1) * (dwdx + dudz);
+        dwdx = (w0 - A(Sc, F_W, -1, 0)) * dxi;
+        dudz = (A(Sc, F_U, 0, 0) - A(Sm, F_U, 0, 0)) * dzi;
+        const double tau31b = s2(Sc, Sm, 0) * (dwdx + dudz);
+        const double d31 = (tau31f - tau31b) * (dxi * cv);
+        double dwdy = (A(Sc, F_W, 0, 1) - w0) * dycp;
+        double dvdz = (A(Sc, F_V, 0, 1) - A(Sm, F_V, 0, 1)) * dzi;
+        const double tau32f = s3(Sc, Sm, 1, wffp, wfbp) * (dwdy + dvdz);
+        dwdy = (w0 - A(Sc, F_W, 0, -1)) * dycj;
+        dvdz = (A(Sc, F_V, 0, 0) - A(Sm, F_V, 0, 0)) * dzi;
+        const double tau32b = s3(Sc, Sm, 0, wff, wfb) * (dwdy + dvdz);
+        const double d32 = (tau32f - tau32b) * (dyfj * cv);
+        ez = ez + d31 + d32 + d33;
+        double r = (gam * ez + roh * Es[2 * IT_EBOX + tid]) * dt;
+        ((double *)d.h0[2])[c] = ez;
+        r -= (p0 - A(Sm, F_P, 0, 0)) * (alp * dt * dzi);
+        if (io.gravdir == 3) {
+          const double rs = th ? (io.D[c] + io.D[c + ozm] + io.D0[c] + io.D0[c + ozm]) * 0.5 * 0.5 : 1.0;
+          r += rs * (alp * dt * io.f_a);
+        }
+        io.g[1 - cur][2][c] = A(Sc, F_GZ, 0, 0) + r;
+      }
+#undef A
+    }
+    __syncthreads();
+  }
+  // every issued plane has been waited for, so no bulk copy is in flight at exit
+  for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+  if ((tid & 31) == 0) red[tid >> 5] = part;
+  __syncthreads();
+  if (tid == 0) {
+    double s = 0.0;
+    for (int q = 0; q < IO_BX * IO_BY / 32; ++q) s += red[q];
+    io.part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = s;
+  }
+}
+
 // DPGRNS (src/RHS_MOM_EXPLICIT_io.f90:200-240): constant mass flux from the
 // block partials in a fixed order, or the constant pressure gradient.
 __global__ void __launch_bounds__(1024) k_io_dpgrns(TGDev d, IODev io, double alp, int npart) {
@@ -587,12 +916,17 @@ int io_thermal_bc(chapsim_ctx *c) {
   return CHAPSIM_OK;
 }
 
+// Phase-timer slots of an IO substep, in execution order: 0 energy RHS,
+// 1 property update + wall ghosts, 2 prep (DrhoDtP, u = G / rho), 3 momentum
+// RHS + DPGRNS, 4-8 the Poisson transforms and y-solve, 9 correction.
 int io_eng(chapsim_ctx *c, int ns) {
   TGDev &d = c->d;
   const SubParams &sp = c->sp[ns];
+  phase_mark(c, 0);
   k_io_eng_rhs<<<cell_grid(d), dim3(IO_BX, IO_BY), 0, c->stream>>>(d, c->io, sp.gam * d.dt, sp.roh * d.dt, c->io_cur);
   LAUNCHED();
   dim3 g2((d.nx + IO_BX - 1) / IO_BX, (d.ny + 2 + IO_BY - 1) / IO_BY, d.nz);
+  phase_mark(c, 1);
   k_io_eng_props<<<g2, dim3(IO_BX, IO_BY), 0, c->stream>>>(d, c->io);
   LAUNCHED();
   return io_thermal_bc(c);
@@ -604,19 +938,85 @@ int io_mom(chapsim_ctx *c, int ns, bool prep) {
   const SubParams &sp = c->sp[ns];
   const int cur = c->io_cur, nxt = 1 - cur;
   const dim3 grid = cell_grid(d), blk(IO_BX, IO_BY);
+  if (!io.thermal) {
+    phase_mark(c, 0);
+    phase_mark(c, 1);
+  }
+  phase_mark(c, 2);
   if (prep) {
     k_io_prep<<<grid, blk, 0, c->stream>>>(d, io, sp.gam + sp.roh, sp.roh, sp.gam - 2.0, cur, io.thermal);
     LAUNCHED();
   }
-  k_io_rhs<<<grid, blk, 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, cur);
+  phase_mark(c, 3);
+  int npart = (int)(grid.x * grid.y * grid.z);
+  if (c->use_tma_io) {
+    IoMaps maps;
+    memcpy(maps.m, c->io_maps, sizeof(maps.m));
+    dim3 g2(grid.x, grid.y, (d.nz + c->io_nzc - 1) / c->io_nzc);
+    k_io_rhs_tma<<<g2, blk, IT_SMEM, c->stream>>>(maps, d, io, sp.gam, sp.roh, sp.alp, cur, c->io_nzc);
+    npart = (int)(g2.x * g2.y * g2.z);
+  } else {
+    k_io_rhs<<<grid, blk, 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, cur);
+  }
   LAUNCHED();
-  k_io_dpgrns<<<1, 1024, 0, c->stream>>>(d, io, sp.alp, (int)(grid.x * grid.y * grid.z));
+  k_io_dpgrns<<<1, 1024, 0, c->stream>>>(d, io, sp.alp, npart);
   LAUNCHED();
   int rc = launch_pois_io(c, ns, io.g[nxt][0], io.g[nxt][1], io.g[nxt][2], io.thermal ? io.drho : nullptr);
   if (rc) return rc;
+  phase_mark(c, CHAPSIM_PH_CORR);
   k_io_corr<<<grid, blk, 0, c->stream>>>(d, io, sp.alp, nxt, 1);
   LAUNCHED();
   c->io_cur = nxt;
+  if (c->timing) {
+    phase_mark(c, CHAPSIM_PH_COUNT);
+    if (++c->ev_pending == chapsim_ctx::kEvSub) return flush_phase_events(c);
+  }
+  return CHAPSIM_OK;
+}
+
+int io_init_maps(chapsim_ctx *c) {
+  TGDev &d = c->d;
+  c->use_tma_io = false;
+  if (d.nx < IT_BXW || d.ny < 8) return CHAPSIM_OK;  // small grids use k_io_rhs
+  PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void **)&encode, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !encode) {
+    cudaGetLastError();
+    return CHAPSIM_OK;
+  }
+  IODev &io = c->io;
+  void *f[14] = {d.u,        d.v,        d.w,        d.p,        io.msum,    io.g[0][0], io.g[0][1],
+                 io.g[0][2], io.g[1][0], io.g[1][1], io.g[1][2], d.h0[0],    d.h0[1],    d.h0[2]};
+  cuuint64_t dims[3] = {(cuuint64_t)d.nx, (cuuint64_t)(d.ny + 2), (cuuint64_t)d.nz};
+  cuuint64_t strides[2] = {(cuuint64_t)d.sy * sizeof(double), (cuuint64_t)d.sz * sizeof(double)};
+  cuuint32_t box[3] = {IT_BXW, IT_BYW, 1}, ebox[3] = {IO_BX, IO_BY, 1};
+  cuuint32_t es[3] = {1, 1, 1};
+  if ((d.sy * sizeof(double)) % 16 != 0) return CHAPSIM_OK;  // TMA strides must be multiples of 16 bytes
+  for (int m = 0; m < 14; ++m) {
+    CUresult r = encode(&c->io_maps[m], CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, f[m], dims, strides, m >= 11 ? ebox : box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+      c->err = "cuTensorMapEncodeTiled failed";
+      return CHAPSIM_ERR_CUDA;
+    }
+  }
+  int dev = 0, optin = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa;
+  CK(cudaFuncGetAttributes(&fa, (const void *)k_io_rhs_tma));
+  if ((size_t)optin < IT_SMEM + fa.sharedSizeBytes) return CHAPSIM_OK;
+  CK(cudaFuncSetAttribute((const void *)k_io_rhs_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          optin - (int)fa.sharedSizeBytes));
+  c->use_tma_io = true;
+  return CHAPSIM_OK;
+}
+
+int io_refresh_msum(chapsim_ctx *c) {
+  k_io_msum<<<148 * 8, 256, 0, c->stream>>>(c->io, (size_t)c->d.sz * c->d.nz);
+  LAUNCHED();
   return CHAPSIM_OK;
 }
 

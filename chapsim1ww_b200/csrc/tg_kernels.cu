@@ -1082,9 +1082,7 @@ __global__ void __launch_bounds__(1024) k_reduce_final(TGDev d, int what, int np
 }
 
 // ============================================================ launchers
-static inline void phase_mark(chapsim_ctx *c, int ph) {
-  if (c->timing) cudaEventRecord(c->evpool[(size_t)c->ev_pending * (CHAPSIM_PH_COUNT + 1) + ph], c->stream);
-}
+
 
 // Read back every buffered substep's phase events and accumulate them.
 int flush_phase_events(chapsim_ctx *c) {

@@ -330,6 +330,7 @@ void bc_wall_copy(oracle_io *o, std::vector<double> &f) {
 // VELOCITY_CALC_io (src/MASSFLUX_CALC_IO.f90:82-142).
 void velocity_calc(oracle_io *o) {
   const int nx = o->nx, ny = o->ny, nz = o->nz;
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
   for (int k = 1; k <= nz; ++k)
     for (int j = 1; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) {
@@ -345,6 +346,7 @@ void velocity_calc(oracle_io *o) {
 void density_time_derivation(oracle_io *o, int ns) {
   const int nx = o->nx, ny = o->ny, nz = o->nz;
   const double gp = o->tgam[ns] + o->troh[ns], zr = o->troh[ns], den = o->tgam[ns] - 2.0;
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
   for (int k = 1; k <= nz; ++k)
     for (int j = 1; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) {
@@ -429,6 +431,7 @@ void convection(oracle_io *o) {
 // DIVG_U_io (src/DIVG.f90:153-259): div u / 3 at cell centres.
 void divg_u(oracle_io *o) {
   const int nx = o->nx, ny = o->ny, nz = o->nz;
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
   for (int k = 1; k <= nz; ++k)
     for (int j = 1; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) {
@@ -546,6 +549,7 @@ void rhs_mom(oracle_io *o, int ns, int idr, std::vector<double> &tmp) {
   const int nx = o->nx, ny = o->ny, nz = o->nz;
   const int nyi = idr == 2 ? 2 : 1;
   const double gam = o->tgam[ns], roh = o->troh[ns], alp = o->talp[ns], dt = o->dt;
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
   for (int k = 1; k <= nz; ++k)
     for (int j = nyi; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) {
@@ -710,6 +714,7 @@ void mom_io(oracle_io *o, int ns) {
   rhs_mom(o, ns, 2, o->dphtmp);
   rhs_mom(o, ns, 3, o->rhsz);
   // MASSFLUX_CALC_IO (src/MASSFLUX_CALC_IO.f90:1-79)
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
   for (int k = 1; k <= nz; ++k)
     for (int j = 1; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) {
@@ -720,6 +725,7 @@ void mom_io(oracle_io *o, int ns) {
   bc_wall_vec(o, o->g);
   // DIVG_io (src/DIVG.f90:60-150)
   const double coe0 = 1.0 / o->dt / o->talp[ns];
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
   for (int k = 1; k <= nz; ++k)
     for (int j = 1; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) {
@@ -730,12 +736,14 @@ void mom_io(oracle_io *o, int ns) {
       }
   fishpack_pois3d(o);
   // PRCALC_io (src/PRESSURE_CORRECTION.f90:86-122), explicit branch
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
   for (int k = 1; k <= nz; ++k)
     for (int j = 1; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) F(pr, i, j, k) += F(dph, i, j, k);
   bc_wall_copy(o, o->pr);
   // MASSFLUX_UPDATE_IO (src/VELO_CORRECTION.f90:107-185)
   const double cx = o->dt * o->talp[ns] * o->dxi, cz = o->dt * o->talp[ns] * o->dzi;
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
   for (int k = 1; k <= nz; ++k)
     for (int j = 1; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) {
@@ -752,6 +760,7 @@ void eng_io(oracle_io *o, int ns) {
   o->dd0 = o->dd;
   rhs_energy(o);
   const double coe1 = o->tgam[ns] * o->dt, coe0 = o->troh[ns] * o->dt;
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
   for (int k = 1; k <= nz; ++k)
     for (int j = 1; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) {

@@ -56,7 +56,8 @@ def test_io_isothermal_parity(dims):
     assert abs(g.bulk_massflux_io() - o.bulk(1)) < 1e-12
 
 
-@pytest.mark.parametrize("dims", [(16, 12, 8), (32, 24, 16), (40, 18, 24)])
+# nx >= 36 runs the TMA z-marching momentum RHS (80: a partial last x tile)
+@pytest.mark.parametrize("dims", [(16, 12, 8), (32, 24, 16), (40, 18, 24), (64, 16, 12), (80, 12, 10)])
 def test_io_thermal_parity(dims):
     g, o = pair(*dims, thermal=1)
     compare(g, o, FLOW + THERMAL, tag="init+projection")
