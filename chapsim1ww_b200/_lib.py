@@ -45,7 +45,7 @@ class ChapsimIOConfig(ctypes.Structure):
 # IO domain field and reduction ids
 F_GX, F_GY, F_GZ, F_G0X, F_G0Y, F_G0Z = 10, 11, 12, 13, 14, 15
 F_H, F_T, F_RHO, F_MU, F_K, F_RHOH, F_RHO0, F_MU0, F_DRHO, F_RHSE0 = range(16, 26)
-R_DIVMAX_Q, R_BULK_G, R_BULK_H, R_BADCELLS = 3, 4, 5, 6
+R_DIVMAX_Q, R_BULK_G, R_BULK_H, R_BADCELLS, R_CFL = 3, 4, 5, 6, 7
 
 # (name, restype, argtypes) for every symbol declared in include/chapsim.h
 _P = ctypes.c_void_p
@@ -112,7 +112,12 @@ SIGNATURES += [
     ("chapsim_rk3_eng_io", _I, [_P, _I]),
     ("chapsim_rk3_mom_io", _I, [_P, _I]),
     ("chapsim_step_io", _I, [_P, _I]),
+    ("chapsim_set_dt", _I, [_P, _D]),
+    ("chapsim_stats", _I, [_P, _I]),
+    ("chapsim_get_stats", _I, [_P, _I, _P, _I64, ctypes.POINTER(_I64)]),
+    ("chapsim_stats_reset", _I, [_P]),
 ]
+STATS_NV = 122
 PROPS_TABLE, PROPS_MLP = 0, 1
 ERR_RANGE = 8
 ERRORS[8] = "CHAPSIM_ERR_RANGE"

@@ -978,6 +978,56 @@ int chapsim_velo_correction(chapsim_ctx *ctx, int domain, int ns) {
   return launch_correction(ctx, ns);
 }
 
+int chapsim_stats(chapsim_ctx *ctx, int accumulate) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(ctx->domain == CHAPSIM_ITG, CHAPSIM_ERR_UNSUPPORTED, "statistics are built for the TG domain");
+  CKC(cudaSetDevice(ctx->device));
+  return stats_run(ctx, accumulate);
+}
+
+int chapsim_get_stats(chapsim_ctx *ctx, int which, double *out, int64_t n, int64_t *nstatis) {
+  REQUIRE(ctx && out, CHAPSIM_ERR_ARG, "null argument");
+  REQUIRE(which == 0 || which == 1, CHAPSIM_ERR_ARG, "which: 0 xz average, 1 time average");
+  REQUIRE(ctx->stats_buf, CHAPSIM_ERR_STATE, "chapsim_stats has not run");
+  REQUIRE(n == (int64_t)ctx->cfg.ny * CHAPSIM_STATS_NV, CHAPSIM_ERR_ARG, "n must be ny * CHAPSIM_STATS_NV");
+  CKC(cudaSetDevice(ctx->device));
+  if (nstatis) *nstatis = ctx->nstatis;
+  return stats_get(ctx, which, out, n);
+}
+
+int chapsim_stats_reset(chapsim_ctx *ctx) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  CKC(cudaSetDevice(ctx->device));
+  return stats_reset(ctx);
+}
+
+int chapsim_set_dt(chapsim_ctx *ctx, double dt) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(dt > 0 && dt < 1e3, CHAPSIM_ERR_ARG, "dt must be positive");
+  CKC(cudaSetDevice(ctx->device));
+  CKC(cudaStreamSynchronize(ctx->stream));
+  // every coefficient table that depends on dt (RK factors, Crank-Nicolson
+  // factors and their banded inverses) is rebuilt; captured graphs go stale
+  double *old = ctx->dcoef;
+  const double dt_old = ctx->cfg.dt;
+  ctx->cfg.dt = dt;
+  int rc = build_tables(ctx);
+  if (rc) {
+    ctx->cfg.dt = dt_old;
+    return rc;
+  }
+  for (auto it = ctx->allocs.begin(); it != ctx->allocs.end(); ++it)
+    if (*it == (void *)old) {
+      cudaFree(old);
+      ctx->allocs.erase(it);
+      break;
+    }
+  if (ctx->step_graph) { cudaGraphExecDestroy(ctx->step_graph); ctx->step_graph = nullptr; }
+  for (auto &g : ctx->io_graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  return CHAPSIM_OK;
+}
+
 int chapsim_set_table(chapsim_ctx *ctx, const double *H, const double *T, const double *D, const double *M,
                       const double *K, int n, int shortcuts) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
@@ -1102,10 +1152,11 @@ int chapsim_reduce(chapsim_ctx *ctx, int domain, int what, double *out) {
     if (what == CHAPSIM_R_DIVMAX_Q || what == CHAPSIM_R_NANCOUNT)
       return launch_reduce(ctx, what == CHAPSIM_R_DIVMAX_Q ? 0 : 2, out);  // on u, v, w (, p)
     REQUIRE(what == CHAPSIM_R_DIVMAX || what == CHAPSIM_R_BULK || what == CHAPSIM_R_BULK_G ||
-                what == CHAPSIM_R_BULK_H,
+                what == CHAPSIM_R_BULK_H || what == CHAPSIM_R_CFL,
             CHAPSIM_ERR_ARG, "unknown reduction");
     return io_reduce(ctx, what, out);
   }
+  if (what == CHAPSIM_R_CFL) return launch_reduce(ctx, 3, out);
   REQUIRE(what >= 0 && what <= 2, CHAPSIM_ERR_ARG, "unknown reduction");
   double v = 0.0;
   int rc = launch_reduce(ctx, what, &v);

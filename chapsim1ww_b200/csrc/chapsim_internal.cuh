@@ -151,6 +151,10 @@ struct chapsim_ctx {
   CUtensorMap io_maps[14];
   bool use_tma_io = false;
   int io_nzc = 16;  // z planes per block of the TMA momentum RHS
+  // on-device statistics (partials, xz averages, time averages) and the
+  // number of samples in the time average
+  double *stats_buf = nullptr;
+  int64_t nstatis = 0;
 };
 
 // Kernel launch wrappers (defined in tg_kernels.cu).
@@ -179,5 +183,9 @@ int io_reduce(chapsim_ctx *c, int what, double *host_out);
 int io_correction(chapsim_ctx *c, int ns);
 int io_init_maps(chapsim_ctx *c);
 int io_refresh_msum(chapsim_ctx *c);
+// TG statistics (stats.cu)
+int stats_run(chapsim_ctx *c, int accumulate);
+int stats_get(chapsim_ctx *c, int which, double *host, int64_t n);
+int stats_reset(chapsim_ctx *c);
 int fill_value(chapsim_ctx *c, double *p, size_t n, double v);
 }  // namespace chapsim

@@ -843,7 +843,9 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_corr(TGDev d, IODev io, dou
 }
 
 // ---------------------------------------------------------------- reductions
-// what 0: max|div G + DrhoDtP| (DIVGCK_io); 1: sum of f / DYFI (bulk values).
+// what 0: max|div G + DrhoDtP| (DIVGCK_io); 1: sum of f / DYFI (bulk values);
+// 2: max CFL of G plus the explicit viscous limit (CFL_io + CFL_VISCOUS,
+// src/CFL.f90:42-133).
 __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_red_part(TGDev d, IODev io, int what, int cur, const double *f) {
   __shared__ double sh[IO_BX * IO_BY / 32];
   const int nx = d.nx, ny = d.ny;
@@ -860,37 +862,45 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_red_part(TGDev d, IODev io,
                         (gz[c + ozp] - gz[c]) * d.dzi + io.drho[c];
       v = fabs(dv);
       if (dv != dv) v = __longlong_as_double(0x7ff0000000000000ll);
+    } else if (what == 2) {
+      const int64_t oxp = wrapp(i, nx) - i, ozp = d.sz * (wrapp(k, d.nz) - k);
+      const double *gx = io.g[cur][0], *gy = io.g[cur][1], *gz = io.g[cur][2];
+      v = (fabs((gx[c] + gx[c + oxp]) * d.dxi) + fabs((gy[c] + gy[c + sy]) * d.dyfi[j]) +
+           fabs((gz[c] + gz[c + ozp]) * d.dzi)) * 0.5;
+      v = v + 2.0 * d.cvisc * (d.dxqi + d.dzqi + d.dyfi[j] * d.dyfi[j]);
     } else {
       v = f[c] / d.dyfi[j];
     }
   }
+  const bool mx = what != 1;
   for (int o = 16; o > 0; o >>= 1) {
     const double x = __shfl_xor_sync(0xffffffffu, v, o);
-    v = what == 0 ? fmax(v, x) : v + x;
+    v = mx ? fmax(v, x) : v + x;
   }
   const int tid = threadIdx.x + IO_BX * threadIdx.y;
   if ((tid & 31) == 0) sh[tid >> 5] = v;
   __syncthreads();
   if (tid == 0) {
     double s = 0.0;
-    for (int q = 0; q < IO_BX * IO_BY / 32; ++q) s = what == 0 ? fmax(s, sh[q]) : s + sh[q];
+    for (int q = 0; q < IO_BX * IO_BY / 32; ++q) s = mx ? fmax(s, sh[q]) : s + sh[q];
     d.partials[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = s;
   }
 }
 
 __global__ void __launch_bounds__(1024) k_io_red_final(TGDev d, int what, int npart) {
   __shared__ double sh[32];
+  const bool mx = what != 1;
   double s = 0.0;
-  for (int t = threadIdx.x; t < npart; t += blockDim.x) s = what == 0 ? fmax(s, d.partials[t]) : s + d.partials[t];
+  for (int t = threadIdx.x; t < npart; t += blockDim.x) s = mx ? fmax(s, d.partials[t]) : s + d.partials[t];
   for (int o = 16; o > 0; o >>= 1) {
     const double x = __shfl_xor_sync(0xffffffffu, s, o);
-    s = what == 0 ? fmax(s, x) : s + x;
+    s = mx ? fmax(s, x) : s + x;
   }
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
   __syncthreads();
   if (threadIdx.x == 0) {
     double r = 0.0;
-    for (int q = 0; q < 32; ++q) r = what == 0 ? fmax(r, sh[q]) : r + sh[q];
+    for (int q = 0; q < 32; ++q) r = mx ? fmax(r, sh[q]) : r + sh[q];
     d.scal[1] = r;
   }
 }
@@ -1035,6 +1045,7 @@ int io_reduce(chapsim_ctx *c, int what, double *host_out) {
   int kind = 1;
   switch (what) {
     case CHAPSIM_R_DIVMAX: kind = 0; break;
+    case CHAPSIM_R_CFL: kind = 2; break;
     case CHAPSIM_R_BULK: f = d.u; break;
     case CHAPSIM_R_BULK_G: f = c->io.g[c->io_cur][0]; break;
     case CHAPSIM_R_BULK_H: f = c->io.h; break;

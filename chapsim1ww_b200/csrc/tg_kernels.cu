@@ -1063,12 +1063,18 @@ __global__ void __launch_bounds__(RHS_BX *RHS_BY) k_reduce_part(TGDev d, int wha
       if (dv != dv) v = __longlong_as_double(0x7ff0000000000000ll);  // NaN -> +inf
     } else if (what == 1) {
       v = d.u[c0] / d.dyfi[j];
+    } else if (what == 3) {
+      // CFL_tg (src/CFL.f90:1-40): 0.5 (|u+u_ip| dxi + |v+v_jp| dyfi + |w+w_kp| dzi)
+      const int ip = wrapp(i, nx), kp = wrapp(k, d.nz);
+      v = (fabs((d.u[c0] + d.u[c0 + (ip - i)]) * d.dxi) + fabs((d.v[c0] + d.v[c0 + d.sy]) * d.dyfi[j]) +
+           fabs((d.w[c0] + d.w[c0 + d.sz * (kp - k)]) * d.dzi)) * 0.5;
     } else {
       v = (double)(!isfinite(d.u[c0])) + (double)(!isfinite(d.v[c0])) + (double)(!isfinite(d.w[c0])) +
           (double)(!isfinite(d.p[c0]));
     }
   }
-  const double s = what == 0 ? block_max(v, sh) : block_sum(v, sh);
+  const bool mx = what == 0 || what == 3;
+  const double s = mx ? block_max(v, sh) : block_sum(v, sh);
   if (threadIdx.x == 0 && threadIdx.y == 0)
     d.partials[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = s;
 }
@@ -1076,8 +1082,9 @@ __global__ void __launch_bounds__(RHS_BX *RHS_BY) k_reduce_part(TGDev d, int wha
 __global__ void __launch_bounds__(1024) k_reduce_final(TGDev d, int what, int npart) {
   __shared__ double sh[32];
   double s = 0.0;
-  for (int t = threadIdx.x; t < npart; t += blockDim.x) s = what == 0 ? fmax(s, d.partials[t]) : s + d.partials[t];
-  s = what == 0 ? block_max(s, sh) : block_sum(s, sh);
+  const bool mx = what == 0 || what == 3;
+  for (int t = threadIdx.x; t < npart; t += blockDim.x) s = mx ? fmax(s, d.partials[t]) : s + d.partials[t];
+  s = mx ? block_max(s, sh) : block_sum(s, sh);
   if (threadIdx.x == 0) d.scal[1] = s;
 }
 

@@ -156,6 +156,55 @@ class TGChannel:
     def nan_count(self):
         return int(self._reduce(_lib.R_NANCOUNT))
 
+    def cfl(self):
+        """CFLMM: CFL_tg (CFL_io + CFL_VISCOUS on an IO context), src/CFL.f90."""
+        return self._reduce(_lib.R_CFL)
+
+    def set_dt(self, dt):
+        """Change DT; the dt-dependent coefficient tables are rebuilt."""
+        self._chk(self.lib.chapsim_set_dt(self.h, dt))
+
+    # ------------------------------------------------------- statistics
+    STATS_LAYOUT = (("U1", 4), ("UP", 3), ("U2", 6), ("U3", 10), ("DVDL1", 9), ("DVDLP", 9), ("DVDL2", 81))
+
+    def pp_mean_zx(self, accumulate=False):
+        """PP_MEAN_ZX_FLOW_TG on the device (and PP_MEAN_T_TG when accumulate)."""
+        self._chk(self.lib.chapsim_stats(self.h, 1 if accumulate else 0))
+
+    def stats(self, which=0):
+        """(ny, 122) array of the xz (which=0) or time (which=1) averages and the sample count."""
+        a = np.empty((self.ny, _lib.STATS_NV))
+        n = ctypes.c_int64()
+        self._chk(self.lib.chapsim_get_stats(self.h, which, a.ctypes.data, a.size, ctypes.byref(n)))
+        return a, n.value
+
+    def stats_reset(self):
+        self._chk(self.lib.chapsim_stats_reset(self.h))
+
+    def monitor(self):
+        """The numbers of the PP_MONITOR_TG line (src/processing/PP_SCN_MONITOR.f90:138-242)
+        from the device statistics: U1 at the channel centre (xz, xzt), the normal
+        stresses and uv there, the skin friction on both walls, bulk and max of U1."""
+        xz, _ = self.stats(0)
+        xzt, _ = self.stats(1)
+        dyfi = self.mesh(2)
+        ren = self.cfg.ren
+        jc = self.ny // 2 - 1
+        mon = {"cflmm_dt": self.cfl() * self.cfg.dt, "dt": self.cfg.dt, "maxdiv": self.divgck_tg()}
+        for tag, s in (("xz", xz), ("xzt", xzt)):
+            mon[f"u_{tag}"], mon[f"v_{tag}"], mon[f"w_{tag}"] = s[jc, 0], s[jc, 1], s[jc, 2]
+            mon[f"uu_{tag}"] = s[jc, 7] - s[jc, 0] * s[jc, 0]
+            mon[f"uv_{tag}"] = s[jc, 8] - s[jc, 0] * s[jc, 1]
+            mon[f"vv_{tag}"] = s[jc, 10] - s[jc, 1] * s[jc, 1]
+            mon[f"ww_{tag}"] = s[jc, 12] - s[jc, 2] * s[jc, 2]
+            mon[f"cf_bottom_{tag}"] = s[0, 0] * dyfi[0] * 2.0 * 2.0 / ren
+            mon[f"cf_top_{tag}"] = s[-1, 0] * dyfi[-1] * 2.0 * 2.0 / ren
+        lz = self.cfg.lz
+        area = (1.0 / dyfi).sum() * lz
+        mon["u1mean"] = (xz[:, 0] / dyfi).sum() * lz / area
+        mon["u1maxx"] = np.abs(xz[:, 0]).max()
+        return mon
+
     # ------------------------------------------------------------- timing
     def phase_timing(self, enable):
         self._chk(self.lib.chapsim_phase_timing(self.h, 1 if enable else 0))

@@ -73,6 +73,8 @@ extern "C" {
 #define CHAPSIM_R_BULK 1   /* bulk velocity, BULK_VELOCITY_TG
                               (src/INITIAL_FL_FLD_TG.f90:122-149)                  */
 #define CHAPSIM_R_NANCOUNT 2 /* number of non-finite values in u, v, w, p          */
+#define CHAPSIM_R_CFL 7      /* CFLMM: TG CFL_tg (src/CFL.f90:1-40) on u, v, w; IO
+                                CFL_io on G plus CFL_VISCOUS (:42-133)            */
 
 /* Per-phase timer slots for chapsim_phase_times (milliseconds, accumulated). */
 #define CHAPSIM_PH_RHS 0     /* convection + RHS assembly (+ mass-flux sum)   */
@@ -167,8 +169,27 @@ int chapsim_pois3d(chapsim_ctx *ctx, int domain);
  * (src/VELO_CORRECTION.f90:19-105, src/PRESSURE_CORRECTION.f90:1-24). */
 int chapsim_velo_correction(chapsim_ctx *ctx, int domain, int ns);
 
-/* Device reductions (DIVGCK_tg, BULK_VELOCITY_TG); synchronises. */
+/* Device reductions (DIVGCK_tg, BULK_VELOCITY_TG, CFL); synchronises. */
 int chapsim_reduce(chapsim_ctx *ctx, int domain, int what, double *out);
+
+/* On-device flow statistics of a TG context.  chapsim_stats computes the
+ * xz-plane averages of PP_MEAN_ZX_FLOW_TG (src/processing/PP_MEAN_ZX.f90:1-294)
+ * for every y-row and, with accumulate != 0, folds them into the running time
+ * average of PP_MEAN_T_TG (src/processing/PP_MEAN_T.f90:322-370, asymptotic
+ * weights 1/N, (N-1)/N).  chapsim_get_stats copies ny * CHAPSIM_STATS_NV
+ * values (which = 0: xz average, 1: time average; row j-1 holds U1 (u, v, w,
+ * p), UP (3), U2 (11 12 13 22 23 33), U3 (111 112 113 122 123 133 222 223 233
+ * 333), DVDL1 (3x3 row-major), DVDLP (3x3), DVDL2 (9x9)) and the sample count.
+ * chapsim_stats_reset clears the time average (PP_TMEAN_INI_ZERO_TG). */
+#define CHAPSIM_STATS_NV 122
+int chapsim_stats(chapsim_ctx *ctx, int accumulate);
+int chapsim_get_stats(chapsim_ctx *ctx, int which, double *out, int64_t n, int64_t *nstatis);
+int chapsim_stats_reset(chapsim_ctx *ctx);
+
+/* Change the time step (DT, the variable of the adaptive step-size control
+ * SOLVE.f90:156-213 leaves commented out: DT = min(DT0, 5 DT, CFLGV/CFLMM)).
+ * Rebuilds every dt-dependent coefficient table; synchronises. */
+int chapsim_set_dt(chapsim_ctx *ctx, double dt);
 
 /* The context's CUDA stream (a cudaStream_t), for callers that time or order
  * work against it. */

@@ -799,6 +799,108 @@ double oracle_tg_divmax(const oracle_tg *o) {
   return dmax;
 }
 
+// CFL_tg (src/CFL.f90:1-40).
+double oracle_tg_cfl(const oracle_tg *o) {
+  double m = 0.0;
+  for (int k = 1; k <= o->nz; ++k)
+    for (int j = 1; j <= o->ny; ++j)
+      for (int i = 1; i <= o->nx; ++i) {
+        const double q = (std::fabs((Q(1, i, j, k) + Q(1, o->ip(i), j, k)) * o->dxi) +
+                          std::fabs((Q(2, i, j, k) + Q(2, i, j + 1, k)) * o->dyfi[j]) +
+                          std::fabs((Q(3, i, j, k) + Q(3, i, j, o->kp(k))) * o->dzi)) * 0.5;
+        m = std::fmax(m, q);
+      }
+  return m;
+}
+
+void oracle_tg_set_dt(oracle_tg *o, double dt) { o->dt = dt; }
+
+// PP_MEAN_ZX_FLOW_TG (src/processing/PP_MEAN_ZX.f90:1-294), channel branch:
+// per y-row U1 (4), UP (3), U2 (6), U3 (10), DVDL1 (9), DVDLP (9), DVDL2 (81),
+// scaled by VL1313 = 1/(nx nz) and the cell-centring factors.  out holds
+// ny * 122 values.
+void oracle_tg_stats(const oracle_tg *o, double *out) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  const double vl = 1.0 / (double)(nx * nz);
+  const double coe0 = vl, coe1 = vl * 0.5, coe2 = vl * (0.5 * 0.5), coe3 = vl * (0.5 * 0.5 * 0.5);
+  double cog1[3][3] = {{vl * o->dxi, vl * 0.25, vl * 0.25 * o->dzi},
+                       {vl * 0.25 * o->dxi, vl, vl * 0.25 * o->dzi},
+                       {vl * 0.25 * o->dxi, vl * 0.25, vl * o->dzi}};
+#pragma omp parallel for schedule(static) num_threads(oracle_get_threads())
+  for (int j = 1; j <= ny; ++j) {
+    double u1[4] = {0, 0, 0, 0}, up[3] = {0, 0, 0}, u2[6] = {0}, u3[10] = {0}, d1[3][3] = {{0}}, dp[3][3] = {{0}};
+    static thread_local double d2[9][9];
+    for (auto &r : d2)
+      for (double &x : r) x = 0.0;
+    const int jp = j + 1, jm = j - 1;
+    for (int i = 1; i <= nx; ++i) {
+      const int ip = o->ip(i), im = o->im(i);
+      for (int k = 1; k <= nz; ++k) {
+        const int kp = o->kp(k), km = o->km(k);
+        double U[3], Uip[3], Uim[3], Ujp[3], Ujm[3], Ukp[3], Ukm[3];
+        U[0] = Q(1, i, j, k) + Q(1, ip, j, k);
+        Ujp[0] = Q(1, i, jp, k) + Q(1, ip, jp, k);
+        Ujm[0] = Q(1, i, jm, k) + Q(1, ip, jm, k);
+        Ukp[0] = Q(1, i, j, kp) + Q(1, ip, j, kp);
+        Ukm[0] = Q(1, i, j, km) + Q(1, ip, j, km);
+        U[2] = Q(3, i, j, k) + Q(3, i, j, kp);
+        Uip[2] = Q(3, ip, j, k) + Q(3, ip, j, kp);
+        Uim[2] = Q(3, im, j, k) + Q(3, im, j, kp);
+        Ujp[2] = Q(3, i, jp, k) + Q(3, i, jp, kp);
+        Ujm[2] = Q(3, i, jm, k) + Q(3, i, jm, kp);
+        U[1] = Q(2, i, j, k) + Q(2, i, jp, k);
+        Uip[1] = Q(2, ip, j, k) + Q(2, ip, jp, k);
+        Uim[1] = Q(2, im, j, k) + Q(2, im, jp, k);
+        Ukp[1] = Q(2, i, j, kp) + Q(2, i, jp, kp);
+        Ukm[1] = Q(2, i, j, km) + Q(2, i, jp, km);
+        const double p = o->pr[o->id(i, j, k)];
+        for (int m = 0; m < 3; ++m) {
+          u1[m] += U[m];
+          up[m] += U[m] * p;
+        }
+        u1[3] += p;
+        int l = 0;
+        for (int m = 0; m < 3; ++m)
+          for (int n = m; n < 3; ++n) u2[l++] += U[m] * U[n];
+        l = 0;
+        for (int m = 0; m < 3; ++m)
+          for (int n = m; n < 3; ++n)
+            for (int h = n; h < 3; ++h) u3[l++] += U[m] * U[n] * U[h];
+        double D[3][3];
+        D[0][0] = Q(1, ip, j, k) - Q(1, i, j, k);
+        D[0][1] = (Ujp[0] - U[0]) * o->dyci[jp] + (U[0] - Ujm[0]) * o->dyci[j];
+        D[0][2] = Ukp[0] - Ukm[0];
+        D[1][0] = Uip[1] - Uim[1];
+        D[1][1] = (Q(2, i, jp, k) - Q(2, i, j, k)) * o->dyfi[j];
+        D[1][2] = Ukp[1] - Ukm[1];
+        D[2][0] = Uip[2] - Uim[2];
+        D[2][1] = (Ujp[2] - U[2]) * o->dyci[jp] + (U[2] - Ujm[2]) * o->dyci[j];
+        D[2][2] = Q(3, i, j, kp) - Q(3, i, j, k);
+        for (int m = 0; m < 3; ++m)
+          for (int n = 0; n < 3; ++n) {
+            d1[m][n] += D[m][n];
+            dp[m][n] += D[m][n] * p;
+          }
+        for (int a = 0; a < 9; ++a)
+          for (int b = 0; b < 9; ++b) d2[a][b] += D[a / 3][a % 3] * D[b / 3][b % 3];
+      }
+    }
+    double *r = out + (size_t)(j - 1) * 122;
+    int q = 0;
+    for (int m = 0; m < 3; ++m) r[q++] = u1[m] * coe1;
+    r[q++] = u1[3] * coe0;
+    for (int m = 0; m < 3; ++m) r[q++] = up[m] * coe1;
+    for (int m = 0; m < 6; ++m) r[q++] = u2[m] * coe2;
+    for (int m = 0; m < 10; ++m) r[q++] = u3[m] * coe3;
+    for (int m = 0; m < 3; ++m)
+      for (int n = 0; n < 3; ++n) r[q++] = d1[m][n] * cog1[m][n];
+    for (int m = 0; m < 3; ++m)
+      for (int n = 0; n < 3; ++n) r[q++] = dp[m][n] * cog1[m][n];
+    for (int a = 0; a < 9; ++a)
+      for (int b = 0; b < 9; ++b) r[q++] = d2[a][b] * (cog1[a / 3][a % 3] * cog1[b / 3][b % 3]);
+  }
+}
+
 double oracle_tg_bulk(const oracle_tg *o) {
   // BULK_VELOCITY_TG (src/INITIAL_FL_FLD_TG.f90:122-149).
   double s = 0.0;

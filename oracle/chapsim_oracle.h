@@ -125,6 +125,11 @@ double oracle_io_divmax(const oracle_io *o);   /* DIVGCK_io: max|div G + DrhoDtP
 double oracle_io_divmax_q(const oracle_io *o); /* max|div u| */
 double oracle_io_bulk(const oracle_io *o, int what); /* 0 BULK_VELOCITY_IO, 1 BULK_MASSFLUX_IO, 2 BULK_H_IO */
 int64_t oracle_io_bad_cells(const oracle_io *o);     /* table look-ups outside the table so far */
+double oracle_io_cfl(const oracle_io *o);            /* CFL_io + CFL_VISCOUS */
+void oracle_io_set_dt(oracle_io *o, double dt);
+double oracle_tg_cfl(const oracle_tg *o);            /* CFL_tg */
+void oracle_tg_set_dt(oracle_tg *o, double dt);
+void oracle_tg_stats(const oracle_tg *o, double *out); /* PP_MEAN_ZX_FLOW_TG, ny * 122 values */
 
 void oracle_set_threads(int n);
 int oracle_get_threads(void);

@@ -1089,4 +1089,23 @@ double oracle_io_bulk(const oracle_io *o, int what) {
 
 int64_t oracle_io_bad_cells(const oracle_io *o) { return o->bad; }
 
+// CFL_io + CFL_VISCOUS (src/CFL.f90:42-133), explicit scheme.
+double oracle_io_cfl(const oracle_io *o) {
+  double m = 0.0;
+  for (int k = 1; k <= o->nz; ++k)
+    for (int j = 1; j <= o->ny; ++j) {
+      const double vis = 2.0 * o->cvisc * (o->dxqi + o->dzqi + o->dyfi[j] * o->dyfi[j]);
+      for (int i = 1; i <= o->nx; ++i) {
+        double q = (std::fabs((FC(g, 1, i, j, k) + FC(g, 1, o->ip(i), j, k)) * o->dxi) +
+                    std::fabs((FC(g, 2, i, j, k) + FC(g, 2, i, j + 1, k)) * o->dyfi[j]) +
+                    std::fabs((FC(g, 3, i, j, k) + FC(g, 3, i, j, o->kp(k))) * o->dzi)) * 0.5;
+        q = q + vis;
+        m = std::fmax(m, q);
+      }
+    }
+  return m;
+}
+
+void oracle_io_set_dt(oracle_io *o, double dt) { o->dt = dt; }
+
 }  // extern "C"

@@ -64,6 +64,12 @@ def load(build=True):
     L.oracle_io_bad_cells.restype = ctypes.c_int64
     L.oracle_io_bad_cells.argtypes = [P]
     L.oracle_synth_table.argtypes = [I, P, P, P, P, P, P, P]
+    for f in ("oracle_tg_cfl", "oracle_io_cfl"):
+        getattr(L, f).restype = D
+        getattr(L, f).argtypes = [P]
+    for f in ("oracle_tg_set_dt", "oracle_io_set_dt"):
+        getattr(L, f).argtypes = [P, D]
+    L.oracle_tg_stats.argtypes = [P, P]
     L.oracle_set_threads.argtypes = [I]
     L.oracle_get_threads.restype = I
     _lib = L
@@ -134,6 +140,18 @@ class OracleTG:
 
     def pois_residual(self):
         return self.L.oracle_tg_pois_residual(self.h)
+
+    def cfl(self):
+        return self.L.oracle_tg_cfl(self.h)
+
+    def set_dt(self, dt):
+        self.L.oracle_tg_set_dt(self.h, dt)
+
+    def stats(self):
+        """PP_MEAN_ZX_FLOW_TG: array (ny, 122)."""
+        a = np.empty((self.ny, 122))
+        self.L.oracle_tg_stats(self.h, a.ctypes.data)
+        return a
 
 
 def set_threads(n):
@@ -227,3 +245,9 @@ class OracleIO:
 
     def bad_cells(self):
         return self.L.oracle_io_bad_cells(self.h)
+
+    def cfl(self):
+        return self.L.oracle_io_cfl(self.h)
+
+    def set_dt(self, dt):
+        self.L.oracle_io_set_dt(self.h, dt)
