@@ -116,6 +116,11 @@ SIGNATURES += [
     ("chapsim_stats", _I, [_P, _I]),
     ("chapsim_get_stats", _I, [_P, _I, _P, _I64, ctypes.POINTER(_I64)]),
     ("chapsim_stats_reset", _I, [_P]),
+    ("chapsim_write_instant", _I, [_P, ctypes.c_char_p, _I, _D]),
+    ("chapsim_read_instant", _I, [_P, ctypes.c_char_p, _D, ctypes.POINTER(_I), _DP]),
+    ("chapsim_instant_file_name", _I, [ctypes.c_char_p, _I, ctypes.c_char_p, _D, ctypes.c_char_p]),
+    ("chapsim_instant_file_write", _I, [ctypes.c_char_p, _I, _I, _I, _I, _D, _D, _D, _P]),
+    ("chapsim_instant_file_read", _I, [ctypes.c_char_p, _I, _I, _I, ctypes.POINTER(_I), _DP, _DP, _DP, _P]),
 ]
 STATS_NV = 122
 PROPS_TABLE, PROPS_MLP = 0, 1

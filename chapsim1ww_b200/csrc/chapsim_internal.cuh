@@ -183,6 +183,7 @@ int io_reduce(chapsim_ctx *c, int what, double *host_out);
 int io_correction(chapsim_ctx *c, int ns);
 int io_init_maps(chapsim_ctx *c);
 int io_refresh_msum(chapsim_ctx *c);
+int io_restart_fields(chapsim_ctx *c);
 // TG statistics (stats.cu)
 int stats_run(chapsim_ctx *c, int accumulate);
 int stats_get(chapsim_ctx *c, int which, double *host, int64_t n);

@@ -237,6 +237,36 @@ __global__ void k_io_eng_ghost(TGDev d, IODev io) {
   io.msum[c] = io.mu0[c] + M;
 }
 
+// THERM_PROP_UPDATE on the interior after a restart (h read from the file),
+// then mu0 = mu, rho0 = rho and mu0 + mu over every row (the ghost rows
+// already hold BC_WALL_ISOFLUX's values).
+__global__ void __launch_bounds__(IO_BX *IO_BY) k_io_props_only(TGDev d, IODev io) {
+  const int nx = d.nx, ny = d.ny;
+  const int i = blockIdx.x * IO_BX + threadIdx.x;
+  const int j = blockIdx.y * IO_BY + threadIdx.y;  // 0 .. ny+1
+  const int k = blockIdx.z;
+  if (i >= nx || j > ny + 1) return;
+  const int64_t c = i + d.sy * j + d.sz * k;
+  if (io.thermal && j >= 1 && j <= ny) {
+    const double h = io.h[c];
+    if (!(io.shortcuts && fabs(h) < 1.0e-10)) {
+      double T, D, M, K;
+      if (look_ht(io, h, T) && look_tprops(io, T, D, M, K)) {
+        io.T[c] = T;
+        io.mu[c] = M;
+        io.kap[c] = K;
+        io.D[c] = D;
+      } else {
+        atomicAdd(io.bad, 1ull);
+      }
+    }
+  }
+  const double mu = io.mu[c];
+  io.mu0[c] = mu;
+  io.D0[c] = io.D[c];
+  io.msum[c] = mu + mu;
+}
+
 // msum = mu0 + mu over the whole array (after the host replaces mu or mu0).
 __global__ void k_io_msum(IODev io, size_t n) {
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
@@ -1026,6 +1056,18 @@ int io_init_maps(chapsim_ctx *c) {
 
 int io_refresh_msum(chapsim_ctx *c) {
   k_io_msum<<<148 * 8, 256, 0, c->stream>>>(c->io, (size_t)c->d.sz * c->d.nz);
+  LAUNCHED();
+  return CHAPSIM_OK;
+}
+
+int io_restart_fields(chapsim_ctx *c) {
+  TGDev &d = c->d;
+  int rc;
+  if (c->io.thermal && (rc = io_thermal_bc(c))) return rc;
+  dim3 g2((d.nx + IO_BX - 1) / IO_BX, (d.ny + 2 + IO_BY - 1) / IO_BY, d.nz);
+  k_io_props_only<<<g2, dim3(IO_BX, IO_BY), 0, c->stream>>>(d, c->io);
+  LAUNCHED();
+  k_io_prep<<<cell_grid(d), dim3(IO_BX, IO_BY), 0, c->stream>>>(d, c->io, 0.0, 0.0, 1.0, c->io_cur, 0);
   LAUNCHED();
   return CHAPSIM_OK;
 }

@@ -164,6 +164,17 @@ class TGChannel:
         """Change DT; the dt-dependent coefficient tables are rebuilt."""
         self._chk(self.lib.chapsim_set_dt(self.h, dt))
 
+    # ------------------------------------------------------- instant files
+    def write_instant(self, directory, iteration, time):
+        """WRT_INSTANT_VARS_* into directory (a path prefix ending in '/')."""
+        self._chk(self.lib.chapsim_write_instant(self.h, directory.encode(), iteration, time))
+
+    def read_instant(self, directory, time):
+        """RESTART_INSTANT_VARS_* from directory; returns (iteration, time)."""
+        it, tm = ctypes.c_int(), ctypes.c_double()
+        self._chk(self.lib.chapsim_read_instant(self.h, directory.encode(), time, ctypes.byref(it), ctypes.byref(tm)))
+        return it.value, tm.value
+
     # ------------------------------------------------------- statistics
     STATS_LAYOUT = (("U1", 4), ("UP", 3), ("U2", 6), ("U3", 10), ("DVDL1", 9), ("DVDLP", 9), ("DVDL2", 81))
 

@@ -186,6 +186,29 @@ int chapsim_stats(chapsim_ctx *ctx, int accumulate);
 int chapsim_get_stats(chapsim_ctx *ctx, int which, double *out, int64_t n, int64_t *nstatis);
 int chapsim_stats_reset(chapsim_ctx *ctx);
 
+/* Instantaneous-field files in the reference's layout (WRT_INSTANT_VARS_TG /
+ * READ_3D_VARS, src/processing/WRT_VARS_TG.f90:1-91,
+ * src/processing/READ_INTP_3D_VARS.f90:1-84): one file per variable, 4 x
+ * int32 (nx, ny, nz, iteration), 3 x float64 (time, Re, dt), then the
+ * interior F(1:nx, 1:ny, 1:nz) in Fortran order, native byte order.  Names
+ * <dir>DNS_perixz_INSTANT_T<time, Fortran ES15.9>_<var>.D; var U, V, W, P
+ * (TG: Q_tg, PR_tg; IO: G_io, PR_io) and, thermal IO, T, D, E.
+ * chapsim_write_instant writes the context's state; chapsim_read_instant
+ * restarts from such files (RESTART_INSTANT_VARS_TG / _IO + FLOWSTART's wall
+ * conditions; TG: CONVH0 = 0; IO: RHOH = D E, wall ghosts, THERM_PROP_UPDATE,
+ * rho0 = rho, mu0 = mu, u = G / rho_stag, G0 = EXPLT0 = RHS_ENERGY0 = 0) and
+ * returns the file's iteration and time.  A mesh other than the context's is
+ * refused (the reference's interpolation, INTP_3D_VARS, is not built).  The
+ * *_file_* calls do the same on host arrays in the F(1:nx, 0:ny+1, 1:nz)
+ * layout (ghost rows untouched) and need no GPU. */
+int chapsim_write_instant(chapsim_ctx *ctx, const char *dir, int iteration, double time);
+int chapsim_read_instant(chapsim_ctx *ctx, const char *dir, double time, int *iteration, double *time_out);
+int chapsim_instant_file_name(char *buf, int buflen, const char *dir, double time, const char *var);
+int chapsim_instant_file_write(const char *path, int nx, int ny, int nz, int iteration, double time, double ren,
+                               double dt, const double *field);
+int chapsim_instant_file_read(const char *path, int nx, int ny, int nz, int *iteration, double *time, double *ren,
+                              double *dt, double *field);
+
 /* Change the time step (DT, the variable of the adaptive step-size control
  * SOLVE.f90:156-213 leaves commented out: DT = min(DT0, 5 DT, CFLGV/CFLMM)).
  * Rebuilds every dt-dependent coefficient table; synchronises. */
