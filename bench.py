@@ -1,22 +1,28 @@
-"""Benchmark of the CHAPSim TG RK3 step on B200 (libchapsim, sm_100a).
+"""Benchmark of the CHAPSim RK3 step on B200 (libchapsim, sm_100a).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload NAME] [--precision fp64|mixed]
 
-A "step" is one full RK3 time step (substeps NS = 1, 2, 3) of the workload's
-channel.  Metric: cell-steps/s = cells x steps / seconds.
+A "step" is one full RK3 time step (substeps NS = 1, 2, 3) of the workload.
+Metric: cell-steps/s = cells x steps / seconds.
 
-Default workload: the 256x192x256 TG channel of the coupled TG+IO
-configuration (Lx = 4 pi, Lz = 4 pi / 3, tanh stretching beta = 2,
-Re_b = 2800, dt = 1e-3, seed 1), synthetic seeded initial field.  With N > 1
-GPUs every rank advances its own independent channel (replicas, weak scaling,
-no data-path collective); timing is the max over ranks.
+Default workload (c1_tg_io): the two sections of the coupled TG + IO
+configuration advanced together every step: the TG channel 256x192x256
+(Lx = 4 pi, Lz = 4 pi / 3, tanh stretching beta = 2, Re_b = 2800, dt = 1e-3,
+seed 1) and the IO section 512x192x256 (Lx = 8 pi) with constant-property
+passive heat (rho = mu = k = cp = 1, T = h), wall heat flux 1, Pr 0.71,
+seed 1; the IO section runs x-periodic because the TG -> IO inlet coupling
+is not built.  Synthetic seeded initial fields.  With N > 1 GPUs every rank
+advances its own independent copy (replicas, weak scaling, no data-path
+collective); timing is the max over ranks.  Other workloads: the TG or IO
+section alone, the heated variable-property IO channel 384x192x192, the
+64-channel batch, the CPU-sized 64^3 TG channel.
 
 Arms:
   ours       libchapsim through the C ABI; `value` with the state resident in
-             HBM (CUDA-graph replay of the step), `e2e` through the public API
-             with host buffers (upload u, v, w, p from pinned memory, one step,
-             download u, v, w, p and max|div u| every step).
+             HBM (CUDA-graph replay of the steps), `e2e` through the public API
+             with host buffers (upload the state fields from pinned memory,
+             one step, download them and max|div| every step).
   reference  the reference algorithm's CPU path: the FP64 oracle port
              (OpenMP, all host threads) on the same workload, rank 0 only.
 """
@@ -43,6 +49,9 @@ WORKLOADS = {
     # variable-property heated IO channel, x-periodic, synthetic 4096-point table
     "io_384x192x192": dict(io=True, nx=384, ny=192, nz=192, lx=8 * math.pi, lz=4 * math.pi / 3, ren=2800.0,
                            dt=1e-3, seed=2, thermal=1, prt=0.71, qw=1.0, table="synthetic"),
+    # the two sections of the coupled TG + IO configuration advanced together
+    # each step (the IO section x-periodic: the TG -> IO inlet coupling is not built)
+    "c1_tg_io": dict(pair=True, tg="tg_256x192x256", io="io_512x192x256"),
     # IO section of the coupled configuration run x-periodic: constant-property
     # passive heat (rho = mu = k = cp = 1, T = h), wall heat flux 1, Pr 0.71
     "io_512x192x256": dict(io=True, nx=512, ny=192, nz=256, lx=8 * math.pi, lz=4 * math.pi / 3, ren=2800.0,
@@ -69,7 +78,7 @@ PHASE_KERNEL = {"rhs": "k_rhs_tma", "adix": "k_adixz_band", "adiz": "k_adixz_ban
 IO_PHASES = ["eng_rhs", "eng_props", "prep", "mom_rhs", "fftx", "fftz", "ysolve", "ifftz", "ifftx", "corr"]
 IO_VALUES_PER_CELL = {"eng_rhs": 13, "eng_props": 10, "prep": 12, "mom_rhs": 17, "fftx": 5, "corr": 9}
 IO_KERNEL = {"eng_rhs": "k_io_eng_rhs", "eng_props": "k_io_eng_props", "prep": "k_io_prep",
-             "mom_rhs": "k_io_rhs", "fftx": "k_fftx", "fftz": "k_fftz", "ysolve": "k_ysolve_line",
+             "mom_rhs": "k_io_rhs_tma", "fftx": "k_fftx", "fftz": "k_fftz", "ysolve": "k_ysolve_line",
              "ifftz": "k_fftz", "ifftx": "k_ifftx", "corr": "k_io_corr"}
 
 
@@ -367,6 +376,186 @@ def run_io(args, wl, ws, rank, local):
     return 0
 
 
+def run_pair(args, wl, ws, rank, local):
+    """TG and IO sections of the coupled configuration, one step of each per
+    step, on their own streams (allowed to overlap, joined before the end
+    event).  value = (TG cells + IO cells) x steps / time."""
+    import torch
+
+    import chapsim1ww_b200 as cs
+    from chapsim1ww_b200 import IOChannel, TGChannel
+
+    wt, wi = WORKLOADS[wl["tg"]], WORKLOADS[wl["io"]]
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    prec = cs.MIXED if args.precision == "mixed" else cs.FP64
+    tg = TGChannel(wt["nx"], wt["ny"], wt["nz"], lx=wt["lx"], lz=wt["lz"], ren=wt["ren"], dt=wt["dt"],
+                   precision=prec, device=local)
+    io = IOChannel(wi["nx"], wi["ny"], wi["nz"], lx=wi["lx"], lz=wi["lz"], ren=wi["ren"], dt=wi["dt"],
+                   thermal=wi["thermal"], prt=wi["prt"], qw=(wi["qw"], wi["qw"]), table=io_table(wi["table"]),
+                   device=local)
+    tg.random_fl_fld_tg(wt["seed"] + rank, 0.1, project=True)
+    io.random_fl_theml_fld_io(wi["seed"] + rank, 0.1)
+    ct, ci = wt["nx"] * wt["ny"] * wt["nz"], wi["nx"] * wi["ny"] * wi["nz"]
+    st = torch.cuda.ExternalStream(tg.stream(), device=local)
+    si = torch.cuda.ExternalStream(io.stream(), device=local)
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    def max_over_ranks(x):
+        if pg is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(fn, steps):
+        e0, ej, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(st)
+        si.wait_event(e0)
+        fn(steps)
+        ej.record(st)
+        si.wait_event(ej)
+        e1.record(si)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    def both(n):
+        tg.step(n)
+        io.step(n)
+
+    both(args.warmup)
+    tg.sync()
+    io.sync()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    n0 = tg.launch_count() + io.launch_count()
+    ms = max_over_ranks(timed(both, args.steps))
+    torch.cuda.synchronize()
+    barrier()
+    launches = tg.launch_count() + io.launch_count() - n0
+    clk = clocks.stop()
+    cells = ct + ci
+    value = cells * ws * args.steps / (ms / 1000.0)
+    ms_tg = timed(tg.step, args.steps) / args.steps
+    ms_io = timed(io.step, args.steps) / args.steps
+
+    # per-phase kernel times of both sections
+    nph = max(1, min(args.steps, 10))
+    tg.phase_timing(True)
+    tg.phase_reset()
+    tg.step(nph)
+    ph_t, n_t = tg.phase_times()
+    tg.phase_timing(False)
+    io.phase_timing(True)
+    io.phase_reset()
+    io.step(nph)
+    ph_i, n_i = io.phase_times()
+    io.phase_timing(False)
+    per_tg = {k: v / max(n_t, 1) for k, v in ph_t.items()}
+    per_io = {IO_PHASES[q]: v / max(n_i, 1) for q, v in enumerate(ph_i.values())}
+    cand = [("tg", k, v) for k, v in per_tg.items()] + [("io", k, v) for k, v in per_io.items()]
+    sec, dom, dom_ms = max(cand, key=lambda x: x[2])
+    peak, peak_kind = measured_peak()
+    if sec == "tg":
+        bytes_dom = phase_bytes(dom, wt["nx"], wt["ny"], wt["nz"])
+        kern = PHASE_KERNEL[dom]
+        traffic = load_traffic(wl["tg"], kern)
+    else:
+        bytes_dom = io_phase_bytes(dom, wi["nx"], wi["ny"], wi["nz"])
+        kern = IO_KERNEL[dom]
+        traffic = load_traffic(wl["io"], kern)
+    achieved = bytes_dom / (dom_ms / 1000.0) / 1e9
+    step_bytes = 3 * (sum(phase_bytes(p, wt["nx"], wt["ny"], wt["nz"]) for p in per_tg) +
+                      sum(io_phase_bytes(p, wi["nx"], wi["ny"], wi["nz"]) for p in IO_PHASES))
+
+    # end to end through the C ABI with host buffers (both sections)
+    tg_names, io_names = ("u", "v", "w", "p"), ("u", "v", "w", "p", "gx", "gy", "gz", "rhoh")
+    host_t = {n: torch.empty(tg.shape, dtype=torch.float64, pin_memory=True).numpy() for n in tg_names}
+    host_i = {n: torch.empty(io.shape, dtype=torch.float64, pin_memory=True).numpy() for n in io_names}
+    for n in tg_names:
+        tg.get_field(n, out=host_t[n])
+    for n in io_names:
+        io.get_field(n, out=host_i[n])
+    barrier()
+    torch.cuda.synchronize()
+    e2e_steps = max(1, min(args.steps, 10))
+
+    def e2e(steps):
+        for _ in range(steps):
+            for n in tg_names:
+                tg.set_field(n, host_t[n])
+            for n in io_names:
+                io.set_field(n, host_i[n])
+            tg.step(1)
+            io.step(1)
+            for n in tg_names:
+                tg.get_field(n, out=host_t[n])
+            for n in io_names:
+                io.get_field(n, out=host_i[n])
+            _ = tg.divgck_tg() + io.divgck_io()
+
+    ms_e2e = max_over_ranks(timed(e2e, e2e_steps))
+    e2e_value = cells * ws * e2e_steps / (ms_e2e / 1000.0)
+    nbytes = (len(tg_names) * tg.n + len(io_names) * io.n) * 8
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            v1, t1, cores = cpu_baseline_oracle(wt, args.cpu_steps)
+            v2, t2, _ = cpu_baseline_io(wi, args.cpu_steps)
+            v = (ct + ci) * args.cpu_steps / (t1 + t2)
+            cpu = {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
+                   "sample": f"{args.cpu_steps} full RK3 steps of each section after init (TG {t1:.1f} s, IO "
+                             f"{t2:.1f} s), FP64 oracle port, OpenMP {cores} threads"}
+        except Exception as ex:
+            cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if prec == cs.FP64 else "f64 state / f32 temporaries (TG)",
+            "data": "synthetic (seeded splitmix64 velocity, NS=0 projection; IO h = 0 with table properties)",
+            "config": {"workload": args.workload,
+                       "tg": {k: wt[k] for k in ("nx", "ny", "nz", "ren", "dt")},
+                       "io": {**{k: wi[k] for k in ("nx", "ny", "nz", "ren", "dt", "prt")},
+                              "table": wi["table"], "wall_heat_flux": wi["qw"], "x": "periodic (inlet coupling not built)"},
+                       "cells": cells, "precision": args.precision,
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU, two streams",
+                       "l2": "working set (>4 GB) larger than the 126 MB L2"},
+            "sections_ms_per_step": {"tg": ms_tg, "io": ms_io, "both": ms / args.steps},
+            "max_div_u_tg": tg.divgck_tg(), "max_div_g_plus_drho_io": io.divgck_io(),
+            "gpu_launches": launches,
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes + 16, "steps": e2e_steps},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "kernel": kern, "phase": f"{sec}:{dom}",
+                         "algorithmic_bytes_per_launch": bytes_dom, "avg_launch_ms": dom_ms,
+                         "peak_source": peak_kind},
+            "phases_ms_per_launch": {"tg": per_tg, "io": per_io},
+            "step_roofline": {"algorithmic_bytes_per_step": step_bytes,
+                              "achieved_gbs": step_bytes / (ms / args.steps / 1000.0) / 1e9,
+                              "frac": step_bytes / (ms / args.steps / 1000.0) / 1e9 / peak},
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    tg.close()
+    io.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
 def cpu_baseline_oracle(wl, steps):
     """FP64 oracle port on the host cores: init + NS=0, then `steps` timed steps."""
     from oracle.pyoracle import OracleTG, get_threads
@@ -380,9 +569,50 @@ def cpu_baseline_oracle(wl, steps):
     return cells * steps / t, t, get_threads()
 
 
+def run_reference_pair(args, wl, ws):
+    """Both sections with the oracle port, at most 8 timed steps (each a full
+    step of both sections) after at most 1 warm-up step."""
+    from oracle.pyoracle import OracleIO, OracleTG, get_threads
+    wt, wi = WORKLOADS[wl["tg"]], WORKLOADS[wl["io"]]
+    ot = OracleTG(wt["nx"], wt["ny"], wt["nz"], lx=wt["lx"], lz=wt["lz"], ren=wt["ren"], dt=wt["dt"])
+    ot.init_random(wt["seed"], 0.1)
+    ot.substep(0)
+    oi = OracleIO(wi["nx"], wi["ny"], wi["nz"], lx=wi["lx"], lz=wi["lz"], ren=wi["ren"], dt=wi["dt"],
+                  thermal=wi["thermal"], prt=wi["prt"], qw=(wi["qw"], wi["qw"]), table=io_table(wi["table"]))
+    oi.init_random(wi["seed"], 0.1)
+    nw, nt = min(args.warmup, 1), min(args.steps, 8)
+    for _ in range(nw):
+        ot.step(1)
+        oi.step(1)
+    t0 = time.perf_counter()
+    for _ in range(nt):
+        ot.step(1)
+        oi.step(1)
+    t = time.perf_counter() - t0
+    cells = wt["nx"] * wt["ny"] * wt["nz"] + wi["nx"] * wi["ny"] * wi["nz"]
+    v = cells * nt / t
+    cores = get_threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * t / nt, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded splitmix64 field)",
+        "config": {"workload": args.workload, "tg": {k: wt[k] for k in ("nx", "ny", "nz", "ren", "dt")},
+                   "io": {k: wi[k] for k in ("nx", "ny", "nz", "ren", "dt", "prt")}, "parallelism": "host threads"},
+        "cpu_baseline": {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
+                         "sample": f"{nt} timed full steps of both sections after {nw} warm-up step(s) (capped at "
+                                   f"8 so the run stays within minutes), FP64 oracle (restatement of the Fortran "
+                                   f"path), OpenMP {cores} threads"},
+        "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference(args, wl, ws, rank):
     if rank != 0:
         return 0
+    if wl.get("pair"):
+        return run_reference_pair(args, wl, ws)
     from oracle.pyoracle import OracleIO, OracleTG, get_threads
     if wl.get("io"):
         o = OracleIO(wl["nx"], wl["ny"], wl["nz"], lx=wl["lx"], lz=wl["lz"], ren=wl["ren"], dt=wl["dt"],
@@ -635,7 +865,7 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="tg_256x192x256")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c1_tg_io")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -653,6 +883,8 @@ def main():
         return run_reference(args, wl, ws, rank)
     if wl.get("batch"):
         return run_batch(args, wl, ws, rank, local)
+    if wl.get("pair"):
+        return run_pair(args, wl, ws, rank, local)
     if wl.get("io"):
         return run_io(args, wl, ws, rank, local)
     return run_ours(args, wl, ws, rank, local)
