@@ -1201,11 +1201,14 @@ int chapsim_phase_reset(chapsim_ctx *ctx) {
 int chapsim_set_tuning(chapsim_ctx *ctx, int rhs_nzc, int fft_lb) {
   if (!ctx || rhs_nzc < 1 || fft_lb < 0 || fft_lb > 64 || (fft_lb & 1)) return CHAPSIM_ERR_ARG;
   ctx->rhs_nzc = rhs_nzc;
+  ctx->io_nzc = rhs_nzc;  // the IO momentum RHS marches the same way
   ctx->fft_lb = fft_lb;
   if (ctx->step_graph) {
     cudaGraphExecDestroy(ctx->step_graph);
     ctx->step_graph = nullptr;
   }
+  for (auto &g : ctx->io_graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   return CHAPSIM_OK;
 }
 

@@ -541,6 +541,7 @@ struct IoMaps {
   CUtensorMap m[14];  // u, v, w, p, msum, g[0][0..2], g[1][0..2], EXPLT0[0..2]
 };
 
+template <bool TH>
 __global__ void __launch_bounds__(IO_BX *IO_BY, 2)
 k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam, double roh, double alp, int cur,
              int nzc) {
@@ -550,7 +551,7 @@ k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam,
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + 4 * IT_SLOT + 2 * IT_ESLOT);
   uint64_t *ebar = bar + 4;
   __shared__ double red[IO_BX * IO_BY / 32];
-  __shared__ double ycoef[IO_BY][8];
+  __shared__ double ycoef[IO_BY][9];
   const int nx = d.nx, ny = d.ny, nz = d.nz;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + IO_BX * ty;
   const int x0 = blockIdx.x * IO_BX, j0 = 1 + blockIdx.y * IO_BY;
@@ -569,8 +570,8 @@ k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam,
     for (int q = 0; q < 6; ++q) mbar_init(&bar[q], 1);
     fence_mbar_init();
   }
-  if (tid < IO_BY * 8) {
-    const int r = tid >> 3, q = tid & 7, jr = j0 + r;
+  if (tid < IO_BY * 9) {
+    const int r = tid / 9, q = tid - 9 * r, jr = j0 + r;
     double v = 0.0;
     if (jr <= ny) {
       switch (q) {
@@ -582,6 +583,7 @@ k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam,
         case 5: v = d.dyci[jr]; break;
         case 6: v = d.dyci[jr + 1]; break;
         case 7: v = d.dyfi[jr - 1]; break;
+        case 8: v = 1.0 / d.dyfi[jr]; break;
       }
     }
     ycoef[r][q] = v;
@@ -632,7 +634,7 @@ k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam,
   const double dxi = d.dxi, dzi = d.dzi, cv = d.cvisc, dt = d.dt;
   const double *yc = ycoef[ty];
   const int xx = tx + 2, yy = ty + 1;
-  const bool th = io.thermal != 0;
+  constexpr bool th = TH;
   for (int k = kbeg; k < kend; ++k) {
     if (tid == 0) {
       fence_proxy_async();
@@ -681,7 +683,7 @@ k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam,
       // DIVG_U_io at (dx, dy) of plane S (its z-plus plane Sn), row jj
       auto divu = [&](const double *S, const double *Sn, int dx, int dy, double dyf) {
         return ((A(S, F_U, dx + 1, dy) - A(S, F_U, dx, dy)) * dxi + (A(S, F_V, dx, dy + 1) - A(S, F_V, dx, dy)) * dyf +
-                (A(Sn, F_W, dx, dy) - A(S, F_W, dx, dy)) * dzi) / 3.0;
+                (A(Sn, F_W, dx, dy) - A(S, F_W, dx, dy)) * dzi) * (1.0 / 3.0);
       };
       const int64_t sy = d.sy, c = i + sy * j + d.sz * k;
       const int64_t oxm = (i == 0 ? nx - 1 : i - 1) - i, ozm = d.sz * ((k == 0 ? nz - 1 : k - 1) - k);
@@ -727,7 +729,7 @@ k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam,
           const double rs = th ? (io.D[c] + io.D[c + oxm] + io.D0[c] + io.D0[c + oxm]) * 0.5 * 0.5 : 1.0;
           r += rs * (alp * dt * io.f_a);
         }
-        part += r / dyfj;
+        part += r * yc[8];  // RHS_x / DYFI
         io.g[1 - cur][0][c] = A(Sc, F_GX, 0, 0) + r;
       }
       // ---------------- y (rows 2..ny)
@@ -993,7 +995,10 @@ int io_mom(chapsim_ctx *c, int ns, bool prep) {
     IoMaps maps;
     memcpy(maps.m, c->io_maps, sizeof(maps.m));
     dim3 g2(grid.x, grid.y, (d.nz + c->io_nzc - 1) / c->io_nzc);
-    k_io_rhs_tma<<<g2, blk, IT_SMEM, c->stream>>>(maps, d, io, sp.gam, sp.roh, sp.alp, cur, c->io_nzc);
+    if (io.thermal)
+      k_io_rhs_tma<true><<<g2, blk, IT_SMEM, c->stream>>>(maps, d, io, sp.gam, sp.roh, sp.alp, cur, c->io_nzc);
+    else
+      k_io_rhs_tma<false><<<g2, blk, IT_SMEM, c->stream>>>(maps, d, io, sp.gam, sp.roh, sp.alp, cur, c->io_nzc);
     npart = (int)(g2.x * g2.y * g2.z);
   } else {
     k_io_rhs<<<grid, blk, 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, cur);
@@ -1045,11 +1050,12 @@ int io_init_maps(chapsim_ctx *c) {
   int dev = 0, optin = 0;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  cudaFuncAttributes fa;
-  CK(cudaFuncGetAttributes(&fa, (const void *)k_io_rhs_tma));
-  if ((size_t)optin < IT_SMEM + fa.sharedSizeBytes) return CHAPSIM_OK;
-  CK(cudaFuncSetAttribute((const void *)k_io_rhs_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                          optin - (int)fa.sharedSizeBytes));
+  for (const void *fn : {(const void *)k_io_rhs_tma<true>, (const void *)k_io_rhs_tma<false>}) {
+    cudaFuncAttributes fa;
+    CK(cudaFuncGetAttributes(&fa, fn));
+    if ((size_t)optin < IT_SMEM + fa.sharedSizeBytes) return CHAPSIM_OK;
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes));
+  }
   c->use_tma_io = true;
   return CHAPSIM_OK;
 }

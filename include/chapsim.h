@@ -226,7 +226,8 @@ int chapsim_phase_times(chapsim_ctx *ctx, double *ms, int n, int64_t *substeps);
 int chapsim_phase_reset(chapsim_ctx *ctx);
 
 /* Launch-shape tuning of one context: z planes per block of the RHS kernel
- * (rhs_nzc) and rows per block of the x transforms (fft_lb, 0 = default).
+ * (rhs_nzc; on an IO context the momentum RHS) and rows per block of the x
+ * transforms (fft_lb, 0 = default).
  * Results do not depend on fft_lb; rhs_nzc changes only the block order of
  * the mass-flux sum (round-off level). */
 int chapsim_set_tuning(chapsim_ctx *ctx, int rhs_nzc, int fft_lb);
