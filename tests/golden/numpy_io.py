@@ -1,0 +1,399 @@
+"""Independent numpy restatement of CHAPSim's IO-section RK3 substep.
+
+Test infrastructure only: a second implementation of the x-periodic IO
+section, written to cross-check the C++ oracle.  It differs from the oracle
+in every non-trivial step: the stencils are whole-array shifts, the FISHPACK
+Poisson solve (real RFFTF/RFFTB transforms and a TRID0 sweep per mode in the
+reference) is done with complex numpy FFTs in x and z and scipy's banded LU
+per (kx, kz) mode, the table splines are built and evaluated with numpy
+(searchsorted), and the synthetic property table is integrated with numpy.
+
+Arrays are numpy views of the Fortran layout F(1:nx, 0:ny+1, 1:nz): shape
+(nz, ny+2, nx), so a[k-1, j, i-1] is F(i, j, k).
+
+Reference files restated (paths relative to the CHAPSim1WW project root):
+src/SOLVERRK3_ENG_IO.f90:1-77, src/RHS_ENERGY_EXPLICIT.f90:1-150,
+src/THERM_PROP_UPDATE.f90:2-291, src/Flow_State.f90:963-990,1015-1070,
+1693-1787, src/BC_WALL.f90:522-627, src/MASSFLUX_CALC_IO.f90:1-311,
+src/SOLVERRK3_MOM_IO.f90:1-168, src/CONVECTION_X.f90:77-176,
+src/CONVECTION_Y.f90:125-230, src/CONVECTION_Z.f90:113-200,
+src/DIVG.f90:58-259, src/VISCOUS_X_EXPLICIT_io.f90:1-112,
+src/VISCOUS_Y_EXPLICIT_io.f90 and src/VISCOUS_Z_EXPLICIT_io.f90 (channel
+branches), src/RHS_MOM_EXPLICIT_io.f90:1-297,
+src/possion3d_fishpack_reform.f90:29-547, src/PRESSURE_CORRECTION.f90:86-122,
+src/VELO_CORRECTION.f90:107-185, src/INITIAL_FL_THEML_FLD_io.f90:133-172,
+352-381,481-560,653-682.
+
+The decisions shared with the oracle and the library: the Poisson mean mode
+takes phi(ny) = 0; the reference-state shortcuts of the table look-ups are
+off; the initial thermal state is the table at h = 0; the initial velocity is
+the counter-based TG recipe scaled to unit bulk mass flux.
+"""
+import numpy as np
+from scipy.linalg import solve_banded
+
+from numpy_tg import TALP, TGAM, TROH, TG
+
+
+def fmm_spline(x, y):
+    """CUBIC_SPLINE (Forsythe, Malcolm & Moler): coefficients b, c, d."""
+    n = len(x)
+    b, c, d = np.zeros(n), np.zeros(n), np.zeros(n)
+    d[0] = x[1] - x[0]
+    c[1] = (y[1] - y[0]) / d[0]
+    for i in range(1, n - 1):
+        d[i] = x[i + 1] - x[i]
+        b[i] = 2.0 * (d[i - 1] + d[i])
+        c[i + 1] = (y[i + 1] - y[i]) / d[i]
+        c[i] = c[i + 1] - c[i]
+    # end conditions from third divided differences
+    b[0], b[-1] = -d[0], -d[n - 2]
+    c[0] = c[2] / (x[3] - x[1]) - c[1] / (x[2] - x[0])
+    c[-1] = c[n - 2] / (x[n - 1] - x[n - 3]) - c[n - 3] / (x[n - 2] - x[n - 4])
+    c[0] = c[0] * d[0] * d[0] / (x[3] - x[0])
+    c[-1] = -c[-1] * d[n - 2] * d[n - 2] / (x[n - 1] - x[n - 4])
+    for i in range(1, n):
+        t = d[i - 1] / b[i - 1]
+        b[i] -= t * d[i - 1]
+        c[i] -= t * c[i - 1]
+    c[-1] /= b[-1]
+    for i in range(n - 2, -1, -1):
+        c[i] = (c[i] - d[i] * c[i + 1]) / b[i]
+    b[-1] = (y[-1] - y[-2]) / d[-2] + d[-2] * (c[-2] + 2.0 * c[-1])
+    b[:-1] = (y[1:] - y[:-1]) / d[:-1] - d[:-1] * (c[1:] + 2.0 * c[:-1])
+    d[:-1] = (c[1:] - c[:-1]) / d[:-1]
+    c *= 3.0
+    d[-1] = d[-2]
+    return b, c, d
+
+
+class Spline:
+    """NIST_SLEVAL: cubic on the bracketing interval; outside the table is an error."""
+
+    def __init__(self, x, y):
+        self.x, self.y = np.asarray(x, float), np.asarray(y, float)
+        self.b, self.c, self.d = fmm_spline(self.x, self.y)
+
+    def __call__(self, u):
+        u = np.asarray(u, float)
+        if not np.all((u > self.x[0]) & (u < self.x[-1])):
+            raise ValueError("table look-up outside the table")
+        i = np.searchsorted(self.x, u, side="right") - 1
+        dx = u - self.x[i]
+        return self.y[i] + dx * (self.b[i] + dx * (self.c[i] + dx * self.d[i]))
+
+
+def synth_table(n=4096):
+    """Synthetic table of the heated IO configuration: h in [-1, 1],
+    cp = 1 + 8 exp(-(h/0.1)^2), T = int_{-1}^h dh/cp (composite Simpson,
+    64 panels per table interval), rho = 1/(1+2T), mu = k = rho^-1/2."""
+    H = -1.0 + 2.0 * np.arange(n) / (n - 1)
+    m = 64
+    wts = np.where(np.arange(m + 1) % 2 == 1, 4.0, 2.0)
+    wts[0] = wts[-1] = 1.0
+    hh = (H[1:] - H[:-1]) / m
+    pts = H[:-1, None] + np.arange(m + 1)[None, :] * hh[:, None]
+    pts[:, -1] = H[1:]
+    seg = (wts[None, :] / (1.0 + 8.0 * np.exp(-(pts / 0.1) ** 2))).sum(axis=1) * hh / 3.0
+    T = np.concatenate([[0.0], np.cumsum(seg)])
+    D = 1.0 / (1.0 + 2.0 * T)
+    M = 1.0 / np.sqrt(D)
+    return H, T, D, M, M.copy()
+
+
+class IO(TG):
+    """x-periodic IO section (explicit viscous scheme, constant mass flux);
+    the y mesh and the Poisson y-operator are the TG restatement's."""
+
+    def __init__(self, nx, ny, nz, lx, lz, str2=2.0, istr2=1, ren=2800.0, dt=1e-3, thermal=0, prt=0.71,
+                 qw=(1.0, 1.0), table=None):
+        super().__init__(nx, ny, nz, lx, lz, str2=str2, istr2=istr2, ren=ren, dt=dt)
+        self.thermal, self.qw = thermal, qw
+        self.cvisc, self.cthecd = 1.0 / ren, 1.0 / ren / prt
+        shape = (nz, ny + 2, nx)
+        z = lambda: np.zeros(shape)
+        self.g = {c: z() for c in (1, 2, 3)}
+        self.g0 = {c: z() for c in (1, 2, 3)}
+        self.ex0 = {c: z() for c in (1, 2, 3)}
+        self.drho, self.rhoh, self.h, self.rhse0 = z(), z(), z(), z()
+        self.T, self.D, self.D0, self.mu, self.mu0, self.k = (np.ones(shape) for _ in range(6))
+        if thermal:
+            H, Tt, D, M, K = (np.asarray(c, float) for c in (table if table is not None else synth_table())[:5])
+            self.ht, self.td, self.tm, self.tk = Spline(H, Tt), Spline(Tt, D), Spline(Tt, M), Spline(Tt, K)
+            n = len(H)
+            hs = H[0] + np.arange(1, 3 * n) * (H[-1] - H[0]) / (3 * n)
+            self.rhohmax = max(-1e-14, float(np.max(Spline(H, D)(hs) * hs)))
+
+    # ---------------------------------------------------------- helpers
+    def X(self, a, di=0, dj=0, dk=0):
+        """a(i+di, j+dj, k+dk) over the interior rows j = 1..ny (periodic i, k)."""
+        b = np.roll(a, shift=(-dk, -di), axis=(0, 2)) if (di or dk) else a
+        return b[:, 1 + dj:self.ny + 1 + dj, :]
+
+    def row(self, v, dj=0):
+        return v[1 + dj:self.ny + 1 + dj][None, :, None]
+
+    def interior(self, a, val):
+        a[:, 1:self.ny + 1, :] = val
+
+    def bc_vec(self, f):
+        """BC_WALL_Q / BC_WALL_G: u, w ghosts 0; v = 0 on and beyond the walls."""
+        ny = self.ny
+        f[1][:, 0, :] = 0.0; f[3][:, 0, :] = 0.0; f[2][:, 1, :] = 0.0; f[2][:, 0, :] = 0.0
+        f[1][:, ny + 1, :] = 0.0; f[3][:, ny + 1, :] = 0.0; f[2][:, ny + 1, :] = 0.0
+
+    def bulk_of(self, a):
+        return np.sum(a[:, 1:self.ny + 1] / self.row(self.dyfi)) / self.dzi / (self.area * self.nx)
+
+    def div(self, G):
+        X = self.X
+        return ((X(G[1], 1) - X(G[1])) * self.dxi + (X(G[2], 0, 1) - X(G[2])) * self.row(self.dyfi) +
+                (X(G[3], 0, 0, 1) - X(G[3])) * self.dzi)
+
+    # ---------------------------------------------------------- staggered rho, mu
+    def rho_stg(self):
+        """DENSITY_Staggered on the u, v, w faces (rows 1..ny)."""
+        if not self.thermal:
+            return 1.0, 1.0, 1.0
+        X, D, D0 = self.X, self.D, self.D0
+        rx = (X(D) + X(D, -1) + X(D0) + X(D0, -1)) * 0.25
+        rz = (X(D) + X(D, 0, 0, -1) + X(D0) + X(D0, 0, 0, -1)) * 0.25
+        ry = (self.row(self.wff) * (X(D) + X(D0)) + self.row(self.wfb) * (X(D, 0, -1) + X(D0, 0, -1))) * 0.5
+        return rx, ry, rz
+
+    def mu_stg(self):
+        """MU_Staggered: the xy-edge (1), xz-edge (2) and yz-edge (3) viscosities,
+        rows 1..ny+1 of 1 and 3 (walls from the ghost cells), rows 1..ny of 2."""
+        ny = self.ny
+        m, m0 = self.mu, self.mu0
+        xm = lambda a: np.roll(a, 1, axis=2)
+        zm = lambda a: np.roll(a, 1, axis=0)
+        s1, s2, s3 = np.zeros(m.shape), np.zeros(m.shape), np.zeros(m.shape)
+        ex = m + xm(m) + m0 + xm(m0)
+        ez = zm(m) + m + zm(m0) + m0
+        wf, wb = self.wff[2:ny + 1][None, :, None], self.wfb[2:ny + 1][None, :, None]
+        s1[:, 2:ny + 1] = (ex[:, 2:ny + 1] * wf + ex[:, 1:ny] * wb) * 0.25
+        s3[:, 2:ny + 1] = (ez[:, 2:ny + 1] * wf + ez[:, 1:ny] * wb) * 0.25
+        s2[:, 1:ny + 1] = (m + xm(m) + m0 + xm(m0) + zm(m) + zm(xm(m)) + zm(m0) + zm(xm(m0)))[:, 1:ny + 1] * 0.125
+        for s in (s1, s3):
+            s[:, 1] = 0.5 * (m0[:, 0] + m[:, 0])
+            s[:, ny + 1] = 0.5 * (m0[:, ny + 1] + m[:, ny + 1])
+        return s1, s2, s3
+
+    # ---------------------------------------------------------- energy
+    def table_props(self, h):
+        T = self.ht(h)
+        return T, self.td(T), self.tm(T), self.tk(T)
+
+    def wall_thermal(self):
+        """BC_WALL_ISOFLUX: ghost enthalpy extrapolated, ghost properties from the table."""
+        ny, h = self.ny, self.h
+        hb = 2.0 * h[:, 1] - self.wff[2] * h[:, 2] - self.wfb[2] * h[:, 1]
+        ht = 2.0 * h[:, ny] - self.wff[ny] * h[:, ny] - self.wfb[ny] * h[:, ny - 1]
+        for j, hg in ((0, hb), (ny + 1, ht)):
+            T, D, M, K = self.table_props(hg)
+            self.h[:, j], self.T[:, j], self.D[:, j], self.mu[:, j], self.k[:, j] = hg, T, D, M, K
+            self.rhoh[:, j] = hg * D
+
+    def eng(self, ns):
+        """SOLVERRK3_ENG_IO: RHS_ENERGY_EXPLICIT, the RK3 update with the RHOHmax
+        limiter, ENTHALPY/DENSITY_UPDATE, THERM_PROP_UPDATE, wall ghosts."""
+        ny, X, row = self.ny, self.X, self.row
+        self.mu0 = self.mu.copy()
+        self.D0 = self.D.copy()
+        H, T, K, G, G0 = self.h, self.T, self.k, self.g, self.g0
+        wff, wfb, wffp, wfbp = row(self.wff), row(self.wfb), row(self.wff, 1), row(self.wfb, 1)
+        dxr = ((X(H, 1) + X(H)) * (X(G0[1], 1) + X(G[1], 1)) - (X(H) + X(H, -1)) * (X(G0[1]) + X(G[1]))) * (self.dxi * 0.25)
+        dyr = ((wffp * X(H, 0, 1) + wfbp * X(H)) * (X(G0[2], 0, 1) + X(G[2], 0, 1)) -
+               (wff * X(H) + wfb * X(H, 0, -1)) * (X(G0[2]) + X(G[2]))) * (row(self.dyfi) * 0.5)
+        dzr = ((X(H, 0, 0, 1) + X(H)) * (X(G0[3], 0, 0, 1) + X(G[3], 0, 0, 1)) -
+               (X(H) + X(H, 0, 0, -1)) * (X(G0[3]) + X(G[3]))) * (self.dzi * 0.25)
+        dxk = ((X(K, 1) + X(K)) * (X(T, 1) - X(T)) - (X(K) + X(K, -1)) * (X(T) - X(T, -1))) * (self.dxi ** 2 * 0.5 * self.cthecd)
+        c_up = self.dyci[2:ny + 2].copy()
+        c_dn = self.dyci[1:ny + 1].copy()
+        c_up[-1] = 1.0
+        c_dn[0] = 1.0
+        k_up = (wffp * X(K, 0, 1) + wfbp * X(K)) * (X(T, 0, 1) - X(T)) * c_up[None, :, None]
+        k_dn = (wff * X(K) + wfb * X(K, 0, -1)) * (X(T) - X(T, 0, -1)) * c_dn[None, :, None]
+        k_dn[:, 0, :] = -self.qw[0]  # heat flux into the fluid through the bottom wall
+        k_up[:, -1, :] = self.qw[1]  # and through the top wall
+        dyk = (k_up - k_dn) * (row(self.dyfi) * self.cthecd)
+        dzk = ((X(K, 0, 0, 1) + X(K)) * (X(T, 0, 0, 1) - X(T)) - (X(K, 0, 0, -1) + X(K)) * (X(T) - X(T, 0, 0, -1))) * (self.dzi ** 2 * 0.5 * self.cthecd)
+        R = -dxr - dyr - dzr + dxk + dyk + dzk
+        rh = np.minimum(self.rhohmax + 1e-14, X(self.rhoh) + TGAM[ns] * self.dt * R + TROH[ns] * self.dt * X(self.rhse0))
+        self.interior(self.rhoh, rh)
+        self.interior(self.rhse0, R)
+        D = self.td(self.ht(rh / X(self.D)))
+        h = rh / D
+        T, D, M, Kp = self.table_props(h)
+        for a, v in ((self.h, h), (self.T, T), (self.D, D), (self.mu, M), (self.k, Kp)):
+            self.interior(a, v)
+        self.wall_thermal()
+
+    # ---------------------------------------------------------- momentum
+    def prep(self, ns):
+        """DENSITY_TIME_DERIVATION (thermal), then VELOCITY_CALC_io: u = G / rho_stag."""
+        if self.thermal:
+            self.interior(self.drho, ((TGAM[ns] + TROH[ns]) * self.div(self.g) + TROH[ns] * self.div(self.g0)) /
+                          (TGAM[ns] - 2.0))
+        X, G = self.X, self.g
+        rx, ry, rz = self.rho_stg()
+        self.interior(self.q[1], X(G[1]) / rx)
+        self.interior(self.q[3], X(G[3]) / rz)
+        self.q[2][:, 2:self.ny + 1, :] = (X(G[2]) / ry)[:, 1:, :]
+        self.bc_vec(self.q)
+
+    def mom(self, ns):
+        """SOLVERRK3_MOM_IO: convection + explicit viscous terms, RHS_MOM_EXPLICIT_io
+        with the constant-mass-flux gradient, MASSFLUX_CALC_IO, DIVG_io, the
+        FISHPACK Poisson solve, PRCALC_io, MASSFLUX_UPDATE_IO."""
+        ny, X, row = self.ny, self.X, self.row
+        self.g0 = {c: self.g[c].copy() for c in (1, 2, 3)}
+        u, v, w = self.q[1], self.q[2], self.q[3]
+        gx, gy, gz = self.g[1], self.g[2], self.g[3]
+        wff, wfb, wffp, wfbp = row(self.wff), row(self.wfb), row(self.wff, 1), row(self.wfb, 1)
+        dyfj, dycj, dycp, dyfm = row(self.dyfi), row(self.dyci), row(self.dyci, 1), row(self.dyfi, -1)
+        dxi, dzi, cv = self.dxi, self.dzi, self.cvisc
+        if self.thermal:
+            ms = self.mu_stg()
+            M = lambda di=0, dj=0, dk=0: 0.5 * (X(self.mu0, di, dj, dk) + X(self.mu, di, dj, dk))
+            S1, S2, S3 = ((lambda di=0, dj=0, dk=0, s=s: X(s, di, dj, dk)) for s in ms)
+        else:
+            M = S1 = S2 = S3 = lambda *a: 1.0
+
+        def divu(di=0, dj=0, dk=0):  # DIVG_U_io: div u / 3 at the cell (i+di, j+dj, k+dk)
+            return ((X(u, di + 1, dj, dk) - X(u, di, dj, dk)) * dxi +
+                    (X(v, di, dj + 1, dk) - X(v, di, dj, dk)) * row(self.dyfi, dj) +
+                    (X(w, di, dj, dk + 1) - X(w, di, dj, dk)) * dzi) / 3.0
+
+        # x-momentum at the u faces
+        ex = -(((X(gx, 1) + X(gx)) * (X(u, 1) + X(u)) - (X(gx) + X(gx, -1)) * (X(u) + X(u, -1))) * (dxi * 0.25) +
+               ((X(gy, 0, 1) + X(gy, -1, 1)) * (wffp * X(u, 0, 1) + wfbp * X(u)) -
+                (X(gy) + X(gy, -1)) * (wff * X(u) + wfb * X(u, 0, -1))) * (dyfj * 0.5) +
+               ((X(gz, 0, 0, 1) + X(gz, -1, 0, 1)) * (X(u, 0, 0, 1) + X(u)) -
+                (X(gz) + X(gz, -1)) * (X(u) + X(u, 0, 0, -1))) * (dzi * 0.25))
+        d11 = (M() * ((X(u, 1) - X(u)) * dxi - divu()) - M(-1) * ((X(u) - X(u, -1)) * dxi - divu(-1))) * (2.0 * dxi * cv)
+        d12 = (S1(0, 1) * ((X(u, 0, 1) - X(u)) * dycp + (X(v, 0, 1) - X(v, -1, 1)) * dxi) -
+               S1() * ((X(u) - X(u, 0, -1)) * dycj + (X(v) - X(v, -1)) * dxi)) * (dyfj * cv)
+        d13 = (S2(0, 0, 1) * ((X(u, 0, 0, 1) - X(u)) * dzi + (X(w, 0, 0, 1) - X(w, -1, 0, 1)) * dxi) -
+               S2() * ((X(u) - X(u, 0, 0, -1)) * dzi + (X(w) - X(w, -1)) * dxi)) * (dzi * cv)
+        ex = ex + d11 + d12 + d13
+        # y-momentum at the v faces (row 1 is the wall and is dropped)
+        ey = -(((wff * X(gx, 1) + wfb * X(gx, 1, -1)) * (X(v, 1) + X(v)) -
+                (wff * X(gx) + wfb * X(gx, 0, -1)) * (X(v) + X(v, -1))) * (dxi * 0.5) +
+               ((X(gy, 0, 1) + X(gy)) * (X(v, 0, 1) + X(v)) - (X(gy) + X(gy, 0, -1)) * (X(v) + X(v, 0, -1))) * (dycj * 0.25) +
+               ((wff * X(gz, 0, 0, 1) + wfb * X(gz, 0, -1, 1)) * (X(v, 0, 0, 1) + X(v)) -
+                (wff * X(gz) + wfb * X(gz, 0, -1)) * (X(v) + X(v, 0, 0, -1))) * (dzi * 0.5))
+        d21 = (S1(1) * ((X(v, 1) - X(v)) * dxi + (X(u, 1) - X(u, 1, -1)) * dycj) -
+               S1() * ((X(v) - X(v, -1)) * dxi + (X(u) - X(u, 0, -1)) * dycj)) * (dxi * cv)
+        d22 = (M() * ((X(v, 0, 1) - X(v)) * dyfj - divu()) - M(0, -1) * ((X(v) - X(v, 0, -1)) * dyfm - divu(0, -1))) * (2.0 * dycj * cv)
+        d23 = (S3(0, 0, 1) * ((X(v, 0, 0, 1) - X(v)) * dzi + (X(w, 0, 0, 1) - X(w, 0, -1, 1)) * dycj) -
+               S3() * ((X(v) - X(v, 0, 0, -1)) * dzi + (X(w) - X(w, 0, -1)) * dycj)) * (dzi * cv)
+        ey = ey + d21 + d22 + d23
+        # z-momentum at the w faces
+        ez = -(((X(gx, 1) + X(gx, 1, 0, -1)) * (X(w, 1) + X(w)) - (X(gx) + X(gx, 0, 0, -1)) * (X(w) + X(w, -1))) * (dxi * 0.25) +
+               ((X(gy, 0, 1) + X(gy, 0, 1, -1)) * (wffp * X(w, 0, 1) + wfbp * X(w)) -
+                (X(gy) + X(gy, 0, 0, -1)) * (wff * X(w) + wfb * X(w, 0, -1))) * (dyfj * 0.5) +
+               ((X(gz, 0, 0, 1) + X(gz)) * (X(w, 0, 0, 1) + X(w)) - (X(gz) + X(gz, 0, 0, -1)) * (X(w) + X(w, 0, 0, -1))) * (dzi * 0.25))
+        d31 = (S2(1) * ((X(w, 1) - X(w)) * dxi + (X(u, 1) - X(u, 1, 0, -1)) * dzi) -
+               S2() * ((X(w) - X(w, -1)) * dxi + (X(u) - X(u, 0, 0, -1)) * dzi)) * (dxi * cv)
+        d32 = (S3(0, 1) * ((X(w, 0, 1) - X(w)) * dycp + (X(v, 0, 1) - X(v, 0, 1, -1)) * dzi) -
+               S3() * ((X(w) - X(w, 0, -1)) * dycj + (X(v) - X(v, 0, 0, -1)) * dzi)) * (dyfj * cv)
+        d33 = (M() * ((X(w, 0, 0, 1) - X(w)) * dzi - divu()) - M(0, 0, -1) * ((X(w) - X(w, 0, 0, -1)) * dzi - divu(0, 0, -1))) * (2.0 * dzi * cv)
+        ez = ez + d31 + d32 + d33
+        # RK3 combination and pressure gradient
+        p, dt, alp = self.p, self.dt, TALP[ns]
+        rx = (TGAM[ns] * ex + TROH[ns] * X(self.ex0[1])) * dt - (X(p) - X(p, -1)) * (alp * dt * dxi)
+        ry = (TGAM[ns] * ey + TROH[ns] * X(self.ex0[2])) * dt - (X(p) - X(p, 0, -1)) * (alp * dt * dycj)
+        rz = (TGAM[ns] * ez + TROH[ns] * X(self.ex0[3])) * dt - (X(p) - X(p, 0, 0, -1)) * (alp * dt * dzi)
+        self.interior(self.ex0[1], ex)
+        self.interior(self.ex0[3], ez)
+        self.ex0[2][:, 2:ny + 1, :] = ey[:, 1:, :]
+        rx = rx - np.sum(rx / dyfj) / self.volm  # DPGRNS: constant mass flux
+        gx[:, 1:ny + 1, :] += rx
+        gz[:, 1:ny + 1, :] += rz
+        gy[:, 2:ny + 1, :] += ry[:, 1:, :]
+        self.bc_vec(self.g)
+        # projection
+        phi = self.poisson_io((self.div(self.g) + X(self.drho)) / (dt * alp))
+        self.phi[:] = 0.0
+        self.interior(self.phi, phi)
+        self.bc_copy(self.phi)
+        self.interior(p, X(p) + X(self.phi))
+        self.bc_copy(p)
+        f = self.phi
+        gx[:, 1:ny + 1, :] -= (X(f) - X(f, -1)) * (dt * alp * dxi)
+        gz[:, 1:ny + 1, :] -= (X(f) - X(f, 0, 0, -1)) * (dt * alp * dzi)
+        gy[:, 2:ny + 1, :] -= ((X(f) - X(f, 0, -1)) * (dt * alp * dycj))[:, 1:, :]
+        self.bc_vec(self.g)
+
+    def poisson_io(self, rhs):
+        """FISHPACK_POIS3D_SIMPLE's operator diagonalised with complex FFTs in x
+        and z; the mean mode drops its last equation and takes phi(ny) = 0."""
+        nx, ny, nz = self.nx, self.ny, self.nz
+        F = np.fft.fft(np.fft.fft(rhs, axis=2), axis=0)  # (kz, j, kx)
+        lam_x = -4.0 * self.dxi ** 2 * np.sin(np.pi * np.arange(nx) / nx) ** 2
+        lam_z = -4.0 * self.dzi ** 2 * np.sin(np.pi * np.arange(nz) / nz) ** 2
+        am, ac, ap = self.amph[1:ny + 1], self.acph[1:ny + 1], self.apph[1:ny + 1]
+        out = np.zeros_like(F)
+        ab = np.zeros((3, ny), dtype=complex)
+        ab[0, 1:] = ap[:-1]
+        ab[2, :-1] = am[1:]
+        for a in range(nz):
+            for b in range(nx):
+                ab[1] = ac + lam_x[b] + lam_z[a]
+                if a == 0 and b == 0:
+                    out[a, :-1, b] = solve_banded((1, 1), ab[:, :-1], F[a, :-1, b])
+                else:
+                    out[a, :, b] = solve_banded((1, 1), ab, F[a, :, b])
+        return np.real(np.fft.ifft(np.fft.ifft(out, axis=0), axis=2))
+
+    # ---------------------------------------------------------- driver
+    def init_random(self, seed, amp):
+        """TG velocity recipe scaled to unit bulk mass flux (VELO2MASSFLUX,
+        Unified_massflux), h = 0 with the table's properties, then
+        CALC_INITIALIZATION_io (energy with NS = 0, momentum with NS = 0)."""
+        ny = self.ny
+        if self.thermal:
+            T0, D0, M0, K0 = (float(x[0]) for x in self.table_props(np.array([0.0])))
+        else:
+            T0 = D0 = M0 = K0 = 1.0
+        for a, val in ((self.T, T0), (self.D, D0), (self.D0, D0), (self.mu, M0), (self.mu0, M0), (self.k, K0)):
+            a[:] = val
+        for a in (self.h, self.rhoh, self.rhse0, self.drho):
+            a[:] = 0.0
+        super().init_random(seed, amp)
+        r_face = (D0 + D0 + D0 + D0) * 0.25
+        r_v = (self.wff * (D0 + D0) + self.wfb * (D0 + D0)) * 0.5
+
+        def velo2massflux():
+            for c in (1, 2, 3):
+                self.g[c][:] = 0.0
+            self.g[1][:, 1:ny + 1] = self.q[1][:, 1:ny + 1] * r_face
+            self.g[3][:, 1:ny + 1] = self.q[3][:, 1:ny + 1] * r_face
+            self.g[2][:, 2:ny + 1] = self.q[2][:, 2:ny + 1] * r_v[2:ny + 1][None, :, None]
+
+        velo2massflux()
+        gm = self.bulk_of(self.g[1])
+        for c in (1, 2, 3):
+            self.q[c] /= gm
+        velo2massflux()
+        self.bc_vec(self.q)
+        self.p[:] = 0.0
+        for c in (1, 2, 3):
+            self.g0[c][:] = 0.0
+            self.ex0[c][:] = 0.0
+        if self.thermal:
+            self.wall_thermal()
+            self.eng(0)
+        self.mom(0)
+
+    def substep(self, ns):
+        if self.thermal:
+            self.eng(ns)
+        self.prep(ns)
+        self.mom(ns)
+
+    def divmax(self):
+        """max |div G + drho| over the cells (DIVGCK_io)."""
+        return float(np.abs(self.div(self.g) + self.X(self.drho)).max())

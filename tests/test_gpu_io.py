@@ -162,3 +162,25 @@ def test_io_density_time_derivation_parity():
         o.mom(ns)
         compare(g, o, FLOW + THERMAL + ("drho",), tag=f"mom{ns}")
     assert np.abs(o.get("drho")).max() > 1e-3
+
+
+@pytest.mark.parametrize("name", ["io_16x12x8_seed3", "io_heated_16x10x8_seed7"])
+def test_io_golden_fixture(name):
+    """The library (graph-replayed full RK3 steps) against the committed
+    fixtures of the independent numpy restatement, tests/golden/numpy_io.py."""
+    _need_gpu()
+    import os
+    from chapsim1ww_b200 import IOChannel
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", name + ".npz"))
+    nx, ny, nz, lx, lz, ren, dt, seed, amp, steps, thermal, prt, qb, qt = z["meta"]
+    g = IOChannel(int(nx), int(ny), int(nz), lx=lx, lz=lz, ren=ren, dt=dt, thermal=int(thermal), prt=prt,
+                  qw=(qb, qt))
+    g.random_fl_theml_fld_io(int(seed), amp)
+    for n in ("gx", "gy", "p"):
+        assert relerr(g.get_field(n), z["ns0_" + n]) < TOL, n
+    g.step(int(steps))
+    names = ["gx", "gy", "gz", "p", "u", "ex0x"] + (["h", "rho", "mu", "rhse0"] if thermal else [])
+    for n in names:
+        assert relerr(g.get_field(n), z["end_" + n]) < TOL, n
+    assert g.divgck_io() < 1e-12
+    assert abs(g.bulk_massflux_io() - float(z["end_bulk_g"])) < 1e-12

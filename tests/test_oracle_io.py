@@ -6,11 +6,14 @@ constant-mass-flux forcing keeps the bulk mass flux, and one energy substep
 changes the total rho h by exactly the iso-flux wall heat input (conservative
 flux form of RHS_ENERGY_EXPLICIT)."""
 import math
+import os
+import sys
 
 import numpy as np
 import pytest
 
 from oracle.pyoracle import OracleIO, OracleTG, synth_table
+from tests.conftest import relerr
 
 
 def laplacian(o, phi, nx, ny, nz, lx, lz, str2=2.0):
@@ -63,3 +66,53 @@ def test_io_rhohmax_and_table_state():
     assert o.bad_cells() == 0
     h = o.get("h")
     assert np.all(np.abs(h[:, 1:-1, :]) < 1e-2)
+
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+IO_GOLDEN = ["io_16x12x8_seed3", "io_heated_16x10x8_seed7"]
+
+
+def load_io_golden(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    nx, ny, nz, lx, lz, ren, dt, seed, amp, steps, thermal, prt, qb, qt = z["meta"]
+    kw = dict(lx=lx, lz=lz, ren=ren, dt=dt, thermal=int(thermal), prt=prt, qw=(qb, qt))
+    return z, (int(nx), int(ny), int(nz)), int(seed), amp, int(steps), kw
+
+
+@pytest.mark.parametrize("name", IO_GOLDEN)
+def test_oracle_io_matches_golden(name):
+    """The C++ oracle against the fixtures of the independent numpy
+    restatement (tests/golden/numpy_io.py): FP64 within 1e-10 relative."""
+    z, dims, seed, amp, steps, kw = load_io_golden(name)
+    o = OracleIO(*dims, **kw)
+    o.init_random(seed, amp)
+    for n, key in (("gx", "ns0_gx"), ("gy", "ns0_gy"), ("p", "ns0_p")):
+        assert relerr(o.get(n), z[key]) < 1e-10, n
+    o.step(steps)
+    names = [("gx", "end_gx"), ("gy", "end_gy"), ("gz", "end_gz"), ("p", "end_p"), ("u", "end_u"),
+             ("ex0x", "end_ex0x")]
+    if kw["thermal"]:
+        names += [("h", "end_h"), ("rho", "end_rho"), ("mu", "end_mu"), ("rhse0", "end_rhse0")]
+    for n, key in names:
+        assert relerr(o.get(n), z[key]) < 1e-10, n
+    assert o.divmax() < 1e-12 and float(z["end_divmax"]) < 1e-12
+    assert abs(o.bulk(1) - float(z["end_bulk_g"])) < 1e-12
+    assert o.bad_cells() == 0
+
+
+def test_oracle_io_matches_numpy_restatement_heated():
+    """A configuration outside the fixtures, run live through both CPU
+    implementations: uniform y mesh, one RK3 step, unequal wall fluxes."""
+    sys.path.insert(0, GOLDEN)
+    from numpy_io import IO
+    dims, lx, lz = (20, 14, 12), 2 * math.pi, math.pi
+    n = IO(*dims, lx, lz, istr2=0, ren=1200.0, dt=1.5e-3, thermal=1, qw=(0.4, 1.1))
+    o = OracleIO(*dims, lx=lx, lz=lz, istr2=0, ren=1200.0, dt=1.5e-3, thermal=1, qw=(0.4, 1.1))
+    n.init_random(11, 0.15)
+    o.init_random(11, 0.15)
+    for ns in (1, 2, 3):
+        n.substep(ns)
+        o.substep(ns)
+    for name, a in (("gx", n.g[1]), ("gy", n.g[2]), ("gz", n.g[3]), ("p", n.p), ("h", n.h), ("mu", n.mu),
+                    ("ex0y", n.ex0[2])):
+        assert relerr(o.get(name), a) < 1e-10, name
