@@ -49,6 +49,9 @@ WORKLOADS = {
     # variable-property heated IO channel, x-periodic, synthetic 4096-point table
     "io_384x192x192": dict(io=True, nx=384, ny=192, nz=192, lx=8 * math.pi, lz=4 * math.pi / 3, ren=2800.0,
                            dt=1e-3, seed=2, thermal=1, prt=0.71, qw=1.0, table="synthetic"),
+    # the same channel with the semi-implicit viscous scheme (visthemflg = 1)
+    "io_384x192x192_si": dict(io=True, nx=384, ny=192, nz=192, lx=8 * math.pi, lz=4 * math.pi / 3, ren=2800.0,
+                              dt=1e-3, seed=2, thermal=1, prt=0.71, qw=1.0, table="synthetic", visc_scheme=1),
     # the two sections of the coupled TG + IO configuration advanced together
     # each step (the IO section x-periodic: the TG -> IO inlet coupling is not built)
     "c1_tg_io": dict(pair=True, tg="tg_256x192x256", io="io_512x192x256"),
@@ -82,10 +85,20 @@ IO_KERNEL = {"eng_rhs": "k_io_eng_rhs", "eng_props": "k_io_eng_props", "prep": "
              "ifftz": "k_fftz", "ifftx": "k_ifftx", "corr": "k_io_corr"}
 
 
-def io_phase_bytes(ph, nx, ny, nz, real_bytes=8):
+# Semi-implicit scheme: the momentum phase is k_io_rhs_si (u, v, w, p, G x3,
+# mu, mu0, DRHOI x3 read; EXPLT0 x3 read and written; RHS x3 written: 21
+# values) and the nine MOMFA line solves (per component and direction RHS in
+# and out plus the four property fields of the coefficients; the y solves
+# also read G and write G*): 78 values per cell with the energy equation on.
+IO_SI_MOM_VALUES = {1: 78, 0: 37}
+IO_SI_KERNEL = "k_io_rhs_si + MOMFA solves (k_io_cyc, k_io_ysi)"
+
+
+def io_phase_bytes(ph, nx, ny, nz, real_bytes=8, visc=0, thermal=1):
     cells = nx * ny * nz
     spec = (nx // 2 + 1) * ny * nz
-    b = IO_VALUES_PER_CELL.get(ph, 0) * real_bytes * cells
+    vals = IO_SI_MOM_VALUES[1 if thermal else 0] if (visc and ph == "mom_rhs") else IO_VALUES_PER_CELL.get(ph, 0)
+    b = vals * real_bytes * cells
     if ph == "ifftx":
         b += real_bytes * cells
     b += PHASE_SPECTRAL_PASSES.get(ph, 0) * 2 * real_bytes * spec
@@ -234,7 +247,8 @@ def cpu_baseline_io(wl, steps):
     """FP64 IO oracle port on the host cores: init + projection, then `steps` timed steps."""
     from oracle.pyoracle import OracleIO, get_threads
     o = OracleIO(wl["nx"], wl["ny"], wl["nz"], lx=wl["lx"], lz=wl["lz"], ren=wl["ren"], dt=wl["dt"],
-                 thermal=wl["thermal"], prt=wl["prt"], qw=(wl["qw"], wl["qw"]), table=io_table(wl["table"]))
+                 thermal=wl["thermal"], prt=wl["prt"], qw=(wl["qw"], wl["qw"]), table=io_table(wl["table"]),
+                 visc_scheme=wl.get("visc_scheme", 0))
     o.init_random(wl["seed"], 0.1)
     t0 = time.perf_counter()
     o.step(steps)
@@ -258,7 +272,7 @@ def run_io(args, wl, ws, rank, local):
         pg = dist
     s = IOChannel(wl["nx"], wl["ny"], wl["nz"], lx=wl["lx"], lz=wl["lz"], ren=wl["ren"], dt=wl["dt"],
                   thermal=wl["thermal"], prt=wl["prt"], qw=(wl["qw"], wl["qw"]), table=io_table(wl["table"]),
-                  device=local)
+                  device=local, visc_scheme=wl.get("visc_scheme", 0))
     s.random_fl_theml_fld_io(wl["seed"] + rank, 0.1)
     cells = wl["nx"] * wl["ny"] * wl["nz"]
     stream = torch.cuda.ExternalStream(s.stream(), device=local)
@@ -304,10 +318,12 @@ def run_io(args, wl, ws, rank, local):
     dom = max(per_launch, key=per_launch.get)
     peak, peak_kind = measured_peak()
     nx, ny, nz = wl["nx"], wl["ny"], wl["nz"]
-    bytes_dom = io_phase_bytes(dom, nx, ny, nz)
+    visc = wl.get("visc_scheme", 0)
+    kernel_dom = IO_SI_KERNEL if (visc and dom == "mom_rhs") else IO_KERNEL[dom]
+    bytes_dom = io_phase_bytes(dom, nx, ny, nz, visc=visc, thermal=wl["thermal"])
     achieved = bytes_dom / (per_launch[dom] / 1000.0) / 1e9
-    total_bytes = sum(io_phase_bytes(p, nx, ny, nz) for p in IO_PHASES)
-    traffic = load_traffic(args.workload, IO_KERNEL[dom])
+    total_bytes = sum(io_phase_bytes(p, nx, ny, nz, visc=visc, thermal=wl["thermal"]) for p in IO_PHASES)
+    traffic = None if visc else load_traffic(args.workload, IO_KERNEL[dom])
 
     names = ("u", "v", "w", "p", "gx", "gy", "gz", "rhoh")
     host = {}
@@ -351,6 +367,7 @@ def run_io(args, wl, ws, rank, local):
             "data": "synthetic (seeded splitmix64 velocity, h = 0, table properties, NS=0 projection)",
             "config": {"workload": args.workload, **{k: wl[k] for k in ("nx", "ny", "nz", "ren", "dt", "prt")},
                        "wall_heat_flux": wl["qw"], "table": wl["table"], "precision": "fp64",
+                       "viscous_scheme": "semi-implicit (MOMFA_io)" if visc else "explicit",
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                        "l2": "working set (>2 GB) larger than the 126 MB L2"},
             "max_div_g_plus_drho": divmax, "out_of_table_cells": bad,
@@ -358,7 +375,7 @@ def run_io(args, wl, ws, rank, local):
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": nbytes,
                     "d2h_bytes_per_step": nbytes + 8, "steps": e2e_steps},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic, "kernel": IO_KERNEL[dom], "phase": dom,
+                         "frac": achieved / peak, "traffic": traffic, "kernel": kernel_dom, "phase": dom,
                          "algorithmic_bytes_per_launch": bytes_dom, "avg_launch_ms": per_launch[dom],
                          "peak_source": peak_kind},
             "phases_ms_per_launch": per_launch,
@@ -616,7 +633,8 @@ def run_reference(args, wl, ws, rank):
     from oracle.pyoracle import OracleIO, OracleTG, get_threads
     if wl.get("io"):
         o = OracleIO(wl["nx"], wl["ny"], wl["nz"], lx=wl["lx"], lz=wl["lz"], ren=wl["ren"], dt=wl["dt"],
-                     thermal=wl["thermal"], prt=wl["prt"], qw=(wl["qw"], wl["qw"]), table=io_table(wl["table"]))
+                     thermal=wl["thermal"], prt=wl["prt"], qw=(wl["qw"], wl["qw"]), table=io_table(wl["table"]),
+                     visc_scheme=wl.get("visc_scheme", 0))
         o.init_random(wl["seed"], 0.1)
     else:
         o = OracleTG(wl["nx"], wl["ny"], wl["nz"], lx=wl["lx"], lz=wl["lz"], ren=wl["ren"], dt=wl["dt"])

@@ -38,7 +38,7 @@ class ChapsimIOConfig(ctypes.Structure):
     _fields_ = [
         ("struct_size", ctypes.c_int32), ("thermal", ctypes.c_int32), ("prt", ctypes.c_double),
         ("qw_bot", ctypes.c_double), ("qw_top", ctypes.c_double), ("gravdir", ctypes.c_int32),
-        ("pad", ctypes.c_int32), ("f_a", ctypes.c_double),
+        ("visc_scheme", ctypes.c_int32), ("f_a", ctypes.c_double),
     ]
 
 

@@ -490,7 +490,9 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
     for (int c = 0; c < 3; ++c) {
       void **tmp[] = {&d.h0[c], &d.rhs[c], &d.dq[c]};
       for (void **f : tmp) {
-        if (iocfg && f != &d.h0[c]) continue;  // the IO substep needs EXPLT0 only
+        // the explicit IO substep needs EXPLT0 only; the semi-implicit one
+        // keeps RHS_io and a solve scratch field per component
+        if (iocfg && f != &d.h0[c] && !iocfg->visc_scheme) continue;
         if ((rc = dalloc(ctx, &p, n * tsz))) goto fail;
         *f = p;
         cudaMemsetAsync(p, 0, n * tsz, ctx->stream);
@@ -505,6 +507,21 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
         if ((rc = dalloc(ctx, &p, n * sizeof(double)))) goto fail;
         *f = (double *)p;
         cudaMemsetAsync(p, 0, n * sizeof(double), ctx->stream);
+      }
+      io.visc = iocfg->visc_scheme ? 1 : 0;
+      if (io.visc) {
+        for (int c = 0; c < 3; ++c)
+          for (double **f : {&io.drhoi[c], &io.si_t[c]}) {
+            if ((rc = dalloc(ctx, &p, n * sizeof(double)))) goto fail;
+            *f = (double *)p;
+            cudaMemsetAsync(p, 0, n * sizeof(double), ctx->stream);
+          }
+        // AMVR1 and APVRN of TDMA_COEF (src/TDMA_COEF.f90:87-96)
+        const int ny = cfg->ny;
+        double ucaj = 4.0 / (2.0 / ctx->dyci[2] + 1.0 / ctx->dyfi[1]);
+        io.amvr1 = ucaj * (2.0 * ctx->dyfi[1]);
+        ucaj = 4.0 / (2.0 / ctx->dyci[ny] + 1.0 / ctx->dyfi[ny]);
+        io.apvrn = ucaj * (2.0 * ctx->dyfi[ny]);
       }
       if ((rc = dalloc(ctx, &p, sizeof(unsigned long long)))) goto fail;
       io.bad = (unsigned long long *)p;
@@ -574,6 +591,7 @@ int chapsim_io_config_default(chapsim_io_config *io) {
   io->qw_bot = 1.0;
   io->qw_top = 1.0;
   io->gravdir = 0;
+  io->visc_scheme = 0;
   io->f_a = 0.0;
   return CHAPSIM_OK;
 }
@@ -583,6 +601,7 @@ int chapsim_create_io(const chapsim_config *cfg, const chapsim_io_config *io, ch
   if (io->struct_size != (int32_t)sizeof(chapsim_io_config)) return CHAPSIM_ERR_ARG;
   if (cfg->precision != CHAPSIM_FP64) return CHAPSIM_ERR_UNSUPPORTED;
   if (!(io->prt > 0) || io->gravdir < 0 || io->gravdir > 3) return CHAPSIM_ERR_ARG;
+  if (io->visc_scheme != 0 && io->visc_scheme != 1) return CHAPSIM_ERR_ARG;
   return create_ctx(cfg, io, out);
 }
 
@@ -859,6 +878,8 @@ static int io_init_random(chapsim_ctx *ctx, uint64_t seed, double amp, int proje
   const size_t bytes = (size_t)n * sizeof(double);
   double *zero[] = {d.p, d.phi, d.rhsphi, io.drho, io.rhoh, io.h, io.rhse0};
   for (double *f : zero) CKC(cudaMemsetAsync(f, 0, bytes, ctx->stream));
+  if (io.visc)  // DRHOI_STG is zero until the first DENSITY_implicit_add
+    for (int c = 0; c < 3; ++c) CKC(cudaMemsetAsync(io.drhoi[c], 0, bytes, ctx->stream));
   CKC(cudaMemsetAsync(io.bad, 0, sizeof(unsigned long long), ctx->stream));
   const double M2 = M0 + M0;
   const double *vals[] = {&T0, &D0, &D0, &M0, &M0, &K0, &M2};

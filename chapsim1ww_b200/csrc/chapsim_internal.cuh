@@ -62,6 +62,13 @@ struct IODev {
   double *dpg;       // device scalar: DPGRNS of the current substep
   double *part;      // per-block partial sums of the x mass-flux forcing
   unsigned long long *bad;  // table look-ups outside the table
+  // semi-implicit viscous scheme (visthemflg = 1): DRHOI_STG per component,
+  // a second scratch field per component for the cyclic solves, and the wall
+  // coefficients AMVR1 / APVRN of TDMA_COEF
+  int visc;
+  double *drhoi[3];
+  double *si_t[3];
+  double amvr1, apvrn;
 };
 
 // Per-substep scalars.
@@ -179,6 +186,10 @@ int launch_pois_io(chapsim_ctx *c, int ns, double *gx, double *gy, double *gz, c
 int io_eng(chapsim_ctx *c, int ns);
 int io_thermal_bc(chapsim_ctx *c);
 int io_mom(chapsim_ctx *c, int ns, bool prep);
+// semi-implicit scheme: right-hand sides (*npart: the DPGRNS partial count),
+// then the x, z, y factor solves writing G* into the other G buffer
+int io_mom_si(chapsim_ctx *c, int ns, int *npart);
+int io_factor_si(chapsim_ctx *c, int ns);
 int io_reduce(chapsim_ctx *c, int what, double *host_out);
 int io_correction(chapsim_ctx *c, int ns);
 int io_init_maps(chapsim_ctx *c);

@@ -224,6 +224,9 @@ int chapsim_read_instant(chapsim_ctx *ctx, const char *dir, double time, int *it
     double *zero[] = {d.phi, d.rhsphi, iv.drho, iv.rhse0};
     for (double *z : zero)
       if (cudaMemsetAsync(z, 0, bytes, ctx->stream) != cudaSuccess) return CHAPSIM_ERR_CUDA;
+    if (iv.visc)
+      for (int q = 0; q < 3; ++q)
+        if (cudaMemsetAsync(iv.drhoi[q], 0, bytes, ctx->stream) != cudaSuccess) return CHAPSIM_ERR_CUDA;
     if (iv.thermal) {
       std::vector<double> rhoh(n, 0.0);
       for (size_t t = 0; t < n; ++t) rhoh[t] = f[5][t] * f[6][t];

@@ -302,6 +302,14 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_prep(TGDev d, IODev io, dou
     rz = (D[c] + D[c + ozm] + D0[c] + D0[c + ozm]) * 0.5 * 0.5;
     if (j >= 2) ry = (d.wff[j] * (D[c] + D0[c]) + d.wfb[j] * (D[c - sy] + D0[c - sy])) * 0.5;
   }
+  if (do_drho && io.visc) {
+    // DENSITY_implicit_add (src/MASSFLUX_CALC_IO.f90:316-399): 1/RHO_STG minus
+    // 1/(the old density on the face); other rows stay zero
+    const double *__restrict__ D0 = io.D0;
+    io.drhoi[0][c] = 1.0 / rx - 1.0 / ((D0[c] + D0[c + oxm]) * 0.5);
+    io.drhoi[2][c] = 1.0 / rz - 1.0 / ((D0[c] + D0[c + ozm]) * 0.5);
+    if (j >= 2) io.drhoi[1][c] = 1.0 / ry - 1.0 / (d.wff[j] * D0[c] + d.wfb[j] * D0[c - sy]);
+  }
   d.u[c] = gx[c] / rx;
   d.w[c] = gz[c] / rz;
   if (j >= 2) d.v[c] = gy[c] / ry;
@@ -851,9 +859,10 @@ __global__ void __launch_bounds__(1024) k_io_dpgrns(TGDev d, IODev io, double al
   }
 }
 
-// PRCALC_io (explicit branch) and MASSFLUX_UPDATE_IO on g[buf], with the
-// deferred DPGRNS on G_x when use_dpg; pressure ghosts by copy (BC_WALL_PR).
-__global__ void __launch_bounds__(IO_BX *IO_BY) k_io_corr(TGDev d, IODev io, double alp, int buf, int use_dpg) {
+// PRCALC_io and MASSFLUX_UPDATE_IO on g[buf], with the deferred DPGRNS on
+// G_x when use_dpg; pressure ghosts by copy (BC_WALL_PR).
+__global__ void __launch_bounds__(IO_BX *IO_BY) k_io_corr(TGDev d, IODev io, double alp, int buf, int use_dpg,
+                                                        double be) {
   const int nx = d.nx, ny = d.ny;
   const int i = blockIdx.x * IO_BX + threadIdx.x;
   const int j = blockIdx.y * IO_BY + threadIdx.y + 1;
@@ -868,7 +877,9 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_corr(TGDev d, IODev io, dou
   gx[c] = gxv - (phi - d.phi[c + oxm]) * (d.dt * alp * d.dxi);
   gz[c] -= (phi - d.phi[c + ozm]) * (d.dt * alp * d.dzi);
   if (j >= 2) gy[c] -= (phi - d.phi[c - sy]) * (d.dt * alp * d.dyci[j]);
-  const double pn = d.p[c] + phi;
+  // semi-implicit PRCALC_io (src/PRESSURE_CORRECTION.f90:100-110) with the
+  // physical Poisson right-hand side; be = 0 for the explicit scheme
+  const double pn = be != 0.0 ? d.p[c] + phi - be * d.rhsphi[c] : d.p[c] + phi;
   d.p[c] = pn;
   if (j == 1) d.p[c - sy] = pn;
   if (j == ny) d.p[c + sy] = pn;
@@ -899,7 +910,7 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_red_part(TGDev d, IODev io,
       const double *gx = io.g[cur][0], *gy = io.g[cur][1], *gz = io.g[cur][2];
       v = (fabs((gx[c] + gx[c + oxp]) * d.dxi) + fabs((gy[c] + gy[c + sy]) * d.dyfi[j]) +
            fabs((gz[c] + gz[c + ozp]) * d.dzi)) * 0.5;
-      v = v + 2.0 * d.cvisc * (d.dxqi + d.dzqi + d.dyfi[j] * d.dyfi[j]);
+      if (!io.visc) v = v + 2.0 * d.cvisc * (d.dxqi + d.dzqi + d.dyfi[j] * d.dyfi[j]);  // zero when implicit
     } else {
       v = f[c] / d.dyfi[j];
     }
@@ -991,6 +1002,26 @@ int io_mom(chapsim_ctx *c, int ns, bool prep) {
   }
   phase_mark(c, 3);
   int npart = (int)(grid.x * grid.y * grid.z);
+  if (io.visc) {
+    // semi-implicit scheme: RHS_io of the three components, DPGRNS, factored
+    // solves into G*
+    int rc = io_mom_si(c, ns, &npart);
+    if (rc) return rc;
+    k_io_dpgrns<<<1, 1024, 0, c->stream>>>(d, io, sp.alp, npart);
+    LAUNCHED();
+    if ((rc = io_factor_si(c, ns))) return rc;
+    rc = launch_pois_io(c, ns, io.g[nxt][0], io.g[nxt][1], io.g[nxt][2], io.thermal ? io.drho : nullptr);
+    if (rc) return rc;
+    phase_mark(c, CHAPSIM_PH_CORR);
+    k_io_corr<<<grid, blk, 0, c->stream>>>(d, io, sp.alp, nxt, 0, 0.5 * sp.alp * d.dt * d.cvisc);
+    LAUNCHED();
+    c->io_cur = nxt;
+    if (c->timing) {
+      phase_mark(c, CHAPSIM_PH_COUNT);
+      if (++c->ev_pending == chapsim_ctx::kEvSub) return flush_phase_events(c);
+    }
+    return CHAPSIM_OK;
+  }
   if (c->use_tma_io) {
     IoMaps maps;
     memcpy(maps.m, c->io_maps, sizeof(maps.m));
@@ -1009,7 +1040,7 @@ int io_mom(chapsim_ctx *c, int ns, bool prep) {
   int rc = launch_pois_io(c, ns, io.g[nxt][0], io.g[nxt][1], io.g[nxt][2], io.thermal ? io.drho : nullptr);
   if (rc) return rc;
   phase_mark(c, CHAPSIM_PH_CORR);
-  k_io_corr<<<grid, blk, 0, c->stream>>>(d, io, sp.alp, nxt, 1);
+  k_io_corr<<<grid, blk, 0, c->stream>>>(d, io, sp.alp, nxt, 1, 0.0);
   LAUNCHED();
   c->io_cur = nxt;
   if (c->timing) {
@@ -1080,7 +1111,8 @@ int io_restart_fields(chapsim_ctx *c) {
 
 int io_correction(chapsim_ctx *c, int ns) {
   // MASSFLUX_UPDATE_IO + PRCALC_io on the current G (no DPGRNS)
-  k_io_corr<<<cell_grid(c->d), dim3(IO_BX, IO_BY), 0, c->stream>>>(c->d, c->io, c->sp[ns].alp, c->io_cur, 0);
+  const double be = c->io.visc ? 0.5 * c->sp[ns].alp * c->d.dt * c->d.cvisc : 0.0;
+  k_io_corr<<<cell_grid(c->d), dim3(IO_BX, IO_BY), 0, c->stream>>>(c->d, c->io, c->sp[ns].alp, c->io_cur, 0, be);
   LAUNCHED();
   return CHAPSIM_OK;
 }

@@ -282,11 +282,14 @@ typedef struct chapsim_io_config {
   double qw_bot;       /* iso-flux bottom wall: heat flux, > 0 heats the fluid      */
   double qw_top;       /* iso-flux top wall (WALLFLUX = -qw_top, Flow_State.f90:124-148) */
   int32_t gravdir;     /* GRAVDIR: 0 none, 1/2/3 buoyancy along x/y/z             */
-  int32_t pad;
+  int32_t visc_scheme; /* visthemflg (readdata.ini:23): 0 explicit viscous terms,
+                          1 semi-implicit (VISCOUS_PAR_EXPLT_*_io + MOMFA_io,
+                          src/SOLVERRK3_MOM_IO.f90:73-87)                       */
   double f_a;          /* F_A, buoyancy coefficient (Flow_State.f90:98-110)         */
 } chapsim_io_config;
 
-/* Defaults: thermal on, Pr = 0.71, qw = 1 on both walls, no buoyancy. */
+/* Defaults: thermal on, Pr = 0.71, qw = 1 on both walls, no buoyancy,
+ * explicit viscous terms. */
 int chapsim_io_config_default(chapsim_io_config *io);
 
 /* IO domain set-up (MEM_ALLOCAT + COORDJR + FISHPACK_POIS3D_INIT,

@@ -127,6 +127,9 @@ double oracle_io_bulk(const oracle_io *o, int what); /* 0 BULK_VELOCITY_IO, 1 BU
 int64_t oracle_io_bad_cells(const oracle_io *o);     /* table look-ups outside the table so far */
 double oracle_io_cfl(const oracle_io *o);            /* CFL_io + CFL_VISCOUS */
 void oracle_io_set_dt(oracle_io *o, double dt);
+/* visthemflg: 0 explicit viscous terms (default), 1 the semi-implicit scheme
+ * (VISCOUS_PAR_EXPLT_*_io + MOMFA_io).  Set before oracle_io_init_random. */
+int oracle_io_set_scheme(oracle_io *o, int implicit);
 double oracle_tg_cfl(const oracle_tg *o);            /* CFL_tg */
 void oracle_tg_set_dt(oracle_tg *o, double dt);
 void oracle_tg_stats(const oracle_tg *o, double *out); /* PP_MEAN_ZX_FLOW_TG, ny * 122 values */

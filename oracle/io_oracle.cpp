@@ -34,6 +34,17 @@
 //                           src/VELO_CORRECTION.f90:107-185, src/BC_WALL.f90
 //   DIVGCK_io               src/DIVGCK.f90:60-190
 //   BULK_*_IO               src/INITIAL_FL_THEML_FLD_io.f90:385-476
+// and the semi-implicit viscous scheme (visthemflg = 1):
+//   VISCOUS_PAR_EXPLT_X/Y/Z_io  src/VISCOUS_X_EXPLICIT_io.f90:124-286,
+//                           VISCOUS_Y_EXPLICIT_io.f90:264-424,
+//                           VISCOUS_Z_EXPLICIT_io.f90:289-460 (channel branches)
+//   RHS_MOM_EXPLICIT_io     src/RHS_MOM_EXPLICIT_io.f90:79-95 (implicit branch)
+//   MOMFA_io, MOMFA1_X_io, MOMFA2_Z_io, MOMFA3_Y_io
+//                           src/MOMFA_io.f90:17-377
+//   TDMAIJI_CYC, TDMAIJJ_nonCYC  src/TDMAIJI_CYC.f90:67-157, src/TDMAIJJ_nonCYC.f90:67-123
+//   AMVR/APVR, AMVR1, APVRN src/TDMA_COEF.f90:77-116
+//   DENSITY_implicit_add    src/MASSFLUX_CALC_IO.f90:316-399
+//   PRCALC_io               src/PRESSURE_CORRECTION.f90:100-110 (implicit branch)
 //
 // Decisions (each also stated where it applies):
 //  * The mean mode (x-slot 1, z-slot 1) of the Poisson y-solve is singular;
@@ -50,7 +61,14 @@
 //    reference's CALC_INITIALIZATION_io projection.
 //  * Y ghosts of MU_STG, RHO_STG and DivU_io, filled by the periodic MPI halo
 //    exchange in the reference, are never read in the channel branch and are
-//    not formed.
+//    not formed.  The y ghosts of DRHOI_STG (periodic halo values there) are
+//    only ever multiplied by wall ghosts of G, which are zero; they are zero
+//    here.
+//  * Semi-implicit PRCALC_io subtracts BE * RHSLLPHI_io, but
+//    FISHPACK_POIS3D_SIMPLE has by then written its x/z-transformed right-hand
+//    side back into RHSLLPHI_io (src/possion3d_fishpack_reform.f90:456-463):
+//    spectral coefficients used as a physical field.  Here the physical
+//    right-hand side of the Poisson equation is used, as PRCALC_tg does.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -123,6 +141,11 @@ struct oracle_io {
   // thermal fields
   std::vector<double> rhoh, hh, tt, dd, dd0, mu, mu0, kk, rhse, rhse0;
   oracle_dft *dftx = nullptr, *dftz = nullptr;
+  // semi-implicit viscous scheme (visthemflg = 1)
+  int implicit = 0;
+  std::vector<double> rhsio[4], adv[4], drhoi[4];  // RHS_io per component, DIVU_io (density part), DRHOI_STG
+  std::vector<double> amvr13, apvr13, amvr2, apvr2;  // TDMA_COEF y-operators, 1-based
+  double amvr1 = 0.0, apvrn = 0.0;
 
   int64_t len() const { return (int64_t)nx * (ny + 2) * nz; }
   inline int64_t id(int i, int j, int k) const {
@@ -544,18 +567,25 @@ void viscous(oracle_io *o) {
 }
 
 // RHS_MOM_EXPLICIT_io(NS, IDR) (src/RHS_MOM_EXPLICIT_io.f90:1-297) for one
-// component; tmp holds EXPLT on entry and RHS_io on exit.
-void rhs_mom(oracle_io *o, int ns, int idr, std::vector<double> &tmp) {
+// component; tmp holds EXPLT on entry.  Explicit scheme: tmp holds RHS_io on
+// exit.  Semi-implicit scheme (:79-95): rhsio[idr] holds the implicit viscous
+// part on entry and RHS_io on exit, with alpha dt times it and alpha dt / 2
+// times the density part adv[idr] added.
+void rhs_mom(oracle_io *o, int ns, int idr, std::vector<double> &texplt) {
   const int nx = o->nx, ny = o->ny, nz = o->nz;
   const int nyi = idr == 2 ? 2 : 1;
   const double gam = o->tgam[ns], roh = o->troh[ns], alp = o->talp[ns], dt = o->dt;
+  const bool imp = o->implicit != 0;
+  std::vector<double> &tmp = imp ? o->rhsio[idr] : texplt;
+  const double coe2 = alp * dt;
 #pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
   for (int k = 1; k <= nz; ++k)
     for (int j = nyi; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) {
         const int64_t c = o->id(i, j, k);
-        const double rhsc = tmp[c], rhsl = o->explt0[idr][c];
+        const double rhsc = texplt[c], rhsl = o->explt0[idr][c];
         double r = (gam * rhsc + roh * rhsl) * dt;
+        if (imp) r = r + coe2 * o->rhsio[idr][c] + 0.5 * coe2 * o->adv[idr][c];
         o->explt0[idr][c] = rhsc;
         double pgm;
         if (idr == 1)
@@ -704,24 +734,432 @@ void fishpack_pois3d(oracle_io *o) {
   bc_wall_copy(o, o->dph);
 }
 
-void mom_io(oracle_io *o, int ns) {
+
+// ------------------------------------------------------------- semi-implicit viscous scheme
+// AMVR/APVR of TDMA_COEF (src/TDMA_COEF.f90:77-116), channel: u and w (IDR 1,
+// 3) with the wall rows of the half-cell distance (AMVR1, APVRN), v (IDR 2)
+// rows 2..ny with row 1 the identity.
+void vis_ycoef(oracle_io *o) {
+  const int ny = o->ny;
+  o->amvr13.assign(ny + 2, 0.0); o->apvr13.assign(ny + 2, 0.0);
+  o->amvr2.assign(ny + 2, 0.0); o->apvr2.assign(ny + 2, 0.0);
+  for (int j = 2; j <= ny - 1; ++j) {
+    o->amvr13[j] = o->dyfi[j] * o->dyci[j];
+    o->apvr13[j] = o->dyfi[j] * o->dyci[j + 1];
+  }
+  double ucaj = 4.0 / (2.0 / o->dyci[2] + 1.0 / o->dyfi[1]);
+  o->apvr13[1] = ucaj * o->dyci[2];
+  o->amvr1 = ucaj * (2.0 * o->dyfi[1]);
+  ucaj = 4.0 / (2.0 / o->dyci[ny] + 1.0 / o->dyfi[ny]);
+  o->amvr13[ny] = ucaj * o->dyci[ny];
+  o->apvrn = ucaj * (2.0 * o->dyfi[ny]);
+  for (int j = 2; j <= ny; ++j) {
+    o->amvr2[j] = o->dyfi[j - 1] * o->dyci[j];
+    o->apvr2[j] = o->dyfi[j] * o->dyci[j];
+  }
+}
+
+// DENSITY_implicit_add (src/MASSFLUX_CALC_IO.f90:316-399): DRHOI_STG = 1/rho_stag
+// (new and old average) - 1/rho_stag (old density only).
+void density_implicit_add(oracle_io *o) {
   const int nx = o->nx, ny = o->ny, nz = o->nz;
-  for (int c = 1; c <= 3; ++c) o->g0[c] = o->g[c];  // :15
-  convection(o);
-  divg_u(o);
-  viscous(o);
-  rhs_mom(o, ns, 1, o->qtmp);
-  rhs_mom(o, ns, 2, o->dphtmp);
-  rhs_mom(o, ns, 3, o->rhsz);
-  // MASSFLUX_CALC_IO (src/MASSFLUX_CALC_IO.f90:1-79)
+  for (int c = 1; c <= 3; ++c) std::fill(o->drhoi[c].begin(), o->drhoi[c].end(), 0.0);
+  if (!o->thermal) return;
 #pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
   for (int k = 1; k <= nz; ++k)
     for (int j = 1; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) {
-        FC(g, 1, i, j, k) += F(qtmp, i, j, k);
-        FC(g, 3, i, j, k) += F(rhsz, i, j, k);
-        if (j >= 2) FC(g, 2, i, j, k) += F(dphtmp, i, j, k);
+        const int imm = o->im(i), kmm = o->km(k);
+        double den = (F(dd0, i, j, k) + F(dd0, imm, j, k)) * XND2CL;
+        FC(drhoi, 1, i, j, k) = 1.0 / FC(rhostg, 1, i, j, k) - 1.0 / den;
+        den = (F(dd0, i, j, k) + F(dd0, i, j, kmm)) * ZND2CL;
+        FC(drhoi, 3, i, j, k) = 1.0 / FC(rhostg, 3, i, j, k) - 1.0 / den;
+        if (j >= 2) {
+          den = o->wff[j] * F(dd0, i, j, k) + o->wfb[j] * F(dd0, i, j - 1, k);
+          FC(drhoi, 2, i, j, k) = 1.0 / FC(rhostg, 2, i, j, k) - 1.0 / den;
+        }
       }
+}
+
+// VISCOUS_PAR_EXPLT_X/Y/Z_io (channel): the viscous terms split into the
+// explicit part (added to the convection term in tmp), the part treated
+// implicitly by MOMFA_io (rhsio) and the density correction of that part
+// (adv, zero unless thermal).  Normal stresses use VISCOUSITY, shear stresses
+// MU_STG, as the reference writes them.
+void viscous_par(oracle_io *o, int idr, std::vector<double> &tmp) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  const double cv = o->cvisc, dxi = o->dxi, dzi = o->dzi;
+  std::fill(o->rhsio[idr].begin(), o->rhsio[idr].end(), 0.0);  // RHS_io = 0
+  const int j0 = idr == 2 ? 2 : 1;
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
+  for (int k = 1; k <= nz; ++k)
+    for (int j = j0; j <= ny; ++j) {
+      const int jp = j + 1, jm = j - 1, kpp = o->kp(k), kmm = o->km(k);
+      for (int i = 1; i <= nx; ++i) {
+        const int ipp = o->ip(i), imm = o->im(i);
+        double ex, im, ad;
+        if (idr == 1) {  // src/VISCOUS_X_EXPLICIT_io.f90:150-280
+          const double coe1 = -2.0 / 3.0 * dxi * cv, coe2 = o->dyfi[j] * cv, coe32 = dzi * cv;
+          double dudx = (FC(q, 1, ipp, j, k) - FC(q, 1, i, j, k)) * dxi;
+          double dvdy = (FC(q, 2, i, jp, k) - FC(q, 2, i, j, k)) * o->dyfi[j];
+          double dwdz = (FC(q, 3, i, j, kpp) - FC(q, 3, i, j, k)) * dzi;
+          const double t11f_ex = F(mu, i, j, k) * (dvdy + dwdz), t11f_im = F(mu, i, j, k) * dudx;
+          dudx = (FC(g, 1, ipp, j, k) * FC(drhoi, 1, ipp, j, k) - FC(g, 1, i, j, k) * FC(drhoi, 1, i, j, k)) * dxi;
+          const double t11f_ad = F(mu, i, j, k) * dudx;
+          dudx = (FC(q, 1, i, j, k) - FC(q, 1, imm, j, k)) * dxi;
+          dvdy = (FC(q, 2, imm, jp, k) - FC(q, 2, imm, j, k)) * o->dyfi[j];
+          dwdz = (FC(q, 3, imm, j, kpp) - FC(q, 3, imm, j, k)) * dzi;
+          const double t11b_ex = F(mu, imm, j, k) * (dvdy + dwdz), t11b_im = F(mu, imm, j, k) * dudx;
+          dudx = (FC(g, 1, i, j, k) * FC(drhoi, 1, i, j, k) - FC(g, 1, imm, j, k) * FC(drhoi, 1, imm, j, k)) * dxi;
+          const double t11b_ad = F(mu, imm, j, k) * dudx;
+          const double d11_ex = (t11f_ex - t11b_ex) * coe1;
+          const double d11_im = (t11f_im - t11b_im) * coe1 * (-2.0);
+          const double d11_ad = (t11f_ad - t11b_ad) * coe1 * (-2.0);
+          const double vis12p = FC(mustg, 1, i, jp, k);
+          double dvdx = (FC(q, 2, i, jp, k) - FC(q, 2, imm, jp, k)) * dxi;
+          double dudy = (FC(q, 1, i, jp, k) - FC(q, 1, i, j, k)) * o->dyci[jp];
+          const double t12f_ex = vis12p * dvdx, t12f_im = vis12p * dudy;
+          dudy = (FC(g, 1, i, jp, k) * FC(drhoi, 1, i, jp, k) - FC(g, 1, i, j, k) * FC(drhoi, 1, i, j, k)) * o->dyci[jp];
+          const double t12f_ad = vis12p * dudy;
+          const double vis12c = FC(mustg, 1, i, j, k);
+          dudy = (FC(q, 1, i, j, k) - FC(q, 1, i, jm, k)) * o->dyci[j];
+          dvdx = (FC(q, 2, i, j, k) - FC(q, 2, imm, j, k)) * dxi;
+          const double t12b_ex = vis12c * dvdx, t12b_im = vis12c * dudy;
+          dudy = (FC(g, 1, i, j, k) * FC(drhoi, 1, i, j, k) - FC(g, 1, i, jm, k) * FC(drhoi, 1, i, jm, k)) * o->dyci[j];
+          const double t12b_ad = vis12c * dudy;
+          const double d12_ex = (t12f_ex - t12b_ex) * coe2, d12_im = (t12f_im - t12b_im) * coe2;
+          const double d12_ad = (t12f_ad - t12b_ad) * coe2;
+          const double vis13p = FC(mustg, 2, i, j, kpp);
+          double dudz = (FC(q, 1, i, j, kpp) - FC(q, 1, i, j, k)) * dzi;
+          double dwdx = (FC(q, 3, i, j, kpp) - FC(q, 3, imm, j, kpp)) * dxi;
+          const double t13f_ex = vis13p * dwdx, t13f_im = vis13p * dudz;
+          // the density part of tau13 differences Q_io (not G_io), as written (:251-252)
+          dudz = (FC(q, 1, i, j, kpp) * FC(drhoi, 1, i, j, kpp) - FC(q, 1, i, j, k) * FC(drhoi, 1, i, j, k)) * dzi;
+          const double t13f_ad = vis13p * dudz;
+          const double vis13c = FC(mustg, 2, i, j, k);
+          dudz = (FC(q, 1, i, j, k) - FC(q, 1, i, j, kmm)) * dzi;
+          dwdx = (FC(q, 3, i, j, k) - FC(q, 3, imm, j, k)) * dxi;
+          const double t13b_ex = vis13c * dwdx, t13b_im = vis13c * dudz;
+          dudz = (FC(q, 1, i, j, k) * FC(drhoi, 1, i, j, k) - FC(q, 1, i, j, kmm) * FC(drhoi, 1, i, j, kmm)) * dzi;
+          const double t13b_ad = vis13c * dudz;
+          const double d13_ex = (t13f_ex - t13b_ex) * coe32, d13_im = (t13f_im - t13b_im) * coe32;
+          const double d13_ad = (t13f_ad - t13b_ad) * coe32;
+          ex = d11_ex + d12_ex + d13_ex;
+          im = d11_im + d12_im + d13_im;
+          ad = d11_ad + d12_ad + d13_ad;
+        } else if (idr == 2) {  // src/VISCOUS_Y_EXPLICIT_io.f90:296-417
+          const double coe1 = dxi * cv, coe3 = dzi * cv, coe2 = -2.0 / 3.0 * o->dyci[j] * cv;
+          double dudx = (FC(q, 1, ipp, j, k) - FC(q, 1, i, j, k)) * dxi;
+          double dvdy = (FC(q, 2, i, jp, k) - FC(q, 2, i, j, k)) * o->dyfi[j];
+          double dwdz = (FC(q, 3, i, j, kpp) - FC(q, 3, i, j, k)) * dzi;
+          const double t22f_ex = F(mu, i, j, k) * (dudx + dwdz), t22f_im = F(mu, i, j, k) * dvdy;
+          dvdy = (FC(g, 2, i, jp, k) * FC(drhoi, 2, i, jp, k) - FC(g, 2, i, j, k) * FC(drhoi, 2, i, j, k)) * o->dyfi[j];
+          const double t22f_ad = F(mu, i, j, k) * dvdy;
+          dudx = (FC(q, 1, ipp, jm, k) - FC(q, 1, i, jm, k)) * dxi;
+          dvdy = (FC(q, 2, i, j, k) - FC(q, 2, i, jm, k)) * o->dyfi[jm];
+          dwdz = (FC(q, 3, i, jm, kpp) - FC(q, 3, i, jm, k)) * dzi;
+          const double t22b_ex = F(mu, i, jm, k) * (dudx + dwdz), t22b_im = F(mu, i, jm, k) * dvdy;
+          dvdy = (FC(g, 2, i, j, k) * FC(drhoi, 2, i, j, k) - FC(g, 2, i, jm, k) * FC(drhoi, 2, i, jm, k)) * o->dyfi[jm];
+          const double t22b_ad = F(mu, i, jm, k) * dvdy;
+          const double d22_ex = (t22f_ex - t22b_ex) * coe2;
+          const double d22_im = (t22f_im - t22b_im) * coe2 * (-2.0);
+          const double d22_ad = (t22f_ad - t22b_ad) * coe2 * (-2.0);
+          const double vis21p = FC(mustg, 1, ipp, j, k);
+          double dvdx = (FC(q, 2, ipp, j, k) - FC(q, 2, i, j, k)) * dxi;
+          double dudy = (FC(q, 1, ipp, j, k) - FC(q, 1, ipp, jm, k)) * o->dyci[j];
+          const double t21f_ex = vis21p * dudy, t21f_im = vis21p * dvdx;
+          dvdx = (FC(g, 2, ipp, j, k) * FC(drhoi, 2, ipp, j, k) - FC(g, 2, i, j, k) * FC(drhoi, 2, i, j, k)) * dxi;
+          const double t21f_ad = vis21p * dvdx;
+          const double vis21c = FC(mustg, 1, i, j, k);
+          dvdx = (FC(q, 2, i, j, k) - FC(q, 2, imm, j, k)) * dxi;
+          dudy = (FC(q, 1, i, j, k) - FC(q, 1, i, jm, k)) * o->dyci[j];
+          const double t21b_ex = vis21c * dudy, t21b_im = vis21c * dvdx;
+          dvdx = (FC(g, 2, i, j, k) * FC(drhoi, 2, i, j, k) - FC(g, 2, imm, j, k) * FC(drhoi, 2, imm, j, k)) * dxi;
+          const double t21b_ad = vis21c * dvdx;
+          const double d21_ex = (t21f_ex - t21b_ex) * coe1, d21_im = (t21f_im - t21b_im) * coe1;
+          const double d21_ad = (t21f_ad - t21b_ad) * coe1;
+          const double vis23p = FC(mustg, 3, i, j, kpp);
+          double dvdz = (FC(q, 2, i, j, kpp) - FC(q, 2, i, j, k)) * dzi;
+          double dwdy = (FC(q, 3, i, j, kpp) - FC(q, 3, i, jm, kpp)) * o->dyci[j];
+          const double t23f_ex = vis23p * dwdy, t23f_im = vis23p * dvdz;
+          dvdz = (FC(g, 2, i, j, kpp) * FC(drhoi, 2, i, j, kpp) - FC(g, 2, i, j, k) * FC(drhoi, 2, i, j, k)) * dzi;
+          const double t23f_ad = vis23p * dvdz;
+          const double vis23c = FC(mustg, 3, i, j, k);
+          dvdz = (FC(q, 2, i, j, k) - FC(q, 2, i, j, kmm)) * dzi;
+          dwdy = (FC(q, 3, i, j, k) - FC(q, 3, i, jm, k)) * o->dyci[j];
+          const double t23b_ex = vis23c * dwdy, t23b_im = vis23c * dvdz;
+          dvdz = (FC(g, 2, i, j, k) * FC(drhoi, 2, i, j, k) - FC(g, 2, i, j, kmm) * FC(drhoi, 2, i, j, kmm)) * dzi;
+          const double t23b_ad = vis23c * dvdz;
+          const double d23_ex = (t23f_ex - t23b_ex) * coe3, d23_im = (t23f_im - t23b_im) * coe3;
+          const double d23_ad = (t23f_ad - t23b_ad) * coe3;
+          ex = d21_ex + d22_ex + d23_ex;
+          im = d21_im + d22_im + d23_im;
+          ad = d21_ad + d22_ad + d23_ad;
+        } else {  // src/VISCOUS_Z_EXPLICIT_io.f90:324-449
+          const double coe1 = dxi * cv, coe3 = -2.0 / 3.0 * dzi * cv, coe2 = o->dyfi[j] * cv;
+          double dudx = (FC(q, 1, ipp, j, k) - FC(q, 1, i, j, k)) * dxi;
+          double dvdy = (FC(q, 2, i, jp, k) - FC(q, 2, i, j, k)) * o->dyfi[j];
+          double dwdz = (FC(q, 3, i, j, kpp) - FC(q, 3, i, j, k)) * dzi;
+          const double t33f_ex = F(mu, i, j, k) * (dudx + dvdy), t33f_im = F(mu, i, j, k) * dwdz;
+          dwdz = (FC(g, 3, i, j, kpp) * FC(drhoi, 3, i, j, kpp) - FC(g, 3, i, j, k) * FC(drhoi, 3, i, j, k)) * dzi;
+          const double t33f_ad = F(mu, i, j, k) * dwdz;
+          dudx = (FC(q, 1, ipp, j, kmm) - FC(q, 1, i, j, kmm)) * dxi;
+          dvdy = (FC(q, 2, i, jp, kmm) - FC(q, 2, i, j, kmm)) * o->dyfi[j];
+          dwdz = (FC(q, 3, i, j, k) - FC(q, 3, i, j, kmm)) * dzi;
+          const double t33b_ex = F(mu, i, j, kmm) * (dudx + dvdy), t33b_im = F(mu, i, j, kmm) * dwdz;
+          dwdz = (FC(g, 3, i, j, k) * FC(drhoi, 3, i, j, k) - FC(g, 3, i, j, kmm) * FC(drhoi, 3, i, j, kmm)) * dzi;
+          const double t33b_ad = F(mu, i, j, kmm) * dwdz;
+          const double d33_ex = (t33f_ex - t33b_ex) * coe3;
+          const double d33_im = (t33f_im - t33b_im) * coe3 * (-2.0);
+          const double d33_ad = (t33f_ad - t33b_ad) * coe3 * (-2.0);
+          const double vis31p = FC(mustg, 2, ipp, j, k);
+          double dwdx = (FC(q, 3, ipp, j, k) - FC(q, 3, i, j, k)) * dxi;
+          double dudz = (FC(q, 1, ipp, j, k) - FC(q, 1, ipp, j, kmm)) * dzi;
+          const double t31f_ex = vis31p * dudz, t31f_im = vis31p * dwdx;
+          dwdx = (FC(g, 3, ipp, j, k) * FC(drhoi, 3, ipp, j, k) - FC(g, 3, i, j, k) * FC(drhoi, 3, i, j, k)) * dxi;
+          const double t31f_ad = vis31p * dwdx;
+          const double vis31c = FC(mustg, 2, i, j, k);
+          dwdx = (FC(q, 3, i, j, k) - FC(q, 3, imm, j, k)) * dxi;
+          dudz = (FC(q, 1, i, j, k) - FC(q, 1, i, j, kmm)) * dzi;
+          const double t31b_ex = vis31c * dudz, t31b_im = vis31c * dwdx;
+          dwdx = (FC(g, 3, i, j, k) * FC(drhoi, 3, i, j, k) - FC(g, 3, imm, j, k) * FC(drhoi, 3, imm, j, k)) * dxi;
+          const double t31b_ad = vis31c * dwdx;
+          const double d31_ex = (t31f_ex - t31b_ex) * coe1, d31_im = (t31f_im - t31b_im) * coe1;
+          const double d31_ad = (t31f_ad - t31b_ad) * coe1;
+          const double vis32p = FC(mustg, 3, i, jp, k);
+          double dwdy = (FC(q, 3, i, jp, k) - FC(q, 3, i, j, k)) * o->dyci[jp];
+          double dvdz = (FC(q, 2, i, jp, k) - FC(q, 2, i, jp, kmm)) * dzi;
+          const double t32f_ex = vis32p * dvdz, t32f_im = vis32p * dwdy;
+          dwdy = (FC(g, 3, i, jp, k) * FC(drhoi, 3, i, jp, k) - FC(g, 3, i, j, k) * FC(drhoi, 3, i, j, k)) * o->dyci[jp];
+          const double t32f_ad = vis32p * dwdy;
+          const double vis32c = FC(mustg, 3, i, j, k);
+          dwdy = (FC(q, 3, i, j, k) - FC(q, 3, i, jm, k)) * o->dyci[j];
+          dvdz = (FC(q, 2, i, j, k) - FC(q, 2, i, j, kmm)) * dzi;
+          const double t32b_ex = vis32c * dvdz, t32b_im = vis32c * dwdy;
+          dwdy = (FC(g, 3, i, j, k) * FC(drhoi, 3, i, j, k) - FC(g, 3, i, jm, k) * FC(drhoi, 3, i, jm, k)) * o->dyci[j];
+          const double t32b_ad = vis32c * dwdy;
+          const double d32_ex = (t32f_ex - t32b_ex) * coe2, d32_im = (t32f_im - t32b_im) * coe2;
+          const double d32_ad = (t32f_ad - t32b_ad) * coe2;
+          ex = d31_ex + d32_ex + d33_ex;
+          im = d31_im + d32_im + d33_im;
+          ad = d31_ad + d32_ad + d33_ad;
+        }
+        const int64_t c = o->id(i, j, k);
+        tmp[c] = ex + tmp[c];
+        o->rhsio[idr][c] = im;
+        o->adv[idr][c] = ad;
+      }
+    }
+}
+
+// TDMAIJI_CYC (src/TDMAIJI_CYC.f90:67-157) for one cyclic line of n >= 3
+// unknowns: a x(i-1) + b x(i) + c x(i+1) = r, indices modulo n.  The first
+// n-1 unknowns are written as g1 + g2 x(n) (two right-hand sides sharing one
+// elimination); the last row then gives x(n).  r is overwritten by x.
+void tdma_cyc(int n, const double *a, const double *b, const double *c, double *r, double *h0, double *g1,
+              double *g2) {
+  h0[0] = c[0] / b[0];
+  g1[0] = r[0] / b[0];
+  g2[0] = -a[0] / b[0];
+  for (int i = 1; i <= n - 3; ++i) {
+    const double pp = 1.0 / (b[i] - h0[i - 1] * a[i]);
+    const double qq1 = g1[i - 1] * a[i], qq2 = g2[i - 1] * a[i];
+    h0[i] = c[i] * pp;
+    g1[i] = (r[i] - qq1) * pp;
+    g2[i] = -qq2 * pp;
+  }
+  {
+    const int i = n - 2;
+    const double pp = 1.0 / (b[i] - h0[i - 1] * a[i]);
+    const double qq1 = g1[i - 1] * a[i], qq2 = g2[i - 1] * a[i];
+    g1[i] = (r[i] - qq1) * pp;
+    g2[i] = (-c[i] - qq2) * pp;
+  }
+  for (int i = n - 3; i >= 0; --i) {
+    g1[i] = -h0[i] * g1[i + 1] + g1[i];
+    g2[i] = -h0[i] * g2[i + 1] + g2[i];
+  }
+  const int l = n - 1;
+  const double pp = r[l] - c[l] * g1[0] - a[l] * g1[l - 1];
+  const double qq = b[l] + c[l] * g2[0] + a[l] * g2[l - 1];
+  r[l] = pp / qq;
+  for (int i = l - 1; i >= 0; --i) r[i] = g1[i] + g2[i] * r[l];
+}
+
+// TDMAIJJ_nonCYC (src/TDMAIJJ_nonCYC.f90:67-123) with zero boundary values:
+// Thomas sweeps; a[0] and c[n-1] are not used.  r is overwritten by x.
+void tdma_noncyc(int n, const double *a, const double *b, const double *c, double *r, double *h, double *g) {
+  h[0] = c[0] / b[0];
+  g[0] = r[0] / b[0];
+  for (int j = 1; j <= n - 2; ++j) {
+    const double pp = 1.0 / (b[j] - h[j - 1] * a[j]);
+    h[j] = c[j] * pp;
+    g[j] = (r[j] - a[j] * g[j - 1]) * pp;
+  }
+  const int l = n - 1;
+  const double pp = 1.0 / (b[l] - h[l - 1] * a[l]);
+  g[l] = (r[l] - a[l] * g[l - 1]) * pp;
+  r[l] = g[l];
+  for (int j = l - 1; j >= 0; --j) r[j] = g[j] - h[j] * r[j + 1];
+}
+
+// MOMFA_io(NS, IDR) (src/MOMFA_io.f90:17-377): (1 - A_x)(1 - A_z)(1 - A_y) dG
+// = RHS_io with variable coefficients from VISCOUSITY, MU_STG and RHO_STG,
+// then G += dG from row N2I.
+void momfa(oracle_io *o, int ns, int idr) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  const double facoe = 0.5 * o->talp[ns] * o->dt * o->cvisc;
+  const int n2i = idr == 2 ? 2 : 1;
+  std::vector<double> &rhs = o->rhsio[idr];
+  const std::vector<double> &rs = o->rhostg[idr];
+  // MOMFA1_X_io (:48-142), periodic x
+  {
+    const double coe1 = facoe * 4.0 / 3.0 * o->dxqi, coe2 = facoe * o->dxqi;
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
+    for (int k = 1; k <= nz; ++k)
+      for (int j = n2i; j <= ny; ++j) {
+        std::vector<double> a(nx), b(nx), c(nx), r(nx), t0(nx), t1(nx), t2(nx);
+        for (int i = 1; i <= nx; ++i) {
+          const int imm = o->im(i), ipp = o->ip(i);
+          double amu, apu;
+          if (idr == 1) {
+            amu = -coe1 * F(mu, imm, j, k);
+            apu = -coe1 * F(mu, i, j, k);
+          } else if (idr == 2) {
+            amu = -coe2 * FC(mustg, 1, i, j, k);
+            apu = -coe2 * FC(mustg, 1, ipp, j, k);
+          } else {
+            amu = -coe2 * FC(mustg, 2, i, j, k);
+            apu = -coe2 * FC(mustg, 2, ipp, j, k);
+          }
+          a[i - 1] = amu / rs[o->id(imm, j, k)];
+          c[i - 1] = apu / rs[o->id(ipp, j, k)];
+          b[i - 1] = 1.0 - (amu + apu) / rs[o->id(i, j, k)];
+          r[i - 1] = rhs[o->id(i, j, k)];
+        }
+        tdma_cyc(nx, a.data(), b.data(), c.data(), r.data(), t0.data(), t1.data(), t2.data());
+        for (int i = 1; i <= nx; ++i) rhs[o->id(i, j, k)] = r[i - 1];
+      }
+  }
+  // MOMFA2_Z_io (:145-231), periodic z (RCCI2 = 1 in a channel)
+  {
+    const double coe1 = facoe * 4.0 / 3.0 * o->dzqi, coe2 = facoe * o->dzqi;
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
+    for (int i = 1; i <= nx; ++i)
+      for (int j = n2i; j <= ny; ++j) {
+        std::vector<double> a(nz), b(nz), c(nz), r(nz), t0(nz), t1(nz), t2(nz);
+        for (int k = 1; k <= nz; ++k) {
+          const int kmm = o->km(k), kpp = o->kp(k);
+          double amu, apu;
+          if (idr == 1) {
+            amu = -coe2 * FC(mustg, 2, i, j, k);
+            apu = -coe2 * FC(mustg, 2, i, j, kpp);
+          } else if (idr == 2) {
+            amu = -coe2 * FC(mustg, 3, i, j, k);
+            apu = -coe2 * FC(mustg, 3, i, j, kpp);
+          } else {
+            amu = -coe1 * F(mu, i, j, kmm);
+            apu = -coe1 * F(mu, i, j, k);
+          }
+          a[k - 1] = amu / rs[o->id(i, j, kmm)];
+          c[k - 1] = apu / rs[o->id(i, j, kpp)];
+          b[k - 1] = 1.0 - (amu + apu) / rs[o->id(i, j, k)];
+          r[k - 1] = rhs[o->id(i, j, k)];
+        }
+        tdma_cyc(nz, a.data(), b.data(), c.data(), r.data(), t0.data(), t1.data(), t2.data());
+        for (int k = 1; k <= nz; ++k) rhs[o->id(i, j, k)] = r[k - 1];
+      }
+  }
+  // MOMFA3_Y_io (:234-377), rows 1..ny for every component
+  {
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
+    for (int k = 1; k <= nz; ++k)
+      for (int i = 1; i <= nx; ++i) {
+        std::vector<double> a(ny), b(ny), c(ny), r(ny), t0(ny), t1(ny);
+        for (int j = 1; j <= ny; ++j) {
+          double amu, apu, am, ap, den;
+          if (idr == 1 || idr == 3) {
+            const std::vector<double> &fmu = o->mustg[idr];
+            const double coe2 = facoe;
+            if (j == 1) {
+              const double muqt = (F(mu, i, j, k) + F(mu, i, j - 1, k)) * 0.5;
+              amu = -coe2 * o->amvr1 * muqt;
+              apu = -coe2 * o->apvr13[j] * fmu[o->id(i, j + 1, k)];
+              am = 0.0;
+              ap = apu / rs[o->id(i, j + 1, k)];
+            } else if (j == ny) {
+              const double muqt = (F(mu, i, ny, k) + F(mu, i, ny + 1, k)) * 0.5;
+              amu = -coe2 * o->amvr13[j] * fmu[o->id(i, j, k)];
+              apu = -coe2 * o->apvrn * muqt;
+              am = amu / rs[o->id(i, j - 1, k)];
+              ap = 0.0;
+            } else {
+              amu = -coe2 * o->amvr13[j] * fmu[o->id(i, j, k)];
+              apu = -coe2 * o->apvr13[j] * fmu[o->id(i, j + 1, k)];
+              am = amu / rs[o->id(i, j - 1, k)];
+              ap = apu / rs[o->id(i, j + 1, k)];
+            }
+            den = rs[o->id(i, j, k)];
+          } else {
+            const double coe1 = facoe * 4.0 / 3.0;
+            amu = -coe1 * o->amvr2[j] * F(mu, i, j - 1, k);
+            apu = -coe1 * o->apvr2[j] * F(mu, i, j, k);
+            if (j == 1) {
+              am = amu / rs[o->id(i, 0, k)];
+              ap = apu / rs[o->id(i, 2, k)];
+            } else {
+              am = amu / rs[o->id(i, j - 1, k)];
+              ap = apu / rs[o->id(i, j, k)];  // the v face j itself, as written (:349)
+            }
+            den = rs[o->id(i, j, k)];
+          }
+          a[j - 1] = am;
+          c[j - 1] = ap;
+          b[j - 1] = 1.0 - (amu + apu) / den;
+          r[j - 1] = rhs[o->id(i, j, k)];
+        }
+        tdma_noncyc(ny, a.data(), b.data(), c.data(), r.data(), t0.data(), t1.data());
+        for (int j = 1; j <= ny; ++j) rhs[o->id(i, j, k)] = r[j - 1];
+      }
+  }
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
+  for (int k = 1; k <= nz; ++k)
+    for (int j = n2i; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) FC(g, idr, i, j, k) = rhs[o->id(i, j, k)] + FC(g, idr, i, j, k);
+}
+
+void mom_io(oracle_io *o, int ns) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  for (int c = 1; c <= 3; ++c) o->g0[c] = o->g[c];  // :15
+  convection(o);
+  if (o->implicit) {
+    // visthemflg = 1 (:73-87): per component the split viscous terms, the
+    // RHS and the factored solve that updates G
+    viscous_par(o, 1, o->qtmp);
+    rhs_mom(o, ns, 1, o->qtmp);
+    momfa(o, ns, 1);
+    viscous_par(o, 2, o->dphtmp);
+    rhs_mom(o, ns, 2, o->dphtmp);
+    momfa(o, ns, 2);
+    viscous_par(o, 3, o->rhsz);
+    rhs_mom(o, ns, 3, o->rhsz);
+    momfa(o, ns, 3);
+  } else {
+    divg_u(o);
+    viscous(o);
+    rhs_mom(o, ns, 1, o->qtmp);
+    rhs_mom(o, ns, 2, o->dphtmp);
+    rhs_mom(o, ns, 3, o->rhsz);
+    // MASSFLUX_CALC_IO (src/MASSFLUX_CALC_IO.f90:1-79)
+#pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
+    for (int k = 1; k <= nz; ++k)
+      for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) {
+          FC(g, 1, i, j, k) += F(qtmp, i, j, k);
+          FC(g, 3, i, j, k) += F(rhsz, i, j, k);
+          if (j >= 2) FC(g, 2, i, j, k) += F(dphtmp, i, j, k);
+        }
+  }
   bc_wall_vec(o, o->g);
   // DIVG_io (src/DIVG.f90:60-150)
   const double coe0 = 1.0 / o->dt / o->talp[ns];
@@ -735,11 +1173,18 @@ void mom_io(oracle_io *o, int ns) {
         F(rhsllphi, i, j, k) = (divx + divy + divz + F(drho, i, j, k)) * coe0;
       }
   fishpack_pois3d(o);
-  // PRCALC_io (src/PRESSURE_CORRECTION.f90:86-122), explicit branch
+  // PRCALC_io (src/PRESSURE_CORRECTION.f90:86-122); the semi-implicit branch
+  // subtracts BE times the physical Poisson right-hand side (see the header)
+  const double be = o->implicit ? 0.5 * o->talp[ns] * o->dt * o->cvisc : 0.0;
 #pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
   for (int k = 1; k <= nz; ++k)
     for (int j = 1; j <= ny; ++j)
-      for (int i = 1; i <= nx; ++i) F(pr, i, j, k) += F(dph, i, j, k);
+      for (int i = 1; i <= nx; ++i) {
+        if (o->implicit)
+          F(pr, i, j, k) = F(pr, i, j, k) + F(dph, i, j, k) - be * F(rhsllphi, i, j, k);
+        else
+          F(pr, i, j, k) += F(dph, i, j, k);
+      }
   bc_wall_copy(o, o->pr);
   // MASSFLUX_UPDATE_IO (src/VELO_CORRECTION.f90:107-185)
   const double cx = o->dt * o->talp[ns] * o->dxi, cz = o->dt * o->talp[ns] * o->dzi;
@@ -898,6 +1343,10 @@ oracle_io *oracle_io_create(int nx, int ny, int nz, double lx, double lz, double
                   &o->hh, &o->rhse, &o->rhse0})
     v->assign(n, 0.0);
   for (auto *v : {&o->tt, &o->dd, &o->dd0, &o->mu, &o->mu0, &o->kk}) v->assign(n, 1.0);
+  for (int c = 1; c <= 3; ++c) {
+    o->rhsio[c].assign(n, 0.0); o->adv[c].assign(n, 0.0); o->drhoi[c].assign(n, 0.0);
+  }
+  vis_ycoef(o);
   o->dftx = oracle_dft_create(nx);
   o->dftz = oracle_dft_create(nz);
   return o;
@@ -1023,6 +1472,7 @@ int oracle_io_mom(oracle_io *o, int ns) {
       density_time_derivation(o, ns);
       density_staggered(o);
       mu_staggered(o);
+      if (o->implicit) density_implicit_add(o);  // src/SOLVE.f90:126-128
     }
     velocity_calc(o);
   }
@@ -1094,7 +1544,8 @@ double oracle_io_cfl(const oracle_io *o) {
   double m = 0.0;
   for (int k = 1; k <= o->nz; ++k)
     for (int j = 1; j <= o->ny; ++j) {
-      const double vis = 2.0 * o->cvisc * (o->dxqi + o->dzqi + o->dyfi[j] * o->dyfi[j]);
+      // CFL_VISCOUS is zero for the semi-implicit scheme (src/CFL.f90:121-130)
+      const double vis = o->implicit ? 0.0 : 2.0 * o->cvisc * (o->dxqi + o->dzqi + o->dyfi[j] * o->dyfi[j]);
       for (int i = 1; i <= o->nx; ++i) {
         double q = (std::fabs((FC(g, 1, i, j, k) + FC(g, 1, o->ip(i), j, k)) * o->dxi) +
                     std::fabs((FC(g, 2, i, j, k) + FC(g, 2, i, j + 1, k)) * o->dyfi[j]) +
@@ -1107,5 +1558,12 @@ double oracle_io_cfl(const oracle_io *o) {
 }
 
 void oracle_io_set_dt(oracle_io *o, double dt) { o->dt = dt; }
+
+int oracle_io_set_scheme(oracle_io *o, int implicit) {
+  if (implicit != 0 && implicit != 1) return -1;
+  o->implicit = implicit;
+  for (int c = 1; c <= 3; ++c) std::fill(o->drhoi[c].begin(), o->drhoi[c].end(), 0.0);
+  return 0;
+}
 
 }  // extern "C"

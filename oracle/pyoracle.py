@@ -69,6 +69,7 @@ def load(build=True):
         getattr(L, f).argtypes = [P]
     for f in ("oracle_tg_set_dt", "oracle_io_set_dt"):
         getattr(L, f).argtypes = [P, D]
+    L.oracle_io_set_scheme.argtypes = [P, I]
     L.oracle_tg_stats.argtypes = [P, P]
     L.oracle_set_threads.argtypes = [I]
     L.oracle_get_threads.restype = I
@@ -178,17 +179,19 @@ def synth_table(n=4096):
 
 class OracleIO:
     """x-periodic IO channel: SOLVERRK3_ENG_IO + SOLVERRK3_MOM_IO (explicit
-    viscous terms, FISHPACK Poisson), optionally with the energy equation."""
+    viscous terms, or with visc_scheme=1 the semi-implicit MOMFA_io scheme;
+    FISHPACK Poisson), optionally with the energy equation."""
 
     def __init__(self, nx, ny, nz, lx=8 * math.pi, lz=4 * math.pi / 3, str2=2.0, istr2=1, ren=2800.0, dt=1e-3,
                  flowdrvtp=1, cfgv=0.0, thermal=1, prt=0.71, qw=(1.0, 1.0), gravdir=0, f_a=0.0, table=None,
-                 shortcuts=0):
+                 shortcuts=0, visc_scheme=0):
         self.L = load()
         self.h = self.L.oracle_io_create(nx, ny, nz, lx, lz, str2, istr2, ren, dt, flowdrvtp, cfgv, thermal, prt,
                                          qw[0], qw[1], gravdir, f_a)
         if not self.h:
             raise ValueError("oracle_io_create rejected the configuration")
         self.nx, self.ny, self.nz = nx, ny, nz
+        assert self.L.oracle_io_set_scheme(self.h, int(visc_scheme)) == 0
         if thermal:
             if table is None:
                 table = synth_table()
@@ -251,3 +254,6 @@ class OracleIO:
 
     def set_dt(self, dt):
         self.L.oracle_io_set_dt(self.h, dt)
+
+    def set_scheme(self, visc_scheme):
+        assert self.L.oracle_io_set_scheme(self.h, int(visc_scheme)) == 0
