@@ -511,7 +511,7 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
       io.visc = iocfg->visc_scheme ? 1 : 0;
       if (io.visc) {
         for (int c = 0; c < 3; ++c)
-          for (double **f : {&io.drhoi[c], &io.si_t[c]}) {
+          for (double **f : {&io.drhoi[c], &io.si_t[c], &io.stg[c], &io.stg[c + 3]}) {
             if ((rc = dalloc(ctx, &p, n * sizeof(double)))) goto fail;
             *f = (double *)p;
             cudaMemsetAsync(p, 0, n * sizeof(double), ctx->stream);

@@ -68,6 +68,7 @@ struct IODev {
   int visc;
   double *drhoi[3];
   double *si_t[3];
+  double *stg[6];  // MU_STG 1-3, RHO_STG 1-3 of the current substep (energy equation on)
   double amvr1, apvrn;
 };
 

@@ -22,8 +22,8 @@
 // Line solves: one thread per line.  x lines march along the contiguous
 // dimension (each thread its own row); z and y lines have consecutive
 // threads on consecutive x, so every step of the march is a coalesced row.
-// The coefficients are formed on the fly from VISCOUSITY, MU_STG and RHO_STG
-// (themselves formed from mu, mu0, rho, rho0 as MU_Staggered and
+// The coefficients are formed on the fly from VISCOUSITY and the MU_STG /
+// RHO_STG fields k_si_stg forms once per substep (as MU_Staggered and
 // DENSITY_Staggered do).  The cyclic elimination keeps its h0 and G2 vectors
 // in two scratch fields, the forward-swept G1 in place.
 #include <cuda_runtime.h>
@@ -50,22 +50,20 @@ constexpr int SI_BX = 32, SI_BY = 8, SI_LINE = 128;
 __device__ __forceinline__ int wp(int i, int n) { return i + 1 == n ? 0 : i + 1; }
 __device__ __forceinline__ int wm(int i, int n) { return i == 0 ? n - 1 : i - 1; }
 
-// VISCOUSITY, MU_STG(1..3) and RHO_STG(1..3) at (i, j, k), periodic in i and
-// k; with the energy equation off all of them are 1.
-struct Prop {
+// MU_Staggered and DENSITY_Staggered (src/MASSFLUX_CALC_IO.f90:147-311) at
+// (i, j, k), periodic in i and k, formed from mu, mu0, rho, rho0.
+struct StgForm {
   const double *__restrict__ mu;
   const double *__restrict__ mu0;
   const double *__restrict__ D;
   const double *__restrict__ D0;
   const double *__restrict__ wff;
   const double *__restrict__ wfb;
-  int nx, ny, nz, th;
+  int nx, ny, nz;
   int64_t sy, sz;
   __device__ __forceinline__ int64_t at(int i, int j, int k) const { return (int64_t)i + sy * j + sz * k; }
-  __device__ __forceinline__ double vis(int i, int j, int k) const { return th ? mu[at(i, j, k)] : 1.0; }
   // x-face / y-face edge; wall rows 1 and ny+1 from the ghost cells
   __device__ __forceinline__ double s1(int i, int j, int k) const {
-    if (!th) return 1.0;
     const int64_t c = at(i, j, k), m = at(wm(i, nx), j, k);
     if (j == 1) return 0.5 * (mu0[c - sy] + mu[c - sy]);
     if (j == ny + 1) return 0.5 * (mu0[c] + mu[c]);
@@ -74,14 +72,12 @@ struct Prop {
   }
   // x-face / z-face edge
   __device__ __forceinline__ double s2(int i, int j, int k) const {
-    if (!th) return 1.0;
     const int im = wm(i, nx), km = wm(k, nz);
     const int64_t c = at(i, j, k), cx = at(im, j, k), cz = at(i, j, km), cxz = at(im, j, km);
     return (mu[c] + mu[cx] + mu0[c] + mu0[cx] + mu[cz] + mu[cxz] + mu0[cz] + mu0[cxz]) * 0.5 * 0.5 * 0.5;
   }
   // y-face / z-face edge; wall rows from the ghost cells
   __device__ __forceinline__ double s3(int i, int j, int k) const {
-    if (!th) return 1.0;
     const int64_t c = at(i, j, k), m = at(i, j, wm(k, nz));
     if (j == 1) return 0.5 * (mu0[c - sy] + mu[c - sy]);
     if (j == ny + 1) return 0.5 * (mu0[c] + mu[c]);
@@ -89,28 +85,71 @@ struct Prop {
            0.5 * 0.5;
   }
   __device__ __forceinline__ double r1(int i, int j, int k) const {
-    if (!th) return 1.0;
     const int64_t c = at(i, j, k), m = at(wm(i, nx), j, k);
     return (D[c] + D[m] + D0[c] + D0[m]) * 0.5 * 0.5;
   }
   // v faces: row 0 keeps the allocation value 1 (never formed by
   // DENSITY_Staggered), rows 1 and ny+1 from the ghost cells
   __device__ __forceinline__ double r2(int i, int j, int k) const {
-    if (!th || j == 0) return 1.0;
+    if (j == 0) return 1.0;
     const int64_t c = at(i, j, k);
     if (j == 1) return 0.5 * (D0[c - sy] + D[c - sy]);
     if (j == ny + 1) return 0.5 * (D0[c] + D[c]);
     return (wff[j] * (D[c] + D0[c]) + wfb[j] * (D[c - sy] + D0[c - sy])) * 0.5;
   }
   __device__ __forceinline__ double r3(int i, int j, int k) const {
-    if (!th) return 1.0;
     const int64_t c = at(i, j, k), m = at(i, j, wm(k, nz));
     return (D[c] + D[m] + D0[c] + D0[m]) * 0.5 * 0.5;
   }
 };
 
+// MU_STG 1-3 and RHO_STG 1-3 of the substep into io.stg, once, for the
+// right-hand sides and the factor solves: rows 0..ny+1 of the faces that
+// have them (s1, s3: 1..ny+1; s2, r1, r3: 1..ny; r2: 0..ny+1).
+__global__ void __launch_bounds__(SI_BX *SI_BY) k_si_stg(TGDev d, IODev io) {
+  const int i = blockIdx.x * SI_BX + threadIdx.x;
+  const int j = blockIdx.y * SI_BY + threadIdx.y;  // 0..ny+1
+  const int k = blockIdx.z;
+  if (i >= d.nx || j > d.ny + 1) return;
+  const StgForm F{io.mu, io.mu0, io.D, io.D0, d.wff, d.wfb, d.nx, d.ny, d.nz, d.sy, d.sz};
+  const int64_t c = F.at(i, j, k);
+  if (j >= 1) {
+    io.stg[0][c] = F.s1(i, j, k);
+    io.stg[2][c] = F.s3(i, j, k);
+  }
+  if (j >= 1 && j <= d.ny) {
+    io.stg[1][c] = F.s2(i, j, k);
+    io.stg[3][c] = F.r1(i, j, k);
+    io.stg[5][c] = F.r3(i, j, k);
+  }
+  io.stg[4][c] = F.r2(i, j, k);
+}
+
+// VISCOUSITY, MU_STG(1..3) and RHO_STG(1..3) at (i, j, k) from the fields
+// k_si_stg formed; with the energy equation off all of them are 1.
+struct Prop {
+  const double *__restrict__ mu;
+  const double *__restrict__ st1;
+  const double *__restrict__ st2;
+  const double *__restrict__ st3;
+  const double *__restrict__ rs1;
+  const double *__restrict__ rs2;
+  const double *__restrict__ rs3;
+  int nx, ny, nz, th;
+  int64_t sy, sz;
+  __device__ __forceinline__ int64_t at(int i, int j, int k) const { return (int64_t)i + sy * j + sz * k; }
+  __device__ __forceinline__ double vis(int i, int j, int k) const { return th ? mu[at(i, j, k)] : 1.0; }
+  __device__ __forceinline__ double s1(int i, int j, int k) const { return th ? st1[at(i, j, k)] : 1.0; }
+  __device__ __forceinline__ double s2(int i, int j, int k) const { return th ? st2[at(i, j, k)] : 1.0; }
+  __device__ __forceinline__ double s3(int i, int j, int k) const { return th ? st3[at(i, j, k)] : 1.0; }
+  __device__ __forceinline__ double r1(int i, int j, int k) const { return th ? rs1[at(i, j, k)] : 1.0; }
+  __device__ __forceinline__ double r2(int i, int j, int k) const { return th ? rs2[at(i, j, k)] : 1.0; }
+  __device__ __forceinline__ double r3(int i, int j, int k) const { return th ? rs3[at(i, j, k)] : 1.0; }
+};
+
 __device__ __forceinline__ Prop make_prop(const TGDev &d, const IODev &io) {
-  return Prop{io.mu, io.mu0, io.D, io.D0, d.wff, d.wfb, d.nx, d.ny, d.nz, io.thermal, d.sy, d.sz};
+  return Prop{io.mu, io.stg[0], io.stg[1], io.stg[2], io.stg[3], io.stg[4], io.stg[5],
+              d.nx, d.ny, d.nz, io.thermal, d.sy, d.sz};
 }
 
 // Convection (CONVECTION_*_io), the split viscous terms (VISCOUS_PAR_EXPLT_*_io)
@@ -508,6 +547,10 @@ int io_mom_si(chapsim_ctx *c, int ns, int *npart) {
   IODev &io = c->io;
   const SubParams &sp = c->sp[ns];
   const dim3 grid = si_cell_grid(d);
+  if (io.thermal) {
+    k_si_stg<<<dim3(grid.x, (d.ny + 2 + SI_BY - 1) / SI_BY, d.nz), dim3(SI_BX, SI_BY), 0, c->stream>>>(d, io);
+    LAUNCHED();
+  }
   k_io_rhs_si<<<grid, dim3(SI_BX, SI_BY), 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, c->io_cur);
   LAUNCHED();
   *npart = (int)(grid.x * grid.y * grid.z);
