@@ -28,7 +28,7 @@ struct TGDev {
   void *rhs[3];
   void *dq[3];      // x/z-solved increments (banded-inverse path)
   void *spec;       // complex spectral array
-  double2 *ypiv;    // Poisson y-line pivots {pp_j, h_j} per (kx, j, kz)
+  double2 *ypiv;    // Poisson y-line pivots: pp_j then h_j, each in the spectral layout
   double *res;      // FP64 Poisson residual (refinement sweep of the mixed form)
   double *partials; // per-block mass-flux partial sums
   double *scal;     // device scalars: [0] dpgrns, [1..] reduction outputs
@@ -44,6 +44,7 @@ struct TGDev {
   // mode at the last y-row instead of decoupling row 1.
   const double *drho;
   int pin_last;
+  int skip_rhs;  // 1: the fused forward x-transform does not store RHSLLPHI
 };
 
 // Device-side state of an IO domain (x-periodic channel section), on top of
@@ -182,7 +183,8 @@ int launch_bc_q(chapsim_ctx *c);
 // Poisson solve of an IO domain: DIVG_io of (gx, gy, gz) + drho fused into the
 // forward x-transform, then the spectral y-solve with the mean mode pinned at
 // the last row, into phi.
-int launch_pois_io(chapsim_ctx *c, int ns, double *gx, double *gy, double *gz, const double *drho);
+int launch_pois_io(chapsim_ctx *c, int ns, double *gx, double *gy, double *gz, const double *drho,
+                   bool store_rhs);
 // IO domain kernels (io_kernels.cu).
 int io_eng(chapsim_ctx *c, int ns);
 int io_thermal_bc(chapsim_ctx *c);

@@ -132,4 +132,53 @@ __device__ C *fft_lines(C *a, C *b, int nlines, int n, int lstride, const int *r
   return a;
 }
 
+// The same stages on lines stored interleaved: element e of line l at
+// buf[e * nl + l] (consecutive lines adjacent).  Consecutive threads take
+// consecutive lines, so each stage's reads and writes are contiguous rows.
+// Per element the arithmetic is that of stockham_stage.
+template <typename C, int R>
+__device__ __forceinline__ void stockham_stage_il(const C *__restrict__ in, C *__restrict__ out, int nl, int n,
+                                                  int Ns, const C *__restrict__ tw, int sign) {
+  const int nb = n / R;
+  const int total = nl * nb;
+  const int tstep = n / (Ns * R);
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int j = t / nl;
+    const int line = t - j * nl;
+    const int k = j % Ns;
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = in[(j + r * nb) * nl + line];
+    if (k != 0) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twiddle(tw, r * k * tstep, sign));
+    }
+    dft_small<C, R>(v, tw, n, sign);
+    const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) out[(base + r * Ns) * nl + line] = v[r];
+  }
+}
+
+template <typename C, bool BIG>
+__device__ C *fft_lines_il(C *a, C *b, int nl, int n, const int *rad, int nrad, const C *__restrict__ tw, int sign) {
+  int Ns = 1;
+  for (int s = 0; s < nrad; ++s) {
+    const int R = rad[s];
+    switch (R) {
+      case 2: stockham_stage_il<C, 2>(a, b, nl, n, Ns, tw, sign); break;
+      case 3: stockham_stage_il<C, 3>(a, b, nl, n, Ns, tw, sign); break;
+      case 4: stockham_stage_il<C, 4>(a, b, nl, n, Ns, tw, sign); break;
+      case 5: stockham_stage_il<C, 5>(a, b, nl, n, Ns, tw, sign); break;
+      case 7: if (BIG) stockham_stage_il<C, 7>(a, b, nl, n, Ns, tw, sign); break;
+      case 11: if (BIG) stockham_stage_il<C, 11>(a, b, nl, n, Ns, tw, sign); break;
+      default: break;
+    }
+    __syncthreads();
+    C *t = a; a = b; b = t;
+    Ns *= R;
+  }
+  return a;
+}
+
 }  // namespace chapsim

@@ -276,6 +276,7 @@ __global__ void k_io_msum(IODev io, size_t n) {
 // ---------------------------------------------------------------- momentum
 // DENSITY_TIME_DERIVATION (gamma - 2 divisor as written) and VELOCITY_CALC_io
 // with its wall BC.  RHO_STG is formed from rho, rho0 (DENSITY_Staggered).
+template <bool VISC>
 __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_prep(TGDev d, IODev io, double gp, double zr, double den,
                                                         int cur, int do_drho) {
   const int nx = d.nx, ny = d.ny;
@@ -302,7 +303,7 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_prep(TGDev d, IODev io, dou
     rz = (D[c] + D[c + ozm] + D0[c] + D0[c + ozm]) * 0.5 * 0.5;
     if (j >= 2) ry = (d.wff[j] * (D[c] + D0[c]) + d.wfb[j] * (D[c - sy] + D0[c - sy])) * 0.5;
   }
-  if (do_drho && io.visc) {
+  if (VISC && do_drho) {
     // DENSITY_implicit_add (src/MASSFLUX_CALC_IO.f90:316-399): 1/RHO_STG minus
     // 1/(the old density on the face); other rows stay zero
     const double *__restrict__ D0 = io.D0;
@@ -997,7 +998,10 @@ int io_mom(chapsim_ctx *c, int ns, bool prep) {
   }
   phase_mark(c, 2);
   if (prep) {
-    k_io_prep<<<grid, blk, 0, c->stream>>>(d, io, sp.gam + sp.roh, sp.roh, sp.gam - 2.0, cur, io.thermal);
+    if (io.visc)
+      k_io_prep<true><<<grid, blk, 0, c->stream>>>(d, io, sp.gam + sp.roh, sp.roh, sp.gam - 2.0, cur, io.thermal);
+    else
+      k_io_prep<false><<<grid, blk, 0, c->stream>>>(d, io, sp.gam + sp.roh, sp.roh, sp.gam - 2.0, cur, io.thermal);
     LAUNCHED();
   }
   phase_mark(c, 3);
@@ -1010,7 +1014,8 @@ int io_mom(chapsim_ctx *c, int ns, bool prep) {
     k_io_dpgrns<<<1, 1024, 0, c->stream>>>(d, io, sp.alp, npart);
     LAUNCHED();
     if ((rc = io_factor_si(c, ns))) return rc;
-    rc = launch_pois_io(c, ns, io.g[nxt][0], io.g[nxt][1], io.g[nxt][2], io.thermal ? io.drho : nullptr);
+    // the semi-implicit PRCALC_io reads RHSLLPHI
+    rc = launch_pois_io(c, ns, io.g[nxt][0], io.g[nxt][1], io.g[nxt][2], io.thermal ? io.drho : nullptr, true);
     if (rc) return rc;
     phase_mark(c, CHAPSIM_PH_CORR);
     k_io_corr<<<grid, blk, 0, c->stream>>>(d, io, sp.alp, nxt, 0, 0.5 * sp.alp * d.dt * d.cvisc);
@@ -1037,7 +1042,8 @@ int io_mom(chapsim_ctx *c, int ns, bool prep) {
   LAUNCHED();
   k_io_dpgrns<<<1, 1024, 0, c->stream>>>(d, io, sp.alp, npart);
   LAUNCHED();
-  int rc = launch_pois_io(c, ns, io.g[nxt][0], io.g[nxt][1], io.g[nxt][2], io.thermal ? io.drho : nullptr);
+  // the explicit PRCALC_io does not read RHSLLPHI: the transform skips storing it
+  int rc = launch_pois_io(c, ns, io.g[nxt][0], io.g[nxt][1], io.g[nxt][2], io.thermal ? io.drho : nullptr, false);
   if (rc) return rc;
   phase_mark(c, CHAPSIM_PH_CORR);
   k_io_corr<<<grid, blk, 0, c->stream>>>(d, io, sp.alp, nxt, 1, 0.0);
@@ -1104,7 +1110,7 @@ int io_restart_fields(chapsim_ctx *c) {
   dim3 g2((d.nx + IO_BX - 1) / IO_BX, (d.ny + 2 + IO_BY - 1) / IO_BY, d.nz);
   k_io_props_only<<<g2, dim3(IO_BX, IO_BY), 0, c->stream>>>(d, c->io);
   LAUNCHED();
-  k_io_prep<<<cell_grid(d), dim3(IO_BX, IO_BY), 0, c->stream>>>(d, c->io, 0.0, 0.0, 1.0, c->io_cur, 0);
+  k_io_prep<false><<<cell_grid(d), dim3(IO_BX, IO_BY), 0, c->stream>>>(d, c->io, 0.0, 0.0, 1.0, c->io_cur, 0);
   LAUNCHED();
   return CHAPSIM_OK;
 }

@@ -711,8 +711,9 @@ __global__ void __launch_bounds__(128) k_adiy_smem(TGDev d, SubParams sp, int fr
 // divergence (and stores RHSLLPHI); mode 1 transforms the stored RHSLLPHI;
 // mode 2 the Poisson residual.
 __host__ __device__ constexpr size_t align128(size_t b) { return (b + 127) & ~(size_t)127; }
-template <typename C> __host__ __device__ constexpr size_t fftx_smem_bytes(int nx, int lb) {
-  return align128((size_t)(lb / 2) * nx * sizeof(C)) + (size_t)(4 * lb + 1) * nx * sizeof(double);
+// dr != 0 reserves lb rows for DrhoDtP (IO contexts)
+template <typename C> __host__ __device__ constexpr size_t fftx_smem_bytes(int nx, int lb, int dr = 0) {
+  return align128((size_t)(lb / 2) * nx * sizeof(C)) + (size_t)((4 + dr) * lb + 1) * nx * sizeof(double);
 }
 
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
@@ -724,7 +725,7 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
 }
 
 template <typename T, bool BIG>
-__global__ void __launch_bounds__(256, 2) k_fftx(TGDev d, SubParams sp, FFTPlan pl, int lb, int mode) {
+__global__ void __launch_bounds__(256, BIG ? 2 : 3) k_fftx(TGDev d, SubParams sp, FFTPlan pl, int lb, int mode) {
   typedef typename Cplx<T>::type C;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t bar;
@@ -739,6 +740,8 @@ __global__ void __launch_bounds__(256, 2) k_fftx(TGDev d, SubParams sp, FFTPlan 
   double *in = reinterpret_cast<double *>(smem_raw + align128((size_t)nl * nx * sizeof(C)));
   C *B = reinterpret_cast<C *>(in);  // FFT scratch, reuses the input area once A is filled
   double *U = in, *V = in + (size_t)lb * nx, *W0 = V + (size_t)(lb + 1) * nx, *W1 = W0 + (size_t)lb * nx;
+  double *DR = W1 + (size_t)lb * nx;  // DrhoDtP rows (IO, mode 0)
+  const bool dr = mode == 0 && d.drho != nullptr;
   if (tid == 0) {
     mbar_init(&bar, 1);
     fence_mbar_init();
@@ -750,11 +753,12 @@ __global__ void __launch_bounds__(256, 2) k_fftx(TGDev d, SubParams sp, FFTPlan 
   const int64_t row0 = d.sy * jbeg;
   if (tid == 0) {
     if (mode == 0) {
-      mbar_expect_tx(&bar, (4 * nrow + 1) * rowb);
+      mbar_expect_tx(&bar, ((dr ? 5 : 4) * nrow + 1) * rowb);
       bulk_g2s(U, d.u + row0 + d.sz * k, nrow * rowb, &bar);
       bulk_g2s(V, d.v + row0 + d.sz * k, (nrow + 1) * rowb, &bar);
       bulk_g2s(W0, d.w + row0 + d.sz * k, nrow * rowb, &bar);
       bulk_g2s(W1, d.w + row0 + d.sz * kp, nrow * rowb, &bar);
+      if (dr) bulk_g2s(DR, d.drho + row0 + d.sz * k, nrow * rowb, &bar);
     } else {
       mbar_expect_tx(&bar, nrow * rowb);
       bulk_g2s(U, (mode == 1 ? d.rhsphi : d.res) + row0 + d.sz * k, nrow * rowb, &bar);
@@ -774,9 +778,9 @@ __global__ void __launch_bounds__(256, 2) k_fftx(TGDev d, SubParams sp, FFTPlan 
         const int j = jbeg + r;
         double dv = (U[r * nx + ip] - U[r * nx + i]) * d.dxi + (V[(r + 1) * nx + i] - V[r * nx + i]) * d.dyfi[j] +
                     (W1[r * nx + i] - W0[r * nx + i]) * d.dzi;
-        if (d.drho) dv += d.drho[row0 + d.sz * k + (int64_t)r * nx + i];  // DIVG_io: + DrhoDtP
+        if (dr) dv += DR[r * nx + i];  // DIVG_io: + DrhoDtP
         val = dv * coe0;
-        d.rhsphi[row0 + d.sz * k + (int64_t)r * nx + i] = val;
+        if (!d.skip_rhs) d.rhsphi[row0 + d.sz * k + (int64_t)r * nx + i] = val;
       } else {
         val = U[r * nx + i];
       }
@@ -806,35 +810,58 @@ __global__ void __launch_bounds__(256, 2) k_fftx(TGDev d, SubParams sp, FFTPlan 
 
 // Complex transform along z for lz consecutive kx at row j
 // (src/possion3d_FFT99.f90:301-317 forward with 1/nz and the (1,1,1) mode
-// zeroed (:324-327); :448-458 inverse).
+// zeroed (:324-327); :448-458 inverse).  The block's nz rows of lz spectral
+// values (contiguous in memory) arrive by one bulk copy each, all completing
+// on one mbarrier, into a line-interleaved buffer A[kz * lz + l]; the
+// Stockham stages then run on the interleaved layout.
 template <typename T, bool BIG>
-__global__ void __launch_bounds__(256, 2) k_fftz(TGDev d, FFTPlan pl, int lz, int sign) {
+__global__ void __launch_bounds__(256, BIG ? 2 : 3) k_fftz(TGDev d, FFTPlan pl, int lz, int sign) {
   typedef typename Cplx<T>::type C;
   extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ uint64_t bar;
+  __shared__ int rad[16];
   const int nz = d.nz, ny = d.ny, lh = d.lh;
   const int j = blockIdx.y + 1;
   const int kx0 = blockIdx.x * lz;
   const int nl = min(lz, lh - kx0);
-  const int ld = nz + 1;
+  // copies move whole 16-byte units: a float2 row is rounded up to an even
+  // count (the pitch lp is even, so the extra value is the row's padding)
+  const int nc = sizeof(C) == 8 ? ((nl + 1) & ~1) : nl;
+  const int tid = threadIdx.x;
   C *A = reinterpret_cast<C *>(smem_raw);
-  C *B = A + lz * ld;
-  __shared__ int rad[16];
-  if (threadIdx.x < 16) rad[threadIdx.x] = pl.rad[threadIdx.x];
+  C *B = A + (size_t)lz * nz;
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  if (tid < 16) rad[tid] = pl.rad[tid];
+  __syncthreads();
   C *S = reinterpret_cast<C *>(d.spec) + kx0 + (int64_t)d.lp * (j - 1);
   const int64_t skz = (int64_t)d.lp * ny;
-  for (int t = threadIdx.x; t < nz * lz; t += blockDim.x) {
-    const int kz = t / lz, l = t - kz * lz;
-    C v;
-    if (l < nl) v = S[skz * kz + l]; else { v.x = 0; v.y = 0; }
-    A[l * ld + kz] = v;
+  const uint32_t rowb = (uint32_t)(nc * sizeof(C));
+  if (tid == 0) mbar_expect_tx(&bar, rowb * (uint32_t)nz);
+  __syncthreads();
+  for (int kz = tid; kz < nz; kz += blockDim.x) bulk_g2s(A + (size_t)kz * lz, S + skz * kz, rowb, &bar);
+  if (nc < lz) {  // columns past the end of the spectrum: zeros
+    const int w = lz - nc;
+    for (int t = tid; t < nz * w; t += blockDim.x) {
+      const int kz = t / w;
+      C z; z.x = 0; z.y = 0;
+      A[(size_t)kz * lz + nc + (t - kz * w)] = z;
+    }
+  }
+  if (!mbar_wait(&bar, 0, d.err)) {
+    mbar_wait(&bar, 0, d.err);  // let copies in flight land before the block exits
+    return;
   }
   __syncthreads();
-  C *res = fft_lines<C, BIG>(A, B, lz, nz, ld, rad, pl.nrad, (const C *)(sizeof(T) == 8 ? (const void *)pl.tw64 : (const void *)pl.tw32), sign);
+  C *res = fft_lines_il<C, BIG>(A, B, lz, nz, rad, pl.nrad,
+                                (const C *)(sizeof(T) == 8 ? (const void *)pl.tw64 : (const void *)pl.tw32), sign);
   const T scale = sign < 0 ? (T)(1.0 / nz) : (T)1;
-  for (int t = threadIdx.x; t < nz * lz; t += blockDim.x) {
+  for (int t = tid; t < nz * lz; t += blockDim.x) {
     const int kz = t / lz, l = t - kz * lz;
     if (l < nl) {
-      C v = res[l * ld + kz];
+      C v = res[t];
       v.x *= scale;
       v.y *= scale;
       if (sign < 0 && j == 1 && kz == 0 && kx0 + l == 0 && !d.pin_last) { v.x = 0; v.y = 0; }
@@ -847,67 +874,104 @@ __global__ void __launch_bounds__(256, 2) k_fftz(TGDev d, FFTPlan pl, int lz, in
 // (kx, kz) the forward-elimination factors pp_j = 1/(B_j - h_{j-1} A_j) and
 // h_j = C_j pp_j of the matrix of src/possion3d_FFT99.f90:334-443 with the
 // coefficients of TDMA_PHI_COEF (:185-220): A = AMPH, B = ACPH - AK1 - AK3,
-// C = APPH, and for the mean mode (kx = kz = 0) row 1 decoupled.  Stored as
-// {pp, h} pairs in the spectral layout.
+// C = APPH, and for the mean mode (kx = kz = 0) row 1 decoupled.  Stored in
+// the spectral layout as two arrays, pp then h (each lp * ny * nz values):
+// the forward sweep reads only pp, the back substitution only h.
 __global__ void k_ypivots(TGDev d) {
   const int lh = d.lh, ny = d.ny;
   const int kx = blockIdx.x * blockDim.x + threadIdx.x;
   const int kz = blockIdx.y;
   if (kx >= lh) return;
-  double2 *P = d.ypiv + kx + (int64_t)d.lp * ny * kz;
+  const int64_t base = kx + (int64_t)d.lp * ny * kz;
+  double *PP = reinterpret_cast<double *>(d.ypiv) + base;
+  double *HH = reinterpret_cast<double *>(d.ypiv) + (int64_t)d.lp * ny * d.nz + base;
   const double shift = d.ak1[kx] + d.ak3[kz];
   const bool mean = (kx == 0 && kz == 0);
   const bool pin1 = mean && !d.pin_last, pinn = mean && d.pin_last;
   double b = d.acph[1] - shift;
   double pp = 1.0 / b;
   double h = (pin1 ? 0.0 : d.apph[1]) * pp;
-  P[0] = make_double2(pin1 ? 0.0 : pp, h);  // pp = 0 zeroes the pinned row
+  PP[0] = pin1 ? 0.0 : pp;  // pp = 0 zeroes the pinned row
+  HH[0] = h;
   for (int j = 2; j <= ny; ++j) {
     b = d.acph[j] - shift;
     // TRID0's zero branch for the singular last pivot of the mean mode
     // (src/possion3d_fishpack_reform.f90:53-58): phi(ny) = 0
     pp = (pinn && j == ny) ? 0.0 : 1.0 / (b - h * d.amph[j]);
     h = j < ny ? d.apph[j] * pp : 0.0;
-    P[(int64_t)d.lp * (j - 1)] = make_double2(pp, h);
+    PP[(int64_t)d.lp * (j - 1)] = pp;
+    HH[(int64_t)d.lp * (j - 1)] = h;
   }
 }
 
 // Poisson y-tridiagonal solves, one thread per (kx, kz) line straight from
 // global memory: consecutive threads own consecutive kx, so every row access
-// is coalesced; the forward-swept g is written over the spectral data in
-// place and read back by the back substitution; with the pivots precomputed
-// no load sits on the serial dependency chain, so the unrolled sweeps keep
-// many loads in flight.
+// is coalesced.  The forward-swept g is written over the spectral data in
+// place and read back by the back substitution.  Each sweep loads the next
+// YB rows (values and pivots) into registers before it computes and stores
+// them, so YB loads per thread are in flight instead of one.
+constexpr int YB = 8;
 template <typename T>
 __global__ void __launch_bounds__(128) k_ysolve_line(TGDev d) {
   typedef typename Cplx<T>::type C;
   const int lh = d.lh, ny = d.ny;
   const int kx = blockIdx.x * blockDim.x + threadIdx.x, kz = blockIdx.y;
   if (kx >= lh) return;
-  C *S = reinterpret_cast<C *>(d.spec) + kx + (int64_t)d.lp * ny * kz;
-  const double2 *P = d.ypiv + kx + (int64_t)d.lp * ny * kz;
-  const int64_t st = d.lp;
-  C r = S[0];
-  double2 pv = P[0];
-  double gr = (double)r.x * pv.x, gi = (double)r.y * pv.x;
-  { C o; o.x = (T)gr; o.y = (T)gi; S[0] = o; }
-#pragma unroll 8
-  for (int j = 2; j <= ny; ++j) {
-    const double a = d.amph[j];
-    pv = P[st * (j - 1)];
-    r = S[st * (j - 1)];
-    gr = ((double)r.x - a * gr) * pv.x;
-    gi = ((double)r.y - a * gi) * pv.x;
-    C o; o.x = (T)gr; o.y = (T)gi; S[st * (j - 1)] = o;
+  const int64_t base = kx + (int64_t)d.lp * ny * kz, st = d.lp;
+  C *__restrict__ S = reinterpret_cast<C *>(d.spec) + base;
+  const double *__restrict__ PP = reinterpret_cast<const double *>(d.ypiv) + base;
+  const double *__restrict__ HH = reinterpret_cast<const double *>(d.ypiv) + (int64_t)d.lp * ny * d.nz + base;
+  double gr = 0.0, gi = 0.0;
+  for (int j0 = 1; j0 <= ny; j0 += YB) {
+    C r[YB];
+    double p[YB], a[YB];
+#pragma unroll
+    for (int u = 0; u < YB; ++u) {
+      const int j = j0 + u;
+      if (j <= ny) {
+        r[u] = S[st * (j - 1)];
+        p[u] = __ldg(PP + st * (j - 1));
+        a[u] = d.amph[j];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < YB; ++u) {
+      const int j = j0 + u;
+      if (j <= ny) {
+        if (j == 1) {
+          gr = (double)r[u].x * p[u];
+          gi = (double)r[u].y * p[u];
+        } else {
+          gr = ((double)r[u].x - a[u] * gr) * p[u];
+          gi = ((double)r[u].y - a[u] * gi) * p[u];
+        }
+        C o; o.x = (T)gr; o.y = (T)gi;
+        S[st * (j - 1)] = o;
+      }
+    }
   }
-  double xr = gr, xi = gi;
-#pragma unroll 8
-  for (int j = ny - 1; j >= 1; --j) {
-    const double hj = P[st * (j - 1)].y;
-    r = S[st * (j - 1)];
-    xr = (double)r.x - hj * xr;
-    xi = (double)r.y - hj * xi;
-    C o; o.x = (T)xr; o.y = (T)xi; S[st * (j - 1)] = o;
+  double xr = gr, xi = gi;  // x_ny = g_ny
+  for (int j0 = ny - 1; j0 >= 1; j0 -= YB) {
+    C r[YB];
+    double h[YB];
+#pragma unroll
+    for (int u = 0; u < YB; ++u) {
+      const int j = j0 - u;
+      if (j >= 1) {
+        r[u] = S[st * (j - 1)];
+        h[u] = __ldg(HH + st * (j - 1));
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < YB; ++u) {
+      const int j = j0 - u;
+      if (j >= 1) {
+        xr = (double)r[u].x - h[u] * xr;
+        xi = (double)r[u].y - h[u] * xi;
+        C o; o.x = (T)xr; o.y = (T)xi;
+        S[st * (j - 1)] = o;
+      }
+    }
   }
 }
 
@@ -921,7 +985,7 @@ template <typename C> __host__ __device__ constexpr size_t ifftx_smem_bytes(int 
 }
 
 template <typename T, bool BIG>
-__global__ void __launch_bounds__(256, 2) k_ifftx(TGDev d, FFTPlan pl, int lb, int accumulate) {
+__global__ void __launch_bounds__(256, BIG ? 2 : 3) k_ifftx(TGDev d, FFTPlan pl, int lb, int accumulate) {
   typedef typename Cplx<T>::type C;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ uint64_t bar;
@@ -1111,29 +1175,40 @@ int flush_phase_events(chapsim_ctx *c) {
 
 template <typename T> struct Prec {
   typedef typename Cplx<T>::type C;
-  static int max_fftx_lb(int nx) {
+  static int max_fftx_lb(int nx, int dr) {
     int lb = 2;
-    while (lb < 32 && fftx_smem_bytes<C>(nx, lb + 2) <= 110 * 1024) lb += 2;
+    while (lb < 32 && fftx_smem_bytes<C>(nx, lb + 2, dr) <= 110 * 1024) lb += 2;
     return lb;
   }
+  static int dr_rows(const chapsim_ctx *c) { return c->domain == CHAPSIM_IIO ? 1 : 0; }
   static int fftx_lb(const chapsim_ctx *c) {
-    if (c->fft_lb >= 2 && c->fft_lb <= max_fftx_lb(c->d.nx)) return c->fft_lb & ~1;
-    return fftx_lb(c->d.nx);
+    const int dr = dr_rows(c);
+    if (c->fft_lb >= 2 && c->fft_lb <= max_fftx_lb(c->d.nx, dr)) return c->fft_lb & ~1;
+    // rows per block of the forward x transform: the most rows whose inputs
+    // fit in 74 KB (three blocks per SM) when that is at least four rows,
+    // else the most that fit in 110 KB (measured on the 256x192x256 and
+    // 512x192x256 channels)
+    int lb = 2;
+    while (lb < 32 && fftx_smem_bytes<C>(c->d.nx, lb + 2, dr) <= 74 * 1024) lb += 2;
+    return lb >= 4 ? lb : max_fftx_lb(c->d.nx, dr);
   }
-  static int fftx_lb(int nx) {
-    // rows per block of the x transforms: the most rows whose bulk-loaded
-    // inputs fit (measured fastest on the 256x192x256 channel)
-    return max_fftx_lb(nx);
+  // rows per block of the inverse x transform: the most rows whose buffers
+  // fit in 74 KB, so that three blocks share an SM
+  static int ifftx_lb(const chapsim_ctx *c) {
+    int lb = 2;
+    while (lb < 32 && ifftx_smem_bytes<C>(c->d.nx, c->d.lp, lb + 2) <= 74 * 1024) lb += 2;
+    return lb;
   }
-  static size_t fftx_smem(int nx, int lb) { return fftx_smem_bytes<C>(nx, lb); }
+  static size_t fftx_smem(const chapsim_ctx *c, int lb) { return fftx_smem_bytes<C>(c->d.nx, lb, dr_rows(c)); }
   static size_t ifftx_smem(int nx, int lp, int lb) { return ifftx_smem_bytes<C>(nx, lp, lb); }
   static int fftz_lz(int nz) {
-    int lz = (int)(96 * 1024 / ((size_t)2 * (nz + 1) * sizeof(C)));
-    if (lz > 16) lz = 16;
-    if (lz < 1) lz = 1;
+    // lines per block of the z transforms: a power of two up to 16 whose two
+    // buffers fit in 72 KB, so that three blocks share an SM
+    int lz = 16;
+    while (lz > 2 && (size_t)2 * lz * nz * sizeof(C) > 72 * 1024) lz >>= 1;
     return lz;
   }
-  static size_t fftz_smem(int nz, int lz) { return (size_t)2 * lz * (nz + 1) * sizeof(C); }
+  static size_t fftz_smem(int nz, int lz) { return (size_t)2 * lz * nz * sizeof(C); }
   static size_t adiy_smem(int ny) { return (size_t)ny * AY_TL * sizeof(T); }
   static int adix_lb(int nx) {
     int lb = (int)(96 * 1024 / ((size_t)(nx + 1) * sizeof(T)));
@@ -1179,16 +1254,16 @@ template <typename T> struct Prec {
     const int lb = fftx_lb(c);
     dim3 grid((d.ny + lb - 1) / lb, d.nz);
     if (c->fft_big)
-      k_fftx<T, true><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->sp[ns], c->fx, lb, mode);
+      k_fftx<T, true><<<grid, 256, fftx_smem(c, lb), c->stream>>>(d, c->sp[ns], c->fx, lb, mode);
     else
-      k_fftx<T, false><<<grid, 256, fftx_smem(d.nx, lb), c->stream>>>(d, c->sp[ns], c->fx, lb, mode);
+      k_fftx<T, false><<<grid, 256, fftx_smem(c, lb), c->stream>>>(d, c->sp[ns], c->fx, lb, mode);
     LAUNCHED();
     return CHAPSIM_OK;
   }
 
   static int spectral_solve(chapsim_ctx *c, int accumulate, bool mark) {
     TGDev &d = c->d;
-    const int lz = fftz_lz(d.nz), lb = fftx_lb(c);
+    const int lz = fftz_lz(d.nz), lb = ifftx_lb(c);
     if (mark) phase_mark(c, CHAPSIM_PH_FFTZ);
     {
       dim3 grid((d.lh + lz - 1) / lz, d.ny);
@@ -1366,11 +1441,13 @@ int launch_divg(chapsim_ctx *c, int ns) {
   return c->cfg.precision == CHAPSIM_MIXED ? Prec<float>::fftx(c, ns, 0) : Prec<double>::fftx(c, ns, 0);
 }
 
-int launch_pois_io(chapsim_ctx *c, int ns, double *gx, double *gy, double *gz, const double *drho) {
+int launch_pois_io(chapsim_ctx *c, int ns, double *gx, double *gy, double *gz, const double *drho,
+                   bool store_rhs) {
   // the fused divergence of the forward x-transform reads u, v, w: point them
   // at the provisional mass flux for these launches only
   const TGDev saved = c->d;
   c->d.u = gx; c->d.v = gy; c->d.w = gz; c->d.drho = drho;
+  c->d.skip_rhs = store_rhs ? 0 : 1;
   const int rc = Prec<double>::poisson(c, ns, 0);
   c->d = saved;
   return rc;
