@@ -491,8 +491,8 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
       void **tmp[] = {&d.h0[c], &d.rhs[c], &d.dq[c]};
       for (void **f : tmp) {
         // the explicit IO substep needs EXPLT0 only; the semi-implicit one
-        // keeps RHS_io and a solve scratch field per component
-        if (iocfg && f != &d.h0[c] && !iocfg->visc_scheme) continue;
+        // also keeps RHS_io per component
+        if (iocfg && (f == &d.dq[c] || (f == &d.rhs[c] && !iocfg->visc_scheme))) continue;
         if ((rc = dalloc(ctx, &p, n * tsz))) goto fail;
         *f = p;
         cudaMemsetAsync(p, 0, n * tsz, ctx->stream);
@@ -511,7 +511,7 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
       io.visc = iocfg->visc_scheme ? 1 : 0;
       if (io.visc) {
         for (int c = 0; c < 3; ++c)
-          for (double **f : {&io.drhoi[c], &io.si_t[c], &io.stg[c], &io.stg[c + 3]}) {
+          for (double **f : {&io.drhoi[c], &io.stg[c], &io.stg[c + 3]}) {
             if ((rc = dalloc(ctx, &p, n * sizeof(double)))) goto fail;
             *f = (double *)p;
             cudaMemsetAsync(p, 0, n * sizeof(double), ctx->stream);

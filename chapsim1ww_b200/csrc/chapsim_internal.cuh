@@ -63,12 +63,10 @@ struct IODev {
   double *dpg;       // device scalar: DPGRNS of the current substep
   double *part;      // per-block partial sums of the x mass-flux forcing
   unsigned long long *bad;  // table look-ups outside the table
-  // semi-implicit viscous scheme (visthemflg = 1): DRHOI_STG per component,
-  // a second scratch field per component for the cyclic solves, and the wall
-  // coefficients AMVR1 / APVRN of TDMA_COEF
+  // semi-implicit viscous scheme (visthemflg = 1): DRHOI_STG per component
+  // and the wall coefficients AMVR1 / APVRN of TDMA_COEF
   int visc;
   double *drhoi[3];
-  double *si_t[3];
   double *stg[6];  // MU_STG 1-3, RHO_STG 1-3 of the current substep (energy equation on)
   double amvr1, apvrn;
 };

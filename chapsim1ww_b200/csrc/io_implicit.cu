@@ -19,13 +19,13 @@
 // pressure and G_io component c only, and MOMFA_io(c) changes G_io component
 // c only, so the reference's interleaved order gives the same values.
 //
-// Line solves: one thread per line.  x lines march along the contiguous
-// dimension (each thread its own row); z and y lines have consecutive
-// threads on consecutive x, so every step of the march is a coalesced row.
-// The coefficients are formed on the fly from VISCOUSITY and the MU_STG /
-// RHO_STG fields k_si_stg forms once per substep (as MU_Staggered and
-// DENSITY_Staggered do).  The cyclic elimination keeps its h0 and G2 vectors
-// in two scratch fields, the forward-swept G1 in place.
+// Line solves: one warp per line with the line in shared memory
+// (warp_part_solve: chunked elimination, then parallel cyclic reduction of
+// the chunk-end system over shuffles), staged by coalesced loads: x lines are
+// rows, z and y lines come in tiles of consecutive x.  The coefficients are
+// formed from VISCOUSITY and the MU_STG / RHO_STG fields k_si_stg forms once
+// per substep (as MU_Staggered and DENSITY_Staggered do).  Nothing but the
+// right-hand sides and the result crosses global memory.
 #include <cuda_runtime.h>
 
 #include <string>
@@ -45,7 +45,7 @@
 namespace chapsim {
 namespace {
 
-constexpr int SI_BX = 32, SI_BY = 8, SI_LINE = 128;
+constexpr int SI_BX = 32, SI_BY = 8;
 
 __device__ __forceinline__ int wp(int i, int n) { return i + 1 == n ? 0 : i + 1; }
 __device__ __forceinline__ int wm(int i, int n) { return i == 0 ? n - 1 : i - 1; }
@@ -153,10 +153,11 @@ __device__ __forceinline__ Prop make_prop(const TGDev &d, const IODev &io) {
 }
 
 // Convection (CONVECTION_*_io), the split viscous terms (VISCOUS_PAR_EXPLT_*_io)
-// and RHS_MOM_EXPLICIT_io's implicit branch for the three components of one
-// cell: RHS_io -> d.rhs[c], EXPLT0_io updated.  Per-block sums of RHS_x / DYFI
+// and RHS_MOM_EXPLICIT_io's implicit branch for component C of one cell
+// (one launch per component): RHS_io -> d.rhs[C], EXPLT0_io updated.  Per-block sums of RHS_x / DYFI
 // feed DPGRNS.  Row 1 of the v right-hand side is zero (VISCOUS_PAR_EXPLT_Y_io
 // clears RHS_io and nothing writes that row before MOMFA3_Y_io).
+template <int C>
 __global__ void __launch_bounds__(SI_BX *SI_BY) k_io_rhs_si(TGDev d, IODev io, double gam, double roh, double alp,
                                                           int cur) {
   __shared__ double red[SI_BX * SI_BY / 32];
@@ -185,7 +186,7 @@ __global__ void __launch_bounds__(SI_BX *SI_BY) k_io_rhs_si(TGDev d, IODev io, d
     const double wff = d.wff[j], wfb = d.wfb[j], wffp = d.wff[j + 1], wfbp = d.wfb[j + 1];
     const int64_t oxp = ip - i, oxm = im - i, ozp = sz * (kp - k), ozm = sz * (km - k);
     // ------------------------------------------------ x
-    {
+    if (C == 0) {
       const double h11 = ((gx[c + oxp] + gx[c]) * (u[c + oxp] + u[c]) - (gx[c] + gx[c + oxm]) * (u[c] + u[c + oxm])) *
                          (dxi * 0.5 * 0.5);
       const double h12 = ((gy[c + sy] + gy[c + sy + oxm]) * (wffp * u[c + sy] + wfbp * u[c]) -
@@ -240,7 +241,7 @@ __global__ void __launch_bounds__(SI_BX *SI_BY) k_io_rhs_si(TGDev d, IODev io, d
       ((double *)d.rhs[0])[c] = r;
     }
     // ------------------------------------------------ y (rows 2..ny)
-    if (j >= 2) {
+    if (C == 1 && j >= 2) {
       const double h21 = ((wff * gx[c + oxp] + wfb * gx[c + oxp - sy]) * (v[c + oxp] + v[c]) -
                           (wff * gx[c] + wfb * gx[c - sy]) * (v[c] + v[c + oxm])) * (dxi * 0.5);
       const double h22 = ((gy[c + sy] + gy[c]) * (v[c + sy] + v[c]) - (gy[c] + gy[c - sy]) * (v[c] + v[c - sy])) *
@@ -291,11 +292,11 @@ __global__ void __launch_bounds__(SI_BX *SI_BY) k_io_rhs_si(TGDev d, IODev io, d
       r -= (p[c] - p[c - sy]) * (alp * dt * dycj);
       if (io.gravdir == 2) r += P.r2(i, j, k) * (alp * dt * io.f_a);
       ((double *)d.rhs[1])[c] = r;
-    } else {
+    } else if (C == 1) {
       ((double *)d.rhs[1])[c] = 0.0;
     }
     // ------------------------------------------------ z
-    {
+    if (C == 2) {
       const double h31 = ((gx[c + oxp] + gx[c + oxp + ozm]) * (w[c + oxp] + w[c]) -
                           (gx[c] + gx[c + ozm]) * (w[c] + w[c + oxm])) * (dxi * 0.5 * 0.5);
       const double h32 = ((gy[c + sy] + gy[c + sy + ozm]) * (wffp * w[c + sy] + wfbp * w[c]) -
@@ -348,15 +349,17 @@ __global__ void __launch_bounds__(SI_BX *SI_BY) k_io_rhs_si(TGDev d, IODev io, d
       ((double *)d.rhs[2])[c] = r;
     }
   }
-  // fixed-order block sum of RHS_x / DYFI
-  for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-  const int tid = threadIdx.x + SI_BX * threadIdx.y;
-  if ((tid & 31) == 0) red[tid >> 5] = part;
-  __syncthreads();
-  if (tid == 0) {
-    double s = 0.0;
-    for (int q = 0; q < SI_BX * SI_BY / 32; ++q) s += red[q];
-    io.part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = s;
+  if (C == 0) {
+    // fixed-order block sum of RHS_x / DYFI
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    const int tid = threadIdx.x + SI_BX * threadIdx.y;
+    if ((tid & 31) == 0) red[tid >> 5] = part;
+    __syncthreads();
+    if (tid == 0) {
+      double s = 0.0;
+      for (int q = 0; q < SI_BX * SI_BY / 32; ++q) s += red[q];
+      io.part[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = s;
+    }
   }
 }
 
@@ -393,72 +396,6 @@ __device__ __forceinline__ void cyc_coef(const Prop &P, int i, int j, int k, dou
   a = amu / rm;
   cc = apu / rp;
   b = 1.0 - (amu + apu) / rc;
-}
-
-// TDMAIJI_CYC along x (X) or z for component C: one thread per line.  The
-// first n-1 unknowns are G1 + G2 x(n) (G1 swept in place in R, h0 in H, G2
-// in T); the last row gives x(n).  For x-momentum the x sweep subtracts
-// DPGRNS from RHS_io as it reads it.
-template <int C, bool X>
-__global__ void __launch_bounds__(SI_LINE) k_io_cyc(TGDev d, IODev io, double coe1, double coe2, int use_dpg) {
-  const int j0 = C == 1 ? 2 : 1, nj = d.ny - j0 + 1;
-  const int t = blockIdx.x * SI_LINE + threadIdx.x;
-  int i = 0, j, k = 0;
-  if (X) {
-    if (t >= nj * d.nz) return;
-    j = j0 + t % nj;
-    k = t / nj;
-  } else {
-    if (t >= nj * d.nx) return;
-    i = t % d.nx;
-    j = j0 + t / d.nx;
-  }
-  const Prop P = make_prop(d, io);
-  const int n = X ? d.nx : d.nz;
-  const int64_t st = X ? 1 : d.sz;
-  const int64_t base = (int64_t)i + d.sy * j + d.sz * k;
-  double *__restrict__ R = (double *)d.rhs[C] + base;
-  double *__restrict__ H = (double *)d.dq[C] + base;
-  double *__restrict__ T = io.si_t[C] + base;
-  const double sub = (X && C == 0 && use_dpg) ? *io.dpg : 0.0;
-  double a, b, cc;
-  auto coef = [&](int m) {
-    if (X) cyc_coef<C, true>(P, m, j, k, coe1, coe2, a, b, cc);
-    else cyc_coef<C, false>(P, i, j, m, coe1, coe2, a, b, cc);
-  };
-  coef(0);
-  double h = cc / b, g1 = (R[0] - sub) / b, g2 = -a / b;
-  H[0] = h; R[0] = g1; T[0] = g2;
-  for (int m = 1; m <= n - 3; ++m) {
-    coef(m);
-    const double pp = 1.0 / (b - h * a);
-    const double qq1 = g1 * a, qq2 = g2 * a;
-    h = cc * pp;
-    g1 = ((R[st * m] - sub) - qq1) * pp;
-    g2 = -qq2 * pp;
-    H[st * m] = h; R[st * m] = g1; T[st * m] = g2;
-  }
-  {
-    const int m = n - 2;
-    coef(m);
-    const double pp = 1.0 / (b - h * a);
-    const double qq1 = g1 * a, qq2 = g2 * a;
-    g1 = ((R[st * m] - sub) - qq1) * pp;
-    g2 = (-cc - qq2) * pp;
-    R[st * m] = g1; T[st * m] = g2;
-  }
-  const double g1l = g1, g2l = g2;  // values at n-2, unchanged by the back substitution
-  for (int m = n - 3; m >= 0; --m) {
-    const double hm = H[st * m];
-    g1 = -hm * g1 + R[st * m];
-    g2 = -hm * g2 + T[st * m];
-    R[st * m] = g1; T[st * m] = g2;
-  }
-  coef(n - 1);
-  const double rl = R[st * (n - 1)] - sub;
-  const double xn = (rl - cc * g1 - a * g1l) / (b + cc * g2 + a * g2l);
-  R[st * (n - 1)] = xn;
-  for (int m = n - 2; m >= 0; --m) R[st * m] = R[st * m] + T[st * m] * xn;
 }
 
 // MOMFA3_Y_io coefficients of row j (1..ny), component C.
@@ -501,38 +438,182 @@ __device__ __forceinline__ void y_coef(const TGDev &d, const IODev &io, const Pr
   b = 1.0 - (amu + apu) / den;
 }
 
-// TDMAIJJ_nonCYC along y (rows 1..ny, zero boundary values) for component C,
-// then G* = G + dG into the other G buffer from row N2I.
-template <int C>
-__global__ void __launch_bounds__(SI_LINE) k_io_ysi(TGDev d, IODev io, double facoe, int cur) {
-  const int t = blockIdx.x * SI_LINE + threadIdx.x;
-  if (t >= d.nx * d.nz) return;
-  const int i = t % d.nx, k = t / d.nx, ny = d.ny;
-  const Prop P = make_prop(d, io);
-  const int64_t sy = d.sy, base = (int64_t)i + d.sz * k;
-  double *__restrict__ R = (double *)d.rhs[C] + base;
-  double *__restrict__ H = (double *)d.dq[C] + base;
-  double a, b, cc;
-  y_coef<C>(d, io, P, i, 1, k, facoe, a, b, cc);
-  double h = cc / b, g = R[sy] / b;
-  H[sy] = h; R[sy] = g;
-  for (int j = 2; j <= ny - 1; ++j) {
-    y_coef<C>(d, io, P, i, j, k, facoe, a, b, cc);
-    const double pp = 1.0 / (b - h * a);
-    h = cc * pp;
-    g = (R[sy * j] - a * g) * pp;
-    H[sy * j] = h; R[sy * j] = g;
+// ------------------------------------------------------------ line solves
+// Warp partition solver for one tridiagonal line of n unknowns,
+// a x(i-1) + b x(i) + c x(i+1) = r, cyclic (CYC) or with a(0) = c(n-1) = 0.
+// The line is split into P equal chunks of m = n / P (P a power of two, at
+// most 32, m >= 2: part_count).  Lane p eliminates its chunk's first m-1
+// unknowns in terms of the chunk-end values L(p-1) and L(p) (one Thomas sweep
+// with three right-hand sides), which leaves a P-unknown tridiagonal system
+// for the chunk ends, cyclic when the line is; parallel cyclic reduction over
+// shuffles solves it; then every lane back-substitutes its chunk.  The
+// arrays live in shared memory with element i = p m + t at t P + p, so the
+// lanes' sweeps touch consecutive words.  The result overwrites R.
+__host__ __device__ inline int part_count(int n) {
+  int P = 1;
+  while (P < 32 && n % (2 * P) == 0 && n / (2 * P) >= 2) P *= 2;
+  return P;
+}
+__device__ __forceinline__ int part_slot(int i, int m, int P) { return (i % m) * P + i / m; }
+
+template <bool CYC>
+__device__ void warp_part_solve(double *__restrict__ A, double *__restrict__ B, double *__restrict__ Cc,
+                                double *__restrict__ R, int P, int m, int lane) {
+  const bool act = lane < P;
+  double yl = 0.0, vl = 0.0, wl = 0.0, yf = 0.0, vf = 0.0, wf = 0.0;
+  double ae = 0.0, be = 1.0, ce = 0.0, re = 0.0;
+  if (act) {
+    double h = 0.0, y = 0.0, v = 0.0, w = 0.0;
+    for (int t = 0; t <= m - 2; ++t) {
+      const int q = t * P + lane;
+      const double a = A[q], b = B[q], c = Cc[q], r = R[q];
+      const double al = t == 0 ? 0.0 : a;       // first row: a couples to L(p-1)
+      const double cu = t == m - 2 ? 0.0 : c;   // last interior row: c couples to L(p)
+      const double inv = 1.0 / (b - al * h);
+      h = cu * inv;
+      y = (r - al * y) * inv;
+      v = ((t == 0 ? -a : 0.0) - al * v) * inv;
+      w = ((t == m - 2 ? -c : 0.0) - al * w) * inv;
+      Cc[q] = h; R[q] = y; A[q] = v; B[q] = w;
+    }
+    yl = y; vl = v; wl = w;
+    for (int t = m - 3; t >= 0; --t) {
+      const int q = t * P + lane;
+      const double hq = Cc[q];
+      y = R[q] - hq * y;
+      v = A[q] - hq * v;
+      w = B[q] - hq * w;
+      R[q] = y; A[q] = v; B[q] = w;
+    }
+    yf = y; vf = v; wf = w;
+    const int qe = (m - 1) * P + lane;
+    ae = A[qe]; be = B[qe]; ce = Cc[qe]; re = R[qe];
   }
-  y_coef<C>(d, io, P, i, ny, k, facoe, a, b, cc);
-  const double pp = 1.0 / (b - h * a);
-  double x = (R[sy * ny] - a * g) * pp;
-  const double *__restrict__ G = io.g[cur][C] + base;
-  double *__restrict__ Gn = io.g[1 - cur][C] + base;
+  const unsigned full = 0xffffffffu;
+  const int nxt = act ? (lane + 1) % P : lane;
+  const double yn = __shfl_sync(full, yf, nxt), vn = __shfl_sync(full, vf, nxt), wn = __shfl_sync(full, wf, nxt);
+  // chunk-end equation: row e with x(e-1) = yl + vl L(p-1) + wl L(p) and
+  // x(e+1) = yn + vn L(p) + wn L(p+1)
+  double Ap = ae * vl, Bp = ae * wl + be + ce * vn, Cp = ce * wn, Rp = re - ae * yl - ce * yn;
+  if (!act) { Ap = 0.0; Bp = 1.0; Cp = 0.0; Rp = 0.0; }
+  for (int hs = 1; hs < P; hs <<= 1) {
+    const int lm = act ? (lane - hs + P) % P : lane, lp = act ? (lane + hs) % P : lane;
+    double Am = __shfl_sync(full, Ap, lm), Bm = __shfl_sync(full, Bp, lm), Cm = __shfl_sync(full, Cp, lm),
+           Rm = __shfl_sync(full, Rp, lm);
+    double Aq = __shfl_sync(full, Ap, lp), Bq = __shfl_sync(full, Bp, lp), Cq = __shfl_sync(full, Cp, lp),
+           Rq = __shfl_sync(full, Rp, lp);
+    if (!CYC) {
+      if (lane - hs < 0) { Am = 0.0; Bm = 1.0; Cm = 0.0; Rm = 0.0; }
+      if (lane + hs >= P) { Aq = 0.0; Bq = 1.0; Cq = 0.0; Rq = 0.0; }
+    }
+    if (act) {
+      const double k1 = Ap / Bm, k2 = Cp / Bq;
+      const double nA = -Am * k1, nC = -Cq * k2;
+      const double nB = Bp - Cm * k1 - Aq * k2;
+      const double nR = Rp - Rm * k1 - Rq * k2;
+      Ap = nA; Bp = nB; Cp = nC; Rp = nR;
+    }
+  }
+  // couplings now reach distance P: the unknown itself (cyclic) or nothing
+  const double L = CYC ? Rp / (Ap + Bp + Cp) : Rp / Bp;
+  double Lm = __shfl_sync(full, L, act ? (lane - 1 + P) % P : lane);
+  if (!CYC && lane == 0) Lm = 0.0;
+  if (act) {
+    for (int t = 0; t <= m - 2; ++t) {
+      const int q = t * P + lane;
+      R[q] = R[q] + A[q] * Lm + B[q] * L;
+    }
+    R[(m - 1) * P + lane] = L;
+  }
+}
+
+// MOMFA1_X_io (TDMAIJI_CYC along x) for component C: one warp per (j, k) row;
+// the row and its coefficients are staged in shared memory with coalesced
+// loads, solved by warp_part_solve and written back in place.  x-momentum
+// subtracts DPGRNS from RHS_io as it is read.
+template <int C>
+__global__ void __launch_bounds__(256) k_si_x(TGDev d, IODev io, double coe1, double coe2, int use_dpg) {
+  extern __shared__ double xs_smem[];
+  const int nx = d.nx, j0 = C == 1 ? 2 : 1, nj = d.ny - j0 + 1;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int line = blockIdx.x * nw + warp;
+  if (line >= nj * d.nz) return;  // whole warp leaves together
+  const int j = j0 + line % nj, k = line / nj;
+  const int P = part_count(nx), m = nx / P;
+  double *A = xs_smem + (size_t)warp * 4 * nx, *B = A + nx, *Cc = B + nx, *Rs = Cc + nx;
+  const Prop Pr = make_prop(d, io);
+  double *__restrict__ R = (double *)d.rhs[C] + d.sy * j + d.sz * k;
+  const double sub = (C == 0 && use_dpg) ? *io.dpg : 0.0;
+#pragma unroll 4
+  for (int i = lane; i < nx; i += 32) {
+    double a, b, cc;
+    cyc_coef<C, true>(Pr, i, j, k, coe1, coe2, a, b, cc);
+    const int q = part_slot(i, m, P);
+    A[q] = a; B[q] = b; Cc[q] = cc; Rs[q] = R[i] - sub;
+  }
+  __syncwarp();
+  warp_part_solve<true>(A, B, Cc, Rs, P, m, lane);
+  __syncwarp();
+  for (int i = lane; i < nx; i += 32) R[i] = Rs[part_slot(i, m, P)];
+}
+
+// Lines along z (MOMFA2_Z_io, cyclic) or y (MOMFA3_Y_io, rows 1..ny, zero
+// boundary values) for component C: a block stages LB lines of consecutive x
+// (each row of the tile one coalesced load), its warps solve them in turn.
+// The y solve ends with G* = G + dG in the other G buffer from row N2I.
+template <int C, bool Y>
+__global__ void __launch_bounds__(256) k_si_zy(TGDev d, IODev io, double coe1, double coe2, int LB, int cur) {
+  extern __shared__ double zs_smem[];
+  const int nx = d.nx, ny = d.ny;
+  const int n = Y ? ny : d.nz;
   const int j0 = C == 1 ? 2 : 1;
-  Gn[sy * ny] = x + G[sy * ny];
-  for (int j = ny - 1; j >= 1; --j) {
-    x = R[sy * j] - H[sy * j] * x;
-    if (j >= j0) Gn[sy * j] = x + G[sy * j];
+  const int i0 = blockIdx.x * LB;
+  const int nl = min(LB, nx - i0);
+  // z lines: blockIdx.y = row j - j0; y lines: blockIdx.y = plane k
+  const int jz = Y ? 0 : j0 + (int)blockIdx.y, ky = Y ? (int)blockIdx.y : 0;
+  const int P = part_count(n), m = n / P;
+  const Prop Pr = make_prop(d, io);
+  const int64_t st = Y ? d.sy : d.sz;
+  const int64_t base = Y ? d.sz * ky : d.sy * jz;  // + i, + st * (index along the line)
+  double *__restrict__ R = (double *)d.rhs[C];
+#pragma unroll 4
+  for (int t = threadIdx.x; t < n * nl; t += blockDim.x) {
+    const int e = t / nl, l = t - e * nl, i = i0 + l;
+    double a, b, cc;
+    int64_t g;
+    if (Y) {
+      const int j = e + 1;
+      y_coef<C>(d, io, Pr, i, j, ky, coe1, a, b, cc);
+      if (j == 1) a = 0.0;    // zero boundary values: the end couplings drop
+      if (j == ny) cc = 0.0;
+      g = i + base + st * j;
+    } else {
+      cyc_coef<C, false>(Pr, i, jz, e, coe1, coe2, a, b, cc);
+      g = i + base + st * e;
+    }
+    double *L = zs_smem + (size_t)l * 4 * n;
+    const int q = part_slot(e, m, P);
+    L[q] = a; L[n + q] = b; L[2 * n + q] = cc; L[3 * n + q] = R[g];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int l = warp; l < nl; l += nw) {
+    double *L = zs_smem + (size_t)l * 4 * n;
+    warp_part_solve<!Y>(L, L + n, L + 2 * n, L + 3 * n, P, m, lane);
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < n * nl; t += blockDim.x) {
+    const int e = t / nl, l = t - e * nl, i = i0 + l;
+    const double x = zs_smem[(size_t)l * 4 * n + 3 * n + part_slot(e, m, P)];
+    if (Y) {
+      const int j = e + 1;
+      if (j >= j0) {
+        const int64_t g = i + base + st * j;
+        io.g[1 - cur][C][g] = x + io.g[cur][C][g];
+      }
+    } else {
+      R[i + base + st * e] = x;
+    }
   }
 }
 
@@ -551,7 +632,12 @@ int io_mom_si(chapsim_ctx *c, int ns, int *npart) {
     k_si_stg<<<dim3(grid.x, (d.ny + 2 + SI_BY - 1) / SI_BY, d.nz), dim3(SI_BX, SI_BY), 0, c->stream>>>(d, io);
     LAUNCHED();
   }
-  k_io_rhs_si<<<grid, dim3(SI_BX, SI_BY), 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, c->io_cur);
+  // one kernel per component: a third of the live values each
+  k_io_rhs_si<0><<<grid, dim3(SI_BX, SI_BY), 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, c->io_cur);
+  LAUNCHED();
+  k_io_rhs_si<1><<<grid, dim3(SI_BX, SI_BY), 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, c->io_cur);
+  LAUNCHED();
+  k_io_rhs_si<2><<<grid, dim3(SI_BX, SI_BY), 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, c->io_cur);
   LAUNCHED();
   *npart = (int)(grid.x * grid.y * grid.z);
   return CHAPSIM_OK;
@@ -559,35 +645,63 @@ int io_mom_si(chapsim_ctx *c, int ns, int *npart) {
 
 // MOMFA_io for the three components: x, z and y factor solves, G* into the
 // other G buffer.
-int io_factor_si(chapsim_ctx *c, int ns) {
+namespace {
+int zy_lines_per_block(int n) {
+  // lines of one z / y block: as many as fit in 100 KB (4 arrays of n values)
+  int lb = (int)(100 * 1024 / ((size_t)32 * n));
+  return lb < 1 ? 1 : (lb > 32 ? 32 : lb);
+}
+template <int C>
+int si_solves(chapsim_ctx *c, double facoe, double cx1, double cx2, double cz1, double cz2) {
   TGDev &d = c->d;
   IODev &io = c->io;
+  const int j0 = C == 1 ? 2 : 1, nj = d.ny - j0 + 1;
+  {
+    // rows per block: as many as fit in 110 KB (4 arrays of nx values each)
+    int wpb = (int)(110 * 1024 / ((size_t)32 * d.nx));
+    wpb = wpb < 1 ? 1 : (wpb > 8 ? 8 : wpb);
+    const size_t sm = (size_t)wpb * 4 * d.nx * sizeof(double);
+    k_si_x<C><<<(nj * d.nz + wpb - 1) / wpb, 32 * wpb, sm, c->stream>>>(d, io, cx1, cx2, 1);
+    LAUNCHED();
+  }
+  {
+    const int lb = zy_lines_per_block(d.nz);
+    k_si_zy<C, false><<<dim3((d.nx + lb - 1) / lb, nj), 256, (size_t)lb * 4 * d.nz * sizeof(double), c->stream>>>(
+        d, io, cz1, cz2, lb, c->io_cur);
+    LAUNCHED();
+  }
+  {
+    const int lb = zy_lines_per_block(d.ny);
+    k_si_zy<C, true><<<dim3((d.nx + lb - 1) / lb, d.nz), 256, (size_t)lb * 4 * d.ny * sizeof(double), c->stream>>>(
+        d, io, facoe, 0.0, lb, c->io_cur);
+    LAUNCHED();
+  }
+  return CHAPSIM_OK;
+}
+}  // namespace
+
+int io_factor_si(chapsim_ctx *c, int ns) {
+  TGDev &d = c->d;
   const double facoe = 0.5 * c->sp[ns].alp * d.dt * d.cvisc;  // FACOE_io
   const double cx1 = facoe * 4.0 / 3.0 * d.dxqi, cx2 = facoe * d.dxqi;
   const double cz1 = facoe * 4.0 / 3.0 * d.dzqi, cz2 = facoe * d.dzqi;
-  const int nl1 = d.ny * d.nz, nl2 = (d.ny - 1) * d.nz;
-  const int zl1 = d.ny * d.nx, zl2 = (d.ny - 1) * d.nx;
-  auto blocks = [](int n) { return (n + SI_LINE - 1) / SI_LINE; };
-  k_io_cyc<0, true><<<blocks(nl1), SI_LINE, 0, c->stream>>>(d, io, cx1, cx2, 1);
-  LAUNCHED();
-  k_io_cyc<1, true><<<blocks(nl2), SI_LINE, 0, c->stream>>>(d, io, cx1, cx2, 0);
-  LAUNCHED();
-  k_io_cyc<2, true><<<blocks(nl1), SI_LINE, 0, c->stream>>>(d, io, cx1, cx2, 0);
-  LAUNCHED();
-  k_io_cyc<0, false><<<blocks(zl1), SI_LINE, 0, c->stream>>>(d, io, cz1, cz2, 0);
-  LAUNCHED();
-  k_io_cyc<1, false><<<blocks(zl2), SI_LINE, 0, c->stream>>>(d, io, cz1, cz2, 0);
-  LAUNCHED();
-  k_io_cyc<2, false><<<blocks(zl1), SI_LINE, 0, c->stream>>>(d, io, cz1, cz2, 0);
-  LAUNCHED();
-  const int yl = d.nx * d.nz;
-  k_io_ysi<0><<<blocks(yl), SI_LINE, 0, c->stream>>>(d, io, facoe, c->io_cur);
-  LAUNCHED();
-  k_io_ysi<1><<<blocks(yl), SI_LINE, 0, c->stream>>>(d, io, facoe, c->io_cur);
-  LAUNCHED();
-  k_io_ysi<2><<<blocks(yl), SI_LINE, 0, c->stream>>>(d, io, facoe, c->io_cur);
-  LAUNCHED();
-  return CHAPSIM_OK;
+  static unsigned attrs = 0;  // devices whose solve kernels got the shared-memory limit
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 32 && !(attrs & (1u << dev))) {  // dynamic shared memory above 48 KB, process wide
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const void *fns[] = {(const void *)k_si_x<0>, (const void *)k_si_x<1>, (const void *)k_si_x<2>,
+                         (const void *)k_si_zy<0, false>, (const void *)k_si_zy<1, false>,
+                         (const void *)k_si_zy<2, false>, (const void *)k_si_zy<0, true>,
+                         (const void *)k_si_zy<1, true>, (const void *)k_si_zy<2, true>};
+    for (const void *f : fns) cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    attrs |= 1u << dev;
+  }
+  int rc;
+  if ((rc = si_solves<0>(c, facoe, cx1, cx2, cz1, cz2))) return rc;
+  if ((rc = si_solves<1>(c, facoe, cx1, cx2, cz1, cz2))) return rc;
+  return si_solves<2>(c, facoe, cx1, cx2, cz1, cz2);
 }
 
 }  // namespace chapsim
