@@ -5,8 +5,10 @@ Run from the repository root:  python tests/golden/make_golden.py
 The fixtures come from the independent numpy restatements in numpy_tg.py
 (FFT circulant solves and banded LU instead of the reference's Thomas
 sweeps) and numpy_io.py (complex FFTs and banded LU instead of FISHPACK's
-real transforms and TRID0 sweeps), so they pin the C++ oracle and the CUDA
-library against a second implementation of the same algorithm.  The
+real transforms and TRID0 sweeps; batched dense LU instead of TDMAIJI_CYC and
+TDMAIJJ_nonCYC for the semi-implicit scheme's factor solves), so they pin the
+C++ oracle and the CUDA library against a second implementation of the same
+algorithm.  The
 reference itself (Fortran + MPI) cannot be built in this environment and
 ships no golden data.
 """
@@ -28,9 +30,13 @@ CASES = {
 }
 
 IO_CASES = {
-    # name: (nx, ny, nz, lx, lz, ren, dt, seed, amp, steps, thermal, prt, qw_bot, qw_top)
+    # name: (nx, ny, nz, lx, lz, ren, dt, seed, amp, steps, thermal, prt, qw_bot, qw_top[, visc_scheme])
     "io_16x12x8_seed3": (16, 12, 8, 4 * math.pi, 4 * math.pi / 3, 2800.0, 1e-3, 3, 0.1, 2, 0, 0.71, 0.0, 0.0),
     "io_heated_16x10x8_seed7": (16, 10, 8, 8 * math.pi, 4 * math.pi / 3, 2000.0, 2e-3, 7, 0.1, 2, 1, 0.71, 1.0, 0.6),
+    # the semi-implicit viscous scheme (visthemflg = 1)
+    "io_si_16x12x8_seed3": (16, 12, 8, 4 * math.pi, 4 * math.pi / 3, 1500.0, 2e-3, 3, 0.1, 2, 0, 0.71, 0.0, 0.0, 1),
+    "io_si_heated_16x10x8_seed7": (16, 10, 8, 8 * math.pi, 4 * math.pi / 3, 2000.0, 2e-3, 7, 0.1, 2, 1, 0.71, 1.0,
+                                   0.6, 1),
 }
 
 
@@ -49,10 +55,10 @@ def run_case(nx, ny, nz, lx, lz, ren, dt, seed, amp, steps):
     return out
 
 
-def run_io_case(nx, ny, nz, lx, lz, ren, dt, seed, amp, steps, thermal, prt, qw_bot, qw_top):
+def run_io_case(nx, ny, nz, lx, lz, ren, dt, seed, amp, steps, thermal, prt, qw_bot, qw_top, visc_scheme=0):
     """Initial field + CALC_INITIALIZATION_io (the state after NS = 0), then
     `steps` full RK3 steps."""
-    t = IO(nx, ny, nz, lx, lz, ren=ren, dt=dt, thermal=thermal, prt=prt, qw=(qw_bot, qw_top))
+    t = IO(nx, ny, nz, lx, lz, ren=ren, dt=dt, thermal=thermal, prt=prt, qw=(qw_bot, qw_top), visc_scheme=visc_scheme)
     t.init_random(seed, amp)
     out = {"ns0_gx": t.g[1].copy(), "ns0_gy": t.g[2].copy(), "ns0_p": t.p.copy()}
     for _ in range(steps):

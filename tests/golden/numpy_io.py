@@ -5,8 +5,10 @@ section, written to cross-check the C++ oracle.  It differs from the oracle
 in every non-trivial step: the stencils are whole-array shifts, the FISHPACK
 Poisson solve (real RFFTF/RFFTB transforms and a TRID0 sweep per mode in the
 reference) is done with complex numpy FFTs in x and z and scipy's banded LU
-per (kx, kz) mode, the table splines are built and evaluated with numpy
-(searchsorted), and the synthetic property table is integrated with numpy.
+per (kx, kz) mode, the semi-implicit scheme's MOMFA_io factors (TDMAIJI_CYC
+and TDMAIJJ_nonCYC in the reference) by batched dense LU, the table splines
+are built and evaluated with numpy (searchsorted), and the synthetic
+property table is integrated with numpy.
 
 Arrays are numpy views of the Fortran layout F(1:nx, 0:ny+1, 1:nz): shape
 (nz, ny+2, nx), so a[k-1, j, i-1] is F(i, j, k).
@@ -22,7 +24,11 @@ src/VISCOUS_Y_EXPLICIT_io.f90 and src/VISCOUS_Z_EXPLICIT_io.f90 (channel
 branches), src/RHS_MOM_EXPLICIT_io.f90:1-297,
 src/possion3d_fishpack_reform.f90:29-547, src/PRESSURE_CORRECTION.f90:86-122,
 src/VELO_CORRECTION.f90:107-185, src/INITIAL_FL_THEML_FLD_io.f90:133-172,
-352-381,481-560,653-682.
+352-381,481-560,653-682; the semi-implicit scheme (visthemflg = 1):
+src/VISCOUS_X_EXPLICIT_io.f90:124-286, src/VISCOUS_Y_EXPLICIT_io.f90:264-424,
+src/VISCOUS_Z_EXPLICIT_io.f90:289-460, src/RHS_MOM_EXPLICIT_io.f90:79-95,
+src/MOMFA_io.f90:17-377, src/TDMA_COEF.f90:77-116,
+src/MASSFLUX_CALC_IO.f90:316-399, src/PRESSURE_CORRECTION.f90:100-110.
 
 The decisions shared with the oracle and the library: the Poisson mean mode
 takes phi(ny) = 0; the reference-state shortcuts of the table look-ups are
@@ -106,9 +112,10 @@ class IO(TG):
     the y mesh and the Poisson y-operator are the TG restatement's."""
 
     def __init__(self, nx, ny, nz, lx, lz, str2=2.0, istr2=1, ren=2800.0, dt=1e-3, thermal=0, prt=0.71,
-                 qw=(1.0, 1.0), table=None):
+                 qw=(1.0, 1.0), table=None, visc_scheme=0):
         super().__init__(nx, ny, nz, lx, lz, str2=str2, istr2=istr2, ren=ren, dt=dt)
-        self.thermal, self.qw = thermal, qw
+        self.thermal, self.qw, self.visc = thermal, qw, visc_scheme
+        self.drhoi = {c: np.zeros((nz, ny + 2, nx)) for c in (1, 2, 3)}
         self.cvisc, self.cthecd = 1.0 / ren, 1.0 / ren / prt
         shape = (nz, ny + 2, nx)
         z = lambda: np.zeros(shape)
@@ -232,12 +239,21 @@ class IO(TG):
 
     # ---------------------------------------------------------- momentum
     def prep(self, ns):
-        """DENSITY_TIME_DERIVATION (thermal), then VELOCITY_CALC_io: u = G / rho_stag."""
+        """DENSITY_TIME_DERIVATION (thermal), DENSITY_implicit_add (thermal,
+        semi-implicit scheme), then VELOCITY_CALC_io: u = G / rho_stag."""
         if self.thermal:
             self.interior(self.drho, ((TGAM[ns] + TROH[ns]) * self.div(self.g) + TROH[ns] * self.div(self.g0)) /
                           (TGAM[ns] - 2.0))
         X, G = self.X, self.g
         rx, ry, rz = self.rho_stg()
+        if self.thermal and self.visc:
+            D0 = self.D0
+            for c in (1, 2, 3):
+                self.drhoi[c][:] = 0.0
+            self.interior(self.drhoi[1], 1.0 / rx - 1.0 / ((X(D0) + X(D0, -1)) * 0.5))
+            self.interior(self.drhoi[3], 1.0 / rz - 1.0 / ((X(D0) + X(D0, 0, 0, -1)) * 0.5))
+            d2 = 1.0 / ry - 1.0 / (self.row(self.wff) * X(D0) + self.row(self.wfb) * X(D0, 0, -1))
+            self.drhoi[2][:, 2:self.ny + 1, :] = d2[:, 1:, :]
         self.interior(self.q[1], X(G[1]) / rx)
         self.interior(self.q[3], X(G[3]) / rz)
         self.q[2][:, 2:self.ny + 1, :] = (X(G[2]) / ry)[:, 1:, :]
@@ -277,7 +293,7 @@ class IO(TG):
                S1() * ((X(u) - X(u, 0, -1)) * dycj + (X(v) - X(v, -1)) * dxi)) * (dyfj * cv)
         d13 = (S2(0, 0, 1) * ((X(u, 0, 0, 1) - X(u)) * dzi + (X(w, 0, 0, 1) - X(w, -1, 0, 1)) * dxi) -
                S2() * ((X(u) - X(u, 0, 0, -1)) * dzi + (X(w) - X(w, -1)) * dxi)) * (dzi * cv)
-        ex = ex + d11 + d12 + d13
+        ex_conv, ex = ex, ex + d11 + d12 + d13
         # y-momentum at the v faces (row 1 is the wall and is dropped)
         ey = -(((wff * X(gx, 1) + wfb * X(gx, 1, -1)) * (X(v, 1) + X(v)) -
                 (wff * X(gx) + wfb * X(gx, 0, -1)) * (X(v) + X(v, -1))) * (dxi * 0.5) +
@@ -289,7 +305,7 @@ class IO(TG):
         d22 = (M() * ((X(v, 0, 1) - X(v)) * dyfj - divu()) - M(0, -1) * ((X(v) - X(v, 0, -1)) * dyfm - divu(0, -1))) * (2.0 * dycj * cv)
         d23 = (S3(0, 0, 1) * ((X(v, 0, 0, 1) - X(v)) * dzi + (X(w, 0, 0, 1) - X(w, 0, -1, 1)) * dycj) -
                S3() * ((X(v) - X(v, 0, 0, -1)) * dzi + (X(w) - X(w, 0, -1)) * dycj)) * (dzi * cv)
-        ey = ey + d21 + d22 + d23
+        ey_conv, ey = ey, ey + d21 + d22 + d23
         # z-momentum at the w faces
         ez = -(((X(gx, 1) + X(gx, 1, 0, -1)) * (X(w, 1) + X(w)) - (X(gx) + X(gx, 0, 0, -1)) * (X(w) + X(w, -1))) * (dxi * 0.25) +
                ((X(gy, 0, 1) + X(gy, 0, 1, -1)) * (wffp * X(w, 0, 1) + wfbp * X(w)) -
@@ -300,7 +316,10 @@ class IO(TG):
         d32 = (S3(0, 1) * ((X(w, 0, 1) - X(w)) * dycp + (X(v, 0, 1) - X(v, 0, 1, -1)) * dzi) -
                S3() * ((X(w) - X(w, 0, -1)) * dycj + (X(v) - X(v, 0, 0, -1)) * dzi)) * (dyfj * cv)
         d33 = (M() * ((X(w, 0, 0, 1) - X(w)) * dzi - divu()) - M(0, 0, -1) * ((X(w) - X(w, 0, 0, -1)) * dzi - divu(0, 0, -1))) * (2.0 * dzi * cv)
-        ez = ez + d31 + d32 + d33
+        ez_conv, ez = ez, ez + d31 + d32 + d33
+        if self.visc:
+            self.mom_semi_implicit(ns, ex_conv, ey_conv, ez_conv)
+            return
         # RK3 combination and pressure gradient
         p, dt, alp = self.p, self.dt, TALP[ns]
         rx = (TGAM[ns] * ex + TROH[ns] * X(self.ex0[1])) * dt - (X(p) - X(p, -1)) * (alp * dt * dxi)
@@ -314,18 +333,241 @@ class IO(TG):
         gz[:, 1:ny + 1, :] += rz
         gy[:, 2:ny + 1, :] += ry[:, 1:, :]
         self.bc_vec(self.g)
-        # projection
-        phi = self.poisson_io((self.div(self.g) + X(self.drho)) / (dt * alp))
+        self.project(ns)
+
+    def project(self, ns):
+        """DIVG_io, the FISHPACK solve, PRCALC_io (the semi-implicit branch with
+        the physical right-hand side), MASSFLUX_UPDATE_IO."""
+        ny, X, row = self.ny, self.X, self.row
+        p, dt, alp = self.p, self.dt, TALP[ns]
+        gx, gy, gz = self.g[1], self.g[2], self.g[3]
+        dxi, dzi, dycj = self.dxi, self.dzi, row(self.dyci)
+        rhs = (self.div(self.g) + X(self.drho)) / (dt * alp)
+        phi = self.poisson_io(rhs)
         self.phi[:] = 0.0
         self.interior(self.phi, phi)
         self.bc_copy(self.phi)
-        self.interior(p, X(p) + X(self.phi))
+        if self.visc:
+            self.interior(p, X(p) + X(self.phi) - 0.5 * alp * dt * self.cvisc * rhs)
+        else:
+            self.interior(p, X(p) + X(self.phi))
         self.bc_copy(p)
         f = self.phi
         gx[:, 1:ny + 1, :] -= (X(f) - X(f, -1)) * (dt * alp * dxi)
         gz[:, 1:ny + 1, :] -= (X(f) - X(f, 0, 0, -1)) * (dt * alp * dzi)
         gy[:, 2:ny + 1, :] -= ((X(f) - X(f, 0, -1)) * (dt * alp * dycj))[:, 1:, :]
         self.bc_vec(self.g)
+
+    # ---------------------------------------------------------- semi-implicit scheme
+    def stg_fields(self):
+        """MU_STG 1-3 and RHO_STG 1-3 as full arrays (ones with the energy
+        equation off); RHO_STG(2) row 0 keeps its allocation value 1."""
+        ny, X = self.ny, self.X
+        shape = self.D.shape
+        if not self.thermal:
+            one = np.ones(shape)
+            return (one, one, one), (one, one, one)
+        s1, s2, s3 = self.mu_stg()
+        D, D0 = self.D, self.D0
+        r1, r2, r3 = np.ones(shape), np.ones(shape), np.ones(shape)
+        self.interior(r1, (X(D) + X(D, -1) + X(D0) + X(D0, -1)) * 0.25)
+        self.interior(r3, (X(D) + X(D, 0, 0, -1) + X(D0) + X(D0, 0, 0, -1)) * 0.25)
+        ry = (self.row(self.wff) * (X(D) + X(D0)) + self.row(self.wfb) * (X(D, 0, -1) + X(D0, 0, -1))) * 0.5
+        r2[:, 2:ny + 1] = ry[:, 1:]
+        r2[:, 1] = 0.5 * (D0[:, 0] + D[:, 0])
+        r2[:, ny + 1] = 0.5 * (D0[:, ny + 1] + D[:, ny + 1])
+        return (s1, s2, s3), (r1, r2, r3)
+
+    def par_viscous(self):
+        """VISCOUS_PAR_EXPLT_X/Y/Z_io: per component the explicit part, the part
+        treated by the factors and the density part (DRHOI_STG)."""
+        ny, X, row = self.ny, self.X, self.row
+        u, v, w = self.q[1], self.q[2], self.q[3]
+        gx, gy, gz = self.g[1], self.g[2], self.g[3]
+        r1, r2, r3 = self.drhoi[1], self.drhoi[2], self.drhoi[3]
+        mu = self.mu
+        (s1, s2, s3), _ = self.stg_fields()
+        dxi, dzi, cv = self.dxi, self.dzi, self.cvisc
+        dyfj, dycj, dycp, dyfm = row(self.dyfi), row(self.dyci), row(self.dyci, 1), row(self.dyfi, -1)
+        out = {}
+        # x (rows 1..ny)
+        c1, c2, c32 = -2.0 / 3.0 * dxi * cv, dyfj * cv, dzi * cv
+        fe = X(mu) * ((X(v, 0, 1) - X(v)) * dyfj + (X(w, 0, 0, 1) - X(w)) * dzi)
+        fi = X(mu) * ((X(u, 1) - X(u)) * dxi)
+        fa = X(mu) * ((X(gx, 1) * X(r1, 1) - X(gx) * X(r1)) * dxi)
+        be = X(mu, -1) * ((X(v, -1, 1) - X(v, -1)) * dyfj + (X(w, -1, 0, 1) - X(w, -1)) * dzi)
+        bi = X(mu, -1) * ((X(u) - X(u, -1)) * dxi)
+        ba = X(mu, -1) * ((X(gx) * X(r1) - X(gx, -1) * X(r1, -1)) * dxi)
+        d11 = ((fe - be) * c1, (fi - bi) * c1 * (-2.0), (fa - ba) * c1 * (-2.0))
+        vp, vc = X(s1, 0, 1), X(s1)
+        fe = vp * ((X(v, 0, 1) - X(v, -1, 1)) * dxi)
+        fi = vp * ((X(u, 0, 1) - X(u)) * dycp)
+        fa = vp * ((X(gx, 0, 1) * X(r1, 0, 1) - X(gx) * X(r1)) * dycp)
+        be = vc * ((X(v) - X(v, -1)) * dxi)
+        bi = vc * ((X(u) - X(u, 0, -1)) * dycj)
+        ba = vc * ((X(gx) * X(r1) - X(gx, 0, -1) * X(r1, 0, -1)) * dycj)
+        d12 = ((fe - be) * c2, (fi - bi) * c2, (fa - ba) * c2)
+        vp, vc = X(s2, 0, 0, 1), X(s2)
+        fe = vp * ((X(w, 0, 0, 1) - X(w, -1, 0, 1)) * dxi)
+        fi = vp * ((X(u, 0, 0, 1) - X(u)) * dzi)
+        fa = vp * ((X(u, 0, 0, 1) * X(r1, 0, 0, 1) - X(u) * X(r1)) * dzi)  # Q_io, as written
+        be = vc * ((X(w) - X(w, -1)) * dxi)
+        bi = vc * ((X(u) - X(u, 0, 0, -1)) * dzi)
+        ba = vc * ((X(u) * X(r1) - X(u, 0, 0, -1) * X(r1, 0, 0, -1)) * dzi)
+        d13 = ((fe - be) * c32, (fi - bi) * c32, (fa - ba) * c32)
+        out[1] = tuple(d11[t] + d12[t] + d13[t] for t in range(3))
+        # y (rows 2..ny; row 1 dropped)
+        c1, c3, c2 = dxi * cv, dzi * cv, -2.0 / 3.0 * dycj * cv
+        fe = X(mu) * ((X(u, 1) - X(u)) * dxi + (X(w, 0, 0, 1) - X(w)) * dzi)
+        fi = X(mu) * ((X(v, 0, 1) - X(v)) * dyfj)
+        fa = X(mu) * ((X(gy, 0, 1) * X(r2, 0, 1) - X(gy) * X(r2)) * dyfj)
+        be = X(mu, 0, -1) * ((X(u, 1, -1) - X(u, 0, -1)) * dxi + (X(w, 0, -1, 1) - X(w, 0, -1)) * dzi)
+        bi = X(mu, 0, -1) * ((X(v) - X(v, 0, -1)) * dyfm)
+        ba = X(mu, 0, -1) * ((X(gy) * X(r2) - X(gy, 0, -1) * X(r2, 0, -1)) * dyfm)
+        d22 = ((fe - be) * c2, (fi - bi) * c2 * (-2.0), (fa - ba) * c2 * (-2.0))
+        vp, vc = X(s1, 1), X(s1)
+        fe = vp * ((X(u, 1) - X(u, 1, -1)) * dycj)
+        fi = vp * ((X(v, 1) - X(v)) * dxi)
+        fa = vp * ((X(gy, 1) * X(r2, 1) - X(gy) * X(r2)) * dxi)
+        be = vc * ((X(u) - X(u, 0, -1)) * dycj)
+        bi = vc * ((X(v) - X(v, -1)) * dxi)
+        ba = vc * ((X(gy) * X(r2) - X(gy, -1) * X(r2, -1)) * dxi)
+        d21 = ((fe - be) * c1, (fi - bi) * c1, (fa - ba) * c1)
+        vp, vc = X(s3, 0, 0, 1), X(s3)
+        fe = vp * ((X(w, 0, 0, 1) - X(w, 0, -1, 1)) * dycj)
+        fi = vp * ((X(v, 0, 0, 1) - X(v)) * dzi)
+        fa = vp * ((X(gy, 0, 0, 1) * X(r2, 0, 0, 1) - X(gy) * X(r2)) * dzi)
+        be = vc * ((X(w) - X(w, 0, -1)) * dycj)
+        bi = vc * ((X(v) - X(v, 0, 0, -1)) * dzi)
+        ba = vc * ((X(gy) * X(r2) - X(gy, 0, 0, -1) * X(r2, 0, 0, -1)) * dzi)
+        d23 = ((fe - be) * c3, (fi - bi) * c3, (fa - ba) * c3)
+        out[2] = tuple(d21[t] + d22[t] + d23[t] for t in range(3))
+        # z (rows 1..ny)
+        c1, c3, c2 = dxi * cv, -2.0 / 3.0 * dzi * cv, dyfj * cv
+        fe = X(mu) * ((X(u, 1) - X(u)) * dxi + (X(v, 0, 1) - X(v)) * dyfj)
+        fi = X(mu) * ((X(w, 0, 0, 1) - X(w)) * dzi)
+        fa = X(mu) * ((X(gz, 0, 0, 1) * X(r3, 0, 0, 1) - X(gz) * X(r3)) * dzi)
+        be = X(mu, 0, 0, -1) * ((X(u, 1, 0, -1) - X(u, 0, 0, -1)) * dxi + (X(v, 0, 1, -1) - X(v, 0, 0, -1)) * dyfj)
+        bi = X(mu, 0, 0, -1) * ((X(w) - X(w, 0, 0, -1)) * dzi)
+        ba = X(mu, 0, 0, -1) * ((X(gz) * X(r3) - X(gz, 0, 0, -1) * X(r3, 0, 0, -1)) * dzi)
+        d33 = ((fe - be) * c3, (fi - bi) * c3 * (-2.0), (fa - ba) * c3 * (-2.0))
+        vp, vc = X(s2, 1), X(s2)
+        fe = vp * ((X(u, 1) - X(u, 1, 0, -1)) * dzi)
+        fi = vp * ((X(w, 1) - X(w)) * dxi)
+        fa = vp * ((X(gz, 1) * X(r3, 1) - X(gz) * X(r3)) * dxi)
+        be = vc * ((X(u) - X(u, 0, 0, -1)) * dzi)
+        bi = vc * ((X(w) - X(w, -1)) * dxi)
+        ba = vc * ((X(gz) * X(r3) - X(gz, -1) * X(r3, -1)) * dxi)
+        d31 = ((fe - be) * c1, (fi - bi) * c1, (fa - ba) * c1)
+        vp, vc = X(s3, 0, 1), X(s3)
+        fe = vp * ((X(v, 0, 1) - X(v, 0, 1, -1)) * dzi)
+        fi = vp * ((X(w, 0, 1) - X(w)) * dycp)
+        fa = vp * ((X(gz, 0, 1) * X(r3, 0, 1) - X(gz) * X(r3)) * dycp)
+        be = vc * ((X(v) - X(v, 0, 0, -1)) * dzi)
+        bi = vc * ((X(w) - X(w, 0, -1)) * dycj)
+        ba = vc * ((X(gz) * X(r3) - X(gz, 0, -1) * X(r3, 0, -1)) * dycj)
+        d32 = ((fe - be) * c2, (fi - bi) * c2, (fa - ba) * c2)
+        out[3] = tuple(d31[t] + d32[t] + d33[t] for t in range(3))
+        return out
+
+    @staticmethod
+    def tri_solve(a, b, c, r, cyclic):
+        """Batched dense LU of tridiagonal lines along the last axis:
+        a x(i-1) + b x(i) + c x(i+1) = r (indices mod n when cyclic)."""
+        n = a.shape[-1]
+        M = np.zeros(a.shape + (n,))
+        idx = np.arange(n)
+        M[..., idx, idx] = b
+        M[..., idx[1:], idx[:-1]] = a[..., 1:]
+        M[..., idx[:-1], idx[1:]] = c[..., :-1]
+        if cyclic:
+            M[..., 0, n - 1] = a[..., 0]
+            M[..., n - 1, 0] = c[..., n - 1]
+        return np.linalg.solve(M, r[..., None])[..., 0]
+
+    def momfa(self, ns, comp, rhs):
+        """MOMFA_io: x, z, y factor solves of component comp on RHS_io (rows
+        1..ny array), then G += dG from row N2I."""
+        ny, X = self.ny, self.X
+        j0 = 1 if comp != 2 else 2  # first row (index into 1..ny) solved in x and z
+        facoe = 0.5 * TALP[ns] * self.dt * self.cvisc
+        (s1, s2, s3), (r1, r2, r3) = self.stg_fields()
+        rs = {1: r1, 2: r2, 3: r3}[comp]
+        vis = self.mu
+        # x
+        c1, c2 = facoe * 4.0 / 3.0 * self.dxi ** 2, facoe * self.dxi ** 2
+        if comp == 1:
+            amu, apu = -c1 * X(vis, -1), -c1 * X(vis)
+        elif comp == 2:
+            amu, apu = -c2 * X(s1), -c2 * X(s1, 1)
+        else:
+            amu, apu = -c2 * X(s2), -c2 * X(s2, 1)
+        a, c, b = amu / X(rs, -1), apu / X(rs, 1), 1.0 - (amu + apu) / X(rs)
+        sl = slice(j0 - 1, ny)
+        rhs[:, sl] = self.tri_solve(a[:, sl], b[:, sl], c[:, sl], rhs[:, sl], True)
+        # z
+        c1, c2 = facoe * 4.0 / 3.0 * self.dzi ** 2, facoe * self.dzi ** 2
+        if comp == 1:
+            amu, apu = -c2 * X(s2), -c2 * X(s2, 0, 0, 1)
+        elif comp == 2:
+            amu, apu = -c2 * X(s3), -c2 * X(s3, 0, 0, 1)
+        else:
+            amu, apu = -c1 * X(vis, 0, 0, -1), -c1 * X(vis)
+        a, c, b = amu / X(rs, 0, 0, -1), apu / X(rs, 0, 0, 1), 1.0 - (amu + apu) / X(rs)
+        tz = lambda f: np.transpose(f[:, sl], (1, 2, 0))  # (rows, x, z)
+        rhs[:, sl] = np.transpose(self.tri_solve(tz(a), tz(b), tz(c), tz(rhs), True), (2, 0, 1))
+        # y (rows 1..ny for every component)
+        jj = np.arange(1, ny + 1)
+        am, ap = self.amvr[comp][jj][None, :, None], self.apvr[comp][jj][None, :, None]
+        if comp in (1, 3):
+            fmu = s1 if comp == 1 else s3
+            amvr1 = 4.0 / (2.0 / self.dyci[2] + 1.0 / self.dyfi[1]) * (2.0 * self.dyfi[1])
+            apvrn = 4.0 / (2.0 / self.dyci[ny] + 1.0 / self.dyfi[ny]) * (2.0 * self.dyfi[ny])
+            amu = -facoe * am * X(fmu)
+            apu = -facoe * ap * X(fmu, 0, 1)
+            amu[:, 0] = -facoe * amvr1 * (X(vis)[:, 0] + X(vis, 0, -1)[:, 0]) * 0.5
+            apu[:, -1] = -facoe * apvrn * (X(vis)[:, -1] + X(vis, 0, 1)[:, -1]) * 0.5
+            a, c = amu / X(rs, 0, -1), apu / X(rs, 0, 1)
+            a[:, 0] = 0.0
+            c[:, -1] = 0.0
+        else:
+            cy = facoe * 4.0 / 3.0
+            amu, apu = -cy * am * X(vis, 0, -1), -cy * ap * X(vis)
+            a, c = amu / X(rs, 0, -1), apu / X(rs)
+            c[:, 0] = apu[:, 0] / X(rs, 0, 1)[:, 0]
+            a[:, 0] = 0.0
+            c[:, -1] = 0.0
+        b = 1.0 - (amu + apu) / X(rs)
+        ty = lambda f: np.transpose(f, (0, 2, 1))  # (z, x, rows)
+        x = np.transpose(self.tri_solve(ty(a), ty(b), ty(c), ty(rhs), False), (0, 2, 1))
+        self.g[comp][:, j0:ny + 1] += x[:, j0 - 1:]
+
+    def mom_semi_implicit(self, ns, cx, cy, cz):
+        """SOLVERRK3_MOM_IO with visthemflg = 1: per component the split
+        viscous terms, RHS_MOM_EXPLICIT_io's implicit branch, MOMFA_io."""
+        ny, X, row = self.ny, self.X, self.row
+        p, dt, alp = self.p, self.dt, TALP[ns]
+        par = self.par_viscous()
+        conv = {1: cx, 2: cy, 3: cz}
+        pg = {1: (X(p) - X(p, -1)) * (alp * dt * self.dxi),
+              2: (X(p) - X(p, 0, -1)) * (alp * dt * row(self.dyci)),
+              3: (X(p) - X(p, 0, 0, -1)) * (alp * dt * self.dzi)}
+        for comp in (1, 2, 3):
+            ex, im, ad = par[comp]
+            explt = ex + conv[comp]
+            r = (TGAM[ns] * explt + TROH[ns] * X(self.ex0[comp])) * dt
+            r = r + alp * dt * im + 0.5 * (alp * dt) * ad
+            r = r - pg[comp]
+            if comp == 2:
+                self.ex0[2][:, 2:ny + 1] = explt[:, 1:]
+                r[:, 0] = 0.0
+            else:
+                self.interior(self.ex0[comp], explt)
+            if comp == 1:
+                r = r - np.sum(r / row(self.dyfi)) / self.volm  # DPGRNS
+            self.momfa(ns, comp, r)
+        self.bc_vec(self.g)
+        self.project(ns)
 
     def poisson_io(self, rhs):
         """FISHPACK_POIS3D_SIMPLE's operator diagonalised with complex FFTs in x

@@ -164,17 +164,20 @@ def test_io_density_time_derivation_parity():
     assert np.abs(o.get("drho")).max() > 1e-3
 
 
-@pytest.mark.parametrize("name", ["io_16x12x8_seed3", "io_heated_16x10x8_seed7"])
+@pytest.mark.parametrize("name", ["io_16x12x8_seed3", "io_heated_16x10x8_seed7", "io_si_16x12x8_seed3",
+                                  "io_si_heated_16x10x8_seed7"])
 def test_io_golden_fixture(name):
     """The library (graph-replayed full RK3 steps) against the committed
-    fixtures of the independent numpy restatement, tests/golden/numpy_io.py."""
+    fixtures of the independent numpy restatement, tests/golden/numpy_io.py
+    (explicit and semi-implicit viscous schemes)."""
     _need_gpu()
     import os
     from chapsim1ww_b200 import IOChannel
     z = np.load(os.path.join(os.path.dirname(__file__), "golden", name + ".npz"))
-    nx, ny, nz, lx, lz, ren, dt, seed, amp, steps, thermal, prt, qb, qt = z["meta"]
+    meta = list(z["meta"]) + [0.0] * (15 - len(z["meta"]))
+    nx, ny, nz, lx, lz, ren, dt, seed, amp, steps, thermal, prt, qb, qt, visc = meta
     g = IOChannel(int(nx), int(ny), int(nz), lx=lx, lz=lz, ren=ren, dt=dt, thermal=int(thermal), prt=prt,
-                  qw=(qb, qt))
+                  qw=(qb, qt), visc_scheme=int(visc))
     g.random_fl_theml_fld_io(int(seed), amp)
     for n in ("gx", "gy", "p"):
         assert relerr(g.get_field(n), z["ns0_" + n]) < TOL, n

@@ -69,20 +69,22 @@ def test_io_rhohmax_and_table_state():
 
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-IO_GOLDEN = ["io_16x12x8_seed3", "io_heated_16x10x8_seed7"]
+IO_GOLDEN = ["io_16x12x8_seed3", "io_heated_16x10x8_seed7", "io_si_16x12x8_seed3", "io_si_heated_16x10x8_seed7"]
 
 
 def load_io_golden(name):
     z = np.load(os.path.join(GOLDEN, name + ".npz"))
-    nx, ny, nz, lx, lz, ren, dt, seed, amp, steps, thermal, prt, qb, qt = z["meta"]
-    kw = dict(lx=lx, lz=lz, ren=ren, dt=dt, thermal=int(thermal), prt=prt, qw=(qb, qt))
+    meta = list(z["meta"]) + [0.0] * (15 - len(z["meta"]))  # visc_scheme defaults to explicit
+    nx, ny, nz, lx, lz, ren, dt, seed, amp, steps, thermal, prt, qb, qt, visc = meta
+    kw = dict(lx=lx, lz=lz, ren=ren, dt=dt, thermal=int(thermal), prt=prt, qw=(qb, qt), visc_scheme=int(visc))
     return z, (int(nx), int(ny), int(nz)), int(seed), amp, int(steps), kw
 
 
 @pytest.mark.parametrize("name", IO_GOLDEN)
 def test_oracle_io_matches_golden(name):
     """The C++ oracle against the fixtures of the independent numpy
-    restatement (tests/golden/numpy_io.py): FP64 within 1e-10 relative."""
+    restatement (tests/golden/numpy_io.py), explicit and semi-implicit
+    viscous schemes: FP64 within 1e-10 relative."""
     z, dims, seed, amp, steps, kw = load_io_golden(name)
     o = OracleIO(*dims, **kw)
     o.init_random(seed, amp)
