@@ -62,6 +62,8 @@ SIGNATURES = [
     ("chapsim_field_len", _I64, [_P]),
     ("chapsim_set_field", _I, [_P, _I, _I, _P, _I64]),
     ("chapsim_get_field", _I, [_P, _I, _I, _P, _I64]),
+    ("chapsim_set_field_async", _I, [_P, _I, _I, _P, _I64]),
+    ("chapsim_get_field_async", _I, [_P, _I, _I, _P, _I64]),
     ("chapsim_set_field_device", _I, [_P, _I, _I, _P, _I64]),
     ("chapsim_get_field_device", _I, [_P, _I, _I, _P, _I64]),
     ("chapsim_get_mesh", _I, [_P, _I, _P, _I64]),

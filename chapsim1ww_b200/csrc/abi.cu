@@ -52,7 +52,7 @@ bool factor_plan(int n, FFTPlan &pl) {
   pl.n = n;
   pl.nrad = 0;
   int m = n;
-  const int radices[] = {4, 2, 3, 5, 7, 11};
+  const int radices[] = {8, 4, 2, 3, 5, 7, 11};
   for (int r : radices)
     while (m % r == 0) {
       if (pl.nrad >= 16) return false;
@@ -679,7 +679,7 @@ static double *field_ptr(chapsim_ctx *ctx, int domain, int field) {
 }
 
 static int xfer(chapsim_ctx *ctx, int domain, int field, void *dst_or_src, int64_t n, cudaMemcpyKind kind,
-                bool to_dev) {
+                bool to_dev, bool async = false) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
   double *f = field_ptr(ctx, domain, field);
   REQUIRE(f, CHAPSIM_ERR_ARG, "unknown domain/field id");
@@ -691,6 +691,7 @@ static int xfer(chapsim_ctx *ctx, int domain, int field, void *dst_or_src, int64
   if (h0f && ctx->cfg.precision == CHAPSIM_MIXED) {
     // CONVH0 is held in FP32 in the mixed form: convert through the host
     REQUIRE(kind != cudaMemcpyDeviceToDevice, CHAPSIM_ERR_UNSUPPORTED, "device copies of FP32 H0 fields");
+    REQUIRE(!async, CHAPSIM_ERR_UNSUPPORTED, "stream-ordered copies of FP32 H0 fields");
     std::vector<float> tmp((size_t)n);
     if (to_dev) {
       const double *src = (const double *)dst_or_src;
@@ -713,7 +714,7 @@ static int xfer(chapsim_ctx *ctx, int domain, int field, void *dst_or_src, int64
     const int rc = io_refresh_msum(ctx);  // keep mu0 + mu in step
     if (rc) return rc;
   }
-  if (kind != cudaMemcpyDeviceToDevice) CKC(cudaStreamSynchronize(ctx->stream));
+  if (kind != cudaMemcpyDeviceToDevice && !async) CKC(cudaStreamSynchronize(ctx->stream));
   return CHAPSIM_OK;
 }
 
@@ -722,6 +723,12 @@ int chapsim_set_field(chapsim_ctx *ctx, int domain, int field, const double *hos
 }
 int chapsim_get_field(chapsim_ctx *ctx, int domain, int field, double *host, int64_t n) {
   return xfer(ctx, domain, field, host, n, cudaMemcpyDeviceToHost, false);
+}
+int chapsim_set_field_async(chapsim_ctx *ctx, int domain, int field, const double *host, int64_t n) {
+  return xfer(ctx, domain, field, (void *)host, n, cudaMemcpyHostToDevice, true, true);
+}
+int chapsim_get_field_async(chapsim_ctx *ctx, int domain, int field, double *host, int64_t n) {
+  return xfer(ctx, domain, field, host, n, cudaMemcpyDeviceToHost, false, true);
 }
 int chapsim_set_field_device(chapsim_ctx *ctx, int domain, int field, const double *dev, int64_t n) {
   return xfer(ctx, domain, field, (void *)dev, n, cudaMemcpyDeviceToDevice, true);

@@ -7,7 +7,8 @@
 // libs/fft99/CFFT99.f90:171-196): forward = sum x e^{-2 pi i jk/N}, inverse =
 // sum C e^{+2 pi i jk/N}; normalisation is applied by the callers.  Unlike
 // FFT99 (radices 2, 3, 5 only) every length whose prime factors are in
-// {2, 3, 5, 7, 11} is supported.
+// {2, 3, 5, 7, 11} is supported; powers of two run as radix-8 stages (a
+// 512-point line takes three stages).
 //
 // Algorithm: self-sorting Stockham decimation in time.  Stage s with radix R
 // and Ns = product of earlier radices maps, for j in [0, N/R):
@@ -45,6 +46,16 @@ template <typename C> __device__ __forceinline__ C twiddle(const C *tw, int m, i
   return t;
 }
 
+// in-place 4-point DFT with root sign * i
+template <typename C> __device__ __forceinline__ void dft4(C &x0, C &x1, C &x2, C &x3, int sign) {
+  C s02 = cadd(x0, x2), d02 = csub(x0, x2);
+  C s13 = cadd(x1, x3), d13 = cmuli(csub(x1, x3), sign);
+  x0 = cadd(s02, s13);
+  x2 = csub(s02, s13);
+  x1 = cadd(d02, d13);
+  x3 = csub(d02, d13);
+}
+
 template <typename C, int R>
 __device__ __forceinline__ void dft_small(C *v, const C *tw, int n, int sign) {
   if (R == 2) {
@@ -52,13 +63,28 @@ __device__ __forceinline__ void dft_small(C *v, const C *tw, int n, int sign) {
     v[0] = cadd(a, b);
     v[1] = csub(a, b);
   } else if (R == 4) {
-    C x0 = v[0], x1 = v[1], x2 = v[2], x3 = v[3];
-    C s02 = cadd(x0, x2), d02 = csub(x0, x2);
-    C s13 = cadd(x1, x3), d13 = cmuli(csub(x1, x3), sign);
-    v[0] = cadd(s02, s13);
-    v[2] = csub(s02, s13);
-    v[1] = cadd(d02, d13);
-    v[3] = csub(d02, d13);
+    dft4(v[0], v[1], v[2], v[3], sign);
+  } else if (R == 8) {
+    // X_{2m} = DFT4(x_r + x_{r+4})_m, X_{2m+1} = DFT4((x_r - x_{r+4}) w^r)_m
+    // with w = exp(sign 2 pi i / 8)
+    typedef typename CTraits<C>::R T;
+    const T h = (T)0.70710678118654752440;  // 1 / sqrt(2)
+    C a0 = cadd(v[0], v[4]), a1 = cadd(v[1], v[5]), a2 = cadd(v[2], v[6]), a3 = cadd(v[3], v[7]);
+    C b0 = csub(v[0], v[4]), b1 = csub(v[1], v[5]), b2 = csub(v[2], v[6]), b3 = csub(v[3], v[7]);
+    // b1 w = b1 (1 + sign i) / sqrt 2, b2 w^2 = sign i b2, b3 w^3 = b3 (-1 + sign i) / sqrt 2
+    C t1, t3;
+    if (sign < 0) {
+      t1.x = (b1.x + b1.y) * h; t1.y = (b1.y - b1.x) * h;
+      t3.x = (b3.y - b3.x) * h; t3.y = -(b3.x + b3.y) * h;
+    } else {
+      t1.x = (b1.x - b1.y) * h; t1.y = (b1.x + b1.y) * h;
+      t3.x = -(b3.x + b3.y) * h; t3.y = (b3.x - b3.y) * h;
+    }
+    b2 = cmuli(b2, sign);
+    dft4(a0, a1, a2, a3, sign);
+    dft4(b0, t1, b2, t3, sign);
+    v[0] = a0; v[2] = a1; v[4] = a2; v[6] = a3;
+    v[1] = b0; v[3] = t1; v[5] = b2; v[7] = t3;
   } else {
     // generic odd radix: V_s = sum_r v_r w_R^{rs}, w_R = table[(n/R) * m]
     C out[R];
@@ -109,7 +135,7 @@ __device__ __forceinline__ void stockham_stage(const C *__restrict__ in, C *__re
 // shared memory buffer a; b is scratch of the same size.  Returns the buffer
 // holding the result.  Must be called by every thread of the block.
 // BIG selects whether radices 7 and 11 are compiled in (they raise register
-// use of every stage, so plans with only 2, 3, 4, 5 use the small variant).
+// use of every stage, so plans with only 2, 3, 4, 5, 8 use the small variant).
 template <typename C, bool BIG>
 __device__ C *fft_lines(C *a, C *b, int nlines, int n, int lstride, const int *rad, int nrad,
                         const C *__restrict__ tw, int sign) {
@@ -120,6 +146,7 @@ __device__ C *fft_lines(C *a, C *b, int nlines, int n, int lstride, const int *r
       case 2: stockham_stage<C, 2>(a, b, nlines, n, lstride, Ns, tw, sign); break;
       case 3: stockham_stage<C, 3>(a, b, nlines, n, lstride, Ns, tw, sign); break;
       case 4: stockham_stage<C, 4>(a, b, nlines, n, lstride, Ns, tw, sign); break;
+      case 8: stockham_stage<C, 8>(a, b, nlines, n, lstride, Ns, tw, sign); break;
       case 5: stockham_stage<C, 5>(a, b, nlines, n, lstride, Ns, tw, sign); break;
       case 7: if (BIG) stockham_stage<C, 7>(a, b, nlines, n, lstride, Ns, tw, sign); break;
       case 11: if (BIG) stockham_stage<C, 11>(a, b, nlines, n, lstride, Ns, tw, sign); break;
@@ -169,6 +196,7 @@ __device__ C *fft_lines_il(C *a, C *b, int nl, int n, const int *rad, int nrad, 
       case 2: stockham_stage_il<C, 2>(a, b, nl, n, Ns, tw, sign); break;
       case 3: stockham_stage_il<C, 3>(a, b, nl, n, Ns, tw, sign); break;
       case 4: stockham_stage_il<C, 4>(a, b, nl, n, Ns, tw, sign); break;
+      case 8: stockham_stage_il<C, 8>(a, b, nl, n, Ns, tw, sign); break;
       case 5: stockham_stage_il<C, 5>(a, b, nl, n, Ns, tw, sign); break;
       case 7: if (BIG) stockham_stage_il<C, 7>(a, b, nl, n, Ns, tw, sign); break;
       case 11: if (BIG) stockham_stage_il<C, 11>(a, b, nl, n, Ns, tw, sign); break;

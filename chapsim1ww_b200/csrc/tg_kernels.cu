@@ -1431,7 +1431,7 @@ int init_kernels(chapsim_ctx *c) {
   }
   c->fft_big = false;
   for (int s2 = 0; s2 < 16; ++s2)
-    if (c->fx.rad[s2] > 5 || c->fz.rad[s2] > 5) c->fft_big = true;
+    if (c->fx.rad[s2] == 7 || c->fx.rad[s2] == 11 || c->fz.rad[s2] == 7 || c->fz.rad[s2] == 11) c->fft_big = true;
   return c->cfg.precision == CHAPSIM_MIXED ? Prec<float>::init(c) : Prec<double>::init(c);
 }
 

@@ -102,6 +102,23 @@ class TGChannel:
         self._chk(self.lib.chapsim_get_field(self.h, self.DOMAIN, self.FIELDS[name], a.ctypes.data, self.n))
         return a
 
+    def set_field_async(self, name, arr):
+        """Stream-ordered upload: arr (C-contiguous float64, page-locked for
+        overlap) must stay alive until sync()."""
+        if not (isinstance(arr, np.ndarray) and arr.dtype == np.float64 and arr.flags.c_contiguous):
+            raise ValueError("set_field_async needs a C-contiguous float64 array")
+        if arr.size != self.n:
+            raise ValueError(f"field {name}: expected {self.n} values, got {arr.size}")
+        self._chk(self.lib.chapsim_set_field_async(self.h, self.DOMAIN, self.FIELDS[name], arr.ctypes.data, self.n))
+
+    def get_field_async(self, name, out):
+        """Stream-ordered download into out (complete after sync())."""
+        if not (isinstance(out, np.ndarray) and out.dtype == np.float64 and out.flags.c_contiguous
+                and out.size == self.n):
+            raise ValueError("get_field_async needs a C-contiguous float64 array of the field's size")
+        self._chk(self.lib.chapsim_get_field_async(self.h, self.DOMAIN, self.FIELDS[name], out.ctypes.data, self.n))
+        return out
+
     def set_field_device(self, name, ptr):
         self._chk(self.lib.chapsim_set_field_device(self.h, self.DOMAIN, self.FIELDS[name], ptr, self.n))
 

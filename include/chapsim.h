@@ -135,6 +135,18 @@ int chapsim_get_field(chapsim_ctx *ctx, int domain, int field, double *host, int
 /* Device-resident variants: dev is a device pointer on the context's device. */
 int chapsim_set_field_device(chapsim_ctx *ctx, int domain, int field, const double *dev, int64_t n);
 int chapsim_get_field_device(chapsim_ctx *ctx, int domain, int field, double *dev, int64_t n);
+/* Stream-ordered variants of chapsim_set_field / chapsim_get_field: the copy
+ * is queued on the context's stream behind earlier work and the call returns
+ * at once; it has completed after chapsim_sync (or any call that returns host
+ * data).  The host buffer must stay valid until then; with page-locked memory
+ * the copy overlaps other contexts' work (two sections, two contexts), with
+ * pageable memory it is as synchronous as the plain call.  The reference has
+ * no counterpart: its module arrays are host memory
+ * (src/MEMALLOCT.f90:99-210); these serve a host that moves the state in and
+ * out every step.  FP32 fields of the mixed form are not accepted
+ * (CHAPSIM_ERR_UNSUPPORTED). */
+int chapsim_set_field_async(chapsim_ctx *ctx, int domain, int field, const double *host, int64_t n);
+int chapsim_get_field_async(chapsim_ctx *ctx, int domain, int field, double *host, int64_t n);
 
 /* Mesh and coefficient arrays (host copies), for checks:
  * what = 0 YND(1:ny+1), 1 YCC(1:ny), 2 DYFI(1:ny), 3 DYCI(1:ny+1). */

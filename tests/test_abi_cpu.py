@@ -51,6 +51,8 @@ def test_create_validates_before_touching_a_device():
     assert lib.chapsim_create(ctypes.byref(cfg), ctypes.byref(h)) == 1
     assert lib.chapsim_destroy(None) == 1
     assert lib.chapsim_sync(None) == 1
+    assert lib.chapsim_set_field_async(None, 0, 0, None, 0) == 1
+    assert lib.chapsim_get_field_async(None, 0, 0, None, 0) == 1
 
 
 def test_no_cpu_fallback_without_gpu():

@@ -52,9 +52,11 @@ def test_autotune_keeps_state_and_results():
     b.sync()
     ref.sync()
     for i in range(2):
-        for n in ("u", "v", "w", "p"):
-            # launch shapes change only the block order of the mass-flux sum
-            assert relerr(b.channels[i].get_field(n), ref.channels[i].get_field(n)) < 1e-12
+        for n, tol in (("u", 1e-12), ("v", 1e-12), ("w", 1e-12), ("p", 1e-11)):
+            # launch shapes change only the block order of the mass-flux sum;
+            # the forcing's last-bit change is not divergence-free after
+            # rounding, and p accumulates the projection of that round-off
+            assert relerr(b.channels[i].get_field(n), ref.channels[i].get_field(n)) < tol, n
 
 
 def test_mixed_batch_divergence_gate():

@@ -95,6 +95,32 @@ def test_io_graph_step_matches_eager_bitwise():
         assert np.array_equal(a.get_field(n), b.get_field(n)), n
 
 
+@pytest.mark.parametrize("visc", [0, 1])
+def test_io_velocity_is_a_result_not_an_input(visc):
+    """u, v, w of an IO context are rebuilt from G and the density before
+    each substep's momentum stage (VELOCITY_CALC_io, src/SOLVE.f90:131-132)
+    and the energy stage does not read them: a step from overwritten u, v, w
+    gives the same bits.  The end-to-end benchmark uploads G, p and rho h
+    only on this basis."""
+    _need_gpu()
+    from chapsim1ww_b200 import IOChannel
+    from oracle.pyoracle import synth_table
+    table = synth_table(4096)
+    a = IOChannel(32, 24, 16, table=table, dt=2e-3, visc_scheme=visc)
+    b = IOChannel(32, 24, 16, table=table, dt=2e-3, visc_scheme=visc)
+    a.random_fl_theml_fld_io(9, 0.1)
+    b.random_fl_theml_fld_io(9, 0.1)
+    a.step(1)
+    b.step(1)
+    rng = np.random.default_rng(3)
+    for n in ("u", "v", "w"):
+        b.set_field(n, rng.standard_normal(b.shape))
+    a.step(1)
+    b.step(1)
+    for n in FLOW + THERMAL:
+        assert np.array_equal(a.get_field(n), b.get_field(n)), n
+
+
 def test_io_fp64_run_to_run_bitwise():
     _need_gpu()
     from chapsim1ww_b200 import IOChannel
