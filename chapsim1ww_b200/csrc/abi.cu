@@ -356,7 +356,7 @@ static int build_tables(chapsim_ctx *ctx) {
   int wx[4], wz[4];
   for (int ns = 0; ns < 4; ++ns) {
     std::vector<double> g;
-    const int band_max = 12;  // BAND_WMAX in tg_kernels.cu
+    const int band_max = BAND_ROWS - 1;  // BAND_WMAX in tg_kernels.cu
     wx[ns] = circulant_band(nx, xa[ns], xb[ns], xqq[ns], &H[o_x[ns][0]], &H[o_x[ns][1]], &H[o_x[ns][2]], band_max, g);
     o_gx[ns] = alloc(band_max + 1);
     if (wx[ns] >= 0) for (int m = 0; m <= wx[ns]; ++m) H[o_gx[ns] + m] = g[m];
@@ -419,6 +419,10 @@ static int build_tables(chapsim_ctx *ctx) {
     sp.gz = D + o_gz[ns];
     sp.wx = wx[ns];
     sp.wz = wz[ns];
+    for (int m = 0; m < BAND_ROWS; ++m) {
+      sp.bgx[m] = (wx[ns] >= 0 && m <= wx[ns]) ? H[o_gx[ns] + m] : 0.0;
+      sp.bgz[m] = (wz[ns] >= 0 && m <= wz[ns]) ? H[o_gz[ns] + m] : 0.0;
+    }
     sp.band = (wx[ns] >= 0 && wz[ns] >= 0 && ctx->allow_band) ? 1 : 0;
     for (int c = 0; c < 3; ++c) sp.yg[c] = D + o_yg[ns][c];
     sp.wy = ctx->allow_band ? wy[ns] : -1;

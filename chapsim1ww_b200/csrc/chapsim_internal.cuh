@@ -72,6 +72,8 @@ struct IODev {
 };
 
 // Per-substep scalars.
+constexpr int BAND_ROWS = 13;  // g_0 .. g_12: the widest truncated x / z inverse kept
+
 struct SubParams {
   int ns;
   double gam, roh, alp;
@@ -87,6 +89,9 @@ struct SubParams {
   // truncated circulant inverses of the x and z factors (first rows g_0..g_W)
   const double *gx, *gz;
   int wx, wz;
+  // the same first rows by value (zero past wx / wz): kernels that index them
+  // with compile-time offsets read them from the parameter bank
+  double bgx[BAND_ROWS], bgz[BAND_ROWS];
   int band;  // 1: x/z factors applied by k_adixz_band
   // banded inverses of the y factors: yg[c][j*(2*16+1) + 16 + m], m in [-wy, wy]
   const double *yg[3];

@@ -501,84 +501,239 @@ __global__ void __launch_bounds__(128) k_adiz(TGDev d, SubParams sp) {
 constexpr int BAND_WMAX = 12;
 // z-marching form: a block owns a 32 (x) by 8 (j) tile and a segment of z
 // planes.  Each rhs plane of the tile (with its periodic x halo) is loaded
-// once (the next plane is prefetched into registers while the current one is
-// processed), the x inverse is applied into a ring of 2*wz+1 x-solved planes
-// in shared memory, and the z inverse over the ring gives the output plane
-// k - wz.
-constexpr int BM_TX = 32, BM_TY = 8, BM_SEG = 32;
-template <typename T>
+// once, BM_PF planes ahead of its use (a register queue, so that enough loads
+// are in flight to cover HBM latency), into a double-buffered shared row; the
+// x inverse is applied from it, and each thread keeps the last 2*WZ+1
+// x-solved values of its own column in registers: the z inverse over that
+// window gives the output plane k - WZ.  WX, WZ are compile-time widths at
+// least the inverses' widths (the extra weights are zero), so both stencils
+// unroll with their weights read from the parameter bank; the plane loop is
+// unrolled by the window length so that the window rotates through static
+// register indices.
+constexpr int BM_TX = 32, BM_TY = 8, BM_SEG = 64, BM_PF = 1;  // deeper queues measured slower (registers)
+constexpr int BAND_TW[5] = {2, 4, 6, 8, 12};  // compiled widths
+static_assert(BAND_TW[4] == BAND_WMAX && BAND_WMAX + 1 == BAND_ROWS, "the widest compiled band is the host's limit");
+template <typename T, int WX, int WZ>
 __global__ void __launch_bounds__(BM_TX *BM_TY) k_adixz_band(TGDev d, SubParams sp) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  const int wx = sp.wx, wz = sp.wz, RS = 2 * wz + 1, XW = BM_TX + 2 * wx;
-  double *ring = reinterpret_cast<double *>(smem_raw);          // [RS][8][32]
-  double *tin = ring + RS * BM_TY * BM_TX;                      // [8][XW]
-  __shared__ double gxs[BAND_WMAX + 1], gzs[BAND_WMAX + 1];
+  constexpr int RS = 2 * WZ + 1, XW = BM_TX + 2 * WX;
+  __shared__ double tin[2][BM_TY][XW];
   const int nx = d.nx, ny = d.ny, nz = d.nz;
-  const int nseg = (nz + BM_SEG - 1) / BM_SEG;
   const int comp = blockIdx.z % 3, seg = blockIdx.z / 3;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int x0 = blockIdx.x * BM_TX, j = 1 + blockIdx.y * BM_TY + ty;
   const int kb = seg * BM_SEG, ke = min(kb + BM_SEG, nz);
-  (void)nseg;
-  if (ty == 0 && tx <= BAND_WMAX) {
-    gxs[tx] = tx <= wx ? sp.gx[tx] : 0.0;
-    gzs[tx] = tx <= wz ? sp.gz[tx] : 0.0;
-  }
   const bool row_ok = (j <= ny) && !(comp == 1 && j == 1);
   const double sub = comp == 0 ? d.scal[0] : 0.0;
   const T *src = reinterpret_cast<const T *>(d.rhs[comp]) + d.sy * (row_ok ? j : 1);
-  // this thread's input columns: x0 - wx + tx and x0 - wx + tx + 32 (if < XW)
-  int xa = (x0 - wx + tx) % nx;
+  // this thread's input columns: x0 - WX + tx and x0 - WX + tx + 32 (if < XW)
+  int xa = (x0 - WX + tx) % nx;
   xa = xa < 0 ? xa + nx : xa;
   const bool has_b = tx + BM_TX < XW;
-  int xb = (x0 - wx + tx + BM_TX) % nx;
+  int xb = (x0 - WX + tx + BM_TX) % nx;
   xb = xb < 0 ? xb + nx : xb;
-  auto zwrap = [&](int k) { k %= nz; return k < 0 ? k + nz : k; };
-  const int pbeg = kb - wz, pend = ke + wz;  // planes [pbeg, pend)
-  double na = 0.0, nb = 0.0;
-  if (row_ok) {
-    const T *r = src + d.sz * (int64_t)zwrap(pbeg);
-    na = (double)r[xa] - sub;
-    if (has_b) nb = (double)r[xb] - sub;
+  // planes [pbeg, pend); the host keeps 2 w + 1 <= nz and WZ <= 2 w, so
+  // -nz < pbeg and one wrap per step suffices
+  const int pbeg = kb - WZ, pend = ke + WZ;
+  const int64_t wrap = d.sz * (int64_t)nz;
+  int lk = pbeg < 0 ? pbeg + nz : pbeg;  // next plane to load
+  const T *lplane = src + d.sz * (int64_t)lk;
+  double na[BM_PF], nb[BM_PF];
+#pragma unroll
+  for (int q = 0; q < BM_PF; ++q) {
+    na[q] = 0.0;
+    nb[q] = 0.0;
+    if (row_ok && pbeg + q < pend) {
+      na[q] = (double)lplane[xa] - sub;
+      if (has_b) nb[q] = (double)lplane[xb] - sub;
+    }
+    lplane += d.sz;
+    if (++lk == nz) { lk = 0; lplane -= wrap; }
   }
   const int i = x0 + tx;
   T *dst = reinterpret_cast<T *>(d.dq[comp]) + d.sy * j + i;
-  const int tid = tx + BM_TX * ty;
-  int slot = 0;  // ring slot of plane p (planes are stored in order, modulo RS)
-  for (int p = pbeg; p < pend; ++p) {
-    // publish the prefetched plane p, prefetch plane p + 1
-    tin[ty * XW + tx] = na;
-    if (has_b) tin[ty * XW + tx + BM_TX] = nb;
-    if (row_ok && p + 1 < pend) {
-      const T *r = src + d.sz * (int64_t)zwrap(p + 1);
-      na = (double)r[xa] - sub;
-      if (has_b) nb = (double)r[xb] - sub;
-    }
-    __syncthreads();
-    {
-      const double *rr = tin + ty * XW + tx + wx;
-      double acc = gxs[0] * rr[0];
-      for (int m = 1; m <= wx; ++m) acc += gxs[m] * (rr[-m] + rr[m]);
-      ring[slot * (BM_TY * BM_TX) + tid] = acc;
-    }
-    __syncthreads();
-    const int k = p - wz;  // output plane once its whole z window is in the ring
-    if (k >= kb) {
-      // planes k - wz .. k + wz = p - 2wz .. p sit in slots slot+1 .. slot (mod RS)
-      int sl = slot + 1 == RS ? 0 : slot + 1;
-      double acc = 0.0;
-      for (int q = -wz; q <= wz; ++q) {
-        acc += gzs[q < 0 ? -q : q] * ring[sl * (BM_TY * BM_TX) + tid];
-        sl = sl + 1 == RS ? 0 : sl + 1;
+  double win[RS];  // slot s: plane p0 + s once written in this chunk
+#pragma unroll
+  for (int q = 0; q < RS; ++q) win[q] = 0.0;
+  int buf = 0;
+  for (int p0 = pbeg; p0 < pend; p0 += RS) {
+#pragma unroll
+    for (int u = 0; u < RS; ++u) {
+      const int p = p0 + u;
+      if (p >= pend) break;  // uniform over the block
+      // publish plane p, queue plane p + BM_PF.  One barrier per plane: a
+      // buffer is rewritten two planes later, after every thread has passed
+      // the barrier of the plane between.
+      double *row = tin[buf][ty];
+      buf ^= 1;
+      row[tx] = na[0];
+      if (has_b) row[tx + BM_TX] = nb[0];
+#pragma unroll
+      for (int q = 0; q + 1 < BM_PF; ++q) {
+        na[q] = na[q + 1];
+        nb[q] = nb[q + 1];
       }
-      if (row_ok && i < nx) dst[d.sz * (int64_t)k] = (T)acc;
+      if (row_ok && p + BM_PF < pend) {
+        na[BM_PF - 1] = (double)lplane[xa] - sub;
+        if (has_b) nb[BM_PF - 1] = (double)lplane[xb] - sub;
+      }
+      lplane += d.sz;
+      if (++lk == nz) { lk = 0; lplane -= wrap; }
+      __syncthreads();
+      const double *rr = row + tx + WX;
+      double xs = sp.bgx[0] * rr[0];
+#pragma unroll
+      for (int m = 1; m <= WX; ++m) xs += sp.bgx[m] * (rr[-m] + rr[m]);
+      win[u] = xs;
+      if (p - WZ >= kb) {
+        // window planes p - 2 WZ .. p; plane p - t sits in slot (u - t) mod RS
+        double acc = sp.bgz[0] * win[(u + WZ + 1) % RS];
+#pragma unroll
+        for (int m = 1; m <= WZ; ++m) acc += sp.bgz[m] * (win[(u + WZ + 1 - m) % RS] + win[(u + WZ + 1 + m) % RS]);
+        if (row_ok && i < nx) dst[d.sz * (int64_t)(p - WZ)] = (T)acc;
+      }
     }
-    slot = slot + 1 == RS ? 0 : slot + 1;
   }
 }
-static size_t band_smem(int wx, int wz) {
-  return ((size_t)(2 * wz + 1) * BM_TY * BM_TX + (size_t)BM_TY * (BM_TX + 2 * wx)) * sizeof(double);
+
+// Row form of the same factors, used when a block can own whole x rows
+// (nx = CPT * blockDim.x with blockDim.x <= 256): each plane of the block's
+// rows arrives as contiguous rows (no x halo is loaded: the periodic halo is
+// written into shared memory from the row itself), thread tx owns columns
+// tx + c * blockDim.x, c < CPT, and keeps their z windows in registers.
+// Segments of seglen planes per block.
+template <typename T, int WX, int WZ, int CPT>
+__global__ void __launch_bounds__(256) k_adixz_row(TGDev d, SubParams sp, int seglen) {
+  constexpr int RS = 2 * WZ + 1;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  double *rows = reinterpret_cast<double *>(smem_raw);  // [2][blockDim.y][nx + 2 WX]
+  const int nx = d.nx, ny = d.ny, nz = d.nz, RW = nx + 2 * WX;
+  const int btx = blockDim.x, tx = threadIdx.x, ty = threadIdx.y;
+  const int j = 1 + blockIdx.x * blockDim.y + ty;
+  const int comp = blockIdx.y % 3, seg = blockIdx.y / 3;
+  const int kb = seg * seglen, ke = min(kb + seglen, nz);
+  const bool row_ok = (j <= ny) && !(comp == 1 && j == 1);
+  const double sub = comp == 0 ? d.scal[0] : 0.0;
+  const T *src = reinterpret_cast<const T *>(d.rhs[comp]) + d.sy * (row_ok ? j : 1) + tx;
+  // planes [pbeg, pend); the host keeps 2 w + 1 <= nz and WZ <= 2 w, so
+  // -nz < pbeg and one wrap per step suffices
+  const int pbeg = kb - WZ, pend = ke + WZ;
+  const int64_t wrap = d.sz * (int64_t)nz;
+  int lk = pbeg < 0 ? pbeg + nz : pbeg;  // next plane to load
+  const T *lplane = src + d.sz * (int64_t)lk;
+  double na[CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) na[c] = row_ok ? (double)lplane[c * btx] - sub : 0.0;
+  lplane += d.sz;
+  if (++lk == nz) { lk = 0; lplane -= wrap; }
+  T *dst = reinterpret_cast<T *>(d.dq[comp]) + d.sy * j + tx;
+  double win[CPT][RS];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c)
+#pragma unroll
+    for (int q = 0; q < RS; ++q) win[c][q] = 0.0;
+  int buf = 0;
+  for (int p0 = pbeg; p0 < pend; p0 += RS) {
+#pragma unroll
+    for (int u = 0; u < RS; ++u) {
+      const int p = p0 + u;
+      if (p >= pend) break;  // uniform over the block
+      // publish plane p with its periodic halo (every position of the row
+      // is written for every plane), load plane p + 1.  One barrier per
+      // plane: a buffer is rewritten two planes later.
+      double *row = rows + (size_t)(buf * blockDim.y + ty) * RW;
+      buf ^= 1;
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        const int col = tx + c * btx;
+        row[col + WX] = na[c];
+        if (col < WX) row[col + nx + WX] = na[c];
+        if (col >= nx - WX) row[col - nx + WX] = na[c];
+      }
+      if (row_ok && p + 1 < pend) {
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) na[c] = (double)lplane[c * btx] - sub;
+      }
+      lplane += d.sz;
+      if (++lk == nz) { lk = 0; lplane -= wrap; }
+      __syncthreads();
+#pragma unroll
+      for (int c = 0; c < CPT; ++c) {
+        const double *rr = row + tx + c * btx + WX;
+        double xs = sp.bgx[0] * rr[0];
+#pragma unroll
+        for (int m = 1; m <= WX; ++m) xs += sp.bgx[m] * (rr[-m] + rr[m]);
+        win[c][u] = xs;
+      }
+      if (p - WZ >= kb) {
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+          // window planes p - 2 WZ .. p; plane p - t sits in slot (u - t) mod RS
+          double acc = sp.bgz[0] * win[c][(u + WZ + 1) % RS];
+#pragma unroll
+          for (int m = 1; m <= WZ; ++m)
+            acc += sp.bgz[m] * (win[c][(u + WZ + 1 - m) % RS] + win[c][(u + WZ + 1 + m) % RS]);
+          if (row_ok) dst[c * btx + d.sz * (int64_t)(p - WZ)] = (T)acc;
+        }
+      }
+    }
+  }
 }
+
+template <typename T, int WX, int WZ>
+static void launch_adixz_w(dim3 grid, cudaStream_t st, const TGDev &d, const SubParams &sp) {
+  k_adixz_band<T, WX, WZ><<<grid, dim3(BM_TX, BM_TY), 0, st>>>(d, sp);
+}
+static int band_tw_index(int w) {
+  for (int q = 0; q < 5; ++q)
+    if (w <= BAND_TW[q]) return q;
+  return -1;
+}
+#define CHAPSIM_ADIXZ_ROW(T, WX)                                                                          \
+  { launch_adixz_w<T, WX, 2>, launch_adixz_w<T, WX, 4>, launch_adixz_w<T, WX, 6>, launch_adixz_w<T, WX, 8>, \
+    launch_adixz_w<T, WX, 12> }
+template <typename T>
+static void launch_adixz(dim3 grid, cudaStream_t st, const TGDev &d, const SubParams &sp) {
+  typedef void (*Fn)(dim3, cudaStream_t, const TGDev &, const SubParams &);
+  static const Fn fns[5][5] = {CHAPSIM_ADIXZ_ROW(T, 2), CHAPSIM_ADIXZ_ROW(T, 4), CHAPSIM_ADIXZ_ROW(T, 6),
+                               CHAPSIM_ADIXZ_ROW(T, 8), CHAPSIM_ADIXZ_ROW(T, 12)};
+  // the band form is on only when 0 <= wx, wz <= BAND_WMAX
+  fns[band_tw_index(sp.wx)][band_tw_index(sp.wz)](grid, st, d, sp);
+}
+#undef CHAPSIM_ADIXZ_ROW
+
+constexpr int AR_SEG = 64;  // planes per block of the row form
+// columns per thread of the row form for this nx (0: the tile form runs)
+static int adixz_row_cpt(int nx) {
+  if (nx <= 256) return 1;
+  if (nx <= 512 && nx % 2 == 0) return 2;
+  return 0;
+}
+template <typename T, int WX, int WZ, int CPT>
+static void launch_adixz_row_w(dim3 grid, dim3 blk, size_t smem, cudaStream_t st, const TGDev &d,
+                               const SubParams &sp) {
+  k_adixz_row<T, WX, WZ, CPT><<<grid, blk, smem, st>>>(d, sp, AR_SEG);
+}
+#define CHAPSIM_ADIXZ_RROW(T, WX, CPT)                                                            \
+  { launch_adixz_row_w<T, WX, 2, CPT>, launch_adixz_row_w<T, WX, 4, CPT>, launch_adixz_row_w<T, WX, 6, CPT>, \
+    launch_adixz_row_w<T, WX, 8, CPT>, launch_adixz_row_w<T, WX, 12, CPT> }
+// the row form of the x / z factors; false when this nx needs the tile form
+template <typename T>
+static bool launch_adixz_rows(cudaStream_t st, const TGDev &d, const SubParams &sp) {
+  const int cpt = adixz_row_cpt(d.nx);
+  if (!cpt) return false;
+  typedef void (*Fn)(dim3, dim3, size_t, cudaStream_t, const TGDev &, const SubParams &);
+  static const Fn f1[5][5] = {CHAPSIM_ADIXZ_RROW(T, 2, 1), CHAPSIM_ADIXZ_RROW(T, 4, 1), CHAPSIM_ADIXZ_RROW(T, 6, 1),
+                              CHAPSIM_ADIXZ_RROW(T, 8, 1), CHAPSIM_ADIXZ_RROW(T, 12, 1)};
+  static const Fn f2[5][5] = {CHAPSIM_ADIXZ_RROW(T, 2, 2), CHAPSIM_ADIXZ_RROW(T, 4, 2), CHAPSIM_ADIXZ_RROW(T, 6, 2),
+                              CHAPSIM_ADIXZ_RROW(T, 8, 2), CHAPSIM_ADIXZ_RROW(T, 12, 2)};
+  const int iw = band_tw_index(sp.wx), iz = band_tw_index(sp.wz);
+  const int btx = d.nx / cpt, bty = btx >= 256 ? 1 : 256 / btx;
+  dim3 blk(btx, bty), grid((d.ny + bty - 1) / bty, 3 * ((d.nz + AR_SEG - 1) / AR_SEG));
+  const size_t smem = (size_t)2 * bty * (d.nx + 2 * BAND_TW[iw]) * sizeof(double);
+  (cpt == 1 ? f1 : f2)[iw][iz](grid, blk, smem, st, d, sp);
+  return true;
+}
+#undef CHAPSIM_ADIXZ_RROW
 
 // MOMFA3_Y_tg (src/MOMFA_tg.f90:173-240) applied as the banded part of the
 // exact inverse of each component's y tridiagonal matrix (rows j = 1..ny),
@@ -1238,7 +1393,7 @@ template <typename T> struct Prec {
     const void *dyn[] = {(const void *)k_rhs_tma<T>,      (const void *)k_adix<T>,           (const void *)k_adiz<T>,
                          (const void *)k_fftx<T, false>,  (const void *)k_ifftx<T, false>,   (const void *)k_fftz<T, false>,
                          (const void *)k_fftx<T, true>,   (const void *)k_ifftx<T, true>,    (const void *)k_fftz<T, true>,
-                         (const void *)k_adiy_smem<T>,    (const void *)k_adixz_band<T>};
+                         (const void *)k_adiy_smem<T>};
     for (const void *f : dyn) {
       cudaFuncAttributes fa;
       CK(cudaFuncGetAttributes(&fa, f));
@@ -1345,7 +1500,7 @@ template <typename T> struct Prec {
     phase_mark(c, CHAPSIM_PH_ADIX);
     if (sp.band) {
       dim3 grid((d.nx + BM_TX - 1) / BM_TX, (d.ny + BM_TY - 1) / BM_TY, 3 * ((d.nz + BM_SEG - 1) / BM_SEG));
-      k_adixz_band<T><<<grid, dim3(BM_TX, BM_TY), band_smem(sp.wx, sp.wz), c->stream>>>(d, sp);
+      if (!launch_adixz_rows<T>(c->stream, d, sp)) launch_adixz<T>(grid, c->stream, d, sp);
       LAUNCHED();
       phase_mark(c, CHAPSIM_PH_ADIZ);
     } else {

@@ -35,10 +35,26 @@ def test_xz_statistics_parity():
     o.step(1)
     g.pp_mean_zx()
     a, n = g.stats(0)
-    b = o.stats()
     assert n == 0
+    # the statistics kernel on its own: the oracle's restatement applied to
+    # the GPU's own fields, 1e-12 per group
+    for f in ("u", "v", "w", "p"):
+        o.set(f, g.get_field(f))
+    b = o.stats()
     for name, (lo, hi) in GROUPS.items():
         assert relerr(a[:, lo:hi], b[:, lo:hi]) <= 1e-12, name
+    # end to end (each side's own step): the fields agree to round-off
+    # (1e-10 is the field parity bound), and the velocity-pressure
+    # correlations, a few percent of max|u| max|p|, show that round-off
+    # magnified; every group within the field bound
+    from oracle.pyoracle import OracleTG
+    o2 = OracleTG(48, 20, 40)
+    o2.init_random(4, 0.1)
+    o2.substep(0)
+    o2.step(1)
+    c = o2.stats()
+    for name, (lo, hi) in GROUPS.items():
+        assert relerr(a[:, lo:hi], c[:, lo:hi]) <= 1e-10, name
     # DVDL2 is symmetric in (m,h) <-> (n,p)
     d2 = a[:, 41:].reshape(-1, 9, 9)
     assert np.array_equal(d2, np.transpose(d2, (0, 2, 1)))
