@@ -413,8 +413,8 @@ def run_io(args, wl, ws, rank, local):
 
 def run_pair(args, wl, ws, rank, local):
     """TG and IO sections of the coupled configuration, one step of each per
-    step, on their own streams (allowed to overlap, joined before the end
-    event).  value = (TG cells + IO cells) x steps / time."""
+    step, on their own streams chained by events (they alternate, joined
+    before the end event).  value = (TG cells + IO cells) x steps / time."""
     import torch
 
     import chapsim1ww_b200 as cs
@@ -463,8 +463,19 @@ def run_pair(args, wl, ws, rank, local):
         return e0.elapsed_time(e1)
 
     def both(n):
-        tg.step(n)
-        io.step(n)
+        # one step of each section per step, on their own streams, chained by
+        # events so that they alternate: measured faster (16.2 against
+        # 16.8-17.7 ms per step at 256x192x256 + 512x192x256) than letting
+        # the two sections' HBM-bound kernels overlap and compete
+        for _ in range(n):
+            tg.step(1)
+            e = torch.cuda.Event()
+            e.record(st)
+            si.wait_event(e)
+            io.step(1)
+            e = torch.cuda.Event()
+            e.record(si)
+            st.wait_event(e)
 
     both(args.warmup)
     tg.sync()
@@ -567,7 +578,7 @@ def run_pair(args, wl, ws, rank, local):
                        "io": {**{k: wi[k] for k in ("nx", "ny", "nz", "ren", "dt", "prt")},
                               "table": wi["table"], "wall_heat_flux": wi["qw"], "x": "periodic (inlet coupling not built)"},
                        "cells": cells, "precision": args.precision,
-                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU, two streams",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU, two streams alternating per step",
                        "l2": "working set (>4 GB) larger than the 126 MB L2"},
             "sections_ms_per_step": {"tg": ms_tg, "io": ms_io, "both": ms / args.steps},
             "max_div_u_tg": tg.divgck_tg(), "max_div_g_plus_drho_io": io.divgck_io(),
