@@ -104,6 +104,14 @@ __device__ __forceinline__ void dft_small(C *v, const C *tw, int n, int sign) {
   }
 }
 
+// Shared-memory position of element p of a line-major buffer: the low three
+// bits are XORed with bits 3..5, a permutation inside every aligned group of
+// eight elements.  The Stockham stages write at stride R (radix 8: eight
+// 16-byte elements, one bank group); swizzled, those writes and the
+// contiguous reads both spread over all banks.  Buffers indexed this way are
+// sized to a multiple of eight elements.
+__device__ __forceinline__ int swz(int p) { return p ^ ((p >> 3) & 7); }
+
 template <typename C, int R>
 __device__ __forceinline__ void stockham_stage(const C *__restrict__ in, C *__restrict__ out, int nlines,
                                                int n, int lstride, int Ns, const C *__restrict__ tw,
@@ -115,25 +123,25 @@ __device__ __forceinline__ void stockham_stage(const C *__restrict__ in, C *__re
     const int line = t / nb;
     const int j = t - line * nb;
     const int k = j % Ns;
-    const C *src = in + line * lstride;
-    C *dst = out + line * lstride;
+    const int l0 = line * lstride;
     C v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = src[j + r * nb];
+    for (int r = 0; r < R; ++r) v[r] = in[swz(l0 + j + r * nb)];
     if (k != 0) {
 #pragma unroll
       for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twiddle(tw, r * k * tstep, sign));  // r k tstep < n
     }
     dft_small<C, R>(v, tw, n, sign);
-    const int base = (j / Ns) * Ns * R + k;
+    const int base = l0 + (j / Ns) * Ns * R + k;
 #pragma unroll
-    for (int r = 0; r < R; ++r) dst[base + r * Ns] = v[r];
+    for (int r = 0; r < R; ++r) out[swz(base + r * Ns)] = v[r];
   }
 }
 
 // Transform nlines lines (each n complex values, stride lstride) held in
-// shared memory buffer a; b is scratch of the same size.  Returns the buffer
-// holding the result.  Must be called by every thread of the block.
+// shared memory buffer a at swizzled positions (swz of line * lstride + e);
+// b is scratch of the same size.  Returns the buffer holding the result.
+// Must be called by every thread of the block.
 // BIG selects whether radices 7 and 11 are compiled in (they raise register
 // use of every stage, so plans with only 2, 3, 4, 5, 8 use the small variant).
 template <typename C, bool BIG>

@@ -940,7 +940,7 @@ __global__ void __launch_bounds__(256, BIG ? 2 : 3) k_fftx(TGDev d, SubParams sp
         val = U[r * nx + i];
       }
     }
-    C *z = A + (r >> 1) * nx + i;
+    C *z = A + swz((r >> 1) * nx + i);
     if (r & 1) z->y = (T)val; else z->x = (T)val;
   }
   __syncthreads();
@@ -949,8 +949,8 @@ __global__ void __launch_bounds__(256, BIG ? 2 : 3) k_fftx(TGDev d, SubParams sp
   C *S = reinterpret_cast<C *>(d.spec);
   for (int t = tid; t < nl * lh; t += blockDim.x) {
     const int p = t / lh, kx = t - p * lh;
-    const C z = res[p * nx + kx];
-    const C zc = cconj(res[p * nx + (kx == 0 ? 0 : nx - kx)]);
+    const C z = res[swz(p * nx + kx)];
+    const C zc = cconj(res[swz(p * nx + (kx == 0 ? 0 : nx - kx))]);
     C x0, x1;
     x0.x = (T)0.5 * (z.x + zc.x) * scale;
     x0.y = (T)0.5 * (z.y + zc.y) * scale;
@@ -1179,10 +1179,10 @@ __global__ void __launch_bounds__(256, BIG ? 2 : 3) k_ifftx(TGDev d, FFTPlan pl,
     if (kx == 0 || 2 * kx == nx) { x0.y = 0; x1.y = 0; }
     // Z(k) = X0 + i X1 ; Z(n-k) = conj(X0) + i conj(X1)
     C z; z.x = x0.x - x1.y; z.y = x0.y + x1.x;
-    A[p * nx + kx] = z;
+    A[swz(p * nx + kx)] = z;
     if (kx != 0 && 2 * kx != nx) {
       C zc; zc.x = x0.x + x1.y; zc.y = -x0.y + x1.x;
-      A[p * nx + (nx - kx)] = zc;
+      A[swz(p * nx + (nx - kx))] = zc;
     }
   }
   __syncthreads();
@@ -1190,7 +1190,7 @@ __global__ void __launch_bounds__(256, BIG ? 2 : 3) k_ifftx(TGDev d, FFTPlan pl,
   for (int t = tid; t < nrow * nx; t += blockDim.x) {
     const int r = t / nx, i = t - r * nx;
     const int j = jbeg + r;
-    const C z = res[(r >> 1) * nx + i];
+    const C z = res[swz((r >> 1) * nx + i)];
     const double val = (r & 1) ? (double)z.y : (double)z.x;
     const int64_t c0 = i + d.sy * j + d.sz * k;
     const double out = accumulate ? d.phi[c0] + val : val;
