@@ -119,10 +119,14 @@ __device__ __forceinline__ void stockham_stage(const C *__restrict__ in, C *__re
   const int nb = n / R;
   const int total = nlines * nb;
   const int tstep = n / (Ns * R);
+  // power-of-two divisors (every stage of a power-of-two plan) by shifts
+  const bool nb2 = (nb & (nb - 1)) == 0, ns2 = (Ns & (Ns - 1)) == 0;
+  const int lnb = __ffs(nb) - 1, lns = __ffs(Ns) - 1;
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    const int line = t / nb;
+    const int line = nb2 ? t >> lnb : t / nb;
     const int j = t - line * nb;
-    const int k = j % Ns;
+    const int jq = ns2 ? j >> lns : j / Ns;
+    const int k = j - jq * Ns;
     const int l0 = line * lstride;
     C v[R];
 #pragma unroll
@@ -132,7 +136,7 @@ __device__ __forceinline__ void stockham_stage(const C *__restrict__ in, C *__re
       for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twiddle(tw, r * k * tstep, sign));  // r k tstep < n
     }
     dft_small<C, R>(v, tw, n, sign);
-    const int base = l0 + (j / Ns) * Ns * R + k;
+    const int base = l0 + jq * Ns * R + k;
 #pragma unroll
     for (int r = 0; r < R; ++r) out[swz(base + r * Ns)] = v[r];
   }
@@ -168,19 +172,25 @@ __device__ C *fft_lines(C *a, C *b, int nlines, int n, int lstride, const int *r
 }
 
 // The same stages on lines stored interleaved: element e of line l at
-// buf[e * nl + l] (consecutive lines adjacent).  Consecutive threads take
-// consecutive lines, so each stage's reads and writes are contiguous rows.
-// Per element the arithmetic is that of stockham_stage.
+// buf[e * nl + l] (consecutive lines adjacent; nl a power of two).
+// Consecutive threads take consecutive lines, so each stage's reads and
+// writes are contiguous rows.  Per element the arithmetic is that of
+// stockham_stage.
 template <typename C, int R>
 __device__ __forceinline__ void stockham_stage_il(const C *__restrict__ in, C *__restrict__ out, int nl, int n,
                                                   int Ns, const C *__restrict__ tw, int sign) {
   const int nb = n / R;
   const int total = nl * nb;
   const int tstep = n / (Ns * R);
+  // nl is a power of two; Ns is one in every power-of-two stage
+  const int lnl = __ffs(nl) - 1;
+  const bool ns2 = (Ns & (Ns - 1)) == 0;
+  const int lns = __ffs(Ns) - 1;
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    const int j = t / nl;
-    const int line = t - j * nl;
-    const int k = j % Ns;
+    const int j = t >> lnl;
+    const int line = t & (nl - 1);
+    const int jq = ns2 ? j >> lns : j / Ns;
+    const int k = j - jq * Ns;
     C v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = in[(j + r * nb) * nl + line];
@@ -189,7 +199,7 @@ __device__ __forceinline__ void stockham_stage_il(const C *__restrict__ in, C *_
       for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twiddle(tw, r * k * tstep, sign));
     }
     dft_small<C, R>(v, tw, n, sign);
-    const int base = (j / Ns) * Ns * R + k;
+    const int base = jq * Ns * R + k;
 #pragma unroll
     for (int r = 0; r < R; ++r) out[(base + r * Ns) * nl + line] = v[r];
   }

@@ -1013,8 +1013,9 @@ __global__ void __launch_bounds__(256, BIG ? 2 : 3) k_fftz(TGDev d, FFTPlan pl, 
   C *res = fft_lines_il<C, BIG>(A, B, lz, nz, rad, pl.nrad,
                                 (const C *)(sizeof(T) == 8 ? (const void *)pl.tw64 : (const void *)pl.tw32), sign);
   const T scale = sign < 0 ? (T)(1.0 / nz) : (T)1;
+  const int llz = __ffs(lz) - 1;  // lz is a power of two
   for (int t = tid; t < nz * lz; t += blockDim.x) {
-    const int kz = t / lz, l = t - kz * lz;
+    const int kz = t >> llz, l = t & (lz - 1);
     if (l < nl) {
       C v = res[t];
       v.x *= scale;
