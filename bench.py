@@ -71,7 +71,7 @@ METRIC = "cell-steps/s"
 # of 8-byte values per cell (spectral phases: per complex spectral value).
 PHASE_VALUES_PER_CELL = {"rhs": 13, "adix": 6, "adiz": 6, "adiy": 9, "fftx": 4, "corr": 10}
 PHASE_SPECTRAL_PASSES = {"fftx": 1, "fftz": 2, "ysolve": 2, "ifftz": 2, "ifftx": 1}
-PHASE_KERNEL = {"rhs": "k_rhs_tma", "adix": "k_adixz_band", "adiz": "k_adixz_band", "adiy": "k_adiy_band",
+PHASE_KERNEL = {"rhs": "k_rhs_tma", "adix": "k_adixz_row", "adiz": "k_adixz_row", "adiy": "k_adiy_band",
                 "fftx": "k_fftx", "fftz": "k_fftz", "ysolve": "k_ysolve_line", "ifftz": "k_fftz", "ifftx": "k_ifftx",
                 "corr": "k_corr"}
 
