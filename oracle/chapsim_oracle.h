@@ -130,6 +130,43 @@ void oracle_io_set_dt(oracle_io *o, double dt);
 /* visthemflg: 0 explicit viscous terms (default), 1 the semi-implicit scheme
  * (VISCOUS_PAR_EXPLT_*_io + MOMFA_io).  Set before oracle_io_init_random. */
 int oracle_io_set_scheme(oracle_io *o, int implicit);
+/* Coupled inflow/outflow boundary planes of the IO section (row a16): ghost
+ * planes i = 0 and i = NCL1_io + 1, each (nz, ny + 2), ids ORC_P_*. */
+#define ORC_P_IN_U 0
+#define ORC_P_IN_V 1
+#define ORC_P_IN_W 2
+#define ORC_P_IN_GX 3
+#define ORC_P_IN_GY 4
+#define ORC_P_IN_GZ 5
+#define ORC_P_IN_P 6
+#define ORC_P_IN_RHO 7
+#define ORC_P_OUT_U 8
+#define ORC_P_OUT_V 9
+#define ORC_P_OUT_W 10
+#define ORC_P_OUT_GX 11
+#define ORC_P_OUT_GY 12
+#define ORC_P_OUT_GZ 13
+#define ORC_P_OUT_RHO 14
+#define ORC_P_OUT_RHOH 15
+#define ORC_P_OUT_H 16
+#define ORC_P_OUT_T 17
+#define ORC_P_OUT_MU 18
+#define ORC_P_OUT_K 19
+#define ORC_P_CONV0_X 20
+#define ORC_P_CONV0_Y 21
+#define ORC_P_CONV0_Z 22
+#define ORC_P_CONV0_ENG 23
+#define ORC_P_COUNT 24
+/* BC_TINLET_FLOW + BC_TINLET_THERML from TG arrays (nz, ny + 2, nxt) */
+void oracle_io_bc_inlet(oracle_io *o, int nxt, const double *tu, const double *tv, const double *tw,
+                        const double *tp);
+int oracle_io_bc_outlet_mom(oracle_io *o, int ns); /* BC_COUTLET_MOM_RK3 with CHK_MassConsv_io */
+int oracle_io_bc_outlet_eng(oracle_io *o, int ns); /* BC_COUTLET_ENEG_RK3 */
+int oracle_io_get_plane(const oracle_io *o, int which, double *out);
+int oracle_io_set_plane(oracle_io *o, int which, const double *in);
+/* U_OUTLET (momentum), CHK_Mass_CONSV0_SCALING, CHK_MASS_CONSV0, inflow,
+ * outflow, mass rate, U_OUTLET (energy) */
+void oracle_io_bc_scalars(const oracle_io *o, double *out);
 double oracle_tg_cfl(const oracle_tg *o);            /* CFL_tg */
 void oracle_tg_set_dt(oracle_tg *o, double dt);
 void oracle_tg_stats(const oracle_tg *o, double *out); /* PP_MEAN_ZX_FLOW_TG, ny * 122 values */

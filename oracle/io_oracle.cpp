@@ -69,6 +69,7 @@
 //    side back into RHSLLPHI_io (src/possion3d_fishpack_reform.f90:456-463):
 //    spectral coefficients used as a physical field.  Here the physical
 //    right-hand side of the Poisson equation is used, as PRCALC_tg does.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -146,8 +147,14 @@ struct oracle_io {
   std::vector<double> rhsio[4], adv[4], drhoi[4];  // RHS_io per component, DIVU_io (density part), DRHOI_STG
   std::vector<double> amvr13, apvr13, amvr2, apvr2;  // TDMA_COEF y-operators, 1-based
   double amvr1 = 0.0, apvrn = 0.0;
+  // coupled inflow/outflow ghost planes (i = 0 and i = NCL1_io + 1), each
+  // (nz, ny + 2), ids ORC_P_*; bcs: U_OUTLET (momentum), scaling, balance,
+  // inflow, outflow, mass rate, U_OUTLET (energy)
+  std::vector<double> bcp[ORC_P_COUNT];
+  double bcs[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 
   int64_t len() const { return (int64_t)nx * (ny + 2) * nz; }
+  inline int64_t pj(int j, int k) const { return (int64_t)j + (int64_t)(ny + 2) * (k - 1); }
   inline int64_t id(int i, int j, int k) const {
     return (int64_t)(i - 1) + (int64_t)nx * ((int64_t)j + (int64_t)(ny + 2) * (k - 1));
   }
@@ -1300,6 +1307,37 @@ void velo2massflux(oracle_io *o) {
   bc_wall_vec(o, o->g);
 }
 
+// ------------------------------------------ coupled inflow/outflow planes
+// CONVCTION_OUTLET_U (src/BC_COUTLET_MOM_RK3.f90:101-174, method two):
+// U_OUTLET = (max + min) / 2 of the outlet-face mean 0.5 (u(NCL1) + u(NCL1+1)).
+double convection_outlet_u(const oracle_io *o) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  double umax = -1.0e20, umin = 1.0e20;
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j) {
+      const double ucc = (FC(q, 1, nx, j, k) + o->bcp[ORC_P_OUT_U][o->pj(j, k)]) * 0.5;
+      if (ucc > umax) umax = ucc;
+      if (ucc < umin) umin = ucc;
+    }
+  return 0.5 * (umax + umin);
+}
+
+// BC_WALL_G_io / BC_WALL_Q_io (src/BC_WALL.f90:233-256, 412-460) on the outlet
+// plane: u, w zero on both ghost rows, v zero on rows 0, 1 and ny + 1.
+void outlet_plane_walls(oracle_io *o) {
+  const int ny = o->ny, nz = o->nz;
+  const int ig[3] = {ORC_P_OUT_GX, ORC_P_OUT_GY, ORC_P_OUT_GZ}, iq[3] = {ORC_P_OUT_U, ORC_P_OUT_V, ORC_P_OUT_W};
+  for (int k = 1; k <= nz; ++k)
+    for (int s = 0; s < 2; ++s) {
+      const int *ids = s ? iq : ig;
+      o->bcp[ids[0]][o->pj(0, k)] = 0.0;
+      o->bcp[ids[2]][o->pj(0, k)] = 0.0;
+      o->bcp[ids[1]][o->pj(1, k)] = 0.0;
+      o->bcp[ids[1]][o->pj(0, k)] = 0.0;
+      for (int c = 0; c < 3; ++c) o->bcp[ids[c]][o->pj(ny + 1, k)] = 0.0;
+    }
+}
+
 }  // namespace
 
 extern "C" {
@@ -1347,6 +1385,8 @@ oracle_io *oracle_io_create(int nx, int ny, int nz, double lx, double lz, double
     o->rhsio[c].assign(n, 0.0); o->adv[c].assign(n, 0.0); o->drhoi[c].assign(n, 0.0);
   }
   vis_ycoef(o);
+  for (int q = 0; q < ORC_P_COUNT; ++q) o->bcp[q].assign((size_t)(ny + 2) * nz, 0.0);
+  o->bcp[ORC_P_IN_RHO].assign((size_t)(ny + 2) * nz, 1.0);
   o->dftx = oracle_dft_create(nx);
   o->dftz = oracle_dft_create(nz);
   return o;
@@ -1564,6 +1604,182 @@ int oracle_io_set_scheme(oracle_io *o, int implicit) {
   o->implicit = implicit;
   for (int c = 1; c <= 3; ++c) std::fill(o->drhoi[c].begin(), o->drhoi[c].end(), 0.0);
   return 0;
+}
+
+
+// BC_TINLET_FLOW + BC_TINLET_THERML (src/BC_INLET.f90:2-51, 54-76): the TG
+// section's last plane (and its first-face u) feed the IO inlet ghost plane
+// i = 0 and the first face i = 1; the inlet ghost properties are the
+// reference state (rho = 1).  TG arrays: (nz, ny + 2, nxt).
+void oracle_io_bc_inlet(oracle_io *o, int nxt, const double *tu, const double *tv, const double *tw,
+                        const double *tp) {
+  const int ny = o->ny, nz = o->nz;
+  auto T = [&](const double *a, int i, int j, int k) {
+    return a[(int64_t)(i - 1) + (int64_t)nxt * ((int64_t)j + (int64_t)(ny + 2) * (k - 1))];
+  };
+  for (int j = 0; j <= ny + 1; ++j)
+    for (int k = 1; k <= nz; ++k) {
+      const int64_t pc = o->pj(j, k);
+      const double rin = 1.0;  // DENSITY(0, J, K) from BC_TINLET_THERML
+      o->bcp[ORC_P_IN_RHO][pc] = rin;
+      o->bcp[ORC_P_IN_U][pc] = T(tu, nxt, j, k);
+      FC(q, 1, 1, j, k) = T(tu, 1, j, k);
+      o->bcp[ORC_P_IN_GX][pc] = o->bcp[ORC_P_IN_U][pc] * rin;
+      FC(g, 1, 1, j, k) = FC(q, 1, 1, j, k) * (rin + F(dd, 1, j, k)) * XND2CL;
+      o->bcp[ORC_P_IN_V][pc] = T(tv, nxt, j, k);
+      o->bcp[ORC_P_IN_GY][pc] = o->bcp[ORC_P_IN_V][pc] * rin;
+      o->bcp[ORC_P_IN_W][pc] = T(tw, nxt, j, k);
+      o->bcp[ORC_P_IN_GZ][pc] = o->bcp[ORC_P_IN_W][pc] * rin;
+      o->bcp[ORC_P_IN_P][pc] = T(tp, nxt, j, k);
+    }
+}
+
+// BC_COUTLET_MOM_RK3 (src/BC_COUTLET_MOM_RK3.f90:2-97): convective outlet
+// dG/dt + U_OUTLET dG/dx = 0 on the ghost plane i = NCL1 + 1 with the RK3
+// weights (BC_CONV0 the previous substep's term), then CHK_MassConsv_io
+// (src/processing/CHK_conservation.f90:2-71) and the rescaling of the outlet
+// x-flux so that inflow - d(rho)/dt = outflow, then the wall conditions.
+int oracle_io_bc_outlet_mom(oracle_io *o, int ns) {
+  if (ns < 0 || ns > 3) return 1;
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  const double U = convection_outlet_u(o);
+  o->bcs[0] = U;
+  const double coe1 = o->dxi * U;
+  const int ig[4] = {0, ORC_P_OUT_GX, ORC_P_OUT_GY, ORC_P_OUT_GZ};
+  const int iq[4] = {0, ORC_P_OUT_U, ORC_P_OUT_V, ORC_P_OUT_W};
+  const int ic[4] = {0, ORC_P_CONV0_X, ORC_P_CONV0_Y, ORC_P_CONV0_Z};
+  for (int idr = 1; idr <= 3; ++idr) {
+    const int n2i = idr == 2 ? 2 : 1;
+    for (int k = 1; k <= nz; ++k)
+      for (int j = n2i; j <= ny; ++j) {
+        const int64_t pc = o->pj(j, k);
+        double &gout = o->bcp[ig[idr]][pc];
+        const double conv = -(gout - FC(g, idr, nx, j, k)) * coe1;
+        const double rhs = o->tgam[ns] * conv + o->troh[ns] * o->bcp[ic[idr]][pc];
+        o->bcp[ic[idr]][pc] = conv;
+        gout = gout + o->dt * rhs;
+        const double rho = (F(dd, nx, j, k) + o->bcp[ORC_P_OUT_RHO][pc]) * XND2CL;
+        o->bcp[iq[idr]][pc] = gout / rho;
+      }
+  }
+  // CHK_MassConsv_io (RCCI1 = 1 in the channel)
+  double fin = 0.0, fout = 0.0, mass = 0.0;
+  for (int j = 1; j <= ny; ++j) {
+    const double coe2 = 1.0 / o->dyfi[j];
+    for (int k = 1; k <= nz; ++k) {
+      fin += FC(g, 1, 1, j, k) * coe2;
+      fout += o->bcp[ORC_P_OUT_GX][o->pj(j, k)] * coe2;
+    }
+  }
+  fin /= o->dzi;
+  fout /= o->dzi;
+  for (int j = 1; j <= ny; ++j) {
+    const double coe2 = 1.0 / o->dyfi[j];
+    for (int k = 1; k <= nz; ++k)
+      for (int i = 1; i <= nx; ++i) mass += F(drho, i, j, k) * coe2;
+  }
+  mass = mass / o->dzi / o->dxi;
+  const double scaling = (fin - mass) / fout;
+  o->bcs[1] = scaling;
+  o->bcs[2] = fin - mass - fout;
+  o->bcs[3] = fin;
+  o->bcs[4] = fout;
+  o->bcs[5] = mass;
+  for (int j = 1; j <= ny; ++j)
+    for (int k = 1; k <= nz; ++k) {
+      const int64_t pc = o->pj(j, k);
+      double &gout = o->bcp[ORC_P_OUT_GX][pc];
+      gout = gout * (scaling - 1.0) + gout;
+      const double rho = (F(dd, nx, j, k) + o->bcp[ORC_P_OUT_RHO][pc]) * XND2CL;
+      o->bcp[ORC_P_OUT_U][pc] = gout / rho;
+    }
+  outlet_plane_walls(o);
+  return 0;
+}
+
+// BC_COUTLET_ENEG_RK3 (src/BC_COUTLET_ENEG_RK3.f90:2-41): convective outlet
+// for rho h with the RK3 weights, then ENTHALPY_UPDATE, DENSITY_UPDATE,
+// ENTHALPY_UPDATE and THERM_PROP_UPDATE on the outlet plane
+// (src/THERM_PROP_UPDATE.f90, region IOULET) and BC_WALL_ISOFLUX on its
+// ghost rows.
+int oracle_io_bc_outlet_eng(oracle_io *o, int ns) {
+  if (ns < 0 || ns > 3 || !o->thermal || !o->has_table) return 1;
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  const double U = convection_outlet_u(o);
+  o->bcs[6] = U;
+  std::vector<double> &rh = o->bcp[ORC_P_OUT_RHOH], &hh = o->bcp[ORC_P_OUT_H], &tt = o->bcp[ORC_P_OUT_T];
+  std::vector<double> &dd = o->bcp[ORC_P_OUT_RHO], &mu = o->bcp[ORC_P_OUT_MU], &kk = o->bcp[ORC_P_OUT_K];
+  std::vector<double> &c0 = o->bcp[ORC_P_CONV0_ENG];
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j) {
+      const int64_t pc = o->pj(j, k);
+      const double conv = -o->dxi * U * (rh[pc] - F(rhoh, nx, j, k));
+      const double rhs = o->tgam[ns] * conv + o->troh[ns] * c0[pc];
+      c0[pc] = conv;
+      rh[pc] = rh[pc] + o->dt * rhs;
+    }
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j) {
+      const int64_t pc = o->pj(j, k);
+      double h = rh[pc] / dd[pc];
+      double T, D;
+      if (lookup_ht(o, h, T) && lookup_t(o, o->td, T, D))
+        dd[pc] = D;
+      else
+        ++o->bad;
+      h = rh[pc] / dd[pc];
+      hh[pc] = h;
+      if (o->shortcuts && std::fabs(h) < 1.0e-10) continue;  // properties kept
+      double M, K;
+      if (!lookup_ht(o, h, T) || !lookup_t(o, o->tm, T, M) || !lookup_t(o, o->tk, T, K) ||
+          !lookup_t(o, o->td, T, D)) {
+        ++o->bad;
+        continue;
+      }
+      tt[pc] = T;
+      mu[pc] = M;
+      kk[pc] = K;
+      dd[pc] = D;
+    }
+  for (int k = 1; k <= nz; ++k)
+    for (int side = 0; side < 2; ++side) {
+      const int j = side == 0 ? 0 : ny + 1;
+      double h;
+      if (side == 0)
+        h = 2.0 * hh[o->pj(1, k)] - o->wff[2] * hh[o->pj(2, k)] - o->wfb[2] * hh[o->pj(1, k)];
+      else
+        h = 2.0 * hh[o->pj(ny, k)] - o->wff[ny] * hh[o->pj(ny, k)] - o->wfb[ny] * hh[o->pj(ny - 1, k)];
+      const int64_t pc = o->pj(j, k);
+      hh[pc] = h;
+      double T, M, K, D;
+      if (!lookup_ht(o, h, T) || !lookup_t(o, o->tm, T, M) || !lookup_t(o, o->tk, T, K) ||
+          !lookup_t(o, o->td, T, D)) {
+        ++o->bad;
+        continue;
+      }
+      dd[pc] = D;
+      tt[pc] = T;
+      mu[pc] = M;
+      kk[pc] = K;
+      rh[pc] = h * D;
+    }
+  return 0;
+}
+
+int oracle_io_get_plane(const oracle_io *o, int which, double *out) {
+  if (which < 0 || which >= ORC_P_COUNT) return 1;
+  std::copy(o->bcp[which].begin(), o->bcp[which].end(), out);
+  return 0;
+}
+
+int oracle_io_set_plane(oracle_io *o, int which, const double *in) {
+  if (which < 0 || which >= ORC_P_COUNT) return 1;
+  std::copy(in, in + o->bcp[which].size(), o->bcp[which].begin());
+  return 0;
+}
+
+void oracle_io_bc_scalars(const oracle_io *o, double *out) {
+  for (int q = 0; q < 7; ++q) out[q] = o->bcs[q];
 }
 
 }  // extern "C"

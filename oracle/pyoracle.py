@@ -70,6 +70,12 @@ def load(build=True):
     for f in ("oracle_tg_set_dt", "oracle_io_set_dt"):
         getattr(L, f).argtypes = [P, D]
     L.oracle_io_set_scheme.argtypes = [P, I]
+    L.oracle_io_bc_inlet.argtypes = [P, I, P, P, P, P]
+    for f in ("oracle_io_bc_outlet_mom", "oracle_io_bc_outlet_eng"):
+        getattr(L, f).argtypes = [P, I]
+    L.oracle_io_get_plane.argtypes = [P, I, P]
+    L.oracle_io_set_plane.argtypes = [P, I, P]
+    L.oracle_io_bc_scalars.argtypes = [P, P]
     L.oracle_tg_stats.argtypes = [P, P]
     L.oracle_set_threads.argtypes = [I]
     L.oracle_get_threads.restype = I
@@ -177,6 +183,15 @@ def synth_table(n=4096):
     return cols
 
 
+# coupled inflow/outflow ghost planes (i = 0 and i = NCL1_io + 1), each
+# (nz, ny + 2); the same ids as the library's CHAPSIM_P_*
+IO_PLANES = {n: q for q, n in enumerate((
+    "in_u", "in_v", "in_w", "in_gx", "in_gy", "in_gz", "in_p", "in_rho",
+    "out_u", "out_v", "out_w", "out_gx", "out_gy", "out_gz", "out_rho", "out_rhoh", "out_h", "out_t", "out_mu",
+    "out_k", "conv0_x", "conv0_y", "conv0_z", "conv0_eng"))}
+IO_BC_SCALARS = ("u_outlet", "scaling", "balance", "inflow", "outflow", "mass_rate", "u_outlet_eng")
+
+
 class OracleIO:
     """x-periodic IO channel: SOLVERRK3_ENG_IO + SOLVERRK3_MOM_IO (explicit
     viscous terms, or with visc_scheme=1 the semi-implicit MOMFA_io scheme;
@@ -217,6 +232,33 @@ class OracleIO:
         a = np.ascontiguousarray(arr, dtype=np.float64)
         assert a.size == self.nx * (self.ny + 2) * self.nz
         assert self.L.oracle_io_set_field(self.h, IO_FIELDS[name], a.ctypes.data) == 0
+
+    # ---- coupled inflow/outflow boundary planes
+    def get_plane(self, name):
+        a = np.empty((self.nz, self.ny + 2))
+        assert self.L.oracle_io_get_plane(self.h, IO_PLANES[name], a.ctypes.data) == 0
+        return a
+
+    def set_plane(self, name, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        assert a.size == self.nz * (self.ny + 2)
+        assert self.L.oracle_io_set_plane(self.h, IO_PLANES[name], a.ctypes.data) == 0
+
+    def bc_tinlet_flow(self, tu, tv, tw, tp):
+        """BC_TINLET_FLOW + BC_TINLET_THERML from TG fields (nz, ny+2, nx_tg)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (tu, tv, tw, tp)]
+        self.L.oracle_io_bc_inlet(self.h, arrs[0].shape[-1], *[a.ctypes.data for a in arrs])
+
+    def bc_coutlet_mom_rk3(self, ns):
+        assert self.L.oracle_io_bc_outlet_mom(self.h, ns) == 0
+
+    def bc_coutlet_eneg_rk3(self, ns):
+        assert self.L.oracle_io_bc_outlet_eng(self.h, ns) == 0
+
+    def bc_scalars(self):
+        a = np.empty(7)
+        self.L.oracle_io_bc_scalars(self.h, a.ctypes.data)
+        return dict(zip(IO_BC_SCALARS, a.tolist()))
 
     def init_random(self, seed, amp=0.1):
         self.L.oracle_io_init_random(self.h, seed, amp)
