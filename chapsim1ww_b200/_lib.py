@@ -53,6 +53,13 @@ _I = ctypes.c_int
 _I64 = ctypes.c_int64
 _D = ctypes.c_double
 _DP = ctypes.POINTER(ctypes.c_double)
+# coupled inflow/outflow ghost planes of an IO context (CHAPSIM_P_*), each (nz, ny + 2)
+IO_PLANES = {n: q for q, n in enumerate((
+    "in_u", "in_v", "in_w", "in_gx", "in_gy", "in_gz", "in_p", "in_rho",
+    "out_u", "out_v", "out_w", "out_gx", "out_gy", "out_gz", "out_rho", "out_rhoh", "out_h", "out_t", "out_mu",
+    "out_k", "conv0_x", "conv0_y", "conv0_z", "conv0_eng"))}
+IO_BC_SCALARS = ("u_outlet", "scaling", "balance", "inflow", "outflow", "mass_rate", "u_outlet_eng")
+
 SIGNATURES = [
     ("chapsim_config_default", _I, [ctypes.POINTER(ChapsimConfig)]),
     ("chapsim_create", _I, [ctypes.POINTER(ChapsimConfig), ctypes.POINTER(_P)]),
@@ -64,6 +71,12 @@ SIGNATURES = [
     ("chapsim_get_field", _I, [_P, _I, _I, _P, _I64]),
     ("chapsim_set_field_async", _I, [_P, _I, _I, _P, _I64]),
     ("chapsim_get_field_async", _I, [_P, _I, _I, _P, _I64]),
+    ("chapsim_io_bc_inlet", _I, [_P, _P]),
+    ("chapsim_io_bc_outlet_mom", _I, [_P, _I]),
+    ("chapsim_io_bc_outlet_eng", _I, [_P, _I]),
+    ("chapsim_io_set_plane", _I, [_P, _I, _P, _I64]),
+    ("chapsim_io_get_plane", _I, [_P, _I, _P, _I64]),
+    ("chapsim_io_bc_scalars", _I, [_P, _P, _I]),
     ("chapsim_set_field_device", _I, [_P, _I, _I, _P, _I64]),
     ("chapsim_get_field_device", _I, [_P, _I, _I, _P, _I64]),
     ("chapsim_get_mesh", _I, [_P, _I, _P, _I64]),

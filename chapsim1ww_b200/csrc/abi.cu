@@ -527,6 +527,11 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
         ucaj = 4.0 / (2.0 / ctx->dyci[ny] + 1.0 / ctx->dyfi[ny]);
         io.apvrn = ucaj * (2.0 * ctx->dyfi[ny]);
       }
+      io.bps = (int64_t)(cfg->ny + 2) * cfg->nz;
+      if ((rc = dalloc(ctx, &p, ((size_t)io.bps * CHAPSIM_P_COUNT + 8) * sizeof(double)))) goto fail;
+      io.bcp = (double *)p;
+      io.bcs = io.bcp + (size_t)io.bps * CHAPSIM_P_COUNT;
+      cudaMemsetAsync(p, 0, ((size_t)io.bps * CHAPSIM_P_COUNT + 8) * sizeof(double), ctx->stream);
       if ((rc = dalloc(ctx, &p, sizeof(unsigned long long)))) goto fail;
       io.bad = (unsigned long long *)p;
       cudaMemsetAsync(p, 0, sizeof(unsigned long long), ctx->stream);
@@ -574,6 +579,7 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
     for (double *f : ones)
       if ((rc = fill_value(ctx, f, n, 1.0))) goto fail;
     if ((rc = fill_value(ctx, io.msum, n, 2.0))) goto fail;
+    if ((rc = fill_value(ctx, io.bcp + (size_t)io.bps * CHAPSIM_P_IN_RHO, (size_t)io.bps, 1.0))) goto fail;
   }
   if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { rc = CHAPSIM_ERR_CUDA; goto fail; }
   *out = ctx;
@@ -1119,6 +1125,74 @@ int chapsim_rk3_mom_io(chapsim_ctx *ctx, int ns) {
   REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
   CKC(cudaSetDevice(ctx->device));
   return io_mom(ctx, ns, ns >= 1);
+}
+
+// Coupled inflow/outflow boundary planes (BC_TINLET_FLOW, BC_COUTLET_MOM_RK3,
+// BC_COUTLET_ENEG_RK3): io_kernels.cu.
+int chapsim_io_bc_inlet(chapsim_ctx *ctx, chapsim_ctx *tg) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(tg, CHAPSIM_ERR_ARG, "null TG context");
+  REQUIRE(ctx->domain == CHAPSIM_IIO, CHAPSIM_ERR_STATE, "not an IO context");
+  REQUIRE(tg->domain == CHAPSIM_ITG, CHAPSIM_ERR_ARG, "the inlet source must be a TG context");
+  REQUIRE(tg->device == ctx->device, CHAPSIM_ERR_UNSUPPORTED, "the TG and IO contexts are on different devices");
+  REQUIRE(tg->cfg.ny == ctx->cfg.ny && tg->cfg.nz == ctx->cfg.nz, CHAPSIM_ERR_ARG,
+          "the TG and IO sections differ in ny or nz");
+  CKC(cudaSetDevice(ctx->device));
+  CKC(cudaStreamSynchronize(tg->stream));  // the TG fields are final
+  const int rc = io_bc_inlet(ctx, tg);
+  if (rc) return rc;
+  CKC(cudaStreamSynchronize(ctx->stream));  // the TG fields may change after return
+  return CHAPSIM_OK;
+}
+
+int chapsim_io_bc_outlet_mom(chapsim_ctx *ctx, int ns) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(ctx->domain == CHAPSIM_IIO, CHAPSIM_ERR_STATE, "not an IO context");
+  REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
+  CKC(cudaSetDevice(ctx->device));
+  return io_bc_outlet_mom(ctx, ns);
+}
+
+int chapsim_io_bc_outlet_eng(chapsim_ctx *ctx, int ns) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(ctx->domain == CHAPSIM_IIO, CHAPSIM_ERR_STATE, "not an IO context");
+  REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
+  REQUIRE(ctx->io.thermal && ctx->has_table, CHAPSIM_ERR_STATE,
+          "the outlet energy condition needs the energy equation and a property table");
+  CKC(cudaSetDevice(ctx->device));
+  return io_bc_outlet_eng(ctx, ns);
+}
+
+static int plane_copy(chapsim_ctx *ctx, int plane, void *host, int64_t n, bool to_dev) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(ctx->domain == CHAPSIM_IIO, CHAPSIM_ERR_STATE, "not an IO context");
+  REQUIRE(plane >= 0 && plane < CHAPSIM_P_COUNT, CHAPSIM_ERR_ARG, "unknown plane id");
+  REQUIRE(host, CHAPSIM_ERR_ARG, "null buffer");
+  REQUIRE(n == ctx->io.bps, CHAPSIM_ERR_ARG, "plane length must be (ny + 2) * nz");
+  CKC(cudaSetDevice(ctx->device));
+  double *p = ctx->io.bcp + (size_t)plane * ctx->io.bps;
+  if (to_dev)
+    CKC(cudaMemcpyAsync(p, host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  else
+    CKC(cudaMemcpyAsync(host, p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CKC(cudaStreamSynchronize(ctx->stream));
+  return CHAPSIM_OK;
+}
+int chapsim_io_set_plane(chapsim_ctx *ctx, int plane, const double *host, int64_t n) {
+  return plane_copy(ctx, plane, (void *)host, n, true);
+}
+int chapsim_io_get_plane(chapsim_ctx *ctx, int plane, double *host, int64_t n) {
+  return plane_copy(ctx, plane, host, n, false);
+}
+
+int chapsim_io_bc_scalars(chapsim_ctx *ctx, double *out, int n) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(ctx->domain == CHAPSIM_IIO, CHAPSIM_ERR_STATE, "not an IO context");
+  REQUIRE(out && n >= 7, CHAPSIM_ERR_ARG, "need 7 values");
+  CKC(cudaSetDevice(ctx->device));
+  CKC(cudaMemcpyAsync(out, ctx->io.bcs, 7 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CKC(cudaStreamSynchronize(ctx->stream));
+  return CHAPSIM_OK;
 }
 
 static int io_substeps(chapsim_ctx *ctx) {

@@ -69,6 +69,10 @@ struct IODev {
   double *drhoi[3];
   double *stg[6];  // MU_STG 1-3, RHO_STG 1-3 of the current substep (energy equation on)
   double amvr1, apvrn;
+  // coupled inflow/outflow ghost planes CHAPSIM_P_* ((ny + 2) * nz each, plane
+  // q at bcp + q * bps) and their scalars (chapsim_io_bc_scalars)
+  double *bcp, *bcs;
+  int64_t bps;
 };
 
 // Per-substep scalars.
@@ -190,6 +194,9 @@ int launch_pois_io(chapsim_ctx *c, int ns, double *gx, double *gy, double *gz, c
                    bool store_rhs);
 // IO domain kernels (io_kernels.cu).
 int io_eng(chapsim_ctx *c, int ns);
+int io_bc_inlet(chapsim_ctx *c, const chapsim_ctx *tg);
+int io_bc_outlet_mom(chapsim_ctx *c, int ns);
+int io_bc_outlet_eng(chapsim_ctx *c, int ns);
 int io_thermal_bc(chapsim_ctx *c);
 int io_mom(chapsim_ctx *c, int ns, bool prep);
 // semi-implicit scheme: right-hand sides (*npart: the DPGRNS partial count),

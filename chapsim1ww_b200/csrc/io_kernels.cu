@@ -1149,4 +1149,269 @@ int io_reduce(chapsim_ctx *c, int what, double *host_out) {
   return CHAPSIM_OK;
 }
 
+
+// ---------------------------------------------------------------- coupled inflow/outflow planes
+// Ghost planes i = 0 and i = NCL1_io + 1 of the coupled IO section, each
+// (nz, ny + 2) at [k * (ny + 2) + j]; the last interior column i = NCL1_io is
+// the context's x index nx - 1.
+namespace {
+
+__device__ __forceinline__ double *bplane(const IODev &io, int q) { return io.bcp + (int64_t)q * io.bps; }
+
+// BC_TINLET_FLOW + BC_TINLET_THERML (src/BC_INLET.f90:2-76), j = 0 .. ny+1
+__global__ void k_bc_inlet(TGDev d, IODev io, const double *__restrict__ tu, const double *__restrict__ tv,
+                           const double *__restrict__ tw, const double *__restrict__ tp, int nxt, int64_t tsy,
+                           int64_t tsz, int cur) {
+  const int ny = d.ny;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (ny + 2) * d.nz) return;
+  const int k = t / (ny + 2), j = t - k * (ny + 2);
+  const int64_t tl = (nxt - 1) + tsy * j + tsz * k, tf = tsy * j + tsz * k;
+  const int64_t c0 = d.sy * j + d.sz * k;  // the first IO cell
+  const double rin = 1.0;                   // DENSITY(0, J, K), BC_TINLET_THERML
+  bplane(io, CHAPSIM_P_IN_RHO)[t] = rin;
+  const double ul = tu[tl], uf = tu[tf], vl = tv[tl], wl = tw[tl];
+  bplane(io, CHAPSIM_P_IN_U)[t] = ul;
+  d.u[c0] = uf;
+  bplane(io, CHAPSIM_P_IN_GX)[t] = ul * rin;
+  io.g[cur][0][c0] = uf * (rin + io.D[c0]) * 0.5;  // * XND2CL
+  bplane(io, CHAPSIM_P_IN_V)[t] = vl;
+  bplane(io, CHAPSIM_P_IN_GY)[t] = vl * rin;
+  bplane(io, CHAPSIM_P_IN_W)[t] = wl;
+  bplane(io, CHAPSIM_P_IN_GZ)[t] = wl * rin;
+  bplane(io, CHAPSIM_P_IN_P)[t] = tp[tl];
+}
+
+// CONVCTION_OUTLET_U (src/BC_COUTLET_MOM_RK3.f90:101-174): (max + min) / 2 of
+// the outlet-face mean 0.5 (u(NCL1) + u(NCL1 + 1)) over j = 1..ny; one block.
+__global__ void __launch_bounds__(1024) k_bc_umax(TGDev d, IODev io, int slot) {
+  __shared__ double smx[32], smn[32];
+  const int nx = d.nx, ny = d.ny;
+  const double *uo = bplane(io, CHAPSIM_P_OUT_U);
+  double mx = -1.0e20, mn = 1.0e20;
+  for (int t = threadIdx.x; t < ny * d.nz; t += blockDim.x) {
+    const int k = t / ny, j = t - k * ny + 1;
+    const double ucc = (d.u[(nx - 1) + d.sy * j + d.sz * k] + uo[j + (ny + 2) * k]) * 0.5;
+    mx = fmax(mx, ucc);
+    mn = fmin(mn, ucc);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    mn = fmin(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    smx[threadIdx.x >> 5] = mx;
+    smn[threadIdx.x >> 5] = mn;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q) {
+      mx = fmax(mx, smx[q]);
+      mn = fmin(mn, smn[q]);
+    }
+    io.bcs[slot] = 0.5 * (mx + mn);
+  }
+}
+
+// BC_COUTLET_MOM_RK3, the convective update (:22-44), j = 1..ny (2..ny for v)
+__global__ void k_bc_outlet_conv(TGDev d, IODev io, double gam, double roh, int cur) {
+  const int nx = d.nx, ny = d.ny;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ny * d.nz) return;
+  const int k = t / ny, j = t - k * ny + 1;
+  const int64_t pc = j + (int64_t)(ny + 2) * k, c = (nx - 1) + d.sy * j + d.sz * k;
+  const double coe1 = d.dxi * io.bcs[0];
+  const double rho = (io.D[c] + bplane(io, CHAPSIM_P_OUT_RHO)[pc]) * 0.5;  // * XND2CL
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    if (q == 1 && j == 1) continue;
+    double *go = bplane(io, CHAPSIM_P_OUT_GX + q), *c0 = bplane(io, CHAPSIM_P_CONV0_X + q);
+    const double conv = -(go[pc] - io.g[cur][q][c]) * coe1;
+    const double rhs = gam * conv + roh * c0[pc];
+    c0[pc] = conv;
+    const double gn = go[pc] + d.dt * rhs;
+    go[pc] = gn;
+    bplane(io, CHAPSIM_P_OUT_U + q)[pc] = gn / rho;
+  }
+}
+
+// CHK_MassConsv_io (src/processing/CHK_conservation.f90:2-71): inflow and
+// outflow from the planes (fixed-order block sums), the mass rate from the
+// grid reduction of DrhoDtP / DYFI in d.scal[1]; one block.
+__global__ void __launch_bounds__(1024) k_bc_mass(TGDev d, IODev io, int cur) {
+  __shared__ double sa[32], sb[32];
+  const int ny = d.ny;
+  const double *go = bplane(io, CHAPSIM_P_OUT_GX);
+  double fin = 0.0, fout = 0.0;
+  for (int t = threadIdx.x; t < ny * d.nz; t += blockDim.x) {
+    const int k = t / ny, j = t - k * ny + 1;
+    const double coe2 = 1.0 / d.dyfi[j];
+    fin += io.g[cur][0][d.sy * j + d.sz * k] * coe2;
+    fout += go[j + (int64_t)(ny + 2) * k] * coe2;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    fin += __shfl_xor_sync(0xffffffffu, fin, o);
+    fout += __shfl_xor_sync(0xffffffffu, fout, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sa[threadIdx.x >> 5] = fin;
+    sb[threadIdx.x >> 5] = fout;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q) {
+      fin += sa[q];
+      fout += sb[q];
+    }
+    fin /= d.dzi;
+    fout /= d.dzi;
+    const double mass = d.scal[1] / d.dzi / d.dxi;
+    io.bcs[1] = (fin - mass) / fout;
+    io.bcs[2] = fin - mass - fout;
+    io.bcs[3] = fin;
+    io.bcs[4] = fout;
+    io.bcs[5] = mass;
+  }
+}
+
+// BC_COUTLET_MOM_RK3 (:47-61): the outlet x-flux rescaled, then
+// BC_WALL_G_io / BC_WALL_Q_io on the plane (src/BC_WALL.f90:233-256, 412-460)
+__global__ void k_bc_outlet_scale(TGDev d, IODev io) {
+  const int nx = d.nx, ny = d.ny;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (ny + 2) * d.nz) return;
+  const int k = t / (ny + 2), j = t - k * (ny + 2);
+  double *gx = bplane(io, CHAPSIM_P_OUT_GX), *gy = bplane(io, CHAPSIM_P_OUT_GY), *gz = bplane(io, CHAPSIM_P_OUT_GZ);
+  double *u = bplane(io, CHAPSIM_P_OUT_U), *v = bplane(io, CHAPSIM_P_OUT_V), *w = bplane(io, CHAPSIM_P_OUT_W);
+  if (j >= 1 && j <= ny) {
+    const double s = io.bcs[1];
+    const int64_t c = (nx - 1) + d.sy * j + d.sz * k;
+    double g = gx[t];
+    g = g * (s - 1.0) + g;
+    gx[t] = g;
+    u[t] = g / ((io.D[c] + bplane(io, CHAPSIM_P_OUT_RHO)[t]) * 0.5);
+  }
+  if (j == 0 || j == ny + 1) {
+    gx[t] = 0.0; gy[t] = 0.0; gz[t] = 0.0;
+    u[t] = 0.0; v[t] = 0.0; w[t] = 0.0;
+  } else if (j == 1) {
+    gy[t] = 0.0;
+    v[t] = 0.0;
+  }
+}
+
+// BC_COUTLET_ENEG_RK3 (src/BC_COUTLET_ENEG_RK3.f90:2-41): the convective
+// update of rho h, then ENTHALPY_UPDATE, DENSITY_UPDATE, ENTHALPY_UPDATE and
+// THERM_PROP_UPDATE of the outlet plane (the steps of k_io_eng_props without
+// the old-value copies), j = 1..ny
+__global__ void k_bc_outlet_eng(TGDev d, IODev io, double gam, double roh) {
+  const int nx = d.nx, ny = d.ny;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ny * d.nz) return;
+  const int k = t / ny, j = t - k * ny + 1;
+  const int64_t pc = j + (int64_t)(ny + 2) * k, c = (nx - 1) + d.sy * j + d.sz * k;
+  double *rh = bplane(io, CHAPSIM_P_OUT_RHOH), *c0 = bplane(io, CHAPSIM_P_CONV0_ENG);
+  const double conv = -d.dxi * io.bcs[6] * (rh[pc] - io.rhoh[c]);
+  const double rhs = gam * conv + roh * c0[pc];
+  c0[pc] = conv;
+  const double r = rh[pc] + d.dt * rhs;
+  rh[pc] = r;
+  double *dd = bplane(io, CHAPSIM_P_OUT_RHO);
+  const double dold = dd[pc];
+  int bad = 0;
+  double h = r / dold, T, D = dold;
+  if (look_ht(io, h, T) && look_td(io, T, D)) {
+  } else {
+    D = dold;
+    ++bad;
+  }
+  h = r / D;
+  bplane(io, CHAPSIM_P_OUT_H)[pc] = h;
+  if (!(io.shortcuts && fabs(h) < 1.0e-10)) {
+    double M, K, D2;
+    if (look_ht(io, h, T) && look_tprops(io, T, D2, M, K)) {
+      bplane(io, CHAPSIM_P_OUT_T)[pc] = T;
+      bplane(io, CHAPSIM_P_OUT_MU)[pc] = M;
+      bplane(io, CHAPSIM_P_OUT_K)[pc] = K;
+      D = D2;
+    } else {
+      ++bad;
+    }
+  }
+  dd[pc] = D;
+  if (bad) atomicAdd(io.bad, (unsigned long long)bad);
+}
+
+// BC_WALL_ISOFLUX (src/BC_WALL.f90:522-627) on the outlet plane's ghost rows;
+// blockIdx.y: 0 bottom, 1 top
+__global__ void k_bc_outlet_eng_ghost(TGDev d, IODev io) {
+  const int ny = d.ny;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.nz) return;
+  const bool top = blockIdx.y == 1;
+  const int64_t row = (int64_t)(ny + 2) * k;
+  double *hh = bplane(io, CHAPSIM_P_OUT_H);
+  double h;
+  if (!top)
+    h = 2.0 * hh[row + 1] - d.wff[2] * hh[row + 2] - d.wfb[2] * hh[row + 1];
+  else
+    h = 2.0 * hh[row + ny] - d.wff[ny] * hh[row + ny] - d.wfb[ny] * hh[row + ny - 1];
+  const int64_t pc = row + (top ? ny + 1 : 0);
+  hh[pc] = h;
+  double T, D, M, K;
+  if (!look_ht(io, h, T) || !look_tprops(io, T, D, M, K)) {
+    atomicAdd(io.bad, 1ull);
+    return;
+  }
+  bplane(io, CHAPSIM_P_OUT_RHO)[pc] = D;
+  bplane(io, CHAPSIM_P_OUT_T)[pc] = T;
+  bplane(io, CHAPSIM_P_OUT_MU)[pc] = M;
+  bplane(io, CHAPSIM_P_OUT_K)[pc] = K;
+  bplane(io, CHAPSIM_P_OUT_RHOH)[pc] = h * D;
+}
+
+}  // namespace
+
+int io_bc_inlet(chapsim_ctx *c, const chapsim_ctx *tg) {
+  const TGDev &d = c->d, &t = tg->d;
+  const int n = (d.ny + 2) * d.nz;
+  k_bc_inlet<<<(n + 255) / 256, 256, 0, c->stream>>>(d, c->io, t.u, t.v, t.w, t.p, t.nx, t.sy, t.sz, c->io_cur);
+  LAUNCHED();
+  return CHAPSIM_OK;
+}
+
+int io_bc_outlet_mom(chapsim_ctx *c, int ns) {
+  TGDev &d = c->d;
+  const SubParams &sp = c->sp[ns];
+  const int np = d.ny * d.nz, nall = (d.ny + 2) * d.nz;
+  k_bc_umax<<<1, 1024, 0, c->stream>>>(d, c->io, 0);
+  LAUNCHED();
+  k_bc_outlet_conv<<<(np + 255) / 256, 256, 0, c->stream>>>(d, c->io, sp.gam, sp.roh, c->io_cur);
+  LAUNCHED();
+  // sum of DrhoDtP / DYFI over the interior into d.scal[1]
+  const dim3 grid = cell_grid(d), blk(IO_BX, IO_BY);
+  k_io_red_part<<<grid, blk, 0, c->stream>>>(d, c->io, 1, c->io_cur, c->io.drho);
+  LAUNCHED();
+  k_io_red_final<<<1, 1024, 0, c->stream>>>(d, 1, (int)(grid.x * grid.y * grid.z));
+  LAUNCHED();
+  k_bc_mass<<<1, 1024, 0, c->stream>>>(d, c->io, c->io_cur);
+  LAUNCHED();
+  k_bc_outlet_scale<<<(nall + 255) / 256, 256, 0, c->stream>>>(d, c->io);
+  LAUNCHED();
+  return CHAPSIM_OK;
+}
+
+int io_bc_outlet_eng(chapsim_ctx *c, int ns) {
+  TGDev &d = c->d;
+  const SubParams &sp = c->sp[ns];
+  const int np = d.ny * d.nz;
+  k_bc_umax<<<1, 1024, 0, c->stream>>>(d, c->io, 6);
+  LAUNCHED();
+  k_bc_outlet_eng<<<(np + 255) / 256, 256, 0, c->stream>>>(d, c->io, sp.gam, sp.roh);
+  LAUNCHED();
+  k_bc_outlet_eng_ghost<<<dim3((d.nz + 127) / 128, 2), 128, 0, c->stream>>>(d, c->io);
+  LAUNCHED();
+  return CHAPSIM_OK;
+}
+
 }  // namespace chapsim

@@ -125,6 +125,39 @@ class IOChannel(TGChannel):
     def bad_cells(self):
         return int(self._reduce(_lib.R_BADCELLS))
 
+    # ---- coupled inflow/outflow boundary planes (ghost columns i = 0 and NCL1_io + 1)
+    def get_plane(self, name):
+        """A ghost plane of the coupled inflow/outflow conditions, (nz, ny+2)."""
+        a = np.empty((self.nz, self.ny + 2))
+        self._chk(self.lib.chapsim_io_get_plane(self.h, _lib.IO_PLANES[name], a.ctypes.data, a.size))
+        return a
+
+    def set_plane(self, name, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if a.size != self.nz * (self.ny + 2):
+            raise ValueError(f"plane {name}: expected {self.nz * (self.ny + 2)} values, got {a.size}")
+        self._chk(self.lib.chapsim_io_set_plane(self.h, _lib.IO_PLANES[name], a.ctypes.data, a.size))
+
+    def bc_tinlet_flow(self, tg):
+        """BC_TINLET_FLOW + BC_TINLET_THERML (src/BC_INLET.f90:2-76) from a TG
+        context of the same ny, nz on the same device."""
+        self._chk(self.lib.chapsim_io_bc_inlet(self.h, tg.h))
+
+    def bc_coutlet_mom_rk3(self, ns):
+        """BC_COUTLET_MOM_RK3(NS) with CHK_MassConsv_io (src/BC_COUTLET_MOM_RK3.f90:2-174)."""
+        self._chk(self.lib.chapsim_io_bc_outlet_mom(self.h, ns))
+
+    def bc_coutlet_eneg_rk3(self, ns):
+        """BC_COUTLET_ENEG_RK3(NS) (src/BC_COUTLET_ENEG_RK3.f90:2-41)."""
+        self._chk(self.lib.chapsim_io_bc_outlet_eng(self.h, ns))
+
+    def bc_scalars(self):
+        """U_OUTLET (momentum and energy calls), CHK_Mass_CONSV0_SCALING, the
+        balance inflow - mass rate - outflow and its three terms."""
+        a = np.empty(7)
+        self._chk(self.lib.chapsim_io_bc_scalars(self.h, a.ctypes.data, 7))
+        return dict(zip(_lib.IO_BC_SCALARS, a.tolist()))
+
     # TG-only entries do not apply
     def solverrk3_mom_tg(self, ns):
         raise ChapsimError(4, "not a TG context")

@@ -279,6 +279,67 @@ int chapsim_launch_count_reset(chapsim_ctx *ctx);
 #define CHAPSIM_F_DRHO 24   /* DrhoDtP     */
 #define CHAPSIM_F_RHSE0 25  /* RHS_ENERGY0 */
 
+/* Coupled inflow/outflow boundary planes of the IO section.  The reference
+ * couples the TG section to the IO section's inlet and gives the IO outlet a
+ * convective condition (TGFLOWFLG): the IO arrays carry ghost columns i = 0
+ * and i = NCL1_io + 1.  An IO context holds those ghost planes, each
+ * (nz, ny + 2) doubles at [k * (ny + 2) + j], plus the outlet's RK3 memory
+ * terms; the operators below fill and advance them from the context's own
+ * fields (its last column i = NCL1_io is the interior next to the outlet).
+ * The inlet ghost properties are the reference state (BC_TINLET_THERML:
+ * rho = T = mu = k = 1, rho h = h = 0); only rho is stored. */
+#define CHAPSIM_P_IN_U 0
+#define CHAPSIM_P_IN_V 1
+#define CHAPSIM_P_IN_W 2
+#define CHAPSIM_P_IN_GX 3
+#define CHAPSIM_P_IN_GY 4
+#define CHAPSIM_P_IN_GZ 5
+#define CHAPSIM_P_IN_P 6
+#define CHAPSIM_P_IN_RHO 7
+#define CHAPSIM_P_OUT_U 8
+#define CHAPSIM_P_OUT_V 9
+#define CHAPSIM_P_OUT_W 10
+#define CHAPSIM_P_OUT_GX 11
+#define CHAPSIM_P_OUT_GY 12
+#define CHAPSIM_P_OUT_GZ 13
+#define CHAPSIM_P_OUT_RHO 14
+#define CHAPSIM_P_OUT_RHOH 15
+#define CHAPSIM_P_OUT_H 16
+#define CHAPSIM_P_OUT_T 17
+#define CHAPSIM_P_OUT_MU 18
+#define CHAPSIM_P_OUT_K 19
+#define CHAPSIM_P_CONV0_X 20   /* BC_CONV0(:, :, 1..3) */
+#define CHAPSIM_P_CONV0_Y 21
+#define CHAPSIM_P_CONV0_Z 22
+#define CHAPSIM_P_CONV0_ENG 23 /* BC_CONV0_ENG */
+#define CHAPSIM_P_COUNT 24
+
+/* BC_TINLET_FLOW + BC_TINLET_THERML (src/BC_INLET.f90:2-76): the TG context's
+ * last plane (u, v, w, p at i = NCL1_tg) becomes the inlet ghost plane, the
+ * TG first-face u becomes the IO first-face u, and G follows with the inlet
+ * density.  Writes the IO context's u and G_io at i = 1 (first face).  Both
+ * contexts on one device with equal ny, nz; waits for the TG context's queued
+ * work and returns when the planes are written. */
+int chapsim_io_bc_inlet(chapsim_ctx *io, chapsim_ctx *tg);
+/* BC_COUTLET_MOM_RK3(NS) (src/BC_COUTLET_MOM_RK3.f90:2-97) with
+ * CONVCTION_OUTLET_U (:101-174) and CHK_MassConsv_io
+ * (src/processing/CHK_conservation.f90:2-71): dG/dt + U_OUTLET dG/dx = 0 on
+ * the outlet plane with the RK3 weights of NS, the outlet x-flux rescaled so
+ * that inflow - d(rho)/dt = outflow, wall conditions on the plane. */
+int chapsim_io_bc_outlet_mom(chapsim_ctx *io, int ns);
+/* BC_COUTLET_ENEG_RK3(NS) (src/BC_COUTLET_ENEG_RK3.f90:2-41): the same
+ * convective condition for rho h, then the property update of the outlet
+ * plane (ENTHALPY_UPDATE, DENSITY_UPDATE, THERM_PROP_UPDATE, region IOULET)
+ * and its iso-flux ghost rows.  Needs the energy equation and a table. */
+int chapsim_io_bc_outlet_eng(chapsim_ctx *io, int ns);
+/* Copy one ghost plane (id CHAPSIM_P_*, n = (ny + 2) * nz) in or out. */
+int chapsim_io_set_plane(chapsim_ctx *io, int plane, const double *host, int64_t n);
+int chapsim_io_get_plane(chapsim_ctx *io, int plane, double *host, int64_t n);
+/* out[0..6]: U_OUTLET of the last momentum call, CHK_Mass_CONSV0_SCALING,
+ * CHK_MASS_CONSV0 (inflow - mass rate - outflow before the rescaling),
+ * inflow, outflow, mass rate, U_OUTLET of the last energy call; n >= 7. */
+int chapsim_io_bc_scalars(chapsim_ctx *io, double *out, int n);
+
 /* IO reductions (chapsim_reduce with domain CHAPSIM_IIO): CHAPSIM_R_DIVMAX is
  * DIVGCK_io's max|div G + DrhoDtP| (src/DIVGCK.f90:60-190), CHAPSIM_R_BULK is
  * BULK_VELOCITY_IO (src/INITIAL_FL_THEML_FLD_io.f90:385-413), and: */
