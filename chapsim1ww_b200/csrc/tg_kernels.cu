@@ -741,47 +741,78 @@ static bool launch_adixz_rows(cudaStream_t st, const TGDev &d, const SubParams &
 // the Thomas sweeps and truncated where the dropped entries of every row sum
 // to < 2^-60 of its largest entry.  Then q += dq and BC_WALL_Q_tg.  A block
 // owns 32 x-columns, AY_JT rows and one z plane; rows outside [1, ny] carry
-// zero weight.  The v line's row-1 right-hand side is the final u increment
-// at j = 1 (the reference quirk described at k_adiy_smem), computed here from
-// the u data.
-constexpr int AY_JT = 32, AY_TX = 32, AY_TY = 8, AYB_WMAX = 16;
-template <typename T>
+// zero weight.  Per component the block stages its tile of dq (with the y
+// halo) and its AY_JT band rows of G (zero past WY, one zero pad) in shared
+// memory; each thread then computes AY_R consecutive rows of its column,
+// reading each tile value once and the band coefficients as 16-byte
+// broadcast pairs.  W is a compile-time width at least WY.  The v line's
+// row-1 right-hand side is the final u increment at j = 1 (the reference
+// quirk described at k_adiy_smem), computed here from the u data.
+constexpr int AY_JT = 32, AY_TX = 32, AY_TY = 8, AYB_WMAX = 16, AY_R = AY_JT / AY_TY;
+constexpr int AY_TW[6] = {2, 4, 6, 8, 12, 16};  // compiled widths
+static_assert(AY_TW[5] == AYB_WMAX, "the widest compiled band is the host's limit");
+template <typename T, int W>
 __global__ void __launch_bounds__(AY_TX *AY_TY) k_adiy_band(TGDev d, SubParams sp) {
-  __shared__ double tile[(AY_JT + 2 * AYB_WMAX) * AY_TX];
+  constexpr int NT = AY_R + 2 * W + 1;  // tile values per thread; the last one meets a zero weight
+  constexpr int GS = 2 * W + 2;         // band row stride in shared memory (even: pairs stay 16-byte aligned)
+  __shared__ double tile[(AY_JT + 2 * W + 1) * AY_TX];
+  __shared__ __align__(16) double gsh[AY_JT * GS];
   __shared__ double du1[AY_TX];
   const int nx = d.nx, ny = d.ny;
-  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + AY_TX * ty;
   const int x0 = blockIdx.x * AY_TX, j0 = 1 + blockIdx.y * AY_JT, k = blockIdx.z;
   const int i = x0 + tx;
   const bool col_ok = i < nx;
   const int64_t base = (int64_t)i + d.sz * k;
-  const int W = sp.wy;
-  const int nrow = AY_JT + 2 * W;  // tile rows j0-W .. j0+AY_JT-1+W
+  const int nrow = AY_JT + 2 * W;  // tile rows j0-W .. j0+AY_JT-1+W, then one zero row
+  const int jr0 = ty * AY_R;
   for (int comp = 0; comp < 3; ++comp) {
     const T *src = reinterpret_cast<const T *>(d.dq[comp]);
-    for (int r = ty; r < nrow; r += AY_TY) {
+    for (int r = ty; r <= nrow; r += AY_TY) {
       const int j = j0 - W + r;
       double v = 0.0;
-      if (col_ok && j >= 1 && j <= ny) v = (double)src[base + d.sy * j];
+      if (col_ok && r < nrow && j >= 1 && j <= ny) v = (double)src[base + d.sy * j];
       tile[r * AY_TX + tx] = v;
+    }
+    // the block's band rows G[j][m], m = -W .. W + 1 (the last zero); rows
+    // past ny repeat row ny and are discarded
+    const double *G = sp.yg[comp];
+    for (int t = tid; t < AY_JT * GS; t += AY_TX * AY_TY) {
+      const int r = t / GS, m = t - r * GS - W, j = min(j0 + r, ny);
+      gsh[t] = m <= W ? G[(size_t)j * (2 * AYB_WMAX + 1) + AYB_WMAX + m] : 0.0;
     }
     if (comp == 1 && j0 == 1) {
       __syncthreads();
       if (ty == 0) tile[(1 - j0 + W) * AY_TX + tx] = du1[tx];  // row j = 1 of v <- u increment
     }
     __syncthreads();
-    const double *G = sp.yg[comp];
     double *q = comp == 0 ? d.u : (comp == 1 ? d.v : d.w);
     const int jlo = comp == 1 ? 2 : 1;
-    for (int jr = ty; jr < AY_JT; jr += AY_TY) {
-      const int j = j0 + jr;
-      if (j > ny) break;
-      const double *g = G + (size_t)j * (2 * AYB_WMAX + 1) + AYB_WMAX;  // g[m], m in [-W, W]
-      const double *t = tile + (jr + W) * AY_TX + tx;
-      double acc = g[0] * t[0];
-      for (int m = 1; m <= W; ++m) acc += g[-m] * t[-m * AY_TX] + g[m] * t[m * AY_TX];
-      if (comp == 0 && j == 1) du1[tx] = acc;
-      if (col_ok && j >= jlo) q[base + d.sy * j] += acc;
+    double acc[AY_R];
+    double2 cp[AY_R];
+#pragma unroll
+    for (int r = 0; r < AY_R; ++r) {
+      acc[r] = 0.0;
+      cp[r] = make_double2(0.0, 0.0);
+    }
+    // tile row jr0 + qq feeds row r with the weight G[j0 + jr0 + r][qq - r - W]
+#pragma unroll
+    for (int qq = 0; qq < NT; ++qq) {
+      const double v = tile[(jr0 + qq) * AY_TX + tx];
+#pragma unroll
+      for (int r = 0; r < AY_R; ++r) {
+        const int m2 = qq - r;  // m + W
+        if (m2 < 0 || m2 > 2 * W + 1) continue;
+        if ((m2 & 1) == 0) cp[r] = *reinterpret_cast<const double2 *>(gsh + (jr0 + r) * GS + m2);
+        acc[r] += ((m2 & 1) ? cp[r].y : cp[r].x) * v;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < AY_R; ++r) {
+      const int j = j0 + jr0 + r;
+      if (j > ny) break;  // uniform over the warp (one warp per ty)
+      if (comp == 0 && j == 1) du1[tx] = acc[r];
+      if (col_ok && j >= jlo) q[base + d.sy * j] += acc[r];
     }
     if (col_ok && ty == 0) {
       if (j0 == 1) {
@@ -792,6 +823,20 @@ __global__ void __launch_bounds__(AY_TX *AY_TY) k_adiy_band(TGDev d, SubParams s
     }
     __syncthreads();
   }
+}
+template <typename T, int W>
+static void launch_adiy_w(dim3 grid, cudaStream_t st, const TGDev &d, const SubParams &sp) {
+  k_adiy_band<T, W><<<grid, dim3(AY_TX, AY_TY), 0, st>>>(d, sp);
+}
+// the band form of the y factors (the host keeps 0 <= wy <= AYB_WMAX when it is on)
+template <typename T>
+static void launch_adiy(dim3 grid, cudaStream_t st, const TGDev &d, const SubParams &sp) {
+  typedef void (*Fn)(dim3, cudaStream_t, const TGDev &, const SubParams &);
+  static const Fn fns[6] = {launch_adiy_w<T, 2>, launch_adiy_w<T, 4>, launch_adiy_w<T, 6>,
+                            launch_adiy_w<T, 8>, launch_adiy_w<T, 12>, launch_adiy_w<T, 16>};
+  int q = 0;
+  while (q < 5 && sp.wy > AY_TW[q]) ++q;
+  fns[q](grid, st, d, sp);
 }
 
 // ============================================================ y lines
@@ -1517,7 +1562,7 @@ template <typename T> struct Prec {
     phase_mark(c, CHAPSIM_PH_ADIY);
     if (sp.band && sp.wy >= 0) {
       dim3 grid((d.nx + AY_TX - 1) / AY_TX, (d.ny + AY_JT - 1) / AY_JT, d.nz);
-      k_adiy_band<T><<<grid, dim3(AY_TX, AY_TY), 0, c->stream>>>(d, sp);
+      launch_adiy<T>(grid, c->stream, d, sp);
       LAUNCHED();
     } else {
       dim3 grid((d.nx + AY_TL - 1) / AY_TL, d.nz);
