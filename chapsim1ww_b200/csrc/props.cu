@@ -417,6 +417,12 @@ static int upload_spline(chapsim_props *pe, const std::vector<double> &x, const 
   if ((rc = palloc(pe, &p, (nb + 1) * sizeof(int)))) return rc;
   PCK(cudaMemcpy(p, blo.data(), (nb + 1) * sizeof(int), cudaMemcpyHostToDevice));
   s.blo = (const int *)p;
+  const std::vector<int2> rng = bucket_ranges(blo, n, nb);
+  if ((rc = palloc(pe, &p, nb * sizeof(int2)))) return rc;
+  PCK(cudaMemcpy(p, rng.data(), nb * sizeof(int2), cudaMemcpyHostToDevice));
+  s.brng = (const int2 *)p;
+  s.xlo = x[0];
+  s.xhi = x[n - 1];
   std::vector<double> rec((size_t)4 * n);
   for (int i = 0; i < n; ++i) { rec[4 * i] = y[i]; rec[4 * i + 1] = b[i]; rec[4 * i + 2] = c[i]; rec[4 * i + 3] = d[i]; }
   if ((rc = palloc(pe, &p, rec.size() * sizeof(double)))) return rc;

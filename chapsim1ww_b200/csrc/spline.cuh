@@ -15,8 +15,10 @@ namespace chapsim_spl {
 struct Spline {
   const double *x, *y, *b, *c, *d;
   const double4 *ybcd;
-  const int *blo;  // bucket -> first candidate interval
+  const int *blo;    // bucket -> first candidate interval
+  const int2 *brng;  // bucket -> search range {blo[b], min(n - 1, blo[b + 1] + 3)}
   double x0, binv;
+  double xlo, xhi;   // x[0] and x[n - 1], held by value for the range test
   int n, nb;
 };
 
@@ -25,7 +27,8 @@ struct Spline {
 __device__ __forceinline__ int spline_find(const Spline &s, double u) {
   int b = (int)((u - s.x0) * s.binv);
   b = b < 0 ? 0 : (b >= s.nb ? s.nb - 1 : b);
-  int i = __ldg(s.blo + b), j = min(s.n - 1, __ldg(s.blo + b + 1) + 3);
+  const int2 rg = __ldg(s.brng + b);
+  int i = rg.x, j = rg.y;
   while (j > i + 1) {
     const int k = (i + j) >> 1;
     if (u < __ldg(s.x + k)) j = k; else i = k;
@@ -41,7 +44,7 @@ __device__ __forceinline__ double spline_at(const Spline &s, int i, double u) {
 }
 __device__ __forceinline__ double spline_eval(const Spline &s, double u) { return spline_at(s, spline_find(s, u), u); }
 
-__device__ __forceinline__ bool inside(const Spline &s, double u) { return u > s.x[0] && u < s.x[s.n - 1]; }
+__device__ __forceinline__ bool inside(const Spline &s, double u) { return u > s.xlo && u < s.xhi; }
 
 
 // Host restatement of CUBIC_SPLINE (Forsythe-Malcolm-Moler, 1977).
@@ -104,6 +107,13 @@ inline void bucket_table(int n, const double *x, int nb, double &x0, double &bin
 }
 
 
+// Search range of each bucket for spline_find: {blo[b], min(n - 1, blo[b + 1] + 3)}.
+inline std::vector<int2> bucket_ranges(const std::vector<int> &blo, int n, int nb) {
+  std::vector<int2> rng(nb);
+  for (int q = 0; q < nb; ++q) rng[q] = make_int2(blo[q], blo[q + 1] + 3 < n - 1 ? blo[q + 1] + 3 : n - 1);
+  return rng;
+}
+
 // Build the spline of y over x on the host and upload x, y, b, c, d, the
 // packed records and the bucket table; every allocation is appended to
 // allocs (freed by the owner).
@@ -129,6 +139,13 @@ inline cudaError_t upload_spline(std::vector<void *> &allocs, const std::vector<
   allocs.push_back(p);
   if ((e = cudaMemcpy(p, blo.data(), (nb + 1) * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess) return e;
   s.blo = (const int *)p;
+  const std::vector<int2> rng = bucket_ranges(blo, n, nb);
+  if ((e = cudaMalloc(&p, nb * sizeof(int2))) != cudaSuccess) return e;
+  allocs.push_back(p);
+  if ((e = cudaMemcpy(p, rng.data(), nb * sizeof(int2), cudaMemcpyHostToDevice)) != cudaSuccess) return e;
+  s.brng = (const int2 *)p;
+  s.xlo = x[0];
+  s.xhi = x[n - 1];
   std::vector<double> rec((size_t)4 * n);
   for (int i = 0; i < n; ++i) { rec[4 * i] = y[i]; rec[4 * i + 1] = b[i]; rec[4 * i + 2] = c[i]; rec[4 * i + 3] = d[i]; }
   if ((e = cudaMalloc(&p, rec.size() * sizeof(double))) != cudaSuccess) return e;
