@@ -104,8 +104,10 @@ __device__ __forceinline__ bool look_tprops(const IODev &io, double T, double &D
 
 // ---------------------------------------------------------------- energy
 // RHS_ENERGY_EXPLICIT and the RHOH update of SOLVERRK3_ENG_IO (:22-35):
-// rhoh += gam dt R + zeta dt R_old, limited to RHOHmax + REALMIN.
-__global__ void __launch_bounds__(IO_BX *IO_BY) k_io_eng_rhs(TGDev d, IODev io, double cdt1, double cdt0, int cur) {
+// rhoh += gam dt R + zeta dt R_old, limited to RHOHmax + REALMIN.  Six blocks
+// per SM (40 registers): latency-bound on its neighbour loads, it gains from
+// the extra resident warps (measured 0.536 -> 0.510 ms at 512x192x256).
+__global__ void __launch_bounds__(IO_BX *IO_BY, 6) k_io_eng_rhs(TGDev d, IODev io, double cdt1, double cdt0, int cur) {
   const int nx = d.nx, ny = d.ny;
   const int i = blockIdx.x * IO_BX + threadIdx.x;
   const int j = blockIdx.y * IO_BY + threadIdx.y + 1;
@@ -276,8 +278,11 @@ __global__ void k_io_msum(IODev io, size_t n) {
 // ---------------------------------------------------------------- momentum
 // DENSITY_TIME_DERIVATION (gamma - 2 divisor as written) and VELOCITY_CALC_io
 // with its wall BC.  RHO_STG is formed from rho, rho0 (DENSITY_Staggered).
+// Eight blocks per SM for the explicit scheme (32 registers, measured 0.459
+// -> 0.410 ms at 512x192x256): latency-bound, it gains from the extra
+// resident warps.  The DRHOI variant keeps its register count (a cap spills).
 template <bool VISC>
-__global__ void __launch_bounds__(IO_BX *IO_BY) k_io_prep(TGDev d, IODev io, double gp, double zr, double den,
+__global__ void __launch_bounds__(IO_BX *IO_BY, VISC ? 1 : 8) k_io_prep(TGDev d, IODev io, double gp, double zr, double den,
                                                         int cur, int do_drho) {
   const int nx = d.nx, ny = d.ny;
   const int i = blockIdx.x * IO_BX + threadIdx.x;
