@@ -104,6 +104,35 @@ __device__ __forceinline__ void dft_small(C *v, const C *tw, int n, int sign) {
   }
 }
 
+// v_r *= w^{r m} for r = 1 .. R-1 (r m < n).  Radix 8 and 4 load w^m, w^2m
+// (and w^4m) from the table and form the other powers as products of two
+// table entries, each within a few ulps of the table value: 3 table loads
+// instead of 7.  In the last stage of a line-major transform the lanes of a
+// warp take consecutive m, so the load of w^{rm} touches r times as many
+// cache lines as that of w^m; the products replace the widest of them.
+template <typename C, int R>
+__device__ __forceinline__ void twiddle_inputs(C *v, const C *__restrict__ tw, int m, int sign) {
+  if (R == 8) {
+    const C w1 = twiddle(tw, m, sign), w2 = twiddle(tw, 2 * m, sign), w4 = twiddle(tw, 4 * m, sign);
+    const C w3 = cmul(w1, w2);
+    v[1] = cmul(v[1], w1);
+    v[2] = cmul(v[2], w2);
+    v[3] = cmul(v[3], w3);
+    v[4] = cmul(v[4], w4);
+    v[5] = cmul(v[5], cmul(w1, w4));
+    v[6] = cmul(v[6], cmul(w2, w4));
+    v[7] = cmul(v[7], cmul(w3, w4));
+  } else if (R == 4) {
+    const C w1 = twiddle(tw, m, sign), w2 = twiddle(tw, 2 * m, sign);
+    v[1] = cmul(v[1], w1);
+    v[2] = cmul(v[2], w2);
+    v[3] = cmul(v[3], cmul(w1, w2));
+  } else {
+#pragma unroll
+    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twiddle(tw, r * m, sign));
+  }
+}
+
 // Shared-memory position of element p of a line-major buffer: the low three
 // bits are XORed with bits 3..5, a permutation inside every aligned group of
 // eight elements.  The Stockham stages write at stride R (radix 8: eight
@@ -131,10 +160,7 @@ __device__ __forceinline__ void stockham_stage(const C *__restrict__ in, C *__re
     C v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = in[swz(l0 + j + r * nb)];
-    if (k != 0) {
-#pragma unroll
-      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], twiddle(tw, r * k * tstep, sign));  // r k tstep < n
-    }
+    if (k != 0) twiddle_inputs<C, R>(v, tw, k * tstep, sign);
     dft_small<C, R>(v, tw, n, sign);
     const int base = l0 + jq * Ns * R + k;
 #pragma unroll
@@ -175,7 +201,8 @@ __device__ C *fft_lines(C *a, C *b, int nlines, int n, int lstride, const int *r
 // buf[e * nl + l] (consecutive lines adjacent; nl a power of two).
 // Consecutive threads take consecutive lines, so each stage's reads and
 // writes are contiguous rows.  Per element the arithmetic is that of
-// stockham_stage.
+// stockham_stage, except that every twiddle comes from the table: the lanes
+// of a warp share the twiddle index, so each table load is one broadcast.
 template <typename C, int R>
 __device__ __forceinline__ void stockham_stage_il(const C *__restrict__ in, C *__restrict__ out, int nl, int n,
                                                   int Ns, const C *__restrict__ tw, int sign) {

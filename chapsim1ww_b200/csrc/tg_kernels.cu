@@ -1180,9 +1180,11 @@ __global__ void __launch_bounds__(128) k_ysolve_line(TGDev d) {
 // block's lb spectral rows (contiguous, pitch lp) arrive by one bulk copy;
 // pairs of rows are rebuilt as one complex Hermitian-extended line and
 // transformed; phi ghosts copied (BC_WALL_DPH, src/BC_WALL.f90:342-364).
-// accumulate != 0 adds the result to phi (refinement sweep).
+// accumulate != 0 adds the result to phi (refinement sweep).  The FFT
+// scratch reuses the staging area of the spectral rows once the lines are
+// packed (lb * lp >= lb / 2 * nx, since lp > nx / 2).
 template <typename C> __host__ __device__ constexpr size_t ifftx_smem_bytes(int nx, int lp, int lb) {
-  return align128((size_t)lb * lp * sizeof(C)) + 2 * align128((size_t)(lb / 2) * nx * sizeof(C));
+  return align128((size_t)lb * lp * sizeof(C)) + align128((size_t)(lb / 2) * nx * sizeof(C));
 }
 
 template <typename T, bool BIG>
@@ -1199,7 +1201,7 @@ __global__ void __launch_bounds__(256, BIG ? 2 : 3) k_ifftx(TGDev d, FFTPlan pl,
   const int tid = threadIdx.x;
   C *SP = reinterpret_cast<C *>(smem_raw);
   C *A = reinterpret_cast<C *>(smem_raw + align128((size_t)lb * lp * sizeof(C)));
-  C *B = reinterpret_cast<C *>(reinterpret_cast<unsigned char *>(A) + align128((size_t)nl * nx * sizeof(C)));
+  C *B = SP;  // FFT scratch: the spectral rows are dead once packed into A
   if (tid == 0) {
     mbar_init(&bar, 1);
     fence_mbar_init();
@@ -1394,10 +1396,12 @@ template <typename T> struct Prec {
     return lb >= 4 ? lb : max_fftx_lb(c->d.nx, dr);
   }
   // rows per block of the inverse x transform: the most rows whose buffers
-  // fit in 74 KB, so that three blocks share an SM
+  // fit in 74 KB, so that three blocks share an SM, as a power of two (at
+  // power-of-two nx the lines' butterflies then fill whole passes of the
+  // block's 256 threads)
   static int ifftx_lb(const chapsim_ctx *c) {
     int lb = 2;
-    while (lb < 32 && ifftx_smem_bytes<C>(c->d.nx, c->d.lp, lb + 2) <= 74 * 1024) lb += 2;
+    while (lb < 32 && ifftx_smem_bytes<C>(c->d.nx, c->d.lp, 2 * lb) <= 74 * 1024) lb *= 2;
     return lb;
   }
   static size_t fftx_smem(const chapsim_ctx *c, int lb) { return fftx_smem_bytes<C>(c->d.nx, lb, dr_rows(c)); }
