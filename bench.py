@@ -96,7 +96,7 @@ IO_KERNEL = {"eng_rhs": "k_io_eng_rhs", "eng_props": "k_io_eng_props", "prep": "
 # and out plus the four property fields of the coefficients; the y solves
 # also read G and write G*): 78 values per cell with the energy equation on.
 IO_SI_MOM_VALUES = {1: 78, 0: 37}
-IO_SI_KERNEL = "k_io_rhs_si + MOMFA solves (k_io_cyc, k_io_ysi)"
+IO_SI_KERNEL = "k_si_stg + k_io_rhs_si + MOMFA solves (k_si_x, k_si_zy)"
 
 
 # End-to-end transfers of an IO step.  Its inputs are the mass flux G, the

@@ -157,8 +157,8 @@ __device__ __forceinline__ Prop make_prop(const TGDev &d, const IODev &io) {
 // (one launch per component): RHS_io -> d.rhs[C], EXPLT0_io updated.  Per-block sums of RHS_x / DYFI
 // feed DPGRNS.  Row 1 of the v right-hand side is zero (VISCOUS_PAR_EXPLT_Y_io
 // clears RHS_io and nothing writes that row before MOMFA3_Y_io).
-template <int C>
-__global__ void __launch_bounds__(SI_BX *SI_BY) k_io_rhs_si(TGDev d, IODev io, double gam, double roh, double alp,
+template <int C, bool TH>
+__global__ void __launch_bounds__(SI_BX *SI_BY, 4) k_io_rhs_si(TGDev d, IODev io, double gam, double roh, double alp,
                                                           int cur) {
   __shared__ double red[SI_BX * SI_BY / 32];
   const int nx = d.nx, ny = d.ny, nz = d.nz;
@@ -169,8 +169,9 @@ __global__ void __launch_bounds__(SI_BX *SI_BY) k_io_rhs_si(TGDev d, IODev io, d
   if (i < nx && j <= ny) {
     const int64_t sy = d.sy, sz = d.sz;
     const int ip = wp(i, nx), im = wm(i, nx), kp = wp(k, nz), km = wm(k, nz);
-    const Prop P = make_prop(d, io);
-    const bool th = io.thermal != 0;
+    Prop P = make_prop(d, io);
+    P.th = TH;  // compile-time: the property loads and density parts fold away without the energy equation
+    constexpr bool th = TH;
     const double *__restrict__ u = d.u, *__restrict__ v = d.v, *__restrict__ w = d.w, *__restrict__ p = d.p;
     const double *__restrict__ gx = io.g[cur][0], *__restrict__ gy = io.g[cur][1], *__restrict__ gz = io.g[cur][2];
     const double *__restrict__ r0 = io.drhoi[0], *__restrict__ r1 = io.drhoi[1], *__restrict__ r2 = io.drhoi[2];
@@ -633,12 +634,21 @@ int io_mom_si(chapsim_ctx *c, int ns, int *npart) {
     LAUNCHED();
   }
   // one kernel per component: a third of the live values each
-  k_io_rhs_si<0><<<grid, dim3(SI_BX, SI_BY), 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, c->io_cur);
-  LAUNCHED();
-  k_io_rhs_si<1><<<grid, dim3(SI_BX, SI_BY), 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, c->io_cur);
-  LAUNCHED();
-  k_io_rhs_si<2><<<grid, dim3(SI_BX, SI_BY), 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, c->io_cur);
-  LAUNCHED();
+  if (io.thermal) {
+    k_io_rhs_si<0, true><<<grid, dim3(SI_BX, SI_BY), 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, c->io_cur);
+    LAUNCHED();
+    k_io_rhs_si<1, true><<<grid, dim3(SI_BX, SI_BY), 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, c->io_cur);
+    LAUNCHED();
+    k_io_rhs_si<2, true><<<grid, dim3(SI_BX, SI_BY), 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, c->io_cur);
+    LAUNCHED();
+  } else {
+    k_io_rhs_si<0, false><<<grid, dim3(SI_BX, SI_BY), 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, c->io_cur);
+    LAUNCHED();
+    k_io_rhs_si<1, false><<<grid, dim3(SI_BX, SI_BY), 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, c->io_cur);
+    LAUNCHED();
+    k_io_rhs_si<2, false><<<grid, dim3(SI_BX, SI_BY), 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, c->io_cur);
+    LAUNCHED();
+  }
   *npart = (int)(grid.x * grid.y * grid.z);
   return CHAPSIM_OK;
 }
