@@ -562,8 +562,12 @@ __global__ void __launch_bounds__(256) k_si_x(TGDev d, IODev io, double coe1, do
 // boundary values) for component C: a block stages LB lines of consecutive x
 // (each row of the tile one coalesced load), its warps solve them in turn.
 // The y solve ends with G* = G + dG in the other G buffer from row N2I.
+// Four blocks per SM (64 registers, a few spilled words) with 8 lines each at
+// n = 192: the blocks' stage / solve / store phases overlap better than two
+// blocks of 16 lines (momentum stage of the heated 384x192x192 channel 8.35
+// -> 7.35 ms per substep).
 template <int C, bool Y>
-__global__ void __launch_bounds__(256) k_si_zy(TGDev d, IODev io, double coe1, double coe2, int LB, int cur) {
+__global__ void __launch_bounds__(256, 4) k_si_zy(TGDev d, IODev io, double coe1, double coe2, int LB, int cur) {
   extern __shared__ double zs_smem[];
   const int nx = d.nx, ny = d.ny;
   const int n = Y ? ny : d.nz;
@@ -657,8 +661,9 @@ int io_mom_si(chapsim_ctx *c, int ns, int *npart) {
 // other G buffer.
 namespace {
 int zy_lines_per_block(int n) {
-  // lines of one z / y block: as many as fit in 100 KB (4 arrays of n values)
-  int lb = (int)(100 * 1024 / ((size_t)32 * n));
+  // lines of one z / y block: as many as fit in 50 KB (4 arrays of n values),
+  // so that four blocks share an SM
+  int lb = (int)(50 * 1024 / ((size_t)32 * n));
   return lb < 1 ? 1 : (lb > 32 ? 32 : lb);
 }
 template <int C>
