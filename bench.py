@@ -892,8 +892,9 @@ def profile_case(spec, precision):
     from chapsim1ww_b200 import TGChannel
     if spec.lower().startswith("io"):
         from chapsim1ww_b200 import IOChannel
-        nx, ny, nz = (int(x) for x in spec.lower()[2:].split("x"))
-        c = IOChannel(nx, ny, nz, table=io_table("synthetic"))
+        si = spec.lower().startswith("iosi")  # the semi-implicit viscous scheme
+        nx, ny, nz = (int(x) for x in spec.lower()[4 if si else 2:].split("x"))
+        c = IOChannel(nx, ny, nz, table=io_table("synthetic"), visc_scheme=1 if si else 0)
         c.random_fl_theml_fld_io(2, 0.1)
         for _ in range(2):
             for ns in (1, 2, 3):
@@ -926,7 +927,8 @@ def main():
     ap.add_argument("--no-props", action="store_true", help="skip the learned-property measurement")
     ap.add_argument("--profile-case", default=None, metavar="NXxNYxNZ",
                     help="run init + NS=0 + 2 eager RK3 steps of a channel of this size and exit "
-                         "(the small case for ncu captures; no timing); prefix io for an IO channel")
+                         "(the small case for ncu captures; no timing); prefix io for an IO channel, "
+                         "iosi for an IO channel with the semi-implicit viscous scheme")
     args = ap.parse_args()
     if args.profile_case:
         return profile_case(args.profile_case, args.precision)

@@ -448,25 +448,40 @@ __device__ __forceinline__ void y_coef(const TGDev &d, const IODev &io, const Pr
 // with three right-hand sides), which leaves a P-unknown tridiagonal system
 // for the chunk ends, cyclic when the line is; parallel cyclic reduction over
 // shuffles solves it; then every lane back-substitutes its chunk.  The
-// arrays live in shared memory with element i = p m + t at t P + p, so the
-// lanes' sweeps touch consecutive words.  The result overwrites R.
+// arrays live in shared memory with element i = p m + t at t Q + p
+// (Q = P + 1, part_slot), so the lanes' sweeps touch consecutive words.  The result overwrites R.
 __host__ __device__ inline int part_count(int n) {
   int P = 1;
   while (P < 32 && n % (2 * P) == 0 && n / (2 * P) >= 2) P *= 2;
   return P;
 }
-__device__ __forceinline__ int part_slot(int i, int m, int P) { return (i % m) * P + i / m; }
+// Shared-memory layout of one line: element i at (i % m) * Q + i / m, rows of
+// pitch Q = P + 1, so the lanes' chunk walks (row t, lane p: t * Q + p) read
+// consecutive words and the coalesced staging loops, whose lanes take
+// consecutive i, spread over the banks instead of hitting one bank at stride P.
+__device__ __forceinline__ int part_slot(int i, int m, int Q) { return (i % m) * Q + i / m; }
+// values of one line array: m rows of pitch P + 1
+__host__ __device__ inline int part_len(int n) {
+  const int P = part_count(n);
+  return (n / P) * (P + 1);
+}
+// stride of the lines of a z / y block (4 arrays), = 2 (mod 16) words: the
+// staging loops' 8 lines x 2 elements per half-warp then fall in 16 banks
+__host__ __device__ inline int zy_stride(int n) {
+  const int s = 4 * part_len(n);
+  return s + ((2 - s) % 16 + 16) % 16;
+}
 
 template <bool CYC>
 __device__ void warp_part_solve(double *__restrict__ A, double *__restrict__ B, double *__restrict__ Cc,
-                                double *__restrict__ R, int P, int m, int lane) {
+                                double *__restrict__ R, int P, int Q, int m, int lane) {
   const bool act = lane < P;
   double yl = 0.0, vl = 0.0, wl = 0.0, yf = 0.0, vf = 0.0, wf = 0.0;
   double ae = 0.0, be = 1.0, ce = 0.0, re = 0.0;
   if (act) {
     double h = 0.0, y = 0.0, v = 0.0, w = 0.0;
     for (int t = 0; t <= m - 2; ++t) {
-      const int q = t * P + lane;
+      const int q = t * Q + lane;
       const double a = A[q], b = B[q], c = Cc[q], r = R[q];
       const double al = t == 0 ? 0.0 : a;       // first row: a couples to L(p-1)
       const double cu = t == m - 2 ? 0.0 : c;   // last interior row: c couples to L(p)
@@ -479,7 +494,7 @@ __device__ void warp_part_solve(double *__restrict__ A, double *__restrict__ B, 
     }
     yl = y; vl = v; wl = w;
     for (int t = m - 3; t >= 0; --t) {
-      const int q = t * P + lane;
+      const int q = t * Q + lane;
       const double hq = Cc[q];
       y = R[q] - hq * y;
       v = A[q] - hq * v;
@@ -487,7 +502,7 @@ __device__ void warp_part_solve(double *__restrict__ A, double *__restrict__ B, 
       R[q] = y; A[q] = v; B[q] = w;
     }
     yf = y; vf = v; wf = w;
-    const int qe = (m - 1) * P + lane;
+    const int qe = (m - 1) * Q + lane;
     ae = A[qe]; be = B[qe]; ce = Cc[qe]; re = R[qe];
   }
   const unsigned full = 0xffffffffu;
@@ -521,10 +536,10 @@ __device__ void warp_part_solve(double *__restrict__ A, double *__restrict__ B, 
   if (!CYC && lane == 0) Lm = 0.0;
   if (act) {
     for (int t = 0; t <= m - 2; ++t) {
-      const int q = t * P + lane;
+      const int q = t * Q + lane;
       R[q] = R[q] + A[q] * Lm + B[q] * L;
     }
-    R[(m - 1) * P + lane] = L;
+    R[(m - 1) * Q + lane] = L;
   }
 }
 
@@ -540,8 +555,8 @@ __global__ void __launch_bounds__(256) k_si_x(TGDev d, IODev io, double coe1, do
   const int line = blockIdx.x * nw + warp;
   if (line >= nj * d.nz) return;  // whole warp leaves together
   const int j = j0 + line % nj, k = line / nj;
-  const int P = part_count(nx), m = nx / P;
-  double *A = xs_smem + (size_t)warp * 4 * nx, *B = A + nx, *Cc = B + nx, *Rs = Cc + nx;
+  const int P = part_count(nx), m = nx / P, Q = P + 1, len = m * Q;
+  double *A = xs_smem + (size_t)warp * 4 * len, *B = A + len, *Cc = B + len, *Rs = Cc + len;
   const Prop Pr = make_prop(d, io);
   double *__restrict__ R = (double *)d.rhs[C] + d.sy * j + d.sz * k;
   const double sub = (C == 0 && use_dpg) ? *io.dpg : 0.0;
@@ -549,13 +564,13 @@ __global__ void __launch_bounds__(256) k_si_x(TGDev d, IODev io, double coe1, do
   for (int i = lane; i < nx; i += 32) {
     double a, b, cc;
     cyc_coef<C, true>(Pr, i, j, k, coe1, coe2, a, b, cc);
-    const int q = part_slot(i, m, P);
+    const int q = part_slot(i, m, Q);
     A[q] = a; B[q] = b; Cc[q] = cc; Rs[q] = R[i] - sub;
   }
   __syncwarp();
-  warp_part_solve<true>(A, B, Cc, Rs, P, m, lane);
+  warp_part_solve<true>(A, B, Cc, Rs, P, Q, m, lane);
   __syncwarp();
-  for (int i = lane; i < nx; i += 32) R[i] = Rs[part_slot(i, m, P)];
+  for (int i = lane; i < nx; i += 32) R[i] = Rs[part_slot(i, m, Q)];
 }
 
 // Lines along z (MOMFA2_Z_io, cyclic) or y (MOMFA3_Y_io, rows 1..ny, zero
@@ -576,7 +591,7 @@ __global__ void __launch_bounds__(256, 4) k_si_zy(TGDev d, IODev io, double coe1
   const int nl = min(LB, nx - i0);
   // z lines: blockIdx.y = row j - j0; y lines: blockIdx.y = plane k
   const int jz = Y ? 0 : j0 + (int)blockIdx.y, ky = Y ? (int)blockIdx.y : 0;
-  const int P = part_count(n), m = n / P;
+  const int P = part_count(n), m = n / P, Q = P + 1, len = m * Q, S = zy_stride(n);
   const Prop Pr = make_prop(d, io);
   const int64_t st = Y ? d.sy : d.sz;
   const int64_t base = Y ? d.sz * ky : d.sy * jz;  // + i, + st * (index along the line)
@@ -596,20 +611,20 @@ __global__ void __launch_bounds__(256, 4) k_si_zy(TGDev d, IODev io, double coe1
       cyc_coef<C, false>(Pr, i, jz, e, coe1, coe2, a, b, cc);
       g = i + base + st * e;
     }
-    double *L = zs_smem + (size_t)l * 4 * n;
-    const int q = part_slot(e, m, P);
-    L[q] = a; L[n + q] = b; L[2 * n + q] = cc; L[3 * n + q] = R[g];
+    double *L = zs_smem + (size_t)l * S;
+    const int q = part_slot(e, m, Q);
+    L[q] = a; L[len + q] = b; L[2 * len + q] = cc; L[3 * len + q] = R[g];
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   for (int l = warp; l < nl; l += nw) {
-    double *L = zs_smem + (size_t)l * 4 * n;
-    warp_part_solve<!Y>(L, L + n, L + 2 * n, L + 3 * n, P, m, lane);
+    double *L = zs_smem + (size_t)l * S;
+    warp_part_solve<!Y>(L, L + len, L + 2 * len, L + 3 * len, P, Q, m, lane);
   }
   __syncthreads();
   for (int t = threadIdx.x; t < n * nl; t += blockDim.x) {
     const int e = t / nl, l = t - e * nl, i = i0 + l;
-    const double x = zs_smem[(size_t)l * 4 * n + 3 * n + part_slot(e, m, P)];
+    const double x = zs_smem[(size_t)l * S + 3 * len + part_slot(e, m, Q)];
     if (Y) {
       const int j = e + 1;
       if (j >= j0) {
@@ -675,19 +690,19 @@ int si_solves(chapsim_ctx *c, double facoe, double cx1, double cx2, double cz1, 
     // rows per block: as many as fit in 110 KB (4 arrays of nx values each)
     int wpb = (int)(110 * 1024 / ((size_t)32 * d.nx));
     wpb = wpb < 1 ? 1 : (wpb > 8 ? 8 : wpb);
-    const size_t sm = (size_t)wpb * 4 * d.nx * sizeof(double);
+    const size_t sm = (size_t)wpb * 4 * part_len(d.nx) * sizeof(double);
     k_si_x<C><<<(nj * d.nz + wpb - 1) / wpb, 32 * wpb, sm, c->stream>>>(d, io, cx1, cx2, 1);
     LAUNCHED();
   }
   {
     const int lb = zy_lines_per_block(d.nz);
-    k_si_zy<C, false><<<dim3((d.nx + lb - 1) / lb, nj), 256, (size_t)lb * 4 * d.nz * sizeof(double), c->stream>>>(
+    k_si_zy<C, false><<<dim3((d.nx + lb - 1) / lb, nj), 256, (size_t)lb * zy_stride(d.nz) * sizeof(double), c->stream>>>(
         d, io, cz1, cz2, lb, c->io_cur);
     LAUNCHED();
   }
   {
     const int lb = zy_lines_per_block(d.ny);
-    k_si_zy<C, true><<<dim3((d.nx + lb - 1) / lb, d.nz), 256, (size_t)lb * 4 * d.ny * sizeof(double), c->stream>>>(
+    k_si_zy<C, true><<<dim3((d.nx + lb - 1) / lb, d.nz), 256, (size_t)lb * zy_stride(d.ny) * sizeof(double), c->stream>>>(
         d, io, facoe, 0.0, lb, c->io_cur);
     LAUNCHED();
   }
