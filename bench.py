@@ -208,6 +208,37 @@ def dist_setup():
     return ws, rank, local
 
 
+def dist_init(ws):
+    """NCCL process group of the replicas (None on one GPU); the timeout
+    bounds any rank that waits for a rank that died."""
+    if ws <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def dist_done(pg):
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def max_over_ranks(pg, local, x):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
 def load_traffic(workload, kernel):
     p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
     try:
@@ -382,11 +413,9 @@ def run_io(args, wl, ws, rank, local):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded splitmix64 velocity, h = 0, table properties, NS=0 projection)",
-            "config": {"workload": args.workload, **{k: wl[k] for k in ("nx", "ny", "nz", "ren", "dt", "prt")},
-                       "wall_heat_flux": wl["qw"], "table": wl["table"], "precision": "fp64",
-                       "viscous_scheme": "semi-implicit (MOMFA_io)" if visc else "explicit",
-                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-                       "l2": "working set (>2 GB) larger than the 126 MB L2"},
+            "config": workload_config(args, wl),
+            "arm": {"parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                    "l2": "working set (>2 GB) larger than the 126 MB L2"},
             "max_div_g_plus_drho": divmax, "out_of_table_cells": bad,
             "gpu_launches": launches,
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
@@ -573,13 +602,9 @@ def run_pair(args, wl, ws, rank, local):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if prec == cs.FP64 else "f64 state / f32 temporaries (TG)",
             "data": "synthetic (seeded splitmix64 velocity, NS=0 projection; IO h = 0 with table properties)",
-            "config": {"workload": args.workload,
-                       "tg": {k: wt[k] for k in ("nx", "ny", "nz", "ren", "dt")},
-                       "io": {**{k: wi[k] for k in ("nx", "ny", "nz", "ren", "dt", "prt")},
-                              "table": wi["table"], "wall_heat_flux": wi["qw"], "x": "periodic (inlet coupling not built)"},
-                       "cells": cells, "precision": args.precision,
-                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU, two streams alternating per step",
-                       "l2": "working set (>4 GB) larger than the 126 MB L2"},
+            "config": workload_config(args, wl),
+            "arm": {"parallelism": f"replicas x{ws}" if ws > 1 else "single GPU, two streams alternating per step",
+                    "l2": "working set (>4 GB) larger than the 126 MB L2"},
             "sections_ms_per_step": {"tg": ms_tg, "io": ms_io, "both": ms / args.steps},
             "max_div_u_tg": tg.divgck_tg(), "max_div_g_plus_drho_io": io.divgck_io(),
             "gpu_launches": launches,
@@ -619,96 +644,152 @@ def cpu_baseline_oracle(wl, steps):
     return cells * steps / t, t, get_threads()
 
 
-def run_reference_pair(args, wl, ws):
-    """Both sections with the oracle port, at most 8 timed steps (each a full
-    step of both sections) after at most 1 warm-up step."""
-    from oracle.pyoracle import OracleIO, OracleTG, get_threads
-    wt, wi = WORKLOADS[wl["tg"]], WORKLOADS[wl["io"]]
-    ot = OracleTG(wt["nx"], wt["ny"], wt["nz"], lx=wt["lx"], lz=wt["lz"], ren=wt["ren"], dt=wt["dt"])
-    ot.init_random(wt["seed"], 0.1)
-    ot.substep(0)
-    oi = OracleIO(wi["nx"], wi["ny"], wi["nz"], lx=wi["lx"], lz=wi["lz"], ren=wi["ren"], dt=wi["dt"],
-                  thermal=wi["thermal"], prt=wi["prt"], qw=(wi["qw"], wi["qw"]), table=io_table(wi["table"]))
-    oi.init_random(wi["seed"], 0.1)
-    nw, nt = min(args.warmup, 1), min(args.steps, 8)
-    for _ in range(nw):
-        ot.step(1)
-        oi.step(1)
+def section_specs(wl):
+    """(kind, spec) of every section a workload advances per step."""
+    if wl.get("pair"):
+        return [("tg", WORKLOADS[wl["tg"]]), ("io", WORKLOADS[wl["io"]])]
+    if wl.get("batch"):
+        from chapsim1ww_b200 import batch64_configs
+        return [("tg", dict(c, seed=wl["seed"] + i)) for i, c in enumerate(batch64_configs(seed=wl["seed"]))]
+    return [("io" if wl.get("io") else "tg", wl)]
+
+
+def make_oracle(kind, spec, nz):
+    """FP64 oracle of one section on a z-slab of nz planes (the same mesh
+    spacing as the full section: Lz scaled by nz / Nz), initialised as the
+    GPU arm is (seeded field, NS=0 projection)."""
+    from oracle.pyoracle import OracleIO, OracleTG
+    lz = spec["lz"] * nz / spec["nz"]
+    if kind == "tg":
+        o = OracleTG(spec["nx"], spec["ny"], nz, lx=spec["lx"], lz=lz, ren=spec["ren"], dt=spec["dt"])
+        o.init_random(spec["seed"], 0.1)
+        o.substep(0)
+    else:
+        o = OracleIO(spec["nx"], spec["ny"], nz, lx=spec["lx"], lz=lz, ren=spec["ren"], dt=spec["dt"],
+                     thermal=spec["thermal"], prt=spec["prt"], qw=(spec["qw"], spec["qw"]),
+                     table=io_table(spec["table"]), visc_scheme=spec.get("visc_scheme", 0))
+        o.init_random(spec["seed"], 0.1)
+    return o
+
+
+def reference_sample(wl, steps, warmup, budget_s):
+    """Pick the bounded sample of the workload the reference arm times: every
+    section (or channel) as a z-slab of the same mesh spacing, sized from one
+    calibration step of 8-plane slabs so that warmup + steps full RK3 steps
+    take about budget_s seconds.  Returns [(kind, spec, nz_sample)]."""
+    secs = section_specs(wl)
+    if wl.get("batch"):
+        secs = secs[:8]  # the first 8 channels, each a slab
+    cal_nz = 8
+    cells_cal = sum(sp["nx"] * sp["ny"] * min(cal_nz, sp["nz"]) for _, sp in secs)
+    objs = [make_oracle(k, sp, min(cal_nz, sp["nz"])) for k, sp in secs]
     t0 = time.perf_counter()
-    for _ in range(nt):
-        ot.step(1)
-        oi.step(1)
-    t = time.perf_counter() - t0
-    cells = wt["nx"] * wt["ny"] * wt["nz"] + wi["nx"] * wi["ny"] * wi["nz"]
-    v = cells * nt / t
-    cores = get_threads()
-    line = {
-        "impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1000 * t / nt, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded splitmix64 field)",
-        "config": {"workload": args.workload, "tg": {k: wt[k] for k in ("nx", "ny", "nz", "ren", "dt")},
-                   "io": {k: wi[k] for k in ("nx", "ny", "nz", "ren", "dt", "prt")}, "parallelism": "host threads"},
-        "cpu_baseline": {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
-                         "sample": f"{nt} timed full steps of both sections after {nw} warm-up step(s) (capped at "
-                                   f"8 so the run stays within minutes), FP64 oracle (restatement of the Fortran "
-                                   f"path), OpenMP {cores} threads"},
-        "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
-    print(json.dumps(line), flush=True)
-    return 0
+    for o in objs:
+        o.step(1)
+    rate = cells_cal / max(time.perf_counter() - t0, 1e-6)  # cell-steps/s of the sample mix
+    del objs
+    cells_target = rate * budget_s / max(steps + warmup, 1)
+    frac = cells_target / sum(sp["nx"] * sp["ny"] * sp["nz"] for _, sp in secs)
+    out = []
+    for k, sp in secs:
+        nz = int(sp["nz"] * min(frac, 1.0)) // 8 * 8
+        out.append((k, sp, max(8, min(nz, sp["nz"]))))
+    return out
 
 
 def run_reference(args, wl, ws, rank):
+    """The reference algorithm's CPU path (the FP64 oracle port, all host
+    threads) on rank 0: W warm-up and K timed full RK3 steps of a bounded
+    sample of the workload (z-slabs with the workload's mesh spacing)."""
     if rank != 0:
         return 0
-    if wl.get("pair"):
-        return run_reference_pair(args, wl, ws)
-    from oracle.pyoracle import OracleIO, OracleTG, get_threads
-    nzc = wl.get("cpu_nz", wl.get("nz"))  # z-slab of a workload too large for the host
-    if wl.get("io"):
-        o = OracleIO(wl["nx"], wl["ny"], nzc, lx=wl["lx"], lz=wl["lz"] * nzc / wl["nz"], ren=wl["ren"], dt=wl["dt"],
-                     thermal=wl["thermal"], prt=wl["prt"], qw=(wl["qw"], wl["qw"]), table=io_table(wl["table"]),
-                     visc_scheme=wl.get("visc_scheme", 0))
-        o.init_random(wl["seed"], 0.1)
-    else:
-        o = OracleTG(wl["nx"], wl["ny"], wl["nz"], lx=wl["lx"], lz=wl["lz"], ren=wl["ren"], dt=wl["dt"])
-        o.init_random(wl["seed"], 0.1)
-        o.substep(0)
+    from oracle.pyoracle import get_threads
+    sample = reference_sample(wl, args.steps, args.warmup, args.ref_budget)
+    objs = [make_oracle(k, sp, nz) for k, sp, nz in sample]
     for _ in range(args.warmup):
-        o.step(1)
+        for o in objs:
+            o.step(1)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        o.step(1)
+        for o in objs:
+            o.step(1)
     t = time.perf_counter() - t0
-    cells = wl["nx"] * wl["ny"] * nzc
+    cells = sum(sp["nx"] * sp["ny"] * nz for _, sp, nz in sample)
     v = cells * args.steps / t
     cores = get_threads()
-    slab = f" ({nzc}-plane z-slab of it, same cell size)" if nzc != wl["nz"] else ""
+    desc = ", ".join(f"{k} {sp['nx']}x{sp['ny']}x{nz} of {sp['nz']} planes" for k, sp, nz in sample)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000 * t / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded splitmix64 field)",
-        "config": {"workload": args.workload, **{k: wl[k] for k in ("nx", "ny", "nz", "ren", "dt")},
-                   "parallelism": "host threads"},
+        "scaling": workload_scaling(wl), "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded splitmix64 field, NS=0 projection)",
+        "config": workload_config(args, wl),
+        "arm": {"impl": "FP64 oracle port (restatement of the Fortran path), OpenMP", "threads": cores},
         "cpu_baseline": {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
-                         "sample": f"{args.steps} full RK3 steps of the {args.workload} channel{slab}, FP64 "
-                                   f"oracle (restatement of the Fortran path), OpenMP {cores} threads"},
+                         "sample": f"{args.warmup} warm-up + {args.steps} timed full RK3 steps of z-slabs with the "
+                                   f"workload's mesh spacing ({desc}; {cells} cells per step, sized to about "
+                                   f"{args.ref_budget:.0f} s of host work), FP64 oracle, OpenMP {cores} threads"},
         "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
+def workload_scaling(wl):
+    # the 64-channel batch is split across ranks (total work fixed); every
+    # other workload runs one independent replica per rank
+    return "strong" if wl.get("batch") else "weak"
+
+
+def workload_config(args, wl):
+    """The config block both arms print for a workload."""
+    if wl.get("batch"):
+        return {"workload": args.workload, "channels": 64, "seed": wl["seed"], "precision": args.precision,
+                "steps_unit": "one RK3 step of every channel"}
+    if wl.get("pair"):
+        wt, wi = WORKLOADS[wl["tg"]], WORKLOADS[wl["io"]]
+        return {"workload": args.workload,
+                "tg": {k: wt[k] for k in ("nx", "ny", "nz", "ren", "dt")},
+                "io": {**{k: wi[k] for k in ("nx", "ny", "nz", "ren", "dt", "prt")},
+                       "table": wi["table"], "wall_heat_flux": wi["qw"], "x": "periodic (inlet coupling not built)"},
+                "cells": wt["nx"] * wt["ny"] * wt["nz"] + wi["nx"] * wi["ny"] * wi["nz"],
+                "precision": args.precision}
+    cfg = {"workload": args.workload, **{k: wl[k] for k in ("nx", "ny", "nz", "ren", "dt")},
+           "cells": wl["nx"] * wl["ny"] * wl["nz"], "precision": args.precision}
+    if wl.get("io"):
+        cfg.update(prt=wl["prt"], wall_heat_flux=wl["qw"], table=wl["table"],
+                   viscous_scheme="semi-implicit (MOMFA_io)" if wl.get("visc_scheme") else "explicit")
+    return cfg
+
+
+def shard_channels(cells, ws, rank):
+    """Channel indices of one rank: channels dealt largest first to the rank
+    with the fewest cells so far (ties to the lower rank), so every rank gets
+    a near-equal share of the work; deterministic and identical on all ranks."""
+    load = [0] * ws
+    own = [[] for _ in range(ws)]
+    for i in sorted(range(len(cells)), key=lambda q: (-cells[q], q)):
+        r = min(range(ws), key=lambda q: (load[q], q))
+        load[r] += cells[i]
+        own[r].append(i)
+    return sorted(own[rank])
+
+
 def run_batch(args, wl, ws, rank, local):
-    """64 uneven channels advanced by one graph launch per step."""
+    """The 64 uneven channels split across the ranks (shard_channels; no
+    data-path collective), each rank advancing its share by one graph launch
+    per step.  value = all 64 channels' cells x steps / max-over-ranks time."""
     import torch
 
     import chapsim1ww_b200 as cs
     from chapsim1ww_b200 import ChannelBatch, batch64_configs
 
     torch.cuda.set_device(local)
+    pg = dist_init(ws)
     prec = cs.FP64 if args.precision == "fp64" else cs.MIXED
-    cfgs = batch64_configs(seed=wl["seed"] + rank)
+    all_cfgs = batch64_configs(seed=wl["seed"])
+    mine = shard_channels([c["nx"] * c["ny"] * c["nz"] for c in all_cfgs], ws, rank)
+    cfgs = [all_cfgs[i] for i in mine]
     b = ChannelBatch(cfgs, precision=prec, device=local)
     t0 = time.perf_counter()
     b.autotune(reps=3)
@@ -719,29 +800,35 @@ def run_batch(args, wl, ws, rank, local):
     stream = torch.cuda.ExternalStream(b.stream(), device=local)
     clocks = ClockSampler(local)
     clocks.start()
+    barrier(pg)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     b.step(args.steps)
     e1.record(stream)
     e1.synchronize()
+    torch.cuda.synchronize()
+    barrier(pg)
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1)
-    divmax = max(ch.divgck_tg() for ch in b.channels)
-    value = b.cells * args.steps / (ms / 1000.0)
+    ms = max_over_ranks(pg, local, e0.elapsed_time(e1))
+    divmax = max_over_ranks(pg, local, max(ch.divgck_tg() for ch in b.channels))
+    total_cells = sum(c["nx"] * c["ny"] * c["nz"] for c in all_cfgs)
+    value = total_cells * args.steps / (ms / 1000.0)
+    launches = int(max_over_ranks(pg, local, float(b.kernels_per_step() * args.steps)))
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if prec == cs.FP64 else "f64 state / f32 temporaries",
+        "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": workload_scaling(wl),
+        "vs_baseline": None, "dtype": "f64" if prec == cs.FP64 else "f64 state / f32 temporaries",
         "data": "synthetic (64 channels, sizes and Re drawn from seed 3)",
-        "config": {"workload": "batch64", "channels": len(cfgs), "cells": b.cells, "precision": args.precision,
-                   "graph": "one CUDA graph launch per step, channels as parallel branches",
-                   "autotune_s": t_tune},
-        "max_div_u": divmax, "gpu_launches": b.kernels_per_step() * args.steps, "clocks": clk,
+        "config": workload_config(args, wl),
+        "arm": {"graph": "one CUDA graph launch per step, channels as parallel branches",
+                "channels_per_rank": len(cfgs), "cells_rank0": b.cells, "autotune_s": t_tune},
+        "max_div_u": divmax, "gpu_launches": launches, "clocks": clk,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
     b.close()
+    dist_done(pg)
     return 0
 
 
@@ -860,9 +947,9 @@ def run_ours(args, wl, ws, rank, local):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if prec == cs.FP64 else "f64 state / f32 temporaries",
             "data": "synthetic (seeded splitmix64 initial field, NS=0 projection)",
-            "config": {"workload": args.workload, **{k: wl[k] for k in ("nx", "ny", "nz", "ren", "dt")},
-                       "precision": args.precision, "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
-                       "l2": "working set (>1 GB) larger than the 126 MB L2"},
+            "config": workload_config(args, wl),
+            "arm": {"parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                    "l2": "working set (>1 GB) larger than the 126 MB L2"},
             "max_div_u": divmax,
             "gpu_launches": launches,
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": nbytes,
@@ -914,6 +1001,20 @@ def profile_case(spec, precision):
     return 0
 
 
+def launch_ranks(n):
+    """Run this same command as n ranks, one per GPU, under
+    torch.distributed.run on 127.0.0.1 (used when --gpus N > 1 is given
+    without an outside launcher); returns the launcher's exit code."""
+    import socket
+    sock = socket.socket()
+    sock.bind(("127.0.0.1", 0))
+    port = sock.getsockname()[1]
+    sock.close()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -923,6 +1024,8 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c1_tg_io")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--ref-budget", type=float, default=100.0,
+                    help="seconds of host work the reference arm's W + K steps are sized to")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-props", action="store_true", help="skip the learned-property measurement")
     ap.add_argument("--profile-case", default=None, metavar="NXxNYxNZ",
@@ -933,6 +1036,8 @@ def main():
     if args.profile_case:
         return profile_case(args.profile_case, args.precision)
     args.warmup = max(args.warmup, 3)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return launch_ranks(args.gpus)
     wl = WORKLOADS[args.workload]
     ws, rank, local = dist_setup()
     if args.impl == "reference":

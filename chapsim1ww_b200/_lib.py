@@ -39,6 +39,7 @@ class ChapsimIOConfig(ctypes.Structure):
         ("struct_size", ctypes.c_int32), ("thermal", ctypes.c_int32), ("prt", ctypes.c_double),
         ("qw_bot", ctypes.c_double), ("qw_top", ctypes.c_double), ("gravdir", ctypes.c_int32),
         ("visc_scheme", ctypes.c_int32), ("f_a", ctypes.c_double),
+        ("coupled", ctypes.c_int32), ("reserved", ctypes.c_int32),
     ]
 
 
@@ -133,7 +134,8 @@ SIGNATURES += [
     ("chapsim_stats_reset", _I, [_P]),
     ("chapsim_write_instant", _I, [_P, ctypes.c_char_p, _I, _D]),
     ("chapsim_read_instant", _I, [_P, ctypes.c_char_p, _D, ctypes.POINTER(_I), _DP]),
-    ("chapsim_instant_file_name", _I, [ctypes.c_char_p, _I, ctypes.c_char_p, _D, ctypes.c_char_p]),
+    ("chapsim_inject_wait_timeout", _I, [_P, _I]),
+    ("chapsim_instant_file_name", _I, [ctypes.c_char_p, _I, ctypes.c_char_p, _D, ctypes.c_char_p, _I]),
     ("chapsim_instant_file_write", _I, [ctypes.c_char_p, _I, _I, _I, _I, _D, _D, _D, _P]),
     ("chapsim_instant_file_read", _I, [ctypes.c_char_p, _I, _I, _I, ctypes.POINTER(_I), _DP, _DP, _DP, _P]),
 ]

@@ -7,7 +7,7 @@ ROOT = os.path.dirname(HERE)
 
 
 def build_library(verbose=False):
-    out = subprocess.run(["make", "-C", os.path.join(HERE, "csrc")], capture_output=True, text=True)
+    out = subprocess.run(["make", "-j8", "-C", os.path.join(HERE, "csrc")], capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("libchapsim build failed:\n" + out.stdout + out.stderr)
     if verbose:

@@ -603,6 +603,8 @@ int chapsim_io_config_default(chapsim_io_config *io) {
   io->gravdir = 0;
   io->visc_scheme = 0;
   io->f_a = 0.0;
+  io->coupled = 0;
+  io->reserved = 0;
   return CHAPSIM_OK;
 }
 
@@ -612,6 +614,7 @@ int chapsim_create_io(const chapsim_config *cfg, const chapsim_io_config *io, ch
   if (cfg->precision != CHAPSIM_FP64) return CHAPSIM_ERR_UNSUPPORTED;
   if (!(io->prt > 0) || io->gravdir < 0 || io->gravdir > 3) return CHAPSIM_ERR_ARG;
   if (io->visc_scheme != 0 && io->visc_scheme != 1) return CHAPSIM_ERR_ARG;
+  if (io->coupled != 0 && io->coupled != 1) return CHAPSIM_ERR_ARG;
   return create_ctx(cfg, io, out);
 }
 
@@ -643,6 +646,12 @@ int chapsim_sync(chapsim_ctx *ctx) {
   if (!ctx) return CHAPSIM_ERR_ARG;
   CKC(cudaStreamSynchronize(ctx->stream));
   return check_device_error(ctx);
+}
+
+int chapsim_inject_wait_timeout(chapsim_ctx *ctx, int polls) {
+  if (!ctx || polls < 1 || polls > (1 << 20)) return CHAPSIM_ERR_ARG;
+  CKC(cudaSetDevice(ctx->device));
+  return chapsim::launch_wait_probe(ctx, polls);
 }
 
 int64_t chapsim_field_len(const chapsim_ctx *ctx) {

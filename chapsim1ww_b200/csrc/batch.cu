@@ -127,45 +127,78 @@ static int time_substeps(chapsim_ctx *c, int reps, float *ms) {
   return rc;
 }
 
+// Time every candidate launch shape of one channel and keep the fastest.
+// The fields the trial substeps overwrite are saved first; on every exit
+// after the save (success or a failed trial) they are copied back and the
+// save buffer is freed, so a failure never leaves trial state behind.
+static int autotune_channel(chapsim_batch *b, chapsim_ctx *c, int reps) {
+  const size_t n = (size_t)c->d.sz * c->d.nz;
+  const size_t tsz = c->cfg.precision == CHAPSIM_MIXED ? sizeof(float) : sizeof(double);
+  char *sp = nullptr;
+  if (cudaMalloc((void **)&sp, n * (4 * sizeof(double) + 3 * tsz)) != cudaSuccess) {
+    cudaGetLastError();
+    b->err = "autotune: cannot allocate the save buffer";
+    return CHAPSIM_ERR_NOMEM;
+  }
+  double *f[4] = {c->d.u, c->d.v, c->d.w, c->d.p};
+  auto copy_all = [&](bool save) {
+    bool ok = true;
+    for (int q = 0; q < 4; ++q) {
+      char *s = sp + q * n * sizeof(double);
+      ok = ok && cudaMemcpyAsync(save ? (void *)s : (void *)f[q], save ? (const void *)f[q] : (const void *)s,
+                                 n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream) == cudaSuccess;
+    }
+    for (int q = 0; q < 3; ++q) {
+      char *s = sp + 4 * n * sizeof(double) + q * n * tsz;
+      ok = ok && cudaMemcpyAsync(save ? (void *)s : c->d.h0[q], save ? (const void *)c->d.h0[q] : (const void *)s,
+                                 n * tsz, cudaMemcpyDeviceToDevice, c->stream) == cudaSuccess;
+    }
+    return ok;
+  };
+  int rc = CHAPSIM_OK;
+  if (!copy_all(true)) {
+    cudaGetLastError();
+    cudaFree(sp);
+    b->err = "autotune: saving the channel state failed";
+    return CHAPSIM_ERR_CUDA;
+  }
+  // candidate launch shapes
+  const int nzc_c[] = {8, 16, 32, 64};
+  const int lb_c[] = {0, 4, 8, 16};
+  float best = 1e30f;
+  int bn = c->rhs_nzc, bl = c->fft_lb;
+  for (int nzc : nzc_c) {
+    if (nzc > c->d.nz || rc) continue;
+    for (int lb : lb_c) {
+      c->rhs_nzc = nzc;
+      c->fft_lb = lb;
+      float ms = 0.f;
+      if ((rc = time_substeps(c, reps, &ms))) break;
+      if (ms < best) { best = ms; bn = nzc; bl = lb; }
+    }
+  }
+  c->rhs_nzc = bn;
+  c->fft_lb = bl;
+  // single exit: restore the saved state, then free the buffer
+  const bool restored = copy_all(false) && cudaStreamSynchronize(c->stream) == cudaSuccess;
+  if (!restored) cudaGetLastError();
+  cudaFree(sp);
+  if (c->step_graph) { cudaGraphExecDestroy(c->step_graph); c->step_graph = nullptr; }
+  if (rc) return rc;
+  if (!restored) {
+    b->err = "autotune: restoring the channel state failed";
+    return CHAPSIM_ERR_CUDA;
+  }
+  return CHAPSIM_OK;
+}
+
 int chapsim_batch_autotune(chapsim_batch *b, int reps) {
   if (!b || reps < 1) return CHAPSIM_ERR_ARG;
   BCK(cudaSetDevice(b->device));
   drop_graph(b);
   for (auto *c : b->ch) {
-    // save the state the trial substeps overwrite
-    const size_t n = (size_t)c->d.sz * c->d.nz;
-    const size_t tsz = c->cfg.precision == CHAPSIM_MIXED ? sizeof(float) : sizeof(double);
-    void *save = nullptr;
-    BCK(cudaMalloc(&save, n * (4 * sizeof(double) + 3 * tsz)));
-    char *sp = (char *)save;
-    double *f[4] = {c->d.u, c->d.v, c->d.w, c->d.p};
-    for (int q = 0; q < 4; ++q) BCK(cudaMemcpyAsync(sp + q * n * sizeof(double), f[q], n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-    for (int q = 0; q < 3; ++q)
-      BCK(cudaMemcpyAsync(sp + 4 * n * sizeof(double) + q * n * tsz, c->d.h0[q], n * tsz, cudaMemcpyDeviceToDevice, c->stream));
-    // candidate launch shapes
-    const int nzc_c[] = {8, 16, 32, 64};
-    const int lb_c[] = {0, 4, 8, 16};
-    float best = 1e30f;
-    int bn = c->rhs_nzc, bl = c->fft_lb;
-    for (int nzc : nzc_c) {
-      if (nzc > c->d.nz) continue;
-      for (int lb : lb_c) {
-        c->rhs_nzc = nzc;
-        c->fft_lb = lb;
-        float ms = 0.f;
-        int rc = time_substeps(c, reps, &ms);
-        if (rc) { cudaFree(save); return rc; }
-        if (ms < best) { best = ms; bn = nzc; bl = lb; }
-      }
-    }
-    c->rhs_nzc = bn;
-    c->fft_lb = bl;
-    for (int q = 0; q < 4; ++q) BCK(cudaMemcpyAsync(f[q], sp + q * n * sizeof(double), n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-    for (int q = 0; q < 3; ++q)
-      BCK(cudaMemcpyAsync(c->d.h0[q], sp + 4 * n * sizeof(double) + q * n * tsz, n * tsz, cudaMemcpyDeviceToDevice, c->stream));
-    BCK(cudaStreamSynchronize(c->stream));
-    cudaFree(save);
-    if (c->step_graph) { cudaGraphExecDestroy(c->step_graph); c->step_graph = nullptr; }
+    const int rc = autotune_channel(b, c, reps);
+    if (rc) return rc;
   }
   return CHAPSIM_OK;
 }

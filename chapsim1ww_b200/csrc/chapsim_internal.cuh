@@ -167,6 +167,7 @@ struct chapsim_ctx {
   CUtensorMap io_maps[14];
   bool use_tma_io = false;
   int io_nzc = 16;  // z planes per block of the TMA momentum RHS
+  bool si_smem_set = false;  // semi-implicit solve kernels got their shared-memory limit
   // on-device statistics (partials, xz averages, time averages) and the
   // number of samples in the time average
   double *stats_buf = nullptr;
@@ -187,6 +188,8 @@ int launch_pois3d(chapsim_ctx *c);
 int launch_correction(chapsim_ctx *c, int ns);
 int launch_reduce(chapsim_ctx *c, int what, double *host_out);
 int launch_bc_q(chapsim_ctx *c);
+// fault-injection hook: a bounded mbarrier wait that nothing completes
+int launch_wait_probe(chapsim_ctx *c, int polls);
 // Poisson solve of an IO domain: DIVG_io of (gx, gy, gz) + drho fused into the
 // forward x-transform, then the spectral y-solve with the mean mode pinned at
 // the last row, into phi.

@@ -11,7 +11,9 @@
 // File names: <dir>DNS_perixz_INSTANT_T<time as ES15.9>_<var>.D with var
 // U, V, W, P (TG: Q_tg and PR_tg; IO: G_io and PR_io, src/processing/
 // WRT_VARS_IO.f90:22-150) and, for a thermal IO section, T, D, E
-// (TEMPERATURE, DENSITY, ENTHALPY).
+// (TEMPERATURE, DENSITY, ENTHALPY).  An IO section that runs beside a TG
+// section writes DNS_perioz_INSTANT_T... instead (WRT_VARS_IO.f90:24-28,
+// RESTART_io.f90:25-29), so the two sections never overwrite each other.
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <string.h>
@@ -32,9 +34,9 @@ std::string es15_9(double t) {
   return std::string(b);
 }
 
-std::string file_name(const char *dir, double time, const char *var) {
+std::string file_name(const char *dir, double time, const char *var, bool tg_and_io) {
   std::string s = dir ? dir : "";
-  s += "DNS_perixz_INSTANT_T";
+  s += tg_and_io ? "DNS_perioz_INSTANT_T" : "DNS_perixz_INSTANT_T";
   s += es15_9(time);
   s += "_";
   s += var;
@@ -46,9 +48,9 @@ std::string file_name(const char *dir, double time, const char *var) {
 
 extern "C" {
 
-int chapsim_instant_file_name(char *buf, int buflen, const char *dir, double time, const char *var) {
+int chapsim_instant_file_name(char *buf, int buflen, const char *dir, double time, const char *var, int tg_and_io) {
   if (!buf || buflen < 1 || !var) return CHAPSIM_ERR_ARG;
-  const std::string s = file_name(dir, time, var);
+  const std::string s = file_name(dir, time, var, tg_and_io != 0);
   if ((int)s.size() + 1 > buflen) return CHAPSIM_ERR_ARG;
   memcpy(buf, s.c_str(), s.size() + 1);
   return CHAPSIM_OK;
@@ -160,7 +162,7 @@ int chapsim_write_instant(chapsim_ctx *ctx, const char *dir, int iteration, doub
   for (size_t q = 0; q < src.size(); ++q) {
     int rc = download(ctx, src[q], host);
     if (rc) return rc;
-    const std::string path = file_name(dir, time, names[q]);
+    const std::string path = file_name(dir, time, names[q], io && ctx->iocfg.coupled);
     rc = chapsim_instant_file_write(path.c_str(), d.nx, d.ny, d.nz, iteration, time, ctx->cfg.ren, ctx->cfg.dt,
                                     host.data());
     if (rc) {
@@ -188,7 +190,7 @@ int chapsim_read_instant(chapsim_ctx *ctx, const char *dir, double time, int *it
   double tm = 0.0;
   for (int q = 0; q < nf; ++q) {
     f[q].assign(n, 0.0);
-    const std::string path = file_name(dir, time, names[q]);
+    const std::string path = file_name(dir, time, names[q], io && ctx->iocfg.coupled);
     const int rc = chapsim_instant_file_read(path.c_str(), d.nx, d.ny, d.nz, &it, &tm, nullptr, nullptr, f[q].data());
     if (rc) {
       ctx->err = "cannot read " + path + " (missing, or written for another mesh)";

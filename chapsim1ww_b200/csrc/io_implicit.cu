@@ -715,18 +715,24 @@ int io_factor_si(chapsim_ctx *c, int ns) {
   const double facoe = 0.5 * c->sp[ns].alp * d.dt * d.cvisc;  // FACOE_io
   const double cx1 = facoe * 4.0 / 3.0 * d.dxqi, cx2 = facoe * d.dxqi;
   const double cz1 = facoe * 4.0 / 3.0 * d.dzqi, cz2 = facoe * d.dzqi;
-  static unsigned attrs = 0;  // devices whose solve kernels got the shared-memory limit
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev < 32 && !(attrs & (1u << dev))) {  // dynamic shared memory above 48 KB, process wide
+  if (!c->si_smem_set) {
+    // dynamic shared memory above 48 KB (k_si_zy at ny = 192 takes 51 KB):
+    // the limit is set per device, with that device current, by every
+    // context before its first solve; setting it again is harmless and it
+    // involves no process-wide bookkeeping shared between host threads
     int optin = 0;
-    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device);
     const void *fns[] = {(const void *)k_si_x<0>, (const void *)k_si_x<1>, (const void *)k_si_x<2>,
                          (const void *)k_si_zy<0, false>, (const void *)k_si_zy<1, false>,
                          (const void *)k_si_zy<2, false>, (const void *)k_si_zy<0, true>,
                          (const void *)k_si_zy<1, true>, (const void *)k_si_zy<2, true>};
-    for (const void *f : fns) cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-    attrs |= 1u << dev;
+    for (const void *f : fns)
+      if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) != cudaSuccess) {
+        cudaGetLastError();
+        c->err = "semi-implicit line solves: cannot raise the shared-memory limit";
+        return CHAPSIM_ERR_CUDA;
+      }
+    c->si_smem_set = true;
   }
   int rc;
   if ((rc = si_solves<0>(c, facoe, cx1, cx2, cz1, cz2))) return rc;

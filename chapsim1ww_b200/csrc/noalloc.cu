@@ -89,6 +89,9 @@ extern "C" int chapsim_divmax_noalloc(const double *u, const double *v, const do
   if (!u || !v || !w || !dyfi || !out || nx < 1 || ny < 1 || nz < 1) return CHAPSIM_ERR_ARG;
   const int64_t tiles = (int64_t)((nx + kTX - 1) / kTX) * ((ny + kTY - 1) / kTY) * nz;
   if (tiles > kNoAllocTiles || nz > 65535) return CHAPSIM_ERR_TOO_LARGE;  // 65,535: grid z limit
+  // an error left pending by the caller's own earlier work is not ours: leave
+  // it in place for the caller and launch nothing
+  if (cudaPeekAtLastError() != cudaSuccess) return CHAPSIM_ERR_CUDA;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
     cudaGetLastError();
@@ -111,6 +114,7 @@ extern "C" int chapsim_divmax_noalloc(const double *u, const double *v, const do
   dim3 grid((nx + kTX - 1) / kTX, (ny + kTY - 1) / kTY, nz);
   k_divmax_tiles<<<grid, dim3(kTX, kTY), 0, s>>>(u, v, w, dyfi, nx, ny, nz, dxi, dzi, partials);
   k_divmax_final<<<1, 1024, 0, s>>>(partials, (int)tiles, out);
+  // no error was pending on entry, so one now comes from these two launches
   if (cudaGetLastError() != cudaSuccess) return CHAPSIM_ERR_CUDA;
   return CHAPSIM_OK;
 }

@@ -1696,4 +1696,28 @@ int launch_reduce(chapsim_ctx *c, int what, double *host_out) {
   return CHAPSIM_OK;
 }
 
+// Fault-injection hook for the bounded waits: one warp initialises an
+// mbarrier that expects one arrival, never arrives on it, and waits with a
+// spin limit of `polls`.  The wait gives up, records kErrTmaTimeout in the
+// context's error word and the kernel returns; no copy is in flight, so
+// nothing else needs draining.  It exercises the same give-up path every TMA
+// consumer uses, with a limit small enough to end in microseconds.
+__global__ void k_wait_probe(int *err, uint32_t polls) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+  mbar_wait(&bar, 0, err, polls);
+  __syncwarp();
+  if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(&bar)) : "memory");
+}
+
+int launch_wait_probe(chapsim_ctx *c, int polls) {
+  k_wait_probe<<<1, 32, 0, c->stream>>>(c->d.err, (uint32_t)polls);
+  LAUNCHED();
+  return CHAPSIM_OK;
+}
+
 }  // namespace chapsim

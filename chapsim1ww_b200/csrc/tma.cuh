@@ -40,9 +40,10 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
 
 // Bounded wait for the phase with the given parity to complete.  Returns
 // false (and records kErrTmaTimeout) when the spin limit is reached.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err) {
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err,
+                                          uint32_t limit = kSpinLimit) {
   const uint32_t a = smem_u32(bar);
-  for (uint32_t it = 0; it < kSpinLimit; ++it) {
+  for (uint32_t it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"

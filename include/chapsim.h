@@ -7,7 +7,8 @@
  * index and work on module-global arrays.  Each entry point below replaces one
  * of those subroutines; the comment names the reference routine (file:line,
  * relative to the CHAPSim1WW project root) it stands in for.  A Fortran host
- * binds them with ISO_C_BINDING interfaces.
+ * binds them with ISO_C_BINDING interfaces, one bind(C) interface per entry
+ * point, passing its module arrays by address.
  *
  * Conventions
  *  - Every function returns an int status: CHAPSIM_OK (0) or a CHAPSIM_ERR_*
@@ -125,6 +126,17 @@ int chapsim_destroy(chapsim_ctx *ctx);
 const char *chapsim_last_error(const chapsim_ctx *ctx);
 int chapsim_sync(chapsim_ctx *ctx);
 
+/* Fault injection for the bounded device waits (no reference counterpart;
+ * the reference's failure path is ERRHDL, print and STOP,
+ * src/WRTHDL.f90:18-30).  Queues one kernel on the context's stream that
+ * waits, with a spin limit of polls (1 .. 2^20), on an mbarrier nothing
+ * completes -- the give-up path of every TMA consumer.  The wait runs out,
+ * the kernel records the timeout in the context's device error word and
+ * returns; the next chapsim_sync reports CHAPSIM_ERR_CUDA ("device-side wait
+ * gave up") and clears the word, after which the context works normally.
+ * Neither faults nor hangs the GPU. */
+int chapsim_inject_wait_timeout(chapsim_ctx *ctx, int polls);
+
 /* Length in doubles of one Fortran-layout field: nx*(ny+2)*nz. */
 int64_t chapsim_field_len(const chapsim_ctx *ctx);
 
@@ -204,7 +216,11 @@ int chapsim_stats_reset(chapsim_ctx *ctx);
  * int32 (nx, ny, nz, iteration), 3 x float64 (time, Re, dt), then the
  * interior F(1:nx, 1:ny, 1:nz) in Fortran order, native byte order.  Names
  * <dir>DNS_perixz_INSTANT_T<time, Fortran ES15.9>_<var>.D; var U, V, W, P
- * (TG: Q_tg, PR_tg; IO: G_io, PR_io) and, thermal IO, T, D, E.
+ * (TG: Q_tg, PR_tg; IO: G_io, PR_io) and, thermal IO, T, D, E.  An IO
+ * context created with coupled = 1 (a TG section runs beside it) uses the
+ * prefix DNS_perioz, as the reference does in its TG + IO mode
+ * (src/processing/WRT_VARS_IO.f90:24-28, RESTART_io.f90:25-29), so the two
+ * sections' files never share a name.
  * chapsim_write_instant writes the context's state; chapsim_read_instant
  * restarts from such files (RESTART_INSTANT_VARS_TG / _IO + FLOWSTART's wall
  * conditions; TG: CONVH0 = 0; IO: RHOH = D E, wall ghosts, THERM_PROP_UPDATE,
@@ -215,7 +231,9 @@ int chapsim_stats_reset(chapsim_ctx *ctx);
  * layout (ghost rows untouched) and need no GPU. */
 int chapsim_write_instant(chapsim_ctx *ctx, const char *dir, int iteration, double time);
 int chapsim_read_instant(chapsim_ctx *ctx, const char *dir, double time, int *iteration, double *time_out);
-int chapsim_instant_file_name(char *buf, int buflen, const char *dir, double time, const char *var);
+/* tg_and_io != 0 gives the DNS_perioz prefix of an IO section that runs
+ * beside a TG section. */
+int chapsim_instant_file_name(char *buf, int buflen, const char *dir, double time, const char *var, int tg_and_io);
 int chapsim_instant_file_write(const char *path, int nx, int ny, int nz, int iteration, double time, double ren,
                                double dt, const double *field);
 int chapsim_instant_file_read(const char *path, int nx, int ny, int nz, int *iteration, double *time, double *ren,
@@ -359,6 +377,11 @@ typedef struct chapsim_io_config {
                           1 semi-implicit (VISCOUS_PAR_EXPLT_*_io + MOMFA_io,
                           src/SOLVERRK3_MOM_IO.f90:73-87)                       */
   double f_a;          /* F_A, buoyancy coefficient (Flow_State.f90:98-110)         */
+  int32_t coupled;     /* TGFLOWFLG beside IOFLOWFLG: a TG section runs with this IO
+                          section (src/READINI.f90:121-131); its instantaneous-field
+                          files then take the prefix DNS_perioz instead of
+                          DNS_perixz (src/processing/WRT_VARS_IO.f90:24-28)      */
+  int32_t reserved;    /* 0                                                       */
 } chapsim_io_config;
 
 /* Defaults: thermal on, Pr = 0.71, qw = 1 on both walls, no buoyancy,
@@ -505,7 +528,9 @@ int chapsim_batch_kernels_per_step(const chapsim_batch *b, int64_t *count);
  * up the scratch address with that device current, so make it before any
  * stream capture.  All calls share the scratch (it keeps the last call's
  * tile maxima; every slot a call reads it writes first), so calls that
- * overlap on the GPU race. */
+ * overlap on the GPU race.  The call reports only its own launches: if a CUDA
+ * error is already pending on the calling thread it returns CHAPSIM_ERR_CUDA
+ * at once, launches nothing and leaves that error for the caller to read. */
 #define CHAPSIM_ERR_TOO_LARGE 9
 int chapsim_divmax_noalloc(const double *u, const double *v, const double *w, const double *dyfi, int nx, int ny,
                            int nz, double dxi, double dzi, double *out, void *stream);

@@ -58,3 +58,32 @@ def test_io_restart_state_and_oracle_parity(tmp_path):
     o.step(1)
     for n in ("u", "v", "w", "p", "gx", "h", "rho"):
         assert relerr(b.get_field(n), o.get(n)) <= 1e-10, n
+
+
+def test_tg_and_io_sections_share_a_directory(tmp_path):
+    """TG and coupled IO sections written into one directory keep separate
+    files (DNS_perixz / DNS_perioz) and each restarts from its own."""
+    _need_gpu()
+    import os
+
+    from chapsim1ww_b200 import IOChannel, TGChannel
+    from oracle.pyoracle import synth_table
+    d = str(tmp_path) + "/"
+    table = synth_table(4096)
+    tg = TGChannel(40, 18, 24)
+    tg.random_fl_fld_tg(1, 0.1)
+    io = IOChannel(40, 18, 24, table=table, coupled=1)
+    io.random_fl_theml_fld_io(2, 0.1)
+    tg.write_instant(d, 3, 0.003)
+    io.write_instant(d, 3, 0.003)
+    names = sorted(os.listdir(d))
+    assert sum(n.startswith("DNS_perixz") for n in names) == 4
+    assert sum(n.startswith("DNS_perioz") for n in names) == 7
+    tg2 = TGChannel(40, 18, 24)
+    tg2.read_instant(d, 0.003)
+    io2 = IOChannel(40, 18, 24, table=table, coupled=1)
+    io2.read_instant(d, 0.003)
+    for n in ("u", "v", "w", "p"):
+        assert np.array_equal(tg2.get_field(n), tg.get_field(n)), n
+    for n in ("gx", "gy", "gz", "p", "t", "rho", "h"):
+        assert relerr(io2.get_field(n)[:, 1:-1, :], io.get_field(n)[:, 1:-1, :]) <= 1e-14, n

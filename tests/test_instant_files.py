@@ -16,10 +16,19 @@ def lib():
 
 def test_file_name_matches_fortran_es15_9():
     buf = ctypes.create_string_buffer(512)
-    assert lib().chapsim_instant_file_name(buf, 512, b"run/", 2655.004202, b"U") == 0
+    assert lib().chapsim_instant_file_name(buf, 512, b"run/", 2655.004202, b"U", 0) == 0
     assert buf.value == b"run/DNS_perixz_INSTANT_T2.655004202E+03_U.D"
-    assert lib().chapsim_instant_file_name(buf, 512, b"", 0.0, b"E") == 0
+    assert lib().chapsim_instant_file_name(buf, 512, b"", 0.0, b"E", 0) == 0
     assert buf.value == b"DNS_perixz_INSTANT_T0.000000000E+00_E.D"
+
+
+def test_file_name_of_io_beside_tg_section():
+    """An IO section that runs beside a TG section names its files
+    DNS_perioz_... (src/processing/WRT_VARS_IO.f90:24-28), so a TG + IO run
+    writing both sections into one directory overwrites nothing."""
+    buf = ctypes.create_string_buffer(512)
+    assert lib().chapsim_instant_file_name(buf, 512, b"run/", 0.5, b"U", 1) == 0
+    assert buf.value == b"run/DNS_perioz_INSTANT_T5.000000000E-01_U.D"
 
 
 def test_write_layout_and_round_trip(tmp_path):
