@@ -102,6 +102,9 @@ SIGNATURES = [
     ("chapsim_props_update", _I, [_P, _I, _P, _P, _P, _P, _P, _P, _I64, ctypes.POINTER(_I64)]),
     ("chapsim_props_train", _I, [_P, _I, ctypes.c_uint64, _I, _D, _DP]),
     ("chapsim_props_gate", _I, [_P, _D, _I, ctypes.POINTER(_I), _DP]),
+    ("chapsim_set_props_mode", _I, [_P, _I, _P]),
+    ("chapsim_therm_prop_update", _I, [_P, _I, _I]),
+    ("chapsim_props_gate_outputs", _I, [_P, ctypes.POINTER(_I), _DP, _I]),
     ("chapsim_props_get_params", _I, [_P, _P, _I, _P, _I]),
     ("chapsim_props_set_params", _I, [_P, _P, _I, _P, _I]),
     ("chapsim_props_loss_grad", _I, [_P, _P, _P, _I, _DP, _P, _I]),

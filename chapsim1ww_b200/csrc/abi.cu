@@ -1115,7 +1115,67 @@ int chapsim_set_table(chapsim_ctx *ctx, const double *H, const double *T, const 
   }
   io.rhohmax = rm;
   ctx->has_table = true;
+  ctx->props_mode = CHAPSIM_PROPS_TABLE;  // a model trained on another table no longer applies
   return CHAPSIM_OK;
+}
+
+int chapsim_set_props_mode(chapsim_ctx *ctx, int mode, const chapsim_props *pe) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(ctx->domain == CHAPSIM_IIO && ctx->io.thermal, CHAPSIM_ERR_STATE,
+          "property modes belong to IO contexts with the energy equation");
+  REQUIRE(ctx->has_table, CHAPSIM_ERR_STATE, "no property table: call chapsim_set_table first");
+  REQUIRE(mode == CHAPSIM_PROPS_TABLE || mode == CHAPSIM_PROPS_MLP, CHAPSIM_ERR_ARG, "unknown property mode");
+  CKC(cudaSetDevice(ctx->device));
+  CKC(cudaStreamSynchronize(ctx->stream));
+  if (mode == CHAPSIM_PROPS_MLP) {
+    REQUIRE(pe, CHAPSIM_ERR_ARG, "the learned mode needs a property engine with a trained model");
+    chapsim_mlp::MlpDev src{};
+    int dev = -1;
+    const int rc = chapsim::props_model(pe, &src, &dev);
+    REQUIRE(rc == CHAPSIM_OK, rc, "the property engine has no trained model");
+    REQUIRE(dev == ctx->device, CHAPSIM_ERR_ARG, "property engine and context on different devices");
+    REQUIRE(chapsim::props_same_table(pe, ctx->tab), CHAPSIM_ERR_ARG,
+            "the model was trained on another table than the context's");
+    const size_t npar = chapsim_mlp::NP * sizeof(float);
+    const size_t nwt = (2 * chapsim_mlp::NH * chapsim_mlp::NH + 2 * chapsim_mlp::NOP * chapsim_mlp::NH) *
+                       sizeof(uint16_t);
+    if (!ctx->mlp_buf) {
+      void *p = nullptr;
+      if (cudaMalloc(&p, npar + nwt + chapsim_mlp::kMaxGateBins) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->err = "cannot allocate the model's buffers";
+        return CHAPSIM_ERR_NOMEM;
+      }
+      ctx->mlp_buf = p;
+      ctx->allocs.push_back(p);
+    }
+    char *b = static_cast<char *>(ctx->mlp_buf);
+    CKC(cudaMemcpyAsync(b, src.par, npar, cudaMemcpyDeviceToDevice, ctx->stream));
+    CKC(cudaMemcpyAsync(b + npar, src.wt, nwt, cudaMemcpyDeviceToDevice, ctx->stream));
+    CKC(cudaMemcpyAsync(b + npar + nwt, src.gate, chapsim_mlp::kMaxGateBins, cudaMemcpyDeviceToDevice, ctx->stream));
+    CKC(cudaStreamSynchronize(ctx->stream));
+    ctx->mlp = src;
+    ctx->mlp.par = reinterpret_cast<const float *>(b);
+    ctx->mlp.wt = reinterpret_cast<const uint16_t *>(b + npar);
+    ctx->mlp.gate = reinterpret_cast<const uint8_t *>(b + npar + nwt);
+  }
+  ctx->props_mode = mode;
+  for (auto &g : ctx->io_graph)  // the captured steps hold the other property kernel
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  return CHAPSIM_OK;
+}
+
+int chapsim_therm_prop_update(chapsim_ctx *ctx, int iregion, int mode) {
+  REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(ctx->domain == CHAPSIM_IIO && ctx->io.thermal && ctx->has_table, CHAPSIM_ERR_STATE,
+          "THERM_PROP_UPDATE needs an IO context with the energy equation and a table");
+  REQUIRE(iregion == CHAPSIM_IMAIND || iregion == CHAPSIM_IALLDM, CHAPSIM_ERR_UNSUPPORTED,
+          "region: the outlet plane (IOULET) is updated by chapsim_io_bc_outlet_eng");
+  REQUIRE(mode == CHAPSIM_PROPS_TABLE || mode == CHAPSIM_PROPS_MLP, CHAPSIM_ERR_ARG, "unknown property mode");
+  REQUIRE(mode == CHAPSIM_PROPS_TABLE || ctx->mlp.par, CHAPSIM_ERR_STATE,
+          "no model on the context: call chapsim_set_props_mode with a trained engine first");
+  CKC(cudaSetDevice(ctx->device));
+  return chapsim::io_therm_props(ctx, mode);
 }
 
 int chapsim_rk3_eng_io(chapsim_ctx *ctx, int ns) {

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/chapsim.h"
+#include "mlp_tc.cuh"
 #include "spline.cuh"
 
 namespace chapsim {
@@ -168,6 +169,12 @@ struct chapsim_ctx {
   bool use_tma_io = false;
   int io_nzc = 16;  // z planes per block of the TMA momentum RHS
   bool si_smem_set = false;  // semi-implicit solve kernels got their shared-memory limit
+  // property evaluation of the energy substep: table splines or the learned
+  // model (a copy of a trained engine's model in context-owned buffers)
+  int props_mode = CHAPSIM_PROPS_TABLE;
+  chapsim_mlp::MlpDev mlp{};
+  void *mlp_buf = nullptr;
+  bool mlp_smem_set = false;
   // on-device statistics (partials, xz averages, time averages) and the
   // number of samples in the time average
   double *stats_buf = nullptr;
@@ -211,6 +218,14 @@ int io_correction(chapsim_ctx *c, int ns);
 int io_init_maps(chapsim_ctx *c);
 int io_refresh_msum(chapsim_ctx *c);
 int io_restart_fields(chapsim_ctx *c);
+// learned properties (io_kernels.cu): THERM_PROP_UPDATE(IMAIND) by the table
+// or the model; kernel attributes; persistent grid size
+int io_therm_props(chapsim_ctx *c, int mode);
+int mlp_kernel_setup(chapsim_ctx *c);
+int mlp_grid(const chapsim_ctx *c);
+// the trained model of a property engine and its table (props.cu)
+int props_model(const chapsim_props *pe, chapsim_mlp::MlpDev *out, int *device);
+bool props_same_table(const chapsim_props *pe, const std::vector<double> *cols5);
 // TG statistics (stats.cu)
 int stats_run(chapsim_ctx *c, int accumulate);
 int stats_get(chapsim_ctx *c, int which, double *host, int64_t n);

@@ -269,6 +269,140 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_props_only(TGDev d, IODev i
   io.msum[c] = mu + mu;
 }
 
+// ------------------------------------------------------ learned properties
+// The property update of SOLVERRK3_ENG_IO (:46-55) with the learned model
+// (mlp_tc.cuh) in place of the table splines: VISCOUSITY0 / DENSITY0 <-
+// VISCOUSITY / DENSITY, then DENSITY_UPDATE on h = rho h / rho_old (the
+// model's rho), ENTHALPY_UPDATE, and THERM_PROP_UPDATE on the new h (the
+// model's T, rho, mu, k).  Cells whose h-bin the error gate has not cleared
+// for all four take the table splines, as do out-of-table checks.  The
+// field is walked as a flat array in 128-cell tiles (ghost rows keep the
+// plain kernel's treatment: mu0, rho0 and mu0 + mu only); every tile runs the
+// model twice on the tensor cores.
+__global__ void __launch_bounds__(chapsim_mlp::TILE, 4) k_io_eng_props_mlp(TGDev d, IODev io, chapsim_mlp::MlpDev M) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  chapsim_mlp::Smem &s = chapsim_mlp::smem_of(smem_raw);
+  chapsim_mlp::cta_setup(s, M);
+  uint32_t phase = 0;
+  const int64_t n = d.sz * d.nz;
+  const int64_t ntiles = (n + chapsim_mlp::TILE - 1) / chapsim_mlp::TILE;
+  const int64_t rows = d.ny + 2;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t c = tile * chapsim_mlp::TILE + threadIdx.x;
+    const bool valid = c < n;
+    const int j = valid ? (int)((c / d.nx) % rows) : 0;
+    const bool interior = valid && j >= 1 && j <= d.ny;
+    double dold = 1.0, muold = 0.0, rh = 0.0;
+    if (valid) {
+      dold = io.D[c];
+      muold = io.mu[c];
+      io.mu0[c] = muold;
+      io.D0[c] = dold;
+      if (!interior) io.msum[c] = muold + muold;  // ghost rows: the ghost kernel sets the new value
+      else rh = io.rhoh[c];
+    }
+    // DENSITY_UPDATE
+    const double h1 = rh / dold;
+    const double x1 = (h1 - M.hmid) / M.hhalf;
+    float y[chapsim_mlp::NO];
+    if (!chapsim_mlp::tile_eval(s, (float)x1, y, phase, d.err)) break;
+    int bad = 0;
+    double D = dold;
+    if (interior) {
+      double T;
+      if (!chapsim_spl::inside(io.ht, h1)) {
+        ++bad;
+      } else if ((chapsim_mlp::gate_mask(M, h1) & chapsim_mlp::kStepMask) == chapsim_mlp::kStepMask) {
+        D = chapsim_mlp::assemble(M, 1, x1, y[1]);
+      } else if (!(look_ht(io, h1, T) && look_td(io, T, D))) {
+        D = dold;
+        ++bad;
+      }
+    }
+    // ENTHALPY_UPDATE + THERM_PROP_UPDATE
+    const double h2 = rh / D;
+    const double x2 = (h2 - M.hmid) / M.hhalf;
+    if (!chapsim_mlp::tile_eval(s, (float)x2, y, phase, d.err)) break;
+    if (!interior) continue;
+    io.h[c] = h2;
+    double munew = muold;
+    if (!(io.shortcuts && fabs(h2) < 1.0e-10)) {
+      double T, M2, K, D2;
+      bool ok = chapsim_spl::inside(io.ht, h2);
+      if (ok && (chapsim_mlp::gate_mask(M, h2) & chapsim_mlp::kStepMask) == chapsim_mlp::kStepMask) {
+        T = chapsim_mlp::assemble(M, 0, x2, y[0]);
+        D2 = chapsim_mlp::assemble(M, 1, x2, y[1]);
+        M2 = chapsim_mlp::assemble(M, 2, x2, y[2]);
+        K = chapsim_mlp::assemble(M, 3, x2, y[3]);
+      } else {
+        ok = ok && look_ht(io, h2, T) && look_tprops(io, T, D2, M2, K);
+      }
+      if (ok) {
+        io.T[c] = T;
+        io.mu[c] = M2;
+        io.kap[c] = K;
+        D = D2;
+        munew = M2;
+      } else {
+        ++bad;
+      }
+    }
+    io.D[c] = D;
+    io.msum[c] = muold + munew;
+    if (bad) atomicAdd(io.bad, (unsigned long long)bad);
+  }
+  chapsim_mlp::cta_teardown(s);
+}
+
+// THERM_PROP_UPDATE(IMAIND) on its own (src/THERM_PROP_UPDATE.f90:129-205):
+// h -> T, mu, k, rho on the interior rows, by the table splines
+// (use_mlp = 0, one thread per cell) or the learned model with the table
+// where the gate has not cleared the bin; mu0 + mu follows the new mu.
+__global__ void __launch_bounds__(chapsim_mlp::TILE, 4) k_io_therm_props(TGDev d, IODev io, chapsim_mlp::MlpDev M,
+                                                                         int use_mlp) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  chapsim_mlp::Smem *sp = nullptr;
+  uint32_t phase = 0;
+  if (use_mlp) {
+    sp = &chapsim_mlp::smem_of(smem_raw);
+    chapsim_mlp::cta_setup(*sp, M);
+  }
+  const int64_t n = d.sz * d.nz;
+  const int64_t ntiles = (n + chapsim_mlp::TILE - 1) / chapsim_mlp::TILE;
+  const int64_t rows = d.ny + 2;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t c = tile * chapsim_mlp::TILE + threadIdx.x;
+    const bool valid = c < n;
+    const int j = valid ? (int)((c / d.nx) % rows) : 0;
+    const bool interior = valid && j >= 1 && j <= d.ny;
+    const double h = interior ? io.h[c] : 0.0;
+    const double x = use_mlp ? (h - M.hmid) / M.hhalf : 0.0;
+    float y[chapsim_mlp::NO];
+    if (use_mlp && !chapsim_mlp::tile_eval(*sp, (float)x, y, phase, d.err)) break;
+    if (!interior || (io.shortcuts && fabs(h) < 1.0e-10)) continue;
+    double T, D, Mu, K;
+    bool ok = chapsim_spl::inside(io.ht, h);
+    if (ok && use_mlp && (chapsim_mlp::gate_mask(M, h) & chapsim_mlp::kStepMask) == chapsim_mlp::kStepMask) {
+      T = chapsim_mlp::assemble(M, 0, x, y[0]);
+      D = chapsim_mlp::assemble(M, 1, x, y[1]);
+      Mu = chapsim_mlp::assemble(M, 2, x, y[2]);
+      K = chapsim_mlp::assemble(M, 3, x, y[3]);
+    } else {
+      ok = ok && look_ht(io, h, T) && look_tprops(io, T, D, Mu, K);
+    }
+    if (!ok) {
+      atomicAdd(io.bad, 1ull);
+      continue;
+    }
+    io.T[c] = T;
+    io.D[c] = D;
+    io.mu[c] = Mu;
+    io.kap[c] = K;
+    io.msum[c] = io.mu0[c] + Mu;
+  }
+  if (use_mlp) chapsim_mlp::cta_teardown(*sp);
+}
+
 // msum = mu0 + mu over the whole array (after the host replaces mu or mu0).
 __global__ void k_io_msum(IODev io, size_t n) {
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
@@ -975,6 +1109,30 @@ int io_thermal_bc(chapsim_ctx *c) {
   return CHAPSIM_OK;
 }
 
+// The learned-property kernels take more than 48 KB of dynamic shared memory
+// (set once per context) and run persistently, four CTAs of 128 threads per
+// SM (their tensor-memory columns fill the SM's 512).
+int mlp_kernel_setup(chapsim_ctx *c) {
+  if (c->mlp_smem_set) return CHAPSIM_OK;
+  const void *fns[] = {(const void *)k_io_eng_props_mlp, (const void *)k_io_therm_props};
+  for (const void *f : fns)
+    if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chapsim_mlp::kSmemBytes) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      c->err = "learned properties: cannot raise the shared-memory limit";
+      return CHAPSIM_ERR_CUDA;
+    }
+  c->mlp_smem_set = true;
+  return CHAPSIM_OK;
+}
+
+int mlp_grid(const chapsim_ctx *c) {
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  const int64_t tiles = (c->d.sz * c->d.nz + chapsim_mlp::TILE - 1) / chapsim_mlp::TILE;
+  return (int)std::min<int64_t>(tiles, (int64_t)nsm * 4);
+}
+
 // Phase-timer slots of an IO substep, in execution order: 0 energy RHS,
 // 1 property update + wall ghosts, 2 prep (DrhoDtP, u = G / rho), 3 momentum
 // RHS + DPGRNS, 4-8 the Poisson transforms and y-solve, 9 correction.
@@ -986,9 +1144,25 @@ int io_eng(chapsim_ctx *c, int ns) {
   LAUNCHED();
   dim3 g2((d.nx + IO_BX - 1) / IO_BX, (d.ny + 2 + IO_BY - 1) / IO_BY, d.nz);
   phase_mark(c, 1);
-  k_io_eng_props<<<g2, dim3(IO_BX, IO_BY), 0, c->stream>>>(d, c->io);
+  if (c->props_mode == CHAPSIM_PROPS_MLP) {
+    int rc = mlp_kernel_setup(c);
+    if (rc) return rc;
+    k_io_eng_props_mlp<<<mlp_grid(c), chapsim_mlp::TILE, chapsim_mlp::kSmemBytes, c->stream>>>(d, c->io, c->mlp);
+  } else {
+    k_io_eng_props<<<g2, dim3(IO_BX, IO_BY), 0, c->stream>>>(d, c->io);
+  }
   LAUNCHED();
   return io_thermal_bc(c);
+}
+
+int io_therm_props(chapsim_ctx *c, int mode) {
+  int rc = mlp_kernel_setup(c);
+  if (rc) return rc;
+  const bool mlp = mode == CHAPSIM_PROPS_MLP;
+  k_io_therm_props<<<mlp_grid(c), chapsim_mlp::TILE, mlp ? chapsim_mlp::kSmemBytes : 0, c->stream>>>(
+      c->d, c->io, c->mlp, mlp ? 1 : 0);
+  LAUNCHED();
+  return CHAPSIM_OK;
 }
 
 int io_mom(chapsim_ctx *c, int ns, bool prep) {

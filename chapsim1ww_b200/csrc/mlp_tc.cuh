@@ -1,0 +1,340 @@
+// Learned property model: inference core on the sm_100a tensor cores
+// (tcgen05.mma, BF16 operands, FP32 accumulators in tensor memory).
+//
+// The model maps x = (h - hmid) / hhalf to the five properties (T, rho, mu,
+// k, cp) as a least-squares polynomial base of degree 5 per output plus an
+// MLP 1 -> 64 -> 64 -> 5 (tanh) that carries the standardised residual:
+//   out_o = base_o(x) + mean_o + std_o * (W3 tanh(W2 tanh(W1 x + b1) + b2) + b3)_o
+// The reference has no such model (its THERM_PROP_UPDATE interpolates the
+// table by cubic splines, src/THERM_PROP_UPDATE.f90:129-205,
+// src/Flow_State.f90:1015-1070,1420-1581); the splines stay as the fallback.
+//
+// One CTA of 128 threads evaluates tiles of 128 cells (one cell per thread,
+// the MMA's M = 128 rows):
+//  - layer 1 on the CUDA cores in FP32 (tanh.approx.f32);
+//  - each activation vector is split into BF16 hi + lo parts (lo = the
+//    rounding error of hi), the weights likewise, and every layer runs as
+//    three BF16 MMAs accumulating in FP32 (hi*hi + hi*lo + lo*hi), which
+//    carries about 16 mantissa bits: plain BF16 operands (8 bits) leave the
+//    outputs about 1e-3 off, above the 1e-4 bound the model is gated on;
+//  - layer 2 (K = 64, N = 64) and layer 3 (K = 64, N = 16, rows 5..15 zero)
+//    are issued by one thread as tcgen05.mma kind::f16 from shared-memory
+//    operands in the canonical no-swizzle K-major layout, committed to one
+//    mbarrier; every thread reads its row back with tcgen05.ld.
+// The CTA holds 128 tensor-memory columns (layer 2 at columns 0..63, layer 3
+// at 64..79); four CTAs per SM use all 512.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tma.cuh"
+
+namespace chapsim_mlp {
+
+using chapsim::mbar_init;
+using chapsim::mbar_wait;
+using chapsim::smem_u32;
+
+constexpr int NH = 64, NO = 5, NOP = 16;  // hidden width, outputs, layer-3 N (padded)
+constexpr int TILE = 128;                 // cells per tile = MMA M
+constexpr int NBASE = 6;                  // polynomial base: degree 5
+constexpr int NP = NH + NH + NH * NH + NH + NO * NH + NO;  // 4613 FP32 parameters
+constexpr int O_W1 = 0, O_B1 = NH, O_W2 = 2 * NH, O_B2 = 2 * NH + NH * NH, O_W3 = O_B2 + NH, O_B3 = O_W3 + NO * NH;
+constexpr int TMEM_COLS = 128;
+constexpr int kMaxGateBins = 4096;
+// gate mask bits: output o may come from the model in a bin when bit o is set
+constexpr unsigned kStepMask = 0xF;  // T, rho, mu, k: what THERM_PROP_UPDATE produces
+
+// Bytes of one operand tile of `rows` rows x 64 BF16 (K) in the canonical
+// no-swizzle K-major layout: 8-row groups of eight 8x16-byte core matrices.
+__host__ __device__ constexpr int tile_bytes(int rows) { return rows * NH * 2; }
+// Byte offset of element (r, k) in such a tile: core matrices of one 8-row
+// group follow each other along K (LBO = 128 B), groups follow at SBO = 1024 B.
+__host__ __device__ constexpr int tile_off(int r, int k) {
+  return (r >> 3) * 1024 + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2;
+}
+
+// Model parameters on the device, passed by value to the kernels.
+struct MlpDev {
+  const float *par;      // NP FP32 parameters (W1, b1, W2, b2, W3, b3)
+  const uint16_t *wt;    // W2 hi, W2 lo (64 rows), W3 hi, W3 lo (16 rows): canonical tiles
+  const uint8_t *gate;   // per h-bin output mask
+  double hmid, hhalf;
+  double mean[NO], stdv[NO], base[NO][NBASE];  // base in powers of x, lowest first
+  double g0, ginv;       // gate bins: bin = (h - g0) * ginv
+  int nbins;
+};
+
+struct __align__(1024) Smem {
+  uint16_t a_hi[TILE * NH];  // 16 KB each
+  uint16_t a_lo[TILE * NH];
+  uint16_t w2_hi[NH * NH];   // 8 KB each
+  uint16_t w2_lo[NH * NH];
+  uint16_t w3_hi[NOP * NH];  // 2 KB each
+  uint16_t w3_lo[NOP * NH];
+  float w1[NH], b1[NH], b2[NH], b3[NOP];
+  uint64_t bar;
+  uint32_t tmem;
+  int fail;
+};
+
+// ---------------------------------------------------------------- PTX
+__device__ __forceinline__ float tanh_approx(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// Instruction descriptor of kind::f16: D FP32 (bits 4-5 = 1), A and B BF16
+// (bits 7-9, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at bits
+// 17-22, M >> 4 at bits 24-28.
+__host__ __device__ constexpr uint32_t idesc_bf16(int m, int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+// Shared-memory matrix descriptor: start address, LBO and SBO in 16-byte
+// units, descriptor version 1 (bits 46-47), no swizzle (bits 61-63 = 0).
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(1024u >> 4) << 32) |
+         (1ull << 46);
+}
+
+__device__ __forceinline__ void umma(uint32_t dtm, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtm),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 32 consecutive FP32 columns of this thread's TMEM lane, waited for in the
+// same statement so no use of the registers can be scheduled before the wait.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v) {
+  uint32_t r[8];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// BF16 round-to-nearest-even of two floats, packed (first in the low half).
+__device__ __forceinline__ uint32_t pack2(float a, float b) {
+  uint32_t r;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
+  return r;
+}
+
+// Write one thread's 64 activations into row r of the hi and lo A tiles.
+__device__ __forceinline__ void store_split(Smem &s, int r, const float *a) {
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    uint32_t hi[4], lo[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float x0 = a[8 * c + 2 * q], x1 = a[8 * c + 2 * q + 1];
+      hi[q] = pack2(x0, x1);
+      const float h0 = __uint_as_float(hi[q] << 16), h1 = __uint_as_float(hi[q] & 0xFFFF0000u);
+      lo[q] = pack2(x0 - h0, x1 - h1);
+    }
+    const int off = tile_off(r, 8 * c);
+    *reinterpret_cast<uint4 *>(reinterpret_cast<char *>(s.a_hi) + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+    *reinterpret_cast<uint4 *>(reinterpret_cast<char *>(s.a_lo) + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+  }
+}
+
+// The CTA's Smem inside its dynamic shared memory, placed on a 1024-byte
+// boundary (the kernels request sizeof(Smem) + 1024 bytes).
+__device__ __forceinline__ Smem &smem_of(unsigned char *raw) {
+  const uint32_t a = smem_u32(raw);
+  return *reinterpret_cast<Smem *>(raw + ((1024u - (a & 1023u)) & 1023u));
+}
+constexpr size_t kSmemBytes = sizeof(Smem) + 1024;
+
+// ------------------------------------------------------------ CTA set-up
+// Load the weights into shared memory, initialise the mbarrier and allocate
+// the CTA's tensor memory (warp 0).  Every thread of the 128 calls it.
+__device__ __forceinline__ void cta_setup(Smem &s, const MlpDev &M) {
+  const int t = threadIdx.x;
+  const uint4 *src = reinterpret_cast<const uint4 *>(M.wt);
+  uint4 *dst = reinterpret_cast<uint4 *>(s.w2_hi);  // w2_hi, w2_lo, w3_hi, w3_lo are contiguous
+  constexpr int n16 = (2 * NH * NH + 2 * NOP * NH) * 2 / 16;
+  for (int q = t; q < n16; q += TILE) dst[q] = src[q];
+  if (t < NH) {
+    s.w1[t] = M.par[O_W1 + t];
+    s.b1[t] = M.par[O_B1 + t];
+    s.b2[t] = M.par[O_B2 + t];
+  }
+  if (t < NOP) s.b3[t] = t < NO ? M.par[O_B3 + t] : 0.f;
+  if (t == 0) {
+    mbar_init(&s.bar, 1);
+    chapsim::fence_mbar_init();
+    s.fail = 0;
+  }
+  if (t < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s.tmem)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  chapsim::fence_proxy_async();  // weight tiles written by plain stores, read by the MMA
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+}
+
+__device__ __forceinline__ void cta_teardown(Smem &s) {
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (threadIdx.x < 32)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s.tmem), "r"(TMEM_COLS) : "memory");
+}
+
+// Issue one layer: D[:, 0:n) = A_hi W_hi^T + A_hi W_lo^T + A_lo W_hi^T over
+// K = 64 (four K = 16 steps each), then commit to the barrier.
+__device__ __forceinline__ void issue_layer(Smem &s, uint32_t dtm, const uint16_t *w_hi, const uint16_t *w_lo, int n) {
+  const uint32_t idesc = idesc_bf16(TILE, n);
+  const uint32_t ah = smem_u32(s.a_hi), al = smem_u32(s.a_lo), bh = smem_u32(w_hi), bl = smem_u32(w_lo);
+  const uint32_t as[3] = {ah, ah, al}, bs[3] = {bh, bl, bh};
+#pragma unroll
+  for (int part = 0; part < 3; ++part)
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks)
+      umma(dtm, sdesc(as[part] + 256u * ks), sdesc(bs[part] + 256u * ks), idesc, (part | ks) ? 1u : 0u);
+  umma_commit(&s.bar);
+}
+
+// Block-uniform bounded wait for the layer's commit: false on every thread
+// when any thread's wait ran out (the error word is set by mbar_wait).
+__device__ __forceinline__ bool layer_wait(Smem &s, uint32_t &phase, int *err) {
+  const bool ok = mbar_wait(&s.bar, phase, err);
+  phase ^= 1u;
+  if (!ok) s.fail = 1;
+  __syncthreads();
+  tc_fence_after();
+  return s.fail == 0;
+}
+
+// Evaluate the MLP on the tile: thread r holds cell r's normalised input x
+// and receives y[0..4] (standardised residual outputs, b3 included).  Every
+// thread of the CTA calls it together.  Returns false when a wait ran out
+// (then y is not valid and the caller stops).
+__device__ __forceinline__ bool tile_eval(Smem &s, float x, float (&y)[NO], uint32_t &phase, int *err) {
+  const int r = threadIdx.x;
+  const uint32_t lane_base = s.tmem + ((uint32_t)(r & ~31) << 16);
+  float a[NH];
+#pragma unroll
+  for (int k = 0; k < NH; ++k) a[k] = tanh_approx(fmaf(s.w1[k], x, s.b1[k]));
+  store_split(s, r, a);
+  chapsim::fence_proxy_async();
+  tc_fence_before();
+  __syncthreads();
+  if (r == 0) {
+    tc_fence_after();
+    issue_layer(s, s.tmem, s.w2_hi, s.w2_lo, NH);
+  }
+  if (!layer_wait(s, phase, err)) return false;
+  tmem_ld32(lane_base, a);
+  tmem_ld32(lane_base + 32, a + 32);
+#pragma unroll
+  for (int k = 0; k < NH; ++k) a[k] = tanh_approx(a[k] + s.b2[k]);
+  store_split(s, r, a);  // the layer-2 MMAs have completed: the A tiles are free
+  chapsim::fence_proxy_async();
+  tc_fence_before();
+  __syncthreads();
+  if (r == 0) {
+    tc_fence_after();
+    issue_layer(s, s.tmem + NH, s.w3_hi, s.w3_lo, NOP);
+  }
+  if (!layer_wait(s, phase, err)) return false;
+  float o[8];
+  tmem_ld8(lane_base + NH, o);
+#pragma unroll
+  for (int q = 0; q < NO; ++q) y[q] = o[q] + s.b3[q];
+  tc_fence_before();  // the next tile's MMAs overwrite these columns after its first __syncthreads
+  return true;
+}
+
+// Assemble output o from the standardised residual y at input x (FP64).
+__device__ __forceinline__ double assemble(const MlpDev &M, int o, double x, float y) {
+  double b = M.base[o][NBASE - 1];
+#pragma unroll
+  for (int p = NBASE - 2; p >= 0; --p) b = fma(b, x, M.base[o][p]);
+  return b + M.mean[o] + M.stdv[o] * (double)y;
+}
+
+__device__ __forceinline__ unsigned gate_mask(const MlpDev &M, double h) {
+  int bin = (int)((h - M.g0) * M.ginv);
+  bin = bin < 0 ? 0 : (bin >= M.nbins ? M.nbins - 1 : bin);
+  return M.gate[bin];
+}
+
+}  // namespace chapsim_mlp
+
+// Host-side helpers (props.cu): build the canonical BF16 hi/lo weight tiles
+// from the FP32 parameters.
+#include <string.h>
+namespace chapsim_mlp {
+inline uint16_t bf16_rn(float f) {
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  if ((u & 0x7F800000u) == 0x7F800000u) return (uint16_t)(u >> 16);  // inf / nan kept
+  u += 0x7FFFu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+inline float bf16_f(uint16_t b) {
+  const uint32_t u = (uint32_t)b << 16;
+  float f;
+  memcpy(&f, &u, 4);
+  return f;
+}
+// out: W2 hi (4096), W2 lo (4096), W3 hi (1024), W3 lo (1024) in tile order
+inline void build_weight_tiles(const float *par, uint16_t *out) {
+  uint16_t *w2h = out, *w2l = out + NH * NH, *w3h = out + 2 * NH * NH, *w3l = w3h + NOP * NH;
+  memset(out, 0, sizeof(uint16_t) * (2 * NH * NH + 2 * NOP * NH));
+  for (int n = 0; n < NH; ++n)
+    for (int k = 0; k < NH; ++k) {
+      const float w = par[O_W2 + n * NH + k];
+      const uint16_t h = bf16_rn(w);
+      const int e = tile_off(n, k) / 2;
+      w2h[e] = h;
+      w2l[e] = bf16_rn(w - bf16_f(h));
+    }
+  for (int n = 0; n < NO; ++n)
+    for (int k = 0; k < NH; ++k) {
+      const float w = par[O_W3 + n * NH + k];
+      const uint16_t h = bf16_rn(w);
+      const int e = tile_off(n, k) / 2;
+      w3h[e] = h;
+      w3l[e] = bf16_rn(w - bf16_f(h));
+    }
+}
+}  // namespace chapsim_mlp

@@ -1,6 +1,7 @@
 // Thermal property engine: table cubic splines (THERM_PROP_UPDATE) and the
-// learned property model (MLP h -> T, rho, mu, k, cp) with its GPU training
-// and an error-gated BF16 tensor-core inference path.
+// learned property model (polynomial base + MLP h -> T, rho, mu, k, cp) with
+// its GPU training and an error-gated inference path on the sm_100a tensor
+// cores (tcgen05, mlp_tc.cuh).
 //
 // Reference (CHAPSim1WW, paths relative to the project root):
 //   THERM_PROP_UPDATE   src/THERM_PROP_UPDATE.f90:129-205
@@ -8,8 +9,7 @@
 //   CUBIC_SPLINE        src/Flow_State.f90:1693-1787 (the published
 //                       Forsythe-Malcolm-Moler spline, restated below)
 //   table columns       src/Flow_State.f90:394-433
-// The MLP has no counterpart in the reference.
-#include <cuda_bf16.h>
+// The learned model has no counterpart in the reference.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <string.h>
@@ -18,27 +18,29 @@
 #include <vector>
 
 #include "../../include/chapsim.h"
+#include "chapsim_internal.cuh"
+#include "mlp_tc.cuh"
 #include "spline.cuh"
 
 namespace {
 
 using namespace chapsim_spl;
-
-constexpr int NH = 64, NO = 5;
-constexpr int NP = NH + NH + NH * NH + NH + NO * NH + NO;  // 4613
-constexpr int O_W1 = 0, O_B1 = NH, O_W2 = 2 * NH, O_B2 = 2 * NH + NH * NH, O_W3 = O_B2 + NH, O_B3 = O_W3 + NO * NH;
+using chapsim_mlp::NH;
+using chapsim_mlp::NO;
+using chapsim_mlp::NP;
+using chapsim_mlp::O_B1;
+using chapsim_mlp::O_B2;
+using chapsim_mlp::O_B3;
+using chapsim_mlp::O_W1;
+using chapsim_mlp::O_W2;
+using chapsim_mlp::O_W3;
+constexpr int NNORM = 2 + 2 * NO + NO * chapsim_mlp::NBASE;  // hmid, hhalf, mean, std, base
 
 struct PropsDev {
   Spline ht, hcp, td, tm, tk;
   int *err_count;
-  // MLP inference
-  const __nv_bfloat16 *w2b;  // [64][64] (row = output unit)
-  const __nv_bfloat16 *w3b;  // [8][64], rows 5..7 zero
-  const float *params;       // W1, b1, b2, b3 read in FP32
-  double hmid, hhalf, mean[NO], stdv[NO];
-  const int *gate;  // per h-bin: 1 = MLP, 0 = table
-  double g0, ginv;
-  int nbins;
+  int *dev_err;  // bounded-wait error word of the inference kernel
+  chapsim_mlp::MlpDev M;
 };
 
 // THERM_PROP_UPDATE for one cell; returns false when h or T is outside the
@@ -74,140 +76,50 @@ __global__ void k_props_table(PropsDev P, const double *__restrict__ h, double *
 }
 
 // ---------------------------------------------------------------- MLP
-__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
-  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
-  return *reinterpret_cast<uint32_t *>(&v);
-}
-
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};"
-      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
-// Hardware tanh approximation (tanh.approx.f32, sm_75+), used only in the
-// BF16 inference path, whose weights and activations carry ~4e-3 relative
-// precision anyway; training uses tanhf.
-__device__ __forceinline__ float tanh_fast(float x) {
-  float y;
-  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-
-// MLP forward for the 16 cells of a warp (m16n8k16 BF16 tensor-core MMA, FP32
-// accumulation): layer 1 in FP32 straight into A fragments, layer 2 as
-// 4 x 8 MMAs against W2 in shared memory, its accumulators re-packed as the A
-// fragments of layer 3 (N = 5 padded to 8).  out[] = standardised outputs of
-// columns 2q, 2q+1 for rows g and g+8 (q = lane & 3, g = lane >> 2).
-__device__ void mlp_warp(const PropsDev &P, const __nv_bfloat16 *sW2, const __nv_bfloat16 *sW3, float xg, float xg8,
-                         float (&out)[4]) {
-  const int lane = threadIdx.x & 31, q = lane & 3;
-  const float *W1 = P.params + O_W1, *b1 = P.params + O_B1, *b2 = P.params + O_B2;
-  uint32_t a[4][4];
-#pragma unroll
-  for (int kt = 0; kt < 4; ++kt) {
-    const int c0 = kt * 16 + q * 2, c1 = c0 + 8;
-    a[kt][0] = pack_bf16(tanh_fast(W1[c0] * xg + b1[c0]), tanh_fast(W1[c0 + 1] * xg + b1[c0 + 1]));
-    a[kt][1] = pack_bf16(tanh_fast(W1[c0] * xg8 + b1[c0]), tanh_fast(W1[c0 + 1] * xg8 + b1[c0 + 1]));
-    a[kt][2] = pack_bf16(tanh_fast(W1[c1] * xg + b1[c1]), tanh_fast(W1[c1 + 1] * xg + b1[c1 + 1]));
-    a[kt][3] = pack_bf16(tanh_fast(W1[c1] * xg8 + b1[c1]), tanh_fast(W1[c1 + 1] * xg8 + b1[c1 + 1]));
-  }
-  const int g = lane >> 2;
-  float acc[8][4];
-#pragma unroll
-  for (int nt = 0; nt < 8; ++nt) {
-    acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
-    const __nv_bfloat16 *wrow = sW2 + (nt * 8 + g) * NH;
-#pragma unroll
-    for (int kt = 0; kt < 4; ++kt) {
-      const uint32_t b0 = *reinterpret_cast<const uint32_t *>(wrow + kt * 16 + q * 2);
-      const uint32_t b1v = *reinterpret_cast<const uint32_t *>(wrow + kt * 16 + q * 2 + 8);
-      mma_bf16(acc[nt], a[kt], b0, b1v);
+// Property update with the learned model: the model on every 128-cell tile
+// (tensor cores), then per cell the reference's skip / range rules and the
+// error gate, per output: an output whose bit is clear in the cell's h-bin
+// comes from the table splines.
+__global__ void __launch_bounds__(chapsim_mlp::TILE, 4)
+    k_props_mlp_tc(PropsDev P, const double *__restrict__ h, double *T, double *rho, double *mu, double *kk,
+                   double *cp, int64_t n) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  chapsim_mlp::Smem &s = chapsim_mlp::smem_of(smem_raw);
+  const chapsim_mlp::MlpDev &M = P.M;
+  chapsim_mlp::cta_setup(s, M);
+  uint32_t phase = 0;
+  const int64_t ntiles = (n + chapsim_mlp::TILE - 1) / chapsim_mlp::TILE;
+  const unsigned need = cp ? 0x1Fu : chapsim_mlp::kStepMask;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t c = tile * chapsim_mlp::TILE + threadIdx.x;
+    const double hv = c < n ? h[c] : 0.0;
+    const double x = (hv - M.hmid) / M.hhalf;
+    float y[NO];
+    if (!chapsim_mlp::tile_eval(s, (float)x, y, phase, P.dev_err)) break;
+    if (c >= n || fabs(hv) < 1.0e-10) continue;  // reference leaves these cells unchanged
+    if (!(hv > P.ht.x[0] && hv < P.ht.x[P.ht.n - 1])) {
+      atomicAdd(P.err_count, 1);
+      continue;
     }
-  }
-  uint32_t a3[4][4];
+    double o[NO];
 #pragma unroll
-  for (int kt = 0; kt < 4; ++kt) {
-    const int n0 = 2 * kt, n1 = 2 * kt + 1;
-    const int c0 = n0 * 8 + q * 2, c1 = n1 * 8 + q * 2;
-    a3[kt][0] = pack_bf16(tanh_fast(acc[n0][0] + b2[c0]), tanh_fast(acc[n0][1] + b2[c0 + 1]));
-    a3[kt][1] = pack_bf16(tanh_fast(acc[n0][2] + b2[c0]), tanh_fast(acc[n0][3] + b2[c0 + 1]));
-    a3[kt][2] = pack_bf16(tanh_fast(acc[n1][0] + b2[c1]), tanh_fast(acc[n1][1] + b2[c1 + 1]));
-    a3[kt][3] = pack_bf16(tanh_fast(acc[n1][2] + b2[c1]), tanh_fast(acc[n1][3] + b2[c1 + 1]));
-  }
-  out[0] = out[1] = out[2] = out[3] = 0.f;
-  const __nv_bfloat16 *w3row = sW3 + g * NH;
-#pragma unroll
-  for (int kt = 0; kt < 4; ++kt) {
-    const uint32_t b0 = *reinterpret_cast<const uint32_t *>(w3row + kt * 16 + q * 2);
-    const uint32_t b1v = *reinterpret_cast<const uint32_t *>(w3row + kt * 16 + q * 2 + 8);
-    mma_bf16(out, a3[kt], b0, b1v);
-  }
-}
-
-constexpr int MI_WARPS = 4, MI_CELLS = MI_WARPS * 16;
-
-// Property update with the learned model: MLP for all cells of the block,
-// then per cell the reference's skip / range rules and the error gate (bins
-// not cleared for the MLP take the table splines).
-__global__ void __launch_bounds__(MI_WARPS * 32) k_props_mlp(PropsDev P, const double *__restrict__ h, double *T,
-                                                              double *rho, double *mu, double *kk, double *cp,
-                                                              int64_t n) {
-  __shared__ __align__(16) __nv_bfloat16 sW2[NH * NH];
-  __shared__ __align__(16) __nv_bfloat16 sW3[8 * NH];
-  __shared__ float sout[MI_CELLS][8];
-  for (int t = threadIdx.x; t < NH * NH; t += blockDim.x) sW2[t] = P.w2b[t];
-  for (int t = threadIdx.x; t < 8 * NH; t += blockDim.x) sW3[t] = P.w3b[t];
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-  const float *b3 = P.params + O_B3;
-  for (int64_t base = (int64_t)blockIdx.x * MI_CELLS; base < n; base += (int64_t)gridDim.x * MI_CELLS) {
-    const int64_t r0 = base + warp * 16 + g, r1 = r0 + 8;
-    const float x0 = r0 < n ? (float)((h[r0] - P.hmid) / P.hhalf) : 0.f;
-    const float x1 = r1 < n ? (float)((h[r1] - P.hmid) / P.hhalf) : 0.f;
-    float o[4];
-    mlp_warp(P, sW2, sW3, x0, x1, o);
-    const int c = q * 2;
-    sout[warp * 16 + g][c] = o[0];
-    sout[warp * 16 + g][c + 1] = o[1];
-    sout[warp * 16 + g + 8][c] = o[2];
-    sout[warp * 16 + g + 8][c + 1] = o[3];
-    __syncthreads();
-    if (threadIdx.x < MI_CELLS) {
-      const int64_t cidx = base + threadIdx.x;
-      if (cidx < n) {
-        const double hv = h[cidx];
-        if (fabs(hv) >= 1.0e-10) {
-          if (!(hv > P.ht.x[0] && hv < P.ht.x[P.ht.n - 1])) {
-            atomicAdd(P.err_count, 1);
-          } else {
-            int bin = (int)((hv - P.g0) * P.ginv);
-            bin = bin < 0 ? 0 : (bin >= P.nbins ? P.nbins - 1 : bin);
-            double t, r, m, kv, cpv;
-            bool ok = true;
-            if (P.gate[bin]) {
-              const float *so = sout[threadIdx.x];
-              t = (so[0] + b3[0]) * P.stdv[0] + P.mean[0];
-              r = (so[1] + b3[1]) * P.stdv[1] + P.mean[1];
-              m = (so[2] + b3[2]) * P.stdv[2] + P.mean[2];
-              kv = (so[3] + b3[3]) * P.stdv[3] + P.mean[3];
-              cpv = (so[4] + b3[4]) * P.stdv[4] + P.mean[4];
-            } else {
-              ok = table_props(P, hv, t, r, m, kv, cpv);
-              if (!ok) atomicAdd(P.err_count, 1);
-            }
-            if (ok) {
-              T[cidx] = t; rho[cidx] = r; mu[cidx] = m; kk[cidx] = kv;
-              if (cp) cp[cidx] = cpv;
-            }
-          }
-        }
+    for (int q = 0; q < NO; ++q) o[q] = chapsim_mlp::assemble(M, q, x, y[q]);
+    const unsigned mask = chapsim_mlp::gate_mask(M, hv);
+    if ((mask & need) != need) {
+      double t, r, m, kv, cpv;
+      if (!table_props(P, hv, t, r, m, kv, cpv)) {
+        atomicAdd(P.err_count, 1);
+        continue;
       }
+      const double tab[NO] = {t, r, m, kv, cpv};
+#pragma unroll
+      for (int q = 0; q < NO; ++q)
+        if (!(mask & (1u << q))) o[q] = tab[q];
     }
-    __syncthreads();
+    T[c] = o[0]; rho[c] = o[1]; mu[c] = o[2]; kk[c] = o[3];
+    if (cp) cp[c] = o[4];
   }
+  chapsim_mlp::cta_teardown(s);
 }
 
 // ------------------------------------------------------------ MLP training
@@ -350,12 +262,6 @@ __global__ void k_loss_sum(const double *lp, int nblk, int nsamp, double *out) {
   }
 }
 
-__global__ void k_to_bf16(const float *params, __nv_bfloat16 *w2b, __nv_bfloat16 *w3b) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t < NH * NH) w2b[t] = __float2bfloat16_rn(params[O_W2 + t]);
-  if (t < 8 * NH) w3b[t] = t < NO * NH ? __float2bfloat16_rn(params[O_W3 + t]) : __float2bfloat16_rn(0.f);
-}
-
 uint64_t splitmix64(uint64_t x) {
   x += 0x9E3779B97F4A7C15ull;
   x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -374,9 +280,12 @@ struct chapsim_props {
   std::vector<void *> allocs;
   PropsDev P{};
   float *params = nullptr, *adam_m = nullptr, *adam_v = nullptr, *grad = nullptr;
-  __nv_bfloat16 *w2b = nullptr, *w3b = nullptr;
-  int *gate = nullptr;
+  uint16_t *wt = nullptr;  // BF16 hi / lo weight tiles of layers 2 and 3 (tensor-core operands)
+  uint8_t *gate = nullptr;  // per h-bin output masks
   bool has_mlp = false;
+  // per-output results of the last gate call
+  int out_bins[NO] = {0, 0, 0, 0, 0};
+  double out_err[NO] = {0, 0, 0, 0, 0};
 };
 
 #define PCK(call)                                                       \
@@ -480,23 +389,30 @@ int chapsim_props_create(const double *H, const double *T, const double *D, cons
   pe->adam_v = (float *)p;
   if ((rc = palloc(pe, &p, NP * sizeof(float)))) goto fail;
   pe->grad = (float *)p;
-  if ((rc = palloc(pe, &p, NH * NH * sizeof(__nv_bfloat16)))) goto fail;
-  pe->w2b = (__nv_bfloat16 *)p;
-  if ((rc = palloc(pe, &p, 8 * NH * sizeof(__nv_bfloat16)))) goto fail;
-  pe->w3b = (__nv_bfloat16 *)p;
-  pe->P.params = pe->params;
-  pe->P.w2b = pe->w2b;
-  pe->P.w3b = pe->w3b;
-  pe->P.hmid = 0.5 * (H[0] + H[n - 1]);
-  pe->P.hhalf = 0.5 * (H[n - 1] - H[0]);
-  for (int o = 0; o < NO; ++o) { pe->P.mean[o] = 0.0; pe->P.stdv[o] = 1.0; }
-  pe->P.nbins = 1;
-  pe->P.g0 = H[0];
-  pe->P.ginv = 1.0 / (H[n - 1] - H[0]);
-  if ((rc = palloc(pe, &p, 4096 * sizeof(int)))) goto fail;
-  pe->gate = (int *)p;
-  pe->P.gate = pe->gate;
-  if (cudaMemset(pe->gate, 0, 4096 * sizeof(int)) != cudaSuccess) { rc = CHAPSIM_ERR_CUDA; goto fail; }
+  if ((rc = palloc(pe, &p, (2 * NH * NH + 2 * chapsim_mlp::NOP * NH) * sizeof(uint16_t)))) goto fail;
+  pe->wt = (uint16_t *)p;
+  if ((rc = palloc(pe, &p, chapsim_mlp::kMaxGateBins))) goto fail;
+  pe->gate = (uint8_t *)p;
+  if ((rc = palloc(pe, &p, sizeof(int)))) goto fail;
+  pe->P.dev_err = (int *)p;
+  if (cudaMemset(pe->P.dev_err, 0, sizeof(int)) != cudaSuccess) { rc = CHAPSIM_ERR_CUDA; goto fail; }
+  {
+    chapsim_mlp::MlpDev &M = pe->P.M;
+    M.par = pe->params;
+    M.wt = pe->wt;
+    M.gate = pe->gate;
+    M.hmid = 0.5 * (H[0] + H[n - 1]);
+    M.hhalf = 0.5 * (H[n - 1] - H[0]);
+    for (int o = 0; o < NO; ++o) {
+      M.mean[o] = 0.0;
+      M.stdv[o] = 1.0;
+      for (int q = 0; q < chapsim_mlp::NBASE; ++q) M.base[o][q] = 0.0;
+    }
+    M.nbins = 1;
+    M.g0 = H[0];
+    M.ginv = 1.0 / (H[n - 1] - H[0]);
+  }
+  if (cudaMemset(pe->gate, 0, chapsim_mlp::kMaxGateBins) != cudaSuccess) { rc = CHAPSIM_ERR_CUDA; goto fail; }
   if (cudaMemset(pe->params, 0, NP * sizeof(float)) != cudaSuccess) { rc = CHAPSIM_ERR_CUDA; goto fail; }
   *out = pe;
   return CHAPSIM_OK;
@@ -517,6 +433,8 @@ int chapsim_props_destroy(chapsim_props *pe) {
 
 const char *chapsim_props_last_error(const chapsim_props *pe) { return pe ? pe->err.c_str() : "null engine"; }
 
+static size_t mlp_smem() { return chapsim_mlp::kSmemBytes; }
+
 static int launch_update(chapsim_props *pe, int mode, const double *h, double *T, double *rho, double *mu, double *k,
                          double *cp, int64_t n) {
   if (n <= 0) return CHAPSIM_OK;
@@ -524,8 +442,12 @@ static int launch_update(chapsim_props *pe, int mode, const double *h, double *T
     const int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
     k_props_table<<<blocks, 256, 0, pe->stream>>>(pe->P, h, T, rho, mu, k, cp, n);
   } else {
-    const int blocks = (int)std::min<int64_t>((n + MI_CELLS - 1) / MI_CELLS, 148 * 32);
-    k_props_mlp<<<blocks, MI_WARPS * 32, 0, pe->stream>>>(pe->P, h, T, rho, mu, k, cp, n);
+    PCK(cudaFuncSetAttribute(k_props_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp_smem()));
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, pe->device);
+    const int64_t tiles = (n + chapsim_mlp::TILE - 1) / chapsim_mlp::TILE;
+    const int blocks = (int)std::min<int64_t>(tiles, (int64_t)nsm * 4);
+    k_props_mlp_tc<<<blocks, chapsim_mlp::TILE, mlp_smem(), pe->stream>>>(pe->P, h, T, rho, mu, k, cp, n);
   }
   PCK(cudaGetLastError());
   return CHAPSIM_OK;
@@ -543,9 +465,15 @@ int chapsim_props_update(chapsim_props *pe, int mode, const double *h, double *T
   PCK(cudaMemsetAsync(pe->P.err_count, 0, sizeof(int), pe->stream));
   int rc = launch_update(pe, mode, h, T, rho, mu, k, cp, n);
   if (rc) return rc;
-  int bad = 0;
+  int bad = 0, werr = 0;
   PCK(cudaMemcpyAsync(&bad, pe->P.err_count, sizeof(int), cudaMemcpyDeviceToHost, pe->stream));
+  PCK(cudaMemcpyAsync(&werr, pe->P.dev_err, sizeof(int), cudaMemcpyDeviceToHost, pe->stream));
   PCK(cudaStreamSynchronize(pe->stream));
+  if (werr) {
+    PCK(cudaMemsetAsync(pe->P.dev_err, 0, sizeof(int), pe->stream));
+    pe->err = "tensor-core inference: a device-side wait gave up";
+    return CHAPSIM_ERR_CUDA;
+  }
   if (n_out_of_range) *n_out_of_range = bad;
   if (bad) {
     pe->err = std::to_string(bad) + " cells outside the property table (left unchanged)";
@@ -554,10 +482,55 @@ int chapsim_props_update(chapsim_props *pe, int mode, const double *h, double *T
   return CHAPSIM_OK;
 }
 
-static int refresh_bf16(chapsim_props *pe) {
-  k_to_bf16<<<(NH * NH + 255) / 256, 256, 0, pe->stream>>>(pe->params, pe->w2b, pe->w3b);
-  PCK(cudaGetLastError());
+// Rebuild the tensor-core weight tiles (BF16 hi / lo of W2 and W3 in the
+// canonical operand layout) from the FP32 parameters on the device.
+static int refresh_tiles(chapsim_props *pe) {
+  std::vector<float> par(NP);
+  PCK(cudaMemcpyAsync(par.data(), pe->params, NP * sizeof(float), cudaMemcpyDeviceToHost, pe->stream));
+  PCK(cudaStreamSynchronize(pe->stream));
+  std::vector<uint16_t> t(2 * NH * NH + 2 * chapsim_mlp::NOP * NH);
+  chapsim_mlp::build_weight_tiles(par.data(), t.data());
+  PCK(cudaMemcpyAsync(pe->wt, t.data(), t.size() * sizeof(uint16_t), cudaMemcpyHostToDevice, pe->stream));
+  PCK(cudaStreamSynchronize(pe->stream));
   return CHAPSIM_OK;
+}
+
+// Least-squares polynomial of degree NBASE-1 in x through (x_s, y_s):
+// normal equations in FP64, solved by Gaussian elimination with partial
+// pivoting (6 x 6, x in [-1, 1]).
+static void poly_fit(const std::vector<double> &x, const double *y, double *coef) {
+  constexpr int nb = chapsim_mlp::NBASE;
+  double A[nb][nb + 1] = {};
+  for (size_t s = 0; s < x.size(); ++s) {
+    double pw[nb];
+    pw[0] = 1.0;
+    for (int q = 1; q < nb; ++q) pw[q] = pw[q - 1] * x[s];
+    for (int r = 0; r < nb; ++r) {
+      for (int q = 0; q < nb; ++q) A[r][q] += pw[r] * pw[q];
+      A[r][nb] += pw[r] * y[s];
+    }
+  }
+  for (int c = 0; c < nb; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < nb; ++r)
+      if (fabs(A[r][c]) > fabs(A[piv][c])) piv = r;
+    for (int q = 0; q <= nb; ++q) std::swap(A[c][q], A[piv][q]);
+    for (int r = c + 1; r < nb; ++r) {
+      const double f = A[r][c] / A[c][c];
+      for (int q = c; q <= nb; ++q) A[r][q] -= f * A[c][q];
+    }
+  }
+  for (int r = nb - 1; r >= 0; --r) {
+    double v = A[r][nb];
+    for (int q = r + 1; q < nb; ++q) v -= A[r][q] * coef[q];
+    coef[r] = v / A[r][r];
+  }
+}
+
+static double poly_at(const double *coef, double x) {
+  double b = coef[chapsim_mlp::NBASE - 1];
+  for (int q = chapsim_mlp::NBASE - 2; q >= 0; --q) b = b * x + coef[q];
+  return b;
 }
 
 static size_t grad_smem() { return (size_t)(2 * TR_S * (NH + 1) + TR_S * NO + NP + TR_S) * sizeof(float); }
@@ -611,20 +584,29 @@ int chapsim_props_train(chapsim_props *pe, int nsamples, uint64_t seed, int step
   std::vector<double> tgt((size_t)nsamples * NO);
   cudaMemcpyAsync(tgt.data(), dout, tgt.size() * sizeof(double), cudaMemcpyDeviceToHost, pe->stream);
   cudaStreamSynchronize(pe->stream);
-  // standardisation
+  // residual targets: a least-squares degree-5 polynomial in x per output,
+  // then the residual standardised (mean, std)
+  chapsim_mlp::MlpDev &M = pe->P.M;
+  std::vector<double> xs(nsamples);
+  for (int s = 0; s < nsamples; ++s) xs[s] = (hs[s] - M.hmid) / M.hhalf;
   for (int o = 0; o < NO; ++o) {
+    double *y = tgt.data() + (size_t)o * nsamples;
+    poly_fit(xs, y, M.base[o]);
     double m = 0.0, v = 0.0;
-    for (int s = 0; s < nsamples; ++s) m += tgt[(size_t)o * nsamples + s];
+    for (int s = 0; s < nsamples; ++s) {
+      y[s] -= poly_at(M.base[o], xs[s]);
+      m += y[s];
+    }
     m /= nsamples;
-    for (int s = 0; s < nsamples; ++s) { const double e = tgt[(size_t)o * nsamples + s] - m; v += e * e; }
-    pe->P.mean[o] = m;
-    pe->P.stdv[o] = sqrt(v / nsamples) + 1e-12;
+    for (int s = 0; s < nsamples; ++s) { const double e = y[s] - m; v += e * e; }
+    M.mean[o] = m;
+    M.stdv[o] = sqrt(v / nsamples) + 1e-12;
   }
   std::vector<float> xf(nsamples), tf((size_t)nsamples * NO);
   for (int s = 0; s < nsamples; ++s) {
-    xf[s] = (float)((hs[s] - pe->P.hmid) / pe->P.hhalf);
+    xf[s] = (float)xs[s];
     for (int o = 0; o < NO; ++o)
-      tf[(size_t)s * NO + o] = (float)((tgt[(size_t)o * nsamples + s] - pe->P.mean[o]) / pe->P.stdv[o]);
+      tf[(size_t)s * NO + o] = (float)((tgt[(size_t)o * nsamples + s] - M.mean[o]) / M.stdv[o]);
   }
   // Xavier-style seeded init
   std::vector<float> w(NP, 0.f);
@@ -661,14 +643,14 @@ int chapsim_props_train(chapsim_props *pe, int nsamples, uint64_t seed, int step
   PCK(cudaStreamSynchronize(pe->stream));
   cleanup();
   if (final_loss) *final_loss = l;
-  rc = refresh_bf16(pe);
+  rc = refresh_tiles(pe);
   if (rc) return rc;
   pe->has_mlp = true;
   return CHAPSIM_OK;
 }
 
 int chapsim_props_gate(chapsim_props *pe, double tol, int nbins, int *n_mlp_bins, double *max_rel_err) {
-  if (!pe || nbins < 1 || nbins > 4096 || !(tol >= 0)) return CHAPSIM_ERR_ARG;
+  if (!pe || nbins < 1 || nbins > chapsim_mlp::kMaxGateBins || !(tol >= 0)) return CHAPSIM_ERR_ARG;
   if (!pe->has_mlp) { pe->err = "no trained model"; return CHAPSIM_ERR_STATE; }
   PCK(cudaSetDevice(pe->device));
   const int n = pe->n;
@@ -688,72 +670,107 @@ int chapsim_props_gate(chapsim_props *pe, double tol, int nbins, int *n_mlp_bins
     return CHAPSIM_ERR_NOMEM;
   }
   cudaMemcpy(dh, hs.data(), m * sizeof(double), cudaMemcpyHostToDevice);
-  // all bins on the MLP for the measurement
-  std::vector<int> ones(4096, 1);
-  cudaMemcpy(pe->gate, ones.data(), 4096 * sizeof(int), cudaMemcpyHostToDevice);
-  pe->P.nbins = 1;
+  // every output of every bin on the model for the measurement
+  std::vector<uint8_t> all(chapsim_mlp::kMaxGateBins, 0x1F);
+  cudaMemcpy(pe->gate, all.data(), all.size(), cudaMemcpyHostToDevice);
+  pe->P.M.nbins = 1;
   cudaMemsetAsync(pe->P.err_count, 0, sizeof(int), pe->stream);
   int rc = launch_update(pe, CHAPSIM_PROPS_TABLE, dh, da, da + m, da + 2 * m, da + 3 * m, da + 4 * m, m);
   if (!rc) rc = launch_update(pe, CHAPSIM_PROPS_MLP, dh, db, db + m, db + 2 * m, db + 3 * m, db + 4 * m, m);
   std::vector<double> A(m * NO), B(m * NO);
+  int werr = 0;
   cudaMemcpyAsync(A.data(), da, A.size() * sizeof(double), cudaMemcpyDeviceToHost, pe->stream);
   cudaMemcpyAsync(B.data(), db, B.size() * sizeof(double), cudaMemcpyDeviceToHost, pe->stream);
+  cudaMemcpyAsync(&werr, pe->P.dev_err, sizeof(int), cudaMemcpyDeviceToHost, pe->stream);
   cudaStreamSynchronize(pe->stream);
   cudaFree(dh); cudaFree(da); cudaFree(db);
   if (rc) return rc;
+  if (werr) {
+    cudaMemsetAsync(pe->P.dev_err, 0, sizeof(int), pe->stream);
+    pe->err = "tensor-core inference: a device-side wait gave up";
+    return CHAPSIM_ERR_CUDA;
+  }
+  // error of each output relative to its largest magnitude over the table
   double scale[NO];
   for (int o = 0; o < NO; ++o) {
     scale[o] = 0.0;
     for (int64_t s = 0; s < m; ++s) scale[o] = fmax(scale[o], fabs(A[o * m + s]));
     scale[o] = scale[o] > 0 ? scale[o] : 1.0;
   }
-  std::vector<double> binerr(nbins, 0.0);
+  std::vector<double> binerr((size_t)nbins * NO, 0.0);
   const double g0 = pe->H[0], ginv = nbins / (pe->H[n - 1] - pe->H[0]);
-  double worst = 0.0;
+  for (int o = 0; o < NO; ++o) pe->out_err[o] = 0.0;
   for (int64_t s = 0; s < m; ++s) {
     int b = (int)((hs[s] - g0) * ginv);
     b = b < 0 ? 0 : (b >= nbins ? nbins - 1 : b);
     for (int o = 0; o < NO; ++o) {
       const double e = fabs(B[o * m + s] - A[o * m + s]) / scale[o];
-      binerr[b] = fmax(binerr[b], e);
-      worst = fmax(worst, e);
+      binerr[(size_t)b * NO + o] = fmax(binerr[(size_t)b * NO + o], e);
+      pe->out_err[o] = fmax(pe->out_err[o], e);
     }
   }
-  std::vector<int> flags(4096, 0);
+  std::vector<uint8_t> flags(chapsim_mlp::kMaxGateBins, 0);
   int cnt = 0;
+  for (int o = 0; o < NO; ++o) pe->out_bins[o] = 0;
   for (int b = 0; b < nbins; ++b) {
-    flags[b] = binerr[b] <= tol ? 1 : 0;
-    cnt += flags[b];
+    unsigned mask = 0;
+    for (int o = 0; o < NO; ++o)
+      if (binerr[(size_t)b * NO + o] <= tol) {
+        mask |= 1u << o;
+        ++pe->out_bins[o];
+      }
+    flags[b] = (uint8_t)mask;
+    cnt += (mask & chapsim_mlp::kStepMask) == chapsim_mlp::kStepMask;
   }
-  cudaMemcpy(pe->gate, flags.data(), 4096 * sizeof(int), cudaMemcpyHostToDevice);
-  pe->P.nbins = nbins;
-  pe->P.g0 = g0;
-  pe->P.ginv = ginv;
+  cudaMemcpy(pe->gate, flags.data(), flags.size(), cudaMemcpyHostToDevice);
+  pe->P.M.nbins = nbins;
+  pe->P.M.g0 = g0;
+  pe->P.M.ginv = ginv;
+  double worst = 0.0;
+  for (int o = 0; o < 4; ++o) worst = fmax(worst, pe->out_err[o]);
   if (n_mlp_bins) *n_mlp_bins = cnt;
   if (max_rel_err) *max_rel_err = worst;
   return CHAPSIM_OK;
 }
 
+int chapsim_props_gate_outputs(const chapsim_props *pe, int *bins, double *max_rel_err, int n) {
+  if (!pe || !bins || !max_rel_err || n != NO) return CHAPSIM_ERR_ARG;
+  for (int o = 0; o < NO; ++o) {
+    bins[o] = pe->out_bins[o];
+    max_rel_err[o] = pe->out_err[o];
+  }
+  return CHAPSIM_OK;
+}
+
 int chapsim_props_get_params(const chapsim_props *pe, float *params, int nparams, double *norm, int nnorm) {
-  if (!pe || !params || nparams != NP || !norm || nnorm != 2 + 2 * NO) return CHAPSIM_ERR_ARG;
+  if (!pe || !params || nparams != NP || !norm || nnorm != NNORM) return CHAPSIM_ERR_ARG;
   cudaSetDevice(pe->device);
   if (cudaMemcpy(params, pe->params, NP * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess) return CHAPSIM_ERR_CUDA;
-  norm[0] = pe->P.hmid;
-  norm[1] = pe->P.hhalf;
-  for (int o = 0; o < NO; ++o) { norm[2 + o] = pe->P.mean[o]; norm[2 + NO + o] = pe->P.stdv[o]; }
+  const chapsim_mlp::MlpDev &M = pe->P.M;
+  norm[0] = M.hmid;
+  norm[1] = M.hhalf;
+  for (int o = 0; o < NO; ++o) {
+    norm[2 + o] = M.mean[o];
+    norm[2 + NO + o] = M.stdv[o];
+    for (int q = 0; q < chapsim_mlp::NBASE; ++q) norm[2 + 2 * NO + o * chapsim_mlp::NBASE + q] = M.base[o][q];
+  }
   return CHAPSIM_OK;
 }
 
 int chapsim_props_set_params(chapsim_props *pe, const float *params, int nparams, const double *norm, int nnorm) {
-  if (!pe || !params || nparams != NP || !norm || nnorm != 2 + 2 * NO) return CHAPSIM_ERR_ARG;
+  if (!pe || !params || nparams != NP || !norm || nnorm != NNORM) return CHAPSIM_ERR_ARG;
   PCK(cudaSetDevice(pe->device));
   PCK(cudaMemcpy(pe->params, params, NP * sizeof(float), cudaMemcpyHostToDevice));
-  pe->P.hmid = norm[0];
-  pe->P.hhalf = norm[1];
-  for (int o = 0; o < NO; ++o) { pe->P.mean[o] = norm[2 + o]; pe->P.stdv[o] = norm[2 + NO + o]; }
-  int rc = refresh_bf16(pe);
+  chapsim_mlp::MlpDev &M = pe->P.M;
+  M.hmid = norm[0];
+  M.hhalf = norm[1];
+  for (int o = 0; o < NO; ++o) {
+    M.mean[o] = norm[2 + o];
+    M.stdv[o] = norm[2 + NO + o];
+    for (int q = 0; q < chapsim_mlp::NBASE; ++q) M.base[o][q] = norm[2 + 2 * NO + o * chapsim_mlp::NBASE + q];
+  }
+  int rc = refresh_tiles(pe);
   if (rc) return rc;
-  PCK(cudaStreamSynchronize(pe->stream));
   pe->has_mlp = true;
   return CHAPSIM_OK;
 }
@@ -786,3 +803,26 @@ int chapsim_props_loss_grad(chapsim_props *pe, const float *x, const float *t, i
 }
 
 }  // extern "C"
+
+namespace chapsim {
+
+// The trained model of an engine, for a context that evaluates it in its own
+// kernels (chapsim_set_props_mode): FP32 parameters, weight tiles, gate
+// masks and the normalisation.  Device pointers stay owned by the engine.
+int props_model(const chapsim_props *pe, chapsim_mlp::MlpDev *out, int *device) {
+  if (!pe || !out) return CHAPSIM_ERR_ARG;
+  if (!pe->has_mlp) return CHAPSIM_ERR_STATE;
+  *out = pe->P.M;
+  if (device) *device = pe->device;
+  return CHAPSIM_OK;
+}
+
+// True when the engine was built on the table columns H, T, D, M, K given.
+bool props_same_table(const chapsim_props *pe, const std::vector<double> *cols5) {
+  const std::vector<double> *mine[5] = {&pe->H, &pe->T, &pe->D, &pe->M, &pe->K};
+  for (int q = 0; q < 5; ++q)
+    if (*mine[q] != cols5[q]) return false;
+  return true;
+}
+
+}  // namespace chapsim

@@ -84,6 +84,16 @@ class IOChannel(TGChannel):
         self._chk(self.lib.chapsim_set_table(self.h, *[c.ctypes.data for c in cols], len(cols[0]),
                                              1 if shortcuts else 0))
 
+    def set_props_mode(self, mode, engine=None):
+        """Property evaluation of the energy substep: _lib.PROPS_TABLE (table
+        splines) or _lib.PROPS_MLP with a trained, gated PropertyEngine on the
+        same table (its model is copied into the context)."""
+        self._chk(self.lib.chapsim_set_props_mode(self.h, mode, engine.h if engine is not None else None))
+
+    def therm_prop_update(self, mode=0, iregion=0):
+        """THERM_PROP_UPDATE(IREGION) on the interior: h -> T, mu, k, rho."""
+        self._chk(self.lib.chapsim_therm_prop_update(self.h, iregion, mode))
+
     # ------------------------------------------------------ reference entries
     def random_fl_theml_fld_io(self, seed=0, amp=0.1, project=True):
         self._chk(self.lib.chapsim_init_random(self.h, seed, amp, 1 if project else 0))

@@ -19,7 +19,8 @@ from . import _lib
 from .solver import ChapsimError
 
 NPARAM = 64 + 64 + 64 * 64 + 64 + 5 * 64 + 5
-NNORM = 12
+NBASE = 6  # the model's polynomial base per output: degree 5 in x = (h - hmid) / hhalf
+NNORM = 2 + 2 * 5 + 5 * NBASE  # hmid, hhalf, mean[5], std[5], base[5][6]
 
 
 def synthetic_table(n=4096):
@@ -87,16 +88,26 @@ class PropertyEngine:
         return self.update_device(mode, h.data_ptr(), T.data_ptr(), rho.data_ptr(), mu.data_ptr(), k.data_ptr(),
                                   cp.data_ptr() if cp is not None else None, h.numel(), raise_on_range)
 
-    def train(self, nsamples=65536, seed=2, steps=4000, lr=3e-3):
+    def train(self, nsamples=65536, seed=2, steps=20000, lr=3e-3):
         loss = ctypes.c_double()
         self._chk(self.lib.chapsim_props_train(self.h, nsamples, seed, steps, lr, ctypes.byref(loss)))
         return loss.value
 
     def gate(self, tol=1e-4, nbins=256):
+        """Judge the model per h-bin and output against the table; returns the
+        number of bins where T, rho, mu and k all pass and their worst error."""
         nb = ctypes.c_int()
         worst = ctypes.c_double()
         self._chk(self.lib.chapsim_props_gate(self.h, tol, nbins, ctypes.byref(nb), ctypes.byref(worst)))
         return nb.value, worst.value
+
+    def gate_outputs(self):
+        """Per output (T, rho, mu, k, cp) of the last gate call: bins passing
+        and worst relative error."""
+        bins = (ctypes.c_int * 5)()
+        errs = (ctypes.c_double * 5)()
+        self._chk(self.lib.chapsim_props_gate_outputs(self.h, bins, errs, 5))
+        return list(bins), list(errs)
 
     def get_params(self):
         p = np.zeros(NPARAM, dtype=np.float32)

@@ -113,6 +113,7 @@ typedef struct chapsim_config {
 } chapsim_config;
 
 typedef struct chapsim_ctx chapsim_ctx;
+typedef struct chapsim_props chapsim_props; /* property engine (declared below) */
 
 /* Fill *cfg with defaults (64^3, Lx=4pi, Lz=4pi/3, beta=2, Re=2800, dt=1e-3,
  * constant mass flux, FP64, device 0). */
@@ -403,6 +404,35 @@ int chapsim_create_io(const chapsim_config *cfg, const chapsim_io_config *io, ch
 int chapsim_set_table(chapsim_ctx *ctx, const double *H, const double *T, const double *D, const double *M,
                       const double *K, int n, int shortcuts);
 
+#define CHAPSIM_PROPS_TABLE 0 /* cubic splines, as THERM_PROP_UPDATE                */
+#define CHAPSIM_PROPS_MLP 1   /* learned model on the tensor cores (BF16 operands, FP32
+                                 accumulation) where the error gate allows it, table
+                                 splines elsewhere                                   */
+/* Property evaluation of an IO context (the THERM_PROP_UPDATE of
+ * src/THERM_PROP_UPDATE.f90:129-205 with its DENSITY_UPDATE / ENTHALPY_UPDATE
+ * companions, as SOLVERRK3_ENG_IO calls them, src/SOLVERRK3_ENG_IO.f90:46-55).
+ * mode CHAPSIM_PROPS_TABLE: the table splines (the default, and the state
+ * after chapsim_set_table).  mode CHAPSIM_PROPS_MLP: the learned model of the
+ * engine pe (trained on the same table and gated by chapsim_props_gate; see
+ * the property engine below), copied into the context, so pe may be
+ * destroyed afterwards; the energy substep then evaluates the model on the
+ * tensor cores and takes the table splines in every h-bin the gate has not
+ * cleared for T, rho, mu and k.  The wall ghost rows (BC_WALL_ISOFLUX) keep
+ * the table splines.  pe is ignored for the table mode. */
+int chapsim_set_props_mode(chapsim_ctx *ctx, int mode, const chapsim_props *pe);
+/* THERM_PROP_UPDATE(IREGION) on an IO context: h -> T, mu, k, rho on the
+ * interior rows by the table (mode CHAPSIM_PROPS_TABLE) or the context's
+ * model (CHAPSIM_PROPS_MLP, after chapsim_set_props_mode); cells with
+ * |h| < 1e-10 keep their properties when the table keeps the reference
+ * shortcuts; out-of-table cells are counted (CHAPSIM_R_BADCELLS).  Regions:
+ * the reference's IMAIND (0) and IALLDM (2), which coincide on an IO
+ * context; IOULET (1), the outlet plane, is updated by
+ * chapsim_io_bc_outlet_eng. */
+#define CHAPSIM_IMAIND 0
+#define CHAPSIM_IOULET 1
+#define CHAPSIM_IALLDM 2
+int chapsim_therm_prop_update(chapsim_ctx *ctx, int iregion, int mode);
+
 /* SOLVERRK3_ENG_IO(NS) (src/SOLVERRK3_ENG_IO.f90:1-77): energy RHS, rho h
  * update with the RHOHmax limiter, ENTHALPY/DENSITY_UPDATE,
  * THERM_PROP_UPDATE and the iso-flux wall ghosts. */
@@ -424,16 +454,12 @@ int chapsim_step_io(chapsim_ctx *ctx, int nsteps);
  * NIST_H, NIST_T, NIST_D, NIST_M, NIST_K, NIST_CP of the reference's
  * thermal_info module after NIST_TABLE_SCALING, src/Flow_State.f90:394-433),
  * its cubic splines (NIST_SPLINE_H / NIST_SPLINE_T, src/Flow_State.f90:916,
- * 1296, coefficients by CUBIC_SPLINE :1693-1787) and, optionally, a trained
- * MLP h -> (T, rho, mu, k, cp) of shape 1 -> 64 -> 64 -> 5 (tanh), which has
- * no counterpart in the reference.
+ * 1296, coefficients by CUBIC_SPLINE :1693-1787) and, optionally, a learned
+ * model h -> (T, rho, mu, k, cp), which has no counterpart in the reference:
+ * per output a least-squares polynomial of degree 5 in x = (h - hmid) / hhalf
+ * plus an MLP 1 -> 64 -> 64 -> 5 (tanh) for the standardised residual,
+ *   out_o = base_o(x) + mean_o + std_o * MLP(x)_o.
  * ====================================================================== */
-typedef struct chapsim_props chapsim_props;
-
-/* property evaluation modes */
-#define CHAPSIM_PROPS_TABLE 0 /* cubic splines, as THERM_PROP_UPDATE          */
-#define CHAPSIM_PROPS_MLP 1   /* MLP (BF16 weights, FP32 accumulation) where the
-                                 error gate allows it, table splines elsewhere */
 
 /* Build the engine from n >= 4 strictly increasing H (with T increasing too).
  * Columns are host arrays of length n. */
@@ -448,29 +474,38 @@ const char *chapsim_props_last_error(const chapsim_props *pe);
  * h or T lies outside the table are left unchanged and counted (the
  * reference STOPs there): the call then returns CHAPSIM_ERR_RANGE and
  * *n_out_of_range holds the count.  cp may be NULL; when given it receives
- * cp(h) (spline in h, NIST_HCP).  Work runs on the engine's stream and the
+ * cp(h) (spline in h, NIST_HCP).  With mode CHAPSIM_PROPS_MLP each output
+ * comes from the learned model where the gate cleared it for the cell's h-bin
+ * and from the splines elsewhere.  Work runs on the engine's stream and the
  * call synchronises. */
 #define CHAPSIM_ERR_RANGE 8
 int chapsim_props_update(chapsim_props *pe, int mode, const double *h, double *T, double *rho, double *mu,
                          double *k, double *cp, int64_t n, int64_t *n_out_of_range);
 
-/* Train the MLP on the GPU (project-written forward, backward and Adam
- * kernels, FP32) on nsamples table samples drawn uniformly in h from seed:
- * full-batch Adam for `steps` steps, learning rate lr decayed by cosine to
- * lr/100.  *final_loss receives the last mean-squared error of the
- * standardised outputs. */
+/* Train the model on the GPU on nsamples table samples drawn uniformly in h
+ * from seed: the polynomial base by least squares (host, FP64), then the MLP
+ * on the standardised residual by the project's own forward, backward and
+ * Adam kernels (FP32): full-batch Adam for `steps` steps, learning rate lr
+ * decayed by cosine to lr/100.  *final_loss receives the last mean-squared
+ * error of the standardised residuals. */
 int chapsim_props_train(chapsim_props *pe, int nsamples, uint64_t seed, int steps, double lr, double *final_loss);
 
-/* Error gate: evaluate MLP (inference precision) and table on a dense h grid,
- * split [H_1, H_n] into nbins bins, and allow the MLP in a bin only where its
- * largest error over T, rho, mu, k, cp, relative to each output's largest
- * magnitude over the table, is <= tol.  Returns the number of MLP bins and
- * the worst relative error seen. */
+/* Error gate: evaluate the model (the tensor-core inference) and the table
+ * splines on 8 points per table interval, split [H_1, H_n] into nbins bins
+ * (<= 4096), and clear output o of bin b for the model when its largest
+ * error there, relative to the output's largest magnitude over the table, is
+ * <= tol; uncleared outputs come from the table.  Returns the number of bins
+ * cleared for all of T, rho, mu and k (the outputs THERM_PROP_UPDATE
+ * produces) and the worst error of those four.
+ * chapsim_props_gate_outputs reports, for the last gate call and each output
+ * (T, rho, mu, k, cp), the bins cleared and the worst error (n = 5). */
 int chapsim_props_gate(chapsim_props *pe, double tol, int nbins, int *n_mlp_bins, double *max_rel_err);
+int chapsim_props_gate_outputs(const chapsim_props *pe, int *bins, double *max_rel_err, int n);
 
-/* MLP parameters (float32, 4613 values: W1[64] b1[64] W2[64][64] b2[64]
- * W3[5][64] b3[5]) and the input/output normalisation (h_mid, h_half, then
- * mean[5], std[5]). */
+/* Model parameters (float32, 4613 values: W1[64] b1[64] W2[64][64] b2[64]
+ * W3[5][64] b3[5]) and its normalisation (42 values: hmid, hhalf, then
+ * mean[5], std[5], base[5][6], the polynomial coefficients of each output in
+ * powers of x, lowest first). */
 int chapsim_props_get_params(const chapsim_props *pe, float *params, int nparams, double *norm, int nnorm);
 int chapsim_props_set_params(chapsim_props *pe, const float *params, int nparams, const double *norm, int nnorm);
 

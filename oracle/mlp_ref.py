@@ -7,8 +7,11 @@ reference; it stands in for the table interpolation of THERM_PROP_UPDATE
 
 Parameter vector layout (float32 on the device, 4613 values):
   W1[64] b1[64] W2[64][64] (row = output unit) b2[64] W3[5][64] b3[5]
-Input x = (h - h_mid) / h_half; outputs are the standardised targets
-(T, rho, mu, k, cp); loss = mean over samples and outputs of (y - t)^2.
+Input x = (h - h_mid) / h_half; outputs are the standardised residual
+targets of (T, rho, mu, k, cp) over a least-squares degree-5 polynomial base
+per output; loss = mean over samples and outputs of (y - t)^2.  The
+normalisation vector is hmid, hhalf, mean[5], std[5], base[5][6] (powers of
+x, lowest first), and the property is base_o(x) + mean_o + std_o * y_o.
 """
 import numpy as np
 
@@ -51,3 +54,20 @@ def loss_and_grad(p, x, t):
     gW1 = d1.T @ x
     gb1 = d1.sum(0)
     return loss, np.concatenate([gW1, gb1, gW2.ravel(), gb2, gW3.ravel(), gb3])
+
+
+NBASE = 6
+
+
+def properties(p, norm, h):
+    """FP64 model output (T, rho, mu, k, cp) at enthalpies h: polynomial base
+    plus the de-standardised network residual."""
+    norm = np.asarray(norm, dtype=np.float64)
+    x = (np.asarray(h, dtype=np.float64) - norm[0]) / norm[1]
+    y, _ = forward(p, x)
+    mean, std = norm[2:2 + NO], norm[2 + NO:2 + 2 * NO]
+    base = norm[2 + 2 * NO:].reshape(NO, NBASE)
+    out = np.empty((len(x), NO))
+    for o in range(NO):
+        out[:, o] = np.polynomial.polynomial.polyval(x, base[o]) + mean[o] + std[o] * y[:, o]
+    return out

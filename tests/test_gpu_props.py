@@ -1,7 +1,9 @@
 """GPU tests of the property engine: table splines (THERM_PROP_UPDATE)
 against the FP64 oracle, the MLP training kernels' loss and gradient against
-the FP64 numpy reference, training convergence, the BF16 tensor-core
-inference, the error gate and the out-of-table error path."""
+the FP64 numpy reference, training convergence, the tcgen05 tensor-core
+inference (BF16 hi/lo operands, FP32 accumulation) against the FP64 forward
+of the same parameters, the per-bin error gate at its 1e-4 bound, and the
+out-of-table error path."""
 import ctypes
 
 import numpy as np
@@ -75,7 +77,7 @@ def test_loss_and_gradient_match_fp64_reference(engine):
     from oracle import mlp_ref
     rng = np.random.default_rng(7)
     p = rng.normal(0, 0.3, mlp_ref.NPARAM).astype(np.float32)
-    norm = np.array([0.0, 1.0] + [0.0] * 5 + [1.0] * 5)
+    norm = np.array([0.0, 1.0] + [0.0] * 5 + [1.0] * 5 + [0.0] * 30)
     engine.set_params(p, norm)
     x = rng.uniform(-1, 1, 300).astype(np.float32)
     t = rng.normal(0, 1, (300, 5)).astype(np.float32)
@@ -86,30 +88,56 @@ def test_loss_and_gradient_match_fp64_reference(engine):
     assert np.abs(g - gr).max() <= 1e-3 * np.abs(gr).max()
 
 
-def test_training_and_tensor_core_inference(engine, table):
+def test_tensor_core_inference_matches_fp64_forward(engine):
+    """Random parameters and base: the tcgen05 kernel (every bin on the
+    model) against the FP64 forward.  A layout or descriptor error gives O(1)
+    differences; the split operands and tanh.approx.f32 leave about 1e-5."""
     import torch
     from oracle import mlp_ref
-    loss = engine.train(nsamples=65536, seed=2, steps=1500, lr=3e-3)
-    assert loss < 2e-3, loss
-    p, norm = engine.get_params()
-    rng = np.random.default_rng(11)
-    h = rng.uniform(-0.999, 0.999, 4096)
-    # MLP everywhere (gate with an infinite bound), compare with the FP64 forward
-    nb, worst = engine.gate(tol=1e9, nbins=64)
+    rng = np.random.default_rng(17)
+    p = rng.normal(0, 0.3, mlp_ref.NPARAM).astype(np.float32)
+    base = rng.normal(0, 0.5, (5, 6))
+    norm = np.concatenate([[0.0, 1.0], rng.normal(0, 0.2, 5), np.full(5, 0.05), base.ravel()])
+    engine.set_params(p, norm)
+    nb, _ = engine.gate(tol=1e9, nbins=64)
     assert nb == 64
+    h = rng.uniform(-0.999, 0.999, 5000)  # a partial last tile (5000 = 39 x 128 + 8)
     hd = torch.tensor(h, dtype=torch.float64, device="cuda")
-    outs = [torch.zeros(4096, dtype=torch.float64, device="cuda") for _ in range(5)]
+    outs = [torch.zeros(len(h), dtype=torch.float64, device="cuda") for _ in range(5)]
     engine.update(hd, *outs[:4], cp=outs[4], mode=1)
-    y, _ = mlp_ref.forward(p.astype(np.float64), (h - norm[0]) / norm[1])
-    ref = y * norm[7:12] + norm[2:7]
+    ref = mlp_ref.properties(p.astype(np.float64), norm, h)
     for o in range(5):
         got = outs[o].cpu().numpy()
-        assert np.abs(got - ref[:, o]).max() <= 3e-2 * np.abs(ref[:, o]).max(), o  # BF16 weights/activations
-    # gate with a zero bound: every bin falls back to the table splines
+        err = np.abs(got - ref[:, o]).max() / np.abs(ref[:, o]).max()
+        assert err <= 1e-4, (o, err)
+
+
+def test_training_gate_and_fallback(engine, table):
+    """Training on 65,536 table samples (seed 2) reaches the 1e-4 bound (error
+    relative to each output's largest magnitude over the table) in at least
+    200 of 256 h-bins for T, rho, mu and k, the outputs THERM_PROP_UPDATE
+    produces; at random points the gated update stays within 2e-4 of the
+    table (the gate samples 128 points per bin)."""
+    import torch
+    loss = engine.train(nsamples=65536, seed=2, steps=20000, lr=3e-3)
+    nb, worst = engine.gate(tol=1e-4, nbins=256)
+    bins, errs = engine.gate_outputs()
+    print(f"trained: loss {loss:.3e}, bins passing (T, rho, mu, k) {nb}/256, per output {bins}, "
+          f"worst per output {['%.2e' % e for e in errs]}")
+    assert nb >= 200, (nb, bins, errs)
+    rng = np.random.default_rng(11)
+    h = rng.uniform(-0.999, 0.999, 100_000)
+    hd = torch.tensor(h, dtype=torch.float64, device="cuda")
+    got = [torch.zeros(len(h), dtype=torch.float64, device="cuda") for _ in range(4)]
+    tab = [torch.zeros(len(h), dtype=torch.float64, device="cuda") for _ in range(4)]
+    engine.update(hd, *got, mode=1)
+    engine.update(hd, *tab)
+    for o in range(4):
+        a, b = got[o].cpu().numpy(), tab[o].cpu().numpy()
+        assert np.abs(a - b).max() <= 2e-4 * np.abs(b).max(), o
+    # gate with a zero bound: every bin falls back to the table splines, bitwise
     nb, _ = engine.gate(tol=0.0, nbins=64)
     assert nb == 0
-    tab = [torch.zeros(4096, dtype=torch.float64, device="cuda") for _ in range(4)]
-    engine.update(hd, *tab)
-    engine.update(hd, *outs[:4], mode=1)
-    for a, b in zip(outs[:4], tab):
+    engine.update(hd, *got, mode=1)
+    for a, b in zip(got, tab):
         assert torch.equal(a, b)
