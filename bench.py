@@ -57,6 +57,12 @@ WORKLOADS = {
     # the same channel with the semi-implicit viscous scheme (visthemflg = 1)
     "io_384x192x192_si": dict(io=True, nx=384, ny=192, nz=192, lx=8 * math.pi, lz=4 * math.pi / 3, ren=2800.0,
                               dt=1e-3, seed=2, thermal=1, prt=0.71, qw=1.0, table="synthetic", visc_scheme=1),
+    # the metric's comparison on the large single domain: the mixed precision
+    # form with the learned property model against the plain FP64 form with
+    # the table splines, both on io_1024x384x512 (201 M cells)
+    "c4_mixed_learned": dict(compare=True, base="io_1024x384x512"),
+    # the same comparison on the heated 384x192x192 channel
+    "c2_mixed_learned": dict(compare=True, base="io_384x192x192"),
     # the two sections of the coupled TG + IO configuration advanced together
     # each step (the IO section x-periodic: the TG -> IO inlet coupling is not built)
     "c1_tg_io": dict(pair=True, tg="tg_256x192x256", io="io_512x192x256"),
@@ -440,6 +446,199 @@ def run_io(args, wl, ws, rank, local):
     return 0
 
 
+def run_compare(args, wl, ws, rank, local):
+    """The metric's comparison: the same IO channel advanced by the plain FP64
+    form (table splines) and by the mixed form (FP32 Poisson spectra with an
+    FP64-residual refinement sweep) with the learned property model on the
+    tensor cores, K graph-replayed steps each after W warm-up steps, both
+    from the same seeded state.  value = the mixed + learned form's
+    cell-steps/s; the FP64 form's figure, their ratio, the property model's
+    gate and the mixed + learned form's error against the FP64 form at full
+    size (u, p, T, max |div|) ride along."""
+    import torch
+
+    import chapsim1ww_b200 as cs
+    from chapsim1ww_b200 import IOChannel, PropertyEngine
+
+    b = WORKLOADS[wl["base"]]
+    torch.cuda.set_device(local)
+    pg = dist_init(ws)
+    nx, ny, nz = b["nx"], b["ny"], b["nz"]
+    cells = nx * ny * nz
+    table = io_table(b["table"])
+
+    def make(precision):
+        ch = IOChannel(nx, ny, nz, lx=b["lx"], lz=b["lz"], ren=b["ren"], dt=b["dt"], thermal=1, prt=b["prt"],
+                       qw=(b["qw"], b["qw"]), table=table, device=local, precision=precision)
+        return ch
+
+    def timed_steps(ch, n):
+        stream = torch.cuda.ExternalStream(ch.stream(), device=local)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ch.step(n)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1)
+
+    # ---- the plain FP64 form (table splines)
+    ref = make(cs.FP64)
+    ref.random_fl_theml_fld_io(b["seed"] + rank, 0.1)
+    ref.step(args.warmup)
+    ref.sync()
+    barrier(pg)
+    torch.cuda.synchronize()
+    ms64 = max_over_ranks(pg, local, timed_steps(ref, args.steps))
+    div64 = ref.divgck_io()
+
+    # ---- the learned property model: trained on the GPU, gated at 1e-4
+    t0 = time.perf_counter()
+    eng = PropertyEngine(*synthetic_table_cols(table), device=local)
+    loss = eng.train(65536, 2, 20000, 3e-3)
+    t_train = time.perf_counter() - t0
+    nbins, worst = eng.gate(1e-4, 256)
+    out_bins, out_err = eng.gate_outputs()
+
+    # ---- the mixed form with the learned properties
+    mix = make(cs.MIXED)
+    mix.set_props_mode(1, eng)
+    mix.random_fl_theml_fld_io(b["seed"] + rank, 0.1)
+    mix.step(args.warmup)
+    mix.sync()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(pg)
+    torch.cuda.synchronize()
+    n0 = mix.launch_count()
+    ms = max_over_ranks(pg, local, timed_steps(mix, args.steps))
+    torch.cuda.synchronize()
+    barrier(pg)
+    launches = mix.launch_count() - n0
+    clk = clocks.stop()
+    value = cells * ws * args.steps / (ms / 1000.0)
+    value64 = cells * ws * args.steps / (ms64 / 1000.0)
+    divmix = mix.divgck_io()
+    bad = mix.bad_cells()
+
+    # error of the mixed + learned form against the FP64 form after the same
+    # W + K steps from the same state (on the device)
+    def field(ch, name):
+        t = torch.empty(ch.shape, dtype=torch.float64, device=f"cuda:{local}")
+        ch.get_field_device(name, t.data_ptr())
+        return t
+
+    errors = {}
+    for name in ("u", "v", "w", "p", "gx", "t", "rho", "mu"):
+        a, r = field(mix, name), field(ref, name)
+        errors[name] = float((a - r).abs().max() / r.abs().max())
+        del a, r
+    torch.cuda.empty_cache()
+    ref.close()
+    del ref
+
+    # per-phase kernel times of the mixed + learned form
+    mix.phase_timing(True)
+    mix.phase_reset()
+    mix.step(max(1, min(args.steps, 5)))
+    ph, nsub = mix.phase_times()
+    mix.phase_timing(False)
+    per_launch = {IO_PHASES[i]: v / max(nsub, 1) for i, v in enumerate(ph.values())}
+    dom = max(per_launch, key=per_launch.get)
+    peak, peak_kind = measured_peak()
+    bytes_dom = io_phase_bytes(dom, nx, ny, nz)
+    if dom in PHASE_SPECTRAL_PASSES or dom == "fftx":
+        bytes_dom -= PHASE_SPECTRAL_PASSES.get(dom, 0) * 2 * 4 * (nx // 2 + 1) * ny * nz  # FP32 spectra
+    achieved = bytes_dom / (per_launch[dom] / 1000.0) / 1e9
+    kern = IO_KERNEL[dom] if dom != "eng_props" else "k_io_eng_props_mlp"
+    # the learned-property kernel: two model evaluations per cell, 2 x 3 BF16
+    # MMAs of 128 x 64 x 64 (layer 2) and 128 x 16 x 64 (layer 3) per tile
+    mlp_flops = cells * 2 * 3 * 2 * 64 * (64 + 16)
+    mlp = {"kernel": "k_io_eng_props_mlp", "avg_launch_ms": per_launch["eng_props"],
+           "mma_tflops": mlp_flops / (per_launch["eng_props"] / 1000.0) / 1e12,
+           "tanh_per_cell": 256, "note": "bound by the 256 tanh.approx evaluations per cell (SFU), not by HBM"}
+
+    # ---- end to end through the public API with host buffers
+    names, inputs = IO_RESULT_FIELDS, IO_INPUT_FIELDS
+    host = {}
+    for n in names:
+        host[n] = torch.empty(mix.shape, dtype=torch.float64, pin_memory=True).numpy()
+        mix.get_field(n, out=host[n])
+    barrier(pg)
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(mix.stream(), device=local)
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(1, min(args.steps, 5))
+    e2.record(stream)
+    for _ in range(e2e_steps):
+        for n in inputs:
+            mix.set_field_async(n, host[n])
+        mix.step(1)
+        for n in names:
+            mix.get_field_async(n, out=host[n])
+        _ = mix.divgck_io()
+    e3.record(stream)
+    e3.synchronize()
+    barrier(pg)
+    ms_e2e = max_over_ranks(pg, local, e2.elapsed_time(e3))
+    e2e_value = cells * ws * e2e_steps / (ms_e2e / 1000.0)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            v, t, cores = cpu_baseline_io(b, args.cpu_steps)
+            slab = f" (a {b['cpu_nz']}-plane z-slab, same cell size)" if b.get("cpu_nz") else ""
+            cpu = {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
+                   "sample": f"{args.cpu_steps} full RK3 steps of the {wl['base']} channel{slab} after init, FP64 "
+                             f"oracle port (table splines), OpenMP {cores} threads, {t:.1f} s"}
+        except Exception as ex:
+            cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64 fields, f32 Poisson spectra, bf16 hi/lo tensor-core property model (f32 accumulate)",
+            "data": "synthetic (seeded splitmix64 velocity, h = 0, synthetic 4096-point table, NS=0 projection)",
+            "config": workload_config(args, wl),
+            "arm": {"parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
+                    "l2": "working set (>40 GB) larger than the 126 MB L2"},
+            "fp64": {"value": value64, "ms_per_step": ms64 / args.steps, "max_div_g_plus_drho": div64,
+                     "form": "plain FP64, table splines"},
+            "ratio_vs_fp64": value / value64,
+            "max_div_g_plus_drho": divmix, "out_of_table_cells": bad,
+            "error_vs_fp64": {"after_steps": args.warmup + args.steps, "relative_max": errors},
+            "property_model": {"train_s": t_train, "train_loss": loss, "gate_tol": 1e-4, "bins": 256,
+                               "bins_cleared_T_rho_mu_k": nbins, "max_rel_err_T_rho_mu_k": worst,
+                               "bins_cleared_per_output": dict(zip(("T", "rho", "mu", "k", "cp"), out_bins)),
+                               "max_rel_err_per_output": dict(zip(("T", "rho", "mu", "k", "cp"), out_err))},
+            "gpu_launches": launches,
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": len(inputs) * mix.n * 8,
+                    "d2h_bytes_per_step": len(names) * mix.n * 8 + 8, "steps": e2e_steps,
+                    "uploaded": list(inputs), "downloaded": list(names)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": kern, "phase": dom,
+                         "algorithmic_bytes_per_launch": bytes_dom, "avg_launch_ms": per_launch[dom],
+                         "peak_source": peak_kind},
+            "learned_property_kernel": mlp,
+            "phases_ms_per_launch": per_launch,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    mix.close()
+    eng.close()
+    dist_done(pg)
+    return 0
+
+
+def synthetic_table_cols(table5):
+    """Columns H, T, D, M, K, CP for a property engine: the workload's table
+    plus cp = dh/dT of the synthetic table."""
+    from chapsim1ww_b200 import synthetic_table
+    full = synthetic_table(len(table5[0]))
+    return list(table5[:5]) + [full[5]]
+
+
 def run_pair(args, wl, ws, rank, local):
     """TG and IO sections of the coupled configuration, one step of each per
     step, on their own streams chained by events (they alternate, joined
@@ -646,6 +845,8 @@ def cpu_baseline_oracle(wl, steps):
 
 def section_specs(wl):
     """(kind, spec) of every section a workload advances per step."""
+    if wl.get("compare"):
+        return [("io", WORKLOADS[wl["base"]])]
     if wl.get("pair"):
         return [("tg", WORKLOADS[wl["tg"]]), ("io", WORKLOADS[wl["io"]])]
     if wl.get("batch"):
@@ -743,6 +944,14 @@ def workload_scaling(wl):
 
 def workload_config(args, wl):
     """The config block both arms print for a workload."""
+    if wl.get("compare"):
+        b = WORKLOADS[wl["base"]]
+        return {"workload": args.workload, **{k: b[k] for k in ("nx", "ny", "nz", "ren", "dt", "prt")},
+                "cells": b["nx"] * b["ny"] * b["nz"], "wall_heat_flux": b["qw"], "table": b["table"],
+                "lx": b["lx"], "lz": b["lz"], "seed": b["seed"],
+                "forms": "mixed precision + learned properties (value) against plain FP64 + table splines",
+                "property_model": "degree-5 polynomial + MLP 1-64-64-5 tanh residual, 65,536 samples, seed 2, "
+                                  "gate 1e-4 over 256 h-bins"}
     if wl.get("batch"):
         return {"workload": args.workload, "channels": 64, "seed": wl["seed"], "precision": args.precision,
                 "steps_unit": "one RK3 step of every channel"}
@@ -1044,6 +1253,8 @@ def main():
         return run_reference(args, wl, ws, rank)
     if wl.get("batch"):
         return run_batch(args, wl, ws, rank, local)
+    if wl.get("compare"):
+        return run_compare(args, wl, ws, rank, local)
     if wl.get("pair"):
         return run_pair(args, wl, ws, rank, local)
     if wl.get("io"):

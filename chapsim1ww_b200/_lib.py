@@ -137,6 +137,7 @@ SIGNATURES += [
     ("chapsim_stats_reset", _I, [_P]),
     ("chapsim_write_instant", _I, [_P, ctypes.c_char_p, _I, _D]),
     ("chapsim_read_instant", _I, [_P, ctypes.c_char_p, _D, ctypes.POINTER(_I), _DP]),
+    ("chapsim_set_refinement", _I, [_P, _I]),
     ("chapsim_inject_wait_timeout", _I, [_P, _I]),
     ("chapsim_instant_file_name", _I, [ctypes.c_char_p, _I, ctypes.c_char_p, _D, ctypes.c_char_p, _I]),
     ("chapsim_instant_file_write", _I, [ctypes.c_char_p, _I, _I, _I, _I, _D, _D, _D, _P]),

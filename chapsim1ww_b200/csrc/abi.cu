@@ -484,7 +484,9 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
   void *p = nullptr;
   {
     const bool mixed = cfg->precision == CHAPSIM_MIXED;
-    const size_t tsz = mixed ? sizeof(float) : sizeof(double);
+    // TG temporaries follow the precision form; the IO kernels keep EXPLT0 and
+    // RHS_io in FP64 (their mixed form narrows only the Poisson spectra)
+    const size_t tsz = (mixed && !iocfg) ? sizeof(float) : sizeof(double);
     double **f64[] = {&d.u, &d.v, &d.w, &d.p, &d.phi, &d.rhsphi, &d.res};
     for (double **f : f64) {
       if ((rc = dalloc(ctx, &p, n * sizeof(double)))) goto fail;
@@ -611,7 +613,7 @@ int chapsim_io_config_default(chapsim_io_config *io) {
 int chapsim_create_io(const chapsim_config *cfg, const chapsim_io_config *io, chapsim_ctx **out) {
   if (!cfg || !io || !out) return CHAPSIM_ERR_ARG;
   if (io->struct_size != (int32_t)sizeof(chapsim_io_config)) return CHAPSIM_ERR_ARG;
-  if (cfg->precision != CHAPSIM_FP64) return CHAPSIM_ERR_UNSUPPORTED;
+  if (cfg->precision == CHAPSIM_MIXED && io->visc_scheme != 0) return CHAPSIM_ERR_UNSUPPORTED;
   if (!(io->prt > 0) || io->gravdir < 0 || io->gravdir > 3) return CHAPSIM_ERR_ARG;
   if (io->visc_scheme != 0 && io->visc_scheme != 1) return CHAPSIM_ERR_ARG;
   if (io->coupled != 0 && io->coupled != 1) return CHAPSIM_ERR_ARG;
@@ -646,6 +648,17 @@ int chapsim_sync(chapsim_ctx *ctx) {
   if (!ctx) return CHAPSIM_ERR_ARG;
   CKC(cudaStreamSynchronize(ctx->stream));
   return check_device_error(ctx);
+}
+
+int chapsim_set_refinement(chapsim_ctx *ctx, int sweeps) {
+  if (!ctx || (sweeps != 0 && sweeps != 1)) return CHAPSIM_ERR_ARG;
+  CKC(cudaSetDevice(ctx->device));
+  CKC(cudaStreamSynchronize(ctx->stream));
+  ctx->refine = sweeps == 1;
+  if (ctx->step_graph) { cudaGraphExecDestroy(ctx->step_graph); ctx->step_graph = nullptr; }
+  for (auto &g : ctx->io_graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  return CHAPSIM_OK;
 }
 
 int chapsim_inject_wait_timeout(chapsim_ctx *ctx, int polls) {
@@ -707,8 +720,8 @@ static int xfer(chapsim_ctx *ctx, int domain, int field, void *dst_or_src, int64
   CKC(cudaSetDevice(ctx->device));
   const size_t bytes = (size_t)n * sizeof(double);
   const bool h0f = field >= CHAPSIM_F_H0U && field <= CHAPSIM_F_H0W;
-  if (h0f && ctx->cfg.precision == CHAPSIM_MIXED) {
-    // CONVH0 is held in FP32 in the mixed form: convert through the host
+  if (h0f && ctx->cfg.precision == CHAPSIM_MIXED && ctx->domain == CHAPSIM_ITG) {
+    // CONVH0 is held in FP32 in the TG mixed form: convert through the host
     REQUIRE(kind != cudaMemcpyDeviceToDevice, CHAPSIM_ERR_UNSUPPORTED, "device copies of FP32 H0 fields");
     REQUIRE(!async, CHAPSIM_ERR_UNSUPPORTED, "stream-ordered copies of FP32 H0 fields");
     std::vector<float> tmp((size_t)n);

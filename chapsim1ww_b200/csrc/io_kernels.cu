@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_props_only(TGDev d, IODev i
 // plain kernel's treatment: mu0, rho0 and mu0 + mu only); every tile runs the
 // model twice on the tensor cores.
 __global__ void __launch_bounds__(chapsim_mlp::TILE, 4) k_io_eng_props_mlp(TGDev d, IODev io, chapsim_mlp::MlpDev M) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   chapsim_mlp::Smem &s = chapsim_mlp::smem_of(smem_raw);
   chapsim_mlp::cta_setup(s, M);
   uint32_t phase = 0;
@@ -360,7 +360,7 @@ __global__ void __launch_bounds__(chapsim_mlp::TILE, 4) k_io_eng_props_mlp(TGDev
 // where the gate has not cleared the bin; mu0 + mu follows the new mu.
 __global__ void __launch_bounds__(chapsim_mlp::TILE, 4) k_io_therm_props(TGDev d, IODev io, chapsim_mlp::MlpDev M,
                                                                          int use_mlp) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   chapsim_mlp::Smem *sp = nullptr;
   uint32_t phase = 0;
   if (use_mlp) {

@@ -99,11 +99,14 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
          (1ull << 46);
 }
 
+// D (+)= A B^T with every output lane enabled (the four 32-bit
+// disable-output-lane masks zero); acc = 0 overwrites D.
 __device__ __forceinline__ void umma(uint32_t dtm, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  const uint32_t z = 0;
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtm),
-      "l"(a), "l"(b), "r"(idesc), "r"(acc)
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(dtm),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z)
       : "memory");
 }
 

@@ -83,7 +83,7 @@ __global__ void k_props_table(PropsDev P, const double *__restrict__ h, double *
 __global__ void __launch_bounds__(chapsim_mlp::TILE, 4)
     k_props_mlp_tc(PropsDev P, const double *__restrict__ h, double *T, double *rho, double *mu, double *kk,
                    double *cp, int64_t n) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   chapsim_mlp::Smem &s = chapsim_mlp::smem_of(smem_raw);
   const chapsim_mlp::MlpDev &M = P.M;
   chapsim_mlp::cta_setup(s, M);

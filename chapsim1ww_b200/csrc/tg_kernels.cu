@@ -1652,8 +1652,10 @@ int launch_pois_io(chapsim_ctx *c, int ns, double *gx, double *gy, double *gz, c
   // at the provisional mass flux for these launches only
   const TGDev saved = c->d;
   c->d.u = gx; c->d.v = gy; c->d.w = gz; c->d.drho = drho;
-  c->d.skip_rhs = store_rhs ? 0 : 1;
-  const int rc = Prec<double>::poisson(c, ns, 0);
+  const bool mixed = c->cfg.precision == CHAPSIM_MIXED;
+  // the mixed form's refinement sweep forms its residual from RHSLLPHI
+  c->d.skip_rhs = (store_rhs || (mixed && c->refine)) ? 0 : 1;
+  const int rc = mixed ? Prec<float>::poisson(c, ns, 0) : Prec<double>::poisson(c, ns, 0);
   c->d = saved;
   return rc;
 }

@@ -134,6 +134,10 @@ class TGChannel:
     def sync(self):
         self._chk(self.lib.chapsim_sync(self.h))
 
+    def set_refinement(self, sweeps):
+        """Refinement sweeps (0 or 1) of the mixed form's Poisson solve."""
+        self._chk(self.lib.chapsim_set_refinement(self.h, sweeps))
+
     def stream(self):
         s = ctypes.c_void_p()
         self._chk(self.lib.chapsim_get_stream(self.h, ctypes.byref(s)))

@@ -54,9 +54,11 @@ extern "C" {
 
 /* precision forms */
 #define CHAPSIM_FP64 0  /* every array and operation in FP64                    */
-#define CHAPSIM_MIXED 1 /* FP64 state; FP32 temporaries, FFT and line solves,
-                           FP64 low-mode Poisson lines, reductions and one
-                           FP64-residual refinement sweep of the Poisson solve */
+#define CHAPSIM_MIXED 1 /* FP64 state; FP32 temporaries and spectra (TG), FP32
+                           Poisson spectra (IO, explicit viscous scheme); FP64
+                           Poisson y-lines, reductions and one FP64-residual
+                           refinement sweep of the Poisson solve
+                           (chapsim_set_refinement) */
 
 /* field ids for chapsim_set_field / chapsim_get_field (TG domain) */
 #define CHAPSIM_F_U 0      /* Q_tg(:,:,:,1)   */
@@ -126,6 +128,12 @@ int chapsim_create(const chapsim_config *cfg, chapsim_ctx **out);
 int chapsim_destroy(chapsim_ctx *ctx);
 const char *chapsim_last_error(const chapsim_ctx *ctx);
 int chapsim_sync(chapsim_ctx *ctx);
+
+/* Refinement sweeps of the mixed form's Poisson solve: 1 (the default) forms
+ * the FP64 residual RHSLLPHI - L phi (the operator of CHECK_FFT_SOLVER,
+ * src/PRESSURE_CORRECTION.f90:159-202) and adds its FP32 spectral solve to
+ * phi; 0 keeps the single FP32 solve.  No effect on the FP64 form. */
+int chapsim_set_refinement(chapsim_ctx *ctx, int sweeps);
 
 /* Fault injection for the bounded device waits (no reference counterpart;
  * the reference's failure path is ERRHDL, print and STOP,
@@ -279,7 +287,8 @@ int chapsim_launch_count_reset(chapsim_ctx *ctx);
  *
  * On an IO context: u, v, w = Q_io, p = PR_io, phi = DPH_io, rhsphi =
  * RHSLLPHI_io, H0U/H0V/H0W = EXPLT0_io(:,:,:,1..3), plus the fields below.
- * The time-step form is FP64 only.
+ * Precision forms: FP64, and (explicit viscous scheme) CHAPSIM_MIXED, whose
+ * fields all stay FP64 and whose Poisson solve runs on FP32 spectra.
  * ====================================================================== */
 #define CHAPSIM_F_GX 10     /* G_io(:,:,:,1), mass flux rho u       */
 #define CHAPSIM_F_GY 11     /* G_io(:,:,:,2)                        */
@@ -391,7 +400,8 @@ int chapsim_io_config_default(chapsim_io_config *io);
 
 /* IO domain set-up (MEM_ALLOCAT + COORDJR + FISHPACK_POIS3D_INIT,
  * src/DNS_THERMAL.f90:117-176, src/possion3d_fishpack_reform.f90:337-430):
- * cfg gives the IO grid (nx = NCL1_io, lx = HX_io); precision must be FP64. */
+ * cfg gives the IO grid (nx = NCL1_io, lx = HX_io); precision FP64, or
+ * CHAPSIM_MIXED with visc_scheme = 0. */
 int chapsim_create_io(const chapsim_config *cfg, const chapsim_io_config *io, chapsim_ctx **out);
 
 /* Property table of an IO context: columns H, T, D, M, K (host, length n >= 4,
