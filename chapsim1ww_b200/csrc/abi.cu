@@ -1149,9 +1149,12 @@ int chapsim_set_props_mode(chapsim_ctx *ctx, int mode, const chapsim_props *pe) 
     REQUIRE(dev == ctx->device, CHAPSIM_ERR_ARG, "property engine and context on different devices");
     REQUIRE(chapsim::props_same_table(pe, ctx->tab), CHAPSIM_ERR_ARG,
             "the model was trained on another table than the context's");
-    const size_t npar = chapsim_mlp::NP * sizeof(float);
-    const size_t nwt = (2 * chapsim_mlp::NH * chapsim_mlp::NH + 2 * chapsim_mlp::NOP * chapsim_mlp::NH) *
-                       sizeof(uint16_t);
+    // the three parts of the copy start on 256-byte boundaries: the kernels
+    // read the weight tiles with 16-byte vector loads
+    const size_t npar_b = chapsim_mlp::NP * sizeof(float);
+    const size_t nwt_b = (2 * chapsim_mlp::NH * chapsim_mlp::NH + 2 * chapsim_mlp::NOP * chapsim_mlp::NH) *
+                         sizeof(uint16_t);
+    const size_t npar = (npar_b + 255) & ~(size_t)255, nwt = (nwt_b + 255) & ~(size_t)255;
     if (!ctx->mlp_buf) {
       void *p = nullptr;
       if (cudaMalloc(&p, npar + nwt + chapsim_mlp::kMaxGateBins) != cudaSuccess) {
@@ -1163,14 +1166,15 @@ int chapsim_set_props_mode(chapsim_ctx *ctx, int mode, const chapsim_props *pe) 
       ctx->allocs.push_back(p);
     }
     char *b = static_cast<char *>(ctx->mlp_buf);
-    CKC(cudaMemcpyAsync(b, src.par, npar, cudaMemcpyDeviceToDevice, ctx->stream));
-    CKC(cudaMemcpyAsync(b + npar, src.wt, nwt, cudaMemcpyDeviceToDevice, ctx->stream));
+    CKC(cudaMemcpyAsync(b, src.par, npar_b, cudaMemcpyDeviceToDevice, ctx->stream));
+    CKC(cudaMemcpyAsync(b + npar, src.wt, nwt_b, cudaMemcpyDeviceToDevice, ctx->stream));
     CKC(cudaMemcpyAsync(b + npar + nwt, src.gate, chapsim_mlp::kMaxGateBins, cudaMemcpyDeviceToDevice, ctx->stream));
     CKC(cudaStreamSynchronize(ctx->stream));
     ctx->mlp = src;
     ctx->mlp.par = reinterpret_cast<const float *>(b);
     ctx->mlp.wt = reinterpret_cast<const uint16_t *>(b + npar);
     ctx->mlp.gate = reinterpret_cast<const uint8_t *>(b + npar + nwt);
+    REQUIRE(((uintptr_t)ctx->mlp.wt & 15) == 0, CHAPSIM_ERR_STATE, "model weight tiles not 16-byte aligned");
   }
   ctx->props_mode = mode;
   for (auto &g : ctx->io_graph)  // the captured steps hold the other property kernel

@@ -186,7 +186,7 @@ constexpr size_t kSmemBytes = sizeof(Smem) + 1024;
 // the CTA's tensor memory (warp 0).  Every thread of the 128 calls it.
 __device__ __forceinline__ void cta_setup(Smem &s, const MlpDev &M) {
   const int t = threadIdx.x;
-  const uint4 *src = reinterpret_cast<const uint4 *>(M.wt);
+  const uint4 *src = reinterpret_cast<const uint4 *>(M.wt);  // 16-byte aligned (host contract)
   uint4 *dst = reinterpret_cast<uint4 *>(s.w2_hi);  // w2_hi, w2_lo, w3_hi, w3_lo are contiguous
   constexpr int n16 = (2 * NH * NH + 2 * NOP * NH) * 2 / 16;
   for (int q = t; q < n16; q += TILE) dst[q] = src[q];
