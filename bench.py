@@ -501,6 +501,7 @@ def run_compare(args, wl, ws, rank, local):
 
     # ---- the mixed form with the learned properties
     mix = make(cs.MIXED)
+    mix.set_refinement(args.refine)
     mix.set_props_mode(1, eng)
     mix.random_fl_theml_fld_io(b["seed"] + rank, 0.1)
     mix.step(args.warmup)
@@ -525,6 +526,7 @@ def run_compare(args, wl, ws, rank, local):
     def field(ch, name):
         t = torch.empty(ch.shape, dtype=torch.float64, device=f"cuda:{local}")
         ch.get_field_device(name, t.data_ptr())
+        ch.sync()  # the copy is ordered on the context's stream, not torch's
         return t
 
     errors = {}
@@ -604,6 +606,7 @@ def run_compare(args, wl, ws, rank, local):
                     "l2": "working set (>40 GB) larger than the 126 MB L2"},
             "fp64": {"value": value64, "ms_per_step": ms64 / args.steps, "max_div_g_plus_drho": div64,
                      "form": "plain FP64, table splines"},
+            "mixed_form": {"poisson_spectra": "fp32", "fp64_residual_refinement_sweeps": args.refine},
             "ratio_vs_fp64": value / value64,
             "max_div_g_plus_drho": divmix, "out_of_table_cells": bad,
             "error_vs_fp64": {"after_steps": args.warmup + args.steps, "relative_max": errors},
@@ -1186,6 +1189,25 @@ def run_ours(args, wl, ws, rank, local):
 def profile_case(spec, precision):
     import chapsim1ww_b200 as cs
     from chapsim1ww_b200 import TGChannel
+    if spec.lower().startswith("iolearn"):
+        # the mixed IO form with the learned property model (model trained
+        # briefly: the kernels' work does not depend on its accuracy)
+        from chapsim1ww_b200 import IOChannel, PropertyEngine, synthetic_table
+        nx, ny, nz = (int(x) for x in spec.lower()[7:].split("x"))
+        eng = PropertyEngine(*synthetic_table(4096))
+        eng.train(65536, 2, 300, 3e-3)
+        eng.gate(1e9, 256)
+        c = IOChannel(nx, ny, nz, table=io_table("synthetic"), precision=cs.MIXED)
+        c.set_refinement(0)
+        c.set_props_mode(1, eng)
+        c.random_fl_theml_fld_io(2, 0.1)
+        for _ in range(2):
+            for ns in (1, 2, 3):
+                c.solverrk3_eng_io(ns)
+                c.solverrk3_mom_io(ns)
+        c.sync()
+        print("profile case ok", spec, "max|div G + drho| =", c.divgck_io())
+        return 0
     if spec.lower().startswith("io"):
         from chapsim1ww_b200 import IOChannel
         si = spec.lower().startswith("iosi")  # the semi-implicit viscous scheme
@@ -1235,6 +1257,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--ref-budget", type=float, default=100.0,
                     help="seconds of host work the reference arm's W + K steps are sized to")
+    ap.add_argument("--refine", type=int, choices=[0, 1], default=0,
+                    help="FP64-residual refinement sweeps of the mixed IO form's Poisson solve")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-props", action="store_true", help="skip the learned-property measurement")
     ap.add_argument("--profile-case", default=None, metavar="NXxNYxNZ",

@@ -153,7 +153,10 @@ int64_t chapsim_field_len(const chapsim_ctx *ctx);
  * chapsim_field_len.  host may be pageable or pinned. */
 int chapsim_set_field(chapsim_ctx *ctx, int domain, int field, const double *host, int64_t n);
 int chapsim_get_field(chapsim_ctx *ctx, int domain, int field, double *host, int64_t n);
-/* Device-resident variants: dev is a device pointer on the context's device. */
+/* Device-resident variants: dev is a device pointer on the context's device.
+ * The copy is queued on the context's stream and the call returns at once:
+ * order other streams' work after it through chapsim_sync or an event on the
+ * stream of chapsim_get_stream. */
 int chapsim_set_field_device(chapsim_ctx *ctx, int domain, int field, const double *dev, int64_t n);
 int chapsim_get_field_device(chapsim_ctx *ctx, int domain, int field, double *dev, int64_t n);
 /* Stream-ordered variants of chapsim_set_field / chapsim_get_field: the copy
