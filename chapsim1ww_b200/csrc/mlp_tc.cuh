@@ -13,7 +13,8 @@
 // the MMA's M = 128 rows):
 //  - layer 1 on the CUDA cores in FP32 (tanh.approx.f32);
 //  - each activation vector is split into BF16 hi + lo parts (lo = the
-//    rounding error of hi), the weights likewise, and every layer runs as
+//    rounding error of hi, split on the integer pipe), the weights likewise,
+//    and every layer runs as
 //    three BF16 MMAs accumulating in FP32 (hi*hi + hi*lo + lo*hi), which
 //    carries about 16 mantissa bits: plain BF16 operands (8 bits) leave the
 //    outputs about 1e-3 off, above the 1e-4 bound the model is gated on;
@@ -148,11 +149,19 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v) {
   for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// BF16 round-to-nearest-even of two floats, packed (first in the low half).
-__device__ __forceinline__ uint32_t pack2(float a, float b) {
-  uint32_t r;
-  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(b), "f"(a));
-  return r;
+// Split of one thread's 64 activations into BF16 hi + lo words on the
+// integer pipe.  hi = x rounded to nearest-even BF16 (add 0x7FFF plus the
+// lowest kept bit, keep the top 16 bits), lo = x - hi truncated to BF16 (its
+// own rounding would change the product by about 2^-17 of x, below what the
+// three-product split resolves).  Pairs are packed by byte permutes.  The
+// cvt.rn.bf16x2.f32 conversion would run on the special-function pipe, which
+// the tanh evaluations already saturate.
+__device__ __forceinline__ void split2(float x0, float x1, uint32_t &hi, uint32_t &lo) {
+  const uint32_t b0 = __float_as_uint(x0), b1 = __float_as_uint(x1);
+  const uint32_t r0 = b0 + 0x7FFFu + ((b0 >> 16) & 1u), r1 = b1 + 0x7FFFu + ((b1 >> 16) & 1u);
+  hi = __byte_perm(r0, r1, 0x7632);
+  const float l0 = x0 - __uint_as_float(r0 & 0xFFFF0000u), l1 = x1 - __uint_as_float(r1 & 0xFFFF0000u);
+  lo = __byte_perm(__float_as_uint(l0), __float_as_uint(l1), 0x7632);
 }
 
 // Write one thread's 64 activations into row r of the hi and lo A tiles.
@@ -161,12 +170,7 @@ __device__ __forceinline__ void store_split(Smem &s, int r, const float *a) {
   for (int c = 0; c < 8; ++c) {
     uint32_t hi[4], lo[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const float x0 = a[8 * c + 2 * q], x1 = a[8 * c + 2 * q + 1];
-      hi[q] = pack2(x0, x1);
-      const float h0 = __uint_as_float(hi[q] << 16), h1 = __uint_as_float(hi[q] & 0xFFFF0000u);
-      lo[q] = pack2(x0 - h0, x1 - h1);
-    }
+    for (int q = 0; q < 4; ++q) split2(a[8 * c + 2 * q], a[8 * c + 2 * q + 1], hi[q], lo[q]);
     const int off = tile_off(r, 8 * c);
     *reinterpret_cast<uint4 *>(reinterpret_cast<char *>(s.a_hi) + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
     *reinterpret_cast<uint4 *>(reinterpret_cast<char *>(s.a_lo) + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);

@@ -1205,6 +1205,18 @@ __global__ void __launch_bounds__(128) k_ysolve_line(TGDev d) {
 // precomputed pivots (lane 0, same operations, same results).
 constexpr double kPartShiftMin = 4.0;
 
+// 1/x from the hardware FP64 reciprocal approximation (rcp.approx.ftz.f64)
+// refined by two Newton-Raphson steps r <- r + r (1 - x r), each of which
+// squares the relative error: full FP64 precision in one special-function
+// instruction and four FMAs instead of a correctly rounded division.
+__device__ __forceinline__ double rcp_nr(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  r = fma(r, fma(-x, r, 1.0), r);
+  r = fma(r, fma(-x, r, 1.0), r);
+  return r;
+}
+
 __host__ __device__ inline int ypart_count(int n) {
   int P = 1;
   while (P < 32 && n % (2 * P) == 0 && n / (2 * P) >= 2) P *= 2;
@@ -1229,7 +1241,7 @@ __device__ __forceinline__ void ypart_line(typename Cplx<T>::type *X, const doub
         const int s = t * Q + lane;
         const double a = ca[s], b = cb[s] - shift, c = cc[s];
         const C r = X[s];
-        const double iv = 1.0 / (b - a * h);
+        const double iv = rcp_nr(b - a * h);
         inv[t] = iv;
         const bool last = t == m - 2;
         yr = ((double)r.x - a * yr) * iv;
@@ -1248,7 +1260,7 @@ __device__ __forceinline__ void ypart_line(typename Cplx<T>::type *X, const doub
         const int s = t * Q + lane;
         const double a = ca[s], b = cb[s] - shift, c = cc[s];
         const C r = X[s];
-        const double iv = 1.0 / (b - c * h);
+        const double iv = rcp_nr(b - c * h);
         yr = ((double)r.x - c * yr) * iv;
         yi = ((double)r.y - c * yi) * iv;
         v = (-c * v - (t == 0 ? a : 0.0)) * iv;
@@ -1280,14 +1292,14 @@ __device__ __forceinline__ void ypart_line(typename Cplx<T>::type *X, const doub
     if (lane - hs < 0) { Am = 0.0; Bm = 1.0; Cm = 0.0; Rmr = 0.0; Rmi = 0.0; }
     if (lane + hs >= P) { Aq = 0.0; Bq = 1.0; Cq = 0.0; Rqr = 0.0; Rqi = 0.0; }
     if (act) {
-      const double k1 = Ap / Bm, k2 = Cp / Bq;
+      const double k1 = Ap * rcp_nr(Bm), k2 = Cp * rcp_nr(Bq);
       const double nA = -Am * k1, nC = -Cq * k2, nB = Bp - Cm * k1 - Aq * k2;
       Rr = Rr - Rmr * k1 - Rqr * k2;
       Ri = Ri - Rmi * k1 - Rqi * k2;
       Ap = nA; Bp = nB; Cp = nC;
     }
   }
-  const double Lr = Rr / Bp, Li = Ri / Bp;
+  const double ib = rcp_nr(Bp), Lr = Rr * ib, Li = Ri * ib;
   double Lmr = __shfl_sync(full, Lr, (lane - 1) & 31), Lmi = __shfl_sync(full, Li, (lane - 1) & 31);
   if (lane == 0) { Lmr = 0.0; Lmi = 0.0; }
   if (act) {
@@ -1335,8 +1347,8 @@ __device__ __forceinline__ void ypart_line(typename Cplx<T>::type *X, const doub
 // warp): the same operations on the same values, with the pivots of
 // k_ypivots read from global memory a few rows ahead.
 template <typename T>
-__device__ __forceinline__ void yserial_line(const TGDev &d, typename Cplx<T>::type *X, int kx, int kz, int m,
-                                             int Q) {
+__device__ __forceinline__ void yserial_line(const TGDev &d, typename Cplx<T>::type *X, int kx, int kz,
+                                             const int *slot) {
   typedef typename Cplx<T>::type C;
   const int ny = d.ny;
   const int64_t base = kx + (int64_t)d.lp * ny * kz, st = d.lp;
@@ -1354,7 +1366,7 @@ __device__ __forceinline__ void yserial_line(const TGDev &d, typename Cplx<T>::t
     for (int u = 0; u < YB; ++u) {
       const int j = j0 + u;
       if (j <= ny) {
-        const int s = ((j - 1) % m) * Q + (j - 1) / m;
+        const int s = slot[j - 1];
         const C r = X[s];
         if (j == 1) {
           gr = (double)r.x * p[u];
@@ -1380,7 +1392,7 @@ __device__ __forceinline__ void yserial_line(const TGDev &d, typename Cplx<T>::t
     for (int u = 0; u < YB; ++u) {
       const int j = j0 - u;
       if (j >= 1) {
-        const int s = ((j - 1) % m) * Q + (j - 1) / m;
+        const int s = slot[j - 1];
         const C r = X[s];
         xr = (double)r.x - h[u] * xr;
         xi = (double)r.y - h[u] * xi;
@@ -1410,7 +1422,9 @@ struct YPartShape {
     while (y.L > 2 && (size_t)y.L * y.ls * sizeof(C) > 100 * 1024) y.L >>= 1;
     return y;
   }
-  size_t smem() const { return (size_t)3 * m * Q * sizeof(double) + (size_t)L * ls * sizeof(C); }
+  size_t smem(int ny) const {
+    return (size_t)3 * m * Q * sizeof(double) + (size_t)L * ls * sizeof(C) + (size_t)ny * sizeof(int);
+  }
   bool usable() const { return P >= 2 && m >= 2 && m <= 16; }
 };
 
@@ -1418,24 +1432,28 @@ template <typename T, int M>
 __global__ void __launch_bounds__(256) k_ysolve_part(TGDev d, int P, int m, int L, int ls) {
   typedef typename Cplx<T>::type C;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  const int Q = P + 1, mq = m * Q;
+  const int Q = P + 1, mq = m * Q, ny = d.ny;
   double *ca = reinterpret_cast<double *>(smem_raw), *cb = ca + mq, *cc = cb + mq;
   C *lines = reinterpret_cast<C *>(cc + mq);
-  const int ny = d.ny, kz = blockIdx.y, kx0 = blockIdx.x * L;
+  int *slot = reinterpret_cast<int *>(lines + (size_t)L * ls);  // slot of line element j
+  const int kz = blockIdx.y, kx0 = blockIdx.x * L;
   const int nl = min(L, d.lh - kx0);
   const int tid = threadIdx.x, nt = blockDim.x;
   // the y-operator rows in the slot layout (no coupling beyond the walls)
   for (int j = tid; j < ny; j += nt) {
     const int s = (j % m) * Q + j / m;
+    slot[j] = s;
     ca[s] = j == 0 ? 0.0 : d.amph[j + 1];
     cb[s] = d.acph[j + 1];
     cc[s] = j == ny - 1 ? 0.0 : d.apph[j + 1];
   }
+  __syncthreads();
+  // staging: thread (w, j0) moves line w's rows j0, j0 + nt / L, ... (L is a
+  // power of two, nt = 32 L): each row of the block's lines is one segment
   C *S = reinterpret_cast<C *>(d.spec) + kx0 + (int64_t)d.lp * ny * kz;
-  for (int f = tid; f < ny * nl; f += nt) {
-    const int j = f / nl, w = f - j * nl;
-    lines[w * ls + (j % m) * Q + j / m] = S[(int64_t)d.lp * j + w];
-  }
+  const int w = tid & (L - 1), jstep = nt / L;
+  if (w < nl)
+    for (int j = tid / L; j < ny; j += jstep) lines[w * ls + slot[j]] = S[(int64_t)d.lp * j + w];
   __syncthreads();
   const int warp = tid >> 5, lane = tid & 31;
   if (warp < nl) {
@@ -1445,13 +1463,11 @@ __global__ void __launch_bounds__(256) k_ysolve_part(TGDev d, int P, int m, int 
     if (shift >= kPartShiftMin)
       ypart_line<T, M>(X, ca, cb, cc, shift, P, m, Q, lane);
     else if (lane == 0)
-      yserial_line<T>(d, X, kx, kz, m, Q);
+      yserial_line<T>(d, X, kx, kz, slot);
   }
   __syncthreads();
-  for (int f = tid; f < ny * nl; f += nt) {
-    const int j = f / nl, w = f - j * nl;
-    S[(int64_t)d.lp * j + w] = lines[w * ls + (j % m) * Q + j / m];
-  }
+  if (w < nl)
+    for (int j = tid / L; j < ny; j += jstep) S[(int64_t)d.lp * j + w] = lines[w * ls + slot[j]];
 }
 
 // Inverse real transform along x (src/possion3d_FFT99.f90:461-485): the
@@ -1762,7 +1778,7 @@ template <typename T> struct Prec {
       const YPartShape<T> y = YPartShape<T>::make(d.ny);
       if (y.usable()) {
         dim3 grid((d.lh + y.L - 1) / y.L, d.nz);
-        const size_t sm = y.smem();
+        const size_t sm = y.smem(d.ny);
         if (y.m <= 4)
           k_ysolve_part<T, 4><<<grid, 32 * y.L, sm, c->stream>>>(d, y.P, y.m, y.L, y.ls);
         else if (y.m <= 8)
