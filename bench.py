@@ -6,17 +6,25 @@
 A "step" is one full RK3 time step (substeps NS = 1, 2, 3) of the workload.
 Metric: cell-steps/s = cells x steps / seconds.
 
-Default workload (c1_tg_io): the two sections of the coupled TG + IO
-configuration advanced together every step: the TG channel 256x192x256
-(Lx = 4 pi, Lz = 4 pi / 3, tanh stretching beta = 2, Re_b = 2800, dt = 1e-3,
-seed 1) and the IO section 512x192x256 (Lx = 8 pi) with constant-property
-passive heat (rho = mu = k = cp = 1, T = h), wall heat flux 1, Pr 0.71,
-seed 1; the IO section runs x-periodic because the TG -> IO inlet coupling
-is not built.  Synthetic seeded initial fields.  With N > 1 GPUs every rank
-advances its own independent copy (replicas, weak scaling, no data-path
-collective); timing is the max over ranks.  Other workloads: the TG or IO
-section alone, the heated variable-property IO channel 384x192x192, the
-64-channel batch, the CPU-sized 64^3 TG channel.
+Default workload (c4_mixed_learned): the metric's comparison on the large
+single domain, io_1024x384x512 (201 M cells, Lx = 8 pi, Lz = 2 pi, tanh
+stretching beta = 2, Re_b = 10,000, dt = 1e-3, heated with the synthetic
+4096-point property table, wall heat flux 1, Pr 0.71, seed 4).  The plain
+FP64 form with the table splines and the mixed form (FP32 Poisson spectra,
+one FP64-residual refinement sweep) with the learned property model (trained
+on the GPU on 65,536 table samples, seed 2, gated at 1e-4 over 256 h-bins)
+advance the same seeded state; `value` is the mixed + learned form's
+cell-steps/s, the FP64 form's figure and their ratio ride along, with the
+mixed + learned form's error against the FP64 form at full size.
+Synthetic seeded initial fields (no public dataset is involved).  With N > 1
+GPUs every rank advances its own independent copy (replicas, weak scaling,
+no data-path collective); timing is the max over ranks.  Other workloads:
+c2_mixed_learned (the same comparison on the heated 384x192x192 channel),
+c1_tg_io (the TG channel 256x192x256 and the IO section 512x192x256 with
+constant-property passive heat, advanced together; the IO section runs
+x-periodic because the TG -> IO inlet coupling is not built), the TG or IO
+section alone, the heated IO channel with the semi-implicit viscous scheme,
+the 64-channel batch (split across ranks), the CPU-sized 64^3 TG channel.
 
 Arms:
   ours       libchapsim through the C ABI; `value` with the state resident in
@@ -1252,12 +1260,12 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c1_tg_io")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="c4_mixed_learned")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--ref-budget", type=float, default=100.0,
                     help="seconds of host work the reference arm's W + K steps are sized to")
-    ap.add_argument("--refine", type=int, choices=[0, 1], default=0,
+    ap.add_argument("--refine", type=int, choices=[0, 1], default=1,
                     help="FP64-residual refinement sweeps of the mixed IO form's Poisson solve")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-props", action="store_true", help="skip the learned-property measurement")

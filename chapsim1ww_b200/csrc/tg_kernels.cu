@@ -1176,300 +1176,6 @@ __global__ void __launch_bounds__(128) k_ysolve_line(TGDev d) {
   }
 }
 
-// ---------------------------------------------------------------------------
-// Poisson y-tridiagonals with each line read from and written to HBM once.
-//
-// A block takes L consecutive kx lines of one kz plane.  The block stages the
-// lines in shared memory with coalesced loads (row j of the L lines is
-// contiguous in the spectral array), every warp solves one line there, and the
-// block writes the lines back: one read and one write of the spectral data,
-// no pivot arrays.  A line element j sits at slot (j % m) * Q + j / m
-// (Q = P + 1) of its line, so the lanes' chunk walks touch consecutive words;
-// lines are ls >= m Q elements apart with ls = 1 (mod 128 / sizeof(C)), so the
-// staging loops' consecutive lines fall in different banks.
-//
-// A line with shift = AK1(kx) + AK3(kz) >= kPartShiftMin is solved by the
-// warp-partition method: the line is cut into P chunks of m rows (P a power
-// of two <= 32), lane p sweeps its chunk top-down and bottom-up to express
-// the chunk's first and last interior unknowns in the chunk-end unknowns
-// L(p-1), L(p); parallel cyclic reduction over shuffles solves the P
-// chunk-end equations; each lane then solves its interior rows by Thomas with
-// the pivots of its first sweep (kept in registers).  The y-operator
-// (AMPH, ACPH - shift, APPH; src/possion3d_FFT99.f90:194-213) comes from the
-// 1-D mesh tables.  For shift >= 4 (above the first nonzero eigenvalue of the
-// Neumann y-operator on [-1, 1]) the lines are well conditioned and the
-// method matches the Thomas sweeps to round-off (forward error and residual
-// within a few ulps of the sequential sweeps, checked on the CPU for
-// ny = 12 ... 384).  Lines with a smaller shift -- the pinned mean mode among
-// them -- are solved by the sequential sweeps of k_ysolve_line with the
-// precomputed pivots (lane 0, same operations, same results).
-constexpr double kPartShiftMin = 4.0;
-
-// 1/x from the hardware FP64 reciprocal approximation (rcp.approx.ftz.f64)
-// refined by two Newton-Raphson steps r <- r + r (1 - x r), each of which
-// squares the relative error: full FP64 precision in one special-function
-// instruction and four FMAs instead of a correctly rounded division.
-__device__ __forceinline__ double rcp_nr(double x) {
-  double r;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
-  r = fma(r, fma(-x, r, 1.0), r);
-  r = fma(r, fma(-x, r, 1.0), r);
-  return r;
-}
-
-__host__ __device__ inline int ypart_count(int n) {
-  int P = 1;
-  while (P < 32 && n % (2 * P) == 0 && n / (2 * P) >= 2) P *= 2;
-  return P;
-}
-
-template <typename T, int M>
-__device__ __forceinline__ void ypart_line(typename Cplx<T>::type *X, const double *ca, const double *cb,
-                                           const double *cc, double shift, int P, int m, int Q, int lane) {
-  typedef typename Cplx<T>::type C;
-  const bool act = lane < P;
-  const unsigned full = 0xffffffffu;
-  double inv[M];
-  double ylr = 0.0, yli = 0.0, vl = 0.0, wl = 0.0, yfr = 0.0, yfi = 0.0, vf = 0.0, wf = 0.0;
-  double ae = 0.0, be = 1.0, ce = 0.0, rer = 0.0, rei = 0.0;
-  if (act) {
-    // top-down: x(m-2) = yl + vl L(p-1) + wl L(p)
-    double h = 0.0, yr = 0.0, yi = 0.0, v = 1.0, w = 0.0;
-#pragma unroll
-    for (int t = 0; t < M - 1; ++t) {
-      if (t < m - 1) {
-        const int s = t * Q + lane;
-        const double a = ca[s], b = cb[s] - shift, c = cc[s];
-        const C r = X[s];
-        const double iv = rcp_nr(b - a * h);
-        inv[t] = iv;
-        const bool last = t == m - 2;
-        yr = ((double)r.x - a * yr) * iv;
-        yi = ((double)r.y - a * yi) * iv;
-        v = (-a * v) * iv;
-        w = (-a * w - (last ? c : 0.0)) * iv;
-        h = (last ? 0.0 : c) * iv;
-      }
-    }
-    ylr = yr; yli = yi; vl = v; wl = w;
-    // bottom-up: x(0) = yf + vf L(p-1) + wf L(p)
-    h = 0.0; yr = 0.0; yi = 0.0; v = 0.0; w = 1.0;
-#pragma unroll
-    for (int t = M - 2; t >= 0; --t) {
-      if (t <= m - 2) {
-        const int s = t * Q + lane;
-        const double a = ca[s], b = cb[s] - shift, c = cc[s];
-        const C r = X[s];
-        const double iv = rcp_nr(b - c * h);
-        yr = ((double)r.x - c * yr) * iv;
-        yi = ((double)r.y - c * yi) * iv;
-        v = (-c * v - (t == 0 ? a : 0.0)) * iv;
-        w = (-c * w) * iv;
-        h = (t == 0 ? 0.0 : a) * iv;
-      }
-    }
-    yfr = yr; yfi = yi; vf = v; wf = w;
-    const int se = (m - 1) * Q + lane;
-    ae = ca[se]; be = cb[se] - shift; ce = cc[se];
-    const C re = X[se];
-    rer = re.x; rei = re.y;
-  }
-  // chunk-end equation of chunk p: ae x(m-2) + be L(p) + ce x_{p+1}(0) = re
-  const bool has_next = act && lane + 1 < P;
-  const int nxt = has_next ? lane + 1 : lane;
-  double ynr = __shfl_sync(full, yfr, nxt), yni = __shfl_sync(full, yfi, nxt);
-  double vn = __shfl_sync(full, vf, nxt), wn = __shfl_sync(full, wf, nxt);
-  if (!has_next) { ynr = 0.0; yni = 0.0; vn = 0.0; wn = 0.0; }  // the last row's APPH is 0
-  double Ap = ae * vl, Bp = ae * wl + be + ce * vn, Cp = ce * wn;
-  double Rr = rer - ae * ylr - ce * ynr, Ri = rei - ae * yli - ce * yni;
-  if (!act) { Ap = 0.0; Bp = 1.0; Cp = 0.0; Rr = 0.0; Ri = 0.0; }
-  for (int hs = 1; hs < P; hs <<= 1) {
-    const int lm = (lane - hs) & 31, lq = (lane + hs) & 31;
-    double Am = __shfl_sync(full, Ap, lm), Bm = __shfl_sync(full, Bp, lm), Cm = __shfl_sync(full, Cp, lm);
-    double Rmr = __shfl_sync(full, Rr, lm), Rmi = __shfl_sync(full, Ri, lm);
-    double Aq = __shfl_sync(full, Ap, lq), Bq = __shfl_sync(full, Bp, lq), Cq = __shfl_sync(full, Cp, lq);
-    double Rqr = __shfl_sync(full, Rr, lq), Rqi = __shfl_sync(full, Ri, lq);
-    if (lane - hs < 0) { Am = 0.0; Bm = 1.0; Cm = 0.0; Rmr = 0.0; Rmi = 0.0; }
-    if (lane + hs >= P) { Aq = 0.0; Bq = 1.0; Cq = 0.0; Rqr = 0.0; Rqi = 0.0; }
-    if (act) {
-      const double k1 = Ap * rcp_nr(Bm), k2 = Cp * rcp_nr(Bq);
-      const double nA = -Am * k1, nC = -Cq * k2, nB = Bp - Cm * k1 - Aq * k2;
-      Rr = Rr - Rmr * k1 - Rqr * k2;
-      Ri = Ri - Rmi * k1 - Rqi * k2;
-      Ap = nA; Bp = nB; Cp = nC;
-    }
-  }
-  const double ib = rcp_nr(Bp), Lr = Rr * ib, Li = Ri * ib;
-  double Lmr = __shfl_sync(full, Lr, (lane - 1) & 31), Lmi = __shfl_sync(full, Li, (lane - 1) & 31);
-  if (lane == 0) { Lmr = 0.0; Lmi = 0.0; }
-  if (act) {
-    // interior rows 0..m-2 with the chunk ends known: forward with the first
-    // sweep's pivots, g kept in the line's own slots, then back substitution
-    double gr = 0.0, gi = 0.0;
-#pragma unroll
-    for (int t = 0; t < M - 1; ++t) {
-      if (t < m - 1) {
-        const int s = t * Q + lane;
-        const double a = ca[s], c = cc[s];
-        const C r = X[s];
-        double qr = r.x, qi = r.y;
-        if (t == 0) { qr -= a * Lmr; qi -= a * Lmi; } else { qr -= a * gr; qi -= a * gi; }
-        if (t == m - 2) { qr -= c * Lr; qi -= c * Li; }
-        gr = qr * inv[t];
-        gi = qi * inv[t];
-        C o; o.x = (T)gr; o.y = (T)gi;
-        X[s] = o;
-      }
-    }
-    double xr = 0.0, xi = 0.0;
-#pragma unroll
-    for (int t = M - 2; t >= 0; --t) {
-      if (t <= m - 2) {
-        const int s = t * Q + lane;
-        const C g = X[s];
-        if (t == m - 2) {
-          xr = g.x; xi = g.y;
-        } else {
-          const double hq = cc[s] * inv[t];
-          xr = (double)g.x - hq * xr;
-          xi = (double)g.y - hq * xi;
-        }
-        C o; o.x = (T)xr; o.y = (T)xi;
-        X[s] = o;
-      }
-    }
-    C o; o.x = (T)Lr; o.y = (T)Li;
-    X[(m - 1) * Q + lane] = o;
-  }
-}
-
-// The sequential sweeps of k_ysolve_line on one staged line (lane 0 of the
-// warp): the same operations on the same values, with the pivots of
-// k_ypivots read from global memory a few rows ahead.
-template <typename T>
-__device__ __forceinline__ void yserial_line(const TGDev &d, typename Cplx<T>::type *X, int kx, int kz,
-                                             const int *slot) {
-  typedef typename Cplx<T>::type C;
-  const int ny = d.ny;
-  const int64_t base = kx + (int64_t)d.lp * ny * kz, st = d.lp;
-  const double *__restrict__ PP = reinterpret_cast<const double *>(d.ypiv) + base;
-  const double *__restrict__ HH = reinterpret_cast<const double *>(d.ypiv) + (int64_t)d.lp * ny * d.nz + base;
-  double gr = 0.0, gi = 0.0;
-  for (int j0 = 1; j0 <= ny; j0 += YB) {
-    double p[YB], a[YB];
-#pragma unroll
-    for (int u = 0; u < YB; ++u) {
-      const int j = j0 + u;
-      if (j <= ny) { p[u] = __ldg(PP + st * (j - 1)); a[u] = d.amph[j]; }
-    }
-#pragma unroll
-    for (int u = 0; u < YB; ++u) {
-      const int j = j0 + u;
-      if (j <= ny) {
-        const int s = slot[j - 1];
-        const C r = X[s];
-        if (j == 1) {
-          gr = (double)r.x * p[u];
-          gi = (double)r.y * p[u];
-        } else {
-          gr = ((double)r.x - a[u] * gr) * p[u];
-          gi = ((double)r.y - a[u] * gi) * p[u];
-        }
-        C o; o.x = (T)gr; o.y = (T)gi;
-        X[s] = o;
-      }
-    }
-  }
-  double xr = gr, xi = gi;
-  for (int j0 = ny - 1; j0 >= 1; j0 -= YB) {
-    double h[YB];
-#pragma unroll
-    for (int u = 0; u < YB; ++u) {
-      const int j = j0 - u;
-      if (j >= 1) h[u] = __ldg(HH + st * (j - 1));
-    }
-#pragma unroll
-    for (int u = 0; u < YB; ++u) {
-      const int j = j0 - u;
-      if (j >= 1) {
-        const int s = slot[j - 1];
-        const C r = X[s];
-        xr = (double)r.x - h[u] * xr;
-        xi = (double)r.y - h[u] * xi;
-        C o; o.x = (T)xr; o.y = (T)xi;
-        X[s] = o;
-      }
-    }
-  }
-}
-
-template <typename T>
-struct YPartShape {
-  typedef typename Cplx<T>::type C;
-  int P, m, Q, ls, L;
-  // 128-byte bank period in elements; lines ls = 1 (mod G) elements apart
-  static constexpr int G = 128 / (int)sizeof(C);
-  static YPartShape make(int ny) {
-    YPartShape y{};
-    y.P = ypart_count(ny);
-    y.m = ny / y.P;
-    y.Q = y.P + 1;
-    const int mq = y.m * y.Q;
-    y.ls = mq + ((1 - mq) % G + G) % G;
-    // lines per block: 8 (256 threads; a row of the block's lines is one
-    // 128-byte segment in FP64), fewer when the lines would take > 100 KB
-    y.L = 8;
-    while (y.L > 2 && (size_t)y.L * y.ls * sizeof(C) > 100 * 1024) y.L >>= 1;
-    return y;
-  }
-  size_t smem(int ny) const {
-    return (size_t)3 * m * Q * sizeof(double) + (size_t)L * ls * sizeof(C) + (size_t)ny * sizeof(int);
-  }
-  bool usable() const { return P >= 2 && m >= 2 && m <= 16; }
-};
-
-template <typename T, int M>
-__global__ void __launch_bounds__(256) k_ysolve_part(TGDev d, int P, int m, int L, int ls) {
-  typedef typename Cplx<T>::type C;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  const int Q = P + 1, mq = m * Q, ny = d.ny;
-  double *ca = reinterpret_cast<double *>(smem_raw), *cb = ca + mq, *cc = cb + mq;
-  C *lines = reinterpret_cast<C *>(cc + mq);
-  int *slot = reinterpret_cast<int *>(lines + (size_t)L * ls);  // slot of line element j
-  const int kz = blockIdx.y, kx0 = blockIdx.x * L;
-  const int nl = min(L, d.lh - kx0);
-  const int tid = threadIdx.x, nt = blockDim.x;
-  // the y-operator rows in the slot layout (no coupling beyond the walls)
-  for (int j = tid; j < ny; j += nt) {
-    const int s = (j % m) * Q + j / m;
-    slot[j] = s;
-    ca[s] = j == 0 ? 0.0 : d.amph[j + 1];
-    cb[s] = d.acph[j + 1];
-    cc[s] = j == ny - 1 ? 0.0 : d.apph[j + 1];
-  }
-  __syncthreads();
-  // staging: thread (w, j0) moves line w's rows j0, j0 + nt / L, ... (L is a
-  // power of two, nt = 32 L): each row of the block's lines is one segment
-  C *S = reinterpret_cast<C *>(d.spec) + kx0 + (int64_t)d.lp * ny * kz;
-  const int w = tid & (L - 1), jstep = nt / L;
-  if (w < nl)
-    for (int j = tid / L; j < ny; j += jstep) lines[w * ls + slot[j]] = S[(int64_t)d.lp * j + w];
-  __syncthreads();
-  const int warp = tid >> 5, lane = tid & 31;
-  if (warp < nl) {
-    const int kx = kx0 + warp;
-    const double shift = d.ak1[kx] + d.ak3[kz];
-    C *X = lines + warp * ls;
-    if (shift >= kPartShiftMin)
-      ypart_line<T, M>(X, ca, cb, cc, shift, P, m, Q, lane);
-    else if (lane == 0)
-      yserial_line<T>(d, X, kx, kz, slot);
-  }
-  __syncthreads();
-  if (w < nl)
-    for (int j = tid / L; j < ny; j += jstep) S[(int64_t)d.lp * j + w] = lines[w * ls + slot[j]];
-}
-
 // Inverse real transform along x (src/possion3d_FFT99.f90:461-485): the
 // block's lb spectral rows (contiguous, pitch lp) arrive by one bulk copy;
 // pairs of rows are rebuilt as one complex Hermitian-extended line and
@@ -1737,8 +1443,7 @@ template <typename T> struct Prec {
     const void *dyn[] = {(const void *)k_rhs_tma<T>,      (const void *)k_adix<T>,           (const void *)k_adiz<T>,
                          (const void *)k_fftx<T, false>,  (const void *)k_ifftx<T, false>,   (const void *)k_fftz<T, false>,
                          (const void *)k_fftx<T, true>,   (const void *)k_ifftx<T, true>,    (const void *)k_fftz<T, true>,
-                         (const void *)k_adiy_smem<T>,      (const void *)k_ysolve_part<T, 4>,
-                         (const void *)k_ysolve_part<T, 8>,  (const void *)k_ysolve_part<T, 16>};
+                         (const void *)k_adiy_smem<T>};
     for (const void *f : dyn) {
       cudaFuncAttributes fa;
       CK(cudaFuncGetAttributes(&fa, f));
@@ -1775,20 +1480,8 @@ template <typename T> struct Prec {
     }
     if (mark) phase_mark(c, CHAPSIM_PH_YSOLVE);
     {
-      const YPartShape<T> y = YPartShape<T>::make(d.ny);
-      if (y.usable()) {
-        dim3 grid((d.lh + y.L - 1) / y.L, d.nz);
-        const size_t sm = y.smem(d.ny);
-        if (y.m <= 4)
-          k_ysolve_part<T, 4><<<grid, 32 * y.L, sm, c->stream>>>(d, y.P, y.m, y.L, y.ls);
-        else if (y.m <= 8)
-          k_ysolve_part<T, 8><<<grid, 32 * y.L, sm, c->stream>>>(d, y.P, y.m, y.L, y.ls);
-        else
-          k_ysolve_part<T, 16><<<grid, 32 * y.L, sm, c->stream>>>(d, y.P, y.m, y.L, y.ls);
-      } else {
-        dim3 grid((d.lh + 127) / 128, d.nz);
-        k_ysolve_line<T><<<grid, 128, 0, c->stream>>>(d);
-      }
+      dim3 grid((d.lh + 127) / 128, d.nz);
+      k_ysolve_line<T><<<grid, 128, 0, c->stream>>>(d);
       LAUNCHED();
     }
     if (mark) phase_mark(c, CHAPSIM_PH_IFFTZ);
