@@ -508,7 +508,7 @@ def run_compare(args, wl, ws, rank, local):
     out_bins, out_err = eng.gate_outputs()
 
     # ---- the mixed form with the learned properties
-    mix = make(cs.MIXED)
+    mix = make(cs.MIXED if args.spectra == "fp32" else cs.FP64)
     mix.set_refinement(args.refine)
     mix.set_props_mode(1, eng)
     mix.random_fl_theml_fld_io(b["seed"] + rank, 0.1)
@@ -607,14 +607,16 @@ def run_compare(args, wl, ws, rank, local):
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f64 fields, f32 Poisson spectra, bf16 hi/lo tensor-core property model (f32 accumulate)",
+            "dtype": (f"f64 fields, {args.spectra} Poisson spectra, bf16 hi/lo tensor-core property model "
+                      "(f32 accumulate)"),
             "data": "synthetic (seeded splitmix64 velocity, h = 0, synthetic 4096-point table, NS=0 projection)",
             "config": workload_config(args, wl),
             "arm": {"parallelism": f"replicas x{ws}" if ws > 1 else "single GPU",
                     "l2": "working set (>40 GB) larger than the 126 MB L2"},
             "fp64": {"value": value64, "ms_per_step": ms64 / args.steps, "max_div_g_plus_drho": div64,
                      "form": "plain FP64, table splines"},
-            "mixed_form": {"poisson_spectra": "fp32", "fp64_residual_refinement_sweeps": args.refine},
+            "mixed_form": {"poisson_spectra": args.spectra,
+                           "fp64_residual_refinement_sweeps": args.refine if args.spectra == "fp32" else 0},
             "ratio_vs_fp64": value / value64,
             "max_div_g_plus_drho": divmix, "out_of_table_cells": bad,
             "error_vs_fp64": {"after_steps": args.warmup + args.steps, "relative_max": errors},
@@ -1267,6 +1269,8 @@ def main():
                     help="seconds of host work the reference arm's W + K steps are sized to")
     ap.add_argument("--refine", type=int, choices=[0, 1], default=1,
                     help="FP64-residual refinement sweeps of the mixed IO form's Poisson solve")
+    ap.add_argument("--spectra", choices=["fp32", "fp64"], default="fp32",
+                    help="precision of the Poisson spectra of the learned-property IO form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-props", action="store_true", help="skip the learned-property measurement")
     ap.add_argument("--profile-case", default=None, metavar="NXxNYxNZ",

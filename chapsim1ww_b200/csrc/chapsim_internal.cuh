@@ -222,7 +222,7 @@ int io_restart_fields(chapsim_ctx *c);
 // or the model; kernel attributes; persistent grid size
 int io_therm_props(chapsim_ctx *c, int mode);
 int mlp_kernel_setup(chapsim_ctx *c);
-int mlp_grid(const chapsim_ctx *c);
+int mlp_grid(const chapsim_ctx *c, int per_sm);
 // the trained model of a property engine and its table (props.cu)
 int props_model(const chapsim_props *pe, chapsim_mlp::MlpDev *out, int *device);
 bool props_same_table(const chapsim_props *pe, const std::vector<double> *cols5);

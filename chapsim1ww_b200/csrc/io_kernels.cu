@@ -272,21 +272,28 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_props_only(TGDev d, IODev i
 // ------------------------------------------------------ learned properties
 // The property update of SOLVERRK3_ENG_IO (:46-55) with the learned model
 // (mlp_tc.cuh) in place of the table splines: VISCOUSITY0 / DENSITY0 <-
-// VISCOUSITY / DENSITY, then DENSITY_UPDATE on h = rho h / rho_old (the
-// model's rho), ENTHALPY_UPDATE, and THERM_PROP_UPDATE on the new h (the
-// model's T, rho, mu, k).  Cells whose h-bin the error gate has not cleared
-// for all four take the table splines, as do out-of-table checks.  The
-// field is walked as a flat array in 128-cell tiles (ghost rows keep the
-// plain kernel's treatment: mu0, rho0 and mu0 + mu only); every tile runs the
-// model twice on the tensor cores.
-__global__ void __launch_bounds__(chapsim_mlp::TILE, 4) k_io_eng_props_mlp(TGDev d, IODev io, chapsim_mlp::MlpDev M) {
+// VISCOUSITY / DENSITY, then DENSITY_UPDATE on h1 = rho h / rho_old (the
+// model's rho), ENTHALPY_UPDATE h2 = rho h / rho_new, and THERM_PROP_UPDATE
+// on h2 (the model's T, rho, mu, k).  Cells whose h-bin the error gate has
+// not cleared for all four take the table splines, as do out-of-table
+// checks.  The field is walked as a flat array in 128-cell tiles (ghost rows
+// keep the plain kernel's treatment: mu0, rho0 and mu0 + mu only).
+// The model is evaluated once per tile, at h1, with its derivative (forward
+// mode on the tensor cores, tile_eval_d); the properties at h2 come from the
+// first-order expansion of the network's residual around h1 plus the exact
+// polynomial base at h2.  h2 differs from h1 by the density change of one
+// substep (|dx| ~ 1e-4); a tile in which any model cell moves further than
+// kTaylorMax evaluates the model a second time at h2.  This halves the tanh
+// evaluations, which bound the kernel on the special-function unit.
+__global__ void __launch_bounds__(chapsim_mlp::TILE, 3) k_io_eng_props_mlp(TGDev d, IODev io, chapsim_mlp::MlpDev M) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  chapsim_mlp::Smem &s = chapsim_mlp::smem_of(smem_raw);
+  chapsim_mlp::SmemD &s = chapsim_mlp::smem_of<chapsim_mlp::SmemD>(smem_raw);
   chapsim_mlp::cta_setup(s, M);
   uint32_t phase = 0;
   const int64_t n = d.sz * d.nz;
   const int64_t ntiles = (n + chapsim_mlp::TILE - 1) / chapsim_mlp::TILE;
   const int64_t rows = d.ny + 2;
+  const double hinv = 1.0 / M.hhalf;
   for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const int64_t c = tile * chapsim_mlp::TILE + threadIdx.x;
     const bool valid = c < n;
@@ -303,9 +310,9 @@ __global__ void __launch_bounds__(chapsim_mlp::TILE, 4) k_io_eng_props_mlp(TGDev
     }
     // DENSITY_UPDATE
     const double h1 = rh / dold;
-    const double x1 = (h1 - M.hmid) / M.hhalf;
-    float y[chapsim_mlp::NO];
-    if (!chapsim_mlp::tile_eval(s, (float)x1, y, phase, d.err)) break;
+    const double x1 = (h1 - M.hmid) * hinv;
+    float y[chapsim_mlp::NO], dy[chapsim_mlp::NO];
+    if (!chapsim_mlp::tile_eval_d(s, (float)x1, y, dy, phase, d.err)) break;
     int bad = 0;
     double D = dold;
     if (interior) {
@@ -319,23 +326,33 @@ __global__ void __launch_bounds__(chapsim_mlp::TILE, 4) k_io_eng_props_mlp(TGDev
         ++bad;
       }
     }
-    // ENTHALPY_UPDATE + THERM_PROP_UPDATE
+    // ENTHALPY_UPDATE; the model at h2 by expansion or, for a far step, anew
     const double h2 = rh / D;
-    const double x2 = (h2 - M.hmid) / M.hhalf;
-    if (!chapsim_mlp::tile_eval(s, (float)x2, y, phase, d.err)) break;
+    const double x2 = (h2 - M.hmid) * hinv;
+    const bool keep = io.shortcuts && fabs(h2) < 1.0e-10;
+    const bool model2 = interior && !keep && chapsim_spl::inside(io.ht, h2) &&
+                        (chapsim_mlp::gate_mask(M, h2) & chapsim_mlp::kStepMask) == chapsim_mlp::kStepMask;
+    const bool again = __syncthreads_or(model2 && fabs(x2 - x1) > chapsim_mlp::kTaylorMax);
+    float y2[chapsim_mlp::NO];
+    if (again) {
+      if (!chapsim_mlp::tile_eval(s, (float)x2, y2, phase, d.err)) break;
+    } else {
+#pragma unroll
+      for (int q = 0; q < chapsim_mlp::NO; ++q) y2[q] = y[q] + dy[q] * (float)(x2 - x1);
+    }
     if (!interior) continue;
     io.h[c] = h2;
     double munew = muold;
-    if (!(io.shortcuts && fabs(h2) < 1.0e-10)) {
+    if (!keep) {
       double T, M2, K, D2;
-      bool ok = chapsim_spl::inside(io.ht, h2);
-      if (ok && (chapsim_mlp::gate_mask(M, h2) & chapsim_mlp::kStepMask) == chapsim_mlp::kStepMask) {
-        T = chapsim_mlp::assemble(M, 0, x2, y[0]);
-        D2 = chapsim_mlp::assemble(M, 1, x2, y[1]);
-        M2 = chapsim_mlp::assemble(M, 2, x2, y[2]);
-        K = chapsim_mlp::assemble(M, 3, x2, y[3]);
+      bool ok = model2;
+      if (model2) {
+        T = chapsim_mlp::assemble(M, 0, x2, y2[0]);
+        D2 = chapsim_mlp::assemble(M, 1, x2, y2[1]);
+        M2 = chapsim_mlp::assemble(M, 2, x2, y2[2]);
+        K = chapsim_mlp::assemble(M, 3, x2, y2[3]);
       } else {
-        ok = ok && look_ht(io, h2, T) && look_tprops(io, T, D2, M2, K);
+        ok = look_ht(io, h2, T) && look_tprops(io, T, D2, M2, K);
       }
       if (ok) {
         io.T[c] = T;
@@ -1110,14 +1127,15 @@ int io_thermal_bc(chapsim_ctx *c) {
 }
 
 // The learned-property kernels take more than 48 KB of dynamic shared memory
-// (set once per context) and run persistently, four CTAs of 128 threads per
-// SM (their tensor-memory columns fill the SM's 512).
+// (set once per context) and run persistently, three (energy substep, with
+// the derivative tile) or four CTAs of 128 threads per SM; each CTA holds 128
+// of the SM's 512 tensor-memory columns.
 int mlp_kernel_setup(chapsim_ctx *c) {
   if (c->mlp_smem_set) return CHAPSIM_OK;
   const void *fns[] = {(const void *)k_io_eng_props_mlp, (const void *)k_io_therm_props};
-  for (const void *f : fns)
-    if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)chapsim_mlp::kSmemBytes) !=
-        cudaSuccess) {
+  const size_t bytes[] = {chapsim_mlp::kSmemDBytes, chapsim_mlp::kSmemBytes};
+  for (int q = 0; q < 2; ++q)
+    if (cudaFuncSetAttribute(fns[q], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes[q]) != cudaSuccess) {
       cudaGetLastError();
       c->err = "learned properties: cannot raise the shared-memory limit";
       return CHAPSIM_ERR_CUDA;
@@ -1126,11 +1144,11 @@ int mlp_kernel_setup(chapsim_ctx *c) {
   return CHAPSIM_OK;
 }
 
-int mlp_grid(const chapsim_ctx *c) {
+int mlp_grid(const chapsim_ctx *c, int per_sm) {
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
   const int64_t tiles = (c->d.sz * c->d.nz + chapsim_mlp::TILE - 1) / chapsim_mlp::TILE;
-  return (int)std::min<int64_t>(tiles, (int64_t)nsm * 4);
+  return (int)std::min<int64_t>(tiles, (int64_t)nsm * per_sm);
 }
 
 // Phase-timer slots of an IO substep, in execution order: 0 energy RHS,
@@ -1147,7 +1165,7 @@ int io_eng(chapsim_ctx *c, int ns) {
   if (c->props_mode == CHAPSIM_PROPS_MLP) {
     int rc = mlp_kernel_setup(c);
     if (rc) return rc;
-    k_io_eng_props_mlp<<<mlp_grid(c), chapsim_mlp::TILE, chapsim_mlp::kSmemBytes, c->stream>>>(d, c->io, c->mlp);
+    k_io_eng_props_mlp<<<mlp_grid(c, 3), chapsim_mlp::TILE, chapsim_mlp::kSmemDBytes, c->stream>>>(d, c->io, c->mlp);
   } else {
     k_io_eng_props<<<g2, dim3(IO_BX, IO_BY), 0, c->stream>>>(d, c->io);
   }
@@ -1159,7 +1177,7 @@ int io_therm_props(chapsim_ctx *c, int mode) {
   int rc = mlp_kernel_setup(c);
   if (rc) return rc;
   const bool mlp = mode == CHAPSIM_PROPS_MLP;
-  k_io_therm_props<<<mlp_grid(c), chapsim_mlp::TILE, mlp ? chapsim_mlp::kSmemBytes : 0, c->stream>>>(
+  k_io_therm_props<<<mlp_grid(c, 4), chapsim_mlp::TILE, mlp ? chapsim_mlp::kSmemBytes : 0, c->stream>>>(
       c->d, c->io, c->mlp, mlp ? 1 : 0);
   LAUNCHED();
   return CHAPSIM_OK;

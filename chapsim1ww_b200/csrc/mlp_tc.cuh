@@ -79,6 +79,12 @@ struct __align__(1024) Smem {
   int fail;
 };
 
+// The same plus one BF16 operand tile for the forward-mode derivative of the
+// activations (tile_eval_d): 16 KB more, three CTAs per SM.
+struct __align__(1024) SmemD : Smem {
+  uint16_t d_hi[TILE * NH];
+};
+
 // ---------------------------------------------------------------- PTX
 __device__ __forceinline__ float tanh_approx(float x) {
   float y;
@@ -179,11 +185,13 @@ __device__ __forceinline__ void store_split(Smem &s, int r, const float *a) {
 
 // The CTA's Smem inside its dynamic shared memory, placed on a 1024-byte
 // boundary (the kernels request sizeof(Smem) + 1024 bytes).
-__device__ __forceinline__ Smem &smem_of(unsigned char *raw) {
+template <class S = Smem>
+__device__ __forceinline__ S &smem_of(unsigned char *raw) {
   const uint32_t a = smem_u32(raw);
-  return *reinterpret_cast<Smem *>(raw + ((1024u - (a & 1023u)) & 1023u));
+  return *reinterpret_cast<S *>(raw + ((1024u - (a & 1023u)) & 1023u));
 }
 constexpr size_t kSmemBytes = sizeof(Smem) + 1024;
+constexpr size_t kSmemDBytes = sizeof(SmemD) + 1024;
 
 // ------------------------------------------------------------ CTA set-up
 // Load the weights into shared memory, initialise the mbarrier and allocate
@@ -226,8 +234,9 @@ __device__ __forceinline__ void cta_teardown(Smem &s) {
 }
 
 // Issue one layer: D[:, 0:n) = A_hi W_hi^T + A_hi W_lo^T + A_lo W_hi^T over
-// K = 64 (four K = 16 steps each), then commit to the barrier.
-__device__ __forceinline__ void issue_layer(Smem &s, uint32_t dtm, const uint16_t *w_hi, const uint16_t *w_lo, int n) {
+// K = 64 (four K = 16 steps each), then (commit) commit to the barrier.
+__device__ __forceinline__ void issue_layer(Smem &s, uint32_t dtm, const uint16_t *w_hi, const uint16_t *w_lo, int n,
+                                            bool commit = true) {
   const uint32_t idesc = idesc_bf16(TILE, n);
   const uint32_t ah = smem_u32(s.a_hi), al = smem_u32(s.a_lo), bh = smem_u32(w_hi), bl = smem_u32(w_lo);
   const uint32_t as[3] = {ah, ah, al}, bs[3] = {bh, bl, bh};
@@ -236,7 +245,31 @@ __device__ __forceinline__ void issue_layer(Smem &s, uint32_t dtm, const uint16_
 #pragma unroll
     for (int ks = 0; ks < 4; ++ks)
       umma(dtm, sdesc(as[part] + 256u * ks), sdesc(bs[part] + 256u * ks), idesc, (part | ks) ? 1u : 0u);
-  umma_commit(&s.bar);
+  if (commit) umma_commit(&s.bar);
+}
+
+// One plain BF16 chain D[:, 0:n) = A W^T (K = 64) from the operand tiles a and w.
+__device__ __forceinline__ void issue_chain(uint32_t dtm, const uint16_t *a, const uint16_t *w, int n) {
+  const uint32_t idesc = idesc_bf16(TILE, n);
+  const uint32_t aa = smem_u32(a), bb = smem_u32(w);
+#pragma unroll
+  for (int ks = 0; ks < 4; ++ks) umma(dtm, sdesc(aa + 256u * ks), sdesc(bb + 256u * ks), idesc, ks ? 1u : 0u);
+}
+
+// Round 32 values to BF16 (nearest-even, integer pipe) into columns
+// c0 .. c0 + 31 of row r of a single operand tile.
+__device__ __forceinline__ void store_bf16_32(uint16_t *tile, int r, int c0, const float *v) {
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    uint32_t w[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t b0 = __float_as_uint(v[8 * c + 2 * q]), b1 = __float_as_uint(v[8 * c + 2 * q + 1]);
+      w[q] = __byte_perm(b0 + 0x7FFFu + ((b0 >> 16) & 1u), b1 + 0x7FFFu + ((b1 >> 16) & 1u), 0x7632);
+    }
+    *reinterpret_cast<uint4 *>(reinterpret_cast<char *>(tile) + tile_off(r, c0 + 8 * c)) =
+        make_uint4(w[0], w[1], w[2], w[3]);
+  }
 }
 
 // Block-uniform bounded wait for the layer's commit: false on every thread
@@ -290,7 +323,84 @@ __device__ __forceinline__ bool tile_eval(Smem &s, float x, float (&y)[NO], uint
   return true;
 }
 
-// Assemble output o from the standardised residual y at input x (FP64).
+// The model at x together with its derivative with respect to x, by forward
+// mode through the same layers: da1 = (1 - a1^2) w1, dz2 = W2 da1,
+// da2 = (1 - a2^2) dz2, dy = W3 da2.  The values are computed exactly as in
+// tile_eval; the derivative products run as one plain BF16 chain per layer
+// next to the value chains (the derivative only ever multiplies a step of at
+// most kTaylorMax, so its ~4e-3 relative precision adds below 1e-5).  Tensor
+// memory: z2 in columns 0..63 and dz2 in 64..127, then y in 0..15 and dy in
+// 16..31.  Every thread of the CTA calls it together; false when a wait ran
+// out.
+__device__ __forceinline__ bool tile_eval_d(SmemD &s, float x, float (&y)[NO], float (&dy)[NO], uint32_t &phase,
+                                            int *err) {
+  const int r = threadIdx.x;
+  const uint32_t lane_base = s.tmem + ((uint32_t)(r & ~31) << 16);
+  float a[NH];
+#pragma unroll
+  for (int k = 0; k < NH; ++k) a[k] = tanh_approx(fmaf(s.w1[k], x, s.b1[k]));
+  store_split(s, r, a);
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    float t[32];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) t[k] = (1.f - a[32 * h + k] * a[32 * h + k]) * s.w1[32 * h + k];
+    store_bf16_32(s.d_hi, r, 32 * h, t);
+  }
+  chapsim::fence_proxy_async();
+  tc_fence_before();
+  __syncthreads();
+  if (r == 0) {
+    tc_fence_after();
+    issue_layer(s, s.tmem, s.w2_hi, s.w2_lo, NH, false);
+    issue_chain(s.tmem + NH, s.d_hi, s.w2_hi, NH);
+    umma_commit(&s.bar);
+  }
+  if (!layer_wait(s, phase, err)) return false;
+  tmem_ld32(lane_base, a);
+  tmem_ld32(lane_base + 32, a + 32);
+#pragma unroll
+  for (int k = 0; k < NH; ++k) a[k] = tanh_approx(a[k] + s.b2[k]);
+  store_split(s, r, a);  // the layer-2 MMAs have completed: the tiles are free
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    float t[32];
+    tmem_ld32(lane_base + NH + 32 * h, t);
+#pragma unroll
+    for (int k = 0; k < 32; ++k) t[k] *= 1.f - a[32 * h + k] * a[32 * h + k];
+    store_bf16_32(s.d_hi, r, 32 * h, t);
+  }
+  chapsim::fence_proxy_async();
+  tc_fence_before();
+  __syncthreads();
+  if (r == 0) {
+    tc_fence_after();
+    issue_layer(s, s.tmem, s.w3_hi, s.w3_lo, NOP, false);
+    issue_chain(s.tmem + NOP, s.d_hi, s.w3_hi, NOP);
+    umma_commit(&s.bar);
+  }
+  if (!layer_wait(s, phase, err)) return false;
+  float o[8], od[8];
+  tmem_ld8(lane_base, o);
+  tmem_ld8(lane_base + NOP, od);
+#pragma unroll
+  for (int q = 0; q < NO; ++q) {
+    y[q] = o[q] + s.b3[q];
+    dy[q] = od[q];
+  }
+  tc_fence_before();
+  return true;
+}
+
+// Largest step |x_new - x_old| over which a tile takes the properties at the
+// second enthalpy from the first-order expansion of the model's residual
+// (the polynomial base is evaluated exactly): the dropped second-order term is
+// below std_o |y''| dx^2 / 2, about 1e-5 of each property's range for the
+// model's curvature here; a larger step in any cell of the tile evaluates the
+// model a second time.
+constexpr double kTaylorMax = 1e-3;
+
+// Assemble output o from the standardised residual y at input x (FP64).// Assemble output o from the standardised residual y at input x (FP64).
 __device__ __forceinline__ double assemble(const MlpDev &M, int o, double x, float y) {
   double b = M.base[o][NBASE - 1];
 #pragma unroll
