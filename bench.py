@@ -528,6 +528,7 @@ def run_compare(args, wl, ws, rank, local):
     value64 = cells * ws * args.steps / (ms64 / 1000.0)
     divmix = mix.divgck_io()
     bad = mix.bad_cells()
+    again = mix.model_again_tiles()
 
     # error of the mixed + learned form against the FP64 form after the same
     # W + K steps from the same state (on the device)
@@ -619,6 +620,8 @@ def run_compare(args, wl, ws, rank, local):
                            "fp64_residual_refinement_sweeps": args.refine if args.spectra == "fp32" else 0},
             "ratio_vs_fp64": value / value64,
             "max_div_g_plus_drho": divmix, "out_of_table_cells": bad,
+            "model_second_evaluations": {"tiles": again, "of": 3 * (args.warmup + args.steps + 1) *
+                                         ((nx * (ny + 2) * nz + 127) // 128)},
             "error_vs_fp64": {"after_steps": args.warmup + args.steps, "relative_max": errors},
             "property_model": {"train_s": t_train, "train_loss": loss, "gate_tol": 1e-4, "bins": 256,
                                "bins_cleared_T_rho_mu_k": nbins, "max_rel_err_T_rho_mu_k": worst,
@@ -1269,7 +1272,7 @@ def main():
                     help="seconds of host work the reference arm's W + K steps are sized to")
     ap.add_argument("--refine", type=int, choices=[0, 1], default=1,
                     help="FP64-residual refinement sweeps of the mixed IO form's Poisson solve")
-    ap.add_argument("--spectra", choices=["fp32", "fp64"], default="fp32",
+    ap.add_argument("--spectra", choices=["fp32", "fp64"], default="fp64",
                     help="precision of the Poisson spectra of the learned-property IO form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-props", action="store_true", help="skip the learned-property measurement")

@@ -534,9 +534,10 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
       io.bcp = (double *)p;
       io.bcs = io.bcp + (size_t)io.bps * CHAPSIM_P_COUNT;
       cudaMemsetAsync(p, 0, ((size_t)io.bps * CHAPSIM_P_COUNT + 8) * sizeof(double), ctx->stream);
-      if ((rc = dalloc(ctx, &p, sizeof(unsigned long long)))) goto fail;
+      if ((rc = dalloc(ctx, &p, 2 * sizeof(unsigned long long)))) goto fail;
       io.bad = (unsigned long long *)p;
-      cudaMemsetAsync(p, 0, sizeof(unsigned long long), ctx->stream);
+      io.model_again = io.bad + 1;
+      cudaMemsetAsync(p, 0, 2 * sizeof(unsigned long long), ctx->stream);
       io.thermal = iocfg->thermal ? 1 : 0;
       io.cthecd = 1.0 / cfg->ren / iocfg->prt;  // CTHECD, src/Flow_State.f90:87
       io.qw_bot = iocfg->qw_bot;
@@ -1334,9 +1335,10 @@ int chapsim_reduce(chapsim_ctx *ctx, int domain, int what, double *out) {
   REQUIRE(domain == ctx->domain, CHAPSIM_ERR_ARG, "domain does not match the context");
   CKC(cudaSetDevice(ctx->device));
   if (domain == CHAPSIM_IIO) {
-    if (what == CHAPSIM_R_BADCELLS) {
+    if (what == CHAPSIM_R_BADCELLS || what == CHAPSIM_R_MODEL_AGAIN) {
       unsigned long long b = 0;
-      CKC(cudaMemcpyAsync(&b, ctx->io.bad, sizeof(b), cudaMemcpyDeviceToHost, ctx->stream));
+      CKC(cudaMemcpyAsync(&b, what == CHAPSIM_R_BADCELLS ? ctx->io.bad : ctx->io.model_again, sizeof(b),
+                          cudaMemcpyDeviceToHost, ctx->stream));
       CKC(cudaStreamSynchronize(ctx->stream));
       *out = (double)b;
       return CHAPSIM_OK;

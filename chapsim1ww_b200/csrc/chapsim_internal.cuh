@@ -64,6 +64,7 @@ struct IODev {
   double *dpg;       // device scalar: DPGRNS of the current substep
   double *part;      // per-block partial sums of the x mass-flux forcing
   unsigned long long *bad;  // table look-ups outside the table
+  unsigned long long *model_again;  // learned-property tiles evaluated a second time
   // semi-implicit viscous scheme (visthemflg = 1): DRHOI_STG per component
   // and the wall coefficients AMVR1 / APVRN of TDMA_COEF
   int visc;

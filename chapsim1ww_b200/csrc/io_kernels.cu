@@ -334,6 +334,7 @@ __global__ void __launch_bounds__(chapsim_mlp::TILE, 3) k_io_eng_props_mlp(TGDev
                         (chapsim_mlp::gate_mask(M, h2) & chapsim_mlp::kStepMask) == chapsim_mlp::kStepMask;
     const bool again = __syncthreads_or(model2 && fabs(x2 - x1) > chapsim_mlp::kTaylorMax);
     float y2[chapsim_mlp::NO];
+    if (again && threadIdx.x == 0) atomicAdd(io.model_again, 1ull);
     if (again) {
       if (!chapsim_mlp::tile_eval(s, (float)x2, y2, phase, d.err)) break;
     } else {

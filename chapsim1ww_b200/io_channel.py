@@ -133,6 +133,11 @@ class IOChannel(TGChannel):
     def bulk_h_io(self):
         return self._reduce(_lib.R_BULK_H)
 
+    def model_again_tiles(self):
+        """Learned-property tiles whose second enthalpy took a second model
+        evaluation (a step beyond the first-order expansion's range)."""
+        return int(self._reduce(8))
+
     def bad_cells(self):
         return int(self._reduce(_lib.R_BADCELLS))
 

@@ -378,6 +378,9 @@ int chapsim_io_bc_scalars(chapsim_ctx *io, double *out, int n);
 #define CHAPSIM_R_BULK_G 4   /* BULK_MASSFLUX_IO                           */
 #define CHAPSIM_R_BULK_H 5   /* BULK_H_IO                                  */
 #define CHAPSIM_R_BADCELLS 6 /* table look-ups outside the table so far    */
+#define CHAPSIM_R_MODEL_AGAIN 8 /* learned properties: 128-cell tiles whose second
+                                   enthalpy was evaluated anew rather than by the
+                                   first-order expansion, so far              */
 
 typedef struct chapsim_io_config {
   int32_t struct_size; /* sizeof(chapsim_io_config)                               */
