@@ -10,12 +10,13 @@ Default workload (c4_mixed_learned): the metric's comparison on the large
 single domain, io_1024x384x512 (201 M cells, Lx = 8 pi, Lz = 2 pi, tanh
 stretching beta = 2, Re_b = 10,000, dt = 1e-3, heated with the synthetic
 4096-point property table, wall heat flux 1, Pr 0.71, seed 4).  The plain
-FP64 form with the table splines and the mixed form (FP32 Poisson spectra,
-one FP64-residual refinement sweep) with the learned property model (trained
-on the GPU on 65,536 table samples, seed 2, gated at 1e-4 over 256 h-bins)
-advance the same seeded state; `value` is the mixed + learned form's
-cell-steps/s, the FP64 form's figure and their ratio ride along, with the
-mixed + learned form's error against the FP64 form at full size.
+FP64 form with the table splines and the learned form (the property model,
+trained on the GPU on 65,536 table samples, seed 2, gated at 1e-4 over 256
+h-bins, in place of the splines; FP64 Poisson spectra, or with --spectra fp32
+the mixed form's FP32 spectra plus one FP64-residual refinement sweep)
+advance the same seeded state; `value` is the learned form's cell-steps/s,
+the FP64 form's figure and their ratio ride along, with the learned form's
+error against the FP64 form at full size.
 Synthetic seeded initial fields (no public dataset is involved).  With N > 1
 GPUs every rank advances its own independent copy (replicas, weak scaling,
 no data-path collective); timing is the max over ranks.  Other workloads:
@@ -93,12 +94,12 @@ PHASE_KERNEL = {"rhs": "k_rhs_tma", "adix": "k_adixz_row", "adiz": "k_adixz_row"
 # IO substep phases (the library's IO timer slots, in execution order) and
 # their algorithmic 8-byte values per cell (thermal form): energy RHS reads
 # h, T, k, G, G0, rho h, R0 and writes rho h, R0; the property update reads
-# rho h, rho, mu and writes mu0, rho0, rho, h, T, mu, k; prep reads G, G0,
+# rho h, rho, mu and writes mu0, rho0, rho, h, T, mu, k, mu0 + mu; prep reads G, G0,
 # rho, rho0 and writes u, v, w, DrhoDtP; the momentum RHS reads u, v, w, G,
 # mu, mu0, p, EXPLT0 and writes EXPLT0 and G*; the x-transform reads G* and
 # DrhoDtP and writes RHSLLPHI; the correction reads G*, phi, p and writes G, p.
 IO_PHASES = ["eng_rhs", "eng_props", "prep", "mom_rhs", "fftx", "fftz", "ysolve", "ifftz", "ifftx", "corr"]
-IO_VALUES_PER_CELL = {"eng_rhs": 13, "eng_props": 10, "prep": 12, "mom_rhs": 17, "fftx": 5, "corr": 9}
+IO_VALUES_PER_CELL = {"eng_rhs": 13, "eng_props": 11, "prep": 12, "mom_rhs": 17, "fftx": 5, "corr": 9}
 IO_KERNEL = {"eng_rhs": "k_io_eng_rhs", "eng_props": "k_io_eng_props", "prep": "k_io_prep",
              "mom_rhs": "k_io_rhs_tma", "fftx": "k_fftx", "fftz": "k_fftz", "ysolve": "k_ysolve_line",
              "ifftz": "k_fftz", "ifftx": "k_ifftx", "corr": "k_io_corr"}
@@ -456,13 +457,14 @@ def run_io(args, wl, ws, rank, local):
 
 def run_compare(args, wl, ws, rank, local):
     """The metric's comparison: the same IO channel advanced by the plain FP64
-    form (table splines) and by the mixed form (FP32 Poisson spectra with an
-    FP64-residual refinement sweep) with the learned property model on the
-    tensor cores, K graph-replayed steps each after W warm-up steps, both
-    from the same seeded state.  value = the mixed + learned form's
-    cell-steps/s; the FP64 form's figure, their ratio, the property model's
-    gate and the mixed + learned form's error against the FP64 form at full
-    size (u, p, T, max |div|) ride along."""
+    form (table splines) and by the learned form (the property model on the
+    tensor cores in place of the splines; FP64 Poisson spectra, or FP32
+    spectra with an FP64-residual refinement sweep when args.spectra is
+    "fp32"), K graph-replayed steps each after W warm-up steps, both from
+    the same seeded state.  value = the learned form's cell-steps/s; the
+    FP64 form's figure, their ratio, the property model's gate and the
+    learned form's error against the FP64 form at full size (u, p, T,
+    max |div|) ride along."""
     import torch
 
     import chapsim1ww_b200 as cs
@@ -530,7 +532,7 @@ def run_compare(args, wl, ws, rank, local):
     bad = mix.bad_cells()
     again = mix.model_again_tiles()
 
-    # error of the mixed + learned form against the FP64 form after the same
+    # error of the learned form against the FP64 form after the same
     # W + K steps from the same state (on the device)
     def field(ch, name):
         t = torch.empty(ch.shape, dtype=torch.float64, device=f"cuda:{local}")
@@ -547,7 +549,7 @@ def run_compare(args, wl, ws, rank, local):
     ref.close()
     del ref
 
-    # per-phase kernel times of the mixed + learned form
+    # per-phase kernel times of the learned form
     mix.phase_timing(True)
     mix.phase_reset()
     mix.step(max(1, min(args.steps, 5)))
@@ -557,16 +559,23 @@ def run_compare(args, wl, ws, rank, local):
     dom = max(per_launch, key=per_launch.get)
     peak, peak_kind = measured_peak()
     bytes_dom = io_phase_bytes(dom, nx, ny, nz)
-    if dom in PHASE_SPECTRAL_PASSES or dom == "fftx":
+    if args.spectra == "fp32" and (dom in PHASE_SPECTRAL_PASSES or dom == "fftx"):
         bytes_dom -= PHASE_SPECTRAL_PASSES.get(dom, 0) * 2 * 4 * (nx // 2 + 1) * ny * nz  # FP32 spectra
     achieved = bytes_dom / (per_launch[dom] / 1000.0) / 1e9
     kern = IO_KERNEL[dom] if dom != "eng_props" else "k_io_eng_props_mlp"
-    # the learned-property kernel: two model evaluations per cell, 2 x 3 BF16
-    # MMAs of 128 x 64 x 64 (layer 2) and 128 x 16 x 64 (layer 3) per tile
-    mlp_flops = cells * 2 * 3 * 2 * 64 * (64 + 16)
+    # the learned-property kernel: one model evaluation per cell with its
+    # forward-mode derivative; per 128-cell tile three BF16 hi/lo MMA chains
+    # plus one derivative chain for layer 2 (128 x 64 x 64) and for layer 3
+    # (128 x 16 x 64); a tile that evaluates the model a second time adds
+    # three chains per layer and 128 more tanh per cell
+    ntiles = (nx * (ny + 2) * nz + 127) // 128
+    again_frac = again / max(1, 3 * (args.warmup + args.steps + 1) * ntiles)
+    mlp_flops = ntiles * 128 * 2 * 64 * (64 + 16) * (4 + 3 * again_frac)
     mlp = {"kernel": "k_io_eng_props_mlp", "avg_launch_ms": per_launch["eng_props"],
            "mma_tflops": mlp_flops / (per_launch["eng_props"] / 1000.0) / 1e12,
-           "tanh_per_cell": 256, "note": "bound by the 256 tanh.approx evaluations per cell (SFU), not by HBM"}
+           "tanh_per_cell": 128 * (1 + again_frac),
+           "note": "bound by instruction issue and tensor-memory round trips (the tanh, BF16 hi/lo splits and "
+                   "derivative factors between the layers), not by HBM bytes or the tensor pipe"}
 
     # ---- end to end through the public API with host buffers
     names, inputs = IO_RESULT_FIELDS, IO_INPUT_FIELDS
@@ -1199,19 +1208,20 @@ def run_ours(args, wl, ws, rank, local):
     return 0
 
 
-def profile_case(spec, precision):
+def profile_case(spec, precision, spectra="fp64", refine=1):
     import chapsim1ww_b200 as cs
     from chapsim1ww_b200 import TGChannel
     if spec.lower().startswith("iolearn"):
-        # the mixed IO form with the learned property model (model trained
-        # briefly: the kernels' work does not depend on its accuracy)
+        # the IO form with the learned property model, Poisson spectra as in
+        # the comparison workload (model trained briefly: the kernels' work
+        # does not depend on its accuracy)
         from chapsim1ww_b200 import IOChannel, PropertyEngine, synthetic_table
         nx, ny, nz = (int(x) for x in spec.lower()[7:].split("x"))
         eng = PropertyEngine(*synthetic_table(4096))
         eng.train(65536, 2, 300, 3e-3)
         eng.gate(1e9, 256)
-        c = IOChannel(nx, ny, nz, table=io_table("synthetic"), precision=cs.MIXED)
-        c.set_refinement(0)
+        c = IOChannel(nx, ny, nz, table=io_table("synthetic"), precision=cs.MIXED if spectra == "fp32" else cs.FP64)
+        c.set_refinement(refine)
         c.set_props_mode(1, eng)
         c.random_fl_theml_fld_io(2, 0.1)
         for _ in range(2):
@@ -1282,7 +1292,7 @@ def main():
                          "iosi for an IO channel with the semi-implicit viscous scheme")
     args = ap.parse_args()
     if args.profile_case:
-        return profile_case(args.profile_case, args.precision)
+        return profile_case(args.profile_case, args.precision, args.spectra, args.refine)
     args.warmup = max(args.warmup, 3)
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         return launch_ranks(args.gpus)

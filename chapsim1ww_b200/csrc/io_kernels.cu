@@ -284,7 +284,8 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_props_only(TGDev d, IODev i
 // polynomial base at h2.  h2 differs from h1 by the density change of one
 // substep (|dx| ~ 1e-4); a tile in which any model cell moves further than
 // kTaylorMax evaluates the model a second time at h2.  This halves the tanh
-// evaluations, which bound the kernel on the special-function unit.
+// evaluations; the elementwise work between the layers runs on packed FP32
+// pairs, and the kernel is bound by its instruction issue rate.
 __global__ void __launch_bounds__(chapsim_mlp::TILE, 3) k_io_eng_props_mlp(TGDev d, IODev io, chapsim_mlp::MlpDev M) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   chapsim_mlp::SmemD &s = chapsim_mlp::smem_of<chapsim_mlp::SmemD>(smem_raw);
@@ -294,19 +295,37 @@ __global__ void __launch_bounds__(chapsim_mlp::TILE, 3) k_io_eng_props_mlp(TGDev
   const int64_t ntiles = (n + chapsim_mlp::TILE - 1) / chapsim_mlp::TILE;
   const int64_t rows = d.ny + 2;
   const double hinv = 1.0 / M.hhalf;
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int64_t c = tile * chapsim_mlp::TILE + threadIdx.x;
+  // The thread's cell advances by a fixed stride per tile: its x index and
+  // row j follow incrementally instead of by two 64-bit divisions per cell.
+  const int64_t stride = (int64_t)gridDim.x * chapsim_mlp::TILE;
+  const int sx = (int)(stride % d.nx), sj = (int)((stride / d.nx) % rows);
+  int64_t c = (int64_t)blockIdx.x * chapsim_mlp::TILE + threadIdx.x;
+  int ix = (int)(c % d.nx), j = (int)((c / d.nx) % rows);
+  // the next tile's inputs are loaded while the current one is evaluated
+  double nD = 1.0, nmu = 0.0, nrh = 0.0;
+  if (c < n) {
+    nD = io.D[c];
+    nmu = io.mu[c];
+    nrh = io.rhoh[c];
+  }
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x, c += stride) {
     const bool valid = c < n;
-    const int j = valid ? (int)((c / d.nx) % rows) : 0;
     const bool interior = valid && j >= 1 && j <= d.ny;
-    double dold = 1.0, muold = 0.0, rh = 0.0;
+    const double dold = nD, muold = nmu, rh = interior ? nrh : 0.0;
+    if (c + stride < n) {
+      nD = io.D[c + stride];
+      nmu = io.mu[c + stride];
+      nrh = io.rhoh[c + stride];
+    }
+    ix += sx;
+    const int carry = ix >= d.nx;
+    ix -= carry ? d.nx : 0;
+    j += sj + carry;
+    j -= j >= rows ? (int)rows : 0;
     if (valid) {
-      dold = io.D[c];
-      muold = io.mu[c];
       io.mu0[c] = muold;
       io.D0[c] = dold;
       if (!interior) io.msum[c] = muold + muold;  // ghost rows: the ghost kernel sets the new value
-      else rh = io.rhoh[c];
     }
     // DENSITY_UPDATE
     const double h1 = rh / dold;
@@ -319,7 +338,7 @@ __global__ void __launch_bounds__(chapsim_mlp::TILE, 3) k_io_eng_props_mlp(TGDev
       double T;
       if (!chapsim_spl::inside(io.ht, h1)) {
         ++bad;
-      } else if ((chapsim_mlp::gate_mask(M, h1) & chapsim_mlp::kStepMask) == chapsim_mlp::kStepMask) {
+      } else if (chapsim_mlp::gate_step(s, M, h1)) {
         D = chapsim_mlp::assemble(M, 1, x1, y[1]);
       } else if (!(look_ht(io, h1, T) && look_td(io, T, D))) {
         D = dold;
@@ -331,7 +350,7 @@ __global__ void __launch_bounds__(chapsim_mlp::TILE, 3) k_io_eng_props_mlp(TGDev
     const double x2 = (h2 - M.hmid) * hinv;
     const bool keep = io.shortcuts && fabs(h2) < 1.0e-10;
     const bool model2 = interior && !keep && chapsim_spl::inside(io.ht, h2) &&
-                        (chapsim_mlp::gate_mask(M, h2) & chapsim_mlp::kStepMask) == chapsim_mlp::kStepMask;
+                        chapsim_mlp::gate_step(s, M, h2);
     const bool again = __syncthreads_or(model2 && fabs(x2 - x1) > chapsim_mlp::kTaylorMax);
     float y2[chapsim_mlp::NO];
     if (again && threadIdx.x == 0) atomicAdd(io.model_again, 1ull);
@@ -400,7 +419,7 @@ __global__ void __launch_bounds__(chapsim_mlp::TILE, 4) k_io_therm_props(TGDev d
     if (!interior || (io.shortcuts && fabs(h) < 1.0e-10)) continue;
     double T, D, Mu, K;
     bool ok = chapsim_spl::inside(io.ht, h);
-    if (ok && use_mlp && (chapsim_mlp::gate_mask(M, h) & chapsim_mlp::kStepMask) == chapsim_mlp::kStepMask) {
+    if (ok && use_mlp && chapsim_mlp::gate_step(*sp, M, h)) {
       T = chapsim_mlp::assemble(M, 0, x, y[0]);
       D = chapsim_mlp::assemble(M, 1, x, y[1]);
       Mu = chapsim_mlp::assemble(M, 2, x, y[2]);
