@@ -144,6 +144,7 @@ SIGNATURES += [
     ("chapsim_instant_file_read", _I, [ctypes.c_char_p, _I, _I, _I, ctypes.POINTER(_I), _DP, _DP, _DP, _P]),
 ]
 STATS_NV = 122
+STATS_IO_NV = 360
 PROPS_TABLE, PROPS_MLP = 0, 1
 ERR_RANGE = 8
 ERRORS[8] = "CHAPSIM_ERR_RANGE"

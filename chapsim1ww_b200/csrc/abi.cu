@@ -1041,7 +1041,6 @@ int chapsim_velo_correction(chapsim_ctx *ctx, int domain, int ns) {
 
 int chapsim_stats(chapsim_ctx *ctx, int accumulate) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
-  REQUIRE(ctx->domain == CHAPSIM_ITG, CHAPSIM_ERR_UNSUPPORTED, "statistics are built for the TG domain");
   CKC(cudaSetDevice(ctx->device));
   return stats_run(ctx, accumulate);
 }
@@ -1050,7 +1049,8 @@ int chapsim_get_stats(chapsim_ctx *ctx, int which, double *out, int64_t n, int64
   REQUIRE(ctx && out, CHAPSIM_ERR_ARG, "null argument");
   REQUIRE(which == 0 || which == 1, CHAPSIM_ERR_ARG, "which: 0 xz average, 1 time average");
   REQUIRE(ctx->stats_buf, CHAPSIM_ERR_STATE, "chapsim_stats has not run");
-  REQUIRE(n == (int64_t)ctx->cfg.ny * CHAPSIM_STATS_NV, CHAPSIM_ERR_ARG, "n must be ny * CHAPSIM_STATS_NV");
+  REQUIRE(n == (int64_t)ctx->cfg.ny * (ctx->domain == CHAPSIM_IIO ? CHAPSIM_STATS_IO_NV : CHAPSIM_STATS_NV),
+          CHAPSIM_ERR_ARG, "n must be ny * CHAPSIM_STATS_NV (TG) or ny * CHAPSIM_STATS_IO_NV (IO)");
   CKC(cudaSetDevice(ctx->device));
   if (nstatis) *nstatis = ctx->nstatis;
   return stats_get(ctx, which, out, n);

@@ -138,6 +138,51 @@ class IOChannel(TGChannel):
         evaluation (a step beyond the first-order expansion's range)."""
         return int(self._reduce(8))
 
+    # ------------------------------------------------------- statistics
+    STATS_LAYOUT = (("U1", 4), ("G1", 3), ("UP", 3), ("U2", 6), ("UG", 6), ("U3", 10), ("UGU", 10), ("DVDL1", 9),
+                    ("DVDLP", 9), ("DVDL2", 81), ("T1", 1), ("D1", 1), ("H1", 1), ("M1", 1), ("T2", 1), ("D2", 1),
+                    ("H2", 1), ("DH", 1), ("PH", 1), ("DVDL1M", 9), ("DVDL1MH", 9), ("DVDL1MU", 27), ("DVDL2M", 81),
+                    ("UH", 3), ("GH", 3), ("U2DH", 6), ("DhDL1", 3), ("DhDLP", 3), ("DTDLK", 3), ("DTDLKU", 9),
+                    ("DTDLKDVDL", 27), ("DHDLMDVDL", 27))
+
+    def pp_mean_zx(self, accumulate=False):
+        """PP_MEAN_ZX_FLOW_Xperiodic_IO on the device (and PP_MEAN_T_Xperiodic_IO
+        when accumulate)."""
+        self._chk(self.lib.chapsim_stats(self.h, 1 if accumulate else 0))
+
+    def stats(self, which=0):
+        """(ny, 360) array of the xz (which=0) or time (which=1) averages, in
+        STATS_LAYOUT order, and the sample count."""
+        a = np.empty((self.ny, _lib.STATS_IO_NV))
+        n = ctypes.c_int64()
+        self._chk(self.lib.chapsim_get_stats(self.h, which, a.ctypes.data, a.size, ctypes.byref(n)))
+        return a, n.value
+
+    def stats_groups(self, which=0):
+        """The statistics as {name: (ny, width) array} in STATS_LAYOUT order."""
+        a, _ = self.stats(which)
+        out, lo = {}, 0
+        for name, width in self.STATS_LAYOUT:
+            out[name] = a[:, lo:lo + width]
+            lo += width
+        return out
+
+    def monitor(self):
+        """The bulk numbers that close PP_MEAN_ZX_FLOW_Xperiodic_IO
+        (src/processing/PP_MEAN_ZX.f90:814-869) from the device xz averages:
+        G1BULK (bulk x mass flux), G1MAXX, and with the energy equation
+        H1bulk (mass-flux-weighted enthalpy) and T1MAXX."""
+        g = self.stats_groups(0)
+        dyfi = self.mesh(2)
+        area = (1.0 / dyfi).sum() * self.cfg.lz  # AREA_INLET of the channel
+        g1rate = (g["G1"][:, 0] / dyfi).sum()
+        mon = {"g1bulk": g1rate * self.cfg.lz / area, "g1maxx": np.abs(g["G1"][:, 0]).max(),
+               "maxdiv": self.divgck_io(), "cflmm_dt": self.cfl() * self.cfg.dt}
+        if self.iocfg.thermal:
+            mon["h1bulk"] = (g["GH"][:, 0] / dyfi).sum() / g1rate
+            mon["t1maxx"] = np.abs(g["T1"][:, 0]).max()
+        return mon
+
     def bad_cells(self):
         return int(self._reduce(_lib.R_BADCELLS))
 

@@ -208,16 +208,26 @@ int chapsim_velo_correction(chapsim_ctx *ctx, int domain, int ns);
 /* Device reductions (DIVGCK_tg, BULK_VELOCITY_TG, CFL); synchronises. */
 int chapsim_reduce(chapsim_ctx *ctx, int domain, int what, double *out);
 
-/* On-device flow statistics of a TG context.  chapsim_stats computes the
- * xz-plane averages of PP_MEAN_ZX_FLOW_TG (src/processing/PP_MEAN_ZX.f90:1-294)
- * for every y-row and, with accumulate != 0, folds them into the running time
- * average of PP_MEAN_T_TG (src/processing/PP_MEAN_T.f90:322-370, asymptotic
- * weights 1/N, (N-1)/N).  chapsim_get_stats copies ny * CHAPSIM_STATS_NV
- * values (which = 0: xz average, 1: time average; row j-1 holds U1 (u, v, w,
- * p), UP (3), U2 (11 12 13 22 23 33), U3 (111 112 113 122 123 133 222 223 233
- * 333), DVDL1 (3x3 row-major), DVDLP (3x3), DVDL2 (9x9)) and the sample count.
- * chapsim_stats_reset clears the time average (PP_TMEAN_INI_ZERO_TG). */
+/* On-device flow statistics.  chapsim_stats computes the xz-plane averages
+ * of PP_MEAN_ZX_FLOW_TG (src/processing/PP_MEAN_ZX.f90:1-294) on a TG context
+ * or of PP_MEAN_ZX_FLOW_Xperiodic_IO (src/processing/PP_MEAN_ZX.f90:299-872)
+ * on an IO context for every y-row and, with accumulate != 0, folds them into
+ * the running time average of PP_MEAN_T_TG / PP_MEAN_T_Xperiodic_IO
+ * (src/processing/PP_MEAN_T.f90:322-370, 436-520; asymptotic weights 1/N,
+ * (N-1)/N).  chapsim_get_stats copies ny * CHAPSIM_STATS_NV (TG) or
+ * ny * CHAPSIM_STATS_IO_NV (IO) values (which = 0: xz average, 1: time
+ * average) and the sample count.  TG row j-1: U1 (u, v, w, p), UP (3), U2 (11
+ * 12 13 22 23 33), U3 (111 112 113 122 123 133 222 223 233 333), DVDL1 (3x3
+ * row-major), DVDLP (3x3), DVDL2 (9x9).  IO row j-1: U1 (u, v, w, p), G1
+ * (3), UP (3), U2 (6), UG (6, u_m g_n for m <= n), U3 (10), UGU (10,
+ * u_m g_n u_h for m <= n <= h), DVDL1 (3x3), DVDLP (3x3), DVDL2 (9x9: row
+ * (m,h), column (n,p)); then, with the energy equation (zero otherwise), T1,
+ * D1, H1, M1, T2, D2, H2, DH, PH, DVDL1M (3x3), DVDL1MH (3x3), DVDL1MU
+ * (m,n,h), DVDL2M (9x9), UH (3), GH (3), U2DH (6), DhDL1 (3), DhDLP (3),
+ * DTDLK (3), DTDLKU (m,n), DTDLKDVDL (m,n,h), DHDLMDVDL (m,n,h).
+ * chapsim_stats_reset clears the time average (PP_TMEAN_INI_ZERO_TG / _IO). */
 #define CHAPSIM_STATS_NV 122
+#define CHAPSIM_STATS_IO_NV 360
 int chapsim_stats(chapsim_ctx *ctx, int accumulate);
 int chapsim_get_stats(chapsim_ctx *ctx, int which, double *out, int64_t n, int64_t *nstatis);
 int chapsim_stats_reset(chapsim_ctx *ctx);

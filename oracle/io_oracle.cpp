@@ -1782,4 +1782,131 @@ void oracle_io_bc_scalars(const oracle_io *o, double *out) {
   for (int q = 0; q < 7; ++q) out[q] = o->bcs[q];
 }
 
+// PP_MEAN_ZX_FLOW_Xperiodic_IO (src/processing/PP_MEAN_ZX.f90:299-872),
+// channel branch (RCCI1 = RNDI1 = 1): per y-row j the xz-plane averages of
+// the cell-centred velocity U, mass flux G, pressure p, velocity gradient
+// D(m,n) = du_m/dx_n and, with the energy equation, of T, rho, h, mu, k and
+// the gradients of h and T, each sum scaled by VL1313_io = 1/(nx nz)
+// (src/CONSPARA.f90:84).  out holds ny * 360 values; row j-1:
+//   U1 (u, v, w, p), G1 (3), UP (3), U2 (6: 11 12 13 22 23 33), UG (6),
+//   U3 (10: 111 112 113 122 123 133 222 223 233 333), UGU (10), DVDL1 (3x3),
+//   DVDLP (3x3), DVDL2 (9x9: row (m,h), column (n,p)); then T1, D1, H1, M1,
+//   T2, D2, H2, DH, PH, DVDL1M (3x3), DVDL1MH (3x3), DVDL1MU (m,n,h),
+//   DVDL2M (9x9), UH (3), GH (3), U2DH (6), DhDL1 (3), DhDLP (3), DTDLK (3),
+//   DTDLKU (m,n), DTDLKDVDL (m,n,h), DHDLMDVDL (m,n,h) — zero without the
+//   energy equation.
+void oracle_io_stats(const oracle_io *o, double *out) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  const double vl = 1.0 / (double)(nx * nz);
+  const bool th = o->thermal != 0;
+#pragma omp parallel for schedule(static) num_threads(nthreads())
+  for (int j = 1; j <= ny; ++j) {
+    std::vector<double> acc(360, 0.0);
+    const int jp = j + 1, jm = j - 1;
+    for (int i = 1; i <= nx; ++i) {
+      const int ip = o->ip(i), im = o->im(i);
+      for (int k = 1; k <= nz; ++k) {
+        const int kp = o->kp(k), km = o->km(k);
+        double U[3], G[3], Uip[3], Uim[3], Ujp[3], Ujm[3], Ukp[3], Ukm[3], D[3][3];
+        G[0] = (FC(g, 1, i, j, k) + FC(g, 1, ip, j, k)) * 0.5;
+        U[0] = (FC(q, 1, i, j, k) + FC(q, 1, ip, j, k)) * 0.5;
+        Ujp[0] = (FC(q, 1, i, jp, k) + FC(q, 1, ip, jp, k)) * 0.5;
+        Ujm[0] = (FC(q, 1, i, jm, k) + FC(q, 1, ip, jm, k)) * 0.5;
+        Ukp[0] = (FC(q, 1, i, j, kp) + FC(q, 1, ip, j, kp)) * 0.5;
+        Ukm[0] = (FC(q, 1, i, j, km) + FC(q, 1, ip, j, km)) * 0.5;
+        G[2] = (FC(g, 3, i, j, k) + FC(g, 3, i, j, kp)) * 0.5;
+        U[2] = (FC(q, 3, i, j, k) + FC(q, 3, i, j, kp)) * 0.5;
+        Uip[2] = (FC(q, 3, ip, j, k) + FC(q, 3, ip, j, kp)) * 0.5;
+        Uim[2] = (FC(q, 3, im, j, k) + FC(q, 3, im, j, kp)) * 0.5;
+        Ujp[2] = (FC(q, 3, i, jp, k) + FC(q, 3, i, jp, kp)) * 0.5;
+        Ujm[2] = (FC(q, 3, i, jm, k) + FC(q, 3, i, jm, kp)) * 0.5;
+        G[1] = (FC(g, 2, i, j, k) + FC(g, 2, i, jp, k)) * 0.5;
+        U[1] = (FC(q, 2, i, j, k) + FC(q, 2, i, jp, k)) * 0.5;
+        Uip[1] = (FC(q, 2, ip, j, k) + FC(q, 2, ip, jp, k)) * 0.5;
+        Uim[1] = (FC(q, 2, im, j, k) + FC(q, 2, im, jp, k)) * 0.5;
+        Ukp[1] = (FC(q, 2, i, j, kp) + FC(q, 2, i, jp, kp)) * 0.5;
+        Ukm[1] = (FC(q, 2, i, j, km) + FC(q, 2, i, jp, km)) * 0.5;
+        D[0][0] = (FC(q, 1, ip, j, k) - FC(q, 1, i, j, k)) * o->dxi;
+        D[0][2] = (Ukp[0] - Ukm[0]) * o->dzi * 0.5;
+        D[0][1] = ((Ujp[0] - U[0]) * o->dyci[jp] + (U[0] - Ujm[0]) * o->dyci[j]) * 0.5;
+        D[1][0] = (Uip[1] - Uim[1]) * o->dxi * 0.5;
+        D[1][2] = (Ukp[1] - Ukm[1]) * o->dzi * 0.5;
+        D[1][1] = (FC(q, 2, i, jp, k) - FC(q, 2, i, j, k)) * o->dyfi[j];
+        D[2][2] = (FC(q, 3, i, j, kp) - FC(q, 3, i, j, k)) * o->dzi;
+        D[2][0] = (Uip[2] - Uim[2]) * o->dxi * 0.5;
+        D[2][1] = ((Ujp[2] - U[2]) * o->dyci[jp] + (U[2] - Ujm[2]) * o->dyci[j]) * 0.5;
+        const double p = F(pr, i, j, k);
+        int a = 0;
+        for (int m = 0; m < 3; ++m) acc[a++] += U[m];
+        acc[a++] += p;
+        for (int m = 0; m < 3; ++m) acc[a++] += G[m];
+        for (int m = 0; m < 3; ++m) acc[a++] += U[m] * p;
+        for (int m = 0; m < 3; ++m)
+          for (int n = m; n < 3; ++n) acc[a++] += U[m] * U[n];
+        for (int m = 0; m < 3; ++m)
+          for (int n = m; n < 3; ++n) acc[a++] += U[m] * G[n];
+        for (int m = 0; m < 3; ++m)
+          for (int n = m; n < 3; ++n)
+            for (int h = n; h < 3; ++h) acc[a++] += U[m] * U[n] * U[h];
+        for (int m = 0; m < 3; ++m)
+          for (int n = m; n < 3; ++n)
+            for (int h = n; h < 3; ++h) acc[a++] += U[m] * G[n] * U[h];
+        for (int m = 0; m < 3; ++m)
+          for (int n = 0; n < 3; ++n) acc[a++] += D[m][n];
+        for (int m = 0; m < 3; ++m)
+          for (int n = 0; n < 3; ++n) acc[a++] += D[m][n] * p;
+        for (int l1 = 0; l1 < 9; ++l1)
+          for (int l2 = 0; l2 < 9; ++l2) acc[a++] += D[l1 / 3][l1 % 3] * D[l2 / 3][l2 % 3];
+        if (!th) continue;
+        const double T = F(tt, i, j, k), R = F(dd, i, j, k), H = F(hh, i, j, k), MU = F(mu, i, j, k),
+                     K = F(kk, i, j, k);
+        double dh[3], dT[3];
+        dh[0] = (F(hh, ip, j, k) - F(hh, im, j, k)) * o->dxi * 0.5;
+        dh[2] = (F(hh, i, j, kp) - F(hh, i, j, km)) * o->dzi * 0.5;
+        dh[1] = ((F(hh, i, jp, k) - F(hh, i, j, k)) * o->dyci[jp] + (F(hh, i, j, k) - F(hh, i, jm, k)) * o->dyci[j]) *
+                0.5;
+        dT[0] = (F(tt, ip, j, k) - F(tt, im, j, k)) * o->dxi * 0.5;
+        dT[2] = (F(tt, i, j, kp) - F(tt, i, j, km)) * o->dzi * 0.5;
+        dT[1] = ((F(tt, i, jp, k) - F(tt, i, j, k)) * o->dyci[jp] + (F(tt, i, j, k) - F(tt, i, jm, k)) * o->dyci[j]) *
+                0.5;
+        acc[a++] += T;
+        acc[a++] += R;
+        acc[a++] += H;
+        acc[a++] += MU;
+        acc[a++] += T * T;
+        acc[a++] += R * R;
+        acc[a++] += H * H;
+        acc[a++] += H * R;
+        acc[a++] += H * p;
+        for (int m = 0; m < 3; ++m)
+          for (int n = 0; n < 3; ++n) acc[a++] += D[m][n] * MU;
+        for (int m = 0; m < 3; ++m)
+          for (int n = 0; n < 3; ++n) acc[a++] += D[m][n] * MU * H;
+        for (int m = 0; m < 3; ++m)
+          for (int n = 0; n < 3; ++n)
+            for (int h = 0; h < 3; ++h) acc[a++] += D[m][n] * MU * U[h];
+        for (int l1 = 0; l1 < 9; ++l1)
+          for (int l2 = 0; l2 < 9; ++l2) acc[a++] += D[l1 / 3][l1 % 3] * D[l2 / 3][l2 % 3] * MU;
+        for (int m = 0; m < 3; ++m) acc[a++] += H * U[m];
+        for (int m = 0; m < 3; ++m) acc[a++] += H * G[m];
+        for (int m = 0; m < 3; ++m)
+          for (int n = m; n < 3; ++n) acc[a++] += R * H * U[m] * U[n];
+        for (int m = 0; m < 3; ++m) acc[a++] += dh[m];
+        for (int m = 0; m < 3; ++m) acc[a++] += dh[m] * p;
+        for (int m = 0; m < 3; ++m) acc[a++] += dT[m] * K;
+        for (int m = 0; m < 3; ++m)
+          for (int n = 0; n < 3; ++n) acc[a++] += dT[m] * K * U[n];
+        for (int m = 0; m < 3; ++m)
+          for (int n = 0; n < 3; ++n)
+            for (int h = 0; h < 3; ++h) acc[a++] += dT[m] * K * D[n][h];
+        for (int m = 0; m < 3; ++m)
+          for (int n = 0; n < 3; ++n)
+            for (int h = 0; h < 3; ++h) acc[a++] += dh[m] * MU * D[n][h];
+      }
+    }
+    double *r = out + (size_t)(j - 1) * 360;
+    for (int a = 0; a < 360; ++a) r[a] = acc[a] * vl;
+  }
+}
+
 }  // extern "C"

@@ -76,6 +76,7 @@ def load(build=True):
     L.oracle_io_get_plane.argtypes = [P, I, P]
     L.oracle_io_set_plane.argtypes = [P, I, P]
     L.oracle_io_bc_scalars.argtypes = [P, P]
+    L.oracle_io_stats.argtypes = [P, P]
     L.oracle_tg_stats.argtypes = [P, P]
     L.oracle_set_threads.argtypes = [I]
     L.oracle_get_threads.restype = I
@@ -293,6 +294,12 @@ class OracleIO:
 
     def cfl(self):
         return self.L.oracle_io_cfl(self.h)
+
+    def stats(self):
+        """PP_MEAN_ZX_FLOW_Xperiodic_IO: (ny, 360) xz-plane averages."""
+        a = np.empty((self.ny, 360))
+        self.L.oracle_io_stats(self.h, a.ctypes.data)
+        return a
 
     def set_dt(self, dt):
         self.L.oracle_io_set_dt(self.h, dt)

@@ -639,3 +639,117 @@ class IO(TG):
     def divmax(self):
         """max |div G + drho| over the cells (DIVGCK_io)."""
         return float(np.abs(self.div(self.g) + self.X(self.drho)).max())
+
+
+def io_stats(f, dxi, dzi, dyfi, dyci, thermal):
+    """PP_MEAN_ZX_FLOW_Xperiodic_IO (src/processing/PP_MEAN_ZX.f90:299-872),
+    channel branch, as whole-array shifts: (ny, 360) xz-plane averages of the
+    cell-centred U, G, p, the velocity gradient D and (thermal) T, rho, h,
+    mu, k and the h and T gradients, in the library's output order.  f maps
+    u, v, w, p, gx, gy, gz (and h, t, rho, mu, k) to (nz, ny + 2, nx) arrays;
+    dyfi and dyci are 1-based arrays of length ny + 2."""
+    nz, ny2, nx = f["u"].shape
+    ny = ny2 - 2
+
+    def S(a, di=0, dj=0, dk=0):
+        b = np.roll(a, shift=(-dk, -di), axis=(0, 2)) if (di or dk) else a
+        return b[:, 1 + dj:ny + 1 + dj, :]
+
+    u, v, w = f["u"], f["v"], f["w"]
+    U = [(S(u) + S(u, 1)) * 0.5, (S(v) + S(v, 0, 1)) * 0.5, (S(w) + S(w, 0, 0, 1)) * 0.5]
+    G = [(S(f["gx"]) + S(f["gx"], 1)) * 0.5, (S(f["gy"]) + S(f["gy"], 0, 1)) * 0.5,
+         (S(f["gz"]) + S(f["gz"], 0, 0, 1)) * 0.5]
+    yc = dyci[2:ny + 2][None, :, None]
+    yj = dyci[1:ny + 1][None, :, None]
+    yf = dyfi[1:ny + 1][None, :, None]
+    cc = lambda a, di=0, dj=0, dk=0, ax=0: (S(a, di, dj, dk) + S(a, di + (ax == 0), dj + (ax == 1), dk + (ax == 2))) * 0.5
+    D = [[None] * 3 for _ in range(3)]
+    D[0][0] = (S(u, 1) - S(u)) * dxi
+    D[0][1] = ((cc(u, 0, 1) - U[0]) * yc + (U[0] - cc(u, 0, -1)) * yj) * 0.5
+    D[0][2] = (cc(u, 0, 0, 1) - cc(u, 0, 0, -1)) * dzi * 0.5
+    D[1][0] = (cc(v, 1, ax=1) - cc(v, -1, ax=1)) * dxi * 0.5
+    D[1][1] = (S(v, 0, 1) - S(v)) * yf
+    D[1][2] = (cc(v, 0, 0, 1, ax=1) - cc(v, 0, 0, -1, ax=1)) * dzi * 0.5
+    D[2][0] = (cc(w, 1, ax=2) - cc(w, -1, ax=2)) * dxi * 0.5
+    D[2][1] = ((cc(w, 0, 1, ax=2) - U[2]) * yc + (U[2] - cc(w, 0, -1, ax=2)) * yj) * 0.5
+    D[2][2] = (S(w, 0, 0, 1) - S(w)) * dzi
+    p = S(f["p"])
+    Dl = [D[l // 3][l % 3] for l in range(9)]
+    vals = []
+    add = vals.append
+    for m in range(3):
+        add(U[m])
+    add(p)
+    for m in range(3):
+        add(G[m])
+    for m in range(3):
+        add(U[m] * p)
+    for m in range(3):
+        for n in range(m, 3):
+            add(U[m] * U[n])
+    for m in range(3):
+        for n in range(m, 3):
+            add(U[m] * G[n])
+    for m in range(3):
+        for n in range(m, 3):
+            for h in range(n, 3):
+                add(U[m] * U[n] * U[h])
+    for m in range(3):
+        for n in range(m, 3):
+            for h in range(n, 3):
+                add(U[m] * G[n] * U[h])
+    for l in range(9):
+        add(Dl[l])
+    for l in range(9):
+        add(Dl[l] * p)
+    for l1 in range(9):
+        for l2 in range(9):
+            add(Dl[l1] * Dl[l2])
+    zero = np.zeros_like(p)
+    if thermal:
+        h, T, R, MU, K = (f[n] for n in ("h", "t", "rho", "mu", "k"))
+
+        def grad(a):
+            return [(S(a, 1) - S(a, -1)) * dxi * 0.5,
+                    ((S(a, 0, 1) - S(a)) * yc + (S(a) - S(a, 0, -1)) * yj) * 0.5,
+                    (S(a, 0, 0, 1) - S(a, 0, 0, -1)) * dzi * 0.5]
+
+        dh, dT = grad(h), grad(T)
+        T, R, H, MU, K = S(T), S(R), S(h), S(MU), S(K)
+        for a in (T, R, H, MU, T * T, R * R, H * H, H * R, H * p):
+            add(a)
+        for l in range(9):
+            add(Dl[l] * MU)
+        for l in range(9):
+            add(Dl[l] * MU * H)
+        for l in range(9):
+            for m in range(3):
+                add(Dl[l] * MU * U[m])
+        for l1 in range(9):
+            for l2 in range(9):
+                add(Dl[l1] * Dl[l2] * MU)
+        for m in range(3):
+            add(H * U[m])
+        for m in range(3):
+            add(H * G[m])
+        for m in range(3):
+            for n in range(m, 3):
+                add(R * H * U[m] * U[n])
+        for m in range(3):
+            add(dh[m])
+        for m in range(3):
+            add(dh[m] * p)
+        for m in range(3):
+            add(dT[m] * K)
+        for m in range(3):
+            for n in range(3):
+                add(dT[m] * K * U[n])
+        for m in range(3):
+            for l in range(9):
+                add(dT[m] * K * Dl[l])
+        for m in range(3):
+            for l in range(9):
+                add(dh[m] * MU * Dl[l])
+    else:
+        vals += [zero] * 219
+    return np.stack([a.sum(axis=(0, 2)) / (nx * nz) for a in vals], axis=1)

@@ -142,3 +142,41 @@ def test_oracle_io_semi_implicit_scheme(thermal):
         diffs.append(max(np.abs(e.get(n) - i.get(n)).max() for n in ("gx", "gy", "gz")))
     assert 3.5 < diffs[0] / diffs[1] < 4.5, diffs
     assert diffs[0] < 1e-6
+
+
+IO_STAT_GROUPS = (("U1", 4), ("G1", 3), ("UP", 3), ("U2", 6), ("UG", 6), ("U3", 10), ("UGU", 10), ("DVDL1", 9),
+                  ("DVDLP", 9), ("DVDL2", 81), ("T1", 1), ("D1", 1), ("H1", 1), ("M1", 1), ("T2", 1), ("D2", 1),
+                  ("H2", 1), ("DH", 1), ("PH", 1), ("DVDL1M", 9), ("DVDL1MH", 9), ("DVDL1MU", 27), ("DVDL2M", 81),
+                  ("UH", 3), ("GH", 3), ("U2DH", 6), ("DhDL1", 3), ("DhDLP", 3), ("DTDLK", 3), ("DTDLKU", 9),
+                  ("DTDLKDVDL", 27), ("DHDLMDVDL", 27))
+
+
+@pytest.mark.parametrize("thermal", [0, 1])
+def test_oracle_io_statistics_match_numpy_restatement(thermal):
+    """PP_MEAN_ZX_FLOW_Xperiodic_IO: the oracle's loop restatement against the
+    numpy whole-array restatement on the oracle's own fields after one RK3
+    step, 1e-12 per statistic group (relative to the group's largest value);
+    without the energy equation the thermal groups are zero."""
+    sys.path.insert(0, GOLDEN)
+    from numpy_io import IO, io_stats
+    dims = (20, 14, 12)
+    o = OracleIO(*dims, thermal=thermal)
+    o.init_random(6, 0.15)
+    o.step(1)
+    n = IO(*dims, 8 * math.pi, 4 * math.pi / 3)
+    names = ("u", "v", "w", "p", "gx", "gy", "gz") + (("h", "t", "rho", "mu", "k") if thermal else ())
+    b = io_stats({f: o.get(f) for f in names}, n.dxi, n.dzi, n.dyfi, n.dyci, thermal)
+    a = o.stats()
+    assert a.shape == b.shape == (dims[1], 360)
+    lo = 0
+    for name, width in IO_STAT_GROUPS:
+        x, y = a[:, lo:lo + width], b[:, lo:lo + width]
+        lo += width
+        if not thermal and lo > 141:
+            assert not np.any(x), name
+            continue
+        assert np.abs(x - y).max() <= 1e-12 * max(np.abs(y).max(), 1e-300), name
+    assert lo == 360
+    # DVDL2 is symmetric in (m,h) <-> (n,p)
+    d2 = a[:, 60:141].reshape(-1, 9, 9)
+    assert np.allclose(d2, np.transpose(d2, (0, 2, 1)), rtol=0, atol=1e-14 * np.abs(d2).max())
