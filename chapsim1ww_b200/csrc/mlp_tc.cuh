@@ -267,14 +267,14 @@ __device__ __forceinline__ void cta_setup(Smem &s, const MlpDev &M) {
   const uint4 *src = reinterpret_cast<const uint4 *>(M.wt);  // 16-byte aligned (host contract)
   uint4 *dst = reinterpret_cast<uint4 *>(s.w2_hi);  // w2_hi, w2_lo, w3_hi, w3_lo are contiguous
   constexpr int n16 = (2 * NH * NH + 2 * NOP * NH) * 2 / 16;
-  for (int q = t; q < n16; q += TILE) dst[q] = src[q];
+  for (int q = t; q < n16; q += blockDim.x) dst[q] = src[q];
   if (t < NH) {
     s.w1[t] = M.par[O_W1 + t];
     s.b1[t] = M.par[O_B1 + t];
     s.b2[t] = M.par[O_B2 + t];
   }
   if (t < NOP) s.b3[t] = t < NO ? M.par[O_B3 + t] : 0.f;
-  for (int w = t; w < kMaxGateBins / 32; w += TILE) {
+  for (int w = t; w < kMaxGateBins / 32; w += blockDim.x) {
     uint32_t bits = 0;
     for (int b = 0; b < 32; ++b)
       if (32 * w + b < M.nbins && (M.gate[32 * w + b] & kStepMask) == kStepMask) bits |= 1u << b;
