@@ -141,3 +141,33 @@ def test_training_gate_and_fallback(engine, table):
     engine.update(hd, *got, mode=1)
     for a, b in zip(got, tab):
         assert torch.equal(a, b)
+
+
+def test_network_gain_over_polynomial_base(table):
+    """What the trained network gains over the model without it: the same
+    normalisation and degree-5 polynomial base with the network's output
+    layer zeroed (a residual of zero) against the trained network, both
+    evaluated on the tensor cores and gated at 1e-4 against the table.  The
+    network lowers the worst error of T, rho, mu and k by more than 10x and
+    clears more h-bins."""
+    _need_gpu()
+    from chapsim1ww_b200 import PropertyEngine
+    from oracle import mlp_ref
+    e = PropertyEngine(*table)
+    e.train(nsamples=65536, seed=2, steps=20000, lr=3e-3)
+    nb_net, _ = e.gate(tol=1e-4, nbins=256)
+    bins_net, errs_net = e.gate_outputs()
+    p, norm = e.get_params()
+    o_w3 = mlp_ref.NH + mlp_ref.NH + mlp_ref.NH * mlp_ref.NH + mlp_ref.NH
+    p0 = p.copy()
+    p0[o_w3:] = 0.0  # W3 and b3: the network adds nothing to the base
+    e.set_params(p0, norm)
+    nb_base, _ = e.gate(tol=1e-4, nbins=256)
+    bins_base, errs_base = e.gate_outputs()
+    print(f"bins cleared for T, rho, mu, k: base alone {nb_base}/256, with the network {nb_net}/256; "
+          f"worst error per output (T, rho, mu, k, cp) base {['%.2e' % x for x in errs_base]}, "
+          f"network {['%.2e' % x for x in errs_net]}")
+    assert nb_net > nb_base and nb_net >= 200
+    for o in range(4):
+        assert errs_net[o] * 10 <= errs_base[o], (o, errs_net[o], errs_base[o])
+    e.close()
