@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_props_only(TGDev d, IODev i
 __global__ void __launch_bounds__(chapsim_mlp::TILE, 3) k_io_eng_props_mlp(TGDev d, IODev io, chapsim_mlp::MlpDev M) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   chapsim_mlp::SmemD &s = chapsim_mlp::smem_of<chapsim_mlp::SmemD>(smem_raw);
-  chapsim_mlp::cta_setup(s, M);
+  chapsim_mlp::cta_setup_d(s, M);
   uint32_t phase = 0;
   const int64_t n = d.sz * d.nz;
   const int64_t ntiles = (n + chapsim_mlp::TILE - 1) / chapsim_mlp::TILE;
@@ -331,7 +331,7 @@ __global__ void __launch_bounds__(chapsim_mlp::TILE, 3) k_io_eng_props_mlp(TGDev
     const double h1 = rh / dold;
     const double x1 = (h1 - M.hmid) * hinv;
     float y[chapsim_mlp::NO], dy[chapsim_mlp::NO];
-    if (!chapsim_mlp::tile_eval_d(s, (float)x1, y, dy, phase, d.err)) break;
+    chapsim_mlp::tile_eval_d(s, (float)x1, y, dy, phase, d.err);  // a failed wait: s.fail, read below
     int bad = 0;
     double D = dold;
     if (interior) {
@@ -352,6 +352,7 @@ __global__ void __launch_bounds__(chapsim_mlp::TILE, 3) k_io_eng_props_mlp(TGDev
     const bool model2 = interior && !keep && chapsim_spl::inside(io.ht, h2) &&
                         chapsim_mlp::gate_step(s, M, h2);
     const bool again = __syncthreads_or(model2 && fabs(x2 - x1) > chapsim_mlp::kTaylorMax);
+    if (s.fail) break;  // block-uniform after the barrier
     float y2[chapsim_mlp::NO];
     if (again && threadIdx.x == 0) atomicAdd(io.model_again, 1ull);
     if (again) {

@@ -88,6 +88,7 @@ struct __align__(1024) Smem {
 // activations (tile_eval_d): 16 KB more, three CTAs per SM.
 struct __align__(1024) SmemD : Smem {
   uint16_t d_hi[TILE * NH];
+  alignas(16) float2 w3p[NH / 2][NO];  // FP32 W3 by pairs of hidden units: (W3[o][2q], W3[o][2q + 1])
 };
 
 // ---------------------------------------------------------------- PTX
@@ -390,6 +391,15 @@ __device__ __forceinline__ void dtanh32(const float *a, const float *g, float *t
   }
 }
 
+// cta_setup plus the FP32 layer-3 weights of tile_eval_d.
+__device__ __forceinline__ void cta_setup_d(SmemD &s, const MlpDev &M) {
+  for (int i = threadIdx.x; i < (NH / 2) * NO; i += blockDim.x) {
+    const int q = i / NO, o = i % NO;
+    s.w3p[q][o] = make_float2(M.par[O_W3 + o * NH + 2 * q], M.par[O_W3 + o * NH + 2 * q + 1]);
+  }
+  cta_setup(s, M);  // ends with a block barrier
+}
+
 // Evaluate the MLP on the tile: thread r holds cell r's normalised input x
 // and receives y[0..4] (standardised residual outputs, b3 included).  Every
 // thread of the CTA calls it together.  Returns false when a wait ran out
@@ -429,14 +439,22 @@ __device__ __forceinline__ bool tile_eval(Smem &s, float x, float (&y)[NO], uint
 
 // The model at x together with its derivative with respect to x, by forward
 // mode through the same layers: da1 = (1 - a1^2) w1, dz2 = W2 da1,
-// da2 = (1 - a2^2) dz2, dy = W3 da2.  The values are computed exactly as in
-// tile_eval; the derivative products run as one plain BF16 chain per layer
-// next to the value chains (the derivative only ever multiplies a step of at
-// most kTaylorMax, so its ~4e-3 relative precision adds below 1e-5).  Tensor
-// memory: z2 in columns 0..63 and dz2 in 64..127, then y in 0..15 and dy in
-// 16..31.  Every thread of the CTA calls it together; false when a wait ran
-// out.
-__device__ __forceinline__ bool tile_eval_d(SmemD &s, float x, float (&y)[NO], float (&dy)[NO], uint32_t &phase,
+// da2 = (1 - a2^2) dz2, dy = W3 da2.  Layers 1 and 2 are computed exactly as
+// in tile_eval, the layer-2 derivative as one plain BF16 chain next to the
+// value chains (the derivative only ever multiplies a step of at most
+// kTaylorMax, so its ~4e-3 relative precision adds below 1e-5).  Layer 3
+// (64 -> 5), value and derivative, runs on the CUDA cores in FP32 on packed
+// pairs from the activations in registers: it costs more instructions than
+// its MMAs but saves their round trip through shared memory, the tensor
+// pipe and tensor memory (one block barrier and one wait per tile), and its
+// FP32 products are more accurate than the split BF16 ones.  Tensor memory:
+// z2 in columns 0..63, dz2 in 64..127.  Every thread of the CTA calls it
+// together.  The layer-2 wait has no block barrier after it (nothing it
+// guards is shared: each thread reads its own tensor-memory lane after
+// seeing the commit itself); a wait that ran out sets s.fail, which the
+// caller reads after its next block barrier (the results are then
+// discarded).
+__device__ __forceinline__ void tile_eval_d(SmemD &s, float x, float (&y)[NO], float (&dy)[NO], uint32_t &phase,
                                             int *err) {
   const int r = threadIdx.x;
   const uint32_t lane_base = s.tmem + ((uint32_t)(r & ~31) << 16);
@@ -458,36 +476,40 @@ __device__ __forceinline__ bool tile_eval_d(SmemD &s, float x, float (&y)[NO], f
     issue_chain(s.tmem + NH, s.d_hi, s.w2_hi, NH);
     umma_commit(&s.bar);
   }
-  if (!layer_wait(s, phase, err)) return false;
+  if (!mbar_wait(&s.bar, phase, err)) s.fail = 1;
+  phase ^= 1u;
+  tc_fence_after();
   tmem_ld64(lane_base, a);
   bias_tanh(s.b2, a);
-  store_split(s, r, a);  // the layer-2 MMAs have completed: the tiles are free
+  uint64_t acc[NO], dacc[NO];
+#pragma unroll
+  for (int o = 0; o < NO; ++o) acc[o] = dacc[o] = 0ull;  // (+0.0f, +0.0f)
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
-    float t[32];
-    tmem_ld32(lane_base + NH + 32 * h, t);
-    dtanh32(a + 32 * h, t, t);
-    store_bf16_32(s.d_hi, r, 32 * h, t);
-  }
-  chapsim::fence_proxy_async();
-  tc_fence_before();
-  __syncthreads();
-  if (r == 0) {
-    tc_fence_after();
-    issue_layer(s, s.tmem, s.w3_hi, s.w3_lo, NOP, false);
-    issue_chain(s.tmem + NOP, s.d_hi, s.w3_hi, NOP);
-    umma_commit(&s.bar);
-  }
-  if (!layer_wait(s, phase, err)) return false;
-  float o[2 * NOP];  // y in columns 0..15, dy in 16..31: one load
-  tmem_ld32(lane_base, o);
+    float g[32];
+    tmem_ld32(lane_base + NH + 32 * h, g);
+    dtanh32(a + 32 * h, g, g);  // da2 for units 32 h .. 32 h + 31
 #pragma unroll
-  for (int q = 0; q < NO; ++q) {
-    y[q] = o[q] + s.b3[q];
-    dy[q] = o[NOP + q];
+    for (int qq = 0; qq < 16; ++qq) {
+      const int q = 16 * h + qq;
+      const uint64_t ap = pk(a[2 * q], a[2 * q + 1]), gp = pk(g[2 * qq], g[2 * qq + 1]);
+#pragma unroll
+      for (int o = 0; o < NO; ++o) {
+        const uint64_t w = *reinterpret_cast<const uint64_t *>(&s.w3p[q][o]);
+        acc[o] = fma2(w, ap, acc[o]);
+        dacc[o] = fma2(w, gp, dacc[o]);
+      }
+    }
   }
-  tc_fence_before();
-  return true;
+#pragma unroll
+  for (int o = 0; o < NO; ++o) {
+    float e0, e1;
+    upk(acc[o], e0, e1);
+    y[o] = (e0 + e1) + s.b3[o];
+    upk(dacc[o], e0, e1);
+    dy[o] = e0 + e1;
+  }
+  tc_fence_before();  // the next tile's MMAs overwrite the columns read here after its first __syncthreads
 }
 
 // Largest step |x_new - x_old| over which a tile takes the properties at the
