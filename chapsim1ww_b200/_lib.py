@@ -96,6 +96,8 @@ SIGNATURES = [
     ("chapsim_launch_count_reset", _I, [_P]),
     ("chapsim_set_tuning", _I, [_P, _I, _I]),
     ("chapsim_get_tuning", _I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
+    ("chapsim_set_line_tuning", _I, [_P, _I]),
+    ("chapsim_get_line_tuning", _I, [_P, ctypes.POINTER(_I)]),
     ("chapsim_props_create", _I, [_P, _P, _P, _P, _P, _P, _I, _I, ctypes.POINTER(_P)]),
     ("chapsim_props_destroy", _I, [_P]),
     ("chapsim_props_last_error", ctypes.c_char_p, [_P]),

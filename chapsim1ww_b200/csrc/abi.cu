@@ -1406,6 +1406,21 @@ int chapsim_set_tuning(chapsim_ctx *ctx, int rhs_nzc, int fft_lb) {
   return CHAPSIM_OK;
 }
 
+int chapsim_set_line_tuning(chapsim_ctx *ctx, int ysolve_bx) {
+  if (!ctx || (ysolve_bx != 64 && ysolve_bx != 128 && ysolve_bx != 256)) return CHAPSIM_ERR_ARG;
+  ctx->ys_bx = ysolve_bx;
+  if (ctx->step_graph) { cudaGraphExecDestroy(ctx->step_graph); ctx->step_graph = nullptr; }
+  for (auto &g : ctx->io_graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  return CHAPSIM_OK;
+}
+
+int chapsim_get_line_tuning(const chapsim_ctx *ctx, int *ysolve_bx) {
+  if (!ctx || !ysolve_bx) return CHAPSIM_ERR_ARG;
+  *ysolve_bx = ctx->ys_bx;
+  return CHAPSIM_OK;
+}
+
 int chapsim_get_tuning(const chapsim_ctx *ctx, int *rhs_nzc, int *fft_lb) {
   if (!ctx || !rhs_nzc || !fft_lb) return CHAPSIM_ERR_ARG;
   *rhs_nzc = ctx->rhs_nzc;

@@ -162,11 +162,13 @@ static int autotune_channel(chapsim_batch *b, chapsim_ctx *c, int reps) {
     b->err = "autotune: saving the channel state failed";
     return CHAPSIM_ERR_CUDA;
   }
-  // candidate launch shapes
+  // candidate launch shapes: RHS z segment x transform rows per block,
+  // then, with those fixed, the y-line block width of the Poisson solve
   const int nzc_c[] = {8, 16, 32, 64};
   const int lb_c[] = {0, 4, 8, 16};
+  const int ys_c[] = {64, 128, 256};
   float best = 1e30f;
-  int bn = c->rhs_nzc, bl = c->fft_lb;
+  int bn = c->rhs_nzc, bl = c->fft_lb, by = c->ys_bx;
   for (int nzc : nzc_c) {
     if (nzc > c->d.nz || rc) continue;
     for (int lb : lb_c) {
@@ -179,6 +181,14 @@ static int autotune_channel(chapsim_batch *b, chapsim_ctx *c, int reps) {
   }
   c->rhs_nzc = bn;
   c->fft_lb = bl;
+  for (int ys : ys_c) {
+    if (rc || ys == by) continue;
+    c->ys_bx = ys;
+    float ms = 0.f;
+    if ((rc = time_substeps(c, reps, &ms))) break;
+    if (ms < best) { best = ms; by = ys; }
+  }
+  c->ys_bx = by;
   // single exit: restore the saved state, then free the buffer
   const bool restored = copy_all(false) && cudaStreamSynchronize(c->stream) == cudaSuccess;
   if (!restored) cudaGetLastError();

@@ -151,6 +151,7 @@ struct chapsim_ctx {
   bool refine = true;       // mixed form: one FP64-residual refinement sweep
   int rhs_nzc = 16;   // z planes per block of k_rhs_tma (autotunable)
   int fft_lb = 0;     // rows per block of the x transforms (0: default)
+  int ys_bx = 128;    // spectral y-lines per block of k_ysolve_line (64, 128 or 256; autotunable)
   // CUDA graph of one full step (NS = 1, 2, 3)
   cudaGraphExec_t step_graph = nullptr;
   int64_t kernels_per_step = 0;

@@ -1113,7 +1113,7 @@ __global__ void k_ypivots(TGDev d) {
 // them, so YB loads per thread are in flight instead of one.
 constexpr int YB = 8;
 template <typename T>
-__global__ void __launch_bounds__(128) k_ysolve_line(TGDev d) {
+__global__ void __launch_bounds__(256) k_ysolve_line(TGDev d) {
   typedef typename Cplx<T>::type C;
   const int lh = d.lh, ny = d.ny;
   const int kx = blockIdx.x * blockDim.x + threadIdx.x, kz = blockIdx.y;
@@ -1480,8 +1480,9 @@ template <typename T> struct Prec {
     }
     if (mark) phase_mark(c, CHAPSIM_PH_YSOLVE);
     {
-      dim3 grid((d.lh + 127) / 128, d.nz);
-      k_ysolve_line<T><<<grid, 128, 0, c->stream>>>(d);
+      const int bx = c->ys_bx;
+      dim3 grid((d.lh + bx - 1) / bx, d.nz);
+      k_ysolve_line<T><<<grid, bx, 0, c->stream>>>(d);
       LAUNCHED();
     }
     if (mark) phase_mark(c, CHAPSIM_PH_IFFTZ);

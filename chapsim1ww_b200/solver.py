@@ -253,6 +253,14 @@ class TGChannel:
     def set_tuning(self, rhs_nzc=16, fft_lb=0):
         self._chk(self.lib.chapsim_set_tuning(self.h, rhs_nzc, fft_lb))
 
+    def set_line_tuning(self, ysolve_bx=128):
+        self._chk(self.lib.chapsim_set_line_tuning(self.h, ysolve_bx))
+
+    def get_line_tuning(self):
+        a = ctypes.c_int()
+        self._chk(self.lib.chapsim_get_line_tuning(self.h, ctypes.byref(a)))
+        return a.value
+
     def get_tuning(self):
         a, b = ctypes.c_int(), ctypes.c_int()
         self._chk(self.lib.chapsim_get_tuning(self.h, ctypes.byref(a), ctypes.byref(b)))

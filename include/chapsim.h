@@ -284,6 +284,10 @@ int chapsim_phase_reset(chapsim_ctx *ctx);
  * the mass-flux sum (round-off level). */
 int chapsim_set_tuning(chapsim_ctx *ctx, int rhs_nzc, int fft_lb);
 int chapsim_get_tuning(const chapsim_ctx *ctx, int *rhs_nzc, int *fft_lb);
+/* Spectral y-lines per block of the Poisson y-solve (64, 128 = default, or
+ * 256).  Results do not depend on it. */
+int chapsim_set_line_tuning(chapsim_ctx *ctx, int ysolve_bx);
+int chapsim_get_line_tuning(const chapsim_ctx *ctx, int *ysolve_bx);
 
 /* Number of kernel launches the library issued on this context since creation
  * (or the last reset). */
@@ -557,9 +561,10 @@ int chapsim_batch_channel(chapsim_batch *b, int i, chapsim_ctx **ctx);
 /* chapsim_init_random on every channel, channel i with seed + i. */
 int chapsim_batch_init_random(chapsim_batch *b, uint64_t seed, double amp, int project);
 /* Autotuner: for every channel, time each candidate launch shape (z-segment
- * length of the RHS kernel, rows per block of the x transforms) over `reps`
- * substeps and keep the fastest.  The channel state is saved before and
- * restored after the trials. */
+ * length of the RHS kernel, rows per block of the x transforms, then the
+ * y-line block width of the Poisson solve) over `reps` substeps and keep the
+ * fastest.  The channel state is saved before and restored after the
+ * trials. */
 int chapsim_batch_autotune(chapsim_batch *b, int reps);
 /* nsteps time steps of every channel (one graph launch per step). */
 int chapsim_batch_step(chapsim_batch *b, int nsteps);

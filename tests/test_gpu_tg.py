@@ -242,3 +242,33 @@ def test_short_lines_wrap():
         g.solverrk3_mom_tg(ns)
         o.substep(ns)
     compare(g, o, tag="short")
+
+
+def test_line_tuning_does_not_change_results():
+    """The y-line block width of the Poisson solve (64, 128, 256: one of the
+    autotuner's launch shapes) leaves every field bitwise unchanged, TG and
+    IO."""
+    _need_gpu()
+    from chapsim1ww_b200 import IOChannel, TGChannel
+    from oracle.pyoracle import synth_table
+    out = []
+    for bx in (64, 128, 256):
+        g = TGChannel(48, 20, 40)
+        g.set_line_tuning(bx)
+        assert g.get_line_tuning() == bx
+        g.random_fl_fld_tg(3, 0.1, project=True)
+        g.step(2)
+        out.append([g.get_field(n) for n in ("u", "v", "w", "p")])
+        g.close()
+    for a in out[1:]:
+        assert all(np.array_equal(x, y) for x, y in zip(out[0], a))
+    table = synth_table(4096)
+    res = []
+    for bx in (64, 256):
+        g = IOChannel(40, 18, 24, table=table)
+        g.set_line_tuning(bx)
+        g.random_fl_theml_fld_io(2, 0.1)
+        g.step(1)
+        res.append([g.get_field(n) for n in ("gx", "p", "h")])
+        g.close()
+    assert all(np.array_equal(x, y) for x, y in zip(*res))
