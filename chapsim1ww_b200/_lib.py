@@ -39,7 +39,7 @@ class ChapsimIOConfig(ctypes.Structure):
         ("struct_size", ctypes.c_int32), ("thermal", ctypes.c_int32), ("prt", ctypes.c_double),
         ("qw_bot", ctypes.c_double), ("qw_top", ctypes.c_double), ("gravdir", ctypes.c_int32),
         ("visc_scheme", ctypes.c_int32), ("f_a", ctypes.c_double),
-        ("coupled", ctypes.c_int32), ("reserved", ctypes.c_int32),
+        ("coupled", ctypes.c_int32), ("isothermal", ctypes.c_int32),
     ]
 
 

@@ -542,6 +542,7 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
       io.cthecd = 1.0 / cfg->ren / iocfg->prt;  // CTHECD, src/Flow_State.f90:87
       io.qw_bot = iocfg->qw_bot;
       io.qw_top = iocfg->qw_top;
+      io.isothermal = iocfg->thermal ? iocfg->isothermal : 0;
       io.gravdir = iocfg->gravdir;
       io.f_a = iocfg->f_a;
       io.cfgv = cfg->cfgv;
@@ -607,7 +608,7 @@ int chapsim_io_config_default(chapsim_io_config *io) {
   io->visc_scheme = 0;
   io->f_a = 0.0;
   io->coupled = 0;
-  io->reserved = 0;
+  io->isothermal = 0;
   return CHAPSIM_OK;
 }
 
@@ -618,6 +619,7 @@ int chapsim_create_io(const chapsim_config *cfg, const chapsim_io_config *io, ch
   if (!(io->prt > 0) || io->gravdir < 0 || io->gravdir > 3) return CHAPSIM_ERR_ARG;
   if (io->visc_scheme != 0 && io->visc_scheme != 1) return CHAPSIM_ERR_ARG;
   if (io->coupled != 0 && io->coupled != 1) return CHAPSIM_ERR_ARG;
+  if (io->isothermal < 0 || io->isothermal > 3 || (io->isothermal && !io->thermal)) return CHAPSIM_ERR_ARG;
   return create_ctx(cfg, io, out);
 }
 
@@ -1128,6 +1130,22 @@ int chapsim_set_table(chapsim_ctx *ctx, const double *H, const double *T, const 
     if (dv * h > rm) rm = dv * h;
   }
   io.rhohmax = rm;
+  // iso-thermal walls (WALL_ISOTHERMAL_GIVEN, src/Flow_State.f90:603-645):
+  // h, rho, mu, k at the wall temperature from the T-splines of the table
+  for (int side = 0; side < 2; ++side) {
+    if (!(io.isothermal & (1 << side))) continue;
+    const double tw = side == 0 ? io.qw_bot : io.qw_top;
+    double v[4];
+    bool ok = true;
+    for (int q = 0; q < 4; ++q) {
+      const int col = q == 0 ? 0 : q + 1;  // H, D, M, K against T
+      const HostSpline sp(ctx->tab[1], ctx->tab[col]);
+      ok = ok && sp.eval(tw, v[q]);
+    }
+    REQUIRE(ok, CHAPSIM_ERR_ARG, "iso-thermal wall temperature outside the property table");
+    io.wall[side][0] = tw;
+    for (int q = 0; q < 4; ++q) io.wall[side][q + 1] = v[q];
+  }
   ctx->has_table = true;
   ctx->props_mode = CHAPSIM_PROPS_TABLE;  // a model trained on another table no longer applies
   return CHAPSIM_OK;
@@ -1246,6 +1264,8 @@ int chapsim_io_bc_outlet_eng(chapsim_ctx *ctx, int ns) {
   REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
   REQUIRE(ctx->io.thermal && ctx->has_table, CHAPSIM_ERR_STATE,
           "the outlet energy condition needs the energy equation and a property table");
+  REQUIRE(!ctx->io.isothermal, CHAPSIM_ERR_UNSUPPORTED,
+          "the outlet plane's wall ghost rows are built for iso-flux walls only");
   CKC(cudaSetDevice(ctx->device));
   return io_bc_outlet_eng(ctx, ns);
 }

@@ -61,6 +61,10 @@ struct IODev {
   chapsim_spl::Spline ht, td, tm, tk;          // h -> T; T -> rho, mu, k
   double cthecd, qw_bot, qw_top, rhohmax, f_a, cfgv;
   int thermal, shortcuts, gravdir, flowdrvtp;
+  // iso-thermal walls: bit 0 bottom, bit 1 top (BCWALLHEAT); wall[side] =
+  // T, h, rho, mu, k at the wall temperature (qw_bot / qw_top hold it)
+  int isothermal;
+  double wall[2][5];
   double *dpg;       // device scalar: DPGRNS of the current substep
   double *part;      // per-block partial sums of the x mass-flux forcing
   unsigned long long *bad;  // table look-ups outside the table

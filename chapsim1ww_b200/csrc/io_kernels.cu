@@ -123,13 +123,17 @@ __global__ void __launch_bounds__(IO_BX *IO_BY, 6) k_io_eng_rhs(TGDev d, IODev i
   const double coe1 = d.dxi * 0.5 * 0.5, coe11 = d.dxqi * 0.5 * io.cthecd;
   const double coe2 = d.dyfi[j] * 0.5, coe3 = d.dzi * 0.5 * 0.5;
   const double coe33 = d.dzqi * 0.5 * io.cthecd, coe22 = d.dyfi[j] * io.cthecd;
+  // the wall rows: an iso-flux wall takes its flux with coefficient 1, an
+  // iso-thermal wall the conduction to its ghost row (the wall values, half a
+  // cell away: DYCI of the wall node), src/RHS_ENERGY_EXPLICIT.f90:41-72
+  const bool iso_bot = io.isothermal & 1, iso_top = io.isothermal & 2;
   double coe221, coe222;
   if (j == 1) {
     coe221 = d.dyci[j + 1];
-    coe222 = 1.0;
+    coe222 = iso_bot ? d.dyci[j] : 1.0;
   } else if (j == ny) {
     coe222 = d.dyci[j];
-    coe221 = 1.0;
+    coe221 = iso_top ? d.dyci[j + 1] : 1.0;
   } else {
     coe221 = d.dyci[j + 1];
     coe222 = d.dyci[j];
@@ -148,9 +152,9 @@ __global__ void __launch_bounds__(IO_BX *IO_BY, 6) k_io_eng_rhs(TGDev d, IODev i
   dx_kdt *= coe11;
   double kdty1 = (wffp * K[c + sy] + wfbp * kc) * (T[c + sy] - tc) * coe221;
   double kdty2 = (wff * kc + wfb * K[c - sy]) * (tc - T[c - sy]) * coe222;
-  if (j == 1)
+  if (j == 1 && !iso_bot)
     kdty2 = -io.qw_bot * coe222;  // WALLFLUX(bottom) = +qw
-  else if (j == ny)
+  else if (j == ny && !iso_top)
     kdty1 = io.qw_top * coe221;   // -WALLFLUX(top), WALLFLUX(top) = -qw
   const double dy_kdt = (kdty1 - kdty2) * coe22;
   double dz_kdt = (K[c + ozp] + kc) * (T[c + ozp] - tc) - (K[c + ozm] + kc) * (tc - T[c + ozm]);
@@ -220,16 +224,26 @@ __global__ void k_io_eng_ghost(TGDev d, IODev io) {
   const bool top = blockIdx.y == 1;
   const int j = top ? ny + 1 : 0;
   const int64_t c = base + sy * j;
-  double h;
-  if (!top)
-    h = 2.0 * io.h[base + sy] - d.wff[2] * io.h[base + 2 * sy] - d.wfb[2] * io.h[base + sy];
-  else
-    h = 2.0 * io.h[base + sy * ny] - d.wff[ny] * io.h[base + sy * ny] - d.wfb[ny] * io.h[base + sy * (ny - 1)];
-  io.h[c] = h;
-  double T, D, M, K;
-  if (!look_ht(io, h, T) || !look_tprops(io, T, D, M, K)) {
-    atomicAdd(io.bad, 1ull);
-    return;
+  const int side = top ? 1 : 0;
+  double h, T, D, M, K;
+  if (io.isothermal & (1 << side)) {
+    // BC_WALL_ISOTHERMAL (src/BC_WALL.f90:462-515): the wall values
+    T = io.wall[side][0];
+    h = io.wall[side][1];
+    D = io.wall[side][2];
+    M = io.wall[side][3];
+    K = io.wall[side][4];
+    io.h[c] = h;
+  } else {
+    if (!top)
+      h = 2.0 * io.h[base + sy] - d.wff[2] * io.h[base + 2 * sy] - d.wfb[2] * io.h[base + sy];
+    else
+      h = 2.0 * io.h[base + sy * ny] - d.wff[ny] * io.h[base + sy * ny] - d.wfb[ny] * io.h[base + sy * (ny - 1)];
+    io.h[c] = h;
+    if (!look_ht(io, h, T) || !look_tprops(io, T, D, M, K)) {
+      atomicAdd(io.bad, 1ull);
+      return;
+    }
   }
   io.D[c] = D;
   io.T[c] = T;

@@ -400,8 +400,10 @@ typedef struct chapsim_io_config {
   int32_t struct_size; /* sizeof(chapsim_io_config)                               */
   int32_t thermal;     /* thermlflg: 1 energy equation + table properties, 0 off   */
   double prt;          /* PRT0, Prandtl number                                     */
-  double qw_bot;       /* iso-flux bottom wall: heat flux, > 0 heats the fluid      */
-  double qw_top;       /* iso-flux top wall (WALLFLUX = -qw_top, Flow_State.f90:124-148) */
+  double qw_bot;       /* iso-flux bottom wall: heat flux, > 0 heats the fluid; an
+                          iso-thermal bottom wall: its temperature (WHEAT0_UNDIM) */
+  double qw_top;       /* iso-flux top wall (WALLFLUX = -qw_top, Flow_State.f90:124-148);
+                          iso-thermal: its temperature                          */
   int32_t gravdir;     /* GRAVDIR: 0 none, 1/2/3 buoyancy along x/y/z             */
   int32_t visc_scheme; /* visthemflg (readdata.ini:23): 0 explicit viscous terms,
                           1 semi-implicit (VISCOUS_PAR_EXPLT_*_io + MOMFA_io,
@@ -411,11 +413,16 @@ typedef struct chapsim_io_config {
                           section (src/READINI.f90:121-131); its instantaneous-field
                           files then take the prefix DNS_perioz instead of
                           DNS_perixz (src/processing/WRT_VARS_IO.f90:24-28)      */
-  int32_t reserved;    /* 0                                                       */
+  int32_t isothermal;  /* BCWALLHEAT: bit 0 the bottom wall, bit 1 the top wall is
+                          iso-thermal (BC_WALL_ISOTHERMAL, src/BC_WALL.f90:462-515:
+                          ghost rows hold the wall values of T, h, rho, mu, k,
+                          from the table at the wall temperature,
+                          WALL_ISOTHERMAL_GIVEN, src/Flow_State.f90:603-645);
+                          a clear bit keeps the iso-flux wall (BC_WALL_ISOFLUX)  */
 } chapsim_io_config;
 
-/* Defaults: thermal on, Pr = 0.71, qw = 1 on both walls, no buoyancy,
- * explicit viscous terms. */
+/* Defaults: thermal on, Pr = 0.71, qw = 1 on both walls (iso-flux), no
+ * buoyancy, explicit viscous terms. */
 int chapsim_io_config_default(chapsim_io_config *io);
 
 /* IO domain set-up (MEM_ALLOCAT + COORDJR + FISHPACK_POIS3D_INIT,
@@ -425,7 +432,10 @@ int chapsim_io_config_default(chapsim_io_config *io);
 int chapsim_create_io(const chapsim_config *cfg, const chapsim_io_config *io, chapsim_ctx **out);
 
 /* Property table of an IO context: columns H, T, D, M, K (host, length n >= 4,
- * H and T increasing), splined as NIST_SPLINE_H / NIST_SPLINE_T.  shortcuts
+ * H and T increasing), splined as NIST_SPLINE_H / NIST_SPLINE_T.  An
+ * iso-thermal wall takes its h, rho, mu, k from the table's T-splines at the
+ * wall temperature here (CHAPSIM_ERR_ARG when that temperature is outside the
+ * table).  shortcuts
  * != 0 keeps the reference-state shortcuts of the look-ups (h = 0 -> T = 1;
  * T = 1 -> rho = mu = k = 1; cells with |h| < 1e-10 keep their properties,
  * src/Flow_State.f90:1068,1470 and src/THERM_PROP_UPDATE.f90:168-173), which

@@ -133,7 +133,11 @@ struct oracle_io {
   // table
   bool has_table = false;
   int shortcuts = 0;
-  Spl ht, td, tm, tk, hd;
+  Spl ht, td, tm, tk, hd, th;
+  // BCWALLHEAT: bit 0 bottom, bit 1 top iso-thermal; wall[side] = T, h, rho,
+  // mu, k at the wall temperature (qw[side] holds it)
+  int isothermal = 0;
+  double wall[2][5] = {{0.0}};
   double rhohmax = 0.0;
   int64_t bad = 0;
   // flow fields (1..3 used)
@@ -187,11 +191,25 @@ bool lookup_t(const oracle_io *o, const Spl &s, double T, double &v) {
 }
 
 // BC_WALL_ISOFLUX (src/BC_WALL.f90:522-627): ghost enthalpy extrapolated from
-// the first two cells, ghost properties from the table.
+// the first two cells, ghost properties from the table; BC_WALL_ISOTHERMAL
+// (src/BC_WALL.f90:462-515) on an iso-thermal wall: the wall values.
 void bc_wall_thermal(oracle_io *o) {
   const int nx = o->nx, ny = o->ny, nz = o->nz;
   for (int side = 0; side < 2; ++side) {
     const int j = side == 0 ? 0 : ny + 1;
+    if (o->isothermal & (1 << side)) {
+      const double *w = o->wall[side];
+      for (int k = 1; k <= nz; ++k)
+        for (int i = 1; i <= nx; ++i) {
+          F(tt, i, j, k) = w[0];
+          F(hh, i, j, k) = w[1];
+          F(dd, i, j, k) = w[2];
+          F(mu, i, j, k) = w[3];
+          F(kk, i, j, k) = w[4];
+          F(rhoh, i, j, k) = w[1] * w[2];
+        }
+      continue;
+    }
     for (int k = 1; k <= nz; ++k)
       for (int i = 1; i <= nx; ++i) {
         double h;
@@ -215,7 +233,8 @@ void bc_wall_thermal(oracle_io *o) {
   }
 }
 
-// RHS_ENERGY_EXPLICIT (src/RHS_ENERGY_EXPLICIT.f90:1-150), iso-flux walls.
+// RHS_ENERGY_EXPLICIT (src/RHS_ENERGY_EXPLICIT.f90:1-150), iso-flux or
+// iso-thermal walls (:41-72, :118-123).
 void rhs_energy(oracle_io *o) {
   const int nx = o->nx, ny = o->ny, nz = o->nz;
   const double coe1 = o->dxi * XND2CL * 0.5, coe11 = o->dxqi * XND2CL * o->cthecd;
@@ -226,13 +245,14 @@ void rhs_energy(oracle_io *o) {
       const int jp = j + 1, jm = j - 1;
       const double coe2 = o->dyfi[j] * 0.5, coe3 = o->dzi * ZND2CL * 0.5;
       const double coe33 = o->dzqi * ZND2CL * o->cthecd, coe22 = o->dyfi[j] * o->cthecd;
+      const bool iso_bot = o->isothermal & 1, iso_top = o->isothermal & 2;
       double coe221, coe222;
       if (j == 1) {
         coe221 = o->dyci[jp];
-        coe222 = 1.0;
+        coe222 = iso_bot ? o->dyci[j] : 1.0;
       } else if (j == ny) {
         coe222 = o->dyci[j];
-        coe221 = 1.0;
+        coe221 = iso_top ? o->dyci[jp] : 1.0;
       } else {
         coe221 = o->dyci[jp];
         coe222 = o->dyci[j];
@@ -255,9 +275,9 @@ void rhs_energy(oracle_io *o) {
         dx_kdt *= coe11;
         double kdty1 = (o->wff[jp] * F(kk, i, jp, k) + o->wfb[jp] * kc) * (F(tt, i, jp, k) - tc) * coe221;
         double kdty2 = (o->wff[j] * kc + o->wfb[j] * F(kk, i, jm, k)) * (tc - F(tt, i, jm, k)) * coe222;
-        if (j == 1)
+        if (j == 1 && !iso_bot)
           kdty2 = -wallflux_bot * coe222;
-        else if (j == ny)
+        else if (j == ny && !iso_top)
           kdty1 = -wallflux_top * coe221;
         const double dy_kdt = (kdty1 - kdty2) * coe22;
         double dz_kdt = (F(kk, i, j, kpp) + kc) * (F(tt, i, j, kpp) - tc) - (F(kk, i, j, kmm) + kc) * (tc - F(tt, i, j, kmm));
@@ -1407,6 +1427,7 @@ int oracle_io_set_table(oracle_io *o, const double *H, const double *T, const do
   o->tm.build(T, M, n);
   o->tk.build(T, K, n);
   o->hd.build(H, D, n);
+  o->th.build(T, H, n);
   o->shortcuts = shortcuts ? 1 : 0;
   o->has_table = true;
   // RHOHmax (src/Flow_State.f90:963-990): max of D(h) h over 3n - 1 samples
@@ -1423,6 +1444,25 @@ int oracle_io_set_table(oracle_io *o, const double *H, const double *T, const do
 }
 
 double oracle_io_rhohmax(const oracle_io *o) { return o->rhohmax; }
+
+// BCWALLHEAT = isoThermalWall on the walls of `bits` (bit 0 bottom, bit 1
+// top), the wall temperature being qw of that wall; WALL_ISOTHERMAL_GIVEN
+// (src/Flow_State.f90:603-645) takes h, rho, mu, k at it from the table's
+// T-splines (NIST_SLEVAL_TH/TD/TM/TK).  Call after oracle_io_set_table and
+// before the initial field; -1 when a wall temperature is outside the table.
+int oracle_io_set_walls(oracle_io *o, int bits) {
+  if (bits < 0 || bits > 3 || (bits && (!o->thermal || !o->has_table))) return -1;
+  for (int side = 0; side < 2; ++side) {
+    if (!(bits & (1 << side))) continue;
+    const double tw = o->qw[side];
+    double *w = o->wall[side];
+    w[0] = tw;
+    if (!o->th.eval(tw, w[1]) || !o->td.eval(tw, w[2]) || !o->tm.eval(tw, w[3]) || !o->tk.eval(tw, w[4]))
+      return -1;
+  }
+  o->isothermal = bits;
+  return 0;
+}
 
 void oracle_io_init_random(oracle_io *o, uint64_t seed, double amp) {
   const int nx = o->nx, ny = o->ny, nz = o->nz;

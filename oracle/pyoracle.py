@@ -77,6 +77,8 @@ def load(build=True):
     L.oracle_io_set_plane.argtypes = [P, I, P]
     L.oracle_io_bc_scalars.argtypes = [P, P]
     L.oracle_io_stats.argtypes = [P, P]
+    L.oracle_io_set_walls.argtypes = [P, I]
+    L.oracle_io_set_walls.restype = I
     L.oracle_tg_stats.argtypes = [P, P]
     L.oracle_set_threads.argtypes = [I]
     L.oracle_get_threads.restype = I
@@ -200,7 +202,7 @@ class OracleIO:
 
     def __init__(self, nx, ny, nz, lx=8 * math.pi, lz=4 * math.pi / 3, str2=2.0, istr2=1, ren=2800.0, dt=1e-3,
                  flowdrvtp=1, cfgv=0.0, thermal=1, prt=0.71, qw=(1.0, 1.0), gravdir=0, f_a=0.0, table=None,
-                 shortcuts=0, visc_scheme=0):
+                 shortcuts=0, visc_scheme=0, isothermal=0):
         self.L = load()
         self.h = self.L.oracle_io_create(nx, ny, nz, lx, lz, str2, istr2, ren, dt, flowdrvtp, cfgv, thermal, prt,
                                          qw[0], qw[1], gravdir, f_a)
@@ -214,6 +216,8 @@ class OracleIO:
             self._table = [np.ascontiguousarray(c, dtype=np.float64) for c in table[:5]]
             assert self.L.oracle_io_set_table(self.h, *[c.ctypes.data for c in self._table], len(self._table[0]),
                                               shortcuts) == 0
+        if isothermal:
+            assert self.L.oracle_io_set_walls(self.h, int(isothermal)) == 0
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -112,9 +112,10 @@ class IO(TG):
     the y mesh and the Poisson y-operator are the TG restatement's."""
 
     def __init__(self, nx, ny, nz, lx, lz, str2=2.0, istr2=1, ren=2800.0, dt=1e-3, thermal=0, prt=0.71,
-                 qw=(1.0, 1.0), table=None, visc_scheme=0):
+                 qw=(1.0, 1.0), table=None, visc_scheme=0, isothermal=0):
         super().__init__(nx, ny, nz, lx, lz, str2=str2, istr2=istr2, ren=ren, dt=dt)
         self.thermal, self.qw, self.visc = thermal, qw, visc_scheme
+        self.iso = (bool(isothermal & 1), bool(isothermal & 2))  # BCWALLHEAT bottom, top
         self.drhoi = {c: np.zeros((nz, ny + 2, nx)) for c in (1, 2, 3)}
         self.cvisc, self.cthecd = 1.0 / ren, 1.0 / ren / prt
         shape = (nz, ny + 2, nx)
@@ -127,6 +128,12 @@ class IO(TG):
         if thermal:
             H, Tt, D, M, K = (np.asarray(c, float) for c in (table if table is not None else synth_table())[:5])
             self.ht, self.td, self.tm, self.tk = Spline(H, Tt), Spline(Tt, D), Spline(Tt, M), Spline(Tt, K)
+            th = Spline(Tt, H)
+            # WALL_ISOTHERMAL_GIVEN: T, h, rho, mu, k at each iso-thermal wall's temperature
+            self.wall = [None if not self.iso[s] else
+                         tuple(float(v) for v in (qw[s], th(np.array([qw[s]]))[0], self.td(np.array([qw[s]]))[0],
+                                                  self.tm(np.array([qw[s]]))[0], self.tk(np.array([qw[s]]))[0]))
+                         for s in (0, 1)]
             n = len(H)
             hs = H[0] + np.arange(1, 3 * n) * (H[-1] - H[0]) / (3 * n)
             self.rhohmax = max(-1e-14, float(np.max(Spline(H, D)(hs) * hs)))
@@ -193,11 +200,17 @@ class IO(TG):
         return T, self.td(T), self.tm(T), self.tk(T)
 
     def wall_thermal(self):
-        """BC_WALL_ISOFLUX: ghost enthalpy extrapolated, ghost properties from the table."""
+        """BC_WALL_ISOFLUX: ghost enthalpy extrapolated, ghost properties from the
+        table; BC_WALL_ISOTHERMAL on an iso-thermal wall: the wall values."""
         ny, h = self.ny, self.h
         hb = 2.0 * h[:, 1] - self.wff[2] * h[:, 2] - self.wfb[2] * h[:, 1]
         ht = 2.0 * h[:, ny] - self.wff[ny] * h[:, ny] - self.wfb[ny] * h[:, ny - 1]
-        for j, hg in ((0, hb), (ny + 1, ht)):
+        for side, j, hg in ((0, 0, hb), (1, ny + 1, ht)):
+            if self.iso[side]:
+                Tw, hw, Dw, Mw, Kw = self.wall[side]
+                self.h[:, j], self.T[:, j], self.D[:, j], self.mu[:, j], self.k[:, j] = hw, Tw, Dw, Mw, Kw
+                self.rhoh[:, j] = hw * Dw
+                continue
             T, D, M, K = self.table_props(hg)
             self.h[:, j], self.T[:, j], self.D[:, j], self.mu[:, j], self.k[:, j] = hg, T, D, M, K
             self.rhoh[:, j] = hg * D
@@ -218,12 +231,16 @@ class IO(TG):
         dxk = ((X(K, 1) + X(K)) * (X(T, 1) - X(T)) - (X(K) + X(K, -1)) * (X(T) - X(T, -1))) * (self.dxi ** 2 * 0.5 * self.cthecd)
         c_up = self.dyci[2:ny + 2].copy()
         c_dn = self.dyci[1:ny + 1].copy()
-        c_up[-1] = 1.0
-        c_dn[0] = 1.0
+        if not self.iso[1]:
+            c_up[-1] = 1.0
+        if not self.iso[0]:
+            c_dn[0] = 1.0
         k_up = (wffp * X(K, 0, 1) + wfbp * X(K)) * (X(T, 0, 1) - X(T)) * c_up[None, :, None]
         k_dn = (wff * X(K) + wfb * X(K, 0, -1)) * (X(T) - X(T, 0, -1)) * c_dn[None, :, None]
-        k_dn[:, 0, :] = -self.qw[0]  # heat flux into the fluid through the bottom wall
-        k_up[:, -1, :] = self.qw[1]  # and through the top wall
+        if not self.iso[0]:
+            k_dn[:, 0, :] = -self.qw[0]  # heat flux into the fluid through the bottom wall
+        if not self.iso[1]:
+            k_up[:, -1, :] = self.qw[1]  # and through the top wall
         dyk = (k_up - k_dn) * (row(self.dyfi) * self.cthecd)
         dzk = ((X(K, 0, 0, 1) + X(K)) * (X(T, 0, 0, 1) - X(T)) - (X(K, 0, 0, -1) + X(K)) * (X(T) - X(T, 0, 0, -1))) * (self.dzi ** 2 * 0.5 * self.cthecd)
         R = -dxr - dyr - dzr + dxk + dyk + dzk

@@ -213,3 +213,36 @@ def test_io_golden_fixture(name):
         assert relerr(g.get_field(n), z["end_" + n]) < TOL, n
     assert g.divgck_io() < 1e-12
     assert abs(g.bulk_massflux_io() - float(z["end_bulk_g"])) < 1e-12
+
+
+@pytest.mark.parametrize("walls,visc", [(3, 0), (1, 0), (2, 1)])
+def test_io_isothermal_wall_parity(walls, visc):
+    """BCWALLHEAT = isoThermalWall (BC_WALL_ISOTHERMAL, src/BC_WALL.f90:462-515,
+    with the wall rows of RHS_ENERGY_EXPLICIT, src/RHS_ENERGY_EXPLICIT.f90:41-72)
+    on both walls or one, explicit and semi-implicit viscous terms: the GPU
+    against the oracle after every substep of two RK3 steps, FP64 within
+    1e-10; the ghost rows hold the wall values."""
+    g, o = pair(40, 18, 24, thermal=1, qw=(0.95, 0.80), isothermal=walls, visc_scheme=visc)
+    compare(g, o, FLOW + THERMAL, tag="init+projection")
+    for step in range(2):
+        for ns in (1, 2, 3):
+            g.solverrk3_eng_io(ns)
+            o.eng(ns)
+            compare(g, o, THERMAL + ("rho0", "mu0", "rhse0"), tag=f"step{step} eng{ns}")
+            g.solverrk3_mom_io(ns)
+            o.mom(ns)
+            compare(g, o, FLOW, tag=f"step{step} mom{ns}")
+    T = g.get_field("t")
+    for side, j in ((0, 0), (1, 19)):
+        if walls & (1 << side):
+            assert np.all(T[:, j, :] == (0.95, 0.80)[side])
+    assert g.bad_cells() == 0 and o.bad_cells() == 0
+    assert g.divgck_io() < 1e-10 and o.divmax() < 1e-10
+
+
+def test_isothermal_wall_outside_table_is_refused():
+    _need_gpu()
+    from chapsim1ww_b200 import ChapsimError, IOChannel
+    from oracle.pyoracle import synth_table
+    with pytest.raises(ChapsimError):
+        IOChannel(16, 12, 8, table=synth_table(4096), qw=(5.0, 0.8), isothermal=1)

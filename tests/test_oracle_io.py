@@ -180,3 +180,35 @@ def test_oracle_io_statistics_match_numpy_restatement(thermal):
     # DVDL2 is symmetric in (m,h) <-> (n,p)
     d2 = a[:, 60:141].reshape(-1, 9, 9)
     assert np.allclose(d2, np.transpose(d2, (0, 2, 1)), rtol=0, atol=1e-14 * np.abs(d2).max())
+
+
+@pytest.mark.parametrize("walls", [3, 1, 2])
+def test_oracle_io_isothermal_walls_match_numpy_restatement(walls):
+    """BCWALLHEAT = isoThermalWall (BC_WALL_ISOTHERMAL, WALL_ISOTHERMAL_GIVEN
+    and the wall rows of RHS_ENERGY_EXPLICIT) on both walls or one: the
+    oracle against the numpy restatement after one RK3 step, FP64 within
+    1e-10; the ghost rows hold the wall values; a wall hotter than the fluid
+    heats the first row and a colder one cools it."""
+    sys.path.insert(0, GOLDEN)
+    from numpy_io import IO
+    dims, lx, lz, tw = (20, 14, 12), 2 * math.pi, math.pi, (0.95, 0.80)
+    n = IO(*dims, lx, lz, istr2=0, ren=1200.0, dt=1.5e-3, thermal=1, qw=tw, isothermal=walls)
+    o = OracleIO(*dims, lx=lx, lz=lz, istr2=0, ren=1200.0, dt=1.5e-3, thermal=1, qw=tw, isothermal=walls)
+    n.init_random(11, 0.15)
+    o.init_random(11, 0.15)
+    h0 = o.get("h")
+    for ns in (1, 2, 3):
+        n.substep(ns)
+        o.substep(ns)
+    for name, a in (("gx", n.g[1]), ("gy", n.g[2]), ("p", n.p), ("h", n.h), ("t", n.T), ("mu", n.mu),
+                    ("rho", n.D)):
+        assert relerr(o.get(name), a) < 1e-10, name
+    T, h = o.get("t"), o.get("h")
+    ny = dims[1]
+    for side, j, jin in ((0, 0, 1), (1, ny + 1, ny)):
+        if walls & (1 << side):
+            assert np.all(T[:, j, :] == tw[side])
+            # T(h = 0) of the table is about 0.867: 0.95 heats, 0.80 cools
+            dh = h[:, jin, :].mean() - h0[:, jin, :].mean()
+            assert (dh > 0) if tw[side] > 0.867 else (dh < 0), (side, dh)
+    assert o.divmax() < 1e-11
