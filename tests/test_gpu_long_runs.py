@@ -10,6 +10,9 @@ The mixed form (FP64 state, FP32 temporaries and spectra, FP64 Poisson lines,
 one FP64-residual refinement sweep) over 50 steps against the FP64 oracle,
 with its errors on u, p and max |div u| printed per checkpoint; stated
 tolerances over 50 steps: u, v, w <= 1e-5, p <= 1e-4, max |div u| <= 1e-8.
+
+Configurations 1 (its TG channel) and 2 run 500 steps, the second form
+against the first from the same state (see the two tests at the end).
 """
 import math
 
@@ -83,3 +86,73 @@ def test_mixed_form_50_steps_against_fp64_oracle():
         assert max(errs["u"], errs["v"], errs["w"]) <= 1e-5, (step, errs)
         assert errs["p"] <= 1e-4, (step, errs)
         assert div <= 1e-8, (step, div)
+
+
+def _rel(a, b):
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def test_config1_tg_channel_500_steps_mixed_against_fp64():
+    """Configuration 1's TG channel (256 x 192 x 256, Lx = 4 pi, Lz = 4 pi / 3,
+    Re_b = 2800, seed 1) run 500 steps in the FP64 and the mixed form from the
+    same state; the mixed form's distance from the FP64 form per 100 steps.
+    Measured on the B200: u 4e-10, v, w 1.5e-8, p 5e-7 at every checkpoint (no
+    growth), max |div u| 5e-15 in both.  Stated bounds: u <= 1e-8, v, w <=
+    1e-6, p <= 1e-5, max |div u| <= 1e-8."""
+    _need_gpu()
+    import chapsim1ww_b200 as cs
+    from chapsim1ww_b200 import TGChannel
+    kw = dict(lx=4 * math.pi, lz=4 * math.pi / 3, ren=2800.0, dt=1e-3)
+    a = TGChannel(256, 192, 256, **kw)
+    b = TGChannel(256, 192, 256, precision=cs.MIXED, **kw)
+    for s in (a, b):
+        s.random_fl_fld_tg(1, 0.1, project=True)
+    for chunk in range(5):
+        a.step(100)
+        b.step(100)
+        e = {n: _rel(b.get_field(n), a.get_field(n)) for n in ("u", "v", "w", "p")}
+        div = b.divgck_tg()
+        print(f"TG 256x192x256, {100 * (chunk + 1)} steps, mixed vs FP64: "
+              + ", ".join(f"{n} {v:.2e}" for n, v in e.items()) + f", max|div u| {div:.2e}")
+        assert e["u"] <= 1e-8 and e["v"] <= 1e-6 and e["w"] <= 1e-6 and e["p"] <= 1e-5, e
+        assert div <= 1e-8
+    a.close()
+    b.close()
+
+
+def test_config2_heated_io_500_steps_learned_against_table():
+    """Configuration 2 (heated IO channel 384 x 192 x 192, synthetic 4096-point
+    table, seed 2) run 500 steps with the table splines and with the learned
+    property model (65,536 samples, seed 2, gated at 1e-4) from the same
+    state.  Measured on the B200 after 500 steps: T 7e-5, rho 7e-5, mu, k
+    2e-5, u 6e-5, p 5e-4, v 1.1e-3 (v is the small wall-normal component; its
+    relative distance grows about linearly, 2e-6 per step), max |div G + drho/dt|
+    4e-15, no tile evaluated twice.  Stated bounds: properties <= 2e-4, u <=
+    2e-4, p <= 2e-3, v <= 5e-3, max |div| <= 1e-8."""
+    _need_gpu()
+    from chapsim1ww_b200 import IOChannel, PropertyEngine, synthetic_table
+    t = synthetic_table(4096)
+    eng = PropertyEngine(*t)
+    eng.train(65536, 2, 20000, 3e-3)
+    assert eng.gate(1e-4, 256)[0] >= 200
+    kw = dict(lx=8 * math.pi, lz=4 * math.pi / 3, ren=2800.0, dt=1e-3, thermal=1, prt=0.71, qw=(1.0, 1.0),
+              table=t[:5])
+    a = IOChannel(384, 192, 192, **kw)
+    b = IOChannel(384, 192, 192, **kw)
+    b.set_props_mode(1, eng)
+    eng.close()
+    for s in (a, b):
+        s.random_fl_theml_fld_io(2, 0.1)
+    for chunk in range(5):
+        a.step(100)
+        b.step(100)
+        e = {n: _rel(b.get_field(n), a.get_field(n)) for n in ("u", "v", "p", "t", "rho", "mu", "k")}
+        div = b.divgck_io()
+        print(f"IO 384x192x192 heated, {100 * (chunk + 1)} steps, learned vs table: "
+              + ", ".join(f"{n} {v:.2e}" for n, v in e.items()) + f", max|div| {div:.2e}")
+        assert max(e["t"], e["rho"], e["mu"], e["k"]) <= 2e-4, e
+        assert e["u"] <= 2e-4 and e["p"] <= 2e-3 and e["v"] <= 5e-3, e
+        assert div <= 1e-8
+    assert b.bad_cells() == 0
+    a.close()
+    b.close()
