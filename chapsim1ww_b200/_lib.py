@@ -40,6 +40,7 @@ class ChapsimIOConfig(ctypes.Structure):
         ("qw_bot", ctypes.c_double), ("qw_top", ctypes.c_double), ("gravdir", ctypes.c_int32),
         ("visc_scheme", ctypes.c_int32), ("f_a", ctypes.c_double),
         ("coupled", ctypes.c_int32), ("isothermal", ctypes.c_int32),
+        ("bcx_in", ctypes.c_int32), ("bcx_out", ctypes.c_int32),
     ]
 
 

@@ -434,6 +434,74 @@ static int build_tables(chapsim_ctx *ctx) {
   return CHAPSIM_OK;
 }
 
+// FISHPACK's x roots and transforms for Dirichlet / Neumann ends
+// (src/possion3d_fishpack_reform.f90:104-163): XRT(I) = -4 DXQI sin^2((I - DI)
+// DX) with DX = pi / (2 (L + LRDEL)); the transforms are FFTPACK's SINT,
+// SINQF / SINQB, COST and COSQF / COSQB (libs/fishpack4.1/fftpack.f, from
+// their documented sums), built as dense matrices, the forward one divided
+// by the final SCALX, both stored transposed for the device kernels.  The
+// spectral descriptor dnp has nx lines with shifts -XRT(I).
+static int xnp_setup(chapsim_ctx *ctx, int lp) {
+  const int n = ctx->cfg.nx;
+  const int lrdel = ((lp - 1) * (lp - 3) * (lp - 5)) / 3;
+  const double sc = (double)(n + lrdel), dx = M_PI / (2.0 * sc);
+  const double di = lp == 2 ? 0.0 : (lp == 4 ? 1.0 : 0.5);
+  const double scalx = (lp == 3 || lp == 5) ? 4.0 * sc : 2.0 * sc;
+  std::vector<double> ak1(n), ft((size_t)n * n), bt((size_t)n * n);
+  for (int i = 1; i <= n; ++i) {
+    const double sn = sin(((double)i - di) * dx);
+    ak1[i - 1] = 4.0 * ctx->d.dxqi * sn * sn;  // -XRT(I)
+  }
+  if (lp == 4) ak1[0] = 0.0;  // sin(0): the zero mode, exactly
+  auto fwd = [&](int i, int k) -> double {  // coefficient of X(K) in the forward output I, 1-based
+    switch (lp) {
+      case 2: return 2.0 * sin((double)k * i * M_PI / (n + 1));
+      case 3: return k == n ? ((i - 1) % 2 ? -1.0 : 1.0) : 2.0 * sin((2.0 * i - 1.0) * k * M_PI / (2.0 * n));
+      case 4:
+        if (k == 1) return 1.0;
+        if (k == n) return (i - 1) % 2 ? -1.0 : 1.0;
+        return 2.0 * cos((double)(k - 1) * (i - 1) * M_PI / (n - 1));
+      default: return k == 1 ? 1.0 : 2.0 * cos((2.0 * i - 1.0) * (k - 1) * M_PI / (2.0 * n));
+    }
+  };
+  auto bwd = [&](int i, int k) -> double {  // coefficient of X(K) in the backward output I
+    switch (lp) {
+      case 3: return 4.0 * sin((2.0 * k - 1.0) * i * M_PI / (2.0 * n));
+      case 5: return 4.0 * cos((2.0 * k - 1.0) * (i - 1) * M_PI / (2.0 * n));
+      default: return fwd(i, k);  // SINT and COST are their own inverses
+    }
+  };
+  for (int i = 1; i <= n; ++i)
+    for (int k = 1; k <= n; ++k) {
+      ft[(size_t)(k - 1) * n + (i - 1)] = fwd(i, k) / scalx;
+      bt[(size_t)(k - 1) * n + (i - 1)] = bwd(i, k);
+    }
+  chapsim::TGDev &s = ctx->dnp;
+  s = ctx->d;
+  s.lh = n;
+  s.lp = n + (n & 1);
+  void *p = nullptr;
+  int rc;
+  const size_t nsp = (size_t)s.lp * ctx->cfg.ny * ctx->cfg.nz;
+  if ((rc = dalloc(ctx, &p, nsp * sizeof(double2)))) return rc;
+  s.spec = p;
+  if ((rc = dalloc(ctx, &p, nsp * sizeof(double2)))) return rc;
+  s.ypiv = (double2 *)p;
+  if ((rc = dalloc(ctx, &p, (size_t)n * sizeof(double)))) return rc;
+  s.ak1 = (const double *)p;
+  CKC(cudaMemcpyAsync(p, ak1.data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  if ((rc = dalloc(ctx, &p, (size_t)n * n * sizeof(double)))) return rc;
+  ctx->xnp_f = (double *)p;
+  CKC(cudaMemcpyAsync(p, ft.data(), (size_t)n * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  if ((rc = dalloc(ctx, &p, (size_t)n * n * sizeof(double)))) return rc;
+  ctx->xnp_b = (double *)p;
+  CKC(cudaMemcpyAsync(p, bt.data(), (size_t)n * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  if ((rc = chapsim::xnp_pivots(ctx))) return rc;
+  CKC(cudaStreamSynchronize(ctx->stream));  // the host vectors go out of scope
+  ctx->xnp = lp;
+  return CHAPSIM_OK;
+}
+
 static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg, chapsim_ctx **out) {
   chapsim_ctx *ctx = nullptr;
   if (!cfg || !out) return CHAPSIM_ERR_ARG;
@@ -575,6 +643,11 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
   ctx->fx = px;
   ctx->fz = pz;
   if ((rc = init_kernels(ctx))) goto fail;
+  if (iocfg && iocfg->bcx_in != 3) {
+    const int b0 = iocfg->bcx_in, b1 = iocfg->bcx_out;
+    const int lp = b0 == 1 ? (b1 == 1 ? 2 : 3) : (b1 == 2 ? 4 : 5);  // LPEROD + 1
+    if ((rc = xnp_setup(ctx, lp))) goto fail;
+  }
   if (iocfg && (rc = io_init_maps(ctx))) goto fail;
   if (iocfg) {
     // reference property values (thermal off, or before the table is set)
@@ -609,6 +682,8 @@ int chapsim_io_config_default(chapsim_io_config *io) {
   io->f_a = 0.0;
   io->coupled = 0;
   io->isothermal = 0;
+  io->bcx_in = 3;
+  io->bcx_out = 3;
   return CHAPSIM_OK;
 }
 
@@ -620,6 +695,10 @@ int chapsim_create_io(const chapsim_config *cfg, const chapsim_io_config *io, ch
   if (io->visc_scheme != 0 && io->visc_scheme != 1) return CHAPSIM_ERR_ARG;
   if (io->coupled != 0 && io->coupled != 1) return CHAPSIM_ERR_ARG;
   if (io->isothermal < 0 || io->isothermal > 3 || (io->isothermal && !io->thermal)) return CHAPSIM_ERR_ARG;
+  if (io->bcx_in < 1 || io->bcx_in > 3 || io->bcx_out < 1 || io->bcx_out > 3 ||
+      ((io->bcx_in == 3) != (io->bcx_out == 3)))
+    return CHAPSIM_ERR_ARG;
+  if (io->bcx_in != 3 && (cfg->precision != CHAPSIM_FP64 || cfg->nx < 4)) return CHAPSIM_ERR_UNSUPPORTED;
   return create_ctx(cfg, io, out);
 }
 
@@ -941,6 +1020,7 @@ static int io_init_random(chapsim_ctx *ctx, uint64_t seed, double amp, int proje
 
 int chapsim_init_random(chapsim_ctx *ctx, uint64_t seed, double amp, int project) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED, "Dirichlet / Neumann x ends (BCX_io): only chapsim_pois3d is built");
   CKC(cudaSetDevice(ctx->device));
   if (ctx->domain == CHAPSIM_IIO) return io_init_random(ctx, seed, amp, project);
   const int nx = ctx->cfg.nx, ny = ctx->cfg.ny, nz = ctx->cfg.nz;
@@ -1009,6 +1089,7 @@ int chapsim_step_tg(chapsim_ctx *ctx, int nsteps) {
 
 int chapsim_divg(chapsim_ctx *ctx, int domain, int ns) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED, "Dirichlet / Neumann x ends (BCX_io): only chapsim_pois3d is built");
   REQUIRE(domain == ctx->domain, CHAPSIM_ERR_ARG, "domain does not match the context");
   REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
   CKC(cudaSetDevice(ctx->device));
@@ -1029,11 +1110,13 @@ int chapsim_pois3d(chapsim_ctx *ctx, int domain) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
   REQUIRE(domain == ctx->domain, CHAPSIM_ERR_ARG, "domain does not match the context");
   CKC(cudaSetDevice(ctx->device));
+  if (ctx->xnp) return xnp_pois3d(ctx);  // Dirichlet / Neumann x ends
   return launch_pois3d(ctx);  // FISHPACK_POIS3D_SIMPLE on an IO context (mean mode pinned last)
 }
 
 int chapsim_velo_correction(chapsim_ctx *ctx, int domain, int ns) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED, "Dirichlet / Neumann x ends (BCX_io): only chapsim_pois3d is built");
   REQUIRE(domain == ctx->domain, CHAPSIM_ERR_ARG, "domain does not match the context");
   REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
   CKC(cudaSetDevice(ctx->device));
@@ -1043,6 +1126,7 @@ int chapsim_velo_correction(chapsim_ctx *ctx, int domain, int ns) {
 
 int chapsim_stats(chapsim_ctx *ctx, int accumulate) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED, "Dirichlet / Neumann x ends (BCX_io): only chapsim_pois3d is built");
   CKC(cudaSetDevice(ctx->device));
   return stats_run(ctx, accumulate);
 }
@@ -1216,6 +1300,7 @@ int chapsim_therm_prop_update(chapsim_ctx *ctx, int iregion, int mode) {
 
 int chapsim_rk3_eng_io(chapsim_ctx *ctx, int ns) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED, "Dirichlet / Neumann x ends (BCX_io): only chapsim_pois3d is built");
   REQUIRE(ctx->domain == CHAPSIM_IIO, CHAPSIM_ERR_STATE, "not an IO context");
   REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
   REQUIRE(ctx->io.thermal, CHAPSIM_ERR_STATE, "thermal is off on this IO context");
@@ -1226,6 +1311,7 @@ int chapsim_rk3_eng_io(chapsim_ctx *ctx, int ns) {
 
 int chapsim_rk3_mom_io(chapsim_ctx *ctx, int ns) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED, "Dirichlet / Neumann x ends (BCX_io): only chapsim_pois3d is built");
   REQUIRE(ctx->domain == CHAPSIM_IIO, CHAPSIM_ERR_STATE, "not an IO context");
   REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
   CKC(cudaSetDevice(ctx->device));
@@ -1313,6 +1399,7 @@ static int io_substeps(chapsim_ctx *ctx) {
 
 int chapsim_step_io(chapsim_ctx *ctx, int nsteps) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED, "Dirichlet / Neumann x ends (BCX_io): only chapsim_pois3d is built");
   REQUIRE(ctx->domain == CHAPSIM_IIO, CHAPSIM_ERR_STATE, "not an IO context");
   REQUIRE(nsteps >= 0, CHAPSIM_ERR_ARG, "nsteps must be >= 0");
   REQUIRE(!ctx->io.thermal || ctx->has_table, CHAPSIM_ERR_STATE, "no property table");
@@ -1351,6 +1438,7 @@ int chapsim_step_io(chapsim_ctx *ctx, int nsteps) {
 
 int chapsim_reduce(chapsim_ctx *ctx, int domain, int what, double *out) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED, "Dirichlet / Neumann x ends (BCX_io): only chapsim_pois3d is built");
   REQUIRE(out, CHAPSIM_ERR_ARG, "null output");
   REQUIRE(domain == ctx->domain, CHAPSIM_ERR_ARG, "domain does not match the context");
   CKC(cudaSetDevice(ctx->device));

@@ -156,6 +156,12 @@ struct chapsim_ctx {
   int rhs_nzc = 16;   // z planes per block of k_rhs_tma (autotunable)
   int fft_lb = 0;     // rows per block of the x transforms (0: default)
   int ys_bx = 128;    // spectral y-lines per block of k_ysolve_line (64, 128 or 256; autotunable)
+  // IO Poisson with Dirichlet / Neumann x ends (BCX_io): FISHPACK's LP, the
+  // spectral descriptor of its nx real x modes and the transposed x-transform
+  // matrices (forward with 1 / SCALX)
+  int xnp = 0;
+  chapsim::TGDev dnp{};
+  double *xnp_f = nullptr, *xnp_b = nullptr;
   // CUDA graph of one full step (NS = 1, 2, 3)
   cudaGraphExec_t step_graph = nullptr;
   int64_t kernels_per_step = 0;
@@ -198,6 +204,8 @@ int flush_phase_events(chapsim_ctx *c);
 int launch_substep(chapsim_ctx *c, int ns);
 int launch_divg(chapsim_ctx *c, int ns);
 int launch_pois3d(chapsim_ctx *c);
+int xnp_pivots(chapsim_ctx *c);
+int xnp_pois3d(chapsim_ctx *c);
 int launch_correction(chapsim_ctx *c, int ns);
 int launch_reduce(chapsim_ctx *c, int what, double *host_out);
 int launch_bc_q(chapsim_ctx *c);

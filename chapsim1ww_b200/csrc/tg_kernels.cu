@@ -1087,7 +1087,9 @@ __global__ void k_ypivots(TGDev d) {
   double *PP = reinterpret_cast<double *>(d.ypiv) + base;
   double *HH = reinterpret_cast<double *>(d.ypiv) + (int64_t)d.lp * ny * d.nz + base;
   const double shift = d.ak1[kx] + d.ak3[kz];
-  const bool mean = (kx == 0 && kz == 0);
+  // the zero-shift line: the mean mode (kx = kz = 0) of periodic x, the first
+  // COST mode of Neumann x ends
+  const bool mean = (d.ak1[kx] == 0.0 && d.ak3[kz] == 0.0);
   const bool pin1 = mean && !d.pin_last, pinn = mean && d.pin_last;
   double b = d.acph[1] - shift;
   double pp = 1.0 / b;
@@ -1659,6 +1661,85 @@ int launch_pois_io(chapsim_ctx *c, int ns, double *gx, double *gy, double *gz, c
   const int rc = mixed ? Prec<float>::poisson(c, ns, 0) : Prec<double>::poisson(c, ns, 0);
   c->d = saved;
   return rc;
+}
+
+// ---------------------------------------------- non-periodic x (IO Poisson)
+// FISHPACK_POIS3D_SIMPLE with Dirichlet / Neumann x ends
+// (src/possion3d_fishpack_reform.f90:104-163, 431-547): the x transform is
+// FFTPACK's SINT, SINQF / SINQB, COST or COSQF / COSQB, applied as a dense
+// nx x nx matrix (stored transposed: threads computing consecutive outputs
+// read consecutive entries) to every (j, k) row.  The real x modes occupy
+// the real parts of a complex spectral array of nx lines, on which the z
+// transforms and the y-line solves of the periodic path run unchanged (line
+// I shifted by -XRT(I)).  The forward matrix carries 1 / SCALX; the z
+// transforms carry 1 / nz, as in the periodic path.
+__global__ void __launch_bounds__(128) k_xnp_fwd(TGDev d, TGDev s, const double *__restrict__ ft) {
+  extern __shared__ double xrow[];
+  const int j = blockIdx.x + 1, k = blockIdx.y, nx = d.nx;
+  const double *src = d.rhsphi + d.sy * j + d.sz * k;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) xrow[i] = src[i];
+  __syncthreads();
+  double2 *dst = reinterpret_cast<double2 *>(s.spec) + (int64_t)s.lp * (j - 1) + (int64_t)s.lp * s.ny * k;
+  for (int m = threadIdx.x; m < s.lp; m += blockDim.x) {
+    double acc = 0.0;
+    if (m < nx)
+      for (int q = 0; q < nx; ++q) acc = fma(ft[(size_t)q * nx + m], xrow[q], acc);
+    dst[m] = make_double2(acc, 0.0);
+  }
+}
+
+__global__ void __launch_bounds__(128) k_xnp_bwd(TGDev d, TGDev s, const double *__restrict__ bt) {
+  extern __shared__ double xrow[];
+  const int j = blockIdx.x + 1, k = blockIdx.y, nx = d.nx, ny = d.ny;
+  const double2 *src = reinterpret_cast<const double2 *>(s.spec) + (int64_t)s.lp * (j - 1) + (int64_t)s.lp * s.ny * k;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) xrow[i] = src[i].x;
+  __syncthreads();
+  double *dst = d.phi + d.sy * j + d.sz * k;
+  for (int m = threadIdx.x; m < nx; m += blockDim.x) {
+    double acc = 0.0;
+    for (int q = 0; q < nx; ++q) acc = fma(bt[(size_t)q * nx + m], xrow[q], acc);
+    dst[m] = acc;
+    if (j == 1) dst[m - d.sy] = acc;   // BC_WALL_DPH: ghost rows by copy
+    if (j == ny) dst[m + d.sy] = acc;
+  }
+}
+
+int xnp_pivots(chapsim_ctx *c) {
+  TGDev &s = c->dnp;
+  dim3 grid((s.lh + 127) / 128, s.nz);
+  k_ypivots<<<grid, 128, 0, c->stream>>>(s);
+  LAUNCHED();
+  return CHAPSIM_OK;
+}
+
+int xnp_pois3d(chapsim_ctx *c) {
+  TGDev &d = c->d, &s = c->dnp;
+  const size_t sm = (size_t)d.nx * sizeof(double);
+  const dim3 rows(d.ny, d.nz);
+  k_xnp_fwd<<<rows, 128, sm, c->stream>>>(d, s, c->xnp_f);
+  LAUNCHED();
+  typedef Prec<double> P;
+  const int lz = P::fftz_lz(d.nz);
+  const dim3 gz((s.lh + lz - 1) / lz, d.ny);
+  if (c->fft_big)
+    k_fftz<double, true><<<gz, 256, P::fftz_smem(d.nz, lz), c->stream>>>(s, c->fz, lz, -1);
+  else
+    k_fftz<double, false><<<gz, 256, P::fftz_smem(d.nz, lz), c->stream>>>(s, c->fz, lz, -1);
+  LAUNCHED();
+  {
+    const int bx = c->ys_bx;
+    dim3 grid((s.lh + bx - 1) / bx, d.nz);
+    k_ysolve_line<double><<<grid, bx, 0, c->stream>>>(s);
+    LAUNCHED();
+  }
+  if (c->fft_big)
+    k_fftz<double, true><<<gz, 256, P::fftz_smem(d.nz, lz), c->stream>>>(s, c->fz, lz, +1);
+  else
+    k_fftz<double, false><<<gz, 256, P::fftz_smem(d.nz, lz), c->stream>>>(s, c->fz, lz, +1);
+  LAUNCHED();
+  k_xnp_bwd<<<rows, 128, sm, c->stream>>>(d, s, c->xnp_b);
+  LAUNCHED();
+  return CHAPSIM_OK;
 }
 
 int launch_pois3d(chapsim_ctx *c) {

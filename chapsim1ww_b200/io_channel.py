@@ -60,12 +60,14 @@ class IOChannel(TGChannel):
 
     def __init__(self, nx=64, ny=64, nz=64, lx=8 * math.pi, lz=4 * math.pi / 3, str2=2.0, istr2=1, ren=2800.0,
                  dt=1e-3, flowdrvtp=1, cfgv=0.0, thermal=1, prt=0.71, qw=(1.0, 1.0), gravdir=0, f_a=0.0,
-                 table=None, shortcuts=0, device=0, visc_scheme=0, coupled=0, precision=_lib.FP64, isothermal=0):
+                 table=None, shortcuts=0, device=0, visc_scheme=0, coupled=0, precision=_lib.FP64, isothermal=0,
+                 bcx=(3, 3)):
         self.lib = _lib.load()
         self.cfg = default_config(nx=nx, ny=ny, nz=nz, lx=lx, lz=lz, str2=str2, istr2=istr2, ren=ren, dt=dt,
                                   flowdrvtp=flowdrvtp, cfgv=cfgv, precision=precision, device=device)
         self.iocfg = io_config(thermal=thermal, prt=prt, qw_bot=qw[0], qw_top=qw[1], gravdir=gravdir, f_a=f_a,
-                               visc_scheme=visc_scheme, coupled=coupled, isothermal=isothermal)
+                               visc_scheme=visc_scheme, coupled=coupled, isothermal=isothermal,
+                               bcx_in=bcx[0], bcx_out=bcx[1])
         h = ctypes.c_void_p()
         rc = self.lib.chapsim_create_io(ctypes.byref(self.cfg), ctypes.byref(self.iocfg), ctypes.byref(h))
         if rc != _lib.CHAPSIM_OK:

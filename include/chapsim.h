@@ -419,6 +419,13 @@ typedef struct chapsim_io_config {
                           from the table at the wall temperature,
                           WALL_ISOTHERMAL_GIVEN, src/Flow_State.f90:603-645);
                           a clear bit keeps the iso-flux wall (BC_WALL_ISOFLUX)  */
+  int32_t bcx_in;      /* BCX_io(1), BCX_io(2) (src/READINI.f90:117-171): 1 Dirichlet, */
+  int32_t bcx_out;     /* 2 Neumann, 3 periodic (both 3, the default).  With
+                          Dirichlet / Neumann ends only chapsim_pois3d runs
+                          (FISHPACK_POIS3D_SIMPLE with the SINT / SINQ / COST /
+                          COSQ x transforms, FP64); the other entry points
+                          return CHAPSIM_ERR_UNSUPPORTED, the non-periodic IO
+                          step (x ghost columns) being unbuilt              */
 } chapsim_io_config;
 
 /* Defaults: thermal on, Pr = 0.71, qw = 1 on both walls (iso-flux), no

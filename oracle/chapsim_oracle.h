@@ -167,6 +167,9 @@ int oracle_io_set_plane(oracle_io *o, int which, const double *in);
 /* U_OUTLET (momentum), CHK_Mass_CONSV0_SCALING, CHK_MASS_CONSV0, inflow,
  * outflow, mass rate, U_OUTLET (energy) */
 void oracle_io_bc_scalars(const oracle_io *o, double *out);
+/* x boundary codes of the IO Poisson solve (BCX_io) and the solve alone */
+int oracle_io_set_bcx(oracle_io *o, int in, int out);
+void oracle_io_pois3d(oracle_io *o);
 /* iso-thermal walls (bit 0 bottom, bit 1 top; io_oracle.cpp) */
 int oracle_io_set_walls(oracle_io *o, int bits);
 /* PP_MEAN_ZX_FLOW_Xperiodic_IO: ny * 360 xz-plane averages (io_oracle.cpp) */

@@ -138,6 +138,11 @@ struct oracle_io {
   // mu, k at the wall temperature (qw[side] holds it)
   int isothermal = 0;
   double wall[2][5] = {{0.0}};
+  // x boundary type of the Poisson solve, FISHPACK's LP = LPEROD + 1
+  // (src/possion3d_fishpack_reform.f90:342-346): 1 periodic, 2 Dirichlet
+  // both ends (SINT), 3 Dirichlet-Neumann (SINQ), 4 Neumann both (COST), 5
+  // Neumann-Dirichlet (COSQ)
+  int lpx = 1;
   double rhohmax = 0.0;
   int64_t bad = 0;
   // flow fields (1..3 used)
@@ -678,8 +683,64 @@ std::vector<double> roots_periodic(int l, double c) {
   return rt;
 }
 
+// FFTPACK_ROOT_1D for LP = 2..5 (src/possion3d_fishpack_reform.f90:104-163):
+// XRT(I) = -4 c sin^2((I - DI) DX), DX = pi / (2 (L + LRDEL)); returns the
+// final SCALX that divides the backward transform's result.
+std::vector<double> roots_nonperiodic(int lp, int l, double c, double &scalx) {
+  const int lrdel = ((lp - 1) * (lp - 3) * (lp - 5)) / 3;
+  const double sc = (double)(l + lrdel), dx = M_PI / (2.0 * sc);
+  const double di = lp == 2 ? 0.0 : (lp == 4 ? 1.0 : 0.5);
+  std::vector<double> rt(l + 1, 0.0);
+  for (int i = 1; i <= l; ++i) {
+    const double s = std::sin(((double)i - di) * dx);
+    rt[i] = -4.0 * c * s * s;
+  }
+  scalx = (lp == 3 || lp == 5) ? 4.0 * sc : 2.0 * sc;
+  return rt;
+}
+
+// The real transforms of FFTPACK (libs/fishpack4.1/fftpack.f, the FFTPACK 4
+// library FISHPACK 4.1 ships) as direct sums from their documented
+// definitions, x 0-based here (x[K - 1] = X(K)): SINT (self-inverse up to
+// 2 (N + 1)), SINQF / SINQB and COSQF / COSQB (inverse pairs up to 4 N), COST
+// (self-inverse up to 2 (N - 1)).  fwd selects SINQF / COSQF over SINQB /
+// COSQB.  O(N^2): test-infrastructure sizes only.
+void fftpack_real(int lp, bool fwd, int n, double *x, double *tmp) {
+  for (int i = 1; i <= n; ++i) {
+    double s = 0.0;
+    switch (lp) {
+      case 2:  // SINT
+        for (int k = 1; k <= n; ++k) s += 2.0 * x[k - 1] * std::sin((double)k * i * M_PI / (n + 1));
+        break;
+      case 3:
+        if (fwd) {  // SINQF
+          s = ((i - 1) % 2 ? -1.0 : 1.0) * x[n - 1];
+          for (int k = 1; k <= n - 1; ++k) s += 2.0 * x[k - 1] * std::sin((2.0 * i - 1.0) * k * M_PI / (2.0 * n));
+        } else {  // SINQB
+          for (int k = 1; k <= n; ++k) s += 4.0 * x[k - 1] * std::sin((2.0 * k - 1.0) * i * M_PI / (2.0 * n));
+        }
+        break;
+      case 4:  // COST
+        s = x[0] + ((i - 1) % 2 ? -1.0 : 1.0) * x[n - 1];
+        for (int k = 2; k <= n - 1; ++k) s += 2.0 * x[k - 1] * std::cos((double)(k - 1) * (i - 1) * M_PI / (n - 1));
+        break;
+      case 5:
+        if (fwd) {  // COSQF
+          s = x[0];
+          for (int k = 2; k <= n; ++k) s += 2.0 * x[k - 1] * std::cos((2.0 * i - 1.0) * (k - 1) * M_PI / (2.0 * n));
+        } else {  // COSQB
+          for (int k = 1; k <= n; ++k) s += 4.0 * x[k - 1] * std::cos((2.0 * k - 1.0) * (i - 1) * M_PI / (2.0 * n));
+        }
+        break;
+    }
+    tmp[i - 1] = s;
+  }
+  std::copy(tmp, tmp + n, x);
+}
+
 // FISHPACK_POIS3D_SIMPLE (src/possion3d_fishpack_reform.f90:431-547) for
-// BCX_io = BCZ = periodic: RHSLLPHI -> DPH (interior), ghosts by copy.
+// periodic z and the x boundary type lpx: RHSLLPHI -> DPH (interior), ghosts
+// by copy.
 void fishpack_pois3d(oracle_io *o) {
   const int l = o->nx, m = o->nz, ng = o->ny;
   std::vector<double> fr((size_t)l * m * ng);  // FR(I, K, J): x fastest, then z, then y
@@ -687,7 +748,10 @@ void fishpack_pois3d(oracle_io *o) {
   for (int j = 1; j <= ng; ++j)
     for (int k = 1; k <= m; ++k)
       for (int i = 1; i <= l; ++i) FR(i, k, j) = F(rhsllphi, i, j, k);
-  const std::vector<double> xrt = roots_periodic(l, o->dxqi), yrt = roots_periodic(m, o->dzqi);
+  double scalx = (double)l;
+  const std::vector<double> xrt = o->lpx == 1 ? roots_periodic(l, o->dxqi)
+                                              : roots_nonperiodic(o->lpx, l, o->dxqi, scalx);
+  const std::vector<double> yrt = roots_periodic(m, o->dzqi);
   const int nmax = std::max(l, m);
 #pragma omp parallel num_threads(nthreads())
   {
@@ -696,7 +760,10 @@ void fishpack_pois3d(oracle_io *o) {
     for (int j = 1; j <= ng; ++j) {
       for (int k = 1; k <= m; ++k) {
         for (int i = 1; i <= l; ++i) t[i - 1] = FR(i, k, j);
-        rfftf(o->dftx, l, t.data(), w.data());
+        if (o->lpx == 1)
+          rfftf(o->dftx, l, t.data(), w.data());
+        else
+          fftpack_real(o->lpx, true, l, t.data(), w.data());
         for (int i = 1; i <= l; ++i) FR(i, k, j) = t[i - 1];
       }
       for (int i = 1; i <= l; ++i) {
@@ -727,7 +794,9 @@ void fishpack_pois3d(oracle_io *o) {
           tt[jy] = (tt[jy] - o->amph[jy] * tt[jy - 1]) * z;
         }
         z = bb[nr] - o->amph[nr] * dd[mm1];
-        const bool singular = (i == 1 && k == 1);  // the mean mode: zero branch
+        // the zero-shift mode takes TRID0's zero branch: the mean mode of
+        // periodic x, the first COST mode
+        const bool singular = (xrt[i] == 0.0 && yrt[k] == 0.0);
         if (!singular && std::fabs(z) > 1.0e-14)
           tt[nr] = (tt[nr] - o->amph[nr] * tt[mm1]) / z;
         else
@@ -748,12 +817,15 @@ void fishpack_pois3d(oracle_io *o) {
       }
       for (int k = 1; k <= m; ++k) {
         for (int i = 1; i <= l; ++i) t[i - 1] = FR(i, k, j);
-        rfftb(o->dftx, l, t.data(), w.data());
+        if (o->lpx == 1)
+          rfftb(o->dftx, l, t.data(), w.data());
+        else
+          fftpack_real(o->lpx, false, l, t.data(), w.data());
         for (int i = 1; i <= l; ++i) FR(i, k, j) = t[i - 1];
       }
     }
   }
-  const double scal = (double)l * (double)m;  // SCALX * SCALY
+  const double scal = scalx * (double)m;  // SCALX * SCALY
   std::fill(o->dph.begin(), o->dph.end(), 0.0);
   for (int j = 1; j <= ng; ++j)
     for (int k = 1; k <= m; ++k)
@@ -1444,6 +1516,23 @@ int oracle_io_set_table(oracle_io *o, const double *H, const double *T, const do
 }
 
 double oracle_io_rhohmax(const oracle_io *o) { return o->rhohmax; }
+
+// BCX_io (Dirichlet 1, Neumann 2, periodic 3, src/READINI.f90:117-171) of the
+// Poisson solve: FISHPACK's LP (src/possion3d_fishpack_reform.f90:342-346).
+int oracle_io_set_bcx(oracle_io *o, int in, int out) {
+  int lp = -1;
+  if (in == 3 && out == 3) lp = 1;
+  if (in == 1 && out == 1) lp = 2;
+  if (in == 1 && out == 2) lp = 3;
+  if (in == 2 && out == 2) lp = 4;
+  if (in == 2 && out == 1) lp = 5;
+  if (lp < 0 || o->nx < 4) return -1;
+  o->lpx = lp;
+  return 0;
+}
+
+// FISHPACK_POIS3D_SIMPLE alone: DPH from the current RHSLLPHI.
+void oracle_io_pois3d(oracle_io *o) { fishpack_pois3d(o); }
 
 // BCWALLHEAT = isoThermalWall on the walls of `bits` (bit 0 bottom, bit 1
 // top), the wall temperature being qw of that wall; WALL_ISOTHERMAL_GIVEN

@@ -79,6 +79,9 @@ def load(build=True):
     L.oracle_io_stats.argtypes = [P, P]
     L.oracle_io_set_walls.argtypes = [P, I]
     L.oracle_io_set_walls.restype = I
+    L.oracle_io_set_bcx.argtypes = [P, I, I]
+    L.oracle_io_set_bcx.restype = I
+    L.oracle_io_pois3d.argtypes = [P]
     L.oracle_tg_stats.argtypes = [P, P]
     L.oracle_set_threads.argtypes = [I]
     L.oracle_get_threads.restype = I
@@ -298,6 +301,14 @@ class OracleIO:
 
     def cfl(self):
         return self.L.oracle_io_cfl(self.h)
+
+    def set_bcx(self, inlet, outlet):
+        """BCX_io of the Poisson solve: 1 Dirichlet, 2 Neumann, 3 periodic."""
+        assert self.L.oracle_io_set_bcx(self.h, int(inlet), int(outlet)) == 0
+
+    def pois3d(self):
+        """FISHPACK_POIS3D_SIMPLE alone: phi from rhsphi."""
+        self.L.oracle_io_pois3d(self.h)
 
     def stats(self):
         """PP_MEAN_ZX_FLOW_Xperiodic_IO: (ny, 360) xz-plane averages."""

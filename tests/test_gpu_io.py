@@ -246,3 +246,31 @@ def test_isothermal_wall_outside_table_is_refused():
     from oracle.pyoracle import synth_table
     with pytest.raises(ChapsimError):
         IOChannel(16, 12, 8, table=synth_table(4096), qw=(5.0, 0.8), isothermal=1)
+
+
+@pytest.mark.parametrize("bcx", [(1, 1), (1, 2), (2, 2), (2, 1)])
+def test_io_poisson_nonperiodic_x_parity(bcx):
+    """FISHPACK_POIS3D_SIMPLE with Dirichlet / Neumann x ends (BCX_io 1 / 2:
+    FISHPACK's SINT, SINQ, COST, COSQ x transforms): chapsim_pois3d against
+    the oracle on the same random right-hand side, FP64 within 1e-10 over the
+    whole field (interior and the copied ghost rows), two grids; the
+    other entry points refuse such a context (its IO step, with x ghost
+    columns, is not built)."""
+    _need_gpu()
+    from chapsim1ww_b200 import ChapsimError, IOChannel
+    from oracle.pyoracle import OracleIO
+    rng = np.random.default_rng(9)
+    for dims in ((24, 18, 16), (40, 20, 12)):
+        g = IOChannel(*dims, thermal=0, bcx=bcx)
+        o = OracleIO(*dims, thermal=0)
+        o.set_bcx(*bcx)
+        rhs = rng.standard_normal((dims[2], dims[1] + 2, dims[0]))
+        g.set_field("rhsphi", rhs)
+        o.set("rhsphi", rhs)
+        g.fishpack_pois3d()
+        o.pois3d()
+        e = relerr(g.get_field("phi"), o.get("phi"))
+        assert e <= 1e-10, (dims, e)
+        with pytest.raises(ChapsimError):
+            g.step(1)
+        g.close()

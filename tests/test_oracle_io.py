@@ -212,3 +212,36 @@ def test_oracle_io_isothermal_walls_match_numpy_restatement(walls):
             dh = h[:, jin, :].mean() - h0[:, jin, :].mean()
             assert (dh > 0) if tw[side] > 0.867 else (dh < 0), (side, dh)
     assert o.divmax() < 1e-11
+
+
+@pytest.mark.parametrize("bcx", [(1, 1), (1, 2), (2, 2), (2, 1)])
+def test_io_poisson_nonperiodic_x_inverts_the_operator(bcx):
+    """FISHPACK_POIS3D_SIMPLE with non-periodic x (BCX_io Dirichlet 1 /
+    Neumann 2 at inlet / outlet: FISHPACK's SINT, SINQ, COST, COSQ transforms,
+    src/possion3d_fishpack_reform.f90:104-163 and FFTPACK's definitions): the
+    solution satisfies the discrete Poisson equation whose x-ends follow the
+    transform's basis (Dirichlet: zero one node beyond; Neumann: even about
+    the end node), periodic z and the y-operator of TDMA_PHI_COEF, to 1e-10 of
+    the right-hand side.  Neumann at both ends is singular in its mean mode;
+    TRID0 pins that mode at the last row, whose equation is then left out."""
+    nx, ny, nz, lx, lz = 20, 16, 12, 8 * math.pi, 4 * math.pi / 3
+    o = OracleIO(nx, ny, nz, lx=lx, lz=lz, thermal=0)
+    o.set_bcx(*bcx)
+    rng = np.random.default_rng(5)
+    rhs = rng.standard_normal((nz, ny + 2, nx))
+    o.set("rhsphi", rhs)
+    o.pois3d()
+    phi = o.get("phi")
+    t = OracleTG(nx, ny, nz, lx=lx, lz=lz)
+    am, ac, ap = (np.concatenate([[0.0], t.coef(w), [0.0]]) for w in (6, 7, 8))
+    dxqi, dzqi = (nx / lx) ** 2, (nz / lz) ** 2
+    f = phi[:, 1:ny + 1, :]
+    zero = np.zeros_like(f[..., :1])
+    left = zero if bcx[0] == 1 else f[..., 1:2]    # Dirichlet: phi_0 = 0; Neumann: phi_0 = phi_2
+    right = zero if bcx[1] == 1 else f[..., -2:-1]  # phi_{N+1} = 0, or phi_{N+1} = phi_{N-1}
+    fx = np.concatenate([left, f, right], axis=2)
+    lap = (fx[..., 2:] - 2 * f + fx[..., :-2]) * dxqi + (np.roll(f, -1, 0) - 2 * f + np.roll(f, 1, 0)) * dzqi
+    lap += am[1:ny + 1, None] * phi[:, 0:ny, :] + ac[1:ny + 1, None] * f + ap[1:ny + 1, None] * phi[:, 2:ny + 2, :]
+    res = lap - rhs[:, 1:ny + 1, :]
+    rows = ny - 1 if bcx == (2, 2) else ny
+    assert np.abs(res[:, :rows, :]).max() <= 1e-10 * np.abs(rhs).max(), np.abs(res[:, :rows, :]).max()
