@@ -1163,6 +1163,17 @@ int chapsim_set_dt(chapsim_ctx *ctx, double dt) {
     ctx->cfg.dt = dt_old;
     return rc;
   }
+  if (ctx->xnp) {
+    // the non-periodic Poisson descriptor points into the coefficient tables
+    // too: refresh it, keeping its own spectral array, pivots and x shifts
+    chapsim::TGDev &s = ctx->dnp;
+    void *spec = s.spec;
+    double2 *ypiv = s.ypiv;
+    const double *ak1 = s.ak1;
+    const int lh = s.lh, lp = s.lp;
+    s = ctx->d;
+    s.spec = spec; s.ypiv = ypiv; s.ak1 = ak1; s.lh = lh; s.lp = lp;
+  }
   for (auto it = ctx->allocs.begin(); it != ctx->allocs.end(); ++it)
     if (*it == (void *)old) {
       cudaFree(old);
