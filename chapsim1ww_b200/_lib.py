@@ -98,6 +98,7 @@ SIGNATURES = [
     ("chapsim_set_tuning", _I, [_P, _I, _I]),
     ("chapsim_get_tuning", _I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I)]),
     ("chapsim_set_line_tuning", _I, [_P, _I]),
+    ("chapsim_io_wall_values", _I, [_P, _DP, _I]),
     ("chapsim_get_line_tuning", _I, [_P, ctypes.POINTER(_I)]),
     ("chapsim_props_create", _I, [_P, _P, _P, _P, _P, _P, _I, _I, ctypes.POINTER(_P)]),
     ("chapsim_props_destroy", _I, [_P]),

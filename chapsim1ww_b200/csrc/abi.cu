@@ -1246,6 +1246,13 @@ int chapsim_set_table(chapsim_ctx *ctx, const double *H, const double *T, const 
   return CHAPSIM_OK;
 }
 
+int chapsim_io_wall_values(const chapsim_ctx *ctx, double *out, int n) {
+  if (!ctx || !out || n != 10 || ctx->domain != CHAPSIM_IIO) return CHAPSIM_ERR_ARG;
+  for (int side = 0; side < 2; ++side)
+    for (int q = 0; q < 5; ++q) out[5 * side + q] = (ctx->io.isothermal & (1 << side)) ? ctx->io.wall[side][q] : 0.0;
+  return CHAPSIM_OK;
+}
+
 int chapsim_set_props_mode(chapsim_ctx *ctx, int mode, const chapsim_props *pe) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
   REQUIRE(ctx->domain == CHAPSIM_IIO && ctx->io.thermal, CHAPSIM_ERR_STATE,

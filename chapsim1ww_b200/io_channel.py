@@ -185,6 +185,42 @@ class IOChannel(TGChannel):
             mon["t1maxx"] = np.abs(g["T1"][:, 0]).max()
         return mon
 
+    def wall_values(self):
+        """(2, 5) array: T, h, rho, mu, k of the bottom and top walls when
+        iso-thermal (WALL_ISOTHERMAL_GIVEN), zero for an iso-flux wall."""
+        a = np.zeros(10)
+        self._chk(self.lib.chapsim_io_wall_values(self.h, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), 10))
+        return a.reshape(2, 5)
+
+    def driven_force(self):
+        """PP_DRIVEN_FORCE (src/processing/PP_MEAN_ZX.f90:969-1056) from the
+        device xz averages of the last pp_mean_zx: the constant-mass-flux
+        driving force FcDrv = (|wall friction 1| + |wall friction 2| -
+        buoyancy) / 2 per unit wall area, and FUxzL_IO = FcDrv (U1, 1) per
+        row.  Defined for FLOWDRVTP = 1; with the energy equation the wall
+        viscosity is M_WAL_GV, which the reference holds for iso-thermal walls
+        only (zero on an iso-flux wall beside an iso-thermal one), so a heated
+        channel with two iso-flux walls raises ValueError."""
+        if self.cfg.flowdrvtp != 1:
+            raise ValueError("PP_DRIVEN_FORCE applies to FLOWDRVTP = 1 only")
+        mu_w = np.ones(2)
+        if self.iocfg.thermal:
+            if not self.iocfg.isothermal:
+                raise ValueError("M_WAL_GV is undefined with two iso-flux walls (the reference never allocates it)")
+            mu_w = self.wall_values()[:, 3]
+        g = self.stats_groups(0)
+        u1 = g["U1"][:, 0]
+        ynd, ycc, dyfi = self.mesh(0), self.mesh(1), self.mesh(2)
+        cv = 1.0 / self.cfg.ren
+        f1 = mu_w[0] * u1[0] / (ycc[0] - ynd[0]) * cv
+        f2 = mu_w[1] * u1[-1] / (ycc[-1] - ynd[-1]) * cv
+        buo = 0.0
+        if self.iocfg.gravdir == 1:
+            buo = float((g["D1"][:, 0] * self.iocfg.f_a / dyfi).sum())
+        fc = (abs(f1) + abs(f2) - buo) / 2.0
+        fu = np.concatenate([fc * g["U1"][:, :3], np.full((self.ny, 1), fc)], axis=1)
+        return fc, fu
+
     def bad_cells(self):
         return int(self._reduce(_lib.R_BADCELLS))
 

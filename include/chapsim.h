@@ -455,6 +455,12 @@ int chapsim_set_table(chapsim_ctx *ctx, const double *H, const double *T, const 
 #define CHAPSIM_PROPS_MLP 1   /* learned model on the tensor cores (BF16 operands, FP32
                                  accumulation) where the error gate allows it, table
                                  splines elsewhere                                   */
+/* The wall values of an IO context's iso-thermal walls (WALL_ISOTHERMAL_GIVEN,
+ * src/Flow_State.f90:603-645: T_WAL_GV, H_WAL_GV, D_WAL_GV, M_WAL_GV, K_WAL_GV):
+ * out[5 * side + q], side 0 bottom, 1 top, q = T, h, rho, mu, k; zero for a
+ * wall that is not iso-thermal (the reference's zero-initialised arrays). */
+int chapsim_io_wall_values(const chapsim_ctx *ctx, double *out, int n);
+
 /* Property evaluation of an IO context (the THERM_PROP_UPDATE of
  * src/THERM_PROP_UPDATE.f90:129-205 with its DENSITY_UPDATE / ENTHALPY_UPDATE
  * companions, as SOLVERRK3_ENG_IO calls them, src/SOLVERRK3_ENG_IO.f90:46-55).

@@ -87,3 +87,38 @@ def test_io_statistics_bit_reproducible():
     g.pp_mean_zx()
     b, _ = g.stats(0)
     assert np.array_equal(a, b)
+
+
+def test_io_driven_force():
+    """PP_DRIVEN_FORCE (src/processing/PP_MEAN_ZX.f90:969-1056) from the device
+    statistics against the reference's sums over the fields themselves: the
+    wall frictions from u in the first and last rows (wall viscosity 1, or
+    M_WAL_GV of iso-thermal walls), no buoyancy; FUxzL_IO = FcDrv (U1, 1).
+    A heated channel with two iso-flux walls, where the reference reads an
+    array it never allocated, is refused."""
+    _need_gpu()
+    from chapsim1ww_b200 import IOChannel
+    from oracle.pyoracle import synth_table
+    table = synth_table(4096)
+    for thermal, iso in ((0, 0), (1, 3), (1, 1)):
+        g = IOChannel(40, 18, 24, thermal=thermal, table=table if thermal else None,
+                      qw=(0.95, 0.80) if iso else (1.0, 1.0), isothermal=iso)
+        g.random_fl_theml_fld_io(5, 0.1)
+        g.step(1)
+        g.pp_mean_zx()
+        fc, fu = g.driven_force()
+        u = g.get_field("u")
+        mu_w = g.wall_values()[:, 3] if thermal else np.ones(2)
+        ynd, ycc = g.mesh(0), g.mesh(1)
+        nxz = u.shape[0] * u.shape[2]
+        f1 = mu_w[0] * u[:, 1, :].sum() / (ycc[0] - ynd[0]) / g.cfg.ren / nxz
+        f2 = mu_w[1] * u[:, -2, :].sum() / (ycc[-1] - ynd[-1]) / g.cfg.ren / nxz
+        ref = (abs(f1) + abs(f2)) / 2.0
+        assert abs(fc - ref) <= 1e-12 * abs(ref), (thermal, iso, fc, ref)
+        assert fu.shape == (18, 4) and np.all(fu[:, 3] == fc)
+        g.close()
+    g = IOChannel(16, 12, 8, table=table)
+    g.random_fl_theml_fld_io(5, 0.1)
+    g.pp_mean_zx()
+    with pytest.raises(ValueError):
+        g.driven_force()
