@@ -135,6 +135,8 @@ SIGNATURES += [
     ("chapsim_rk3_eng_io", _I, [_P, _I]),
     ("chapsim_rk3_mom_io", _I, [_P, _I]),
     ("chapsim_step_io", _I, [_P, _I]),
+    ("chapsim_io_set_inlet", _I, [_P, _P]),
+    ("chapsim_step_coupled", _I, [_P, _P, _I]),
     ("chapsim_set_dt", _I, [_P, _D]),
     ("chapsim_stats", _I, [_P, _I]),
     ("chapsim_get_stats", _I, [_P, _I, _P, _I64, ctypes.POINTER(_I64)]),

@@ -146,11 +146,22 @@ int chapsim_config_default(chapsim_config *cfg) {
   return CHAPSIM_OK;
 }
 
-static void free_all(chapsim_ctx *ctx) {
-  if (ctx->step_graph) cudaGraphExecDestroy(ctx->step_graph);
-  ctx->step_graph = nullptr;
+// Captured graphs go stale when a launch parameter or a table they point to
+// changes; a TG context's change also stales the pair graphs of the coupled
+// sections it feeds (they hold its kernels).
+static void drop_graphs(chapsim_ctx *ctx) {
+  if (ctx->step_graph) { cudaGraphExecDestroy(ctx->step_graph); ctx->step_graph = nullptr; }
   for (auto &g : ctx->io_graph)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  for (auto &g : ctx->pair_graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  for (chapsim_ctx *io : ctx->fed)
+    for (auto &g : io->pair_graph)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+static void free_all(chapsim_ctx *ctx) {
+  drop_graphs(ctx);
   for (void *p : ctx->table_allocs) cudaFree(p);
   ctx->table_allocs.clear();
   for (void *p : ctx->allocs) cudaFree(p);
@@ -160,7 +171,8 @@ static void free_all(chapsim_ctx *ctx) {
   for (auto &e : ctx->evpool)
     if (e) cudaEventDestroy(e);
   ctx->evpool.clear();
-  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  ctx->own_stream = nullptr;
   ctx->stream = nullptr;
 }
 
@@ -537,6 +549,7 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
     delete ctx;
     return CHAPSIM_ERR_CUDA;
   }
+  ctx->own_stream = ctx->stream;
   for (auto &e : ctx->ev)
     if (cudaEventCreate(&e) != cudaSuccess) { free_all(ctx); delete ctx; return CHAPSIM_ERR_CUDA; }
   ctx->evpool.assign((size_t)chapsim_ctx::kEvSub * (CHAPSIM_PH_COUNT + 1), nullptr);
@@ -547,8 +560,20 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
   d.nx = cfg->nx; d.ny = cfg->ny; d.nz = cfg->nz; d.lh = cfg->nx / 2 + 1;
   d.lp = (d.lh + 1) & ~1;
   d.sy = cfg->nx;
-  d.sz = (int64_t)cfg->nx * (cfg->ny + 2);
+  if (iocfg && iocfg->bcx_in != 3) {
+    // the coupled inflow / outflow section: x ghost columns IC = 0 and
+    // NCL1_io + 1 in every field (NCL1S:NCL1E, src/MEMALLOCT.f90:154-168);
+    // field pointers address IC = 1
+    d.xnp = 1;
+    d.sy = cfg->nx + 2;
+    ctx->xoff = 1;
+  }
+  d.sz = d.sy * (cfg->ny + 2);
   const size_t n = (size_t)d.sz * cfg->nz;
+  // every field allocation carries two values of slack past its n, so that
+  // a whole-array pass from the offset pointer stays inside it
+  const size_t nal = n + 2;
+  const int xo = ctx->xoff;
   void *p = nullptr;
   {
     const bool mixed = cfg->precision == CHAPSIM_MIXED;
@@ -557,9 +582,9 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
     const size_t tsz = (mixed && !iocfg) ? sizeof(float) : sizeof(double);
     double **f64[] = {&d.u, &d.v, &d.w, &d.p, &d.phi, &d.rhsphi, &d.res};
     for (double **f : f64) {
-      if ((rc = dalloc(ctx, &p, n * sizeof(double)))) goto fail;
-      *f = (double *)p;
-      cudaMemsetAsync(p, 0, n * sizeof(double), ctx->stream);
+      if ((rc = dalloc(ctx, &p, nal * sizeof(double)))) goto fail;
+      *f = (double *)p + xo;
+      cudaMemsetAsync(p, 0, nal * sizeof(double), ctx->stream);
     }
     for (int c = 0; c < 3; ++c) {
       void **tmp[] = {&d.h0[c], &d.rhs[c], &d.dq[c]};
@@ -567,9 +592,9 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
         // the explicit IO substep needs EXPLT0 only; the semi-implicit one
         // also keeps RHS_io per component
         if (iocfg && (f == &d.dq[c] || (f == &d.rhs[c] && !iocfg->visc_scheme))) continue;
-        if ((rc = dalloc(ctx, &p, n * tsz))) goto fail;
-        *f = p;
-        cudaMemsetAsync(p, 0, n * tsz, ctx->stream);
+        if ((rc = dalloc(ctx, &p, nal * tsz))) goto fail;
+        *f = (char *)p + xo * tsz;
+        cudaMemsetAsync(p, 0, nal * tsz, ctx->stream);
       }
     }
     if (iocfg) {
@@ -578,9 +603,9 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
                           &io.drho, &io.rhoh, &io.h, &io.T, &io.D, &io.D0, &io.mu, &io.mu0, &io.kap, &io.rhse0,
                           &io.msum};
       for (double **f : f64io) {
-        if ((rc = dalloc(ctx, &p, n * sizeof(double)))) goto fail;
-        *f = (double *)p;
-        cudaMemsetAsync(p, 0, n * sizeof(double), ctx->stream);
+        if ((rc = dalloc(ctx, &p, nal * sizeof(double)))) goto fail;
+        *f = (double *)p + xo;
+        cudaMemsetAsync(p, 0, nal * sizeof(double), ctx->stream);
       }
       io.visc = iocfg->visc_scheme ? 1 : 0;
       if (io.visc) {
@@ -598,10 +623,10 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
         io.apvrn = ucaj * (2.0 * ctx->dyfi[ny]);
       }
       io.bps = (int64_t)(cfg->ny + 2) * cfg->nz;
-      if ((rc = dalloc(ctx, &p, ((size_t)io.bps * CHAPSIM_P_COUNT + 8) * sizeof(double)))) goto fail;
+      if ((rc = dalloc(ctx, &p, ((size_t)io.bps * chapsim::P_ALL + 8) * sizeof(double)))) goto fail;
       io.bcp = (double *)p;
-      io.bcs = io.bcp + (size_t)io.bps * CHAPSIM_P_COUNT;
-      cudaMemsetAsync(p, 0, ((size_t)io.bps * CHAPSIM_P_COUNT + 8) * sizeof(double), ctx->stream);
+      io.bcs = io.bcp + (size_t)io.bps * chapsim::P_ALL;
+      cudaMemsetAsync(p, 0, ((size_t)io.bps * chapsim::P_ALL + 8) * sizeof(double), ctx->stream);
       if ((rc = dalloc(ctx, &p, 2 * sizeof(unsigned long long)))) goto fail;
       io.bad = (unsigned long long *)p;
       io.model_again = io.bad + 1;
@@ -654,8 +679,8 @@ static int create_ctx(const chapsim_config *cfg, const chapsim_io_config *iocfg,
     IODev &io = ctx->io;
     double *ones[] = {io.T, io.D, io.D0, io.mu, io.mu0, io.kap};
     for (double *f : ones)
-      if ((rc = fill_value(ctx, f, n, 1.0))) goto fail;
-    if ((rc = fill_value(ctx, io.msum, n, 2.0))) goto fail;
+      if ((rc = fill_value(ctx, f - xo, nal, 1.0))) goto fail;
+    if ((rc = fill_value(ctx, io.msum - xo, nal, 2.0))) goto fail;
     if ((rc = fill_value(ctx, io.bcp + (size_t)io.bps * CHAPSIM_P_IN_RHO, (size_t)io.bps, 1.0))) goto fail;
   }
   if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { rc = CHAPSIM_ERR_CUDA; goto fail; }
@@ -698,14 +723,33 @@ int chapsim_create_io(const chapsim_config *cfg, const chapsim_io_config *io, ch
   if (io->bcx_in < 1 || io->bcx_in > 3 || io->bcx_out < 1 || io->bcx_out > 3 ||
       ((io->bcx_in == 3) != (io->bcx_out == 3)))
     return CHAPSIM_ERR_ARG;
-  if (io->bcx_in != 3 && (cfg->precision != CHAPSIM_FP64 || cfg->nx < 4)) return CHAPSIM_ERR_UNSUPPORTED;
+  // the coupled section (non-periodic x): FP64, explicit viscous terms (the
+  // reference's semi-implicit inlet terms BC_CBC_TDMA are unfinished,
+  // src/SOLVERRK3_MOM_IO.f90:22), iso-flux walls (BC_COUTLET_ENEG_RK3's
+  // outlet-plane walls)
+  if (io->bcx_in != 3 && (cfg->precision != CHAPSIM_FP64 || cfg->nx < 4 || io->visc_scheme != 0 || io->isothermal))
+    return CHAPSIM_ERR_UNSUPPORTED;
   return create_ctx(cfg, io, out);
+}
+
+// A coupled section leaves its TG source: back on its own stream.
+static void detach_inlet(chapsim_ctx *io) {
+  chapsim_ctx *tg = io->inlet;
+  if (!tg) return;
+  cudaStreamSynchronize(io->stream);
+  for (auto it = tg->fed.begin(); it != tg->fed.end(); ++it)
+    if (*it == io) { tg->fed.erase(it); break; }
+  drop_graphs(io);
+  io->inlet = nullptr;
+  io->stream = io->own_stream;
 }
 
 int chapsim_destroy(chapsim_ctx *ctx) {
   if (!ctx) return CHAPSIM_ERR_ARG;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  detach_inlet(ctx);
+  while (!ctx->fed.empty()) detach_inlet(ctx->fed.back());
   free_all(ctx);
   delete ctx;
   return CHAPSIM_OK;
@@ -737,9 +781,7 @@ int chapsim_set_refinement(chapsim_ctx *ctx, int sweeps) {
   CKC(cudaSetDevice(ctx->device));
   CKC(cudaStreamSynchronize(ctx->stream));
   ctx->refine = sweeps == 1;
-  if (ctx->step_graph) { cudaGraphExecDestroy(ctx->step_graph); ctx->step_graph = nullptr; }
-  for (auto &g : ctx->io_graph)
-    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  drop_graphs(ctx);
   return CHAPSIM_OK;
 }
 
@@ -820,10 +862,13 @@ static int xfer(chapsim_ctx *ctx, int domain, int field, void *dst_or_src, int64
     }
     return CHAPSIM_OK;
   }
+  // the whole array, from its first value (the inlet ghost column of the
+  // first row in the coupled section)
+  double *base = f - ctx->xoff;
   if (to_dev)
-    CKC(cudaMemcpyAsync(f, dst_or_src, bytes, kind, ctx->stream));
+    CKC(cudaMemcpyAsync(base, dst_or_src, bytes, kind, ctx->stream));
   else
-    CKC(cudaMemcpyAsync(dst_or_src, f, bytes, kind, ctx->stream));
+    CKC(cudaMemcpyAsync(dst_or_src, base, bytes, kind, ctx->stream));
   if (to_dev && domain == CHAPSIM_IIO && (field == CHAPSIM_F_MU || field == CHAPSIM_F_MU0)) {
     const int rc = io_refresh_msum(ctx);  // keep mu0 + mu in step
     if (rc) return rc;
@@ -944,8 +989,13 @@ struct HostSpline {
 static int io_init_random(chapsim_ctx *ctx, uint64_t seed, double amp, int project) {
   IODev &io = ctx->io;
   REQUIRE(!io.thermal || ctx->has_table, CHAPSIM_ERR_STATE, "thermal IO domain without a property table");
+  REQUIRE(!ctx->xnp || ctx->inlet, CHAPSIM_ERR_STATE,
+          "coupled IO section without its TG inlet source (chapsim_io_set_inlet)");
   const int nx = ctx->cfg.nx, ny = ctx->cfg.ny, nz = ctx->cfg.nz;
+  // the seeded field is built on the interior columns (sy = nx), then laid
+  // out in the context's fields (with the coupled section's ghost columns)
   const int64_t sy = nx, sz = (int64_t)nx * (ny + 2), n = sz * nz;
+  const int64_t nf = ctx->d.sz * nz;
   auto id = [&](int i, int j, int k) { return (size_t)((i - 1) + sy * j + sz * (k - 1)); };
   std::vector<double> q[3], g[3];
   for (auto &f : q) f.assign((size_t)n, 0.0);
@@ -986,27 +1036,50 @@ static int io_init_random(chapsim_ctx *ctx, uint64_t seed, double amp, int proje
   for (int c = 0; c < 3; ++c)
     for (auto &x : q[c]) x /= gm;
   velo2massflux();
+  if (ctx->xnp) {
+    // coupled section: the interior into the ghost-column layout, and the
+    // outlet ghost column IC = NCL1_io + 1 a copy of the last interior column
+    // (the inlet column comes from the TG section in the projection's
+    // BC_TINLET_FLOW)
+    const int64_t fy = ctx->d.sy, fz = ctx->d.sz;
+    for (auto *set : {q, g})
+      for (int c = 0; c < 3; ++c) {
+        std::vector<double> e((size_t)nf, 0.0);
+        for (int k = 0; k < nz; ++k)
+          for (int j = 0; j <= ny + 1; ++j) {
+            const double *src = set[c].data() + sy * j + sz * k;
+            double *dst = e.data() + 1 + fy * j + fz * k;
+            for (int i = 0; i < nx; ++i) dst[i] = src[i];
+            dst[nx] = src[nx - 1];
+          }
+        set[c].swap(e);
+      }
+  }
   int rc;
+  const size_t fbytes = (size_t)nf * sizeof(double);
+  const int xo = ctx->xoff;
   for (int c = 0; c < 3; ++c) {
-    if ((rc = chapsim_set_field(ctx, CHAPSIM_IIO, CHAPSIM_F_U + c, q[c].data(), n))) return rc;
-    CKC(cudaMemcpyAsync(io.g[0][c], g[c].data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    CKC(cudaMemsetAsync(io.g[1][c], 0, (size_t)n * sizeof(double), ctx->stream));  // G0_io = 0 until MOM_IO
-    CKC(cudaMemsetAsync(ctx->d.h0[c], 0, (size_t)n * sizeof(double), ctx->stream));
+    if ((rc = chapsim_set_field(ctx, CHAPSIM_IIO, CHAPSIM_F_U + c, q[c].data(), nf))) return rc;
+    CKC(cudaMemcpyAsync(io.g[0][c] - xo, g[c].data(), fbytes, cudaMemcpyHostToDevice, ctx->stream));
+    CKC(cudaMemsetAsync(io.g[1][c] - xo, 0, fbytes, ctx->stream));  // G0_io = 0 until MOM_IO
+    CKC(cudaMemsetAsync((double *)ctx->d.h0[c] - xo, 0, fbytes, ctx->stream));
   }
   CKC(cudaStreamSynchronize(ctx->stream));
   ctx->io_cur = 0;
   TGDev &d = ctx->d;
-  const size_t bytes = (size_t)n * sizeof(double);
   double *zero[] = {d.p, d.phi, d.rhsphi, io.drho, io.rhoh, io.h, io.rhse0};
-  for (double *f : zero) CKC(cudaMemsetAsync(f, 0, bytes, ctx->stream));
+  for (double *f : zero) CKC(cudaMemsetAsync(f - xo, 0, fbytes, ctx->stream));
   if (io.visc)  // DRHOI_STG is zero until the first DENSITY_implicit_add
-    for (int c = 0; c < 3; ++c) CKC(cudaMemsetAsync(io.drhoi[c], 0, bytes, ctx->stream));
+    for (int c = 0; c < 3; ++c) CKC(cudaMemsetAsync(io.drhoi[c] - xo, 0, fbytes, ctx->stream));
   CKC(cudaMemsetAsync(io.bad, 0, sizeof(unsigned long long), ctx->stream));
+  if (ctx->xnp)  // the boundary operators' RK3 memory terms BC_CONV0, BC_CONV0_ENG
+    CKC(cudaMemsetAsync(io.bcp + (size_t)io.bps * CHAPSIM_P_CONV0_X, 0, (size_t)io.bps * 4 * sizeof(double),
+                        ctx->stream));
   const double M2 = M0 + M0;
   const double *vals[] = {&T0, &D0, &D0, &M0, &M0, &K0, &M2};
   double *arrs[] = {io.T, io.D, io.D0, io.mu, io.mu0, io.kap, io.msum};
   for (int a = 0; a < 7; ++a)
-    if ((rc = fill_value(ctx, arrs[a], (size_t)n, *vals[a]))) return rc;
+    if ((rc = fill_value(ctx, arrs[a] - xo, (size_t)nf, *vals[a]))) return rc;
   if (project) {  // CALC_INITIALIZATION_io
     if (io.thermal) {
       if ((rc = io_thermal_bc(ctx))) return rc;
@@ -1020,7 +1093,6 @@ static int io_init_random(chapsim_ctx *ctx, uint64_t seed, double amp, int proje
 
 int chapsim_init_random(chapsim_ctx *ctx, uint64_t seed, double amp, int project) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
-  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED, "Dirichlet / Neumann x ends (BCX_io): only chapsim_pois3d is built");
   CKC(cudaSetDevice(ctx->device));
   if (ctx->domain == CHAPSIM_IIO) return io_init_random(ctx, seed, amp, project);
   const int nx = ctx->cfg.nx, ny = ctx->cfg.ny, nz = ctx->cfg.nz;
@@ -1089,10 +1161,10 @@ int chapsim_step_tg(chapsim_ctx *ctx, int nsteps) {
 
 int chapsim_divg(chapsim_ctx *ctx, int domain, int ns) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
-  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED, "Dirichlet / Neumann x ends (BCX_io): only chapsim_pois3d is built");
   REQUIRE(domain == ctx->domain, CHAPSIM_ERR_ARG, "domain does not match the context");
   REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
   CKC(cudaSetDevice(ctx->device));
+  if (ctx->xnp) return chapsim::io_np_divg(ctx, ns, ctx->io_cur);  // coupled section: RHSLLPHI only
   if (domain == CHAPSIM_IIO) {
     // DIVG_io (src/DIVG.f90:60-150) of the current G and DrhoDtP
     const TGDev saved = ctx->d;
@@ -1116,7 +1188,6 @@ int chapsim_pois3d(chapsim_ctx *ctx, int domain) {
 
 int chapsim_velo_correction(chapsim_ctx *ctx, int domain, int ns) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
-  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED, "Dirichlet / Neumann x ends (BCX_io): only chapsim_pois3d is built");
   REQUIRE(domain == ctx->domain, CHAPSIM_ERR_ARG, "domain does not match the context");
   REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
   CKC(cudaSetDevice(ctx->device));
@@ -1126,7 +1197,8 @@ int chapsim_velo_correction(chapsim_ctx *ctx, int domain, int ns) {
 
 int chapsim_stats(chapsim_ctx *ctx, int accumulate) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
-  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED, "Dirichlet / Neumann x ends (BCX_io): only chapsim_pois3d is built");
+  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED,
+          "the IO statistics are PP_MEAN_ZX_FLOW_Xperiodic_IO's: x-periodic sections only");
   CKC(cudaSetDevice(ctx->device));
   return stats_run(ctx, accumulate);
 }
@@ -1180,9 +1252,7 @@ int chapsim_set_dt(chapsim_ctx *ctx, double dt) {
       ctx->allocs.erase(it);
       break;
     }
-  if (ctx->step_graph) { cudaGraphExecDestroy(ctx->step_graph); ctx->step_graph = nullptr; }
-  for (auto &g : ctx->io_graph)
-    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  drop_graphs(ctx);
   return CHAPSIM_OK;
 }
 
@@ -1195,8 +1265,7 @@ int chapsim_set_table(chapsim_ctx *ctx, const double *H, const double *T, const 
     REQUIRE(H[i] > H[i - 1] && T[i] > T[i - 1], CHAPSIM_ERR_ARG, "H and T must increase strictly");
   CKC(cudaSetDevice(ctx->device));
   CKC(cudaStreamSynchronize(ctx->stream));
-  for (auto &g : ctx->io_graph)
-    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  drop_graphs(ctx);
   for (void *p : ctx->table_allocs) cudaFree(p);
   ctx->table_allocs.clear();
   const double *cols[5] = {H, T, D, M, K};
@@ -1258,6 +1327,8 @@ int chapsim_set_props_mode(chapsim_ctx *ctx, int mode, const chapsim_props *pe) 
   REQUIRE(ctx->domain == CHAPSIM_IIO && ctx->io.thermal, CHAPSIM_ERR_STATE,
           "property modes belong to IO contexts with the energy equation");
   REQUIRE(ctx->has_table, CHAPSIM_ERR_STATE, "no property table: call chapsim_set_table first");
+  REQUIRE(!ctx->xnp || mode == CHAPSIM_PROPS_TABLE, CHAPSIM_ERR_UNSUPPORTED,
+          "the learned property kernel walks x-periodic fields (no ghost columns)");
   REQUIRE(mode == CHAPSIM_PROPS_TABLE || mode == CHAPSIM_PROPS_MLP, CHAPSIM_ERR_ARG, "unknown property mode");
   CKC(cudaSetDevice(ctx->device));
   CKC(cudaStreamSynchronize(ctx->stream));
@@ -1298,13 +1369,14 @@ int chapsim_set_props_mode(chapsim_ctx *ctx, int mode, const chapsim_props *pe) 
     REQUIRE(((uintptr_t)ctx->mlp.wt & 15) == 0, CHAPSIM_ERR_STATE, "model weight tiles not 16-byte aligned");
   }
   ctx->props_mode = mode;
-  for (auto &g : ctx->io_graph)  // the captured steps hold the other property kernel
-    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  drop_graphs(ctx);  // the captured steps hold the other property kernel
   return CHAPSIM_OK;
 }
 
 int chapsim_therm_prop_update(chapsim_ctx *ctx, int iregion, int mode) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED,
+          "THERM_PROP_UPDATE alone walks x-periodic fields (the coupled section updates inside its substeps)");
   REQUIRE(ctx->domain == CHAPSIM_IIO && ctx->io.thermal && ctx->has_table, CHAPSIM_ERR_STATE,
           "THERM_PROP_UPDATE needs an IO context with the energy equation and a table");
   REQUIRE(iregion == CHAPSIM_IMAIND || iregion == CHAPSIM_IALLDM, CHAPSIM_ERR_UNSUPPORTED,
@@ -1318,7 +1390,6 @@ int chapsim_therm_prop_update(chapsim_ctx *ctx, int iregion, int mode) {
 
 int chapsim_rk3_eng_io(chapsim_ctx *ctx, int ns) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
-  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED, "Dirichlet / Neumann x ends (BCX_io): only chapsim_pois3d is built");
   REQUIRE(ctx->domain == CHAPSIM_IIO, CHAPSIM_ERR_STATE, "not an IO context");
   REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
   REQUIRE(ctx->io.thermal, CHAPSIM_ERR_STATE, "thermal is off on this IO context");
@@ -1329,7 +1400,6 @@ int chapsim_rk3_eng_io(chapsim_ctx *ctx, int ns) {
 
 int chapsim_rk3_mom_io(chapsim_ctx *ctx, int ns) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
-  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED, "Dirichlet / Neumann x ends (BCX_io): only chapsim_pois3d is built");
   REQUIRE(ctx->domain == CHAPSIM_IIO, CHAPSIM_ERR_STATE, "not an IO context");
   REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
   CKC(cudaSetDevice(ctx->device));
@@ -1338,8 +1408,11 @@ int chapsim_rk3_mom_io(chapsim_ctx *ctx, int ns) {
 
 // Coupled inflow/outflow boundary planes (BC_TINLET_FLOW, BC_COUTLET_MOM_RK3,
 // BC_COUTLET_ENEG_RK3): io_kernels.cu.
+static const char *kCoupledBc = "the coupled section runs its boundary operators inside its substeps";
+
 int chapsim_io_bc_inlet(chapsim_ctx *ctx, chapsim_ctx *tg) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED, kCoupledBc);
   REQUIRE(tg, CHAPSIM_ERR_ARG, "null TG context");
   REQUIRE(ctx->domain == CHAPSIM_IIO, CHAPSIM_ERR_STATE, "not an IO context");
   REQUIRE(tg->domain == CHAPSIM_ITG, CHAPSIM_ERR_ARG, "the inlet source must be a TG context");
@@ -1356,6 +1429,7 @@ int chapsim_io_bc_inlet(chapsim_ctx *ctx, chapsim_ctx *tg) {
 
 int chapsim_io_bc_outlet_mom(chapsim_ctx *ctx, int ns) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED, kCoupledBc);
   REQUIRE(ctx->domain == CHAPSIM_IIO, CHAPSIM_ERR_STATE, "not an IO context");
   REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
   CKC(cudaSetDevice(ctx->device));
@@ -1364,6 +1438,7 @@ int chapsim_io_bc_outlet_mom(chapsim_ctx *ctx, int ns) {
 
 int chapsim_io_bc_outlet_eng(chapsim_ctx *ctx, int ns) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED, kCoupledBc);
   REQUIRE(ctx->domain == CHAPSIM_IIO, CHAPSIM_ERR_STATE, "not an IO context");
   REQUIRE(ns >= 0 && ns <= 3, CHAPSIM_ERR_ARG, "NS must be in 0..3");
   REQUIRE(ctx->io.thermal && ctx->has_table, CHAPSIM_ERR_STATE,
@@ -1417,7 +1492,6 @@ static int io_substeps(chapsim_ctx *ctx) {
 
 int chapsim_step_io(chapsim_ctx *ctx, int nsteps) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
-  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED, "Dirichlet / Neumann x ends (BCX_io): only chapsim_pois3d is built");
   REQUIRE(ctx->domain == CHAPSIM_IIO, CHAPSIM_ERR_STATE, "not an IO context");
   REQUIRE(nsteps >= 0, CHAPSIM_ERR_ARG, "nsteps must be >= 0");
   REQUIRE(!ctx->io.thermal || ctx->has_table, CHAPSIM_ERR_STATE, "no property table");
@@ -1454,9 +1528,86 @@ int chapsim_step_io(chapsim_ctx *ctx, int nsteps) {
   return CHAPSIM_OK;
 }
 
+int chapsim_io_set_inlet(chapsim_ctx *io, chapsim_ctx *tg) {
+  chapsim_ctx *ctx = io;  // error messages go to the IO context
+  REQUIRE(io, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(io->domain == CHAPSIM_IIO && io->xnp, CHAPSIM_ERR_STATE,
+          "not a coupled IO section (create it with non-periodic bcx_in / bcx_out)");
+  CKC(cudaSetDevice(io->device));
+  detach_inlet(io);
+  if (!tg) return CHAPSIM_OK;
+  REQUIRE(tg->domain == CHAPSIM_ITG, CHAPSIM_ERR_ARG, "the inlet source must be a TG context");
+  REQUIRE(tg->device == io->device, CHAPSIM_ERR_UNSUPPORTED, "the TG and IO contexts are on different devices");
+  REQUIRE(tg->cfg.ny == io->cfg.ny && tg->cfg.nz == io->cfg.nz, CHAPSIM_ERR_ARG,
+          "the TG and IO sections differ in ny or nz");
+  CKC(cudaStreamSynchronize(io->stream));
+  CKC(cudaStreamSynchronize(tg->stream));
+  // the section's kernels run in the TG stream's order from now on: its
+  // BC_TINLET_FLOW reads the TG fields between the TG's substeps
+  io->inlet = tg;
+  io->stream = tg->stream;
+  tg->fed.push_back(io);
+  drop_graphs(io);
+  return CHAPSIM_OK;
+}
+
+// SOLVE.f90's substep loop (src/SOLVE.f90:119-134) over both sections:
+// SOLVERRK3_MOM_tg(NS), then SOLVERRK3_ENG_IO(NS) with the density terms,
+// VELOCITY_CALC_io and SOLVERRK3_MOM_IO(NS), which reads the TG's new fields.
+static int pair_substeps(chapsim_ctx *tg, chapsim_ctx *io) {
+  for (int ns = 1; ns <= 3; ++ns) {
+    int rc;
+    if ((rc = launch_substep(tg, ns))) return rc;
+    if (io->io.thermal && (rc = io_eng(io, ns))) return rc;
+    if ((rc = io_mom(io, ns, true))) return rc;
+  }
+  return CHAPSIM_OK;
+}
+
+int chapsim_step_coupled(chapsim_ctx *tg, chapsim_ctx *io, int nsteps) {
+  chapsim_ctx *ctx = io;  // error messages go to the IO context
+  REQUIRE(tg && io, CHAPSIM_ERR_ARG, "null context");
+  REQUIRE(io->domain == CHAPSIM_IIO && io->xnp && io->inlet == tg, CHAPSIM_ERR_STATE,
+          "the IO section is not coupled to this TG context (chapsim_io_set_inlet)");
+  REQUIRE(nsteps >= 0, CHAPSIM_ERR_ARG, "nsteps must be >= 0");
+  REQUIRE(!io->io.thermal || io->has_table, CHAPSIM_ERR_STATE, "no property table");
+  CKC(cudaSetDevice(io->device));
+  if (tg->timing || io->timing) {
+    for (int s = 0; s < nsteps; ++s) {
+      int rc = pair_substeps(tg, io);
+      if (rc) return rc;
+    }
+    return CHAPSIM_OK;
+  }
+  for (int s = 0; s < nsteps; ++s) {
+    const int par = io->io_cur;
+    if (!io->pair_graph[par]) {
+      cudaGraph_t g = nullptr;
+      const int64_t bt = tg->launches, bi = io->launches;
+      CKC(cudaStreamBeginCapture(io->stream, cudaStreamCaptureModeThreadLocal));
+      int rc = pair_substeps(tg, io);
+      cudaError_t e = cudaStreamEndCapture(io->stream, &g);
+      io->io_cur = par;  // captured, not run
+      io->pair_kernels = (tg->launches - bt) + (io->launches - bi);
+      tg->launches = bt;
+      io->launches = bi;
+      if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+      if (e != cudaSuccess) { io->err = cudaGetErrorString(e); return CHAPSIM_ERR_CUDA; }
+      e = cudaGraphInstantiate(&io->pair_graph[par], g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) { io->pair_graph[par] = nullptr; io->err = cudaGetErrorString(e); return CHAPSIM_ERR_CUDA; }
+    }
+    CKC(cudaGraphLaunch(io->pair_graph[par], io->stream));
+    io->launches += io->pair_kernels;
+    io->io_cur = 1 - par;
+  }
+  return CHAPSIM_OK;
+}
+
 int chapsim_reduce(chapsim_ctx *ctx, int domain, int what, double *out) {
   REQUIRE(ctx, CHAPSIM_ERR_ARG, "null context");
-  REQUIRE(!ctx->xnp, CHAPSIM_ERR_UNSUPPORTED, "Dirichlet / Neumann x ends (BCX_io): only chapsim_pois3d is built");
+  REQUIRE(!ctx->xnp || what != CHAPSIM_R_DIVMAX_Q, CHAPSIM_ERR_UNSUPPORTED,
+          "max|div u| of the coupled section: use CHAPSIM_R_DIVMAX (div G + DrhoDtP)");
   REQUIRE(out, CHAPSIM_ERR_ARG, "null output");
   REQUIRE(domain == ctx->domain, CHAPSIM_ERR_ARG, "domain does not match the context");
   CKC(cudaSetDevice(ctx->device));
@@ -1523,21 +1674,14 @@ int chapsim_set_tuning(chapsim_ctx *ctx, int rhs_nzc, int fft_lb) {
   ctx->rhs_nzc = rhs_nzc;
   ctx->io_nzc = rhs_nzc;  // the IO momentum RHS marches the same way
   ctx->fft_lb = fft_lb;
-  if (ctx->step_graph) {
-    cudaGraphExecDestroy(ctx->step_graph);
-    ctx->step_graph = nullptr;
-  }
-  for (auto &g : ctx->io_graph)
-    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  drop_graphs(ctx);
   return CHAPSIM_OK;
 }
 
 int chapsim_set_line_tuning(chapsim_ctx *ctx, int ysolve_bx) {
   if (!ctx || (ysolve_bx != 64 && ysolve_bx != 128 && ysolve_bx != 256)) return CHAPSIM_ERR_ARG;
   ctx->ys_bx = ysolve_bx;
-  if (ctx->step_graph) { cudaGraphExecDestroy(ctx->step_graph); ctx->step_graph = nullptr; }
-  for (auto &g : ctx->io_graph)
-    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  drop_graphs(ctx);
   return CHAPSIM_OK;
 }
 

@@ -46,6 +46,10 @@ struct TGDev {
   const double *drho;
   int pin_last;
   int skip_rhs;  // 1: the fused forward x-transform does not store RHSLLPHI
+  // 1: the coupled inflow / outflow IO section (non-periodic x): the fields
+  // carry the ghost columns i = -1 (IC = 0) and i = nx (IC = NCL1_io + 1),
+  // sy = nx + 2, and x neighbours do not wrap
+  int xnp;
 };
 
 // Device-side state of an IO domain (x-periodic channel section), on top of
@@ -76,10 +80,20 @@ struct IODev {
   double *stg[6];  // MU_STG 1-3, RHO_STG 1-3 of the current substep (energy equation on)
   double amvr1, apvrn;
   // coupled inflow/outflow ghost planes CHAPSIM_P_* ((ny + 2) * nz each, plane
-  // q at bcp + q * bps) and their scalars (chapsim_io_bc_scalars)
+  // q at bcp + q * bps; the coupled substep's own planes P_SAVE_* follow) and
+  // their scalars (chapsim_io_bc_scalars)
   double *bcp, *bcs;
   int64_t bps;
 };
+
+// Planes after the public CHAPSIM_P_* ones: G0_io of the boundary columns
+// kept across a coupled momentum substep (the boundary operators overwrite
+// G_io there before the substep's G* is formed): G x, y, z of the inlet ghost
+// column, G x of the first face, G x, y, z of the outlet ghost column.
+constexpr int P_SAVE_IN = CHAPSIM_P_COUNT;       // + 0..2
+constexpr int P_SAVE_FACE1 = CHAPSIM_P_COUNT + 3;
+constexpr int P_SAVE_OUT = CHAPSIM_P_COUNT + 4;  // + 0..2
+constexpr int P_ALL = CHAPSIM_P_COUNT + 7;
 
 // Per-substep scalars.
 constexpr int BAND_ROWS = 13;  // g_0 .. g_12: the widest truncated x / z inverse kept
@@ -160,6 +174,12 @@ struct chapsim_ctx {
   // spectral descriptor of its nx real x modes and the transposed x-transform
   // matrices (forward with 1 / SCALX)
   int xnp = 0;
+  int xoff = 0;  // field pointers start this many values into their allocation (1 with x ghost columns)
+  chapsim_ctx *inlet = nullptr;      // coupled section: the TG context feeding BC_TINLET_FLOW
+  std::vector<chapsim_ctx *> fed;    // TG context: the coupled sections it feeds
+  cudaStream_t own_stream = nullptr;  // the context's stream (a coupled section runs on its TG's)
+  cudaGraphExec_t pair_graph[2] = {nullptr, nullptr};  // TG + IO step, by the IO's io_cur at its start
+  int64_t pair_kernels = 0;                             // kernels of both contexts in one pair step
   chapsim::TGDev dnp{};
   double *xnp_f = nullptr, *xnp_b = nullptr;
   // CUDA graph of one full step (NS = 1, 2, 3)
@@ -205,7 +225,7 @@ int launch_substep(chapsim_ctx *c, int ns);
 int launch_divg(chapsim_ctx *c, int ns);
 int launch_pois3d(chapsim_ctx *c);
 int xnp_pivots(chapsim_ctx *c);
-int xnp_pois3d(chapsim_ctx *c);
+int xnp_pois3d(chapsim_ctx *c, bool mark = false);  // mark: phase timers 5-8 of a substep
 int launch_correction(chapsim_ctx *c, int ns);
 int launch_reduce(chapsim_ctx *c, int what, double *host_out);
 int launch_bc_q(chapsim_ctx *c);
@@ -221,6 +241,8 @@ int io_eng(chapsim_ctx *c, int ns);
 int io_bc_inlet(chapsim_ctx *c, const chapsim_ctx *tg);
 int io_bc_outlet_mom(chapsim_ctx *c, int ns);
 int io_bc_outlet_eng(chapsim_ctx *c, int ns);
+// coupled section (xnp): DIVG_io of the G buffer buf into RHSLLPHI
+int io_np_divg(chapsim_ctx *c, int ns, int buf);
 int io_thermal_bc(chapsim_ctx *c);
 int io_mom(chapsim_ctx *c, int ns, bool prep);
 // semi-implicit scheme: right-hand sides (*npart: the DPGRNS partial count),

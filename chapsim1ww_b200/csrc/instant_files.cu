@@ -146,6 +146,7 @@ extern "C" {
 
 int chapsim_write_instant(chapsim_ctx *ctx, const char *dir, int iteration, double time) {
   if (!ctx) return CHAPSIM_ERR_ARG;
+  if (ctx->xnp) return CHAPSIM_ERR_UNSUPPORTED;  // files of the x-periodic layout only
   if (cudaSetDevice(ctx->device) != cudaSuccess) return CHAPSIM_ERR_CUDA;
   TGDev &d = ctx->d;
   const bool io = ctx->domain == CHAPSIM_IIO;
@@ -175,6 +176,7 @@ int chapsim_write_instant(chapsim_ctx *ctx, const char *dir, int iteration, doub
 
 int chapsim_read_instant(chapsim_ctx *ctx, const char *dir, double time, int *iteration, double *time_out) {
   if (!ctx) return CHAPSIM_ERR_ARG;
+  if (ctx->xnp) return CHAPSIM_ERR_UNSUPPORTED;  // files of the x-periodic layout only
   if (cudaSetDevice(ctx->device) != cudaSuccess) return CHAPSIM_ERR_CUDA;
   TGDev &d = ctx->d;
   const bool io = ctx->domain == CHAPSIM_IIO;

@@ -74,6 +74,11 @@ constexpr int IO_BX = 32, IO_BY = 8;
 
 __device__ __forceinline__ int wrapp(int i, int n) { return i + 1 == n ? 0 : i + 1; }
 __device__ __forceinline__ int wrapm(int i, int n) { return i == 0 ? n - 1 : i - 1; }
+// x-neighbour offsets: the periodic wrap (IPV_io / IMV_io of the x-periodic
+// section), or the coupled section's ghost columns (IPV_io(NCL1_io) =
+// NCL1_io + 1, IMV_io(1) = 0, src/INDEXSET.f90:25-32)
+__device__ __forceinline__ int64_t xplus(const TGDev &d, int i) { return d.xnp ? 1 : (int64_t)(wrapp(i, d.nx) - i); }
+__device__ __forceinline__ int64_t xminus(const TGDev &d, int i) { return d.xnp ? -1 : (int64_t)(wrapm(i, d.nx) - i); }
 
 // ---------------------------------------------------------------- table look-ups
 // NIST_SLEVAL_HT (src/Flow_State.f90:1015-1070): false outside the table.
@@ -114,7 +119,7 @@ __global__ void __launch_bounds__(IO_BX *IO_BY, 6) k_io_eng_rhs(TGDev d, IODev i
   const int k = blockIdx.z;
   if (i >= nx || j > ny) return;
   const int64_t sy = d.sy, c = i + sy * j + d.sz * k;
-  const int64_t oxp = wrapp(i, nx) - i, oxm = wrapm(i, nx) - i;
+  const int64_t oxp = xplus(d, i), oxm = xminus(d, i);
   const int64_t ozp = d.sz * (wrapp(k, d.nz) - k), ozm = d.sz * (wrapm(k, d.nz) - k);
   const double *__restrict__ gx = io.g[cur][0], *__restrict__ gy = io.g[cur][1], *__restrict__ gz = io.g[cur][2];
   const double *__restrict__ hx = io.g[1 - cur][0], *__restrict__ hy = io.g[1 - cur][1],
@@ -476,7 +481,7 @@ __global__ void __launch_bounds__(IO_BX *IO_BY, VISC ? 1 : 8) k_io_prep(TGDev d,
   const int k = blockIdx.z;
   if (i >= nx || j > ny) return;
   const int64_t sy = d.sy, c = i + sy * j + d.sz * k;
-  const int64_t oxp = wrapp(i, nx) - i, oxm = wrapm(i, nx) - i;
+  const int64_t oxp = xplus(d, i), oxm = xminus(d, i);
   const int64_t ozp = d.sz * (wrapp(k, d.nz) - k), ozm = d.sz * (wrapm(k, d.nz) - k);
   const double *__restrict__ gx = io.g[cur][0], *__restrict__ gy = io.g[cur][1], *__restrict__ gz = io.g[cur][2];
   if (do_drho) {
@@ -559,7 +564,7 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_rhs(TGDev d, IODev io, doub
   double part = 0.0;
   if (i < nx && j <= ny) {
     const int64_t sy = d.sy, c = i + sy * j + d.sz * k;
-    const int64_t oxp = wrapp(i, nx) - i, oxm = wrapm(i, nx) - i;
+    const int64_t oxp = xplus(d, i), oxm = xminus(d, i);
     const int64_t ozp = d.sz * (wrapp(k, d.nz) - k), ozm = d.sz * (wrapm(k, d.nz) - k);
     const double *__restrict__ u = d.u, *__restrict__ v = d.v, *__restrict__ w = d.w, *__restrict__ p = d.p;
     const double *__restrict__ gx = io.g[cur][0], *__restrict__ gy = io.g[cur][1], *__restrict__ gz = io.g[cur][2];
@@ -572,13 +577,18 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_rhs(TGDev d, IODev io, doub
     const double wff = d.wff[j], wfb = d.wfb[j], wffp = d.wff[j + 1], wfbp = d.wfb[j + 1];
     // DIVG_U_io at cell (ii, jj, kk) = cc
     auto divu = [&](int64_t cc, int ii, int jj, int kk) {
-      const int64_t op = (ii + 1 == nx) ? -(int64_t)(nx - 1) : 1;
+      const int64_t op = (!d.xnp && ii + 1 == nx) ? -(int64_t)(nx - 1) : 1;
       const int64_t oz = (kk + 1 == d.nz) ? -(int64_t)d.sz * (d.nz - 1) : d.sz;
       return ((u[cc + op] - u[cc]) * dxi + (v[cc + sy] - v[cc]) * d.dyfi[jj] + (w[cc + oz] - w[cc]) * dzi) / 3.0;
     };
     const double divc = divu(c, i, j, k);
-    // ---------------- x: CONVECTION_X_io + VISCOUS_ALL_EXPLT_X_io
-    {
+    // the coupled section's staggered viscosities MU_STG on the outlet ghost
+    // face keep their initial value 1 (MU_Staggered covers IC = 1..NCL1_io,
+    // src/MASSFLUX_CALC_IO.f90:147-237, MEMALLOCT.f90:201)
+    const bool xout = d.xnp && i == nx - 1;
+    // ---------------- x: CONVECTION_X_io + VISCOUS_ALL_EXPLT_X_io; the coupled
+    // section's inlet face (NXI = 2) keeps its value (copied by k_np_gbound)
+    if (!d.xnp || i > 0) {
       double h11f = (gx[c + oxp] + gx[c]) * (u[c + oxp] + u[c]);
       double h11b = (gx[c] + gx[c + oxm]) * (u[c] + u[c + oxm]);
       double h11 = (h11f - h11b) * (dxi * 0.5 * 0.5);
@@ -639,7 +649,7 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_rhs(TGDev d, IODev io, doub
       const double d22 = (tau22f - tau22b) * (2.0 * dycj * cv);
       double dvdx = (v[c + oxp] - v[c]) * dxi;
       double dudy = (u[c + oxp] - u[c + oxp - sy]) * dycj;
-      const double tau21f = mv.s1(c + oxp, j, -oxp) * (dvdx + dudy);
+      const double tau21f = (xout ? 1.0 : mv.s1(c + oxp, j, -oxp)) * (dvdx + dudy);
       dvdx = (v[c] - v[c + oxm]) * dxi;
       dudy = (u[c] - u[c - sy]) * dycj;
       const double tau21b = mv.s1(c, j, oxm) * (dvdx + dudy);
@@ -681,7 +691,7 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_rhs(TGDev d, IODev io, doub
       const double d33 = (tau33f - tau33b) * (2.0 * dzi * cv);
       double dwdx = (w[c + oxp] - w[c]) * dxi;
       double dudz = (u[c + oxp] - u[c + oxp + ozm]) * dzi;
-      const double tau31f = mv.s2(c + oxp, -oxp, ozm) * (dwdx + dudz);
+      const double tau31f = (xout ? 1.0 : mv.s2(c + oxp, -oxp, ozm)) * (dwdx + dudz);
       dwdx = (w[c] - w[c + oxm]) * dxi;
       dudz = (u[c] - u[c + ozm]) * dzi;
       const double tau31b = mv.s2(c, oxm, ozm) * (dwdx + dudz);
@@ -1061,12 +1071,16 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_corr(TGDev d, IODev io, dou
   const int k = blockIdx.z;
   if (i >= nx || j > ny) return;
   const int64_t sy = d.sy, c = i + sy * j + d.sz * k;
-  const int64_t oxm = wrapm(i, nx) - i, ozm = d.sz * (wrapm(k, d.nz) - k);
+  const int64_t oxm = xminus(d, i), ozm = d.sz * (wrapm(k, d.nz) - k);
   double *gx = io.g[buf][0], *gy = io.g[buf][1], *gz = io.g[buf][2];
   const double phi = d.phi[c];
   double gxv = gx[c];
   if (use_dpg) gxv -= *io.dpg;
-  gx[c] = gxv - (phi - d.phi[c + oxm]) * (d.dt * alp * d.dxi);
+  // the coupled section corrects the x flux from NXI = 2 to NXE = NCL1_io + 1:
+  // the inlet face keeps its value, the outlet face takes the ghost
+  // DPH_io(NCL1_io + 1), which no routine writes (zero)
+  if (!d.xnp || i > 0) gx[c] = gxv - (phi - d.phi[c + oxm]) * (d.dt * alp * d.dxi);
+  if (d.xnp && i == nx - 1) gx[c + 1] -= (0.0 - phi) * (d.dt * alp * d.dxi);
   gz[c] -= (phi - d.phi[c + ozm]) * (d.dt * alp * d.dzi);
   if (j >= 2) gy[c] -= (phi - d.phi[c - sy]) * (d.dt * alp * d.dyci[j]);
   // semi-implicit PRCALC_io (src/PRESSURE_CORRECTION.f90:100-110) with the
@@ -1091,14 +1105,14 @@ __global__ void __launch_bounds__(IO_BX *IO_BY) k_io_red_part(TGDev d, IODev io,
   if (i < nx && j <= ny) {
     const int64_t sy = d.sy, c = i + sy * j + d.sz * k;
     if (what == 0) {
-      const int64_t oxp = wrapp(i, nx) - i, ozp = d.sz * (wrapp(k, d.nz) - k);
+      const int64_t oxp = xplus(d, i), ozp = d.sz * (wrapp(k, d.nz) - k);
       const double *gx = io.g[cur][0], *gy = io.g[cur][1], *gz = io.g[cur][2];
       const double dv = (gx[c + oxp] - gx[c]) * d.dxi + (gy[c + sy] - gy[c]) * d.dyfi[j] +
                         (gz[c + ozp] - gz[c]) * d.dzi + io.drho[c];
       v = fabs(dv);
       if (dv != dv) v = __longlong_as_double(0x7ff0000000000000ll);
     } else if (what == 2) {
-      const int64_t oxp = wrapp(i, nx) - i, ozp = d.sz * (wrapp(k, d.nz) - k);
+      const int64_t oxp = xplus(d, i), ozp = d.sz * (wrapp(k, d.nz) - k);
       const double *gx = io.g[cur][0], *gy = io.g[cur][1], *gz = io.g[cur][2];
       v = (fabs((gx[c] + gx[c + oxp]) * d.dxi) + fabs((gy[c] + gy[c + sy]) * d.dyfi[j]) +
            fabs((gz[c] + gz[c + ozp]) * d.dzi)) * 0.5;
@@ -1186,6 +1200,9 @@ int mlp_grid(const chapsim_ctx *c, int per_sm) {
   return (int)std::min<int64_t>(tiles, (int64_t)nsm * per_sm);
 }
 
+int io_np_eng_bc(chapsim_ctx *c, int ns);
+int io_np_mom(chapsim_ctx *c, int ns);
+
 // Phase-timer slots of an IO substep, in execution order: 0 energy RHS,
 // 1 property update + wall ghosts, 2 prep (DrhoDtP, u = G / rho), 3 momentum
 // RHS + DPGRNS, 4-8 the Poisson transforms and y-solve, 9 correction.
@@ -1205,6 +1222,10 @@ int io_eng(chapsim_ctx *c, int ns) {
     k_io_eng_props<<<g2, dim3(IO_BX, IO_BY), 0, c->stream>>>(d, c->io);
   }
   LAUNCHED();
+  if (c->xnp) {
+    const int rc = io_np_eng_bc(c, ns);
+    if (rc) return rc;
+  }
   return io_thermal_bc(c);
 }
 
@@ -1237,6 +1258,7 @@ int io_mom(chapsim_ctx *c, int ns, bool prep) {
     LAUNCHED();
   }
   phase_mark(c, 3);
+  if (c->xnp) return io_np_mom(c, ns);
   int npart = (int)(grid.x * grid.y * grid.z);
   if (io.visc) {
     // semi-implicit scheme: RHS_io of the three components, DPGRNS, factored
@@ -1291,7 +1313,8 @@ int io_mom(chapsim_ctx *c, int ns, bool prep) {
 int io_init_maps(chapsim_ctx *c) {
   TGDev &d = c->d;
   c->use_tma_io = false;
-  if (d.nx < IT_BXW || d.ny < 8) return CHAPSIM_OK;  // small grids use k_io_rhs
+  // small grids and the coupled section (ghost columns) use k_io_rhs
+  if (d.nx < IT_BXW || d.ny < 8 || c->xnp) return CHAPSIM_OK;
   PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   cudaDriverEntryPointQueryResult q;
   if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void **)&encode, cudaEnableDefault, &q) != cudaSuccess ||
@@ -1602,6 +1625,135 @@ __global__ void k_bc_outlet_eng_ghost(TGDev d, IODev io) {
   bplane(io, CHAPSIM_P_OUT_RHOH)[pc] = h * D;
 }
 
+
+// ---------------------------------------------------------------- coupled section (xnp)
+// The coupled inflow / outflow section holds its x ghost columns in the
+// fields (i = -1: IC = 0, i = nx: IC = NCL1_io + 1).  The boundary operators
+// above work on planes: k_np_mom_pre / k_np_eng_pre copy the columns they
+// read into the planes, k_np_mom_post / k_np_eng_post write their results
+// back.  Every kernel runs one thread per (j, k), j = 0..ny+1.
+__device__ __forceinline__ int64_t col(const TGDev &d, int i, int j, int k) {
+  return (int64_t)i + d.sy * j + d.sz * k;
+}
+
+// Start of a coupled SOLVERRK3_MOM_IO (:15-21): G0_io = G_io happens by the
+// buffer swap, except on the columns the boundary operators rewrite in
+// place; their old G goes to the P_SAVE planes.  The outlet planes get u, v,
+// w, G and rho of the outlet ghost column.
+__global__ void k_np_mom_pre(TGDev d, IODev io, int cur) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (d.ny + 2) * d.nz) return;
+  const int k = t / (d.ny + 2), j = t - k * (d.ny + 2);
+  const int64_t ci = col(d, -1, j, k), c1 = col(d, 0, j, k), co = col(d, d.nx, j, k);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    bplane(io, P_SAVE_IN + q)[t] = io.g[cur][q][ci];
+    bplane(io, P_SAVE_OUT + q)[t] = io.g[cur][q][co];
+    bplane(io, CHAPSIM_P_OUT_GX + q)[t] = io.g[cur][q][co];
+  }
+  bplane(io, P_SAVE_FACE1)[t] = io.g[cur][0][c1];
+  bplane(io, CHAPSIM_P_OUT_U)[t] = d.u[co];
+  bplane(io, CHAPSIM_P_OUT_V)[t] = d.v[co];
+  bplane(io, CHAPSIM_P_OUT_W)[t] = d.w[co];
+  bplane(io, CHAPSIM_P_OUT_RHO)[t] = io.D[co];
+}
+
+// After BC_TINLET_FLOW and BC_COUTLET_MOM_RK3: the inlet planes into ghost
+// column IC = 0 (u, v, w, G, p, rho; DPH_io(0) stays zero), the outlet
+// planes into IC = NCL1_io + 1 (u, v, w, G).
+__global__ void k_np_mom_post(TGDev d, IODev io, int cur) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (d.ny + 2) * d.nz) return;
+  const int k = t / (d.ny + 2), j = t - k * (d.ny + 2);
+  const int64_t ci = col(d, -1, j, k), co = col(d, d.nx, j, k);
+  double *q3[3] = {d.u, d.v, d.w};
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    q3[q][ci] = bplane(io, CHAPSIM_P_IN_U + q)[t];
+    io.g[cur][q][ci] = bplane(io, CHAPSIM_P_IN_GX + q)[t];
+    q3[q][co] = bplane(io, CHAPSIM_P_OUT_U + q)[t];
+    io.g[cur][q][co] = bplane(io, CHAPSIM_P_OUT_GX + q)[t];
+  }
+  d.p[ci] = bplane(io, CHAPSIM_P_IN_P)[t];
+  io.D[ci] = bplane(io, CHAPSIM_P_IN_RHO)[t];
+}
+
+// After the momentum RHS wrote G* into g[nxt]: the boundary columns the
+// substep does not advance (the ghost columns and the inlet face) carry the
+// boundary operators' G into G*, and g[cur], which becomes G0_io, gets back
+// its values from the start of the substep.
+__global__ void k_np_gbound(TGDev d, IODev io, int cur) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (d.ny + 2) * d.nz) return;
+  const int k = t / (d.ny + 2), j = t - k * (d.ny + 2);
+  const int nxt = 1 - cur;
+  const int64_t ci = col(d, -1, j, k), c1 = col(d, 0, j, k), co = col(d, d.nx, j, k);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    io.g[nxt][q][ci] = io.g[cur][q][ci];
+    io.g[nxt][q][co] = io.g[cur][q][co];
+    io.g[cur][q][ci] = bplane(io, P_SAVE_IN + q)[t];
+    io.g[cur][q][co] = bplane(io, P_SAVE_OUT + q)[t];
+  }
+  io.g[nxt][0][c1] = io.g[cur][0][c1];
+  io.g[cur][0][c1] = bplane(io, P_SAVE_FACE1)[t];
+}
+
+// DIVG_io (src/DIVG.f90:60-150) of the coupled section: RHSLLPHI = (div G +
+// DrhoDtP) / (dt alpha) on the interior, the outlet face from the ghost column.
+__global__ void __launch_bounds__(IO_BX *IO_BY) k_np_divg(TGDev d, IODev io, int buf, double coe0) {
+  const int i = blockIdx.x * IO_BX + threadIdx.x;
+  const int j = blockIdx.y * IO_BY + threadIdx.y + 1;
+  const int k = blockIdx.z;
+  if (i >= d.nx || j > d.ny) return;
+  const int64_t sy = d.sy, c = i + sy * j + d.sz * k, ozp = d.sz * (wrapp(k, d.nz) - k);
+  const double *gx = io.g[buf][0], *gy = io.g[buf][1], *gz = io.g[buf][2];
+  const double dv = (gx[c + 1] - gx[c]) * d.dxi + (gy[c + sy] - gy[c]) * d.dyfi[j] + (gz[c + ozp] - gz[c]) * d.dzi;
+  d.rhsphi[c] = (dv + (io.thermal ? io.drho[c] : 0.0)) * coe0;
+}
+
+// Coupled SOLVERRK3_ENG_IO after the interior property update: VISCOUSITY0 /
+// DENSITY0 <- VISCOUSITY / DENSITY on both ghost columns (:13-16), then
+// BC_TINLET_THERML (src/BC_INLET.f90:54-76: the reference state on IC = 0),
+// and the outlet planes of BC_COUTLET_ENEG_RK3 from IC = NCL1_io + 1.
+__global__ void k_np_eng_pre(TGDev d, IODev io) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (d.ny + 2) * d.nz) return;
+  const int k = t / (d.ny + 2), j = t - k * (d.ny + 2);
+  const int64_t ci = col(d, -1, j, k), co = col(d, d.nx, j, k);
+  io.D0[ci] = io.D[ci];
+  io.mu0[ci] = io.mu[ci];
+  io.D0[co] = io.D[co];
+  io.mu0[co] = io.mu[co];
+  io.T[ci] = 1.0;
+  io.kap[ci] = 1.0;
+  io.D[ci] = 1.0;
+  io.mu[ci] = 1.0;
+  io.rhoh[ci] = 0.0;
+  io.h[ci] = 0.0;
+  io.msum[ci] = io.mu0[ci] + 1.0;
+  bplane(io, CHAPSIM_P_OUT_U)[t] = d.u[co];
+  bplane(io, CHAPSIM_P_OUT_RHO)[t] = io.D[co];
+  bplane(io, CHAPSIM_P_OUT_RHOH)[t] = io.rhoh[co];
+  bplane(io, CHAPSIM_P_OUT_H)[t] = io.h[co];
+  bplane(io, CHAPSIM_P_OUT_T)[t] = io.T[co];
+  bplane(io, CHAPSIM_P_OUT_MU)[t] = io.mu[co];
+  bplane(io, CHAPSIM_P_OUT_K)[t] = io.kap[co];
+}
+
+__global__ void k_np_eng_post(TGDev d, IODev io) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (d.ny + 2) * d.nz) return;
+  const int k = t / (d.ny + 2), j = t - k * (d.ny + 2);
+  const int64_t co = col(d, d.nx, j, k);
+  io.D[co] = bplane(io, CHAPSIM_P_OUT_RHO)[t];
+  io.rhoh[co] = bplane(io, CHAPSIM_P_OUT_RHOH)[t];
+  io.h[co] = bplane(io, CHAPSIM_P_OUT_H)[t];
+  io.T[co] = bplane(io, CHAPSIM_P_OUT_T)[t];
+  io.mu[co] = bplane(io, CHAPSIM_P_OUT_MU)[t];
+  io.kap[co] = bplane(io, CHAPSIM_P_OUT_K)[t];
+  io.msum[co] = io.mu0[co] + io.mu[co];
+}
 }  // namespace
 
 int io_bc_inlet(chapsim_ctx *c, const chapsim_ctx *tg) {
@@ -1646,4 +1798,70 @@ int io_bc_outlet_eng(chapsim_ctx *c, int ns) {
   return CHAPSIM_OK;
 }
 
+
+// Coupled SOLVERRK3_ENG_IO boundaries (:61-64) after the interior property
+// update: ghost-column DENSITY0 / VISCOUSITY0, BC_TINLET_THERML, and
+// BC_COUTLET_ENEG_RK3 on the outlet column.
+int io_np_eng_bc(chapsim_ctx *c, int ns) {
+  TGDev &d = c->d;
+  const int nb = ((d.ny + 2) * d.nz + 255) / 256;
+  k_np_eng_pre<<<nb, 256, 0, c->stream>>>(d, c->io);
+  LAUNCHED();
+  int rc = io_bc_outlet_eng(c, ns);
+  if (rc) return rc;
+  k_np_eng_post<<<nb, 256, 0, c->stream>>>(d, c->io);
+  LAUNCHED();
+  return CHAPSIM_OK;
+}
+
+int io_np_divg(chapsim_ctx *c, int ns, int buf) {
+  TGDev &d = c->d;
+  k_np_divg<<<cell_grid(d), dim3(IO_BX, IO_BY), 0, c->stream>>>(d, c->io, buf, 1.0 / d.dt / c->sp[ns].alp);
+  LAUNCHED();
+  return CHAPSIM_OK;
+}
+
+// Coupled SOLVERRK3_MOM_IO(NS) after VELOCITY_CALC_io (src/SOLVERRK3_MOM_IO.f90:
+// 15-168 with TGFLOWFLG): BC_TINLET_FLOW from the TG context and
+// BC_COUTLET_MOM_RK3 on the ghost columns, the momentum RHS and
+// MASSFLUX_CALC_IO from the second x face (no DPGRNS forcing, :218), DIVG_io
+// into RHSLLPHI, FISHPACK_POIS3D_SIMPLE with the non-periodic x transform on
+// the IO arrays (the coupled branch of :116-121 solves on the TG arrays; the
+// IO-only branch's arrays are used), PRCALC_io and MASSFLUX_UPDATE_IO with
+// the outlet face.
+int io_np_mom(chapsim_ctx *c, int ns) {
+  TGDev &d = c->d;
+  IODev &io = c->io;
+  if (!c->inlet) {
+    c->err = "coupled IO section without its TG inlet source (chapsim_io_set_inlet)";
+    return CHAPSIM_ERR_STATE;
+  }
+  const SubParams &sp = c->sp[ns];
+  const int cur = c->io_cur, nxt = 1 - cur;
+  const dim3 grid = cell_grid(d), blk(IO_BX, IO_BY);
+  const int nb = ((d.ny + 2) * d.nz + 255) / 256;
+  k_np_mom_pre<<<nb, 256, 0, c->stream>>>(d, io, cur);
+  LAUNCHED();
+  int rc = io_bc_inlet(c, c->inlet);
+  if (rc) return rc;
+  if ((rc = io_bc_outlet_mom(c, ns))) return rc;
+  k_np_mom_post<<<nb, 256, 0, c->stream>>>(d, io, cur);
+  LAUNCHED();
+  k_io_rhs<<<grid, blk, 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, cur);
+  LAUNCHED();
+  k_np_gbound<<<nb, 256, 0, c->stream>>>(d, io, cur);
+  LAUNCHED();
+  phase_mark(c, CHAPSIM_PH_FFTX);
+  if ((rc = io_np_divg(c, ns, nxt))) return rc;
+  if ((rc = xnp_pois3d(c, true))) return rc;
+  phase_mark(c, CHAPSIM_PH_CORR);
+  k_io_corr<<<grid, blk, 0, c->stream>>>(d, io, sp.alp, nxt, 0, 0.0);
+  LAUNCHED();
+  c->io_cur = nxt;
+  if (c->timing) {
+    phase_mark(c, CHAPSIM_PH_COUNT);
+    if (++c->ev_pending == chapsim_ctx::kEvSub) return flush_phase_events(c);
+  }
+  return CHAPSIM_OK;
+}
 }  // namespace chapsim

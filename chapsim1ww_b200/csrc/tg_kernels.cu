@@ -1595,7 +1595,9 @@ template <typename T> struct Prec {
 static int make_rhs_maps(chapsim_ctx *c) {
   TGDev &d = c->d;
   c->use_tma_rhs = false;
-  if (d.nx < RT_BXW || d.ny < 8) return CHAPSIM_OK;  // small grids use k_rhs
+  // small grids use k_rhs; the coupled IO section (fields offset by its ghost
+  // column) never runs the TG momentum RHS
+  if (d.nx < RT_BXW || d.ny < 8 || d.xnp) return CHAPSIM_OK;
   PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   cudaDriverEntryPointQueryResult q;
   if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void **)&encode, cudaEnableDefault, &q) != cudaSuccess ||
@@ -1712,7 +1714,7 @@ int xnp_pivots(chapsim_ctx *c) {
   return CHAPSIM_OK;
 }
 
-int xnp_pois3d(chapsim_ctx *c) {
+int xnp_pois3d(chapsim_ctx *c, bool mark) {
   TGDev &d = c->d, &s = c->dnp;
   const size_t sm = (size_t)d.nx * sizeof(double);
   const dim3 rows(d.ny, d.nz);
@@ -1721,22 +1723,26 @@ int xnp_pois3d(chapsim_ctx *c) {
   typedef Prec<double> P;
   const int lz = P::fftz_lz(d.nz);
   const dim3 gz((s.lh + lz - 1) / lz, d.ny);
+  if (mark) phase_mark(c, CHAPSIM_PH_FFTZ);
   if (c->fft_big)
     k_fftz<double, true><<<gz, 256, P::fftz_smem(d.nz, lz), c->stream>>>(s, c->fz, lz, -1);
   else
     k_fftz<double, false><<<gz, 256, P::fftz_smem(d.nz, lz), c->stream>>>(s, c->fz, lz, -1);
   LAUNCHED();
+  if (mark) phase_mark(c, CHAPSIM_PH_YSOLVE);
   {
     const int bx = c->ys_bx;
     dim3 grid((s.lh + bx - 1) / bx, d.nz);
     k_ysolve_line<double><<<grid, bx, 0, c->stream>>>(s);
     LAUNCHED();
   }
+  if (mark) phase_mark(c, CHAPSIM_PH_IFFTZ);
   if (c->fft_big)
     k_fftz<double, true><<<gz, 256, P::fftz_smem(d.nz, lz), c->stream>>>(s, c->fz, lz, +1);
   else
     k_fftz<double, false><<<gz, 256, P::fftz_smem(d.nz, lz), c->stream>>>(s, c->fz, lz, +1);
   LAUNCHED();
+  if (mark) phase_mark(c, CHAPSIM_PH_IFFTX);
   k_xnp_bwd<<<rows, 128, sm, c->stream>>>(d, s, c->xnp_b);
   LAUNCHED();
   return CHAPSIM_OK;

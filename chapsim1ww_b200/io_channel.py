@@ -1,10 +1,14 @@
 """Host-side mirror of the reference's IO-section entry points over libchapsim.
 
-An ``IOChannel`` is the inflow/outflow channel section run x-periodic
-(BCX_io = 3), with the explicit viscous scheme (``visc_scheme=0``) or the
-semi-implicit one (``visc_scheme=1``: VISCOUS_PAR_EXPLT_*_io and MOMFA_io,
-src/SOLVERRK3_MOM_IO.f90:73-87) and, when thermal is on, the energy equation
-with table properties and iso-flux walls.  Method names follow
+An ``IOChannel`` is the inflow/outflow channel section, run x-periodic
+(BCX_io = 3, the default) with the explicit viscous scheme
+(``visc_scheme=0``) or the semi-implicit one (``visc_scheme=1``:
+VISCOUS_PAR_EXPLT_*_io and MOMFA_io, src/SOLVERRK3_MOM_IO.f90:73-87), or as
+the coupled section (``bcx`` Dirichlet / Neumann, e.g. ``(2, 1)``: TGFLOWFLG)
+whose inlet a ``TGChannel`` feeds (``set_inlet``) and whose outlet is
+convective; its fields carry the x ghost columns, shape (nz, ny + 2, nx + 2).
+With thermal on, the energy equation runs with table properties and iso-flux
+(or, x-periodic, iso-thermal) walls.  Method names follow
 the Fortran subroutines they replace (CHAPSim1WW, paths relative to the
 project root):
 
@@ -20,6 +24,8 @@ project root):
 ``divgck_io()``            DIVGCK_io, src/DIVGCK.f90:60-190
 ``random_fl_theml_fld_io`` RANDOM_FL_THEML_FLD_io + CALC_INITIALIZATION_io,
                            src/INITIAL_FL_THEML_FLD_io.f90:2-172
+``step_coupled(tg, n)``    SOLVE's substep loop over both sections,
+                           src/SOLVE.f90:119-134
 =========================  ==================================================
 
 Every compute call goes to libchapsim.so; there is no CPU fallback.
@@ -74,12 +80,19 @@ class IOChannel(TGChannel):
             raise ChapsimError(rc, "chapsim_create_io failed")
         self.h = h
         self.nx, self.ny, self.nz = nx, ny, nz
+        # x extent of the fields: the coupled section adds the ghost columns IC = 0, NCL1_io + 1
+        self.sx = nx if tuple(bcx) == (3, 3) else nx + 2
         self.n = self.lib.chapsim_field_len(self.h)
+        self._inlet = None
         if thermal:
             if table is None:
                 from .props import synthetic_table
                 table = synthetic_table()
             self.set_table(table, shortcuts)
+
+    @property
+    def shape(self):
+        return (self.nz, self.ny + 2, self.sx)
 
     def set_table(self, table, shortcuts=0):
         """Columns H, T, D, M, K (extra columns ignored)."""
@@ -110,6 +123,18 @@ class IOChannel(TGChannel):
     def step(self, nsteps=1):
         """NS = 1, 2, 3 (energy then momentum) for each of nsteps steps (graph-replayed)."""
         self._chk(self.lib.chapsim_step_io(self.h, nsteps))
+
+    # ---- the coupled section (non-periodic bcx)
+    def set_inlet(self, tg):
+        """The TG section whose fields BC_TINLET_FLOW reads (same device, ny,
+        nz); None detaches.  Set it before the initial field."""
+        self._chk(self.lib.chapsim_io_set_inlet(self.h, tg.h if tg is not None else None))
+        self._inlet = tg
+
+    def step_coupled(self, tg, nsteps=1):
+        """nsteps steps of the TG section and this one in SOLVE's order: per
+        substep SOLVERRK3_MOM_tg, then SOLVERRK3_ENG_IO and SOLVERRK3_MOM_IO."""
+        self._chk(self.lib.chapsim_step_coupled(tg.h, self.h, nsteps))
 
     def divg_io(self, ns):
         self._chk(self.lib.chapsim_divg(self.h, _lib.IIO, ns))

@@ -420,12 +420,19 @@ typedef struct chapsim_io_config {
                           WALL_ISOTHERMAL_GIVEN, src/Flow_State.f90:603-645);
                           a clear bit keeps the iso-flux wall (BC_WALL_ISOFLUX)  */
   int32_t bcx_in;      /* BCX_io(1), BCX_io(2) (src/READINI.f90:117-171): 1 Dirichlet, */
-  int32_t bcx_out;     /* 2 Neumann, 3 periodic (both 3, the default).  With
-                          Dirichlet / Neumann ends only chapsim_pois3d runs
-                          (FISHPACK_POIS3D_SIMPLE with the SINT / SINQ / COST /
-                          COSQ x transforms, FP64); the other entry points
-                          return CHAPSIM_ERR_UNSUPPORTED, the non-periodic IO
-                          step (x ghost columns) being unbuilt              */
+  int32_t bcx_out;     /* 2 Neumann, 3 periodic (both 3, the default).  Dirichlet /
+                          Neumann ends make the section the coupled inflow /
+                          outflow one (TGFLOWFLG, src/READINI.f90:127-131; the
+                          reference's example is 2, 1): its fields carry the x
+                          ghost columns IC = 0 and NCL1_io + 1, so every field
+                          is (nz, ny + 2, nx + 2) (chapsim_field_len), the
+                          Poisson solve takes FISHPACK's SINT / SINQ / COST /
+                          COSQ x transform, a TG context feeds the inlet
+                          (chapsim_io_set_inlet) and the outlet is convective.
+                          FP64, explicit viscous terms, iso-flux walls, table
+                          properties; statistics, instantaneous-field files and
+                          the stand-alone boundary and property entry points
+                          are for x-periodic sections                        */
 } chapsim_io_config;
 
 /* Defaults: thermal on, Pr = 0.71, qw = 1 on both walls (iso-flux), no
@@ -495,8 +502,33 @@ int chapsim_rk3_eng_io(chapsim_ctx *ctx, int ns);
  * (src/SOLVE.f90:121-132): DENSITY_TIME_DERIVATION, DENSITY_Staggered,
  * MU_Staggered (formed on the fly) and VELOCITY_CALC_io. */
 int chapsim_rk3_mom_io(chapsim_ctx *ctx, int ns);
-/* nsteps full steps: for NS = 1, 2, 3, eng (thermal) then mom. */
+/* nsteps full steps: for NS = 1, 2, 3, eng (thermal) then mom.  A coupled
+ * section reads its TG source's fields as they stand (a frozen inflow). */
 int chapsim_step_io(chapsim_ctx *ctx, int nsteps);
+
+/* The coupled inflow / outflow section (non-periodic bcx_in / bcx_out).
+ * chapsim_io_set_inlet names the TG context (same device, ny, nz) whose
+ * fields BC_TINLET_FLOW reads in the section's momentum substeps; from then
+ * on the section's kernels run in the TG context's stream order.  tg = NULL
+ * detaches (so does destroying either context).  Set it before
+ * chapsim_init_random, whose NS = 0 projection applies the inlet.  In a
+ * coupled substep (SOLVERRK3_MOM_IO / SOLVERRK3_ENG_IO with TGFLOWFLG,
+ * src/SOLVERRK3_MOM_IO.f90:15-168, src/SOLVERRK3_ENG_IO.f90:57-64):
+ * BC_TINLET_FLOW and BC_COUTLET_MOM_RK3 with CHK_MassConsv_io on the ghost
+ * columns, the x-momentum from the second face (NXI = 2) with no DPGRNS
+ * forcing, DIVG_io and FISHPACK_POIS3D_SIMPLE on the IO arrays (the
+ * reference's coupled branch passes the TG arrays, :116-121; the IO-only
+ * branch's are used here), MASSFLUX_UPDATE_IO up to the outlet face
+ * (src/VELO_CORRECTION.f90:124-139), BC_TINLET_THERML and
+ * BC_COUTLET_ENEG_RK3.  The inlet face keeps its value, so div G is not
+ * projected out of the first column (the cosine basis of the Neumann inlet
+ * is even about that column's face); the other columns are divergence-free
+ * to round-off. */
+int chapsim_io_set_inlet(chapsim_ctx *io, chapsim_ctx *tg);
+/* nsteps steps of both sections in SOLVE's order (src/SOLVE.f90:119-134):
+ * for NS = 1, 2, 3, SOLVERRK3_MOM_tg(NS), then SOLVERRK3_ENG_IO(NS) and
+ * SOLVERRK3_MOM_IO(NS); one captured graph per step. */
+int chapsim_step_coupled(chapsim_ctx *tg, chapsim_ctx *io, int nsteps);
 
 
 /* ======================================================================

@@ -113,7 +113,7 @@ void oracle_io_destroy(oracle_io *o);
 int oracle_io_set_table(oracle_io *o, const double *H, const double *T, const double *D, const double *M,
                         const double *K, int n, int shortcuts);
 double oracle_io_rhohmax(const oracle_io *o);
-void oracle_io_init_random(oracle_io *o, uint64_t seed, double amp);
+int oracle_io_init_random(oracle_io *o, uint64_t seed, double amp); /* -1: coupled without an inlet source */
 int oracle_io_eng(oracle_io *o, int ns);      /* SOLVERRK3_ENG_IO(ns) */
 int oracle_io_mom(oracle_io *o, int ns);      /* ns >= 1: DENSITY_TIME_DERIVATION, DENSITY_/MU_Staggered,
                                                  VELOCITY_CALC_io, then SOLVERRK3_MOM_IO(ns); ns = 0: MOM only */
@@ -167,8 +167,16 @@ int oracle_io_set_plane(oracle_io *o, int which, const double *in);
 /* U_OUTLET (momentum), CHK_Mass_CONSV0_SCALING, CHK_MASS_CONSV0, inflow,
  * outflow, mass rate, U_OUTLET (energy) */
 void oracle_io_bc_scalars(const oracle_io *o, double *out);
-/* x boundary codes of the IO Poisson solve (BCX_io) and the solve alone */
+/* x boundary codes of the IO Poisson solve (BCX_io: 1 Dirichlet, 2 Neumann, 3
+ * periodic) and the solve alone.  Non-periodic codes make the section the
+ * coupled inflow / outflow one (TGFLOWFLG): the arrays are re-created with the
+ * x ghost columns i = 0 and nx + 1, (nz, ny + 2, nx + 2), so set them before
+ * the initial field. */
 int oracle_io_set_bcx(oracle_io *o, int in, int out);
+/* Coupled section (non-periodic BCX_io, TGFLOWFLG): the TG arrays (nz, ny + 2,
+ * nxt) that BC_TINLET_FLOW reads in the following substeps; kept by pointer. */
+int oracle_io_set_inlet(oracle_io *o, int nxt, const double *tu, const double *tv, const double *tw,
+                        const double *tp);
 void oracle_io_pois3d(oracle_io *o);
 /* iso-thermal walls (bit 0 bottom, bit 1 top; io_oracle.cpp) */
 int oracle_io_set_walls(oracle_io *o, int bits);

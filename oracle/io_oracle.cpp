@@ -162,13 +162,27 @@ struct oracle_io {
   std::vector<double> bcp[ORC_P_COUNT];
   double bcs[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 
-  int64_t len() const { return (int64_t)nx * (ny + 2) * nz; }
+  // TGFLOWFLG (a TG section feeds the inlet; src/READINI.f90:127-131: any
+  // non-periodic BCX_io): the arrays carry the x ghost columns i = 0 and
+  // NCL1_io + 1 (NCL1S:NCL1E, src/MEMALLOCT.f90:154-168) and the x neighbours
+  // do not wrap (IPV_io / IMV_io, src/INDEXSET.f90:25-32)
+  int coupled = 0;
+  int sx = 0;  // x extent of the arrays: nx, or nx + 2 with the ghost columns
+  // TG arrays (nz, ny + 2, tg_nx) that feed BC_TINLET_FLOW during a coupled substep
+  int tg_nx = 0;
+  const double *tg_u = nullptr, *tg_v = nullptr, *tg_w = nullptr, *tg_p = nullptr;
+
+  int64_t len() const { return (int64_t)sx * (ny + 2) * nz; }
   inline int64_t pj(int j, int k) const { return (int64_t)j + (int64_t)(ny + 2) * (k - 1); }
   inline int64_t id(int i, int j, int k) const {
-    return (int64_t)(i - 1) + (int64_t)nx * ((int64_t)j + (int64_t)(ny + 2) * (k - 1));
+    return (int64_t)(i - 1 + coupled) + (int64_t)sx * ((int64_t)j + (int64_t)(ny + 2) * (k - 1));
   }
-  inline int ip(int i) const { return i == nx ? 1 : i + 1; }
-  inline int im(int i) const { return i == 1 ? nx : i - 1; }
+  inline int ip(int i) const { return coupled ? i + 1 : (i == nx ? 1 : i + 1); }
+  inline int im(int i) const { return coupled ? i - 1 : (i == 1 ? nx : i - 1); }
+  // first x face the x-momentum equation advances (NXI of CONVECTION_X_io,
+  // VISCOUS_ALL_EXPLT_X_io, RHS_MOM_EXPLICIT_io, MASSFLUX_CALC_IO): the
+  // coupled inlet face keeps the value BC_TINLET_FLOW gives it
+  inline int nxi() const { return coupled ? 2 : 1; }
   inline int kp(int k) const { return k == nz ? 1 : k + 1; }
   inline int km(int k) const { return k == 1 ? nz : k - 1; }
 };
@@ -428,8 +442,8 @@ void convection(oracle_io *o) {
       const int jp = j + 1, jm = j - 1, kpp = o->kp(k), kmm = o->km(k);
       for (int i = 1; i <= nx; ++i) {
         const int ipp = o->ip(i), imm = o->im(i);
-        // CONVECTION_X_io (src/CONVECTION_X.f90:98-140)
-        {
+        // CONVECTION_X_io (src/CONVECTION_X.f90:98-140), IC >= NXI
+        if (i >= o->nxi()) {
           const double coe1 = o->dxi * XND2CL * XND2CL, coe3 = o->dzi * XND2CL * ZND2CL;
           const double coe2 = o->dyfi[j] * XND2CL, coe32 = coe3;
           double h11f = (FC(g, 1, ipp, j, k) + FC(g, 1, i, j, k)) * (FC(q, 1, ipp, j, k) + FC(q, 1, i, j, k));
@@ -510,8 +524,8 @@ void viscous(oracle_io *o) {
       const int jp = j + 1, jm = j - 1, kpp = o->kp(k), kmm = o->km(k);
       for (int i = 1; i <= nx; ++i) {
         const int ipp = o->ip(i), imm = o->im(i);
-        // X (src/VISCOUS_X_EXPLICIT_io.f90:38-104)
-        {
+        // X (src/VISCOUS_X_EXPLICIT_io.f90:38-104), IC >= NXI
+        if (i >= o->nxi()) {
           const double coe1 = 2.0 * o->dxi * cv, coe3 = o->dzi * cv, coe2 = o->dyfi[j] * cv, coe32 = coe3;
           double dudx = (FC(q, 1, ipp, j, k) - FC(q, 1, i, j, k)) * o->dxi;
           double tau11f = muc(o, i, j, k) * (dudx - F(divu, i, j, k));
@@ -610,10 +624,11 @@ void rhs_mom(oracle_io *o, int ns, int idr, std::vector<double> &texplt) {
   const bool imp = o->implicit != 0;
   std::vector<double> &tmp = imp ? o->rhsio[idr] : texplt;
   const double coe2 = alp * dt;
+  const int nxi = idr == 1 ? o->nxi() : 1;
 #pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
   for (int k = 1; k <= nz; ++k)
     for (int j = nyi; j <= ny; ++j)
-      for (int i = 1; i <= nx; ++i) {
+      for (int i = nxi; i <= nx; ++i) {
         const int64_t c = o->id(i, j, k);
         const double rhsc = texplt[c], rhsl = o->explt0[idr][c];
         double r = (gam * rhsc + roh * rhsl) * dt;
@@ -630,7 +645,7 @@ void rhs_mom(oracle_io *o, int ns, int idr, std::vector<double> &texplt) {
         if (o->gravdir == idr) r += o->rhostg[idr][c] * (alp * dt * o->f_a);
         tmp[c] = r;
       }
-  if (idr == 1) {  // NFLOW = 1, no TG section
+  if (idr == 1 && !o->coupled) {  // NFLOW = 1 without a TG section (:218)
     double dpgrns = 0.0;
     if (o->flowdrvtp == 1) {
       double s = 0.0;
@@ -1227,9 +1242,69 @@ void momfa(oracle_io *o, int ns, int idr) {
       for (int i = 1; i <= nx; ++i) FC(g, idr, i, j, k) = rhs[o->id(i, j, k)] + FC(g, idr, i, j, k);
 }
 
+// ------------------------------------------ coupled section: ghost columns
+// The boundary operators (oracle_io_bc_*) work on (nz, ny + 2) planes; a
+// coupled substep copies the ghost columns they read into the planes and
+// writes their results back, so the columns hold the state.
+void column_to_plane(oracle_io *o, const std::vector<double> &f, int i, int q) {
+  for (int k = 1; k <= o->nz; ++k)
+    for (int j = 0; j <= o->ny + 1; ++j) o->bcp[q][o->pj(j, k)] = f[o->id(i, j, k)];
+}
+void plane_to_column(oracle_io *o, std::vector<double> &f, int i, int q) {
+  for (int k = 1; k <= o->nz; ++k)
+    for (int j = 0; j <= o->ny + 1; ++j) f[o->id(i, j, k)] = o->bcp[q][o->pj(j, k)];
+}
+
+// Coupled momentum boundaries at the start of SOLVERRK3_MOM_IO (:19-24):
+// BC_TINLET_FLOW from the TG arrays (ghost column 0 and the first face's u,
+// G), then BC_COUTLET_MOM_RK3 on the outlet ghost column NCL1_io + 1.
+void coupled_mom_bc(oracle_io *o, int ns) {
+  const int nx = o->nx;
+  oracle_io_bc_inlet(o, o->tg_nx, o->tg_u, o->tg_v, o->tg_w, o->tg_p);
+  for (int c = 1; c <= 3; ++c) {
+    plane_to_column(o, o->q[c], 0, ORC_P_IN_U + c - 1);
+    plane_to_column(o, o->g[c], 0, ORC_P_IN_GX + c - 1);
+  }
+  plane_to_column(o, o->pr, 0, ORC_P_IN_P);
+  plane_to_column(o, o->dd, 0, ORC_P_IN_RHO);
+  for (int c = 1; c <= 3; ++c) {
+    column_to_plane(o, o->q[c], nx + 1, ORC_P_OUT_U + c - 1);
+    column_to_plane(o, o->g[c], nx + 1, ORC_P_OUT_GX + c - 1);
+  }
+  column_to_plane(o, o->dd, nx + 1, ORC_P_OUT_RHO);
+  oracle_io_bc_outlet_mom(o, ns);
+  for (int c = 1; c <= 3; ++c) {
+    plane_to_column(o, o->q[c], nx + 1, ORC_P_OUT_U + c - 1);
+    plane_to_column(o, o->g[c], nx + 1, ORC_P_OUT_GX + c - 1);
+  }
+}
+
+// Coupled energy boundaries of SOLVERRK3_ENG_IO (:61-64): BC_TINLET_THERML
+// (the reference state on ghost column 0, rows 0..ny+1) and
+// BC_COUTLET_ENEG_RK3 on the outlet ghost column.
+void coupled_eng_bc(oracle_io *o, int ns) {
+  const int nx = o->nx, ny = o->ny, nz = o->nz;
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 0; j <= ny + 1; ++j) {
+      F(tt, 0, j, k) = 1.0;
+      F(kk, 0, j, k) = 1.0;
+      F(dd, 0, j, k) = 1.0;
+      F(mu, 0, j, k) = 1.0;
+      F(rhoh, 0, j, k) = 0.0;
+      F(hh, 0, j, k) = 0.0;
+    }
+  column_to_plane(o, o->q[1], nx + 1, ORC_P_OUT_U);
+  std::vector<double> *fs[6] = {&o->dd, &o->rhoh, &o->hh, &o->tt, &o->mu, &o->kk};
+  const int qs[6] = {ORC_P_OUT_RHO, ORC_P_OUT_RHOH, ORC_P_OUT_H, ORC_P_OUT_T, ORC_P_OUT_MU, ORC_P_OUT_K};
+  for (int a = 0; a < 6; ++a) column_to_plane(o, *fs[a], nx + 1, qs[a]);
+  oracle_io_bc_outlet_eng(o, ns);
+  for (int a = 0; a < 6; ++a) plane_to_column(o, *fs[a], nx + 1, qs[a]);
+}
+
 void mom_io(oracle_io *o, int ns) {
   const int nx = o->nx, ny = o->ny, nz = o->nz;
   for (int c = 1; c <= 3; ++c) o->g0[c] = o->g[c];  // :15
+  if (o->coupled) coupled_mom_bc(o, ns);
   convection(o);
   if (o->implicit) {
     // visthemflg = 1 (:73-87): per component the split viscous terms, the
@@ -1254,7 +1329,7 @@ void mom_io(oracle_io *o, int ns) {
     for (int k = 1; k <= nz; ++k)
       for (int j = 1; j <= ny; ++j)
         for (int i = 1; i <= nx; ++i) {
-          FC(g, 1, i, j, k) += F(qtmp, i, j, k);
+          if (i >= o->nxi()) FC(g, 1, i, j, k) += F(qtmp, i, j, k);
           FC(g, 3, i, j, k) += F(rhsz, i, j, k);
           if (j >= 2) FC(g, 2, i, j, k) += F(dphtmp, i, j, k);
         }
@@ -1285,13 +1360,17 @@ void mom_io(oracle_io *o, int ns) {
           F(pr, i, j, k) += F(dph, i, j, k);
       }
   bc_wall_copy(o, o->pr);
-  // MASSFLUX_UPDATE_IO (src/VELO_CORRECTION.f90:107-185)
+  // MASSFLUX_UPDATE_IO (src/VELO_CORRECTION.f90:107-185); coupled: the x
+  // flux from NXI = 2 to NXE = NCL1_io + 1, the outlet face against the
+  // ghost DPH_io(NCL1_io + 1), which no routine writes (zero)
   const double cx = o->dt * o->talp[ns] * o->dxi, cz = o->dt * o->talp[ns] * o->dzi;
+  const int nxe = o->coupled ? nx + 1 : nx;
 #pragma omp parallel for collapse(2) schedule(static) num_threads(nthreads())
   for (int k = 1; k <= nz; ++k)
     for (int j = 1; j <= ny; ++j)
-      for (int i = 1; i <= nx; ++i) {
-        FC(g, 1, i, j, k) -= (F(dph, i, j, k) - F(dph, o->im(i), j, k)) * cx;
+      for (int i = 1; i <= nxe; ++i) {
+        if (i >= o->nxi()) FC(g, 1, i, j, k) -= (F(dph, i, j, k) - F(dph, o->im(i), j, k)) * cx;
+        if (i > nx) continue;
         FC(g, 3, i, j, k) -= (F(dph, i, j, k) - F(dph, i, j, o->km(k))) * cz;
         if (j >= 2) FC(g, 2, i, j, k) -= (F(dph, i, j, k) - F(dph, i, j - 1, k)) * (o->dt * o->talp[ns] * o->dyci[j]);
       }
@@ -1343,6 +1422,7 @@ void eng_io(oracle_io *o, int ns) {
         o->dd[c] = D;
       }
   o->bad += bad;
+  if (o->coupled) coupled_eng_bc(o, ns);
   bc_wall_thermal(o);
 }
 
@@ -1430,6 +1510,26 @@ void outlet_plane_walls(oracle_io *o) {
     }
 }
 
+// The arrays of the current layout, as MEMALLOCT.f90 initialises them
+// (src/MEMALLOCT.f90:154-215): zero, properties and the staggered density /
+// viscosity 1 (ghost columns keep those values where no routine writes them).
+void alloc_fields(oracle_io *o) {
+  const int64_t n = o->len();
+  for (int c = 1; c <= 3; ++c) {
+    o->q[c].assign(n, 0.0); o->g[c].assign(n, 0.0); o->g0[c].assign(n, 0.0); o->explt0[c].assign(n, 0.0);
+    o->mustg[c].assign(n, 1.0); o->rhostg[c].assign(n, 1.0);
+  }
+  for (auto *v : {&o->pr, &o->dph, &o->rhsllphi, &o->qtmp, &o->dphtmp, &o->rhsz, &o->divu, &o->drho, &o->rhoh,
+                  &o->hh, &o->rhse, &o->rhse0})
+    v->assign(n, 0.0);
+  for (auto *v : {&o->tt, &o->dd, &o->dd0, &o->mu, &o->mu0, &o->kk}) v->assign(n, 1.0);
+  for (int c = 1; c <= 3; ++c) {
+    o->rhsio[c].assign(n, 0.0); o->adv[c].assign(n, 0.0); o->drhoi[c].assign(n, 0.0);
+  }
+  for (int q = 0; q < ORC_P_COUNT; ++q) o->bcp[q].assign((size_t)(o->ny + 2) * o->nz, 0.0);
+  o->bcp[ORC_P_IN_RHO].assign((size_t)(o->ny + 2) * o->nz, 1.0);
+}
+
 }  // namespace
 
 extern "C" {
@@ -1464,21 +1564,9 @@ oracle_io *oracle_io_create(int nx, int ny, int nz, double lx, double lz, double
   o->tgam[0] = 1.0; o->tgam[1] = 8.0 / 15.0; o->tgam[2] = 5.0 / 12.0; o->tgam[3] = 3.0 / 4.0;
   o->troh[0] = 0.0; o->troh[1] = 0.0; o->troh[2] = -17.0 / 60.0; o->troh[3] = -5.0 / 12.0;
   for (int n = 0; n < 4; ++n) o->talp[n] = o->tgam[n] + o->troh[n];
-  const int64_t n = o->len();
-  for (int c = 1; c <= 3; ++c) {
-    o->q[c].assign(n, 0.0); o->g[c].assign(n, 0.0); o->g0[c].assign(n, 0.0); o->explt0[c].assign(n, 0.0);
-    o->mustg[c].assign(n, 1.0); o->rhostg[c].assign(n, 1.0);
-  }
-  for (auto *v : {&o->pr, &o->dph, &o->rhsllphi, &o->qtmp, &o->dphtmp, &o->rhsz, &o->divu, &o->drho, &o->rhoh,
-                  &o->hh, &o->rhse, &o->rhse0})
-    v->assign(n, 0.0);
-  for (auto *v : {&o->tt, &o->dd, &o->dd0, &o->mu, &o->mu0, &o->kk}) v->assign(n, 1.0);
-  for (int c = 1; c <= 3; ++c) {
-    o->rhsio[c].assign(n, 0.0); o->adv[c].assign(n, 0.0); o->drhoi[c].assign(n, 0.0);
-  }
+  o->sx = nx;
+  alloc_fields(o);
   vis_ycoef(o);
-  for (int q = 0; q < ORC_P_COUNT; ++q) o->bcp[q].assign((size_t)(ny + 2) * nz, 0.0);
-  o->bcp[ORC_P_IN_RHO].assign((size_t)(ny + 2) * nz, 1.0);
   o->dftx = oracle_dft_create(nx);
   o->dftz = oracle_dft_create(nz);
   return o;
@@ -1528,6 +1616,15 @@ int oracle_io_set_bcx(oracle_io *o, int in, int out) {
   if (in == 2 && out == 1) lp = 5;
   if (lp < 0 || o->nx < 4) return -1;
   o->lpx = lp;
+  // a non-periodic x is the coupled inflow / outflow section (TGFLOWFLG):
+  // the arrays are re-created with the x ghost columns, so this comes before
+  // the initial field
+  const int coupled = lp != 1 ? 1 : 0;
+  if (coupled != o->coupled) {
+    o->coupled = coupled;
+    o->sx = coupled ? o->nx + 2 : o->nx;
+    alloc_fields(o);
+  }
   return 0;
 }
 
@@ -1553,8 +1650,9 @@ int oracle_io_set_walls(oracle_io *o, int bits) {
   return 0;
 }
 
-void oracle_io_init_random(oracle_io *o, uint64_t seed, double amp) {
+int oracle_io_init_random(oracle_io *o, uint64_t seed, double amp) {
   const int nx = o->nx, ny = o->ny, nz = o->nz;
+  if (o->coupled && !o->tg_u) return -1;
   o->bad = 0;
   // thermal field (INIFIELD_THERMAL_io, src/INITIAL_FL_THEML_FLD_io.f90:352-381)
   std::fill(o->rhoh.begin(), o->rhoh.end(), 0.0);
@@ -1614,6 +1712,18 @@ void oracle_io_init_random(oracle_io *o, uint64_t seed, double amp) {
     for (auto &x : o->q[c]) x /= gm;
   velo2massflux(o);
   bc_wall_vec(o, o->q);
+  if (o->coupled) {
+    for (int q = ORC_P_CONV0_X; q <= ORC_P_CONV0_ENG; ++q) std::fill(o->bcp[q].begin(), o->bcp[q].end(), 0.0);
+    // outlet ghost column NCL1_io + 1: a copy of the last interior column
+    // (the seeded recipe covers the interior; the inlet column comes from
+    // the TG section in the projection's BC_TINLET_FLOW)
+    for (int c = 1; c <= 3; ++c)
+      for (int k = 1; k <= nz; ++k)
+        for (int j = 0; j <= ny + 1; ++j) {
+          FC(q, c, nx + 1, j, k) = FC(q, c, nx, j, k);
+          FC(g, c, nx + 1, j, k) = FC(g, c, nx, j, k);
+        }
+  }
   std::fill(o->pr.begin(), o->pr.end(), 0.0);
   std::fill(o->dph.begin(), o->dph.end(), 0.0);
   std::fill(o->drho.begin(), o->drho.end(), 0.0);
@@ -1626,6 +1736,15 @@ void oracle_io_init_random(oracle_io *o, uint64_t seed, double amp) {
     mu_staggered(o);
   }
   mom_io(o, 0);
+  return 0;
+}
+
+int oracle_io_set_inlet(oracle_io *o, int nxt, const double *tu, const double *tv, const double *tw,
+                        const double *tp) {
+  if (!o->coupled || nxt < 1 || !tu || !tv || !tw || !tp) return -1;
+  o->tg_nx = nxt;
+  o->tg_u = tu; o->tg_v = tv; o->tg_w = tw; o->tg_p = tp;
+  return 0;
 }
 
 int oracle_io_eng(oracle_io *o, int ns) {
@@ -1635,7 +1754,9 @@ int oracle_io_eng(oracle_io *o, int ns) {
 }
 
 int oracle_io_mom(oracle_io *o, int ns) {
-  if (ns < 0 || ns > 3) return -1;
+  // the coupled section's semi-implicit boundary terms (BC_CBC_TDMA) are
+  // unfinished in the reference (src/SOLVERRK3_MOM_IO.f90:22)
+  if (ns < 0 || ns > 3 || (o->coupled && (!o->tg_u || o->implicit))) return -1;
   if (ns >= 1) {
     if (o->thermal) {
       density_time_derivation(o, ns);
@@ -1650,7 +1771,7 @@ int oracle_io_mom(oracle_io *o, int ns) {
 }
 
 int oracle_io_substep(oracle_io *o, int ns) {
-  if (ns < 1 || ns > 3) return -1;
+  if (ns < 1 || ns > 3 || (o->coupled && !o->tg_u)) return -1;
   if (o->thermal) eng_io(o, ns);
   return oracle_io_mom(o, ns);
 }

@@ -51,6 +51,9 @@ def load(build=True):
     L.oracle_io_destroy.argtypes = [P]
     L.oracle_io_set_table.argtypes = [P, P, P, P, P, P, I, I]
     L.oracle_io_init_random.argtypes = [P, ctypes.c_uint64, D]
+    L.oracle_io_init_random.restype = I
+    L.oracle_io_set_inlet.argtypes = [P, I, P, P, P, P]
+    L.oracle_io_set_inlet.restype = I
     for f in ("oracle_io_eng", "oracle_io_mom", "oracle_io_substep"):
         getattr(L, f).argtypes = [P, I]
     L.oracle_io_step.argtypes = [P]
@@ -212,6 +215,7 @@ class OracleIO:
         if not self.h:
             raise ValueError("oracle_io_create rejected the configuration")
         self.nx, self.ny, self.nz = nx, ny, nz
+        self.sx = nx  # x extent of the arrays (nx + 2 with the coupled section's ghost columns)
         assert self.L.oracle_io_set_scheme(self.h, int(visc_scheme)) == 0
         if thermal:
             if table is None:
@@ -229,7 +233,7 @@ class OracleIO:
 
     @property
     def shape(self):
-        return (self.nz, self.ny + 2, self.nx)
+        return (self.nz, self.ny + 2, self.sx)
 
     def get(self, name):
         a = np.empty(self.shape)
@@ -238,7 +242,7 @@ class OracleIO:
 
     def set(self, name, arr):
         a = np.ascontiguousarray(arr, dtype=np.float64)
-        assert a.size == self.nx * (self.ny + 2) * self.nz
+        assert a.size == self.sx * (self.ny + 2) * self.nz
         assert self.L.oracle_io_set_field(self.h, IO_FIELDS[name], a.ctypes.data) == 0
 
     # ---- coupled inflow/outflow boundary planes
@@ -269,7 +273,7 @@ class OracleIO:
         return dict(zip(IO_BC_SCALARS, a.tolist()))
 
     def init_random(self, seed, amp=0.1):
-        self.L.oracle_io_init_random(self.h, seed, amp)
+        assert self.L.oracle_io_init_random(self.h, seed, amp) == 0
 
     def eng(self, ns):
         assert self.L.oracle_io_eng(self.h, ns) == 0
@@ -303,8 +307,19 @@ class OracleIO:
         return self.L.oracle_io_cfl(self.h)
 
     def set_bcx(self, inlet, outlet):
-        """BCX_io of the Poisson solve: 1 Dirichlet, 2 Neumann, 3 periodic."""
+        """BCX_io of the Poisson solve: 1 Dirichlet, 2 Neumann, 3 periodic.
+        Non-periodic codes make this the coupled inflow / outflow section
+        (TGFLOWFLG): arrays with the x ghost columns, (nz, ny + 2, nx + 2);
+        set them before the initial field."""
         assert self.L.oracle_io_set_bcx(self.h, int(inlet), int(outlet)) == 0
+        self.sx = self.nx + 2 if (inlet, outlet) != (3, 3) else self.nx
+
+    def set_inlet(self, tu, tv, tw, tp):
+        """The TG section's u, v, w, p (nz, ny + 2, nx_tg) that BC_TINLET_FLOW
+        reads in the coupled substeps that follow (held until replaced)."""
+        self._inlet = [np.ascontiguousarray(a, dtype=np.float64) for a in (tu, tv, tw, tp)]
+        assert self.L.oracle_io_set_inlet(self.h, self._inlet[0].shape[-1],
+                                          *[a.ctypes.data for a in self._inlet]) == 0
 
     def pois3d(self):
         """FISHPACK_POIS3D_SIMPLE alone: phi from rhsphi."""

@@ -253,9 +253,8 @@ def test_io_poisson_nonperiodic_x_parity(bcx):
     """FISHPACK_POIS3D_SIMPLE with Dirichlet / Neumann x ends (BCX_io 1 / 2:
     FISHPACK's SINT, SINQ, COST, COSQ x transforms): chapsim_pois3d against
     the oracle on the same random right-hand side, FP64 within 1e-10 over the
-    whole field (interior and the copied ghost rows), two grids; the
-    other entry points refuse such a context (its IO step, with x ghost
-    columns, is not built)."""
+    whole field (interior, the copied ghost rows, the untouched ghost
+    columns), two grids."""
     _need_gpu()
     from chapsim1ww_b200 import ChapsimError, IOChannel
     from oracle.pyoracle import OracleIO
@@ -264,7 +263,7 @@ def test_io_poisson_nonperiodic_x_parity(bcx):
         g = IOChannel(*dims, thermal=0, bcx=bcx)
         o = OracleIO(*dims, thermal=0)
         o.set_bcx(*bcx)
-        rhs = rng.standard_normal((dims[2], dims[1] + 2, dims[0]))
+        rhs = rng.standard_normal((dims[2], dims[1] + 2, dims[0] + 2))  # with the x ghost columns
         g.set_field("rhsphi", rhs)
         o.set("rhsphi", rhs)
         g.fishpack_pois3d()
@@ -272,7 +271,7 @@ def test_io_poisson_nonperiodic_x_parity(bcx):
         e = relerr(g.get_field("phi"), o.get("phi"))
         assert e <= 1e-10, (dims, e)
         with pytest.raises(ChapsimError):
-            g.step(1)
+            g.step(1)  # a coupled section steps only with its TG inlet source
         # a DT change rebuilds the coefficient tables the solve reads: same result
         g.set_dt(2e-3)
         g.fishpack_pois3d()

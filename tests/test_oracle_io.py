@@ -223,15 +223,19 @@ def test_io_poisson_nonperiodic_x_inverts_the_operator(bcx):
     transform's basis (Dirichlet: zero one node beyond; Neumann: even about
     the end node), periodic z and the y-operator of TDMA_PHI_COEF, to 1e-10 of
     the right-hand side.  Neumann at both ends is singular in its mean mode;
-    TRID0 pins that mode at the last row, whose equation is then left out."""
+    TRID0 pins that mode at the last row, whose equation is then left out.
+    The section's fields carry the x ghost columns (the coupled layout);
+    the solve reads and writes the interior columns."""
     nx, ny, nz, lx, lz = 20, 16, 12, 8 * math.pi, 4 * math.pi / 3
     o = OracleIO(nx, ny, nz, lx=lx, lz=lz, thermal=0)
     o.set_bcx(*bcx)
     rng = np.random.default_rng(5)
-    rhs = rng.standard_normal((nz, ny + 2, nx))
+    rhs = rng.standard_normal((nz, ny + 2, nx + 2))
     o.set("rhsphi", rhs)
     o.pois3d()
     phi = o.get("phi")
+    assert not phi[..., 0].any() and not phi[..., -1].any()  # ghost columns untouched
+    phi, rhs = phi[..., 1:nx + 1], rhs[..., 1:nx + 1]
     t = OracleTG(nx, ny, nz, lx=lx, lz=lz)
     am, ac, ap = (np.concatenate([[0.0], t.coef(w), [0.0]]) for w in (6, 7, 8))
     dxqi, dzqi = (nx / lx) ** 2, (nz / lz) ** 2
