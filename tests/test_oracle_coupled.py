@@ -28,6 +28,7 @@ def _pair(bcx=(2, 1), thermal=1, nxt=16, nxi=24, ny=16, nz=12, seed=1):
     lz = 4 * math.pi / 3
     t = OracleTG(nxt, ny, nz, lx=4 * math.pi, lz=lz)
     t.init_random(seed, 0.1)
+    t.substep(0)  # CALC_INITIALIZATION_tg
     h = np.linspace(-1.0, 1.0, 4096)
     one = np.ones_like(h)
     o = OracleIO(nxi, ny, nz, lx=8 * math.pi, lz=lz, thermal=thermal, table=[h, h.copy(), one, one, one])
