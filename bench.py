@@ -21,9 +21,9 @@ Synthetic seeded initial fields (no public dataset is involved).  With N > 1
 GPUs every rank advances its own independent copy (replicas, weak scaling,
 no data-path collective); timing is the max over ranks.  Other workloads:
 c2_mixed_learned (the same comparison on the heated 384x192x192 channel),
-c1_tg_io (the TG channel 256x192x256 and the IO section 512x192x256 with
-constant-property passive heat, advanced together; the IO section runs
-x-periodic because the TG -> IO inlet coupling is not built), the TG or IO
+c1_tg_io (the TG channel 256x192x256 feeding the inlet of the IO section
+512x192x256, Lx = 8 pi, with constant-property passive heat and a convective
+outlet: BCX_io = 2, 1, the coupled step of SOLVE's substep loop), the TG or IO
 section alone, the heated IO channel with the semi-implicit viscous scheme,
 the 64-channel batch (split across ranks), the CPU-sized 64^3 TG channel.
 
@@ -72,10 +72,10 @@ WORKLOADS = {
     "c4_mixed_learned": dict(compare=True, base="io_1024x384x512"),
     # the same comparison on the heated 384x192x192 channel
     "c2_mixed_learned": dict(compare=True, base="io_384x192x192"),
-    # the two sections of the coupled TG + IO configuration advanced together
-    # each step (the IO section x-periodic: the TG -> IO inlet coupling is not built)
-    "c1_tg_io": dict(pair=True, tg="tg_256x192x256", io="io_512x192x256"),
-    # IO section of the coupled configuration run x-periodic: constant-property
+    # the coupled TG + IO configuration: the TG section feeds the IO section's
+    # inlet (BCX_io = 2, 1: Neumann inlet, Dirichlet outlet, convective outflow)
+    "c1_tg_io": dict(pair=True, tg="tg_256x192x256", io="io_512x192x256", bcx=(2, 1)),
+    # IO section of the coupled configuration (alone: x-periodic): constant-property
     # passive heat (rho = mu = k = cp = 1, T = h), wall heat flux 1, Pr 0.71
     "io_512x192x256": dict(io=True, nx=512, ny=192, nz=256, lx=8 * math.pi, lz=4 * math.pi / 3, ren=2800.0,
                            dt=1e-3, seed=1, thermal=1, prt=0.71, qw=1.0, table="constant"),
@@ -697,10 +697,51 @@ def synthetic_table_cols(table5):
     return list(table5[:5]) + [full[5]]
 
 
+# Coupled IO section (x ghost columns, the non-periodic Poisson transforms):
+# its phase kernels and algorithmic 8-byte values per cell.  The divergence
+# reads G and DrhoDtP and writes RHSLLPHI, which the forward x transform reads
+# and writes as nx complex modes per row (the real x modes in complex lines);
+# the z transforms and y-lines pass over nx complex values per row.
+IO_KERNEL_COUPLED = dict(IO_KERNEL, mom_rhs="k_io_rhs", fftx="k_np_divg + k_xnp_qfwd", ifftx="k_xnp_qbwd")
+IO_COUPLED_VALUES = dict(IO_VALUES_PER_CELL, fftx=8, fftz=4, ysolve=4, ifftz=4, ifftx=3)
+
+
+def io_phase_bytes_coupled(ph, nx, ny, nz):
+    return IO_COUPLED_VALUES.get(ph, 0) * 8 * nx * ny * nz
+
+
+class CoupledOracle:
+    """The TG oracle feeding the coupled IO oracle in SOLVE's order (per
+    substep: SOLVERRK3_MOM_tg, then the IO section, whose BC_TINLET_FLOW reads
+    the TG fields), on z-slabs of nz planes with the sections' mesh spacing."""
+
+    def __init__(self, wt, wi, bcx, nz):
+        from oracle.pyoracle import OracleIO
+        self.t = make_oracle("tg", wt, nz)
+        self.o = OracleIO(wi["nx"], wi["ny"], nz, lx=wi["lx"], lz=wi["lz"] * nz / wi["nz"], ren=wi["ren"],
+                          dt=wi["dt"], thermal=wi["thermal"], prt=wi["prt"], qw=(wi["qw"], wi["qw"]),
+                          table=io_table(wi["table"]))
+        self.o.set_bcx(*bcx)
+        self._feed()
+        self.o.init_random(wi["seed"], 0.1)
+
+    def _feed(self):
+        self.o.set_inlet(*[self.t.get(f) for f in ("u", "v", "w", "p")])
+
+    def step(self, n=1):
+        for _ in range(n):
+            for ns in (1, 2, 3):
+                self.t.substep(ns)
+                self._feed()
+                self.o.substep(ns)
+
+
 def run_pair(args, wl, ws, rank, local):
-    """TG and IO sections of the coupled configuration, one step of each per
-    step, on their own streams chained by events (they alternate, joined
-    before the end event).  value = (TG cells + IO cells) x steps / time."""
+    """Configuration 1: the TG section feeds the inlet of the IO section
+    (chapsim_io_set_inlet; BCX_io = 2, 1, convective outlet) and both advance
+    by chapsim_step_coupled (SOLVE's substep loop: per substep the TG
+    momentum, the IO energy and the IO momentum; one captured graph per step
+    on the TG's stream).  value = (TG cells + IO cells) x steps / time."""
     import torch
 
     import chapsim1ww_b200 as cs
@@ -719,12 +760,12 @@ def run_pair(args, wl, ws, rank, local):
                    precision=prec, device=local)
     io = IOChannel(wi["nx"], wi["ny"], wi["nz"], lx=wi["lx"], lz=wi["lz"], ren=wi["ren"], dt=wi["dt"],
                    thermal=wi["thermal"], prt=wi["prt"], qw=(wi["qw"], wi["qw"]), table=io_table(wi["table"]),
-                   device=local)
+                   device=local, bcx=wl["bcx"])
+    io.set_inlet(tg)
     tg.random_fl_fld_tg(wt["seed"] + rank, 0.1, project=True)
     io.random_fl_theml_fld_io(wi["seed"] + rank, 0.1)
     ct, ci = wt["nx"] * wt["ny"] * wt["nz"], wi["nx"] * wi["ny"] * wi["nz"]
-    st = torch.cuda.ExternalStream(tg.stream(), device=local)
-    si = torch.cuda.ExternalStream(io.stream(), device=local)
+    st = torch.cuda.ExternalStream(io.stream(), device=local)  # the TG's stream, shared
 
     def barrier():
         if pg is not None:
@@ -738,33 +779,17 @@ def run_pair(args, wl, ws, rank, local):
         return float(t.item())
 
     def timed(fn, steps):
-        e0, ej, e1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(st)
-        si.wait_event(e0)
         fn(steps)
-        ej.record(st)
-        si.wait_event(ej)
-        e1.record(si)
+        e1.record(st)
         e1.synchronize()
         return e0.elapsed_time(e1)
 
     def both(n):
-        # one step of each section per step, on their own streams, chained by
-        # events so that they alternate: measured faster (16.2 against
-        # 16.8-17.7 ms per step at 256x192x256 + 512x192x256) than letting
-        # the two sections' HBM-bound kernels overlap and compete
-        for _ in range(n):
-            tg.step(1)
-            e = torch.cuda.Event()
-            e.record(st)
-            si.wait_event(e)
-            io.step(1)
-            e = torch.cuda.Event()
-            e.record(si)
-            st.wait_event(e)
+        io.step_coupled(tg, n)
 
     both(args.warmup)
-    tg.sync()
     io.sync()
     clocks = ClockSampler(local)
     clocks.start()
@@ -778,6 +803,7 @@ def run_pair(args, wl, ws, rank, local):
     clk = clocks.stop()
     cells = ct + ci
     value = cells * ws * args.steps / (ms / 1000.0)
+    # each section alone (the IO one with its inflow as it stands)
     ms_tg = timed(tg.step, args.steps) / args.steps
     ms_io = timed(io.step, args.steps) / args.steps
 
@@ -803,14 +829,15 @@ def run_pair(args, wl, ws, rank, local):
         kern = PHASE_KERNEL[dom]
         traffic = load_traffic(wl["tg"], kern)
     else:
-        bytes_dom = io_phase_bytes(dom, wi["nx"], wi["ny"], wi["nz"])
-        kern = IO_KERNEL[dom]
-        traffic = load_traffic(wl["io"], kern)
+        bytes_dom = io_phase_bytes_coupled(dom, wi["nx"], wi["ny"], wi["nz"])
+        kern = IO_KERNEL_COUPLED[dom]
+        traffic = load_traffic("c1_io_coupled", kern)
     achieved = bytes_dom / (dom_ms / 1000.0) / 1e9
     step_bytes = 3 * (sum(phase_bytes(p, wt["nx"], wt["ny"], wt["nz"]) for p in per_tg) +
-                      sum(io_phase_bytes(p, wi["nx"], wi["ny"], wi["nz"]) for p in IO_PHASES))
+                      sum(io_phase_bytes_coupled(p, wi["nx"], wi["ny"], wi["nz"]) for p in IO_PHASES))
 
-    # end to end through the C ABI with host buffers (both sections)
+    # end to end through the C ABI with host buffers (both sections): uploads,
+    # one coupled step and downloads, stream-ordered on the shared stream
     tg_names, io_names = ("u", "v", "w", "p"), IO_RESULT_FIELDS
     host_t = {n: torch.empty(tg.shape, dtype=torch.float64, pin_memory=True).numpy() for n in tg_names}
     host_i = {n: torch.empty(io.shape, dtype=torch.float64, pin_memory=True).numpy() for n in io_names}
@@ -822,48 +849,54 @@ def run_pair(args, wl, ws, rank, local):
     torch.cuda.synchronize()
     e2e_steps = max(1, min(args.steps, 10))
 
-    def queue(sec, inputs, names, host):
-        # uploads, one step and downloads, stream-ordered on the section's
-        # own stream, so one section's copies overlap the other's work
-        for n in inputs:
-            sec.set_field_async(n, host[n])
-        sec.step(1)
-        for n in names:
-            sec.get_field_async(n, out=host[n])
-
     def e2e(steps):
         for _ in range(steps):
-            queue(tg, tg_names, tg_names, host_t)
-            queue(io, IO_INPUT_FIELDS, io_names, host_i)
-            _ = tg.divgck_tg() + io.divgck_io()  # each waits for its stream
+            for n in tg_names:
+                tg.set_field_async(n, host_t[n])
+            for n in IO_INPUT_FIELDS:
+                io.set_field_async(n, host_i[n])
+            io.step_coupled(tg, 1)
+            for n in tg_names:
+                tg.get_field_async(n, out=host_t[n])
+            for n in io_names:
+                io.get_field_async(n, out=host_i[n])
+            _ = tg.divgck_tg() + io.divgck_io()
 
     ms_e2e = max_over_ranks(timed(e2e, e2e_steps))
     e2e_value = cells * ws * e2e_steps / (ms_e2e / 1000.0)
     h2d = (len(tg_names) * tg.n + len(IO_INPUT_FIELDS) * io.n) * 8
     nbytes = (len(tg_names) * tg.n + len(io_names) * io.n) * 8
+    bcs = io.bc_scalars()
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
-            v1, t1, cores = cpu_baseline_oracle(wt, args.cpu_steps)
-            v2, t2, _ = cpu_baseline_io(wi, args.cpu_steps)
-            v = (ct + ci) * args.cpu_steps / (t1 + t2)
+            from oracle.pyoracle import get_threads
+            nzc = 32  # a z-slab of both sections with their mesh spacing
+            co = CoupledOracle(wt, wi, wl["bcx"], nzc)
+            t0 = time.perf_counter()
+            co.step(args.cpu_steps)
+            t1 = time.perf_counter() - t0
+            v = (wt["nx"] + wi["nx"]) * wt["ny"] * nzc * args.cpu_steps / t1
+            cores = get_threads()
             cpu = {"value": v, "unit": METRIC, "cores": cores, "kind": "port",
-                   "sample": f"{args.cpu_steps} full RK3 steps of each section after init (TG {t1:.1f} s, IO "
-                             f"{t2:.1f} s), FP64 oracle port, OpenMP {cores} threads"}
+                   "sample": f"{args.cpu_steps} full coupled RK3 steps of {nzc}-plane z-slabs of both sections "
+                             f"(same cell size) after init, {t1:.1f} s, FP64 oracle port, OpenMP {cores} threads"}
         except Exception as ex:
             cpu = {"value": None, "unit": METRIC, "cores": 0, "kind": "port", "sample": f"failed: {ex}"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if prec == cs.FP64 else "f64 state / f32 temporaries (TG)",
-            "data": "synthetic (seeded splitmix64 velocity, NS=0 projection; IO h = 0 with table properties)",
+            "vs_baseline": None, "dtype": "f64" if prec == cs.FP64 else "TG f64 state / f32 temporaries, IO f64",
+            "data": "synthetic (seeded splitmix64 velocity, NS=0 projection; IO h = 0, constant properties)",
             "config": workload_config(args, wl),
-            "arm": {"parallelism": f"replicas x{ws}" if ws > 1 else "single GPU, two streams alternating per step",
+            "arm": {"parallelism": f"replicas x{ws}" if ws > 1 else "single GPU, both sections on one stream",
                     "l2": "working set (>4 GB) larger than the 126 MB L2"},
             "sections_ms_per_step": {"tg": ms_tg, "io": ms_io, "both": ms / args.steps},
             "max_div_u_tg": tg.divgck_tg(), "max_div_g_plus_drho_io": io.divgck_io(),
+            "io_boundary": {"u_outlet": bcs["u_outlet"], "mass_scaling": bcs["scaling"],
+                            "inflow": bcs["inflow"], "outflow": bcs["outflow"]},
             "gpu_launches": launches,
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": nbytes + 16, "steps": e2e_steps,
@@ -881,8 +914,8 @@ def run_pair(args, wl, ws, rank, local):
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
-    tg.close()
     io.close()
+    tg.close()
     if pg is not None:
         pg.destroy_process_group()
     return 0
@@ -906,7 +939,9 @@ def section_specs(wl):
     if wl.get("compare"):
         return [("io", WORKLOADS[wl["base"]])]
     if wl.get("pair"):
-        return [("tg", WORKLOADS[wl["tg"]]), ("io", WORKLOADS[wl["io"]])]
+        # both sections as one coupled object (equal ny, nz): nx counts both
+        wt, wi = WORKLOADS[wl["tg"]], WORKLOADS[wl["io"]]
+        return [("pair", dict(nx=wt["nx"] + wi["nx"], ny=wt["ny"], nz=wt["nz"], tg=wt, io=wi, bcx=wl["bcx"]))]
     if wl.get("batch"):
         from chapsim1ww_b200 import batch64_configs
         return [("tg", dict(c, seed=wl["seed"] + i)) for i, c in enumerate(batch64_configs(seed=wl["seed"]))]
@@ -918,6 +953,8 @@ def make_oracle(kind, spec, nz):
     spacing as the full section: Lz scaled by nz / Nz), initialised as the
     GPU arm is (seeded field, NS=0 projection)."""
     from oracle.pyoracle import OracleIO, OracleTG
+    if kind == "pair":
+        return CoupledOracle(spec["tg"], spec["io"], spec["bcx"], nz)
     lz = spec["lz"] * nz / spec["nz"]
     if kind == "tg":
         o = OracleTG(spec["nx"], spec["ny"], nz, lx=spec["lx"], lz=lz, ren=spec["ren"], dt=spec["dt"])
@@ -1018,7 +1055,8 @@ def workload_config(args, wl):
         return {"workload": args.workload,
                 "tg": {k: wt[k] for k in ("nx", "ny", "nz", "ren", "dt")},
                 "io": {**{k: wi[k] for k in ("nx", "ny", "nz", "ren", "dt", "prt")},
-                       "table": wi["table"], "wall_heat_flux": wi["qw"], "x": "periodic (inlet coupling not built)"},
+                       "table": wi["table"], "wall_heat_flux": wi["qw"],
+                       "x": "inflow from the TG section, convective outflow", "bcx_io": list(wl["bcx"])},
                 "cells": wt["nx"] * wt["ny"] * wt["nz"] + wi["nx"] * wi["ny"] * wi["nz"],
                 "precision": args.precision}
     cfg = {"workload": args.workload, **{k: wl[k] for k in ("nx", "ny", "nz", "ren", "dt")},

@@ -509,6 +509,17 @@ static int xnp_setup(chapsim_ctx *ctx, int lp) {
   ctx->xnp_b = (double *)p;
   CKC(cudaMemcpyAsync(p, bt.data(), (size_t)n * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   if ((rc = chapsim::xnp_pivots(ctx))) return rc;
+  std::vector<double2> qw;
+  if (lp == 3 || lp == 5) {
+    // the quarter-wave pairs through the complex FFT: exp(-i pi m / (2 N))
+    qw.resize(n);
+    for (int m = 0; m < n; ++m) qw[m] = make_double2(cos(M_PI * m / (2.0 * n)), -sin(M_PI * m / (2.0 * n)));
+    if ((rc = dalloc(ctx, &p, (size_t)n * sizeof(double2)))) return rc;
+    ctx->xnp_qw = (double2 *)p;
+    CKC(cudaMemcpyAsync(p, qw.data(), (size_t)n * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+    ctx->xnp_rscal = 1.0 / scalx;
+    if ((rc = chapsim::xnp_q_setup(ctx))) return rc;
+  }
   CKC(cudaStreamSynchronize(ctx->stream));  // the host vectors go out of scope
   ctx->xnp = lp;
   return CHAPSIM_OK;

@@ -182,6 +182,10 @@ struct chapsim_ctx {
   int64_t pair_kernels = 0;                             // kernels of both contexts in one pair step
   chapsim::TGDev dnp{};
   double *xnp_f = nullptr, *xnp_b = nullptr;
+  // LP 3 / 5 (SINQ / COSQ) run through the complex FFT: exp(-i pi m / (2 nx)),
+  // m < nx, and 1 / SCALX of the forward transform
+  double2 *xnp_qw = nullptr;
+  double xnp_rscal = 1.0;
   // CUDA graph of one full step (NS = 1, 2, 3)
   cudaGraphExec_t step_graph = nullptr;
   int64_t kernels_per_step = 0;
@@ -225,6 +229,7 @@ int launch_substep(chapsim_ctx *c, int ns);
 int launch_divg(chapsim_ctx *c, int ns);
 int launch_pois3d(chapsim_ctx *c);
 int xnp_pivots(chapsim_ctx *c);
+int xnp_q_setup(chapsim_ctx *c);  // shared-memory limits of the quarter-wave FFT kernels
 int xnp_pois3d(chapsim_ctx *c, bool mark = false);  // mark: phase timers 5-8 of a substep
 int launch_correction(chapsim_ctx *c, int ns);
 int launch_reduce(chapsim_ctx *c, int what, double *host_out);

@@ -1706,6 +1706,111 @@ __global__ void __launch_bounds__(128) k_xnp_bwd(TGDev d, TGDev s, const double 
   }
 }
 
+
+// The quarter-wave pairs (LP 5: COSQF / COSQB, LP 3: SINQF / SINQB) through
+// the N-point complex FFT of the periodic path (Makhoul's even-odd reordering,
+// IEEE Trans. ASSP 28 (1980) 27-34), two real rows per complex line:
+//   COSQB(X)_k = 4 Re(q_k V_k),  V = FFT(v), v_n = X_{2n}, v_{N-1-n} = X_{2n+1};
+//   COSQF(x)_{2n} = w_n, COSQF(x)_{2n+1} = w_{N-1-n},
+//     w = sum_m conj(q_m) (x_m - i x_{N-m}) e^{+2 pi i m n / N}  (x_N = 0);
+//   SINQF(x)_k = (-1)^k COSQF(x reversed)_k,
+//   SINQB(X)_k = COSQB((-1)^n X_n)_{N-1-k},
+// with q_m = exp(-i pi m / (2N)) (table qw).  They equal FFTPACK's documented
+// sums (the dense-matrix kernels above) to round-off.  Rows of lb per block;
+// the rows sit at an 8-byte offset in the coupled layout, so they are read
+// with plain loads.
+__host__ __device__ constexpr size_t xq_cplx(int nx, int lb) { return (((size_t)(lb / 2) * nx + 7) / 8) * 8; }
+__host__ __device__ constexpr size_t xq_smem_bytes(int nx, int lb) { return 2 * align128(xq_cplx(nx, lb) * sizeof(double2)); }
+
+template <bool BIG>
+__global__ void __launch_bounds__(256) k_xnp_qfwd(TGDev d, TGDev s, FFTPlan pl, const double2 *__restrict__ qw, int lb,
+                                                  int sinq, double rscal) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ int rad[16];
+  const int nx = d.nx, ny = d.ny, k = blockIdx.y, jbeg = 1 + blockIdx.x * lb;
+  const int nrow = min(lb, ny - jbeg + 1), nl = lb / 2, tid = threadIdx.x;
+  double2 *A = reinterpret_cast<double2 *>(smem_raw);
+  double *in = reinterpret_cast<double *>(smem_raw + align128(xq_cplx(nx, lb) * sizeof(double2)));
+  double2 *B = reinterpret_cast<double2 *>(in);  // FFT scratch once A is filled
+  if (tid < 16) rad[tid] = pl.rad[tid];
+  for (int t = tid; t < lb * nx; t += blockDim.x) {
+    const int r = t / nx, i = t - r * nx;
+    in[t] = r < nrow ? d.rhsphi[d.sy * (jbeg + r) + d.sz * k + i] : 0.0;
+  }
+  __syncthreads();
+  for (int t = tid; t < nl * nx; t += blockDim.x) {
+    const int p = t / nx, m = t - p * nx;
+    const double *r0 = in + (size_t)2 * p * nx, *r1 = r0 + nx;
+    const int im = sinq ? nx - 1 - m : m, ic = sinq ? m - 1 : nx - m;  // x_m, x_{N-m} (SINQF: reversed row)
+    const double a0 = r0[im], a1 = r1[im];
+    const double b0 = m ? r0[ic] : 0.0, b1 = m ? r1[ic] : 0.0;
+    const double2 q = qw[m];  // conj(q) (a - i b) = (qx a - qy b) + i (-qy a - qx b)
+    const double v1x = q.x * a0 - q.y * b0, v1y = -q.y * a0 - q.x * b0;
+    const double v2x = q.x * a1 - q.y * b1, v2y = -q.y * a1 - q.x * b1;
+    A[swz(p * nx + m)] = make_double2(v1x - v2y, v1y + v2x);  // V1 + i V2
+  }
+  __syncthreads();
+  const double2 *res = fft_lines<double2, BIG>(A, B, nl, nx, nx, rad, pl.nrad, pl.tw64, +1);
+  double2 *S = reinterpret_cast<double2 *>(s.spec);
+  for (int t = tid; t < nrow * nx; t += blockDim.x) {
+    const int r = t / nx, m = t - r * nx;
+    const int n = (m & 1) ? nx - 1 - (m >> 1) : (m >> 1);
+    const double2 z = res[swz((r >> 1) * nx + n)];
+    double y = (r & 1) ? z.y : z.x;
+    if (sinq && (m & 1)) y = -y;
+    S[m + (int64_t)s.lp * ((jbeg + r - 1) + (int64_t)ny * k)] = make_double2(y * rscal, 0.0);
+  }
+}
+
+template <bool BIG>
+__global__ void __launch_bounds__(256) k_xnp_qbwd(TGDev d, TGDev s, FFTPlan pl, const double2 *__restrict__ qw, int lb,
+                                                  int sinq) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ int rad[16];
+  const int nx = d.nx, ny = d.ny, k = blockIdx.y, jbeg = 1 + blockIdx.x * lb;
+  const int nrow = min(lb, ny - jbeg + 1), nl = lb / 2, tid = threadIdx.x;
+  double2 *A = reinterpret_cast<double2 *>(smem_raw);
+  double *in = reinterpret_cast<double *>(smem_raw + align128(xq_cplx(nx, lb) * sizeof(double2)));
+  double2 *B = reinterpret_cast<double2 *>(in);
+  if (tid < 16) rad[tid] = pl.rad[tid];
+  const double2 *S = reinterpret_cast<const double2 *>(s.spec);
+  for (int t = tid; t < lb * nx; t += blockDim.x) {
+    const int r = t / nx, m = t - r * nx;
+    double x = r < nrow ? S[m + (int64_t)s.lp * ((jbeg + r - 1) + (int64_t)ny * k)].x : 0.0;
+    if (sinq && (m & 1)) x = -x;  // SINQB: (-1)^n X_n
+    in[t] = x;
+  }
+  __syncthreads();
+  for (int t = tid; t < nl * nx; t += blockDim.x) {
+    const int p = t / nx, n = t - p * nx;
+    const int q = 2 * n < nx ? 2 * n : 2 * (nx - 1 - n) + 1;  // v_n = X_{2n}, v_{N-1-n} = X_{2n+1}
+    A[swz(p * nx + n)] = make_double2(in[(size_t)2 * p * nx + q], in[(size_t)(2 * p + 1) * nx + q]);
+  }
+  __syncthreads();
+  const double2 *res = fft_lines<double2, BIG>(A, B, nl, nx, nx, rad, pl.nrad, pl.tw64, -1);
+  for (int t = tid; t < nrow * nx; t += blockDim.x) {
+    const int r = t / nx, m = t - r * nx;
+    const int kk = sinq ? nx - 1 - m : m;
+    const double2 z = res[swz((r >> 1) * nx + kk)], zc = res[swz((r >> 1) * nx + (kk ? nx - kk : 0))];
+    // V1 = (Z_k + conj Z_{N-k}) / 2, V2 = (Z_k - conj Z_{N-k}) / (2i)
+    double vx, vy;
+    if (r & 1) {
+      vx = 0.5 * (z.y + zc.y);
+      vy = -0.5 * (z.x - zc.x);
+    } else {
+      vx = 0.5 * (z.x + zc.x);
+      vy = 0.5 * (z.y - zc.y);
+    }
+    const double2 q = qw[kk];
+    const double y = 4.0 * (q.x * vx - q.y * vy);
+    const int j = jbeg + r;
+    double *dst = d.phi + d.sy * j + d.sz * k;
+    dst[m] = y;
+    if (j == 1) dst[m - d.sy] = y;  // BC_WALL_DPH: ghost rows by copy
+    if (j == ny) dst[m + d.sy] = y;
+  }
+}
+
 int xnp_pivots(chapsim_ctx *c) {
   TGDev &s = c->dnp;
   dim3 grid((s.lh + 127) / 128, s.nz);
@@ -1714,11 +1819,37 @@ int xnp_pivots(chapsim_ctx *c) {
   return CHAPSIM_OK;
 }
 
+// rows per block of the quarter-wave transforms: the most, as a power of two
+// up to 32, whose two buffers fit in 74 KB (three blocks per SM)
+int xnp_q_lb(int nx) {
+  int lb = 2;
+  while (lb < 32 && xq_smem_bytes(nx, 2 * lb) <= 74 * 1024) lb *= 2;
+  return lb;
+}
+
+int xnp_q_setup(chapsim_ctx *c) {
+  const size_t sm = xq_smem_bytes(c->d.nx, xnp_q_lb(c->d.nx));
+  for (const void *f : {(const void *)k_xnp_qfwd<false>, (const void *)k_xnp_qfwd<true>,
+                        (const void *)k_xnp_qbwd<false>, (const void *)k_xnp_qbwd<true>})
+    CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  return CHAPSIM_OK;
+}
+
 int xnp_pois3d(chapsim_ctx *c, bool mark) {
   TGDev &d = c->d, &s = c->dnp;
   const size_t sm = (size_t)d.nx * sizeof(double);
   const dim3 rows(d.ny, d.nz);
-  k_xnp_fwd<<<rows, 128, sm, c->stream>>>(d, s, c->xnp_f);
+  const bool q = c->xnp_qw != nullptr;  // LP 3 / 5 through the FFT
+  const int lb = xnp_q_lb(d.nx);
+  const size_t smq = xq_smem_bytes(d.nx, lb);
+  const dim3 qgrid((d.ny + lb - 1) / lb, d.nz);
+  const int sinq = c->xnp == 3;
+  if (q && c->fft_big)
+    k_xnp_qfwd<true><<<qgrid, 256, smq, c->stream>>>(d, s, c->fx, c->xnp_qw, lb, sinq, c->xnp_rscal);
+  else if (q)
+    k_xnp_qfwd<false><<<qgrid, 256, smq, c->stream>>>(d, s, c->fx, c->xnp_qw, lb, sinq, c->xnp_rscal);
+  else
+    k_xnp_fwd<<<rows, 128, sm, c->stream>>>(d, s, c->xnp_f);
   LAUNCHED();
   typedef Prec<double> P;
   const int lz = P::fftz_lz(d.nz);
@@ -1743,7 +1874,12 @@ int xnp_pois3d(chapsim_ctx *c, bool mark) {
     k_fftz<double, false><<<gz, 256, P::fftz_smem(d.nz, lz), c->stream>>>(s, c->fz, lz, +1);
   LAUNCHED();
   if (mark) phase_mark(c, CHAPSIM_PH_IFFTX);
-  k_xnp_bwd<<<rows, 128, sm, c->stream>>>(d, s, c->xnp_b);
+  if (q && c->fft_big)
+    k_xnp_qbwd<true><<<qgrid, 256, smq, c->stream>>>(d, s, c->fx, c->xnp_qw, lb, sinq);
+  else if (q)
+    k_xnp_qbwd<false><<<qgrid, 256, smq, c->stream>>>(d, s, c->fx, c->xnp_qw, lb, sinq);
+  else
+    k_xnp_bwd<<<rows, 128, sm, c->stream>>>(d, s, c->xnp_b);
   LAUNCHED();
   return CHAPSIM_OK;
 }

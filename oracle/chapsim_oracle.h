@@ -178,6 +178,10 @@ int oracle_io_set_bcx(oracle_io *o, int in, int out);
 int oracle_io_set_inlet(oracle_io *o, int nxt, const double *tu, const double *tv, const double *tw,
                         const double *tp);
 void oracle_io_pois3d(oracle_io *o);
+/* One x transform of FISHPACK's LP 2..5 (fwd 1: SINT / SINQF / COST / COSQF,
+ * 0: the backward ones): direct sums, or with fast = 1 the DFT route of the
+ * quarter-wave pairs (LP 3 / 5, even n) that lines longer than 64 take. */
+int oracle_fftpack_real(int lp, int fwd, int n, double *x, int fast);
 /* iso-thermal walls (bit 0 bottom, bit 1 top; io_oracle.cpp) */
 int oracle_io_set_walls(oracle_io *o, int bits);
 /* PP_MEAN_ZX_FLOW_Xperiodic_IO: ny * 360 xz-plane averages (io_oracle.cpp) */

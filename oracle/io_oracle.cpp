@@ -753,6 +753,52 @@ void fftpack_real(int lp, bool fwd, int n, double *x, double *tmp) {
   std::copy(tmp, tmp + n, x);
 }
 
+// The quarter-wave pairs (LP 5 COSQF / COSQB, LP 3 SINQF / SINQB) in
+// O(N log N) through the N-point complex DFT, by Makhoul's even-odd
+// reordering (IEEE Trans. ASSP 28 (1980) 27-34); q_m = exp(-i pi m / (2N)):
+//   COSQB(X)_k = 4 Re(q_k V_k), V = DFT(v), v_n = X_{2n}, v_{N-1-n} = X_{2n+1};
+//   COSQF(x)_{2n} = Re w_n, COSQF(x)_{2n+1} = Re w_{N-1-n},
+//     w = inverse DFT (unnormalised) of conj(q_m) (x_m - i x_{N-m}), x_N = 0;
+//   SINQF(x)_k = (-1)^k COSQF(x reversed)_k;  SINQB(X)_k = COSQB((-1)^n X_n)_{N-1-k}.
+// w: 6 N doubles of scratch.  N even.
+void qwave_fast(int lp, bool fwd, int n, double *x, const oracle_dft *f, double *w) {
+  const bool sinq = lp == 3;
+  double *in = w, *out = w + 2 * n, *tmp = w + 4 * n;
+  auto qc = [&](int m) { return std::cos(M_PI * m / (2.0 * n)); };
+  auto qs = [&](int m) { return -std::sin(M_PI * m / (2.0 * n)); };
+  if (fwd) {
+    for (int m = 0; m < n; ++m) {
+      const double a = x[sinq ? n - 1 - m : m], b = m ? x[sinq ? m - 1 : n - m] : 0.0;
+      in[2 * m] = qc(m) * a - qs(m) * b;        // conj(q) (a - i b)
+      in[2 * m + 1] = -qs(m) * a - qc(m) * b;
+    }
+    oracle_dft_run(f, in, out, +1, tmp);
+    for (int m = 0; m < n; ++m) {
+      const int nn = (m & 1) ? n - 1 - (m >> 1) : (m >> 1);
+      const double y = out[2 * nn];
+      x[m] = (sinq && (m & 1)) ? -y : y;
+    }
+  } else {
+    std::vector<double> xs(x, x + n);
+    if (sinq)
+      for (int m = 1; m < n; m += 2) xs[m] = -xs[m];
+    for (int nn = 0; nn < n; ++nn) {
+      const int q = 2 * nn < n ? 2 * nn : 2 * (n - 1 - nn) + 1;
+      in[2 * nn] = xs[q];
+      in[2 * nn + 1] = 0.0;
+    }
+    oracle_dft_run(f, in, out, -1, tmp);
+    for (int m = 0; m < n; ++m) {
+      const int kk = sinq ? n - 1 - m : m;
+      x[m] = 4.0 * (qc(kk) * out[2 * kk] - qs(kk) * out[2 * kk + 1]);
+    }
+  }
+}
+
+// Lines longer than this take the quarter-wave pairs through the DFT (the
+// GPU parity cases, shorter, keep the direct sums as an independent check).
+constexpr int kQwaveFastMin = 64;
+
 // FISHPACK_POIS3D_SIMPLE (src/possion3d_fishpack_reform.f90:431-547) for
 // periodic z and the x boundary type lpx: RHSLLPHI -> DPH (interior), ghosts
 // by copy.
@@ -777,6 +823,8 @@ void fishpack_pois3d(oracle_io *o) {
         for (int i = 1; i <= l; ++i) t[i - 1] = FR(i, k, j);
         if (o->lpx == 1)
           rfftf(o->dftx, l, t.data(), w.data());
+        else if ((o->lpx == 3 || o->lpx == 5) && l > kQwaveFastMin)
+          qwave_fast(o->lpx, true, l, t.data(), o->dftx, w.data());
         else
           fftpack_real(o->lpx, true, l, t.data(), w.data());
         for (int i = 1; i <= l; ++i) FR(i, k, j) = t[i - 1];
@@ -834,6 +882,8 @@ void fishpack_pois3d(oracle_io *o) {
         for (int i = 1; i <= l; ++i) t[i - 1] = FR(i, k, j);
         if (o->lpx == 1)
           rfftb(o->dftx, l, t.data(), w.data());
+        else if ((o->lpx == 3 || o->lpx == 5) && l > kQwaveFastMin)
+          qwave_fast(o->lpx, false, l, t.data(), o->dftx, w.data());
         else
           fftpack_real(o->lpx, false, l, t.data(), w.data());
         for (int i = 1; i <= l; ++i) FR(i, k, j) = t[i - 1];
@@ -1630,6 +1680,22 @@ int oracle_io_set_bcx(oracle_io *o, int in, int out) {
 
 // FISHPACK_POIS3D_SIMPLE alone: DPH from the current RHSLLPHI.
 void oracle_io_pois3d(oracle_io *o) { fishpack_pois3d(o); }
+
+// One real x transform of FISHPACK's LP 2..5 on x (n values): the direct
+// documented sums, or (fast, LP 3 / 5 only) the DFT route.
+int oracle_fftpack_real(int lp, int fwd, int n, double *x, int fast) {
+  if (lp < 2 || lp > 5 || n < 2) return -1;
+  std::vector<double> w(6 * (size_t)n);
+  if (fast) {
+    if ((lp != 3 && lp != 5) || (n & 1)) return -1;
+    oracle_dft *f = oracle_dft_create(n);
+    qwave_fast(lp, fwd != 0, n, x, f, w.data());
+    oracle_dft_destroy(f);
+  } else {
+    fftpack_real(lp, fwd != 0, n, x, w.data());
+  }
+  return 0;
+}
 
 // BCWALLHEAT = isoThermalWall on the walls of `bits` (bit 0 bottom, bit 1
 // top), the wall temperature being qw of that wall; WALL_ISOTHERMAL_GIVEN

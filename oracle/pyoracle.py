@@ -85,6 +85,8 @@ def load(build=True):
     L.oracle_io_set_bcx.argtypes = [P, I, I]
     L.oracle_io_set_bcx.restype = I
     L.oracle_io_pois3d.argtypes = [P]
+    L.oracle_fftpack_real.argtypes = [I, I, I, P, I]
+    L.oracle_fftpack_real.restype = I
     L.oracle_tg_stats.argtypes = [P, P]
     L.oracle_set_threads.argtypes = [I]
     L.oracle_get_threads.restype = I

@@ -249,3 +249,25 @@ def test_io_poisson_nonperiodic_x_inverts_the_operator(bcx):
     res = lap - rhs[:, 1:ny + 1, :]
     rows = ny - 1 if bcx == (2, 2) else ny
     assert np.abs(res[:, :rows, :]).max() <= 1e-10 * np.abs(rhs).max(), np.abs(res[:, :rows, :]).max()
+
+
+@pytest.mark.parametrize("lp", [3, 5])
+@pytest.mark.parametrize("n", [96, 128, 192])
+def test_quarter_wave_transforms_fast_route_matches_the_sums(lp, n):
+    """SINQF / SINQB (LP 3) and COSQF / COSQB (LP 5) through the N-point DFT
+    (the route the oracle takes on lines longer than 64 and the library on
+    every line) against FFTPACK's documented sums, to round-off; forward then
+    backward returns 4 N times the input."""
+    from oracle.pyoracle import load
+    L = load()
+    rng = np.random.default_rng(n + lp)
+    x = rng.standard_normal(n)
+    for fwd in (1, 0):
+        a, b = x.copy(), x.copy()
+        assert L.oracle_fftpack_real(lp, fwd, n, a.ctypes.data, 0) == 0
+        assert L.oracle_fftpack_real(lp, fwd, n, b.ctypes.data, 1) == 0
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max(), (fwd, np.abs(a - b).max())
+    y = x.copy()
+    assert L.oracle_fftpack_real(lp, 1, n, y.ctypes.data, 1) == 0
+    assert L.oracle_fftpack_real(lp, 0, n, y.ctypes.data, 1) == 0
+    assert np.abs(y / (4 * n) - x).max() <= 1e-12
