@@ -702,7 +702,7 @@ def synthetic_table_cols(table5):
 # reads G and DrhoDtP and writes RHSLLPHI, which the forward x transform reads
 # and writes as nx complex modes per row (the real x modes in complex lines);
 # the z transforms and y-lines pass over nx complex values per row.
-IO_KERNEL_COUPLED = dict(IO_KERNEL, mom_rhs="k_io_rhs", fftx="k_np_divg + k_xnp_qfwd", ifftx="k_xnp_qbwd")
+IO_KERNEL_COUPLED = dict(IO_KERNEL, mom_rhs="k_io_rhs_tma (coupled layout)", fftx="k_np_divg + k_xnp_qfwd", ifftx="k_xnp_qbwd")
 IO_COUPLED_VALUES = dict(IO_VALUES_PER_CELL, fftx=8, fftz=4, ysolve=4, ifftz=4, ifftx=3)
 
 
@@ -1301,6 +1301,26 @@ def profile_case(spec, precision, spectra="fp64", refine=1):
                 c.solverrk3_mom_io(ns)
         c.sync()
         print("profile case ok", spec, "max|div G + drho| =", c.divgck_io())
+        return 0
+    if spec.lower().startswith("cpl"):
+        # the coupled pair: TG nx/2 x ny x nz feeding the IO section nx x ny x
+        # nz (BCX_io = 2, 1, constant properties), eager substeps in SOLVE's order
+        from chapsim1ww_b200 import IOChannel
+        nx, ny, nz = (int(x) for x in spec.lower()[3:].split("x"))
+        t = TGChannel(nx // 2, ny, nz)
+        c = IOChannel(nx, ny, nz, table=io_table("constant"), bcx=(2, 1))
+        c.set_inlet(t)
+        t.random_fl_fld_tg(1, 0.1, project=True)
+        c.random_fl_theml_fld_io(1, 0.1)
+        for _ in range(2):
+            for ns in (1, 2, 3):
+                t.solverrk3_mom_tg(ns)
+                c.solverrk3_eng_io(ns)
+                c.solverrk3_mom_io(ns)
+        c.sync()
+        print("profile case ok", spec, "max|div G + drho| =", c.divgck_io())
+        c.close()
+        t.close()
         return 0
     if spec.lower().startswith("io"):
         from chapsim1ww_b200 import IOChannel

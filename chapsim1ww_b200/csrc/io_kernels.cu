@@ -744,21 +744,37 @@ constexpr int F_U = 0, F_V = 1, F_W = 2, F_GX = 3, F_GY = 4, F_GZ = 5, F_P = 6, 
 constexpr int IT_EBOX = IO_BX * IO_BY;  // EXPLT0 boxes: the tile's own 32 x 8 cells
 constexpr size_t IT_SLOT = (size_t)IT_NF * IT_PST * sizeof(double);
 constexpr size_t IT_ESLOT = (size_t)3 * IT_EBOX * sizeof(double);
-constexpr size_t IT_SMEM = 4 * IT_SLOT + 2 * IT_ESLOT + 6 * sizeof(uint64_t);
 static_assert((IT_PST * 8) % 128 == 0 && IT_PST >= IT_PLANE, "TMA destinations must stay 128-byte aligned");
 static_assert(IT_SLOT % 128 == 0 && IT_ESLOT % 128 == 0 && (IT_EBOX * 8) % 128 == 0, "128-byte aligned slots");
 struct IoMaps {
   CUtensorMap m[14];  // u, v, w, p, msum, g[0][0..2], g[1][0..2], EXPLT0[0..2]
 };
 
-template <bool TH>
+// Plane geometry.  The coupled section's fields start one value before
+// column 0 (its inlet ghost column), and its maps start there: the box that
+// covers columns x0 - 2 .. x0 + 33 must start at an even map coordinate, so
+// it starts at column x0 - 3 (map x0 - 2) and is 38 wide.  Its EXPLT0 is
+// read with plain loads (a 32-wide box at column x0 would start at an odd map
+// coordinate).
+template <bool CPL> struct ItGeo {
+  static constexpr int BXW = CPL ? 38 : IT_BXW, PLANE = BXW * IT_BYW, PST = CPL ? 384 : IT_PST, XO = CPL ? 3 : 2;
+  static constexpr size_t SLOT = (size_t)IT_NF * PST * sizeof(double);
+  static constexpr size_t ESLOTS = CPL ? 0 : 2 * IT_ESLOT;
+  static constexpr size_t SMEM = 4 * SLOT + ESLOTS + 6 * sizeof(uint64_t);
+};
+static_assert((ItGeo<true>::PST * 8) % 128 == 0 && ItGeo<true>::PST >= ItGeo<true>::PLANE &&
+                  (ItGeo<true>::BXW * 8) % 16 == 0,
+              "coupled TMA boxes: 128-byte aligned destinations, 16-byte rows");
+
+template <bool TH, bool CPL>
 __global__ void __launch_bounds__(IO_BX *IO_BY, 2)
 k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam, double roh, double alp, int cur,
              int nzc) {
+  typedef ItGeo<CPL> G;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  auto slot = [&](int sl) { return reinterpret_cast<double *>(smem_raw + (size_t)sl * IT_SLOT); };
-  auto eslot = [&](int sl) { return reinterpret_cast<double *>(smem_raw + 4 * IT_SLOT + (size_t)sl * IT_ESLOT); };
-  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + 4 * IT_SLOT + 2 * IT_ESLOT);
+  auto slot = [&](int sl) { return reinterpret_cast<double *>(smem_raw + (size_t)sl * G::SLOT); };
+  auto eslot = [&](int sl) { return reinterpret_cast<double *>(smem_raw + 4 * G::SLOT + (size_t)sl * IT_ESLOT); };
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + 4 * G::SLOT + G::ESLOTS);
   uint64_t *ebar = bar + 4;
   __shared__ double red[IO_BX * IO_BY / 32];
   __shared__ double ycoef[IO_BY][9];
@@ -772,7 +788,7 @@ k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam,
   const bool left_edge = (x0 == 0), right_edge = (x0 + IO_BX >= nx);
   const int right_col = nx - x0 + 2;  // smem column of x = nx (wraps to 0)
   const int nf = io.thermal ? 8 : 7;
-  const uint32_t tx_bytes = (uint32_t)(nf * IT_PLANE * sizeof(double));
+  const uint32_t tx_bytes = (uint32_t)(nf * G::PLANE * sizeof(double));
   const CUtensorMap *mp[IT_NF] = {&maps.m[0], &maps.m[1], &maps.m[2], &maps.m[5 + 3 * cur], &maps.m[6 + 3 * cur],
                                   &maps.m[7 + 3 * cur], &maps.m[3], &maps.m[4]};
   const double *gsrc[IT_NF] = {d.u, d.v, d.w, io.g[cur][0], io.g[cur][1], io.g[cur][2], d.p, io.msum};
@@ -806,7 +822,7 @@ k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam,
     mbar_expect_tx(&bar[sl], tx_bytes);
 #pragma unroll
     for (int f = 0; f < IT_NF; ++f)
-      if (f < nf) tma_load_3d(slot(sl) + f * IT_PST, mp[f], x0 - 2, j0 - 1, kz, &bar[sl]);
+      if (f < nf) tma_load_3d(slot(sl) + f * G::PST, mp[f], x0 - 2, j0 - 1, kz, &bar[sl]);
   };
   uint32_t par = 0;
   auto wait_plane = [&](int k) -> bool {
@@ -814,6 +830,7 @@ k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam,
     const bool ok = mbar_wait(&bar[sl], (par >> sl) & 1u, d.err);
     par ^= 1u << sl;
     const int kz = k < 0 ? k + nz : (k >= nz ? k - nz : k);
+    if (CPL) return ok;  // the coupled section's ghost columns came with the box
     if (left_edge && tid < 10 * IT_NF) {
       const int f = tid / 10, r = tid - f * 10, jr = j0 - 1 + r;
       if (f < nf && jr <= ny + 1) slot(sl)[f * IT_PST + r * IT_BXW + 1] = gsrc[f][(nx - 1) + d.sy * jr + d.sz * kz];
@@ -836,23 +853,32 @@ k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam,
     issue(kbeg - 1);
     issue(kbeg);
     issue(kbeg + 1);
-    issue_e(kbeg);
+    if (!CPL) issue_e(kbeg);
   }
   bool ok = wait_plane(kbeg - 1);
   ok = wait_plane(kbeg) && ok;
   double part = 0.0;
   const double dxi = d.dxi, dzi = d.dzi, cv = d.cvisc, dt = d.dt;
   const double *yc = ycoef[ty];
-  const int xx = tx + 2, yy = ty + 1;
+  const int xx = tx + G::XO, yy = ty + 1;
   constexpr bool th = TH;
+  // coupled layout: EXPLT0 of the cell by plain loads, issued before the
+  // plane waits so that their latency hides behind them (the stores of the
+  // plane's results may alias them, so they could not move later)
+  double e0r[3] = {0.0, 0.0, 0.0};
   for (int k = kbeg; k < kend; ++k) {
+    if (CPL && active) {
+      const int64_t ce = i + d.sy * j + d.sz * k;
+#pragma unroll
+      for (int q = 0; q < 3; ++q) e0r[q] = ((const double *)d.h0[q])[ce];
+    }
     if (tid == 0) {
       fence_proxy_async();
       if (k + 2 <= kend) issue(k + 2);
-      if (k + 1 < kend) issue_e(k + 1);
+      if (!CPL && k + 1 < kend) issue_e(k + 1);
     }
     ok = wait_plane(k + 1) && ok;
-    {
+    if (!CPL) {
       const int esl = (k - kbeg) & 1;
       ok = mbar_wait(&ebar[esl], (epar >> esl) & 1u, d.err) && ok;
       epar ^= 1u << esl;
@@ -863,7 +889,7 @@ k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam,
       const double *Sm = slot(slot_of(k - 1));
       const double *Sc = slot(slot_of(k));
       const double *Sp = slot(slot_of(k + 1));
-#define A(S, f, dx, dy) S[(f) * IT_PST + (yy + (dy)) * IT_BXW + xx + (dx)]
+#define A(S, f, dx, dy) S[(f) * G::PST + (yy + (dy)) * G::BXW + xx + (dx)]
       const double wff = yc[0], wfb = yc[1], wffp = yc[2], wfbp = yc[3], dyfj = yc[4], dycj = yc[5], dycp = yc[6];
       // cell-centred 0.5 (mu0 + mu), M = mu0 + mu
       auto muc = [&](const double *S, int dx, int dy) { return th ? 0.5 * A(S, F_M, dx, dy) : 1.0; };
@@ -896,11 +922,15 @@ k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam,
                 (A(Sn, F_W, dx, dy) - A(S, F_W, dx, dy)) * dzi) * (1.0 / 3.0);
       };
       const int64_t sy = d.sy, c = i + sy * j + d.sz * k;
-      const int64_t oxm = (i == 0 ? nx - 1 : i - 1) - i, ozm = d.sz * ((k == 0 ? nz - 1 : k - 1) - k);
+      const int64_t oxm = CPL ? -1 : (i == 0 ? nx - 1 : i - 1) - i, ozm = d.sz * ((k == 0 ? nz - 1 : k - 1) - k);
       const double p0 = A(Sc, F_P, 0, 0);
       const double divc = divu(Sc, Sp, 0, 0, dyfj);
-      // ---------------- x
-      {
+      // EXPLT0 of the cell: the staged box, or (coupled) a plain load
+      auto e0of = [&](int q) { return CPL ? e0r[q] : Es[q * IT_EBOX + tid]; };
+      // the coupled outlet ghost face keeps MU_STG = 1 (MU_Staggered covers IC <= NCL1_io)
+      const bool xout = CPL && i == nx - 1;
+      // ---------------- x (the coupled inlet face, NXI = 2, keeps its value: k_np_gbound)
+      if (!CPL || i > 0) {
         const double u0 = A(Sc, F_U, 0, 0);
         double h11f = (A(Sc, F_GX, 1, 0) + A(Sc, F_GX, 0, 0)) * (A(Sc, F_U, 1, 0) + u0);
         double h11b = (A(Sc, F_GX, 0, 0) + A(Sc, F_GX, -1, 0)) * (u0 + A(Sc, F_U, -1, 0));
@@ -932,7 +962,7 @@ k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam,
         const double tau13b = s2(Sc, Sm, 0) * (dudz + dwdx);
         const double d13 = (tau13f - tau13b) * (dzi * cv);
         ex = ex + d11 + d12 + d13;
-        double r = (gam * ex + roh * Es[tid]) * dt;
+        double r = (gam * ex + roh * e0of(0)) * dt;
         ((double *)d.h0[0])[c] = ex;
         r -= (p0 - A(Sc, F_P, -1, 0)) * (alp * dt * dxi);
         if (io.gravdir == 1) {
@@ -962,7 +992,7 @@ k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam,
         const double d22 = (tau22f - tau22b) * (2.0 * dycj * cv);
         double dvdx = (A(Sc, F_V, 1, 0) - v0) * dxi;
         double dudy = (A(Sc, F_U, 1, 0) - A(Sc, F_U, 1, -1)) * dycj;
-        const double tau21f = s1(Sc, 1, 0, wff, wfb) * (dvdx + dudy);
+        const double tau21f = (xout ? 1.0 : s1(Sc, 1, 0, wff, wfb)) * (dvdx + dudy);
         dvdx = (v0 - A(Sc, F_V, -1, 0)) * dxi;
         dudy = (A(Sc, F_U, 0, 0) - A(Sc, F_U, 0, -1)) * dycj;
         const double tau21b = s1(Sc, 0, 0, wff, wfb) * (dvdx + dudy);
@@ -975,7 +1005,7 @@ k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam,
         const double tau23b = s3(Sc, Sm, 0, wff, wfb) * (dvdz + dwdy);
         const double d23 = (tau23f - tau23b) * (dzi * cv);
         ey = ey + d21 + d22 + d23;
-        double r = (gam * ey + roh * Es[IT_EBOX + tid]) * dt;
+        double r = (gam * ey + roh * e0of(1)) * dt;
         ((double *)d.h0[1])[c] = ey;
         r -= (p0 - A(Sc, F_P, 0, -1)) * (alp * dt * dycj);
         if (io.gravdir == 2) {
@@ -1004,7 +1034,7 @@ k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam,
         const double d33 = (tau33f - tau33b) * (2.0 * dzi * cv);
         double dwdx = (A(Sc, F_W, 1, 0) - w0) * dxi;
         double dudz = (A(Sc, F_U, 1, 0) - A(Sm, F_U, 1, 0)) * dzi;
-        const double tau31f = s2(Sc, Sm, 1) * (dwdx + dudz);
+        const double tau31f = (xout ? 1.0 : s2(Sc, Sm, 1)) * (dwdx + dudz);
         dwdx = (w0 - A(Sc, F_W, -1, 0)) * dxi;
         dudz = (A(Sc, F_U, 0, 0) - A(Sm, F_U, 0, 0)) * dzi;
         const double tau31b = s2(Sc, Sm, 0) * (dwdx + dudz);
@@ -1017,7 +1047,7 @@ k_io_rhs_tma(const __grid_constant__ IoMaps maps, TGDev d, IODev io, double gam,
         const double tau32b = s3(Sc, Sm, 0, wff, wfb) * (dwdy + dvdz);
         const double d32 = (tau32f - tau32b) * (dyfj * cv);
         ez = ez + d31 + d32 + d33;
-        double r = (gam * ez + roh * Es[2 * IT_EBOX + tid]) * dt;
+        double r = (gam * ez + roh * e0of(2)) * dt;
         ((double *)d.h0[2])[c] = ez;
         r -= (p0 - A(Sm, F_P, 0, 0)) * (alp * dt * dzi);
         if (io.gravdir == 3) {
@@ -1285,10 +1315,11 @@ int io_mom(chapsim_ctx *c, int ns, bool prep) {
     IoMaps maps;
     memcpy(maps.m, c->io_maps, sizeof(maps.m));
     dim3 g2(grid.x, grid.y, (d.nz + c->io_nzc - 1) / c->io_nzc);
+    constexpr size_t sm = ItGeo<false>::SMEM;
     if (io.thermal)
-      k_io_rhs_tma<true><<<g2, blk, IT_SMEM, c->stream>>>(maps, d, io, sp.gam, sp.roh, sp.alp, cur, c->io_nzc);
+      k_io_rhs_tma<true, false><<<g2, blk, sm, c->stream>>>(maps, d, io, sp.gam, sp.roh, sp.alp, cur, c->io_nzc);
     else
-      k_io_rhs_tma<false><<<g2, blk, IT_SMEM, c->stream>>>(maps, d, io, sp.gam, sp.roh, sp.alp, cur, c->io_nzc);
+      k_io_rhs_tma<false, false><<<g2, blk, sm, c->stream>>>(maps, d, io, sp.gam, sp.roh, sp.alp, cur, c->io_nzc);
     npart = (int)(g2.x * g2.y * g2.z);
   } else {
     k_io_rhs<<<grid, blk, 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, cur);
@@ -1313,8 +1344,8 @@ int io_mom(chapsim_ctx *c, int ns, bool prep) {
 int io_init_maps(chapsim_ctx *c) {
   TGDev &d = c->d;
   c->use_tma_io = false;
-  // small grids and the coupled section (ghost columns) use k_io_rhs
-  if (d.nx < IT_BXW || d.ny < 8 || c->xnp) return CHAPSIM_OK;
+  if (d.nx < IT_BXW || d.ny < 8) return CHAPSIM_OK;  // small grids use k_io_rhs
+  const bool cpl = c->xnp != 0;  // the coupled layout: maps from the inlet ghost column
   PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   cudaDriverEntryPointQueryResult q;
   if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", (void **)&encode, cudaEnableDefault, &q) != cudaSuccess ||
@@ -1323,11 +1354,14 @@ int io_init_maps(chapsim_ctx *c) {
     return CHAPSIM_OK;
   }
   IODev &io = c->io;
-  void *f[14] = {d.u,        d.v,        d.w,        d.p,        io.msum,    io.g[0][0], io.g[0][1],
-                 io.g[0][2], io.g[1][0], io.g[1][1], io.g[1][2], d.h0[0],    d.h0[1],    d.h0[2]};
-  cuuint64_t dims[3] = {(cuuint64_t)d.nx, (cuuint64_t)(d.ny + 2), (cuuint64_t)d.nz};
+  const int xo = c->xoff;
+  void *f[14] = {d.u - xo,        d.v - xo,        d.w - xo,        d.p - xo,        io.msum - xo,
+                 io.g[0][0] - xo, io.g[0][1] - xo, io.g[0][2] - xo, io.g[1][0] - xo, io.g[1][1] - xo,
+                 io.g[1][2] - xo, (double *)d.h0[0] - xo, (double *)d.h0[1] - xo, (double *)d.h0[2] - xo};
+  cuuint64_t dims[3] = {(cuuint64_t)(d.nx + 2 * xo), (cuuint64_t)(d.ny + 2), (cuuint64_t)d.nz};
   cuuint64_t strides[2] = {(cuuint64_t)d.sy * sizeof(double), (cuuint64_t)d.sz * sizeof(double)};
-  cuuint32_t box[3] = {IT_BXW, IT_BYW, 1}, ebox[3] = {IO_BX, IO_BY, 1};
+  cuuint32_t box[3] = {(cuuint32_t)(cpl ? ItGeo<true>::BXW : ItGeo<false>::BXW), IT_BYW, 1};
+  cuuint32_t ebox[3] = {IO_BX, IO_BY, 1};
   cuuint32_t es[3] = {1, 1, 1};
   if ((d.sy * sizeof(double)) % 16 != 0) return CHAPSIM_OK;  // TMA strides must be multiples of 16 bytes
   for (int m = 0; m < 14; ++m) {
@@ -1342,10 +1376,13 @@ int io_init_maps(chapsim_ctx *c) {
   int dev = 0, optin = 0;
   CK(cudaGetDevice(&dev));
   CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  for (const void *fn : {(const void *)k_io_rhs_tma<true>, (const void *)k_io_rhs_tma<false>}) {
+  const size_t smem = cpl ? ItGeo<true>::SMEM : ItGeo<false>::SMEM;
+  const void *fns[2] = {cpl ? (const void *)k_io_rhs_tma<true, true> : (const void *)k_io_rhs_tma<true, false>,
+                        cpl ? (const void *)k_io_rhs_tma<false, true> : (const void *)k_io_rhs_tma<false, false>};
+  for (const void *fn : fns) {
     cudaFuncAttributes fa;
     CK(cudaFuncGetAttributes(&fa, fn));
-    if ((size_t)optin < IT_SMEM + fa.sharedSizeBytes) return CHAPSIM_OK;
+    if ((size_t)optin < smem + fa.sharedSizeBytes) return CHAPSIM_OK;
     CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes));
   }
   c->use_tma_io = true;
@@ -1847,7 +1884,18 @@ int io_np_mom(chapsim_ctx *c, int ns) {
   if ((rc = io_bc_outlet_mom(c, ns))) return rc;
   k_np_mom_post<<<nb, 256, 0, c->stream>>>(d, io, cur);
   LAUNCHED();
-  k_io_rhs<<<grid, blk, 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, cur);
+  if (c->use_tma_io) {
+    IoMaps maps;
+    memcpy(maps.m, c->io_maps, sizeof(maps.m));
+    const dim3 g2(grid.x, grid.y, (d.nz + c->io_nzc - 1) / c->io_nzc);
+    constexpr size_t sm = ItGeo<true>::SMEM;
+    if (io.thermal)
+      k_io_rhs_tma<true, true><<<g2, blk, sm, c->stream>>>(maps, d, io, sp.gam, sp.roh, sp.alp, cur, c->io_nzc);
+    else
+      k_io_rhs_tma<false, true><<<g2, blk, sm, c->stream>>>(maps, d, io, sp.gam, sp.roh, sp.alp, cur, c->io_nzc);
+  } else {
+    k_io_rhs<<<grid, blk, 0, c->stream>>>(d, io, sp.gam, sp.roh, sp.alp, cur);
+  }
   LAUNCHED();
   k_np_gbound<<<nb, 256, 0, c->stream>>>(d, io, cur);
   LAUNCHED();

@@ -85,6 +85,9 @@ def _compare(tg, ot, g, o, thermal, what):
     dict(nxt=32, nxi=40, ny=20, nz=16, bcx=(2, 1), thermal=1, table="synthetic"),
     dict(nxt=16, nxi=24, ny=18, nz=8, bcx=(2, 1), thermal=0),
     dict(nxt=16, nxi=20, ny=16, nz=12, bcx=(1, 1), thermal=1, table="constant"),
+    # two x tiles of the TMA-staged momentum RHS (nx >= 36)
+    dict(nxt=32, nxi=72, ny=24, nz=20, bcx=(2, 1), thermal=1, table="synthetic"),
+    dict(nxt=32, nxi=64, ny=16, nz=12, bcx=(2, 1), thermal=0),
 ])
 def test_coupled_step_parity(case):
     tg, ot, g, o = _pair(**case)
