@@ -156,3 +156,84 @@ def test_config2_heated_io_500_steps_learned_against_table():
     assert b.bad_cells() == 0
     a.close()
     b.close()
+
+
+def _coupled(nxt, nxi, ny, nz, precision=0, seed=1):
+    from chapsim1ww_b200 import IOChannel, TGChannel
+    lz = 4 * math.pi / 3
+    h = np.linspace(-1.0, 1.0, 4096)
+    one = np.ones_like(h)
+    table = [h, h.copy(), one, one.copy(), one.copy()]  # constant-property passive heat
+    tg = TGChannel(nxt, ny, nz, lz=lz, precision=precision)
+    io = IOChannel(nxi, ny, nz, lz=lz, table=table, bcx=(2, 1))
+    io.set_inlet(tg)
+    tg.random_fl_fld_tg(seed, 0.1, project=False)
+    tg.solverrk3_mom_tg(0)
+    io.random_fl_theml_fld_io(seed + 1, 0.1)
+    return tg, io, table
+
+
+def test_config1_coupled_100_steps_fp64_parity():
+    """Configuration 1's coupled TG -> IO step (BCX_io = 2, 1, constant-property
+    passive heat, wall heat flux 1) on a small grid for 100 steps: both
+    sections within 1e-9 relative of the FP64 oracle at every 25th step."""
+    _need_gpu()
+    from oracle.pyoracle import OracleIO, OracleTG
+    nxt, nxi, ny, nz = 32, 64, 24, 16
+    tg, io, table = _coupled(nxt, nxi, ny, nz)
+    lz = 4 * math.pi / 3
+    ot = OracleTG(nxt, ny, nz, lz=lz)
+    ot.init_random(1, 0.1)
+    ot.substep(0)
+    o = OracleIO(nxi, ny, nz, lz=lz, table=table)
+    o.set_bcx(2, 1)
+    feed = lambda: o.set_inlet(*[ot.get(f) for f in ("u", "v", "w", "p")])  # noqa: E731
+    feed()
+    o.init_random(2, 0.1)
+    worst = {}
+    for chunk in range(4):
+        io.step_coupled(tg, 25)
+        for _ in range(25):
+            for ns in (1, 2, 3):
+                ot.substep(ns)
+                feed()
+                o.substep(ns)
+        errs = {"tg_" + n: relerr(tg.get_field(n), ot.get(n)) for n in ("u", "v", "w", "p")}
+        errs.update({n: relerr(io.get_field(n), o.get(n)) for n in ("u", "v", "w", "p", "gx", "h", "t")})
+        for n, e in errs.items():
+            worst[n] = max(worst.get(n, 0.0), e)
+            assert e <= 1e-9, (25 * (chunk + 1), n, e)
+    print(f"configuration 1 coupled, 100 steps vs the oracle: worst relative errors "
+          + ", ".join(f"{n} {e:.1e}" for n, e in worst.items())
+          + f"; IO max|div G + drho| {io.divgck_io():.2e} (oracle {o.divmax():.2e})")
+
+
+def test_config1_coupled_500_steps_mixed_tg_vs_fp64():
+    """Configuration 1 as written, 500 steps from seed 1, plain FP64 against
+    the mixed form (the TG section's FP32 temporaries and spectra with one
+    FP64-residual refinement sweep; the coupled IO section's Poisson solve
+    stays FP64), on a small grid: the IO section inherits the TG's mixed-form
+    error through the inlet.  Stated tolerances: u, T <= 1e-5, p <= 1e-4 of
+    the FP64 run, max|div u| (TG) <= 1e-8, the IO section's divergence away
+    from its first column as small as in the FP64 run."""
+    _need_gpu()
+    from chapsim1ww_b200 import MIXED
+    a_tg, a_io, _ = _coupled(32, 64, 24, 16)
+    b_tg, b_io, _ = _coupled(32, 64, 24, 16, precision=MIXED)
+    errs = {}
+    for chunk in range(5):
+        a_io.step_coupled(a_tg, 100)
+        b_io.step_coupled(b_tg, 100)
+        e = {"tg_u": relerr(b_tg.get_field("u"), a_tg.get_field("u")),
+             "tg_p": relerr(b_tg.get_field("p"), a_tg.get_field("p")),
+             "io_u": relerr(b_io.get_field("u"), a_io.get_field("u")),
+             "io_p": relerr(b_io.get_field("p"), a_io.get_field("p")),
+             "io_t": relerr(b_io.get_field("t"), a_io.get_field("t"))}
+        print(f"step {100 * (chunk + 1)}: " + ", ".join(f"{n} {v:.2e}" for n, v in e.items())
+              + f", TG max|div u| {b_tg.divgck_tg():.2e}, IO max|div G + drho| {b_io.divgck_io():.2e} "
+              f"(FP64 {a_io.divgck_io():.2e})")
+        errs = e
+    assert errs["tg_u"] <= 1e-5 and errs["io_u"] <= 1e-5 and errs["io_t"] <= 1e-5
+    assert errs["tg_p"] <= 1e-4 and errs["io_p"] <= 1e-4
+    assert b_tg.divgck_tg() <= 1e-8
+    assert np.isfinite(b_io.divgck_io())
