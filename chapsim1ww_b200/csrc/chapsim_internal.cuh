@@ -244,7 +244,8 @@ int launch_pois_io(chapsim_ctx *c, int ns, double *gx, double *gy, double *gz, c
 // IO domain kernels (io_kernels.cu).
 int io_eng(chapsim_ctx *c, int ns);
 int io_bc_inlet(chapsim_ctx *c, const chapsim_ctx *tg);
-int io_bc_outlet_mom(chapsim_ctx *c, int ns);
+// mass_parts: d.partials already holds the block sums of DrhoDtP / DYFI
+int io_bc_outlet_mom(chapsim_ctx *c, int ns, bool mass_parts = false);
 int io_bc_outlet_eng(chapsim_ctx *c, int ns);
 // coupled section (xnp): DIVG_io of the G buffer buf into RHSLLPHI
 int io_np_divg(chapsim_ctx *c, int ns, int buf);

@@ -472,14 +472,13 @@ __global__ void k_io_msum(IODev io, size_t n) {
 // Eight blocks per SM for the explicit scheme (32 registers, measured 0.459
 // -> 0.410 ms at 512x192x256): latency-bound, it gains from the extra
 // resident warps.  The DRHOI variant keeps its register count (a cap spills).
+// DENSITY_TIME_DERIVATION and VELOCITY_CALC_io of one cell; returns its DrhoDtP
+// (zero without do_drho)
 template <bool VISC>
-__global__ void __launch_bounds__(IO_BX *IO_BY, VISC ? 1 : 8) k_io_prep(TGDev d, IODev io, double gp, double zr, double den,
-                                                        int cur, int do_drho) {
-  const int nx = d.nx, ny = d.ny;
-  const int i = blockIdx.x * IO_BX + threadIdx.x;
-  const int j = blockIdx.y * IO_BY + threadIdx.y + 1;
-  const int k = blockIdx.z;
-  if (i >= nx || j > ny) return;
+__device__ __forceinline__ double io_prep_cell(TGDev d, IODev io, double gp, double zr, double den, int cur,
+                                               int do_drho, int i, int j, int k) {
+  const int ny = d.ny;
+  double drho_c = 0.0;
   const int64_t sy = d.sy, c = i + sy * j + d.sz * k;
   const int64_t oxp = xplus(d, i), oxm = xminus(d, i);
   const int64_t ozp = d.sz * (wrapp(k, d.nz) - k), ozm = d.sz * (wrapm(k, d.nz) - k);
@@ -490,7 +489,8 @@ __global__ void __launch_bounds__(IO_BX *IO_BY, VISC ? 1 : 8) k_io_prep(TGDev d,
     const double divx = (gx[c + oxp] - gx[c]) * d.dxi, divx0 = (hx[c + oxp] - hx[c]) * d.dxi;
     const double divy = (gy[c + sy] - gy[c]) * d.dyfi[j], divy0 = (hy[c + sy] - hy[c]) * d.dyfi[j];
     const double divz = (gz[c + ozp] - gz[c]) * d.dzi, divz0 = (hz[c + ozp] - hz[c]) * d.dzi;
-    io.drho[c] = (gp * (divx + divy + divz) + zr * (divx0 + divy0 + divz0)) / den;
+    drho_c = (gp * (divx + divy + divz) + zr * (divx0 + divy0 + divz0)) / den;
+    io.drho[c] = drho_c;
   }
   double rx = 1.0, ry = 1.0, rz = 1.0;
   if (io.thermal) {
@@ -516,7 +516,38 @@ __global__ void __launch_bounds__(IO_BX *IO_BY, VISC ? 1 : 8) k_io_prep(TGDev d,
   if (j == ny) {
     d.u[c + sy] = 0.0; d.w[c + sy] = 0.0; d.v[c + sy] = 0.0;
   }
+  return drho_c;
 }
+
+// mass_part (the coupled section): the block sums of DrhoDtP / DYFI, which
+// CHK_MassConsv_io's mass rate needs, go to d.partials in the order of
+// k_io_red_part (same bits), saving that kernel's pass over DrhoDtP.
+template <bool VISC>
+__global__ void __launch_bounds__(IO_BX *IO_BY, VISC ? 1 : 8) k_io_prep(TGDev d, IODev io, double gp, double zr, double den,
+                                                        int cur, int do_drho, int mass_part) {
+  const int nx = d.nx, ny = d.ny;
+  const int i = blockIdx.x * IO_BX + threadIdx.x;
+  const int j = blockIdx.y * IO_BY + threadIdx.y + 1;
+  const int k = blockIdx.z;
+  if (mass_part) {
+    __shared__ double red[IO_BX * IO_BY / 32];
+    double v = 0.0;
+    if (i < nx && j <= ny) v = io_prep_cell<VISC>(d, io, gp, zr, den, cur, do_drho, i, j, k) / d.dyfi[j];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int tid = threadIdx.x + IO_BX * threadIdx.y;
+    if ((tid & 31) == 0) red[tid >> 5] = v;
+    __syncthreads();
+    if (tid == 0) {
+      double sum = 0.0;
+      for (int q = 0; q < IO_BX * IO_BY / 32; ++q) sum += red[q];
+      d.partials[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = sum;
+    }
+    return;
+  }
+  if (i >= nx || j > ny) return;
+  io_prep_cell<VISC>(d, io, gp, zr, den, cur, do_drho, i, j, k);
+}
+
 
 // Staggered viscosities of MU_Staggered, formed on demand.  mustg1: x-face /
 // y-face edge, rows 2..ny, wall rows 1 and ny+1 from the ghost cells;
@@ -1238,7 +1269,7 @@ int mlp_grid(const chapsim_ctx *c, int per_sm) {
 }
 
 int io_np_eng_bc(chapsim_ctx *c, int ns);
-int io_np_mom(chapsim_ctx *c, int ns);
+int io_np_mom(chapsim_ctx *c, int ns, bool mass_parts);
 
 // Phase-timer slots of an IO substep, in execution order: 0 energy RHS,
 // 1 property update + wall ghosts, 2 prep (DrhoDtP, u = G / rho), 3 momentum
@@ -1289,13 +1320,14 @@ int io_mom(chapsim_ctx *c, int ns, bool prep) {
   phase_mark(c, 2);
   if (prep) {
     if (io.visc)
-      k_io_prep<true><<<grid, blk, 0, c->stream>>>(d, io, sp.gam + sp.roh, sp.roh, sp.gam - 2.0, cur, io.thermal);
+      k_io_prep<true><<<grid, blk, 0, c->stream>>>(d, io, sp.gam + sp.roh, sp.roh, sp.gam - 2.0, cur, io.thermal, 0);
     else
-      k_io_prep<false><<<grid, blk, 0, c->stream>>>(d, io, sp.gam + sp.roh, sp.roh, sp.gam - 2.0, cur, io.thermal);
+      k_io_prep<false><<<grid, blk, 0, c->stream>>>(d, io, sp.gam + sp.roh, sp.roh, sp.gam - 2.0, cur, io.thermal,
+                                                     c->xnp ? 1 : 0);
     LAUNCHED();
   }
   phase_mark(c, 3);
-  if (c->xnp) return io_np_mom(c, ns);
+  if (c->xnp) return io_np_mom(c, ns, prep);
   int npart = (int)(grid.x * grid.y * grid.z);
   if (io.visc) {
     // semi-implicit scheme: RHS_io of the three components, DPGRNS, factored
@@ -1409,7 +1441,7 @@ int io_restart_fields(chapsim_ctx *c) {
   dim3 g2((d.nx + IO_BX - 1) / IO_BX, (d.ny + 2 + IO_BY - 1) / IO_BY, d.nz);
   k_io_props_only<<<g2, dim3(IO_BX, IO_BY), 0, c->stream>>>(d, c->io);
   LAUNCHED();
-  k_io_prep<false><<<cell_grid(d), dim3(IO_BX, IO_BY), 0, c->stream>>>(d, c->io, 0.0, 0.0, 1.0, c->io_cur, 0);
+  k_io_prep<false><<<cell_grid(d), dim3(IO_BX, IO_BY), 0, c->stream>>>(d, c->io, 0.0, 0.0, 1.0, c->io_cur, 0, 0);
   LAUNCHED();
   return CHAPSIM_OK;
 }
@@ -1488,6 +1520,7 @@ __global__ void __launch_bounds__(1024) k_bc_umax(TGDev d, IODev io, int slot) {
   const int nx = d.nx, ny = d.ny;
   const double *uo = bplane(io, CHAPSIM_P_OUT_U);
   double mx = -1.0e20, mn = 1.0e20;
+#pragma unroll 8
   for (int t = threadIdx.x; t < ny * d.nz; t += blockDim.x) {
     const int k = t / ny, j = t - k * ny + 1;
     const double ucc = (d.u[(nx - 1) + d.sy * j + d.sz * k] + uo[j + (ny + 2) * k]) * 0.5;
@@ -1542,6 +1575,7 @@ __global__ void __launch_bounds__(1024) k_bc_mass(TGDev d, IODev io, int cur) {
   const int ny = d.ny;
   const double *go = bplane(io, CHAPSIM_P_OUT_GX);
   double fin = 0.0, fout = 0.0;
+#pragma unroll 8
   for (int t = threadIdx.x; t < ny * d.nz; t += blockDim.x) {
     const int k = t / ny, j = t - k * ny + 1;
     const double coe2 = 1.0 / d.dyfi[j];
@@ -1808,7 +1842,7 @@ int io_bc_inlet(chapsim_ctx *c, const chapsim_ctx *tg) {
   return CHAPSIM_OK;
 }
 
-int io_bc_outlet_mom(chapsim_ctx *c, int ns) {
+int io_bc_outlet_mom(chapsim_ctx *c, int ns, bool mass_parts) {
   TGDev &d = c->d;
   const SubParams &sp = c->sp[ns];
   const int np = d.ny * d.nz, nall = (d.ny + 2) * d.nz;
@@ -1816,10 +1850,13 @@ int io_bc_outlet_mom(chapsim_ctx *c, int ns) {
   LAUNCHED();
   k_bc_outlet_conv<<<(np + 255) / 256, 256, 0, c->stream>>>(d, c->io, sp.gam, sp.roh, c->io_cur);
   LAUNCHED();
-  // sum of DrhoDtP / DYFI over the interior into d.scal[1]
+  // sum of DrhoDtP / DYFI over the interior into d.scal[1] (its block sums
+  // already in d.partials when the substep's k_io_prep formed them)
   const dim3 grid = cell_grid(d), blk(IO_BX, IO_BY);
-  k_io_red_part<<<grid, blk, 0, c->stream>>>(d, c->io, 1, c->io_cur, c->io.drho);
-  LAUNCHED();
+  if (!mass_parts) {
+    k_io_red_part<<<grid, blk, 0, c->stream>>>(d, c->io, 1, c->io_cur, c->io.drho);
+    LAUNCHED();
+  }
   k_io_red_final<<<1, 1024, 0, c->stream>>>(d, 1, (int)(grid.x * grid.y * grid.z));
   LAUNCHED();
   k_bc_mass<<<1, 1024, 0, c->stream>>>(d, c->io, c->io_cur);
@@ -1873,7 +1910,7 @@ int io_np_divg(chapsim_ctx *c, int ns, int buf) {
 // the IO arrays (the coupled branch of :116-121 solves on the TG arrays; the
 // IO-only branch's arrays are used), PRCALC_io and MASSFLUX_UPDATE_IO with
 // the outlet face.
-int io_np_mom(chapsim_ctx *c, int ns) {
+int io_np_mom(chapsim_ctx *c, int ns, bool mass_parts) {
   TGDev &d = c->d;
   IODev &io = c->io;
   if (!c->inlet) {
@@ -1888,7 +1925,7 @@ int io_np_mom(chapsim_ctx *c, int ns) {
   LAUNCHED();
   int rc = io_bc_inlet(c, c->inlet);
   if (rc) return rc;
-  if ((rc = io_bc_outlet_mom(c, ns))) return rc;
+  if ((rc = io_bc_outlet_mom(c, ns, mass_parts))) return rc;
   k_np_mom_post<<<nb, 256, 0, c->stream>>>(d, io, cur);
   LAUNCHED();
   if (c->use_tma_io) {
