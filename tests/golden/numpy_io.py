@@ -280,8 +280,33 @@ class IO(TG):
         """SOLVERRK3_MOM_IO: convection + explicit viscous terms, RHS_MOM_EXPLICIT_io
         with the constant-mass-flux gradient, MASSFLUX_CALC_IO, DIVG_io, the
         FISHPACK Poisson solve, PRCALC_io, MASSFLUX_UPDATE_IO."""
-        ny, X, row = self.ny, self.X, self.row
         self.g0 = {c: self.g[c].copy() for c in (1, 2, 3)}
+        ex, ey, ez, ex_conv, ey_conv, ez_conv = self.mom_terms()
+        ny, X, row = self.ny, self.X, self.row
+        gx, gy, gz = self.g[1], self.g[2], self.g[3]
+        dycj, dxi, dzi = row(self.dyci), self.dxi, self.dzi
+        if self.visc:
+            self.mom_semi_implicit(ns, ex_conv, ey_conv, ez_conv)
+            return
+        # RK3 combination and pressure gradient
+        p, dt, alp = self.p, self.dt, TALP[ns]
+        rx = (TGAM[ns] * ex + TROH[ns] * X(self.ex0[1])) * dt - (X(p) - X(p, -1)) * (alp * dt * dxi)
+        ry = (TGAM[ns] * ey + TROH[ns] * X(self.ex0[2])) * dt - (X(p) - X(p, 0, -1)) * (alp * dt * dycj)
+        rz = (TGAM[ns] * ez + TROH[ns] * X(self.ex0[3])) * dt - (X(p) - X(p, 0, 0, -1)) * (alp * dt * dzi)
+        self.interior(self.ex0[1], ex)
+        self.interior(self.ex0[3], ez)
+        self.ex0[2][:, 2:ny + 1, :] = ey[:, 1:, :]
+        rx = rx - np.sum(rx / row(self.dyfi)) / self.volm  # DPGRNS: constant mass flux
+        gx[:, 1:ny + 1, :] += rx
+        gz[:, 1:ny + 1, :] += rz
+        gy[:, 2:ny + 1, :] += ry[:, 1:, :]
+        self.bc_vec(self.g)
+        self.project(ns)
+
+    def mom_terms(self):
+        """The convection + explicit viscous terms of the three momentum
+        components on the interior (with the bare convection terms)."""
+        ny, X, row = self.ny, self.X, self.row
         u, v, w = self.q[1], self.q[2], self.q[3]
         gx, gy, gz = self.g[1], self.g[2], self.g[3]
         wff, wfb, wffp, wfbp = row(self.wff), row(self.wfb), row(self.wff, 1), row(self.wfb, 1)
@@ -334,23 +359,7 @@ class IO(TG):
                S3() * ((X(w) - X(w, 0, -1)) * dycj + (X(v) - X(v, 0, 0, -1)) * dzi)) * (dyfj * cv)
         d33 = (M() * ((X(w, 0, 0, 1) - X(w)) * dzi - divu()) - M(0, 0, -1) * ((X(w) - X(w, 0, 0, -1)) * dzi - divu(0, 0, -1))) * (2.0 * dzi * cv)
         ez_conv, ez = ez, ez + d31 + d32 + d33
-        if self.visc:
-            self.mom_semi_implicit(ns, ex_conv, ey_conv, ez_conv)
-            return
-        # RK3 combination and pressure gradient
-        p, dt, alp = self.p, self.dt, TALP[ns]
-        rx = (TGAM[ns] * ex + TROH[ns] * X(self.ex0[1])) * dt - (X(p) - X(p, -1)) * (alp * dt * dxi)
-        ry = (TGAM[ns] * ey + TROH[ns] * X(self.ex0[2])) * dt - (X(p) - X(p, 0, -1)) * (alp * dt * dycj)
-        rz = (TGAM[ns] * ez + TROH[ns] * X(self.ex0[3])) * dt - (X(p) - X(p, 0, 0, -1)) * (alp * dt * dzi)
-        self.interior(self.ex0[1], ex)
-        self.interior(self.ex0[3], ez)
-        self.ex0[2][:, 2:ny + 1, :] = ey[:, 1:, :]
-        rx = rx - np.sum(rx / dyfj) / self.volm  # DPGRNS: constant mass flux
-        gx[:, 1:ny + 1, :] += rx
-        gz[:, 1:ny + 1, :] += rz
-        gy[:, 2:ny + 1, :] += ry[:, 1:, :]
-        self.bc_vec(self.g)
-        self.project(ns)
+        return ex, ey, ez, ex_conv, ey_conv, ez_conv
 
     def project(self, ns):
         """DIVG_io, the FISHPACK solve, PRCALC_io (the semi-implicit branch with
@@ -770,3 +779,309 @@ def io_stats(f, dxi, dzi, dyfi, dyci, thermal):
     else:
         vals += [zero] * 219
     return np.stack([a.sum(axis=(0, 2)) / (nx * nz) for a in vals], axis=1)
+
+
+class IOCoupled(IO):
+    """The coupled inflow / outflow section (TGFLOWFLG: non-periodic BCX_io),
+    a numpy restatement written beside the C++ oracle's.  Arrays carry the x
+    ghost columns: shape (nz, ny + 2, nx + 2), a[k-1, j, i] is F(i, j, k) for
+    i = 0 .. NCL1_io + 1 (src/MEMALLOCT.f90:154-168); x neighbours do not wrap
+    (src/INDEXSET.f90:25-32).  Per substep (src/SOLVE.f90:119-134 with
+    src/SOLVERRK3_MOM_IO.f90:15-168 and src/SOLVERRK3_ENG_IO.f90:57-64):
+    BC_TINLET_FLOW from the TG arrays set by set_inlet (src/BC_INLET.f90:2-51),
+    BC_COUTLET_MOM_RK3 with CONVCTION_OUTLET_U and CHK_MassConsv_io
+    (src/BC_COUTLET_MOM_RK3.f90:2-174, src/processing/CHK_conservation.f90:
+    2-71), the x-momentum from the second face (NXI = 2) without the constant
+    mass-flux forcing, MU_STG = 1 on the ghost faces, DIVG_io and
+    FISHPACK_POIS3D_SIMPLE on the IO arrays with the x transform of BCX_io
+    (here: the documented FFTPACK sums as dense matrices), PRCALC_io, and
+    MASSFLUX_UPDATE_IO from the second face to the outlet face against
+    DPH_io(NCL1_io + 1) = 0 (src/VELO_CORRECTION.f90:124-139); the energy
+    substep adds BC_TINLET_THERML (src/BC_INLET.f90:54-76) and
+    BC_COUTLET_ENEG_RK3 (src/BC_COUTLET_ENEG_RK3.f90:2-41).  The shared
+    decisions: the initial outlet ghost column is a copy of the last interior
+    column; the boundary operators' RK3 memory starts at zero."""
+
+    LP = {(1, 1): 2, (1, 2): 3, (2, 2): 4, (2, 1): 5}
+
+    def __init__(self, nx, ny, nz, lx, lz, bcx=(2, 1), **kw):
+        super().__init__(nx, ny, nz, lx, lz, **kw)
+        self._mesh = dict(nx=nx, ny=ny, nz=nz, lx=lx, lz=lz,
+                          **{k: kw[k] for k in ("str2", "istr2", "ren", "dt") if k in kw})
+        shape = (nz, ny + 2, nx + 2)
+        z = lambda: np.zeros(shape)
+        self.q = [None] + [z() for _ in range(3)]
+        self.p, self.phi = z(), z()
+        self.g = {c: z() for c in (1, 2, 3)}
+        self.g0 = {c: z() for c in (1, 2, 3)}
+        self.ex0 = {c: z() for c in (1, 2, 3)}
+        self.drho, self.rhoh, self.h, self.rhse0 = z(), z(), z(), z()
+        self.T, self.D, self.D0, self.mu, self.mu0, self.k = (np.ones(shape) for _ in range(6))
+        self.lp = self.LP[tuple(bcx)]
+        self.conv0 = {c: np.zeros((nz, ny + 2)) for c in (1, 2, 3)}
+        self.conv0_eng = np.zeros((nz, ny + 2))
+        self.tg = None
+        self.bcs = {}
+
+    def set_inlet(self, tu, tv, tw, tp):
+        """The TG section's u, v, w, p, (nz, ny + 2, nx_tg)."""
+        self.tg = [np.array(a, dtype=float) for a in (tu, tv, tw, tp)]
+
+    # ---------------------------------------------------------- layout
+    def X(self, a, di=0, dj=0, dk=0):
+        b = np.roll(a, -dk, axis=0) if dk else a
+        return b[:, 1 + dj:self.ny + 1 + dj, 1 + di:self.nx + 1 + di]
+
+    def interior(self, a, val):
+        a[:, 1:self.ny + 1, 1:self.nx + 1] = val
+
+    def bc_vec(self, f):
+        ny, c = self.ny, slice(1, self.nx + 1)
+        f[1][:, 0, c] = 0.0; f[3][:, 0, c] = 0.0; f[2][:, 1, c] = 0.0; f[2][:, 0, c] = 0.0
+        f[1][:, ny + 1, c] = 0.0; f[3][:, ny + 1, c] = 0.0; f[2][:, ny + 1, c] = 0.0
+
+    def bc_copy(self, f):
+        c = slice(1, self.nx + 1)
+        f[:, 0, c] = f[:, 1, c]
+        f[:, self.ny + 1, c] = f[:, self.ny, c]
+
+    def mu_stg(self):
+        """MU_Staggered on IC = 1..NCL1_io; the ghost faces keep 1."""
+        ny, nx = self.ny, self.nx
+        m, m0 = self.mu, self.mu0
+        xm = lambda a: np.concatenate([np.zeros_like(a[..., :1]), a[..., :-1]], axis=2)
+        zm = lambda a: np.roll(a, 1, axis=0)
+        s1, s2, s3 = np.ones(m.shape), np.ones(m.shape), np.ones(m.shape)
+        ex = m + xm(m) + m0 + xm(m0)
+        ez = zm(m) + m + zm(m0) + m0
+        wf, wb = self.wff[2:ny + 1][None, :, None], self.wfb[2:ny + 1][None, :, None]
+        c = slice(1, nx + 1)
+        s1[:, 2:ny + 1, c] = ((ex[:, 2:ny + 1] * wf + ex[:, 1:ny] * wb) * 0.25)[..., c]
+        s3[:, 2:ny + 1, c] = ((ez[:, 2:ny + 1] * wf + ez[:, 1:ny] * wb) * 0.25)[..., c]
+        s2[:, 1:ny + 1, c] = ((m + xm(m) + m0 + xm(m0) + zm(m) + zm(xm(m)) + zm(m0) + zm(xm(m0)))[:, 1:ny + 1] * 0.125)[..., c]
+        for s in (s1, s3):
+            s[:, 1, c] = 0.5 * (m0[:, 0, c] + m[:, 0, c])
+            s[:, ny + 1, c] = 0.5 * (m0[:, ny + 1, c] + m[:, ny + 1, c])
+        return s1, s2, s3
+
+    def wall_thermal(self):
+        """BC_WALL_THERMAL(IMAIND): the interior columns."""
+        ny, c, h = self.ny, slice(1, self.nx + 1), self.h
+        hb = 2.0 * h[:, 1, c] - self.wff[2] * h[:, 2, c] - self.wfb[2] * h[:, 1, c]
+        ht = 2.0 * h[:, ny, c] - self.wff[ny] * h[:, ny, c] - self.wfb[ny] * h[:, ny - 1, c]
+        for j, hg in ((0, hb), (ny + 1, ht)):
+            T, D, M, K = self.table_props(hg)
+            self.h[:, j, c], self.T[:, j, c], self.D[:, j, c], self.mu[:, j, c], self.k[:, j, c] = hg, T, D, M, K
+            self.rhoh[:, j, c] = hg * D
+
+    # ---------------------------------------------------------- boundary operators
+    def u_outlet(self):
+        """CONVCTION_OUTLET_U: (max + min) / 2 of 0.5 (u(NCL1) + u(NCL1 + 1))."""
+        ny, nx = self.ny, self.nx
+        ucc = 0.5 * (self.q[1][:, 1:ny + 1, nx] + self.q[1][:, 1:ny + 1, nx + 1])
+        return 0.5 * (ucc.max() + ucc.min())
+
+    def inlet(self):
+        tu, tv, tw, tp = self.tg
+        q, g = self.q, self.g
+        q[1][:, :, 0], q[2][:, :, 0], q[3][:, :, 0] = tu[:, :, -1], tv[:, :, -1], tw[:, :, -1]
+        g[1][:, :, 0], g[2][:, :, 0], g[3][:, :, 0] = tu[:, :, -1] * 1.0, tv[:, :, -1] * 1.0, tw[:, :, -1] * 1.0
+        q[1][:, :, 1] = tu[:, :, 0]
+        g[1][:, :, 1] = q[1][:, :, 1] * (1.0 + self.D[:, :, 1]) * 0.5
+        self.p[:, :, 0] = tp[:, :, -1]
+        self.D[:, :, 0] = 1.0
+
+    def outlet_mom(self, ns):
+        ny, nx = self.ny, self.nx
+        U = self.u_outlet()
+        coe1 = self.dxi * U
+        rho = lambda: (self.D[:, :, nx] + self.D[:, :, nx + 1]) * 0.5
+        for c in (1, 2, 3):
+            j0 = 2 if c == 2 else 1
+            go, gi = self.g[c][:, j0:ny + 1, nx + 1], self.g[c][:, j0:ny + 1, nx]
+            conv = -(go - gi) * coe1
+            rhs = TGAM[ns] * conv + TROH[ns] * self.conv0[c][:, j0:ny + 1]
+            self.conv0[c][:, j0:ny + 1] = conv
+            self.g[c][:, j0:ny + 1, nx + 1] = go + self.dt * rhs
+            self.q[c][:, j0:ny + 1, nx + 1] = self.g[c][:, j0:ny + 1, nx + 1] / rho()[:, j0:ny + 1]
+        w = 1.0 / self.dyfi[1:ny + 1][None, :]
+        fin = np.sum(self.g[1][:, 1:ny + 1, 1] * w) / self.dzi
+        fout = np.sum(self.g[1][:, 1:ny + 1, nx + 1] * w) / self.dzi
+        mass = np.sum(self.X(self.drho) / self.row(self.dyfi)) / self.dzi / self.dxi
+        scaling = (fin - mass) / fout
+        self.bcs.update(u_outlet=U, scaling=scaling, inflow=fin, outflow=fout, mass_rate=mass)
+        gn = self.g[1][:, 1:ny + 1, nx + 1]
+        self.g[1][:, 1:ny + 1, nx + 1] = gn * (scaling - 1.0) + gn
+        self.q[1][:, 1:ny + 1, nx + 1] = self.g[1][:, 1:ny + 1, nx + 1] / rho()[:, 1:ny + 1]
+        for f in (self.g, self.q):  # BC_WALL_G_io / BC_WALL_Q_io on the outlet column
+            f[1][:, 0, nx + 1] = 0.0; f[3][:, 0, nx + 1] = 0.0; f[2][:, 1, nx + 1] = 0.0; f[2][:, 0, nx + 1] = 0.0
+            f[1][:, ny + 1, nx + 1] = 0.0; f[2][:, ny + 1, nx + 1] = 0.0; f[3][:, ny + 1, nx + 1] = 0.0
+
+    def outlet_eng(self, ns):
+        ny, nx = self.ny, self.nx
+        U = self.u_outlet()
+        rh = self.rhoh[:, 1:ny + 1, nx + 1]
+        conv = -self.dxi * U * (rh - self.rhoh[:, 1:ny + 1, nx])
+        rhs = TGAM[ns] * conv + TROH[ns] * self.conv0_eng[:, 1:ny + 1]
+        self.conv0_eng[:, 1:ny + 1] = conv
+        rh = rh + self.dt * rhs
+        self.rhoh[:, 1:ny + 1, nx + 1] = rh
+        D = self.td(self.ht(rh / self.D[:, 1:ny + 1, nx + 1]))
+        h = rh / D
+        T, D, M, K = self.table_props(h)
+        for a, v in ((self.h, h), (self.T, T), (self.D, D), (self.mu, M), (self.k, K)):
+            a[:, 1:ny + 1, nx + 1] = v
+        hh = self.h[:, :, nx + 1]
+        for j, hg in ((0, 2.0 * hh[:, 1] - self.wff[2] * hh[:, 2] - self.wfb[2] * hh[:, 1]),
+                      (ny + 1, 2.0 * hh[:, ny] - self.wff[ny] * hh[:, ny] - self.wfb[ny] * hh[:, ny - 1])):
+            T, D, M, K = self.table_props(hg)
+            self.h[:, j, nx + 1], self.T[:, j, nx + 1], self.D[:, j, nx + 1] = hg, T, D
+            self.mu[:, j, nx + 1], self.k[:, j, nx + 1], self.rhoh[:, j, nx + 1] = M, K, hg * D
+
+    # ---------------------------------------------------------- substeps
+    def eng(self, ns):
+        super().eng(ns)
+        for a, val in ((self.T, 1.0), (self.k, 1.0), (self.D, 1.0), (self.mu, 1.0), (self.rhoh, 0.0), (self.h, 0.0)):
+            a[:, :, 0] = val  # BC_TINLET_THERML
+        self.outlet_eng(ns)
+
+    def prep(self, ns):
+        if self.thermal:
+            self.interior(self.drho, ((TGAM[ns] + TROH[ns]) * self.div(self.g) + TROH[ns] * self.div(self.g0)) /
+                          (TGAM[ns] - 2.0))
+        X, G, c = self.X, self.g, slice(1, self.nx + 1)
+        rx, ry, rz = self.rho_stg()
+        self.interior(self.q[1], X(G[1]) / rx)
+        self.interior(self.q[3], X(G[3]) / rz)
+        self.q[2][:, 2:self.ny + 1, c] = (X(G[2]) / ry)[:, 1:, :]
+        self.bc_vec(self.q)
+
+    def mom(self, ns):
+        ny, nx, X, row = self.ny, self.nx, self.X, self.row
+        self.g0 = {c: self.g[c].copy() for c in (1, 2, 3)}
+        self.inlet()
+        self.outlet_mom(ns)
+        ex, ey, ez, _, _, _ = self.mom_terms()
+        p, dt, alp, dxi, dzi, dycj = self.p, self.dt, TALP[ns], self.dxi, self.dzi, row(self.dyci)
+        rx = (TGAM[ns] * ex + TROH[ns] * X(self.ex0[1])) * dt - (X(p) - X(p, -1)) * (alp * dt * dxi)
+        ry = (TGAM[ns] * ey + TROH[ns] * X(self.ex0[2])) * dt - (X(p) - X(p, 0, -1)) * (alp * dt * dycj)
+        rz = (TGAM[ns] * ez + TROH[ns] * X(self.ex0[3])) * dt - (X(p) - X(p, 0, 0, -1)) * (alp * dt * dzi)
+        c, c2 = slice(1, nx + 1), slice(2, nx + 1)  # all faces, faces from the second (NXI = 2)
+        self.ex0[1][:, 1:ny + 1, c2] = ex[:, :, 1:]
+        self.ex0[3][:, 1:ny + 1, c] = ez
+        self.ex0[2][:, 2:ny + 1, c] = ey[:, 1:, :]
+        self.g[1][:, 1:ny + 1, c2] += rx[:, :, 1:]
+        self.g[3][:, 1:ny + 1, c] += rz
+        self.g[2][:, 2:ny + 1, c] += ry[:, 1:, :]
+        self.bc_vec(self.g)
+        self.project(ns)
+
+    def project(self, ns):
+        ny, nx, X, row = self.ny, self.nx, self.X, self.row
+        p, dt, alp = self.p, self.dt, TALP[ns]
+        rhs = (self.div(self.g) + X(self.drho)) / (dt * alp)
+        self.phi[:] = 0.0
+        self.interior(self.phi, self.poisson_io(rhs))
+        self.bc_copy(self.phi)
+        self.interior(p, X(p) + X(self.phi))
+        self.bc_copy(p)
+        f, c, c2 = self.phi, slice(1, nx + 1), slice(2, nx + 2)
+        # x flux from the second face to the outlet face: f(i) - f(i - 1) with f(NCL1 + 1) = 0
+        fx = f[:, 1:ny + 1, 1:nx + 2] - f[:, 1:ny + 1, 0:nx + 1]
+        self.g[1][:, 1:ny + 1, c2] -= fx[:, :, 1:] * (dt * alp * self.dxi)
+        self.g[3][:, 1:ny + 1, c] -= (X(f) - X(f, 0, 0, -1)) * (dt * alp * self.dzi)
+        self.g[2][:, 2:ny + 1, c] -= ((X(f) - X(f, 0, -1)) * (dt * alp * row(self.dyci)))[:, 1:, :]
+        self.bc_vec(self.g)
+
+    def poisson_io(self, rhs):
+        """FISHPACK_POIS3D_SIMPLE with the x transform of LP as the matrices of
+        FFTPACK's documented sums, complex FFTs in z, banded y solves."""
+        nx, ny, nz, lp = self.nx, self.ny, self.nz, self.lp
+        n = nx
+        i = np.arange(1, n + 1)[:, None]
+        k = np.arange(1, n + 1)[None, :]
+        lrdel = ((lp - 1) * (lp - 3) * (lp - 5)) // 3
+        sc = n + lrdel
+        di = {2: 0.0, 3: 0.5, 4: 1.0, 5: 0.5}[lp]
+        xrt = -4.0 * self.dxi ** 2 * np.sin((np.arange(1, n + 1) - di) * np.pi / (2.0 * sc)) ** 2
+        scalx = 4.0 * sc if lp in (3, 5) else 2.0 * sc
+        sign = np.where((i - 1) % 2 == 1, -1.0, 1.0)
+        if lp == 2:
+            fw = 2.0 * np.sin(k * i * np.pi / (n + 1)); bw = fw
+        elif lp == 3:
+            fw = np.where(k == n, sign, 2.0 * np.sin((2.0 * i - 1.0) * k * np.pi / (2.0 * n)))
+            bw = 4.0 * np.sin((2.0 * k - 1.0) * i * np.pi / (2.0 * n))
+        elif lp == 4:
+            fw = np.where(k == 1, 1.0, np.where(k == n, sign, 2.0 * np.cos((k - 1) * (i - 1) * np.pi / (n - 1)))); bw = fw
+            xrt[0] = 0.0
+        else:
+            fw = np.where(k == 1, 1.0, 2.0 * np.cos((2.0 * i - 1.0) * (k - 1) * np.pi / (2.0 * n)))
+            bw = 4.0 * np.cos((2.0 * k - 1.0) * (i - 1) * np.pi / (2.0 * n))
+        X = np.einsum('ik,zjk->zji', fw, rhs)           # (kz, j, x-mode)
+        F = np.fft.fft(X, axis=0)
+        lam_z = -4.0 * self.dzi ** 2 * np.sin(np.pi * np.arange(nz) / nz) ** 2
+        am, ac, ap = self.amph[1:ny + 1], self.acph[1:ny + 1], self.apph[1:ny + 1]
+        out = np.zeros_like(F)
+        ab = np.zeros((3, ny), dtype=complex)
+        ab[0, 1:] = ap[:-1]
+        ab[2, :-1] = am[1:]
+        for a in range(nz):
+            for b in range(nx):
+                ab[1] = ac + xrt[b] + lam_z[a]
+                if xrt[b] == 0.0 and a == 0:
+                    out[a, :-1, b] = solve_banded((1, 1), ab[:, :-1], F[a, :-1, b])
+                else:
+                    out[a, :, b] = solve_banded((1, 1), ab, F[a, :, b])
+        Y = np.real(np.fft.ifft(out, axis=0))
+        return np.einsum('ik,zjk->zji', bw, Y) / (scalx * nz) * nz
+
+    def init_random(self, seed, amp):
+        """The x-periodic recipe on the interior (velocity, unit bulk mass
+        flux), the outlet ghost column a copy of the last interior column, then
+        the coupled NS = 0 projection."""
+        base = IO(thermal=0, **self._mesh)
+        TG.init_random(base, seed, amp)  # the TG velocity recipe on the interior layout
+        ny, nx = self.ny, self.nx
+        if self.thermal:
+            T0, D0, M0, K0 = (float(x[0]) for x in self.table_props(np.array([0.0])))
+        else:
+            T0 = D0 = M0 = K0 = 1.0
+        for a, val in ((self.T, T0), (self.D, D0), (self.D0, D0), (self.mu, M0), (self.mu0, M0), (self.k, K0)):
+            a[:] = val
+        for a in (self.h, self.rhoh, self.rhse0, self.drho, self.p, self.phi):
+            a[:] = 0.0
+        for c in (1, 2, 3):
+            self.conv0[c][:] = 0.0
+            self.g0[c][:] = 0.0
+            self.ex0[c][:] = 0.0
+        self.conv0_eng[:] = 0.0
+        r_face = (D0 + D0 + D0 + D0) * 0.25
+        r_v = (self.wff * (D0 + D0) + self.wfb * (D0 + D0)) * 0.5
+        q = {c: base.q[c].copy() for c in (1, 2, 3)}
+
+        def velo2massflux():
+            g = {c: np.zeros_like(q[c]) for c in (1, 2, 3)}
+            g[1][:, 1:ny + 1] = q[1][:, 1:ny + 1] * r_face
+            g[3][:, 1:ny + 1] = q[3][:, 1:ny + 1] * r_face
+            g[2][:, 2:ny + 1] = q[2][:, 2:ny + 1] * r_v[2:ny + 1][None, :, None]
+            return g
+
+        g = velo2massflux()
+        gm = np.sum(g[1][:, 1:ny + 1] / self.row(self.dyfi)) / self.dzi / (self.area * nx)
+        for c in (1, 2, 3):
+            q[c] /= gm
+        g = velo2massflux()
+        for f in (q,):
+            f[1][:, 0] = 0.0; f[3][:, 0] = 0.0; f[2][:, 1] = 0.0; f[2][:, 0] = 0.0
+            f[1][:, ny + 1] = 0.0; f[3][:, ny + 1] = 0.0; f[2][:, ny + 1] = 0.0
+        for c in (1, 2, 3):
+            self.q[c][:] = 0.0
+            self.g[c][:] = 0.0
+            self.q[c][:, :, 1:nx + 1] = q[c]
+            self.g[c][:, :, 1:nx + 1] = g[c]
+            self.q[c][:, :, nx + 1] = q[c][:, :, nx - 1]
+            self.g[c][:, :, nx + 1] = g[c][:, :, nx - 1]
+        if self.thermal:
+            self.wall_thermal()
+            self.eng(0)
+        self.mom(0)

@@ -13,13 +13,23 @@ coupled branches (src/SOLVERRK3_MOM_IO.f90:15-168, src/SOLVERRK3_ENG_IO.f90:
   reported);
 * CHK_MassConsv_io: after the rescaling the outlet flux equals inflow minus
   the mass rate;
-* the x-periodic layout is untouched by the coupled one.
+* the x-periodic layout is untouched by the coupled one;
+and the whole coupled substep against the independent numpy restatement
+(`tests/golden/numpy_io.py`, `IOCoupled`: whole-array shifts, the x
+transforms as matrices of FFTPACK's sums with numpy einsum, complex numpy FFTs
+in z, scipy banded y solves, the boundary operators on the ghost columns),
+both fed the same TG fields every substep.
 """
 import math
+import os
+import sys
 
 import numpy as np
+import pytest
 
 from oracle.pyoracle import OracleIO, OracleTG
+
+sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
 
 TG_F = ("u", "v", "w", "p")
 
@@ -102,3 +112,49 @@ def test_periodic_layout_unchanged():
     assert o.get("u").shape == (8, 14, 18)
     o.set_bcx(3, 3)
     assert o.get("u").shape == (8, 14, 16)
+
+
+@pytest.mark.parametrize("table", ["constant", "synthetic", None])
+@pytest.mark.parametrize("bcx", [(2, 1), (1, 1)])
+def test_coupled_oracle_matches_numpy_restatement(table, bcx):
+    """The oracle's coupled section against the numpy restatement after the
+    initial field and two steps, both fed the TG oracle's fields every
+    substep: every field within 1e-10 relative (max |a - b| / max |b|)."""
+    from numpy_io import IOCoupled, synth_table
+    nxt, nxi, ny, nz = 16, 24, 16, 12
+    lz = 4 * math.pi / 3
+    thermal = 1 if table else 0
+    h = np.linspace(-1.0, 1.0, 4096)
+    one = np.ones_like(h)
+    tab = {"constant": [h, h.copy(), one, one.copy(), one.copy()], "synthetic": list(synth_table(4096)[:5]),
+           None: None}[table]
+    t = OracleTG(nxt, ny, nz, lx=4 * math.pi, lz=lz)
+    t.init_random(1, 0.1)
+    t.substep(0)
+    o = OracleIO(nxi, ny, nz, lx=8 * math.pi, lz=lz, thermal=thermal, table=tab)
+    o.set_bcx(*bcx)
+    n = IOCoupled(nxi, ny, nz, 8 * math.pi, lz, bcx=bcx, thermal=thermal, table=tab)
+
+    def feed():
+        f = [t.get(x) for x in TG_F]
+        o.set_inlet(*f)
+        n.set_inlet(*f)
+
+    feed()
+    o.init_random(2, 0.1)
+    n.init_random(2, 0.1)
+    for step in range(3):
+        if step:
+            for ns in (1, 2, 3):
+                t.substep(ns)
+                feed()
+                o.substep(ns)
+                n.substep(ns)
+        fields = [("u", n.q[1]), ("v", n.q[2]), ("w", n.q[3]), ("p", n.p), ("gx", n.g[1]), ("gy", n.g[2]),
+                  ("gz", n.g[3]), ("g0x", n.g0[1]), ("drho", n.drho)]
+        if thermal:
+            fields += [("h", n.h), ("t", n.T), ("rho", n.D), ("mu", n.mu), ("k", n.k), ("rhoh", n.rhoh)]
+        for name, a in fields:
+            b = o.get(name)
+            e = np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+            assert e <= 1e-10, (table, bcx, step, name, e)
