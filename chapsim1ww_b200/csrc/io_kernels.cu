@@ -1,9 +1,12 @@
-// IO-domain kernels: one RK3 substep of the x-periodic inflow/outflow channel
-// section with the explicit viscous scheme, variable density and viscosity,
-// and the energy equation with table properties.
+// IO-domain kernels: one RK3 substep of the inflow/outflow channel section,
+// x-periodic or coupled to a TG section (x ghost columns, the inlet and
+// convective outlet operators; the io_np_* functions at the end), with the
+// explicit viscous scheme, variable density and viscosity, and the energy
+// equation with table properties.
 //
 // Reference (CHAPSim1WW, paths relative to the project root), channel branch
-// (RCCI1 = RCCI2 = RNDI1 = 1), x periodic (IPV_io/IMV_io wrap):
+// (RCCI1 = RCCI2 = RNDI1 = 1), x periodic (IPV_io/IMV_io wrap) or not
+// (TGFLOWFLG, src/INDEXSET.f90:25-32):
 //   SOLVERRK3_ENG_IO        src/SOLVERRK3_ENG_IO.f90:1-77
 //   RHS_ENERGY_EXPLICIT     src/RHS_ENERGY_EXPLICIT.f90:1-150
 //   ENTHALPY/DENSITY_UPDATE, THERM_PROP_UPDATE, DENSITY_TIME_DERIVATION

@@ -1,4 +1,6 @@
-// CPU FP64 oracle for the CHAPSim IO-section substep (x-periodic channel).
+// CPU FP64 oracle for the CHAPSim IO-section substep (the x-periodic channel
+// section, and the section coupled to a TG section: x ghost columns, the
+// inlet and convective outlet operators, non-periodic Poisson in x).
 //
 // TEST INFRASTRUCTURE ONLY: the checker for the CUDA IO path.  The product
 // never links or calls it.  Parity against reference outputs is unpinned (the
@@ -7,7 +9,10 @@
 // Restates (paths relative to the CHAPSim1WW project root), channel branches
 // only, so RCCI1 = RCCI2 = RNDI1 = RNDI2 = 1 (src/COORDJR.f90:20-23), the
 // explicit viscous scheme (visthemflg = 0, src/readdata.ini:23), no weighted
-// pressure, x periodic (BCX_io = 3: IPV_io/IMV_io wrap, src/INDEXSET.f90:24-32):
+// pressure, x periodic (BCX_io = 3: IPV_io/IMV_io wrap, src/INDEXSET.f90:24-32)
+// or coupled (TGFLOWFLG: the ghost columns, NXI = 2, the boundary operators
+// below; src/SOLVERRK3_MOM_IO.f90:15-21, src/SOLVERRK3_ENG_IO.f90:57-64,
+// src/VELO_CORRECTION.f90:124-139, src/MEMALLOCT.f90:154-168):
 //   SOLVERRK3_ENG_IO        src/SOLVERRK3_ENG_IO.f90:1-77
 //   RHS_ENERGY_EXPLICIT     src/RHS_ENERGY_EXPLICIT.f90:1-150
 //   ENTHALPY/DENSITY_UPDATE, THERM_PROP_UPDATE, DENSITY_TIME_DERIVATION
