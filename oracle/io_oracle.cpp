@@ -69,6 +69,13 @@
 //    not formed.  The y ghosts of DRHOI_STG (periodic halo values there) are
 //    only ever multiplied by wall ghosts of G, which are zero; they are zero
 //    here.
+//  * Coupled section: the Poisson solve runs on the IO arrays (the
+//    reference's coupled branch passes the TG arrays,
+//    src/SOLVERRK3_MOM_IO.f90:116-121, which leaves the IO velocity
+//    unprojected); the initial outlet ghost column is a copy of the last
+//    interior column and the boundary operators' RK3 memory starts at zero;
+//    lines longer than 64 take the quarter-wave transforms (LP 3, 5)
+//    through the DFT (qwave_fast), shorter ones the documented sums.
 //  * Semi-implicit PRCALC_io subtracts BE * RHSLLPHI_io, but
 //    FISHPACK_POIS3D_SIMPLE has by then written its x/z-transformed right-hand
 //    side back into RHSLLPHI_io (src/possion3d_fishpack_reform.f90:456-463):
