@@ -700,10 +700,11 @@ def synthetic_table_cols(table5):
 # Coupled IO section (x ghost columns, the non-periodic Poisson transforms):
 # its phase kernels and algorithmic 8-byte values per cell.  The divergence
 # reads G and DrhoDtP and writes RHSLLPHI, which the forward x transform reads
-# and writes as nx complex modes per row (the real x modes in complex lines);
-# the z transforms and y-lines pass over nx complex values per row.
-IO_KERNEL_COUPLED = dict(IO_KERNEL, mom_rhs="k_io_rhs_tma (coupled layout)", fftx="k_np_divg + k_xnp_qfwd", ifftx="k_xnp_qbwd")
-IO_COUPLED_VALUES = dict(IO_VALUES_PER_CELL, fftx=8, fftz=4, ysolve=4, ifftz=4, ifftx=3)
+# and writes as nx real modes per row, two to a complex line; the z transforms
+# and y-lines pass over nx / 2 complex values per row.
+IO_KERNEL_COUPLED = dict(IO_KERNEL, mom_rhs="k_io_rhs_tma (coupled layout)", fftx="k_np_divg + k_xnp_qfwd",
+                         ysolve="k_ysolve_pair", ifftx="k_xnp_qbwd")
+IO_COUPLED_VALUES = dict(IO_VALUES_PER_CELL, fftx=7, fftz=2, ysolve=2, ifftz=2, ifftx=2)
 
 
 def io_phase_bytes_coupled(ph, nx, ny, nz):

@@ -1178,6 +1178,98 @@ __global__ void __launch_bounds__(256) k_ysolve_line(TGDev d) {
   }
 }
 
+// Poisson y-lines of the quarter-wave x transforms (LP 3 and 5), whose nx
+// real x modes sit two to a complex line: line p holds mode 2p in its real
+// and mode 2p + 1 in its imaginary part, so after the complex z transform
+// Z(kz) = A(kz) + i B(kz), with A and B the z transforms of the two real mode
+// planes (A(nz - kz) = conj A(kz), B likewise).  One thread takes rows kz and
+// nz - kz of line p: A = (Z(kz) + conj Z(nz - kz)) / 2 and B = (Z(kz) -
+// conj Z(nz - kz)) / 2i are solved with the pivots of modes 2p and 2p + 1
+// (q: the packed descriptor; s: the descriptor of nx single lines that holds
+// the pivots, whose shifts at kz and nz - kz are equal) and packed back into
+// both rows.  The forward sweep keeps g_A in row kz and g_B in row nz - kz;
+// rows 0 and nz / 2 are their own partners, where A and B are real and share
+// the row's one complex value.  These transforms have no zero shift, so no
+// mode is pinned.  Half the lines of the unpacked form go through the z
+// transforms and the y-lines.
+constexpr int YP = 8;
+__global__ void __launch_bounds__(128) k_ysolve_pair(TGDev q, TGDev s) {
+  const int ny = q.ny, nz = q.nz;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x, kz = blockIdx.y;
+  if (p >= q.lh) return;
+  const int kc = kz ? nz - kz : 0;
+  const bool self = kc == kz;
+  const int64_t st = q.lp, sp = s.lp;
+  double2 *__restrict__ Z1 = reinterpret_cast<double2 *>(q.spec) + p + st * ny * kz;
+  double2 *__restrict__ Z2 = reinterpret_cast<double2 *>(q.spec) + p + st * ny * kc;
+  // pivots of modes 2p and 2p + 1 side by side (16-byte aligned: sp even)
+  const double *__restrict__ PP = reinterpret_cast<const double *>(s.ypiv) + 2 * p + sp * ny * kz;
+  const double *__restrict__ HH = PP + sp * ny * s.nz;
+  double ar = 0.0, ai = 0.0, br = 0.0, bi = 0.0;
+  for (int j0 = 1; j0 <= ny; j0 += YP) {
+    double2 z1[YP], z2[YP], pv[YP];
+    double a[YP];
+#pragma unroll
+    for (int u = 0; u < YP; ++u) {
+      const int j = j0 + u;
+      if (j <= ny) {
+        z1[u] = Z1[st * (j - 1)];
+        z2[u] = Z2[st * (j - 1)];
+        pv[u] = __ldg(reinterpret_cast<const double2 *>(PP + sp * (j - 1)));
+        a[u] = q.amph[j];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < YP; ++u) {
+      const int j = j0 + u;
+      if (j <= ny) {
+        const double Ar = 0.5 * (z1[u].x + z2[u].x), Ai = 0.5 * (z1[u].y - z2[u].y);
+        const double Br = 0.5 * (z1[u].y + z2[u].y), Bi = -0.5 * (z1[u].x - z2[u].x);
+        if (j == 1) {
+          ar = Ar * pv[u].x; ai = Ai * pv[u].x;
+          br = Br * pv[u].y; bi = Bi * pv[u].y;
+        } else {
+          ar = (Ar - a[u] * ar) * pv[u].x; ai = (Ai - a[u] * ai) * pv[u].x;
+          br = (Br - a[u] * br) * pv[u].y; bi = (Bi - a[u] * bi) * pv[u].y;
+        }
+        if (self) {
+          Z1[st * (j - 1)] = make_double2(ar, br);  // ai = bi = 0 here
+        } else {
+          Z1[st * (j - 1)] = make_double2(ar, ai);
+          Z2[st * (j - 1)] = make_double2(br, bi);
+        }
+      }
+    }
+  }
+  // x_ny = g_ny; each row packed back: Z(kz) = A + i B, Z(nz - kz) = conj A + i conj B
+  Z1[st * (ny - 1)] = make_double2(ar - bi, ai + br);
+  if (!self) Z2[st * (ny - 1)] = make_double2(ar + bi, br - ai);
+  for (int j0 = ny - 1; j0 >= 1; j0 -= YP) {
+    double2 g1[YP], g2[YP], hv[YP];
+#pragma unroll
+    for (int u = 0; u < YP; ++u) {
+      const int j = j0 - u;
+      if (j >= 1) {
+        g1[u] = Z1[st * (j - 1)];
+        g2[u] = Z2[st * (j - 1)];
+        hv[u] = __ldg(reinterpret_cast<const double2 *>(HH + sp * (j - 1)));
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < YP; ++u) {
+      const int j = j0 - u;
+      if (j >= 1) {
+        const double gar = g1[u].x, gai = self ? 0.0 : g1[u].y;
+        const double gbr = self ? g1[u].y : g2[u].x, gbi = self ? 0.0 : g2[u].y;
+        ar = gar - hv[u].x * ar; ai = gai - hv[u].x * ai;
+        br = gbr - hv[u].y * br; bi = gbi - hv[u].y * bi;
+        Z1[st * (j - 1)] = make_double2(ar - bi, ai + br);
+        if (!self) Z2[st * (j - 1)] = make_double2(ar + bi, br - ai);
+      }
+    }
+  }
+}
+
 // Inverse real transform along x (src/possion3d_FFT99.f90:461-485): the
 // block's lb spectral rows (contiguous, pitch lp) arrive by one bulk copy;
 // pairs of rows are rebuilt as one complex Hermitian-extended line and
@@ -1751,14 +1843,14 @@ __global__ void __launch_bounds__(256) k_xnp_qfwd(TGDev d, TGDev s, FFTPlan pl, 
   }
   __syncthreads();
   const double2 *res = fft_lines<double2, BIG>(A, B, nl, nx, nx, rad, pl.nrad, pl.tw64, +1);
-  double2 *S = reinterpret_cast<double2 *>(s.spec);
+  double *S = reinterpret_cast<double *>(s.spec);
   for (int t = tid; t < nrow * nx; t += blockDim.x) {
     const int r = t / nx, m = t - r * nx;
     const int n = (m & 1) ? nx - 1 - (m >> 1) : (m >> 1);
     const double2 z = res[swz((r >> 1) * nx + n)];
     double y = (r & 1) ? z.y : z.x;
     if (sinq && (m & 1)) y = -y;
-    S[m + (int64_t)s.lp * ((jbeg + r - 1) + (int64_t)ny * k)] = make_double2(y * rscal, 0.0);
+    S[m + 2 * (int64_t)s.lp * ((jbeg + r - 1) + (int64_t)ny * k)] = y * rscal;  // mode m: line m / 2, part m % 2
   }
 }
 
@@ -1773,10 +1865,10 @@ __global__ void __launch_bounds__(256) k_xnp_qbwd(TGDev d, TGDev s, FFTPlan pl, 
   double *in = reinterpret_cast<double *>(smem_raw + align128(xq_cplx(nx, lb) * sizeof(double2)));
   double2 *B = reinterpret_cast<double2 *>(in);
   if (tid < 16) rad[tid] = pl.rad[tid];
-  const double2 *S = reinterpret_cast<const double2 *>(s.spec);
+  const double *S = reinterpret_cast<const double *>(s.spec);
   for (int t = tid; t < lb * nx; t += blockDim.x) {
     const int r = t / nx, m = t - r * nx;
-    double x = r < nrow ? S[m + (int64_t)s.lp * ((jbeg + r - 1) + (int64_t)ny * k)].x : 0.0;
+    double x = r < nrow ? S[m + 2 * (int64_t)s.lp * ((jbeg + r - 1) + (int64_t)ny * k)] : 0.0;
     if (sinq && (m & 1)) x = -x;  // SINQB: (-1)^n X_n
     in[t] = x;
   }
@@ -1844,40 +1936,49 @@ int xnp_pois3d(chapsim_ctx *c, bool mark) {
   const size_t smq = xq_smem_bytes(d.nx, lb);
   const dim3 qgrid((d.ny + lb - 1) / lb, d.nz);
   const int sinq = c->xnp == 3;
+  // the quarter-wave transforms' modes two to a complex line (nx even): nx / 2
+  // lines in the spectral array of s
+  TGDev qs = s;
+  qs.lh = d.nx / 2;
+  qs.lp = (qs.lh + 1) & ~1;
+  const TGDev &z = q ? qs : s;
   if (q && c->fft_big)
-    k_xnp_qfwd<true><<<qgrid, 256, smq, c->stream>>>(d, s, c->fx, c->xnp_qw, lb, sinq, c->xnp_rscal);
+    k_xnp_qfwd<true><<<qgrid, 256, smq, c->stream>>>(d, qs, c->fx, c->xnp_qw, lb, sinq, c->xnp_rscal);
   else if (q)
-    k_xnp_qfwd<false><<<qgrid, 256, smq, c->stream>>>(d, s, c->fx, c->xnp_qw, lb, sinq, c->xnp_rscal);
+    k_xnp_qfwd<false><<<qgrid, 256, smq, c->stream>>>(d, qs, c->fx, c->xnp_qw, lb, sinq, c->xnp_rscal);
   else
     k_xnp_fwd<<<rows, 128, sm, c->stream>>>(d, s, c->xnp_f);
   LAUNCHED();
   typedef Prec<double> P;
   const int lz = P::fftz_lz(d.nz);
-  const dim3 gz((s.lh + lz - 1) / lz, d.ny);
+  const dim3 gz((z.lh + lz - 1) / lz, d.ny);
   if (mark) phase_mark(c, CHAPSIM_PH_FFTZ);
   if (c->fft_big)
-    k_fftz<double, true><<<gz, 256, P::fftz_smem(d.nz, lz), c->stream>>>(s, c->fz, lz, -1);
+    k_fftz<double, true><<<gz, 256, P::fftz_smem(d.nz, lz), c->stream>>>(z, c->fz, lz, -1);
   else
-    k_fftz<double, false><<<gz, 256, P::fftz_smem(d.nz, lz), c->stream>>>(s, c->fz, lz, -1);
+    k_fftz<double, false><<<gz, 256, P::fftz_smem(d.nz, lz), c->stream>>>(z, c->fz, lz, -1);
   LAUNCHED();
   if (mark) phase_mark(c, CHAPSIM_PH_YSOLVE);
-  {
+  if (q) {
+    dim3 grid((qs.lh + 127) / 128, d.nz / 2 + 1);
+    k_ysolve_pair<<<grid, 128, 0, c->stream>>>(qs, s);
+  } else {
     const int bx = c->ys_bx;
     dim3 grid((s.lh + bx - 1) / bx, d.nz);
     k_ysolve_line<double><<<grid, bx, 0, c->stream>>>(s);
-    LAUNCHED();
   }
+  LAUNCHED();
   if (mark) phase_mark(c, CHAPSIM_PH_IFFTZ);
   if (c->fft_big)
-    k_fftz<double, true><<<gz, 256, P::fftz_smem(d.nz, lz), c->stream>>>(s, c->fz, lz, +1);
+    k_fftz<double, true><<<gz, 256, P::fftz_smem(d.nz, lz), c->stream>>>(z, c->fz, lz, +1);
   else
-    k_fftz<double, false><<<gz, 256, P::fftz_smem(d.nz, lz), c->stream>>>(s, c->fz, lz, +1);
+    k_fftz<double, false><<<gz, 256, P::fftz_smem(d.nz, lz), c->stream>>>(z, c->fz, lz, +1);
   LAUNCHED();
   if (mark) phase_mark(c, CHAPSIM_PH_IFFTX);
   if (q && c->fft_big)
-    k_xnp_qbwd<true><<<qgrid, 256, smq, c->stream>>>(d, s, c->fx, c->xnp_qw, lb, sinq);
+    k_xnp_qbwd<true><<<qgrid, 256, smq, c->stream>>>(d, qs, c->fx, c->xnp_qw, lb, sinq);
   else if (q)
-    k_xnp_qbwd<false><<<qgrid, 256, smq, c->stream>>>(d, s, c->fx, c->xnp_qw, lb, sinq);
+    k_xnp_qbwd<false><<<qgrid, 256, smq, c->stream>>>(d, qs, c->fx, c->xnp_qw, lb, sinq);
   else
     k_xnp_bwd<<<rows, 128, sm, c->stream>>>(d, s, c->xnp_b);
   LAUNCHED();
