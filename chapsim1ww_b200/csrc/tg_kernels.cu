@@ -1812,27 +1812,51 @@ __global__ void __launch_bounds__(128) k_xnp_bwd(TGDev d, TGDev s, const double 
 // the rows sit at an 8-byte offset in the coupled layout, so they are read
 // with plain loads.
 __host__ __device__ constexpr size_t xq_cplx(int nx, int lb) { return (((size_t)(lb / 2) * nx + 7) / 8) * 8; }
-__host__ __device__ constexpr size_t xq_smem_bytes(int nx, int lb) { return 2 * align128(xq_cplx(nx, lb) * sizeof(double2)); }
+// the second buffer holds lb input rows of nx + 2 values (ghost columns
+// included) first, the FFT scratch afterwards
+__host__ __device__ constexpr size_t xq_in_bytes(int nx, int lb) {
+  return align128(xq_cplx(nx, lb) * sizeof(double2)) > align128((size_t)lb * (nx + 2) * sizeof(double))
+             ? align128(xq_cplx(nx, lb) * sizeof(double2))
+             : align128((size_t)lb * (nx + 2) * sizeof(double));
+}
+__host__ __device__ constexpr size_t xq_smem_bytes(int nx, int lb) {
+  return align128(xq_cplx(nx, lb) * sizeof(double2)) + xq_in_bytes(nx, lb);
+}
 
 template <bool BIG>
 __global__ void __launch_bounds__(256) k_xnp_qfwd(TGDev d, TGDev s, FFTPlan pl, const double2 *__restrict__ qw, int lb,
                                                   int sinq, double rscal) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ int rad[16];
+  __shared__ uint64_t bar;
   const int nx = d.nx, ny = d.ny, k = blockIdx.y, jbeg = 1 + blockIdx.x * lb;
   const int nrow = min(lb, ny - jbeg + 1), nl = lb / 2, tid = threadIdx.x;
+  const int sy = d.sy;  // nx + 2: rows from the inlet ghost column, one value before the field pointer
   double2 *A = reinterpret_cast<double2 *>(smem_raw);
   double *in = reinterpret_cast<double *>(smem_raw + align128(xq_cplx(nx, lb) * sizeof(double2)));
   double2 *B = reinterpret_cast<double2 *>(in);  // FFT scratch once A is filled
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
   if (tid < 16) rad[tid] = pl.rad[tid];
-  for (int t = tid; t < lb * nx; t += blockDim.x) {
-    const int r = t / nx, i = t - r * nx;
-    in[t] = r < nrow ? d.rhsphi[d.sy * (jbeg + r) + d.sz * k + i] : 0.0;
+  __syncthreads();
+  // the block's rows of RHSLLPHI by one bulk copy each ((nx + 2) * 8 bytes,
+  // 16-byte aligned: nx is even and the allocation starts at the ghost column)
+  const uint32_t rowb = (uint32_t)(sy * sizeof(double));
+  if (tid == 0) mbar_expect_tx(&bar, rowb * (uint32_t)nrow);
+  __syncthreads();
+  const double *src = d.rhsphi - 1 + (int64_t)d.sz * k + (int64_t)sy * jbeg;
+  for (int r = tid; r < nrow; r += blockDim.x) bulk_g2s(in + (size_t)r * sy, src + (int64_t)sy * r, rowb, &bar);
+  for (int t = tid; t < (lb - nrow) * sy; t += blockDim.x) in[(size_t)nrow * sy + t] = 0.0;
+  if (!mbar_wait(&bar, 0, d.err)) {
+    mbar_wait(&bar, 0, d.err);  // let copies in flight land before the block exits
+    return;
   }
   __syncthreads();
   for (int t = tid; t < nl * nx; t += blockDim.x) {
     const int p = t / nx, m = t - p * nx;
-    const double *r0 = in + (size_t)2 * p * nx, *r1 = r0 + nx;
+    const double *r0 = in + (size_t)2 * p * sy + 1, *r1 = r0 + sy;
     const int im = sinq ? nx - 1 - m : m, ic = sinq ? m - 1 : nx - m;  // x_m, x_{N-m} (SINQF: reversed row)
     const double a0 = r0[im], a1 = r1[im];
     const double b0 = m ? r0[ic] : 0.0, b1 = m ? r1[ic] : 0.0;
@@ -1859,24 +1883,37 @@ __global__ void __launch_bounds__(256) k_xnp_qbwd(TGDev d, TGDev s, FFTPlan pl, 
                                                   int sinq) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ int rad[16];
+  __shared__ uint64_t bar;
   const int nx = d.nx, ny = d.ny, k = blockIdx.y, jbeg = 1 + blockIdx.x * lb;
   const int nrow = min(lb, ny - jbeg + 1), nl = lb / 2, tid = threadIdx.x;
   double2 *A = reinterpret_cast<double2 *>(smem_raw);
   double *in = reinterpret_cast<double *>(smem_raw + align128(xq_cplx(nx, lb) * sizeof(double2)));
   double2 *B = reinterpret_cast<double2 *>(in);
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
   if (tid < 16) rad[tid] = pl.rad[tid];
-  const double *S = reinterpret_cast<const double *>(s.spec);
-  for (int t = tid; t < lb * nx; t += blockDim.x) {
-    const int r = t / nx, m = t - r * nx;
-    double x = r < nrow ? S[m + 2 * (int64_t)s.lp * ((jbeg + r - 1) + (int64_t)ny * k)] : 0.0;
-    if (sinq && (m & 1)) x = -x;  // SINQB: (-1)^n X_n
-    in[t] = x;
+  __syncthreads();
+  // the block's packed spectral rows (nx values each, 16-byte aligned: the
+  // pitch 2 lp is a multiple of 4) by one bulk copy each
+  const uint32_t rowb = (uint32_t)(nx * sizeof(double));
+  if (tid == 0) mbar_expect_tx(&bar, rowb * (uint32_t)nrow);
+  __syncthreads();
+  const double *S = reinterpret_cast<const double *>(s.spec) + 2 * (int64_t)s.lp * ((jbeg - 1) + (int64_t)ny * k);
+  for (int r = tid; r < nrow; r += blockDim.x)
+    bulk_g2s(in + (size_t)r * nx, S + 2 * (int64_t)s.lp * r, rowb, &bar);
+  for (int t = tid; t < (lb - nrow) * nx; t += blockDim.x) in[(size_t)nrow * nx + t] = 0.0;
+  if (!mbar_wait(&bar, 0, d.err)) {
+    mbar_wait(&bar, 0, d.err);  // let copies in flight land before the block exits
+    return;
   }
   __syncthreads();
   for (int t = tid; t < nl * nx; t += blockDim.x) {
     const int p = t / nx, n = t - p * nx;
     const int q = 2 * n < nx ? 2 * n : 2 * (nx - 1 - n) + 1;  // v_n = X_{2n}, v_{N-1-n} = X_{2n+1}
-    A[swz(p * nx + n)] = make_double2(in[(size_t)2 * p * nx + q], in[(size_t)(2 * p + 1) * nx + q]);
+    const double sg = (sinq && (q & 1)) ? -1.0 : 1.0;          // SINQB: (-1)^n X_n
+    A[swz(p * nx + n)] = make_double2(sg * in[(size_t)2 * p * nx + q], sg * in[(size_t)(2 * p + 1) * nx + q]);
   }
   __syncthreads();
   const double2 *res = fft_lines<double2, BIG>(A, B, nl, nx, nx, rad, pl.nrad, pl.tw64, -1);
