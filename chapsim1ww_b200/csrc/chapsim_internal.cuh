@@ -260,6 +260,7 @@ int io_correction(chapsim_ctx *c, int ns);
 int io_init_maps(chapsim_ctx *c);
 int io_refresh_msum(chapsim_ctx *c);
 int io_restart_fields(chapsim_ctx *c);
+int io_np_restart(chapsim_ctx *c);  // the coupled section's restart sequence
 // learned properties (io_kernels.cu): THERM_PROP_UPDATE(IMAIND) by the table
 // or the model; kernel attributes; persistent grid size
 int io_therm_props(chapsim_ctx *c, int mode);

@@ -14,6 +14,9 @@
 // (TEMPERATURE, DENSITY, ENTHALPY).  An IO section that runs beside a TG
 // section writes DNS_perioz_INSTANT_T... instead (WRT_VARS_IO.f90:24-28,
 // RESTART_io.f90:25-29), so the two sections never overwrite each other.
+// The coupled inflow / outflow section (x ghost columns) writes and reads
+// I = 1..NCL1E = NCL1_io + 1, its outlet ghost column included, with NCL1E in
+// the header (WRT_VARS_IO.f90:21-60, RESTART_io.f90:16-47).
 #include <cuda_runtime.h>
 #include <stdio.h>
 #include <string.h>
@@ -146,10 +149,10 @@ extern "C" {
 
 int chapsim_write_instant(chapsim_ctx *ctx, const char *dir, int iteration, double time) {
   if (!ctx) return CHAPSIM_ERR_ARG;
-  if (ctx->xnp) return CHAPSIM_ERR_UNSUPPORTED;  // files of the x-periodic layout only
   if (cudaSetDevice(ctx->device) != cudaSuccess) return CHAPSIM_ERR_CUDA;
   TGDev &d = ctx->d;
   const bool io = ctx->domain == CHAPSIM_IIO;
+  const int xo = ctx->xoff, nxf = d.nx + xo;  // the file's x extent: NCL1E
   std::vector<const double *> src = io ? std::vector<const double *>{ctx->io.g[ctx->io_cur][0],
                                                                    ctx->io.g[ctx->io_cur][1],
                                                                    ctx->io.g[ctx->io_cur][2], d.p}
@@ -159,13 +162,18 @@ int chapsim_write_instant(chapsim_ctx *ctx, const char *dir, int iteration, doub
     src.insert(src.end(), {ctx->io.T, ctx->io.D, ctx->io.h});
     names.insert(names.end(), {"T", "D", "E"});
   }
-  std::vector<double> host;
+  std::vector<double> host, cols;
   for (size_t q = 0; q < src.size(); ++q) {
-    int rc = download(ctx, src[q], host);
+    int rc = download(ctx, src[q] - xo, host);
     if (rc) return rc;
-    const std::string path = file_name(dir, time, names[q], io && ctx->iocfg.coupled);
-    rc = chapsim_instant_file_write(path.c_str(), d.nx, d.ny, d.nz, iteration, time, ctx->cfg.ren, ctx->cfg.dt,
-                                    host.data());
+    if (xo) {  // columns IC = 1 .. NCL1_io + 1 of every row
+      cols.resize((size_t)nxf * (d.ny + 2) * d.nz);
+      for (size_t r = 0; r < (size_t)(d.ny + 2) * d.nz; ++r)
+        memcpy(cols.data() + r * nxf, host.data() + r * d.sy + 1, (size_t)nxf * sizeof(double));
+    }
+    const std::string path = file_name(dir, time, names[q], io && (ctx->iocfg.coupled || ctx->xnp));
+    rc = chapsim_instant_file_write(path.c_str(), nxf, d.ny, d.nz, iteration, time, ctx->cfg.ren, ctx->cfg.dt,
+                                    xo ? cols.data() : host.data());
     if (rc) {
       ctx->err = "cannot write " + path;
       return rc;
@@ -176,11 +184,15 @@ int chapsim_write_instant(chapsim_ctx *ctx, const char *dir, int iteration, doub
 
 int chapsim_read_instant(chapsim_ctx *ctx, const char *dir, double time, int *iteration, double *time_out) {
   if (!ctx) return CHAPSIM_ERR_ARG;
-  if (ctx->xnp) return CHAPSIM_ERR_UNSUPPORTED;  // files of the x-periodic layout only
   if (cudaSetDevice(ctx->device) != cudaSuccess) return CHAPSIM_ERR_CUDA;
   TGDev &d = ctx->d;
   const bool io = ctx->domain == CHAPSIM_IIO;
   const size_t n = (size_t)d.sz * d.nz;
+  const int xo = ctx->xoff, nxf = d.nx + xo;  // the file's x extent: NCL1E
+  if (xo && !ctx->inlet) {
+    ctx->err = "coupled IO restart needs its TG inlet source (chapsim_io_set_inlet)";
+    return CHAPSIM_ERR_STATE;
+  }
   std::vector<double> f[7];
   const char *names[7] = {"U", "V", "W", "P", "T", "D", "E"};
   const int nf = (io && ctx->io.thermal) ? 7 : 4;
@@ -190,17 +202,26 @@ int chapsim_read_instant(chapsim_ctx *ctx, const char *dir, double time, int *it
   }
   int it = 0;
   double tm = 0.0;
+  std::vector<double> cols;
   for (int q = 0; q < nf; ++q) {
     f[q].assign(n, 0.0);
-    const std::string path = file_name(dir, time, names[q], io && ctx->iocfg.coupled);
-    const int rc = chapsim_instant_file_read(path.c_str(), d.nx, d.ny, d.nz, &it, &tm, nullptr, nullptr, f[q].data());
+    const std::string path = file_name(dir, time, names[q], io && (ctx->iocfg.coupled || ctx->xnp));
+    if (xo) cols.assign((size_t)nxf * (d.ny + 2) * d.nz, 0.0);
+    const int rc = chapsim_instant_file_read(path.c_str(), nxf, d.ny, d.nz, &it, &tm, nullptr, nullptr,
+                                             xo ? cols.data() : f[q].data());
     if (rc) {
       ctx->err = "cannot read " + path + " (missing, or written for another mesh)";
       return rc;
     }
+    if (xo)  // into columns IC = 1 .. NCL1_io + 1 of the ghost-column rows
+      for (size_t r = 0; r < (size_t)(d.ny + 2) * d.nz; ++r)
+        memcpy(f[q].data() + r * d.sy + 1, cols.data() + r * nxf, (size_t)nxf * sizeof(double));
   }
-  wall_bc_vec(d, f);
-  wall_bc_copy(d, f[3]);
+  // wall rows over every stored column (from the first one of the allocation)
+  TGDev dw = d;
+  dw.nx = (int)d.sy;
+  wall_bc_vec(dw, f);
+  wall_bc_copy(dw, f[3]);
   int rc;
   const size_t bytes = n * sizeof(double);
   if (!io) {
@@ -217,28 +238,33 @@ int chapsim_read_instant(chapsim_ctx *ctx, const char *dir, double time, int *it
     // PR from U, V, W, P; T, D, E, RHOH = D E; then the wall ghosts, the
     // property update and u = G / rho_stag.  G0_io, EXPLT0_io and
     // RHS_ENERGY0 start at zero as after the reference's allocation.
+    // The coupled section's arrays are addressed from their first (ghost)
+    // column; its BC_CONV0 terms restart at zero too.
     IODev &iv = ctx->io;
     ctx->io_cur = 0;
     for (int q = 0; q < 3; ++q) {
-      if ((rc = upload(ctx, iv.g[0][q], f[q]))) return rc;
-      if (cudaMemsetAsync(iv.g[1][q], 0, bytes, ctx->stream) != cudaSuccess) return CHAPSIM_ERR_CUDA;
-      if (cudaMemsetAsync(d.h0[q], 0, bytes, ctx->stream) != cudaSuccess) return CHAPSIM_ERR_CUDA;
+      if ((rc = upload(ctx, iv.g[0][q] - xo, f[q]))) return rc;
+      if (cudaMemsetAsync(iv.g[1][q] - xo, 0, bytes, ctx->stream) != cudaSuccess) return CHAPSIM_ERR_CUDA;
+      if (cudaMemsetAsync((double *)d.h0[q] - xo, 0, bytes, ctx->stream) != cudaSuccess) return CHAPSIM_ERR_CUDA;
     }
-    if ((rc = upload(ctx, d.p, f[3]))) return rc;
+    if ((rc = upload(ctx, d.p - xo, f[3]))) return rc;
     double *zero[] = {d.phi, d.rhsphi, iv.drho, iv.rhse0};
     for (double *z : zero)
-      if (cudaMemsetAsync(z, 0, bytes, ctx->stream) != cudaSuccess) return CHAPSIM_ERR_CUDA;
+      if (cudaMemsetAsync(z - xo, 0, bytes, ctx->stream) != cudaSuccess) return CHAPSIM_ERR_CUDA;
     if (iv.visc)
       for (int q = 0; q < 3; ++q)
         if (cudaMemsetAsync(iv.drhoi[q], 0, bytes, ctx->stream) != cudaSuccess) return CHAPSIM_ERR_CUDA;
+    if (xo && cudaMemsetAsync(iv.bcp + (size_t)iv.bps * CHAPSIM_P_CONV0_X, 0, (size_t)iv.bps * 4 * sizeof(double),
+                              ctx->stream) != cudaSuccess)
+      return CHAPSIM_ERR_CUDA;
     if (iv.thermal) {
       std::vector<double> rhoh(n, 0.0);
       for (size_t t = 0; t < n; ++t) rhoh[t] = f[5][t] * f[6][t];
-      if ((rc = upload(ctx, iv.T, f[4])) || (rc = upload(ctx, iv.D, f[5])) || (rc = upload(ctx, iv.h, f[6])) ||
-          (rc = upload(ctx, iv.rhoh, rhoh)))
+      if ((rc = upload(ctx, iv.T - xo, f[4])) || (rc = upload(ctx, iv.D - xo, f[5])) ||
+          (rc = upload(ctx, iv.h - xo, f[6])) || (rc = upload(ctx, iv.rhoh - xo, rhoh)))
         return rc;
     }
-    if ((rc = io_restart_fields(ctx))) return rc;
+    if ((rc = xo ? io_np_restart(ctx) : io_restart_fields(ctx))) return rc;
     if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return CHAPSIM_ERR_CUDA;
   }
   for (auto &g : ctx->io_graph)

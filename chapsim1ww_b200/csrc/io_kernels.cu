@@ -1822,6 +1822,43 @@ __global__ void k_np_eng_pre(TGDev d, IODev io) {
   bplane(io, CHAPSIM_P_OUT_K)[t] = io.kap[co];
 }
 
+// Restart of the coupled section: BC_TINLET_THERML's reference state on the
+// inlet ghost column IC = 0 (src/BC_INLET.f90:54-76), with DENSITY0 and
+// VISCOUSITY0 equal to it.
+__global__ void k_np_restart_inlet(TGDev d, IODev io) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (d.ny + 2) * d.nz) return;
+  const int k = t / (d.ny + 2), j = t - k * (d.ny + 2);
+  const int64_t ci = col(d, -1, j, k);
+  io.T[ci] = 1.0;
+  io.kap[ci] = 1.0;
+  io.D[ci] = 1.0;
+  io.D0[ci] = 1.0;
+  io.mu[ci] = 1.0;
+  io.mu0[ci] = 1.0;
+  io.msum[ci] = 2.0;
+  io.h[ci] = 0.0;
+  io.rhoh[ci] = 0.0;
+}
+
+// Restart of the coupled section: u, v, w of the outlet ghost column from its
+// G and the outlet-face density 0.5 (rho(NCL1_io) + rho(NCL1_io + 1)), the
+// relation BC_COUTLET_MOM_RK3 keeps between them; zero on the wall rows.  The
+// reference leaves Q_io(NCL1_io + 1) at its allocation value here, which
+// halves U_OUTLET in the first substep after a restart; this rebuilds it so
+// that a restart continues the run.
+__global__ void k_np_restart_outlet(TGDev d, IODev io, int cur) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (d.ny + 2) * d.nz) return;
+  const int k = t / (d.ny + 2), j = t - k * (d.ny + 2);
+  const int64_t co = col(d, d.nx, j, k), cl = col(d, d.nx - 1, j, k);
+  double *q3[3] = {d.u, d.v, d.w};
+  const bool wall = j == 0 || j == d.ny + 1;
+  const double rho = (io.D[cl] + io.D[co]) * 0.5;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) q3[q][co] = (wall || (q == 1 && j == 1)) ? 0.0 : io.g[cur][q][co] / rho;
+}
+
 __global__ void k_np_eng_post(TGDev d, IODev io) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (d.ny + 2) * d.nz) return;
@@ -1894,6 +1931,46 @@ int io_np_eng_bc(chapsim_ctx *c, int ns) {
   int rc = io_bc_outlet_eng(c, ns);
   if (rc) return rc;
   k_np_eng_post<<<nb, 256, 0, c->stream>>>(d, c->io);
+  LAUNCHED();
+  return CHAPSIM_OK;
+}
+
+// RESTART_INSTANT_VARS_IO of the coupled section (src/processing/RESTART_io.f90:
+// 80-120 with TGFLOWFLG) once G, PR (and T, DENSITY, ENTHALPY, RHOH) of
+// IC = 1 .. NCL1_io + 1 are in place: BC_WALL_THERMAL and THERM_PROP_UPDATE
+// over those columns (rho0 = rho, mu0 = mu), BC_TINLET_THERML, BC_TINLET_FLOW
+// from the TG context, the outlet column's velocity, then DENSITY_Staggered,
+// MU_Staggered and VELOCITY_CALC_io on the interior.
+int io_np_restart(chapsim_ctx *c) {
+  TGDev &d = c->d;
+  IODev &io = c->io;
+  if (!c->inlet) {
+    c->err = "coupled IO section without its TG inlet source (chapsim_io_set_inlet)";
+    return CHAPSIM_ERR_STATE;
+  }
+  TGDev e = d;
+  e.nx = d.nx + 1;  // IC = 1 .. NCL1_io + 1 from the field pointers
+  if (io.thermal) {
+    k_io_eng_ghost<<<dim3((e.nx * e.nz + 127) / 128, 2), 128, 0, c->stream>>>(e, io);
+    LAUNCHED();
+  }
+  const dim3 blk(IO_BX, IO_BY), g2((e.nx + IO_BX - 1) / IO_BX, (d.ny + 2 + IO_BY - 1) / IO_BY, d.nz);
+  k_io_props_only<<<g2, blk, 0, c->stream>>>(e, io);
+  LAUNCHED();
+  const int nb = ((d.ny + 2) * d.nz + 255) / 256, cur = c->io_cur;
+  if (io.thermal) {
+    k_np_restart_inlet<<<nb, 256, 0, c->stream>>>(d, io);
+    LAUNCHED();
+  }
+  k_np_mom_pre<<<nb, 256, 0, c->stream>>>(d, io, cur);  // the outlet planes hold the outlet column
+  LAUNCHED();
+  int rc = io_bc_inlet(c, c->inlet);
+  if (rc) return rc;
+  k_np_mom_post<<<nb, 256, 0, c->stream>>>(d, io, cur);
+  LAUNCHED();
+  k_np_restart_outlet<<<nb, 256, 0, c->stream>>>(d, io, cur);
+  LAUNCHED();
+  k_io_prep<false><<<cell_grid(d), blk, 0, c->stream>>>(d, io, 0.0, 0.0, 1.0, cur, 0, 0);
   LAUNCHED();
   return CHAPSIM_OK;
 }

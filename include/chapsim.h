@@ -247,7 +247,13 @@ int chapsim_stats_reset(chapsim_ctx *ctx);
  * restarts from such files (RESTART_INSTANT_VARS_TG / _IO + FLOWSTART's wall
  * conditions; TG: CONVH0 = 0; IO: RHOH = D E, wall ghosts, THERM_PROP_UPDATE,
  * rho0 = rho, mu0 = mu, u = G / rho_stag, G0 = EXPLT0 = RHS_ENERGY0 = 0) and
- * returns the file's iteration and time.  A mesh other than the context's is
+ * returns the file's iteration and time.  The coupled inflow / outflow
+ * section (non-periodic bcx_in / bcx_out) writes DNS_perioz files of
+ * I = 1..NCL1E = nx + 1 (its outlet ghost column; NCL1E in the header) and
+ * restarts from them with its inlet source set (chapsim_io_set_inlet, the TG
+ * context restarted first): BC_TINLET_THERML and BC_TINLET_FLOW fill the
+ * inlet ghost column, the outlet column's u, v, w = G / its face density,
+ * the BC_CONV0 terms = 0.  A mesh other than the context's is
  * refused (the reference's interpolation, INTP_3D_VARS, is not built).  The
  * *_file_* calls do the same on host arrays in the F(1:nx, 0:ny+1, 1:nz)
  * layout (ghost rows untouched) and need no GPU. */

@@ -12,6 +12,7 @@ inlet face carries the TG's first face exactly, and the IO section's
 divergence vanishes to round-off in every column but the first.
 """
 import math
+import os
 
 import numpy as np
 import pytest
@@ -152,8 +153,8 @@ def test_coupled_graph_equals_eager_substeps():
 
 def test_coupled_section_refusals():
     """What the coupled section does not run: a step without its inlet
-    source, the x-periodic statistics, instantaneous-field files, the
-    learned property kernel and the stand-alone boundary operators."""
+    source, the x-periodic statistics, the learned property kernel and the
+    stand-alone boundary operators."""
     _need_gpu()
     from chapsim1ww_b200 import ChapsimError, IOChannel, TGChannel, _lib
     g = IOChannel(16, 12, 8, table=_table("constant"), bcx=(2, 1))
@@ -179,3 +180,53 @@ def test_coupled_section_refusals():
     with pytest.raises(ChapsimError):
         g.solverrk3_mom_io(1)
     g.close()
+
+
+def test_coupled_restart_files_and_continuation(tmp_path):
+    """WRT_INSTANT_VARS_IO / RESTART_INSTANT_VARS_IO of the coupled section
+    (src/processing/WRT_VARS_IO.f90:21-60, RESTART_io.f90:16-120): files of
+    I = 1..NCL1_io + 1 (the outlet ghost column included, NCL1E in the
+    header) named DNS_perioz beside the TG section's DNS_perixz files; the
+    restarted section holds the written G, p, T, rho, h on those columns and
+    the TG's last column in its inlet ghost column, and one step from the
+    restarted state agrees with the oracle given that state."""
+    from chapsim1ww_b200 import IOChannel, TGChannel
+    from oracle.pyoracle import OracleIO, OracleTG
+    d = str(tmp_path) + "/"
+    nxt, nxi, ny, nz = 16, 24, 16, 12
+    lz = 4 * math.pi / 3
+    tg, ot, g, o = _pair(nxt, nxi, ny, nz, thermal=1, table="synthetic")
+    g.step_coupled(tg, 2)
+    tg.write_instant(d, 6, 0.006)
+    g.write_instant(d, 6, 0.006)
+    names = sorted(os.listdir(d))
+    assert sum(n.startswith("DNS_perixz") for n in names) == 4
+    assert sum(n.startswith("DNS_perioz") for n in names) == 7
+    u_file = [n for n in names if n.startswith("DNS_perioz") and n.endswith("_U.D")][0]
+    hdr = np.fromfile(d + u_file, dtype=np.int32, count=4)
+    assert tuple(int(x) for x in hdr) == (nxi + 1, ny, nz, 6)
+    assert os.path.getsize(d + u_file) == 16 + 24 + 8 * (nxi + 1) * ny * nz
+    tg2 = TGChannel(nxt, ny, nz, lz=lz)
+    g2 = IOChannel(nxi, ny, nz, lz=lz, table=_table("synthetic"), bcx=(2, 1))
+    g2.set_inlet(tg2)
+    assert tg2.read_instant(d, 0.006) == (6, 0.006)
+    assert g2.read_instant(d, 0.006) == (6, 0.006)
+    for n in ("gx", "gy", "gz", "p", "t", "rho", "h"):
+        assert relerr(g2.get_field(n)[:, 1:-1, 1:], g.get_field(n)[:, 1:-1, 1:]) <= 1e-14, n
+    u2, tu2 = g2.get_field("u"), tg2.get_field("u")
+    assert np.array_equal(u2[:, :, 0], tu2[:, :, -1])
+    # the first face: BC_TINLET_FLOW's G, then VELOCITY_CALC_io's G / RHO_STG
+    assert relerr(u2[:, 1:-1, 1], tu2[:, 1:-1, 0]) <= 1e-14
+    ot2 = OracleTG(nxt, ny, nz, lz=lz)
+    for n in TG_F:
+        ot2.set(n, tg2.get_field(n))
+    o2 = OracleIO(nxi, ny, nz, lz=lz, thermal=1, table=_table("synthetic"))
+    o2.set_bcx(2, 1)
+    o2.set_inlet(*[ot2.get(f) for f in TG_F])
+    for n in IO_FLOW + IO_THERMAL:
+        o2.set(n, g2.get_field(n))
+    g2.step_coupled(tg2, 1)
+    _oracle_steps(ot2, o2, 1)
+    _compare(tg2, ot2, g2, o2, 1, "one step after the restart")
+    tg.close()
+    tg2.close()
